@@ -1,0 +1,141 @@
+/*
+ * helm_b200.h -- C ABI of the B200 (sm_100a) pseudo-spectral Helmholtz solver.
+ *
+ * Solves (d2/dx2 + d2/dy2 [+ d2/dz2] - lambda) u = f with Fourier collocation
+ * in the periodic directions and Gauss-Lobatto-Legendre (GLL) collocation in the
+ * last direction, with Robin conditions alpha du/dn + beta u = g (outward
+ * normal) at both ends of the GLL direction:
+ *     bottom:  betal u - alphal du/dy = gl        top:  betar u + alphar du/dy = gr
+ * exactly as the reference's DirectPseudoSpectral solvers do.  The solve is an
+ * FFT along the periodic directions, one collocation system per wavenumber, an
+ * element-interface tridiagonal sweep, and the inverse FFT.
+ *
+ * Every entry point returns an int status (HELM_OK = 0); none aborts.  All
+ * array arguments of the solve calls are DEVICE pointers on the plan's device;
+ * `stream` is a cudaStream_t passed as void* (NULL = legacy default stream).
+ *
+ * Array layouts (row-major, GLL index fastest, as the reference stores them):
+ *   2D   f, u : [Ns][Nx][N]        gl, gr : [Nx]
+ *   3D   f, u : [Ns][Nx][Ny][N]    gl, gr : [Nx][Ny]
+ * with the strides of helm_plan_set_layout (default: compact).  The reference's
+ * own arrays (rhsPDE[Ns][2Nx][N], U.phi[2Nx][N]; 3D [Ns][2Nx][2Ny][N],
+ * leftBC[2Nx][2Ny]) are addressed by passing their strides.  f is read only at
+ * the interior GLL nodes of each element, like the reference (its boundary
+ * slots carry no equation).
+ *
+ * Grid convention kept from the reference: the GLL nodes of element jj lie on
+ * [jj*L/Ns, (jj+1)*L/Ns] measured from 0 (not from the user's lower bound), and
+ * x_i = xl + i*Lx/Nx.  helm_plan_get_grid returns the nodes.
+ */
+#ifndef HELM_B200_H
+#define HELM_B200_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes (the reference calls ErrorMessage -> exit(1) instead) ---- */
+enum {
+    HELM_OK = 0,
+    HELM_ERR_INVALID = 1,     /* bad size / argument / NULL pointer                      */
+    HELM_ERR_NOT_POW2 = 2,    /* Fourier size not a power of 2 (Fourier_Quadrature.cpp:429-432) */
+    HELM_ERR_SINGULAR = 3,    /* a shifted GLL operator is singular (LU_Decomposition.cpp:49-50) */
+    HELM_ERR_OOM = 4,         /* device or host allocation failed (General.h:311-312)     */
+    HELM_ERR_CUDA = 5,        /* a CUDA call or kernel launch failed                       */
+    HELM_ERR_UNSUPPORTED = 6, /* combination not built (e.g. size beyond the kernels' range) */
+    HELM_ERR_NO_DEVICE = 7    /* no usable CUDA device                                     */
+};
+
+/* ---- arithmetic of the solve ---- */
+enum {
+    HELM_FP64 = 0,        /* FFTs, back-solves and epilogue in FP64                       */
+    HELM_FP32 = 1,        /* everything in FP32 (FP32 factors, FP32 spectrum)             */
+    HELM_FP32_REFINE = 2  /* FP64 FFTs; FP32 back-solves with FP64-residual refinement   */
+};
+
+/* ---- per-wavenumber solve method ---- */
+enum {
+    HELM_METHOD_AUTO = 0, /* the autotuner's choice for this shape                        */
+    HELM_METHOD_LU = 1,   /* per-wavenumber LU with scaled partial pivoting (the reference's) */
+    HELM_METHOD_FDM = 2   /* fast diagonalisation of the interior GLL operator            */
+};
+
+typedef struct helm_plan_s* helm_plan_t;
+
+/* Robin coefficients of the two ends of the GLL direction (the reference's
+ * globals alphal, betal, alphar, betar; NonPeriodic2D_MPI.h:27). */
+typedef struct {
+    double alphal, betal, alphar, betar;
+} helm_robin_t;
+
+/* Replaces CreatePDEPlan(Nx,Ny,N,xl,xr,yl,yr) + CreateFFTPlan(Nx)
+ * (NonPeriodic2D_MPI.h:33, Fourier_Quadrature.h:43) together with the
+ * reference's globals Lambda/alphal..betar and its ConstructOperator callback
+ * (TestNonPeriodic2D_MPI.cpp:67-74): every shifted operator is built and
+ * factored here, once, in FP64.  Ny/N elements: Ns = ceil(Ny/N)
+ * (NonPeriodic2D_MPI.cpp:62, one rank).  bc == NULL means Dirichlet (0,1,0,1). */
+int helm2d_plan_create(int Nx, int Ny, int N, double xl, double xr, double yl, double yr,
+                       const helm_robin_t* bc, double lambda, int precision, int method,
+                       helm_plan_t* plan);
+
+/* Replaces CreatePDEPlan(Nx,Ny,Nz,N,xl,xr,yl,yr,zl,zr) + CreateFFTPlan(max(Nx,Ny))
+ * (NonPeriodic3D_MPI.h:33) with the operator of TestNonPeriodic3D_MPI.cpp:71-79. */
+int helm3d_plan_create(int Nx, int Ny, int Nz, int N, double xl, double xr, double yl, double yr,
+                       double zl, double zr, const helm_robin_t* bc, double lambda, int precision,
+                       int method, helm_plan_t* plan);
+
+/* Strides (in elements) of f/u and of gl/gr; 0 keeps the compact value.
+ *   x_stride    : between consecutive x rows of f and u   (compact: N in 2D, Ny*N in 3D)
+ *   elem_stride : between consecutive GLL elements         (compact: Nx*x_stride)
+ *   bc_x_stride : 3D only, between x rows of gl and gr     (compact: Ny)
+ * The reference's own arrays: 2D x_stride=N, elem_stride=2*Nx*N;
+ * 3D x_stride=2*Ny*N, elem_stride=2*Nx*2*Ny*N, bc_x_stride=2*Ny. */
+int helm_plan_set_layout(helm_plan_t plan, long long x_stride, long long elem_stride, long long bc_x_stride);
+
+/* Element type of f and u for HELM_FP32 plans: 8 (double, default) or 4 (float).
+ * FP64 and FP32_REFINE plans always read and write double. */
+int helm_plan_set_io_bytes(helm_plan_t plan, int bytes);
+
+/* Number of refinement sweeps of a HELM_FP32_REFINE plan (default 2, 0..8). */
+int helm_plan_set_refine_sweeps(helm_plan_t plan, int sweeps);
+
+/* SolvePDE(U, ConstructOperator) (NonPeriodic2D_MPI.cpp:228-474,
+ * NonPeriodic3D_MPI.cpp:237-591): u = solution, device pointers.  Unlike the
+ * reference, f is not overwritten by its spectrum.  gl/gr may be NULL (zero
+ * boundary data).  Asynchronous on `stream`. */
+int helm_solve(helm_plan_t plan, const void* f, const double* gl, const double* gr, void* u, void* stream);
+
+/* Adjoint of helm_solve as a linear map (f, gl, gr) -> u.  Given ubar = dL/du
+ * (same layout as u), writes fbar = dL/df (zero on the GLL boundary slots, which
+ * the solve never reads), glbar = dL/dgl, grbar = dL/dgr (any may be NULL), and,
+ * when lambda_bar != NULL, the scalar
+ *     dL/dlambda = sum over the interior collocation nodes of fbar * u
+ * (d(A u)/d lambda = -u on the interior rows, so du/dlambda = A^-1 u), where u
+ * must be the forward solution of the same plan; the sum is written to the
+ * DEVICE double *lambda_bar.  Ns = 1 plans.  No counterpart in the reference,
+ * which has no gradients. */
+int helm_solve_adjoint(helm_plan_t plan, const double* ubar, double* fbar, double* glbar, double* grbar,
+                       const double* u, double* lambda_bar, void* stream);
+
+/* Node coordinates: 2D y[Ns*(N-1)+1] / 3D z[...], and the scaled first and
+ * second GLL derivative matrices D[N*N], D2[N*N] (row-major), host pointers,
+ * any may be NULL.  The reference's globals y/z, Dy/Dz, Dyy/Dzz. */
+int helm_plan_get_grid(helm_plan_t plan, double* nodes, double* D, double* D2);
+
+/* Plan facts: Ns, the number of distinct shifted operators, the method the
+ * plan runs, and the device bytes it holds. */
+int helm_plan_info(helm_plan_t plan, int* Ns, int* n_operators, int* method, long long* device_bytes);
+
+/* Replaces DestroyPDEPlan() + DestroyFFTPlan(). NULL is accepted. */
+int helm_plan_destroy(helm_plan_t plan);
+
+/* Human-readable status text (static storage). */
+const char* helm_status_string(int status);
+
+/* Last CUDA error text recorded by this library on the calling thread. */
+const char* helm_last_error(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* HELM_B200_H */

@@ -1,0 +1,91 @@
+"""ctypes binding of the C ABI in include/helm_b200.h (libhelm_b200.so, built in-tree).
+
+There is no fallback: if the library is missing or cannot be loaded, every
+entry point raises.  Build it with ``python -m mpi_b200.build``.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libhelm_b200.so")
+
+HELM_OK = 0
+HELM_ERR_INVALID = 1
+HELM_ERR_NOT_POW2 = 2
+HELM_ERR_SINGULAR = 3
+HELM_ERR_OOM = 4
+HELM_ERR_CUDA = 5
+HELM_ERR_UNSUPPORTED = 6
+HELM_ERR_NO_DEVICE = 7
+
+HELM_FP64 = 0
+HELM_FP32 = 1
+HELM_FP32_REFINE = 2
+
+HELM_METHOD_AUTO = 0
+HELM_METHOD_LU = 1
+HELM_METHOD_FDM = 2
+
+# Every symbol the header declares (tests check the library exports them all).
+EXPORTS = (
+    "helm2d_plan_create", "helm3d_plan_create", "helm_plan_set_layout", "helm_plan_set_io_bytes",
+    "helm_plan_set_refine_sweeps", "helm_solve", "helm_solve_adjoint", "helm_plan_get_grid",
+    "helm_plan_info", "helm_plan_destroy", "helm_status_string", "helm_last_error",
+)
+
+
+class HelmError(RuntimeError):
+    def __init__(self, status: int, where: str):
+        self.status = status
+        lib = _lib
+        msg = lib.helm_status_string(status).decode() if lib else str(status)
+        last = lib.helm_last_error().decode() if lib else ""
+        super().__init__(f"{where}: {msg} ({status})" + (f" [{last}]" if last else ""))
+
+
+class robin_t(ctypes.Structure):
+    _fields_ = [("alphal", ctypes.c_double), ("betal", ctypes.c_double),
+                ("alphar", ctypes.c_double), ("betar", ctypes.c_double)]
+
+
+_lib = None
+
+
+def lib() -> ctypes.CDLL:
+    """Load libhelm_b200.so (raises when it is absent: no CPU fallback exists)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise ImportError(f"{LIB_PATH} is missing; build it with `python -m mpi_b200.build`")
+    L = ctypes.CDLL(LIB_PATH)
+    i, d, ll, vp = ctypes.c_int, ctypes.c_double, ctypes.c_longlong, ctypes.c_void_p
+    P = ctypes.POINTER
+    L.helm2d_plan_create.argtypes = [i, i, i, d, d, d, d, P(robin_t), d, i, i, P(vp)]
+    L.helm3d_plan_create.argtypes = [i, i, i, i, d, d, d, d, d, d, P(robin_t), d, i, i, P(vp)]
+    L.helm_plan_set_layout.argtypes = [vp, ll, ll, ll]
+    L.helm_plan_set_io_bytes.argtypes = [vp, i]
+    L.helm_plan_set_refine_sweeps.argtypes = [vp, i]
+    L.helm_solve.argtypes = [vp, vp, vp, vp, vp, vp]
+    L.helm_solve_adjoint.argtypes = [vp, vp, vp, vp, vp, vp, vp, vp]
+    L.helm_plan_get_grid.argtypes = [vp, vp, vp, vp]
+    L.helm_plan_info.argtypes = [vp, P(i), P(i), P(i), P(ll)]
+    L.helm_plan_destroy.argtypes = [vp]
+    L.helm_status_string.argtypes = [i]
+    L.helm_status_string.restype = ctypes.c_char_p
+    L.helm_last_error.argtypes = []
+    L.helm_last_error.restype = ctypes.c_char_p
+    for name in EXPORTS:
+        f = getattr(L, name)
+        if f.restype is None or f.restype is ctypes.c_int:
+            if name not in ("helm_status_string", "helm_last_error"):
+                f.restype = ctypes.c_int
+    _lib = L
+    return L
+
+
+def check(status: int, where: str) -> None:
+    if status != HELM_OK:
+        raise HelmError(status, where)

@@ -1,0 +1,103 @@
+// Device building blocks of the Helmholtz kernels: complex arithmetic on
+// float2/double2, in-register power-of-2 DFTs, and one Stockham pass of a
+// batched strided-axis FFT held in shared memory.
+#pragma once
+#include <cuda_runtime.h>
+#include <cstdint>
+
+namespace helm {
+
+template <typename T> struct cplx_of;
+template <> struct cplx_of<float> { using type = float2; };
+template <> struct cplx_of<double> { using type = double2; };
+template <typename T> using cplx_t = typename cplx_of<T>::type;
+
+__device__ __forceinline__ float2 mk(float a, float b) { return make_float2(a, b); }
+__device__ __forceinline__ double2 mk(double a, double b) { return make_double2(a, b); }
+__device__ __forceinline__ float2 operator+(float2 a, float2 b) { return make_float2(a.x + b.x, a.y + b.y); }
+__device__ __forceinline__ float2 operator-(float2 a, float2 b) { return make_float2(a.x - b.x, a.y - b.y); }
+__device__ __forceinline__ double2 operator+(double2 a, double2 b) { return make_double2(a.x + b.x, a.y + b.y); }
+__device__ __forceinline__ double2 operator-(double2 a, double2 b) { return make_double2(a.x - b.x, a.y - b.y); }
+template <typename C, typename T> __device__ __forceinline__ C cscale(C a, T s) { return mk(a.x * s, a.y * s); }
+// a * b
+template <typename C> __device__ __forceinline__ C cmul(C a, C b)
+{
+    return mk(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+// a * conj(b)
+template <typename C> __device__ __forceinline__ C cmulc(C a, C b)
+{
+    return mk(a.x * b.x + a.y * b.y, a.y * b.x - a.x * b.y);
+}
+
+// cos and sin of 2*pi*m/16 for m = 0..7 (exact constants of the 16th roots of unity).
+__device__ __forceinline__ double root16_cos(int m)
+{
+    const double c[8] = {1.0, 0.92387953251128675613, 0.70710678118654752440, 0.38268343236508977173,
+                         0.0, -0.38268343236508977173, -0.70710678118654752440, -0.92387953251128675613};
+    return c[m];
+}
+__device__ __forceinline__ double root16_sin(int m)
+{
+    const double s[8] = {0.0, 0.38268343236508977173, 0.70710678118654752440, 0.92387953251128675613,
+                         1.0, 0.92387953251128675613, 0.70710678118654752440, 0.38268343236508977173};
+    return s[m];
+}
+
+// d * exp(DIR * 2 pi i m / 16) for compile-time-foldable m in [0, 8).
+template <int DIR, typename T>
+__device__ __forceinline__ cplx_t<T> rot16(cplx_t<T> d, int m)
+{
+    if (m == 0) return d;
+    if (m == 4) return DIR < 0 ? mk(d.y, -d.x) : mk(-d.y, d.x);  // * (-i) or * (+i)
+    const T c = (T)root16_cos(m), s = (T)(DIR * root16_sin(m));
+    return mk(d.x * c - d.y * s, d.x * s + d.y * c);
+}
+
+__host__ __device__ constexpr int bitrev(int i, int R)
+{
+    int r = 0;
+    for (int b = 1; b < R; b <<= 1) { r = (r << 1) | (i & 1); i >>= 1; }
+    return r;
+}
+
+// In-register DFT of R = 2, 4, 8 or 16 points, natural order in and out:
+// v_m <- sum_j v_j exp(DIR * 2 pi i j m / R).  Radix-2 decimation in frequency
+// with a compile-time bit-reversal at the end.
+template <int R, int DIR, typename T>
+__device__ __forceinline__ void dft_reg(cplx_t<T> (&v)[R])
+{
+#pragma unroll
+    for (int len = R; len >= 2; len >>= 1) {
+        const int h = len >> 1;
+#pragma unroll
+        for (int s = 0; s < R; s += len) {
+#pragma unroll
+            for (int k = 0; k < h; ++k) {
+                cplx_t<T> a = v[s + k], b = v[s + k + h];
+                v[s + k] = a + b;
+                v[s + k + h] = rot16<DIR, T>(a - b, k * (16 / len));
+            }
+        }
+    }
+#pragma unroll
+    for (int i = 0; i < R; ++i) {
+        const int j = bitrev(i, R);
+        if (j > i) { cplx_t<T> t = v[i]; v[i] = v[j]; v[j] = t; }
+    }
+}
+
+// Radix schedule of a length-L transform: up to three passes of radix <= 16,
+// largest first.  L = 4 .. 4096.
+template <int L> struct Radix;
+template <> struct Radix<4> { static constexpr int n = 1, r0 = 4, r1 = 1, r2 = 1; };
+template <> struct Radix<8> { static constexpr int n = 1, r0 = 8, r1 = 1, r2 = 1; };
+template <> struct Radix<16> { static constexpr int n = 1, r0 = 16, r1 = 1, r2 = 1; };
+template <> struct Radix<32> { static constexpr int n = 2, r0 = 8, r1 = 4, r2 = 1; };
+template <> struct Radix<64> { static constexpr int n = 2, r0 = 8, r1 = 8, r2 = 1; };
+template <> struct Radix<128> { static constexpr int n = 2, r0 = 16, r1 = 8, r2 = 1; };
+template <> struct Radix<256> { static constexpr int n = 2, r0 = 16, r1 = 16, r2 = 1; };
+template <> struct Radix<512> { static constexpr int n = 3, r0 = 8, r1 = 8, r2 = 8; };
+template <> struct Radix<1024> { static constexpr int n = 3, r0 = 16, r1 = 8, r2 = 8; };
+
+}  // namespace helm

@@ -1,0 +1,680 @@
+// CUDA kernels of the Helmholtz solve (sm_100a):
+//   * fft_kernel  -- batched FFT along a strided (non-contiguous) axis, real-to-
+//     complex, complex-to-real or complex-to-complex, one tile of columns per
+//     CTA with the whole transform length staged in shared memory, radix-8/16
+//     Stockham passes in registers.  Replaces FourierTransformX / Y / XY
+//     (Fourier_Quadrature.cpp:516-609, 719-926, 1097-1155).
+//   * rows_kernel -- the per-wavenumber collocation solves of every spectrum
+//     row (ConstructFundamentalSolutions + LUSolve, NonPeriodic2D_MPI.cpp:176-223,
+//     LU_Decomposition.cpp:78-108), the element-interface tridiagonal sweep with
+//     the Robin ends (NonPeriodic2D_MPI.cpp:265-295, 414-424) and the combination
+//     u = phi + zl ul + zr ur (:466-470), fused, one warp per complex row.
+#include "helm_device.cuh"
+#include "helm_kernels.cuh"
+
+namespace helm {
+
+constexpr int FFT_THREADS = 256;
+
+template <typename T, int L>
+struct FftShape {
+    static constexpr int R0 = Radix<L>::r0, R1 = Radix<L>::r1, R2 = Radix<L>::r2, NP = Radix<L>::n;
+    static constexpr int TPC = L / R0;          // threads per column
+    static constexpr int CT = FFT_THREADS / TPC;  // columns per tile
+    static constexpr size_t smem = (size_t)L * CT * sizeof(cplx_t<T>);
+};
+
+template <int R, int DIR, typename T>
+__device__ __forceinline__ void dft_sub(cplx_t<T>* v)
+{
+    cplx_t<T> w[R];
+#pragma unroll
+    for (int r = 0; r < R; ++r) w[r] = v[r];
+    dft_reg<R, DIR, T>(w);
+#pragma unroll
+    for (int r = 0; r < R; ++r) v[r] = w[r];
+}
+
+// One Stockham pass (radix R, NS = product of the earlier radices) reading
+// shared memory: every thread loads, twiddles and transforms its R0/R items.
+template <typename T, int L, int R, int NS, int DIR, int TPC, int CT, int R0>
+__device__ __forceinline__ void pass_from_smem(const cplx_t<T>* sm, const cplx_t<T>* tw, int tc, int cl,
+                                               cplx_t<T> (&v)[R0])
+{
+    constexpr int IPT = R0 / R;
+#pragma unroll
+    for (int t = 0; t < IPT; ++t) {
+        const int j = tc + t * TPC;
+        const int jm = j % NS;
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+            cplx_t<T> x = sm[(j + r * (L / R)) * CT + cl];
+            if (NS > 1 && r > 0) {
+                const cplx_t<T> w = tw[r * jm * (L / (NS * R))];
+                x = (DIR < 0) ? cmul(x, w) : cmulc(x, w);
+            }
+            v[t * R + r] = x;
+        }
+        dft_sub<R, DIR, T>(&v[t * R]);
+    }
+}
+
+// Output row of item (t, r) of a pass with radix R and NS.
+template <int R, int NS, int TPC>
+__device__ __forceinline__ int pass_out_row(int tc, int t, int r)
+{
+    const int j = tc + t * TPC;
+    return (j / NS) * NS * R + (j % NS) + r * NS;
+}
+
+template <typename T, int L, int R, int NS, int TPC, int CT, int R0>
+__device__ __forceinline__ void pass_to_smem(cplx_t<T>* sm, int tc, int cl, const cplx_t<T> (&v)[R0])
+{
+#pragma unroll
+    for (int t = 0; t < R0 / R; ++t)
+#pragma unroll
+        for (int r = 0; r < R; ++r) sm[pass_out_row<R, NS, TPC>(tc, t, r) * CT + cl] = v[t * R + r];
+}
+
+template <typename T, typename TIO, int L, int DIR, int MODE>
+__global__ void __launch_bounds__(FFT_THREADS) fft_kernel(FftArgs a, long long total_cols)
+{
+    using C = cplx_t<T>;
+    using S = FftShape<T, L>;
+    constexpr int R0 = S::R0, R1 = S::R1, R2 = S::R2, NP = S::NP, TPC = S::TPC, CT = S::CT;
+    extern __shared__ __align__(16) unsigned char fft_smem[];
+    C* sm = reinterpret_cast<C*>(fft_smem);
+    const C* tw = static_cast<const C*>(a.tw);
+
+    const int tc = threadIdx.x / CT;
+    const int cl = threadIdx.x - tc * CT;
+    const long long g = (long long)blockIdx.x * CT + cl;
+    const bool valid = g < total_cols;
+    const int ccols = (MODE == FFT_C2C) ? a.ncols : (a.ncols + 1) >> 1;
+    const long long gg = valid ? g : 0;
+    const int b = (int)(gg / ccols);
+    const int c = (int)(gg - (long long)b * ccols);
+    const int c0 = 2 * c, c1 = 2 * c + 1;  // real columns of an R2C / C2R pair
+    const bool has1 = c1 < a.ncols;
+
+    C v[R0];
+    // ---------------------------------------------------------- pass 0 --
+    if constexpr (MODE == FFT_C2R) {
+        // Z_k = A_k + i B_k over the full length from the two half spectra
+        const C* in = static_cast<const C*>(a.in) + (long long)b * a.in_batch;
+        for (int k = tc; k <= L / 2; k += TPC) {
+            C A = mk((T)0, (T)0), B = mk((T)0, (T)0);
+            if (valid) {
+                A = in[(long long)k * a.in_row + c0];
+                if (has1) B = in[(long long)k * a.in_row + c1];
+            }
+            if (k == 0 || k == L / 2) { A.y = 0; B.y = 0; }
+            sm[k * CT + cl] = mk(A.x - B.y, A.y + B.x);
+            if (k != 0 && k != L / 2) sm[(L - k) * CT + cl] = mk(A.x + B.y, B.x - A.y);
+        }
+        __syncthreads();
+#pragma unroll
+        for (int r = 0; r < R0; ++r) v[r] = sm[(tc + r * TPC) * CT + cl];
+    } else if constexpr (MODE == FFT_R2C) {
+        const TIO* in = static_cast<const TIO*>(a.in) + (long long)b * a.in_batch;
+        int k0 = -1, k1 = -1, j0 = 0, j1 = 0;  // GLL slot of the two real columns
+        if (a.P > 0) { k0 = c0 % a.P; j0 = c0 / a.P; k1 = c1 % a.P; j1 = c1 / a.P; }
+        const bool bnd0 = (k0 == 0 || k0 == a.P - 1), bnd1 = (k1 == 0 || k1 == a.P - 1);
+        const double* s0 = (k0 == 0) ? (b == a.gl_batch ? a.gl : nullptr) : (b == a.gr_batch ? a.gr : nullptr);
+        const double* s1 = (k1 == 0) ? (b == a.gl_batch ? a.gl : nullptr) : (b == a.gr_batch ? a.gr : nullptr);
+#pragma unroll
+        for (int r = 0; r < R0; ++r) {
+            const long long row = tc + r * TPC;
+            T x0 = 0, x1 = 0;
+            if (valid) {
+                if (!bnd0) x0 = (T)in[row * a.in_row + c0];
+                else if (s0) x0 = (T)s0[row * a.bc_row + j0];
+                if (has1) {
+                    if (!bnd1) x1 = (T)in[row * a.in_row + c1];
+                    else if (s1) x1 = (T)s1[row * a.bc_row + j1];
+                }
+            }
+            v[r] = mk(x0, x1);
+        }
+    } else {
+        const C* in = static_cast<const C*>(a.in) + (long long)b * a.in_batch;
+#pragma unroll
+        for (int r = 0; r < R0; ++r) v[r] = valid ? in[(long long)(tc + r * TPC) * a.in_row + c] : mk((T)0, (T)0);
+    }
+    dft_reg<R0, DIR, T>(v);
+
+    // --------------------------------------------------- later passes --
+    if constexpr (NP >= 2) {
+        if constexpr (MODE == FFT_C2R) __syncthreads();  // pass 0 read shared memory
+        pass_to_smem<T, L, R0, 1, TPC, CT, R0>(sm, tc, cl, v);
+        __syncthreads();
+        pass_from_smem<T, L, R1, R0, DIR, TPC, CT, R0>(sm, tw, tc, cl, v);
+    }
+    if constexpr (NP >= 3) {
+        __syncthreads();
+        pass_to_smem<T, L, R1, R0, TPC, CT, R0>(sm, tc, cl, v);
+        __syncthreads();
+        pass_from_smem<T, L, R2, R0 * R1, DIR, TPC, CT, R0>(sm, tw, tc, cl, v);
+    }
+    constexpr int RL = (NP == 1) ? R0 : (NP == 2 ? R1 : R2);   // radix of the last pass
+    constexpr int NSL = L / RL;                                 // its NS
+
+    // ---------------------------------------------------------- output --
+    const T sc = (T)a.scale;
+    if constexpr (MODE == FFT_C2C) {
+        if (valid) {
+            C* out = static_cast<C*>(a.out) + (long long)b * a.out_batch;
+#pragma unroll
+            for (int t = 0; t < R0 / RL; ++t)
+#pragma unroll
+                for (int r = 0; r < RL; ++r) {
+                    const int row = pass_out_row<RL, NSL, TPC>(tc, t, r);
+                    out[(long long)row * a.out_row + c] = cscale(v[t * RL + r], sc);
+                }
+        }
+    } else if constexpr (MODE == FFT_C2R) {
+        if (valid) {
+            TIO* out = static_cast<TIO*>(a.out) + (long long)b * a.out_batch;
+#pragma unroll
+            for (int t = 0; t < R0 / RL; ++t)
+#pragma unroll
+                for (int r = 0; r < RL; ++r) {
+                    const long long row = pass_out_row<RL, NSL, TPC>(tc, t, r);
+                    out[row * a.out_row + c0] = (TIO)(v[t * RL + r].x * sc);
+                    if (has1) out[row * a.out_row + c1] = (TIO)(v[t * RL + r].y * sc);
+                }
+        }
+    } else {  // R2C: separate the two real columns' spectra, keep k = 0 .. L/2
+        __syncthreads();
+        pass_to_smem<T, L, RL, NSL, TPC, CT, R0>(sm, tc, cl, v);
+        __syncthreads();
+        if (valid) {
+            C* out = static_cast<C*>(a.out) + (long long)b * a.out_batch;
+            const T h = (T)0.5 * sc;
+            for (int k = tc; k <= L / 2; k += TPC) {
+                const C Z = sm[k * CT + cl];
+                const C Zm = sm[((L - k) & (L - 1)) * CT + cl];
+                out[(long long)k * a.out_row + c0] = mk((Z.x + Zm.x) * h, (Z.y - Zm.y) * h);
+                if (has1) out[(long long)k * a.out_row + c1] = mk((Z.y + Zm.y) * h, (Zm.x - Z.x) * h);
+            }
+        }
+    }
+}
+
+template <typename T, typename TIO, int L, int DIR, int MODE>
+static int run_fft(const FftArgs& a, long long total_cols, cudaStream_t s)
+{
+    using S = FftShape<T, L>;
+    auto k = fft_kernel<T, TIO, L, DIR, MODE>;
+    static bool attr_done = false;  // per instantiation
+    if (!attr_done) {
+        cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)S::smem);
+        if (e != cudaSuccess) return (int)e;
+        attr_done = true;
+    }
+    const long long blocks = (total_cols + S::CT - 1) / S::CT;
+    if (blocks <= 0) return 0;
+    k<<<(unsigned)blocks, FFT_THREADS, S::smem, s>>>(a, total_cols);
+    return (int)cudaGetLastError();
+}
+
+template <typename T, typename TIO, int L>
+static int fft_dispatch_mode(int mode, int dir, const FftArgs& a, long long tc, cudaStream_t s)
+{
+    if (mode == FFT_C2C) return dir < 0 ? run_fft<T, T, L, -1, FFT_C2C>(a, tc, s) : run_fft<T, T, L, 1, FFT_C2C>(a, tc, s);
+    if (mode == FFT_R2C) return run_fft<T, TIO, L, -1, FFT_R2C>(a, tc, s);
+    return run_fft<T, TIO, L, 1, FFT_C2R>(a, tc, s);
+}
+
+template <typename T, typename TIO>
+static int fft_dispatch_len(int L, int mode, int dir, const FftArgs& a, long long tc, cudaStream_t s)
+{
+    switch (L) {
+        case 4: return fft_dispatch_mode<T, TIO, 4>(mode, dir, a, tc, s);
+        case 8: return fft_dispatch_mode<T, TIO, 8>(mode, dir, a, tc, s);
+        case 16: return fft_dispatch_mode<T, TIO, 16>(mode, dir, a, tc, s);
+        case 32: return fft_dispatch_mode<T, TIO, 32>(mode, dir, a, tc, s);
+        case 64: return fft_dispatch_mode<T, TIO, 64>(mode, dir, a, tc, s);
+        case 128: return fft_dispatch_mode<T, TIO, 128>(mode, dir, a, tc, s);
+        case 256: return fft_dispatch_mode<T, TIO, 256>(mode, dir, a, tc, s);
+        case 512: return fft_dispatch_mode<T, TIO, 512>(mode, dir, a, tc, s);
+        case 1024: return fft_dispatch_mode<T, TIO, 1024>(mode, dir, a, tc, s);
+        default: return (int)cudaErrorInvalidValue;
+    }
+}
+
+int launch_fft(int L, int mode, int dir, int t_double, int io_bytes, const FftArgs& a, long long total_cols,
+               cudaStream_t s)
+{
+    if (t_double) return fft_dispatch_len<double, double>(L, mode, dir, a, total_cols, s);
+    if (io_bytes == 8) return fft_dispatch_len<float, double>(L, mode, dir, a, total_cols, s);
+    return fft_dispatch_len<float, float>(L, mode, dir, a, total_cols, s);
+}
+
+// ======================================================== row solves ==
+
+constexpr int ROW_WARPS = 4;
+constexpr int ROW_NSMAX = 64;  // max GLL elements per row handled by rows_kernel
+
+__device__ __forceinline__ float shfl(float v, int src) { return __shfl_sync(0xffffffffu, v, src); }
+__device__ __forceinline__ double shfl(double v, int src) { return __shfl_sync(0xffffffffu, v, src); }
+template <typename T> __device__ __forceinline__ T warp_sum(T v)
+{
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
+// x <- (P A)^-1 P x with the combined column-major L\U factor F (unit lower L),
+// dinv = 1/U_ii, perm = source row of each position.  Lane l owns rows l + 32 s.
+template <typename TF, int NSLOT>
+__device__ __forceinline__ void lu_core(const TF* F, int ld, const TF* dinv, const int* perm, int n, TF (&xr)[NSLOT],
+                                        TF (&xi)[NSLOT], TF* scr, int lane)
+{
+#pragma unroll
+    for (int s = 0; s < NSLOT; ++s) {
+        scr[lane + 32 * s] = xr[s];
+        scr[32 * NSLOT + lane + 32 * s] = xi[s];
+    }
+    __syncwarp();
+#pragma unroll
+    for (int s = 0; s < NSLOT; ++s) {
+        const int i = lane + 32 * s;
+        const int p = (i < n) ? perm[i] : i;
+        xr[s] = scr[p];
+        xi[s] = scr[32 * NSLOT + p];
+    }
+    __syncwarp();
+    // forward substitution with the unit lower factor
+#pragma unroll
+    for (int ks = 0; ks < NSLOT; ++ks) {
+        for (int kl = 0; kl < 32; ++kl) {
+            const int k = ks * 32 + kl;
+            if (k >= n - 1) break;
+            const TF yr = shfl(xr[ks], kl), yi = shfl(xi[ks], kl);
+            const TF* col = F + (size_t)k * ld;
+#pragma unroll
+            for (int s = ks; s < NSLOT; ++s) {
+                if (s > ks || lane > kl) {
+                    const TF f = col[lane + 32 * s];
+                    xr[s] -= f * yr;
+                    xi[s] -= f * yi;
+                }
+            }
+        }
+    }
+    // back substitution with U, column by column
+#pragma unroll
+    for (int ks = NSLOT - 1; ks >= 0; --ks) {
+        for (int kl = 31; kl >= 0; --kl) {
+            const int k = ks * 32 + kl;
+            if (k >= n) continue;
+            const TF di = dinv[k];
+            const TF yr = shfl(xr[ks], kl) * di, yi = shfl(xi[ks], kl) * di;
+            if (lane == kl) { xr[ks] = yr; xi[ks] = yi; }
+            const TF* col = F + (size_t)k * ld;
+#pragma unroll
+            for (int s = 0; s <= ks; ++s) {
+                if (s < ks || lane < kl) {
+                    const TF f = col[lane + 32 * s];
+                    xr[s] -= f * yr;
+                    xi[s] -= f * yi;
+                }
+            }
+        }
+    }
+}
+
+// x <- V diag(1/(lam - sigma)) V^-1 x (fast diagonalisation of the interior
+// operator); vinvT / vT column-major with leading dimension ld.
+template <typename TF, int NSLOT>
+__device__ __forceinline__ void fdm_core(const TF* vinvT, const TF* vT, int ld, const TF* rdiag, int n,
+                                         TF (&xr)[NSLOT], TF (&xi)[NSLOT], cplx_t<TF>* scr, int lane)
+{
+#pragma unroll
+    for (int s = 0; s < NSLOT; ++s) scr[lane + 32 * s] = mk(xr[s], xi[s]);
+    __syncwarp();
+    TF wr[NSLOT], wi[NSLOT];
+#pragma unroll
+    for (int s = 0; s < NSLOT; ++s) { wr[s] = 0; wi[s] = 0; }
+    for (int k = 0; k < n; ++k) {
+        const cplx_t<TF> f = scr[k];
+        const TF* col = vinvT + (size_t)k * ld;
+#pragma unroll
+        for (int s = 0; s < NSLOT; ++s) {
+            const TF v = col[lane + 32 * s];
+            wr[s] += v * f.x;
+            wi[s] += v * f.y;
+        }
+    }
+#pragma unroll
+    for (int s = 0; s < NSLOT; ++s) {
+        const TF d = rdiag[lane + 32 * s];
+        wr[s] *= d;
+        wi[s] *= d;
+    }
+    __syncwarp();
+#pragma unroll
+    for (int s = 0; s < NSLOT; ++s) scr[lane + 32 * s] = mk(wr[s], wi[s]);
+    __syncwarp();
+#pragma unroll
+    for (int s = 0; s < NSLOT; ++s) { xr[s] = 0; xi[s] = 0; }
+    for (int k = 0; k < n; ++k) {
+        const cplx_t<TF> w = scr[k];
+        const TF* col = vT + (size_t)k * ld;
+#pragma unroll
+        for (int s = 0; s < NSLOT; ++s) {
+            const TF v = col[lane + 32 * s];
+            xr[s] += v * w.x;
+            xi[s] += v * w.y;
+        }
+    }
+    __syncwarp();
+}
+
+// Shared-memory layout of rows_kernel.
+struct RowSmem {
+    size_t mat, diag, perm, scr, d2, ns, total;
+};
+__host__ __device__ inline size_t align_up(size_t v, size_t a) { return (v + a - 1) / a * a; }
+template <typename TS, typename TF, int METHOD, bool REFINE>
+__host__ __device__ inline RowSmem row_smem_layout(int n, int ld)
+{
+    RowSmem L{};
+    size_t o = 0;
+    L.mat = o;
+    o += (size_t)(METHOD == 1 ? 1 : 2) * n * ld * sizeof(TF);
+    o = align_up(o, 16);
+    L.diag = o;                                   // LU: 1/U_ii ; FDM: 1/(lam - sigma) per warp
+    o += (size_t)(METHOD == 1 ? 1 : ROW_WARPS) * ld * sizeof(TF);
+    o = align_up(o, 16);
+    L.perm = o;
+    o += (size_t)ld * sizeof(int);
+    o = align_up(o, 16);
+    L.scr = o;  // per warp: 2 * ld values of the widest type, complex-interleaved
+    o += (size_t)ROW_WARPS * ld * 2 * (sizeof(TS) > sizeof(TF) ? sizeof(TS) : sizeof(TF));
+    o = align_up(o, 16);
+    L.ns = o;   // per warp: Ns sweep scalars (rhs re/im, b, c, zl re/im)
+    o += (size_t)ROW_WARPS * (ROW_NSMAX + 1) * 6 * sizeof(TS);
+    o = align_up(o, 16);
+    L.d2 = o;
+    if (REFINE) o += (size_t)n * ld * sizeof(double);
+    L.total = align_up(o, 16);
+    return L;
+}
+
+template <typename TS, typename TF, int NSLOT, int METHOD, bool REFINE>
+__global__ void __launch_bounds__(ROW_WARPS * 32) rows_kernel(RowArgs a)
+{
+    using CS = cplx_t<TS>;
+    using CF = cplx_t<TF>;
+    extern __shared__ __align__(16) unsigned char row_smem[];
+    const int n = a.n, P = a.P, ld = a.ldf, Ns = a.Ns;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const RowSmem Lay = row_smem_layout<TS, TF, METHOD, REFINE>(n, ld);
+    TF* sMat = reinterpret_cast<TF*>(row_smem + Lay.mat);
+    TF* sDiag = reinterpret_cast<TF*>(row_smem + Lay.diag);
+    int* sPerm = reinterpret_cast<int*>(row_smem + Lay.perm);
+    unsigned char* scrRaw = row_smem + Lay.scr + (size_t)warp * ld * 2 * (sizeof(TS) > sizeof(TF) ? sizeof(TS) : sizeof(TF));
+    TS* sNs = reinterpret_cast<TS*>(row_smem + Lay.ns) + (size_t)warp * (ROW_NSMAX + 1) * 6;
+    double* sD2 = reinterpret_cast<double*>(row_smem + Lay.d2);
+
+    // shared operator data: the FDM transforms once per CTA; refinement D2
+    if (METHOD == 2) {
+        const TF* vi = static_cast<const TF*>(a.vinvT);
+        const TF* vv = static_cast<const TF*>(a.vT);
+        for (int e = threadIdx.x; e < n * ld; e += blockDim.x) { sMat[e] = vi[e]; sMat[(size_t)n * ld + e] = vv[e]; }
+    }
+    if (REFINE)
+        for (int e = threadIdx.x; e < n * ld; e += blockDim.x) sD2[e] = a.d2t[e];
+    __syncthreads();
+
+    const bool hom_active = a.hom != nullptr;
+    CS* spec = static_cast<CS*>(a.spec);
+
+    // one CTA per group (LU: its factor is staged once); FDM: grid-stride over groups
+    for (int grp = blockIdx.x; grp < a.ngroups; grp += gridDim.x) {
+        if (METHOD == 1) {
+            __syncthreads();
+            const TF* fsrc = static_cast<const TF*>(a.fac) + (size_t)grp * a.fac_stride;
+            const TF* dsrc = static_cast<const TF*>(a.dinv) + (size_t)grp * ld;
+            const uint8_t* psrc = a.perm + (size_t)grp * ld;
+            for (int e = threadIdx.x; e < n * ld; e += blockDim.x) sMat[e] = fsrc[e];
+            for (int e = threadIdx.x; e < ld; e += blockDim.x) { sDiag[e] = dsrc[e]; sPerm[e] = psrc[e]; }
+            __syncthreads();
+        }
+        const double sig = a.sigma[grp];
+        TF* rdiag = sDiag + (size_t)warp * ld;  // FDM: this warp's 1/(lam - sigma)
+        if (METHOD == 2) {
+            for (int j = lane; j < ld; j += 32) rdiag[j] = (j < n) ? (TF)(1.0 / (a.lam[j] - sig)) : (TF)0;
+            __syncwarp();
+        }
+        const double* ul = hom_active ? a.hom + (size_t)grp * 2 * P : nullptr;
+        const double* ur = hom_active ? ul + P : nullptr;
+        double d0ul = 0, d0ur = 0, dNul = 0, dNur = 0;
+        if (hom_active) {
+            d0ul = a.homs[grp * 4 + 0]; d0ur = a.homs[grp * 4 + 1];
+            dNul = a.homs[grp * 4 + 2]; dNur = a.homs[grp * 4 + 3];
+        }
+        const int r0 = a.grp_start[grp], r1 = a.grp_start[grp + 1];
+        for (int rr = r0 + warp; rr < r1; rr += ROW_WARPS) {
+            const long long rowoff = (long long)a.grp_rows[rr] * P;
+            TS pr = 0, pi = 0;                        // running d/dy of the previous element (Ns > 1)
+            TS rhs_r = 0, rhs_i = 0, bprev = 0, cprev = 0;
+            TS d0r = 0, d0i = 0, dNr = 0, dNi = 0;
+            TS xr[NSLOT], xi[NSLOT];
+            for (int jj = 0; jj < Ns; ++jj) {
+                CS* row = spec + (long long)jj * a.elem_stride + rowoff;
+                TS fr[NSLOT], fi[NSLOT];
+#pragma unroll
+                for (int s = 0; s < NSLOT; ++s) {
+                    const int i = lane + 32 * s;
+                    CS v = mk((TS)0, (TS)0);
+                    if (i < n) v = row[1 + i];
+                    fr[s] = v.x;
+                    fi[s] = v.y;
+                }
+                // ---- collocation solve of the interior nodes ----
+                TF yr[NSLOT], yi[NSLOT];
+#pragma unroll
+                for (int s = 0; s < NSLOT; ++s) { yr[s] = (TF)fr[s]; yi[s] = (TF)fi[s]; }
+                if (METHOD == 1) lu_core<TF, NSLOT>(sMat, ld, sDiag, sPerm, n, yr, yi, reinterpret_cast<TF*>(scrRaw), lane);
+                else fdm_core<TF, NSLOT>(sMat, sMat + (size_t)n * ld, ld, rdiag, n, yr, yi, reinterpret_cast<CF*>(scrRaw), lane);
+#pragma unroll
+                for (int s = 0; s < NSLOT; ++s) { xr[s] = (TS)yr[s]; xi[s] = (TS)yi[s]; }
+                if (REFINE) {
+                    // FP64 residual r = f - (D2int x - sigma x), then a corrected FP32 solve
+                    CS* scr = reinterpret_cast<CS*>(scrRaw);
+                    for (int sw = 0; sw < a.sweeps; ++sw) {
+                        __syncwarp();
+#pragma unroll
+                        for (int s = 0; s < NSLOT; ++s) scr[lane + 32 * s] = mk(xr[s], xi[s]);
+                        __syncwarp();
+                        TS rr_[NSLOT], ri_[NSLOT];
+#pragma unroll
+                        for (int s = 0; s < NSLOT; ++s) {
+                            rr_[s] = fr[s] + (TS)sig * xr[s];
+                            ri_[s] = fi[s] + (TS)sig * xi[s];
+                        }
+                        for (int k = 0; k < n; ++k) {
+                            const CS xk = scr[k];
+                            const double* col = sD2 + (size_t)k * ld;
+#pragma unroll
+                            for (int s = 0; s < NSLOT; ++s) {
+                                const double d = col[lane + 32 * s];
+                                rr_[s] -= d * xk.x;
+                                ri_[s] -= d * xk.y;
+                            }
+                        }
+                        __syncwarp();
+#pragma unroll
+                        for (int s = 0; s < NSLOT; ++s) { yr[s] = (TF)rr_[s]; yi[s] = (TF)ri_[s]; }
+                        if (METHOD == 1) lu_core<TF, NSLOT>(sMat, ld, sDiag, sPerm, n, yr, yi, reinterpret_cast<TF*>(scrRaw), lane);
+                        else fdm_core<TF, NSLOT>(sMat, sMat + (size_t)n * ld, ld, rdiag, n, yr, yi, reinterpret_cast<CF*>(scrRaw), lane);
+#pragma unroll
+                        for (int s = 0; s < NSLOT; ++s) { xr[s] += (TS)yr[s]; xi[s] += (TS)yi[s]; }
+                    }
+                }
+                if (!hom_active) {
+#pragma unroll
+                    for (int s = 0; s < NSLOT; ++s) {
+                        const int i = lane + 32 * s;
+                        if (i < n) row[1 + i] = mk(xr[s], xi[s]);
+                    }
+                    if (lane == 0) { row[0] = mk((TS)0, (TS)0); row[P - 1] = mk((TS)0, (TS)0); }
+                    continue;
+                }
+                // ---- d/dy of the particular solution at both ends ----
+                TS a0r = 0, a0i = 0, aNr = 0, aNi = 0;
+#pragma unroll
+                for (int s = 0; s < NSLOT; ++s) {
+                    const int i = lane + 32 * s;
+                    if (i < n) {
+                        const TS c0 = (TS)a.d0[1 + i], cN = (TS)a.dN[1 + i];
+                        a0r += c0 * xr[s]; a0i += c0 * xi[s];
+                        aNr += cN * xr[s]; aNi += cN * xi[s];
+                    }
+                }
+                d0r = warp_sum(a0r); d0i = warp_sum(a0i);
+                dNr = warp_sum(aNr); dNi = warp_sum(aNi);
+                // ---- forward sweep of the interface system ----
+                TS bj, cj;
+                if (jj == 0) {
+                    bj = (TS)(-a.al * d0ul + a.bl);
+                    cj = (TS)(-a.al * d0ur);
+                    const CS gl = row[0];
+                    rhs_r = gl.x + (TS)a.al * d0r;
+                    rhs_i = gl.y + (TS)a.al * d0i;
+                } else {
+                    const TS q = (TS)dNul / bprev;
+                    bj = (TS)dNur - (TS)d0ul - cprev * q;
+                    cj = (TS)(-d0ur);
+                    rhs_r = d0r - pr - rhs_r * q;
+                    rhs_i = d0i - pi - rhs_i * q;
+                }
+                bprev = bj; cprev = cj; pr = dNr; pi = dNi;
+                if (Ns > 1) {
+                    if (lane == 0) {
+                        sNs[jj * 6 + 0] = rhs_r; sNs[jj * 6 + 1] = rhs_i;
+                        sNs[jj * 6 + 2] = bj;    sNs[jj * 6 + 3] = cj;
+                    }
+#pragma unroll
+                    for (int s = 0; s < NSLOT; ++s) {  // park phi of this element in place
+                        const int i = lane + 32 * s;
+                        if (i < n) row[1 + i] = mk(xr[s], xi[s]);
+                    }
+                }
+            }
+            if (!hom_active) continue;
+            // ---- right end, back sweep, combination ----
+            CS* lastrow = spec + (long long)(Ns - 1) * a.elem_stride + rowoff;
+            const CS gr = lastrow[P - 1];
+            const TS lb = (TS)(a.ar * dNul);
+            const TS bR = (TS)(a.ar * dNur + a.br) - (cprev / bprev) * lb;
+            const TS rRr = gr.x - (TS)a.ar * dNr - (rhs_r / bprev) * lb;
+            const TS rRi = gr.y - (TS)a.ar * dNi - (rhs_i / bprev) * lb;
+            TS zr_r = rRr / bR, zr_i = rRi / bR;
+            if (Ns == 1) {
+                const TS zl_r = (rhs_r - cprev * zr_r) / bprev, zl_i = (rhs_i - cprev * zr_i) / bprev;
+                CS* row = spec + rowoff;
+#pragma unroll
+                for (int s = 0; s < NSLOT; ++s) {
+                    const int i = lane + 32 * s;
+                    if (i < n) {
+                        const TS l = (TS)ul[1 + i], r = (TS)ur[1 + i];
+                        row[1 + i] = mk(xr[s] + zl_r * l + zr_r * r, xi[s] + zl_i * l + zr_i * r);
+                    }
+                }
+                if (lane == 0) { row[0] = mk(zl_r, zl_i); row[P - 1] = mk(zr_r, zr_i); }
+            } else {
+                __syncwarp();
+                if (lane == 0) {
+                    for (int jj = Ns - 1; jj >= 0; --jj) {
+                        const TS rr_ = sNs[jj * 6 + 0], ri_ = sNs[jj * 6 + 1], bj = sNs[jj * 6 + 2], cj = sNs[jj * 6 + 3];
+                        const TS zl_r = (rr_ - cj * zr_r) / bj, zl_i = (ri_ - cj * zr_i) / bj;
+                        sNs[jj * 6 + 4] = zl_r; sNs[jj * 6 + 5] = zl_i;
+                        sNs[(jj + 1) * 6 + 0] = zr_r; sNs[(jj + 1) * 6 + 1] = zr_i;  // zr of element jj
+                        zr_r = zl_r; zr_i = zl_i;
+                    }
+                }
+                __syncwarp();
+                for (int jj = 0; jj < Ns; ++jj) {
+                    CS* row = spec + (long long)jj * a.elem_stride + rowoff;
+                    const TS zl_r = sNs[jj * 6 + 4], zl_i = sNs[jj * 6 + 5];
+                    const TS zrr = sNs[(jj + 1) * 6 + 0], zri = sNs[(jj + 1) * 6 + 1];
+#pragma unroll
+                    for (int s = 0; s < NSLOT; ++s) {
+                        const int i = lane + 32 * s;
+                        if (i < n) {
+                            const CS x = row[1 + i];
+                            const TS l = (TS)ul[1 + i], r = (TS)ur[1 + i];
+                            row[1 + i] = mk(x.x + zl_r * l + zrr * r, x.y + zl_i * l + zri * r);
+                        }
+                    }
+                    if (lane == 0) { row[0] = mk(zl_r, zl_i); row[P - 1] = mk(zrr, zri); }
+                }
+                __syncwarp();
+            }
+        }
+    }
+}
+
+template <typename TS, typename TF, int NSLOT, int METHOD, bool REFINE>
+static int run_rows(const RowArgs& a, cudaStream_t s)
+{
+    auto k = rows_kernel<TS, TF, NSLOT, METHOD, REFINE>;
+    const RowSmem L = row_smem_layout<TS, TF, METHOD, REFINE>(a.n, a.ldf);
+    cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L.total);
+    if (e != cudaSuccess) return (int)e;
+    int grid = a.ngroups;
+    if (METHOD == 2) {
+        int dev = 0, sms = 148, per = 1;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k, ROW_WARPS * 32, L.total);
+        if (per < 1) per = 1;
+        grid = a.ngroups < sms * per ? a.ngroups : sms * per;
+    }
+    if (grid <= 0) return 0;
+    k<<<grid, ROW_WARPS * 32, L.total, s>>>(a);
+    return (int)cudaGetLastError();
+}
+
+template <int NSLOT>
+static int rows_dispatch_prec(int method, int prec, const RowArgs& a, cudaStream_t s)
+{
+    if (method == 1) {
+        if (prec == 0) return run_rows<double, double, NSLOT, 1, false>(a, s);
+        if (prec == 1) return run_rows<float, float, NSLOT, 1, false>(a, s);
+        return run_rows<double, float, NSLOT, 1, true>(a, s);
+    }
+    if (prec == 0) return run_rows<double, double, NSLOT, 2, false>(a, s);
+    if (prec == 1) return run_rows<float, float, NSLOT, 2, false>(a, s);
+    return run_rows<double, float, NSLOT, 2, true>(a, s);
+}
+
+size_t rows_smem_bytes(int method, int prec, int n, int ld)
+{
+    if (method == 1) {
+        if (prec == 0) return row_smem_layout<double, double, 1, false>(n, ld).total;
+        if (prec == 1) return row_smem_layout<float, float, 1, false>(n, ld).total;
+        return row_smem_layout<double, float, 1, true>(n, ld).total;
+    }
+    if (prec == 0) return row_smem_layout<double, double, 2, false>(n, ld).total;
+    if (prec == 1) return row_smem_layout<float, float, 2, false>(n, ld).total;
+    return row_smem_layout<double, float, 2, true>(n, ld).total;
+}
+
+int launch_rows(int method, int prec, const RowArgs& a, cudaStream_t s)
+{
+    if (a.Ns > ROW_NSMAX) return (int)cudaErrorInvalidValue;
+    switch ((a.n + 31) / 32) {
+        case 1: return rows_dispatch_prec<1>(method, prec, a, s);
+        case 2: return rows_dispatch_prec<2>(method, prec, a, s);
+        case 3: return rows_dispatch_prec<3>(method, prec, a, s);
+        case 4: return rows_dispatch_prec<4>(method, prec, a, s);
+        default: return (int)cudaErrorInvalidValue;
+    }
+}
+
+}  // namespace helm

@@ -1,0 +1,73 @@
+// Kernel argument blocks shared by the launchers (helm_kernels.cu) and the plan
+// (helm_plan.cu).
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace helm {
+
+enum FftMode { FFT_C2C = 0, FFT_R2C = 1, FFT_C2R = 2 };
+
+// One batched FFT along a strided axis.  The transform index is the row; the
+// data of one row are `ncols` contiguous columns; batches are `*_batch` apart.
+// Units: elements of the in/out array type (real for the R2C input and the C2R
+// output, complex otherwise).
+struct FftArgs {
+    const void* in;
+    void* out;
+    long long in_row, out_row;
+    long long in_batch, out_batch;
+    int ncols;      // complex columns per batch (C2C) or real columns (R2C/C2R)
+    int nbatch;
+    double scale;   // applied to every output value
+    const void* tw; // exp(DIR * 2 pi i e / L), e in [0, L), compute precision
+    // R2C only: GLL boundary slots k == 0 / k == P-1 of batch gl_batch /
+    // gr_batch read the boundary data gl / gr [row][col / P] instead of the
+    // input; the boundary slots of the other batches read 0.  P = 0 disables.
+    const double* gl;
+    const double* gr;
+    long long bc_row;
+    int P, gl_batch, gr_batch;
+};
+
+// Per-wavenumber solve of the spectrum rows, grouped by shift sigma.
+struct RowArgs {
+    void* spec;                // complex [Ns][nrows][P]
+    long long elem_stride;     // complex elements between GLL elements
+    int P, n, Ns;
+    int ngroups;
+    const int* grp_start;      // [ngroups + 1]
+    const int* grp_rows;       // complex row index (spec offset row * P)
+    // LU method: per group, column-major combined L\U factor, 1/U_ii, row permutation
+    const void* fac;
+    const void* dinv;
+    const uint8_t* perm;
+    int ldf;                   // leading dimension of a factor column
+    long long fac_stride;      // elements between two groups' factors
+    // FDM method: shared interior eigen-decomposition D2int = V diag(lam) V^-1
+    const void* vinvT;         // column-major V^-1: vinvT[k*ldf + j] = Vinv[j][k]
+    const void* vT;            // column-major V:    vT[k*ldf + i]    = V[i][k]
+    const double* lam;         // eigenvalues [n]
+    // homogeneous solutions and scalars (FP64), per group
+    const double* hom;         // [ngroups][2][P]: ul, ur
+    const double* homs;        // [ngroups][4]: D0.ul, D0.ur, DN.ul, DN.ur
+    const double* d0;          // [P] first row of the scaled first-derivative matrix
+    const double* dN;          // [P] last row
+    const double* sigma;       // [ngroups]
+    const double* d2t;         // refinement: column-major interior D2 [n][n]
+    int sweeps;
+    double al, bl, ar, br;
+};
+
+// Launchers (helm_kernels.cu).  Return a cudaError_t.
+// T: compute precision (0 = float, 1 = double); io: real element bytes for
+// R2C input / C2R output (4 or 8).
+int launch_fft(int L, int mode, int dir, int t_double, int io_bytes, const FftArgs& a, long long total_cols,
+               cudaStream_t s);
+// method: 1 = LU, 2 = FDM; prec: 0 = FP64, 1 = FP32, 2 = FP32 with FP64 refinement
+int launch_rows(int method, int prec, const RowArgs& a, cudaStream_t s);
+// Dynamic shared memory rows_kernel needs for this method / precision / size.
+size_t rows_smem_bytes(int method, int prec, int n, int ld);
+constexpr size_t kMaxSmemPerBlock = 232448;  // 227 KB opt-in limit of sm_100
+
+}  // namespace helm

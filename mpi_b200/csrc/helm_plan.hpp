@@ -1,0 +1,61 @@
+// The plan object behind helm_plan_t (include/helm_b200.h).
+#pragma once
+#include <cuda_runtime.h>
+#include <cstdint>
+#include <vector>
+
+#include "../../include/helm_b200.h"
+#include "helm_setup.hpp"
+
+namespace helm {
+
+struct Plan {
+    int dim = 2;                 // 2: Fourier x GLL, 3: Fourier x Fourier x GLL
+    int Nx = 0, Ny = 1, N = 0, Ns = 1, n = 0;
+    int nslot = 1, ld = 32;      // 32-lane slots per interior vector, padded length
+    double xl = 0, xr = 1, yl = 0, yr = 1, zl = 0, zr = 1;
+    double Lx = 1, Ly = 1, Lgll = 1;
+    helm_robin_t bc{0.0, 1.0, 0.0, 1.0};
+    double lambda = 0;
+    int precision = HELM_FP64, method = HELM_METHOD_AUTO;
+    int io_bytes = 8, sweeps = 2;
+    long long x_stride = 0, elem_stride = 0, bc_x_stride = 0;
+    int device = 0;
+    GllSetup gll;
+
+    // rows grouped by shift
+    int ngroups = 0;
+    long long nrows = 0, elem_spec = 0;
+    std::vector<int> grp_start, grp_rows, grp_iw, grp_jw;
+    std::vector<double> sigma;
+    std::vector<double> h_lam, h_V, h_Vi;
+
+    // device memory
+    void* d_spec = nullptr;
+    void* d_tw_x = nullptr;
+    void* d_tw_y = nullptr;
+    int* d_grp_start = nullptr;
+    int* d_grp_rows = nullptr;
+    double* d_sigma = nullptr;
+    void* d_fac = nullptr;
+    void* d_dinv = nullptr;
+    uint8_t* d_perm = nullptr;
+    void* d_vinvT = nullptr;
+    void* d_vT = nullptr;
+    double* d_lam = nullptr;
+    double* d_hom = nullptr;
+    double* d_homs = nullptr;
+    double* d_d0 = nullptr;
+    double* d_dN = nullptr;
+    double* d_d2t = nullptr;
+    std::vector<void*> allocations;
+    long long device_bytes = 0;
+
+    int alloc(void** p, size_t bytes);
+    int upload(void** p, const void* host, size_t bytes);
+    void release();
+};
+
+int solve(Plan& p, const void* f, const double* gl, const double* gr, void* u, cudaStream_t s);
+
+}  // namespace helm

@@ -1,0 +1,212 @@
+"""Host-side mirror of the reference's solver interface over the C ABI.
+
+The reference (HelmholtzSolvers/DirectPseudoSpectral) exposes, per solver
+family, ``CreatePDEPlan(...)`` / ``SolvePDE(U, ConstructOperator)`` /
+``DestroyPDEPlan()`` over global arrays (NonPeriodic2D_MPI.h:33-37,
+NonPeriodic3D_MPI.h:33-37).  Here each family is a class whose constructor is
+CreatePDEPlan (plus the Lambda / alpha / beta globals and the shifted-Laplacian
+ConstructOperator of the reference's tests), whose ``SolvePDE`` runs the solve on
+the GPU, and whose ``DestroyPDEPlan`` frees it.  Arrays are torch CUDA tensors
+in the reference's index order (GLL index fastest):
+
+* ``NonPeriodic2D``: f, u ``[Ns, Nx, N]`` (or ``[Nx, N]`` when Ns == 1), gl/gr ``[Nx]``
+* ``NonPeriodic3D``: f, u ``[Ns, Nx, Ny, N]`` (or ``[Nx, Ny, N]``), gl/gr ``[Nx, Ny]``
+
+Errors raise :class:`mpi_b200._lib.HelmError` with the C status code (the
+reference prints a message and exits).
+"""
+from __future__ import annotations
+
+import ctypes
+import math
+from typing import Optional, Sequence
+
+import torch
+
+from . import _lib as L
+
+_PREC = {"fp64": L.HELM_FP64, "fp32": L.HELM_FP32, "fp32_refine": L.HELM_FP32_REFINE}
+_METHOD = {"auto": L.HELM_METHOD_AUTO, "lu": L.HELM_METHOD_LU, "fdm": L.HELM_METHOD_FDM}
+_METHOD_NAME = {v: k for k, v in _METHOD.items()}
+
+
+def _stream_ptr(stream) -> int:
+    if stream is None:
+        stream = torch.cuda.current_stream()
+    return int(stream.cuda_stream) if hasattr(stream, "cuda_stream") else int(stream)
+
+
+class _PlanBase:
+    dim = 0
+
+    def __init__(self):
+        self._plan = ctypes.c_void_p()
+        self._lib = L.lib()
+
+    # -------------------------------------------------------------- info --
+    @property
+    def handle(self) -> int:
+        return self._plan.value or 0
+
+    def info(self) -> dict:
+        ns, nop, meth = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+        nb = ctypes.c_longlong()
+        L.check(self._lib.helm_plan_info(self._plan, ctypes.byref(ns), ctypes.byref(nop), ctypes.byref(meth),
+                                         ctypes.byref(nb)), "helm_plan_info")
+        return {"Ns": ns.value, "n_operators": nop.value, "method": _METHOD_NAME[meth.value],
+                "device_bytes": nb.value}
+
+    @property
+    def Ns(self) -> int:
+        return self.info()["Ns"]
+
+    def grid(self):
+        """(nodes, D, D2) of the GLL direction as float64 CPU tensors (the
+        reference's y/z, Dy/Dz and Dyy/Dzz globals)."""
+        ns = self.Ns
+        N = self.N
+        nodes = torch.zeros(ns * (N - 1) + 1, dtype=torch.float64)
+        D = torch.zeros(N, N, dtype=torch.float64)
+        D2 = torch.zeros(N, N, dtype=torch.float64)
+        L.check(self._lib.helm_plan_get_grid(self._plan, nodes.data_ptr(), D.data_ptr(), D2.data_ptr()),
+                "helm_plan_get_grid")
+        return nodes, D, D2
+
+    def set_layout(self, x_stride: int = 0, elem_stride: int = 0, bc_x_stride: int = 0) -> None:
+        L.check(self._lib.helm_plan_set_layout(self._plan, x_stride, elem_stride, bc_x_stride), "helm_plan_set_layout")
+
+    def set_refine_sweeps(self, sweeps: int) -> None:
+        L.check(self._lib.helm_plan_set_refine_sweeps(self._plan, sweeps), "helm_plan_set_refine_sweeps")
+
+    def set_io_bytes(self, nbytes: int) -> None:
+        L.check(self._lib.helm_plan_set_io_bytes(self._plan, nbytes), "helm_plan_set_io_bytes")
+        self.io_dtype = torch.float32 if nbytes == 4 else torch.float64
+
+    # ------------------------------------------------------------- solve --
+    def _shape(self, Ns: int):
+        raise NotImplementedError
+
+    def _bc_shape(self):
+        raise NotImplementedError
+
+    def SolvePDE(self, f: torch.Tensor, gl: Optional[torch.Tensor] = None, gr: Optional[torch.Tensor] = None,
+                 out: Optional[torch.Tensor] = None, stream=None) -> torch.Tensor:
+        """u = solution of (lap - lambda) u = f with the plan's Robin data gl/gr
+        (None: zero).  f, gl, gr, out: contiguous CUDA tensors."""
+        ns = self.Ns
+        full = self._shape(ns)
+        if f.dim() == len(full) - 1 and ns == 1:
+            fv = f.unsqueeze(0)
+        else:
+            fv = f
+        if tuple(fv.shape) != full:
+            raise ValueError(f"f has shape {tuple(f.shape)}, expected {full}")
+        if not fv.is_cuda or fv.dtype != self.io_dtype or not fv.is_contiguous():
+            raise ValueError(f"f must be a contiguous CUDA {self.io_dtype} tensor")
+        bshape = self._bc_shape()
+        for g, nm in ((gl, "gl"), (gr, "gr")):
+            if g is not None and (tuple(g.shape) != bshape or g.dtype != torch.float64 or not g.is_cuda
+                                  or not g.is_contiguous()):
+                raise ValueError(f"{nm} must be a contiguous CUDA float64 tensor of shape {bshape}")
+        if out is None:
+            out = torch.empty(f.shape, dtype=self.io_dtype, device=f.device)
+        elif tuple(out.shape) != tuple(f.shape) or out.dtype != self.io_dtype or not out.is_contiguous():
+            raise ValueError("out does not match f")
+        st = self._lib.helm_solve(self._plan, fv.data_ptr(), gl.data_ptr() if gl is not None else None,
+                                  gr.data_ptr() if gr is not None else None, out.data_ptr(), _stream_ptr(stream))
+        L.check(st, "helm_solve")
+        return out
+
+    solve = SolvePDE
+
+    def SolveAdjoint(self, ubar: torch.Tensor, u: Optional[torch.Tensor] = None, want_bc: bool = False,
+                     stream=None):
+        """(fbar, lambda_bar, glbar, grbar) of the linear map (f, gl, gr) -> u
+        for the cotangent ubar; lambda_bar needs the forward solution u."""
+        fbar = torch.empty_like(ubar, dtype=torch.float64)
+        lam = torch.zeros(1, dtype=torch.float64, device=ubar.device) if u is not None else None
+        glb = torch.empty(self._bc_shape(), dtype=torch.float64, device=ubar.device) if want_bc else None
+        grb = torch.empty(self._bc_shape(), dtype=torch.float64, device=ubar.device) if want_bc else None
+        st = self._lib.helm_solve_adjoint(self._plan, ubar.data_ptr(), fbar.data_ptr(),
+                                          glb.data_ptr() if glb is not None else None,
+                                          grb.data_ptr() if grb is not None else None,
+                                          u.data_ptr() if u is not None else None,
+                                          lam.data_ptr() if lam is not None else None, _stream_ptr(stream))
+        L.check(st, "helm_solve_adjoint")
+        return fbar, lam, glb, grb
+
+    def DestroyPDEPlan(self) -> None:
+        if self._plan.value:
+            self._lib.helm_plan_destroy(self._plan)
+            self._plan = ctypes.c_void_p()
+
+    close = DestroyPDEPlan
+
+    def __del__(self):
+        try:
+            self.DestroyPDEPlan()
+        except Exception:
+            pass
+
+
+class NonPeriodic2D(_PlanBase):
+    """2D Fourier (x) x GLL (y) solver: CreatePDEPlan(Nx, Ny, N, xl, xr, yl, yr)
+    of NonPeriodic2D_MPI.cpp:40-126 with Lambda and the Robin coefficients
+    (alphal, betal, alphar, betar) of NonPeriodic2D_MPI.h:27."""
+
+    dim = 2
+
+    def __init__(self, Nx: int, Ny: int, N: int, xl: float, xr: float, yl: float, yr: float, *,
+                 Lambda: float, bc: Sequence[float] = (0.0, 1.0, 0.0, 1.0), precision: str = "fp64",
+                 method: str = "auto"):
+        super().__init__()
+        self.Nx, self.N = Nx, N
+        self.xl, self.xr, self.yl, self.yr = xl, xr, yl, yr
+        self.Lambda = Lambda
+        self.bc = tuple(float(b) for b in bc)
+        self.precision = precision
+        self.io_dtype = torch.float64
+        r = L.robin_t(*self.bc)
+        L.check(self._lib.helm2d_plan_create(Nx, Ny, N, xl, xr, yl, yr, ctypes.byref(r), Lambda, _PREC[precision],
+                                             _METHOD[method], ctypes.byref(self._plan)), "helm2d_plan_create")
+
+    def _shape(self, Ns):
+        return (Ns, self.Nx, self.N)
+
+    def _bc_shape(self):
+        return (self.Nx,)
+
+
+class NonPeriodic3D(_PlanBase):
+    """3D Fourier (x, y) x GLL (z) solver: CreatePDEPlan(Nx, Ny, Nz, N, xl, xr,
+    yl, yr, zl, zr) of NonPeriodic3D_MPI.cpp:40-134."""
+
+    dim = 3
+
+    def __init__(self, Nx: int, Ny: int, Nz: int, N: int, xl: float, xr: float, yl: float, yr: float, zl: float,
+                 zr: float, *, Lambda: float, bc: Sequence[float] = (0.0, 1.0, 0.0, 1.0), precision: str = "fp64",
+                 method: str = "auto"):
+        super().__init__()
+        self.Nx, self.Ny, self.N = Nx, Ny, N
+        self.Lambda = Lambda
+        self.bc = tuple(float(b) for b in bc)
+        self.precision = precision
+        self.io_dtype = torch.float64
+        r = L.robin_t(*self.bc)
+        L.check(self._lib.helm3d_plan_create(Nx, Ny, Nz, N, xl, xr, yl, yr, zl, zr, ctypes.byref(r), Lambda,
+                                             _PREC[precision], _METHOD[method], ctypes.byref(self._plan)),
+                "helm3d_plan_create")
+
+    def _shape(self, Ns):
+        return (Ns, self.Nx, self.Ny, self.N)
+
+    def _bc_shape(self):
+        return (self.Nx, self.Ny)
+
+
+def gdof(Nx: int, Ny: int, N: int, Ns: int = 1) -> int:
+    """Degrees of freedom of one solve: grid values of u (Ns elements of N GLL points)."""
+    return Nx * Ny * N * Ns
+
+
+__all__ = ["NonPeriodic2D", "NonPeriodic3D", "gdof", "math"]

@@ -1,0 +1,195 @@
+"""Python access to the CPU oracles (TEST INFRASTRUCTURE ONLY).
+
+Two libraries, both built by ``oracle/Makefile``:
+
+* ``liboracle.so`` -- the plain-C restatement (``helm_oracle.c``) of the
+  reference's DirectPseudoSpectral solve and of the HypreFDM stencil solved by
+  FFT/Thomas.  Always buildable (gcc only).
+* ``_ref/libref2d.so`` / ``_ref/libref3d.so`` -- the reference's own C++
+  sources compiled unchanged, wrapped by ``ref_driver2d.cpp`` /
+  ``ref_driver3d.cpp``.  Present only where the reference tree was available
+  at build time; :func:`have_reference` says whether they were built.
+
+Only ``tests/``, ``__graft_entry__.smoke`` and the CPU-baseline leg of
+``bench.py`` may import this module, and only as the checker.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_D = ctypes.c_double
+_I = ctypes.c_int
+_P = ctypes.POINTER(ctypes.c_double)
+
+_lib = None
+_ref2d = None
+_ref3d = None
+
+
+def build(quiet: bool = True) -> None:
+    """Compile the C restatement (and the reference wrappers when the reference
+    sources are present on this machine)."""
+    out = subprocess.DEVNULL if quiet else None
+    subprocess.run(["make", "-s", "-C", _HERE], check=True, stdout=out)
+    ref_root = os.environ.get("REF_ROOT", "/root/reference")
+    if os.path.isdir(os.path.join(ref_root, "HelmholtzSolvers", "DirectPseudoSpectral")):
+        subprocess.run(["make", "-s", "-C", _HERE, "ref", f"REF_ROOT={ref_root}"], check=True, stdout=out)
+
+
+def _p(a: np.ndarray):
+    return a.ctypes.data_as(_P)
+
+
+def _c64(a) -> np.ndarray:
+    return np.ascontiguousarray(a, dtype=np.float64)
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        path = os.path.join(_HERE, "liboracle.so")
+        if not os.path.exists(path):
+            build()
+        _lib = ctypes.CDLL(path)
+        _lib.orc_solve2d.restype = _I
+        _lib.orc_solve2d.argtypes = [_I, _I, _I] + [_D] * 7 + [_P] * 4
+        _lib.orc_solve3d.restype = _I
+        _lib.orc_solve3d.argtypes = [_I, _I, _I, _I] + [_D] * 8 + [_P] * 4
+        _lib.orc_residual3d.restype = _D
+        _lib.orc_residual3d.argtypes = [_I, _I, _I] + [_D] * 8 + [_P] * 5
+        _lib.orc_fd3d_solve.restype = _I
+        _lib.orc_fd3d_solve.argtypes = [_I, _I, _I] + [_D] * 8 + [_P] * 4
+        _lib.orc_fd3d_residual.restype = _D
+        _lib.orc_fd3d_residual.argtypes = [_I, _I, _I] + [_D] * 8 + [_P] * 4
+        _lib.orc_gll_setup.restype = None
+        _lib.orc_gll_setup.argtypes = [_I, _I, _D, _P, _P, _P]
+        _lib.orc_lu_decompose.restype = _I
+        _lib.orc_lu_decompose.argtypes = [_I, _P, ctypes.POINTER(_I)]
+        _lib.orc_lu_solve.restype = None
+        _lib.orc_lu_solve.argtypes = [_I, _P, ctypes.POINTER(_I), _P]
+    return _lib
+
+
+def have_reference() -> bool:
+    return all(os.path.exists(os.path.join(_HERE, "_ref", n)) for n in ("libref2d.so", "libref3d.so"))
+
+
+def _ref(which: int):
+    global _ref2d, _ref3d
+    if which == 2:
+        if _ref2d is None:
+            _ref2d = ctypes.CDLL(os.path.join(_HERE, "_ref", "libref2d.so"))
+            _ref2d.oracle_ref2d_solve.restype = _I
+            _ref2d.oracle_ref2d_solve.argtypes = [_I] * 3 + [_D] * 9 + [_P] * 6
+        return _ref2d
+    if _ref3d is None:
+        _ref3d = ctypes.CDLL(os.path.join(_HERE, "_ref", "libref3d.so"))
+        _ref3d.oracle_ref3d_solve.restype = _I
+        _ref3d.oracle_ref3d_solve.argtypes = [_I] * 4 + [_D] * 11 + [_P] * 6
+    return _ref3d
+
+
+# ------------------------------------------------------------------ grid --
+def gll_grid(N: int, Ns: int, L: float):
+    """(nodes[Ns*(N-1)+1], D[N,N], D2[N,N]) of one element of length L/Ns,
+    nodes placed from 0 as the reference does."""
+    y = np.zeros(Ns * (N - 1) + 1)
+    D = np.zeros((N, N))
+    D2 = np.zeros((N, N))
+    lib().orc_gll_setup(N, Ns, L, _p(y), _p(D), _p(D2))
+    return y, D, D2
+
+
+# ------------------------------------------------------ restatement solves --
+def solve2d(f, gl, gr, *, Lx, Ly, lam, bc=(0.0, 1.0, 0.0, 1.0)):
+    """f: [Ns, Nx, N] or [Nx, N]; returns u of the same shape."""
+    f = _c64(f)
+    squeeze = f.ndim == 2
+    if squeeze:
+        f = f[None]
+    Ns, Nx, N = f.shape
+    u = np.zeros_like(f)
+    st = lib().orc_solve2d(Nx, N, Ns, Lx, Ly, *bc, lam, _p(f), _p(_c64(gl)), _p(_c64(gr)), _p(u))
+    if st:
+        raise RuntimeError(f"orc_solve2d status {st}")
+    return u[0] if squeeze else u
+
+
+def solve3d(f, gl, gr, *, Lx, Ly, Lz, lam, bc=(0.0, 1.0, 0.0, 1.0)):
+    """f: [Ns, Nx, Ny, N] or [Nx, Ny, N]; returns u of the same shape."""
+    f = _c64(f)
+    squeeze = f.ndim == 3
+    if squeeze:
+        f = f[None]
+    Ns, Nx, Ny, N = f.shape
+    u = np.zeros_like(f)
+    st = lib().orc_solve3d(Nx, Ny, N, Ns, Lx, Ly, Lz, *bc, lam, _p(f), _p(_c64(gl)), _p(_c64(gr)), _p(u))
+    if st:
+        raise RuntimeError(f"orc_solve3d status {st}")
+    return u[0] if squeeze else u
+
+
+def residual3d(u, f, gl, gr, *, Lx, Ly, Lz, lam, bc=(0.0, 1.0, 0.0, 1.0)):
+    """Max-abs collocation residual (FP64) of a single-element 3D solution."""
+    u = _c64(u)
+    Nx, Ny, N = u.shape
+    r = np.zeros_like(u)
+    return lib().orc_residual3d(Nx, Ny, N, Lx, Ly, Lz, *bc, lam, _p(_c64(f)), _p(_c64(gl)), _p(_c64(gr)), _p(u), _p(r))
+
+
+def fd3d_solve(f, gb, gf, *, Lx, Ly, Lz, lam, bc=(0.0, 1.0, 0.0, 1.0)):
+    f = _c64(f)
+    Nx, Ny, Nz = f.shape
+    u = np.zeros_like(f)
+    st = lib().orc_fd3d_solve(Nx, Ny, Nz, Lx, Ly, Lz, *bc, lam, _p(f), _p(_c64(gb)), _p(_c64(gf)), _p(u))
+    if st:
+        raise RuntimeError(f"orc_fd3d_solve status {st}")
+    return u
+
+
+def fd3d_residual(u, f, gb, gf, *, Lx, Ly, Lz, lam, bc=(0.0, 1.0, 0.0, 1.0)):
+    u = _c64(u)
+    Nx, Ny, Nz = u.shape
+    return lib().orc_fd3d_residual(Nx, Ny, Nz, Lx, Ly, Lz, *bc, lam, _p(_c64(f)), _p(_c64(gb)), _p(_c64(gf)), _p(u))
+
+
+# ------------------------------------------------------- the reference itself --
+def ref_solve2d(f, gl, gr, *, xl, xr, yl, yr, lam, bc=(0.0, 1.0, 0.0, 1.0), return_time=False):
+    """The reference's own SolvePDE (2D).  f: [Ns, Nx, N] or [Nx, N]."""
+    f = _c64(f)
+    squeeze = f.ndim == 2
+    if squeeze:
+        f = f[None]
+    Ns, Nx, N = f.shape
+    u = np.zeros_like(f)
+    y = np.zeros(Ns * (N - 1) + 1)
+    ms = np.zeros(1)
+    ns = _ref(2).oracle_ref2d_solve(Nx, Ns * N, N, xl, xr, yl, yr, *bc, lam,
+                                    _p(f), _p(_c64(gl)), _p(_c64(gr)), _p(u), _p(y), _p(ms))
+    if ns != Ns:
+        raise RuntimeError(f"reference chose Ns={ns}, expected {Ns}")
+    out = u[0] if squeeze else u
+    return (out, ms[0]) if return_time else out
+
+
+def ref_solve3d(f, gl, gr, *, xl, xr, yl, yr, zl, zr, lam, bc=(0.0, 1.0, 0.0, 1.0), return_time=False):
+    """The reference's own SolvePDE (3D).  f: [Ns, Nx, Ny, N] or [Nx, Ny, N]."""
+    f = _c64(f)
+    squeeze = f.ndim == 3
+    if squeeze:
+        f = f[None]
+    Ns, Nx, Ny, N = f.shape
+    u = np.zeros_like(f)
+    z = np.zeros(Ns * (N - 1) + 1)
+    ms = np.zeros(1)
+    ns = _ref(3).oracle_ref3d_solve(Nx, Ny, Ns * N, N, xl, xr, yl, yr, zl, zr, *bc, lam,
+                                    _p(f), _p(_c64(gl)), _p(_c64(gr)), _p(u), _p(z), _p(ms))
+    if ns != Ns:
+        raise RuntimeError(f"reference chose Ns={ns}, expected {Ns}")
+    out = u[0] if squeeze else u
+    return (out, ms[0]) if return_time else out

@@ -1,0 +1,63 @@
+// Test infrastructure (oracle), never shipped: a C entry point around the
+// reference's own 2D Fourier x GLL solver so the tests can run it on the same
+// inputs as the CUDA path.  The reference sources are compiled unchanged from
+// HelmholtzSolvers/DirectPseudoSpectral/src by oracle/Makefile.
+//
+// Follows the reference's test driver TestNonPeriodic2D_MPI.cpp:79-142:
+// CreatePDEPlan -> CreateFFTPlan -> fill rhsPDE/leftBC/rightBC -> SolvePDE with the
+// shifted-Laplacian ConstructOperator (TestNonPeriodic2D_MPI.cpp:67-74) -> read U.
+#include "NonPeriodic2D_MPI.h"
+#include <chrono>
+
+// The operator the reference's tests pass to SolvePDE: Dyy on the interior
+// nodes minus (lambda + (2 pi iw / Lx)^2) on the diagonal, LU-factored in place.
+static void oracle_construct_operator_2d(const int iw)
+{
+    for (int i = 0; i < N - 2; ++i)
+        for (int j = 0; j < N - 2; ++j)
+            Operator[i][j] = Dyy[i + 1][j + 1] - (i == j ? (Lambda + 4.0 * PI * PI * iw * iw / (Lx * Lx)) : 0.0);
+    LUDecomposition(Operator, npivot, determinant, N - 2);
+}
+
+// f, u: [Ns][Nx][N] (row-major, GLL index fastest); gl, gr: [Nx];
+// ygrid: Ns*(N-1)+1 node coordinates.  Ns = ceil(ny / n) as in CreatePDEPlan.
+extern "C" int oracle_ref2d_solve(int nx, int ny, int n,
+                                  double xl_, double xr_, double yl_, double yr_,
+                                  double al, double bl, double ar, double br_, double lam,
+                                  const double* f, const double* gl, const double* gr,
+                                  double* u, double* ygrid, double* solve_ms)
+{
+    Rank = 0;
+    size = 1;
+    CreatePDEPlan(nx, ny, n, xl_, xr_, yl_, yr_);
+    CreateFFTPlan(Nx);
+    alphal = al; betal = bl; alphar = ar; betar = br_; Lambda = lam;
+
+    FieldVariable* V = new FieldVariable[Ns];
+    for (int jj = 0; jj < Ns; ++jj) Allocate(V[jj].phi, NX, N);
+
+    for (int jj = 0; jj < Ns; ++jj)
+        for (int i = 0; i < Nx; ++i)
+            for (int j = 0; j < N; ++j)
+                rhsPDE[jj][i][j] = f[((size_t)jj * Nx + i) * N + j];
+    for (int i = 0; i < Nx; ++i) { leftBC[i] = gl[i]; rightBC[i] = gr[i]; }
+
+    auto t0 = std::chrono::steady_clock::now();
+    SolvePDE(V, oracle_construct_operator_2d);
+    auto t1 = std::chrono::steady_clock::now();
+    if (solve_ms) *solve_ms = std::chrono::duration<double, std::milli>(t1 - t0).count();
+
+    for (int jj = 0; jj < Ns; ++jj)
+        for (int i = 0; i < Nx; ++i)
+            for (int j = 0; j < N; ++j)
+                u[((size_t)jj * Nx + i) * N + j] = V[jj].phi[i][j];
+    if (ygrid)
+        for (int j = 0; j < Ns * (N - 1) + 1; ++j) ygrid[j] = y[j];
+
+    int ns = Ns;
+    for (int jj = 0; jj < Ns; ++jj) Deallocate(V[jj].phi, NX, N);
+    delete[] V;
+    DestroyFFTPlan(Nx);
+    DestroyPDEPlan();
+    return ns;
+}

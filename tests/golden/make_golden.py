@@ -1,0 +1,72 @@
+"""Generate the golden vectors in tests/golden/ from the reference's own solver.
+
+Runs the reference's DirectPseudoSpectral SolvePDE (compiled from its sources by
+oracle/Makefile into oracle/_ref) on small seeded problems and stores inputs and
+outputs as compressed .npz files.  Needs the reference tree at build time; the
+committed .npz files are what the tests read.
+
+    python tests/golden/make_golden.py
+"""
+import math
+import os
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.dirname(os.path.dirname(HERE)))
+
+from mpi_b200 import workloads as W  # noqa: E402
+from oracle import oracle as O  # noqa: E402
+
+
+def main():
+    O.build()
+    if not O.have_reference():
+        raise SystemExit("reference oracle (oracle/_ref) not built: reference tree absent")
+    rng = np.random.default_rng(20240601)
+    out = {}
+
+    # config-1 manufactured problem, Dirichlet
+    f, ue = W.manufactured_2d(64, 33, 1.0)
+    z = np.zeros(64)
+    u = O.ref_solve2d(f, z, z, xl=0.0, xr=2 * math.pi, yl=-1.0, yr=1.0, lam=1.0)
+    out["cfg1_2d"] = dict(f=f, u=u, u_exact=ue, Nx=64, N=33, Ns=1, dom=[0.0, 2 * math.pi, -1.0, 1.0], lam=1.0,
+                          bc=[0.0, 1.0, 0.0, 1.0])
+
+    # 2D Robin, three elements
+    Nx, N, Ns = 16, 9, 3
+    f = rng.standard_normal((Ns, Nx, N)); gl = rng.standard_normal(Nx); gr = rng.standard_normal(Nx)
+    bc = [1.0, 0.5, 0.7, 2.0]
+    u = O.ref_solve2d(f, gl, gr, xl=0.1, xr=1.4, yl=0.0, yr=0.9, lam=2.0, bc=tuple(bc))
+    out["robin_2d_ns3"] = dict(f=f, gl=gl, gr=gr, u=u, Nx=Nx, N=N, Ns=Ns, dom=[0.1, 1.4, 0.0, 0.9], lam=2.0, bc=bc)
+
+    # 3D Robin, one element, Lx != Ly
+    Nx, Ny, N = 8, 16, 9
+    f = rng.standard_normal((Nx, Ny, N)); gl = rng.standard_normal((Nx, Ny)); gr = rng.standard_normal((Nx, Ny))
+    u = O.ref_solve3d(f, gl, gr, xl=0.0, xr=1.3, yl=0.0, yr=0.7, zl=0.0, zr=0.9, lam=2.0, bc=tuple(bc))
+    out["robin_3d"] = dict(f=f, gl=gl, gr=gr, u=u, Nx=Nx, Ny=Ny, N=N, Ns=1,
+                           dom=[0.0, 1.3, 0.0, 0.7, 0.0, 0.9], lam=2.0, bc=bc)
+
+    # 3D Robin, two elements
+    Nx, Ny, N, Ns = 8, 4, 7, 2
+    f = rng.standard_normal((Ns, Nx, Ny, N)); gl = rng.standard_normal((Nx, Ny)); gr = rng.standard_normal((Nx, Ny))
+    u = O.ref_solve3d(f, gl, gr, xl=0.0, xr=1.0, yl=0.0, yr=2.0, zl=0.0, zr=1.5, lam=0.5, bc=tuple(bc))
+    out["robin_3d_ns2"] = dict(f=f, gl=gl, gr=gr, u=u, Nx=Nx, Ny=Ny, N=N, Ns=Ns,
+                               dom=[0.0, 1.0, 0.0, 2.0, 0.0, 1.5], lam=0.5, bc=bc)
+
+    # config-2 shape in miniature: smooth seeded field, Dirichlet, lambda = 10
+    Nx = Ny = 16; N = 17
+    f = W.smooth_field_3d(Nx, Ny, N, seed=1236)
+    zb = np.zeros((Nx, Ny))
+    u = O.ref_solve3d(f, zb, zb, xl=0.0, xr=2 * math.pi, yl=0.0, yr=2 * math.pi, zl=0.0, zr=2.0, lam=10.0)
+    out["smooth_3d"] = dict(f=f, u=u, Nx=Nx, Ny=Ny, N=N, Ns=1, dom=[0.0, 2 * math.pi, 0.0, 2 * math.pi, 0.0, 2.0],
+                            lam=10.0, bc=[0.0, 1.0, 0.0, 1.0])
+
+    for name, d in out.items():
+        np.savez_compressed(os.path.join(HERE, name + ".npz"), **{k: np.asarray(v) for k, v in d.items()})
+        print(name, {k: np.asarray(v).shape for k, v in d.items()})
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,170 @@
+"""Parity of the CUDA solve with the oracle (GPU).
+
+Golden vectors come from the reference's own SolvePDE (tests/golden); larger
+cases are checked against the C restatement (oracle/helm_oracle.c), which
+tests/test_oracle.py pins to the reference.  Tolerances: FP64 plans 1e-12
+relative (max-norm); FP32 plans 1e-5 relative L2; FP32 plans with FP64-residual
+refinement 1e-10 relative L2 (the accuracy target of the mixed-precision solve).
+"""
+import math
+
+import numpy as np
+import pytest
+import torch
+
+from mpi_b200 import NonPeriodic2D, NonPeriodic3D
+from mpi_b200 import workloads as W
+from oracle import oracle as O
+from tests.helpers import golden, max_rel, rel_l2
+
+pytestmark = pytest.mark.gpu
+
+TOL = {"fp64": 1e-12, "fp32": 1e-5, "fp32_refine": 1e-10}
+
+
+def _dev(a):
+    return torch.from_numpy(np.ascontiguousarray(a, dtype=np.float64)).cuda()
+
+
+def _plan2d(g, precision="fp64", method="auto"):
+    xl, xr, yl, yr = [float(v) for v in g["dom"]]
+    return NonPeriodic2D(int(g["Nx"]), int(g["Ns"]) * int(g["N"]), int(g["N"]), xl, xr, yl, yr,
+                         Lambda=float(g["lam"]), bc=tuple(g["bc"]), precision=precision, method=method)
+
+
+def _plan3d(g, precision="fp64", method="auto"):
+    xl, xr, yl, yr, zl, zr = [float(v) for v in g["dom"]]
+    return NonPeriodic3D(int(g["Nx"]), int(g["Ny"]), int(g["Ns"]) * int(g["N"]), int(g["N"]), xl, xr, yl, yr, zl, zr,
+                         Lambda=float(g["lam"]), bc=tuple(g["bc"]), precision=precision, method=method)
+
+
+def _solve(plan, g):
+    gl = _dev(g["gl"]) if "gl" in g else None
+    gr = _dev(g["gr"]) if "gr" in g else None
+    u = plan.SolvePDE(_dev(g["f"]), gl, gr)
+    torch.cuda.synchronize()
+    return u.cpu().numpy()
+
+
+def _check(u, ref, precision):
+    if precision == "fp64":
+        assert max_rel(u, ref) < TOL["fp64"]
+    else:
+        assert rel_l2(u, ref) < TOL[precision]
+
+
+@pytest.mark.parametrize("method", ["lu", "fdm"])
+@pytest.mark.parametrize("precision", ["fp64", "fp32", "fp32_refine"])
+@pytest.mark.parametrize("name", ["cfg1_2d", "robin_2d_ns3"])
+def test_golden_2d(cuda, name, precision, method):
+    g = golden(name)
+    p = _plan2d(g, precision, method)
+    assert p.info()["method"] == method
+    _check(_solve(p, g), g["u"], precision)
+
+
+@pytest.mark.parametrize("method", ["lu", "fdm"])
+@pytest.mark.parametrize("precision", ["fp64", "fp32", "fp32_refine"])
+@pytest.mark.parametrize("name", ["robin_3d", "robin_3d_ns2", "smooth_3d"])
+def test_golden_3d(cuda, name, precision, method):
+    g = golden(name)
+    p = _plan3d(g, precision, method)
+    _check(_solve(p, g), g["u"], precision)
+
+
+@pytest.mark.parametrize("method", ["lu", "fdm"])
+def test_cfg1_exact_solution(cuda, method):
+    f, ue = W.manufactured_2d(64, 33, 1.0)
+    p = NonPeriodic2D(64, 33, 33, 0.0, 2 * math.pi, -1.0, 1.0, Lambda=1.0, method=method)
+    u = p.SolvePDE(_dev(f)).cpu().numpy()
+    assert np.abs(u - ue).max() < 1e-13
+
+
+@pytest.mark.parametrize("method", ["lu", "fdm"])
+def test_reference_stock_2d(cuda, method):
+    """The reference's NonPeriodic2D test (Ns = 52 elements, Neumann/Dirichlet)."""
+    f, gl, gr, ue, bc = W.stock_2d()
+    p = NonPeriodic2D(512, 512, 10, 0.0, 1.0, 0.0, 1.0, Lambda=1.0, bc=bc, method=method)
+    assert p.Ns == 52
+    u = p.SolvePDE(_dev(f), _dev(gl), _dev(gr)).cpu().numpy()
+    assert np.abs(u - ue).max() < 1e-12
+
+
+@pytest.mark.parametrize("method", ["lu", "fdm"])
+def test_reference_stock_3d(cuda, method):
+    """The reference's NonPeriodic3D test (64 x 32 x 250, N = 10, Ns = 25)."""
+    f, gl, gr, ue, bc = W.stock_3d()
+    p = NonPeriodic3D(64, 32, 250, 10, 0.0, 1.0, 0.0, 1.0, 0.0, 1.0, Lambda=1.0, bc=bc, method=method)
+    u = p.SolvePDE(_dev(f), _dev(gl), _dev(gr)).cpu().numpy()
+    assert np.abs(u - ue).max() < 1e-12
+
+
+@pytest.mark.parametrize("Nx,N,lam", [(128, 65, 5.0), (256, 65, 10.0)])
+@pytest.mark.parametrize("precision,method", [("fp64", "lu"), ("fp64", "fdm"), ("fp32", "fdm"),
+                                              ("fp32_refine", "fdm"), ("fp32_refine", "lu")])
+def test_full_size_3d_vs_oracle(cuda, Nx, N, lam, precision, method):
+    """The 3D workloads at full size (128^2 x 65, lambda 5; 256^2 x 65, lambda 10)."""
+    f = W.smooth_field_3d(Nx, Nx, N, seed=1236)
+    z = np.zeros((Nx, Nx))
+    ref = O.solve3d(f, z, z, Lx=2 * math.pi, Ly=2 * math.pi, Lz=2.0, lam=lam)
+    p = NonPeriodic3D(Nx, Nx, N, N, 0.0, 2 * math.pi, 0.0, 2 * math.pi, 0.0, 2.0, Lambda=lam,
+                      precision=precision, method=method)
+    u = p.SolvePDE(_dev(f)).cpu().numpy()
+    if precision == "fp64":
+        assert rel_l2(u, ref) < 1e-12
+    else:
+        assert rel_l2(u, ref) < TOL[precision]
+
+
+def test_reference_array_layout_3d(cuda):
+    """The reference's own arrays: rhsPDE[2Nx][2Ny][N] and leftBC[2Nx][2Ny]."""
+    g = golden("robin_3d")
+    Nx, Ny, N = int(g["Nx"]), int(g["Ny"]), int(g["N"])
+    F = np.zeros((2 * Nx, 2 * Ny, N)); F[:Nx, :Ny] = g["f"]
+    GL = np.zeros((2 * Nx, 2 * Ny)); GL[:Nx, :Ny] = g["gl"]
+    GR = np.zeros((2 * Nx, 2 * Ny)); GR[:Nx, :Ny] = g["gr"]
+    p = _plan3d(g)
+    p.set_layout(x_stride=2 * Ny * N, elem_stride=2 * Nx * 2 * Ny * N, bc_x_stride=2 * Ny)
+    fd, ud = _dev(F), torch.full((2 * Nx, 2 * Ny, N), 7.0, dtype=torch.float64, device="cuda")
+    st = p._lib.helm_solve(p._plan, fd.data_ptr(), _dev(GL).data_ptr(), _dev(GR).data_ptr(), ud.data_ptr(),
+                           torch.cuda.current_stream().cuda_stream)
+    assert st == 0
+    U = ud.cpu().numpy()
+    assert max_rel(U[:Nx, :Ny], g["u"]) < 1e-12
+    assert np.all(U[Nx:] == 7.0) and np.all(U[:, Ny:] == 7.0)  # padding untouched
+
+
+def test_fp32_io(cuda):
+    g = golden("smooth_3d")
+    p = _plan3d(g, "fp32")
+    p.set_io_bytes(4)
+    u = p.SolvePDE(torch.from_numpy(g["f"].astype(np.float32)).cuda()).cpu().numpy()
+    assert rel_l2(u, g["u"]) < 1e-5
+
+
+def test_repeated_solves_and_streams(cuda):
+    """Plan reuse on a side stream, the input left untouched (the reference
+    overwrites rhsPDE with its spectrum; this solver does not)."""
+    g = golden("robin_2d_ns3")
+    p = _plan2d(g)
+    f = _dev(g["f"])
+    f0 = f.clone()
+    s = torch.cuda.Stream()
+    with torch.cuda.stream(s):
+        for _ in range(3):
+            u = p.SolvePDE(f, _dev(g["gl"]), _dev(g["gr"]), stream=s)
+    s.synchronize()
+    assert torch.equal(f, f0)
+    assert max_rel(u.cpu().numpy(), g["u"]) < 1e-12
+
+
+def test_linearity_full_size(cuda):
+    """Size-independent property at the 256^2 x 65 size: S(a f1 + b f2) = a S f1 + b S f2."""
+    Nx, N = 256, 65
+    f1 = _dev(W.smooth_field_3d(Nx, Nx, N, seed=1))
+    f2 = _dev(W.smooth_field_3d(Nx, Nx, N, seed=2))
+    p = NonPeriodic3D(Nx, Nx, N, N, 0.0, 2 * math.pi, 0.0, 2 * math.pi, 0.0, 2.0, Lambda=10.0)
+    u1, u2 = p.SolvePDE(f1), p.SolvePDE(f2)
+    u12 = p.SolvePDE(2.0 * f1 - 3.0 * f2)
+    err = (u12 - (2.0 * u1 - 3.0 * u2)).norm() / u12.norm()
+    assert err.item() < 1e-13
