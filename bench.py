@@ -1,0 +1,389 @@
+#!/usr/bin/env python
+"""Headline benchmark: the 3D Fourier x Fourier x GLL Helmholtz solve.
+
+Workload (one "step" = one solve): Nx = Ny = 256 Fourier modes, GLL N = 64
+(65 points) in z, lambda = 10, homogeneous Dirichlet, f a seeded smooth field
+(complex Gaussian Fourier/Legendre coefficients with amplitude (1+|k|^2)^-1.5,
+zero mean).  DOF per solve = 256 * 256 * 65 = 4,259,840 grid values of u.
+
+`value` is the FP32 + FP64-residual-refinement solve in GDOF/s with inputs
+resident in HBM, the L2 flushed (256 MB write) before every timed solve, and
+device time from CUDA events; `fp64` gives the plain FP64 solve beside it.
+`e2e` is the same solve through the public API from pinned host memory
+(H2D of f and D2H of u inside the timed region).  Multi-GPU runs are replicas
+(the path has no exchange step): every rank solves its own copy, the time is
+the max over ranks, and `value` counts all ranks' DOF.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+"""
+from __future__ import annotations
+
+import argparse
+import datetime
+import json
+import math
+import os
+import re
+import signal
+import subprocess
+import sys
+import tempfile
+import time
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, HERE)
+
+METRIC = "GDOF/s FP32+refine vs FP64 on B200 at ≤1e-10 rel err; fwd+adjoint ms; %HBM"
+NX = NY = 256
+NGLL = 65
+LAM = 10.0
+SEED = 1236
+DOM = (0.0, 2 * math.pi, 0.0, 2 * math.pi, 0.0, 2.0)
+WORKLOAD = "3D Helmholtz, Fourier 256 x Fourier 256 x GLL 65 (N=64), lambda=10, Dirichlet, seeded smooth field"
+FALLBACK_HBM_GBS = 6650.0
+
+
+def _args():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--warmup", type=int, default=20)
+    ap.add_argument("--impl", choices=("ours", "reference"), default="ours")
+    ap.add_argument("--skip-cpu-baseline", action="store_true", help="omit the CPU leg (profiling runs)")
+    return ap.parse_args()
+
+
+def _dist():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+# ----------------------------------------------------------------- clocks --
+class ClockSampler:
+    """nvidia-smi sampling (200 ms) of SM clocks and throttle reasons."""
+
+    FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+              "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_id: str):
+        self.path = tempfile.mktemp(suffix=".csv")
+        self.proc = None
+        self.gpu_id = gpu_id
+
+    def start(self):
+        try:
+            self.fh = open(self.path, "w")
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", self.gpu_id, f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=self.fh, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self) -> dict:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"], "samples": 0}
+        self.proc.send_signal(signal.SIGTERM)
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        self.fh.close()
+        rows = []
+        for line in open(self.path):
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) >= 8:
+                rows.append(parts)
+        os.unlink(self.path)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+        sm = [float(r[0]) for r in rows if r[0].replace(".", "").isdigit()]
+        smax = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        power = [float(r[2]) for r in rows if re.match(r"^[\d.]+$", r[2])]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[4 + i].lower().startswith("active")})
+        loaded = [s for s, p in zip(sm, power) if p > 250.0] or sm
+        loaded.sort()
+        return {"sm_mhz": loaded[len(loaded) // 2] if loaded else None, "sm_max_mhz": max(smax) if smax else None,
+                "reasons": reasons, "samples": len(rows), "power_w_max": max(power) if power else None}
+
+
+# ------------------------------------------------------------- reference --
+def _ref_worker_init():
+    sys.path.insert(0, HERE)
+
+
+def _ref_solve_slab(ny: int):
+    """One reference SolvePDE of the 256 x ny x 65 slab of the workload (seeded)."""
+    import numpy as np
+
+    from mpi_b200 import workloads as W
+    from oracle import oracle as O
+
+    f = W.smooth_field_3d(NX, ny, NGLL, seed=SEED)
+    z = np.zeros((NX, ny))
+    t = time.perf_counter()
+    if O.have_reference():
+        O.ref_solve3d(f, z, z, xl=DOM[0], xr=DOM[1], yl=DOM[2], yr=DOM[3], zl=DOM[4], zr=DOM[5], lam=LAM)
+    else:
+        O.solve3d(f, z, z, Lx=DOM[1] - DOM[0], Ly=DOM[3] - DOM[2], Lz=DOM[5] - DOM[4], lam=LAM)
+    return time.perf_counter() - t
+
+
+def run_reference_arm(args, ws, rank):
+    """The reference's own CPU solver (oracle/_ref, compiled from its sources;
+    the C restatement when the reference was not available at build time) on
+    every host core: each worker process runs one SolvePDE per step."""
+    if rank != 0:
+        return
+    import multiprocessing as mp
+
+    from oracle import oracle as O
+
+    O.build()
+    kind = "reference" if O.have_reference() else "port"
+    cores = max(1, min(os.cpu_count() or 1, 64))
+    # calibrate one 256 x 32 x 65 slab and size the per-worker sample so the
+    # (steps + warmup) rounds stay near two minutes
+    t32 = _ref_solve_slab(32)
+    budget = 120.0 / max(1, args.steps + args.warmup)
+    ny = 32
+    while ny < NY and t32 * (2 * ny / 32) <= budget:
+        ny *= 2
+    ctx = mp.get_context("spawn")
+    with ctx.Pool(cores, initializer=_ref_worker_init) as pool:
+        for _ in range(args.warmup):
+            pool.map(_ref_solve_slab, [ny] * cores)
+        times = []
+        for _ in range(args.steps):
+            t = time.perf_counter()
+            pool.map(_ref_solve_slab, [ny] * cores)
+            times.append(time.perf_counter() - t)
+    dof = NX * ny * NGLL * cores
+    ms = 1e3 * sum(times) / len(times)
+    val = dof / (ms * 1e-3) / 1e9
+    sample = f"{cores} processes x one SolvePDE of the 256x{ny}x65 slab of the workload per step"
+    line = {
+        "impl": "reference", "metric": METRIC, "value": val, "unit": "GDOF/s", "n_gpus": ws, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64", "data": "synthetic", "config": {"workload": WORKLOAD, "precision": "fp64", "device": "cpu"},
+        "cpu_baseline": {"value": val, "unit": "GDOF/s", "cores": cores, "kind": kind, "sample": sample},
+        "e2e": {"value": val, "unit": "GDOF/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+# ------------------------------------------------------------------- ours --
+def _peak_hbm():
+    try:
+        with open(os.path.join(HERE, "MEASURED_PEAKS.json")) as fh:
+            return float(json.load(fh)["hbm_gbs"]), "measured"
+    except Exception:
+        return FALLBACK_HBM_GBS, "fallback"
+
+
+def _traffic_from_profiles(stage: str):
+    """DRAM bytes per launch of a stage's kernel at this workload, from the
+    committed ncu summary (profiles/), or None."""
+    path = os.path.join(HERE, "profiles", "traffic_256x256x65.txt")
+    try:
+        for line in open(path):
+            m = re.match(r"^\s*(\w+)\s+(fp64|fp32_refine|fp32)\s+([\d.eE+]+)\s*$", line)
+            if m and m.group(1) == stage:
+                return {m.group(2): float(m.group(3))}
+    except OSError:
+        pass
+    return None
+
+
+def _stage_bytes(stage: str, spec_bytes: float, io_bytes: float) -> float:
+    """Algorithmic HBM bytes of one launch of each stage (inputs read once,
+    outputs written once)."""
+    return {"fft_x": io_bytes + spec_bytes, "fft_y": 2 * spec_bytes, "rows": 2 * spec_bytes,
+            "ifft_y": 2 * spec_bytes, "ifft_x": spec_bytes + io_bytes}[stage]
+
+
+def run_ours(args, ws, rank, local):
+    import numpy as np
+    import torch
+
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    if ws > 1:
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    from mpi_b200 import NonPeriodic3D
+    from mpi_b200 import workloads as W
+
+    fnp = W.smooth_field_3d(NX, NY, NGLL, seed=SEED)
+    f = torch.from_numpy(fnp).to(dev)
+    dof = NX * NY * NGLL
+    plans = {
+        "fp32_refine": NonPeriodic3D(NX, NY, NGLL, NGLL, *DOM, Lambda=LAM, precision="fp32_refine"),
+        "fp64": NonPeriodic3D(NX, NY, NGLL, NGLL, *DOM, Lambda=LAM, precision="fp64"),
+    }
+    outs = {k: p.SolvePDE(f) for k, p in plans.items()}
+    torch.cuda.synchronize()
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+    stream = torch.cuda.current_stream()
+    uuid = str(torch.cuda.get_device_properties(local).uuid)
+    clocks = ClockSampler(uuid if uuid.startswith("GPU-") else f"GPU-{uuid}")
+    clocks.start()
+
+    def barrier():
+        torch.cuda.synchronize()
+        if ws > 1:
+            import torch.distributed as dist
+
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    def timed(fn):
+        for _ in range(args.warmup):
+            flush.add_(1.0)
+            fn()
+        barrier()
+        evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+        for e0, e1 in evs:
+            flush.add_(1.0)  # evicts L2 (126 MB) between steps
+            e0.record(stream)
+            fn()
+            e1.record(stream)
+        barrier()
+        return sum(e0.elapsed_time(e1) for e0, e1 in evs)
+
+    res = {}
+    launches = 0
+    for name, p in plans.items():
+        total_ms = timed(lambda p=p, name=name: p.SolvePDE(f, out=outs[name]))
+        res[name] = total_ms
+    launches = 5 * args.steps  # five kernels per 3D solve, refined plan in the headline
+
+    # end to end through the public API: pinned host f -> H2D -> solve -> D2H
+    fh = torch.from_numpy(fnp).pin_memory()
+    uh = torch.empty_like(fh).pin_memory()
+    fd = torch.empty_like(f)
+
+    def e2e_step():
+        fd.copy_(fh, non_blocking=True)
+        plans["fp32_refine"].SolvePDE(fd, out=outs["fp32_refine"])
+        uh.copy_(outs["fp32_refine"], non_blocking=True)
+
+    e2e_ms = timed(e2e_step)
+
+    # per-stage device time of the refined solve (events on its stream)
+    pref = plans["fp32_refine"]
+    pref.enable_stage_timing(True)
+    acc = {}
+    nst = max(5, min(args.steps, 50))
+    for _ in range(nst):
+        flush.add_(1.0)
+        pref.SolvePDE(f, out=outs["fp32_refine"])
+        for k, v in pref.stage_times().items():
+            acc[k] = acc.get(k, 0.0) + v / nst
+    pref.enable_stage_timing(False)
+    clk = clocks.stop()
+
+    # max over ranks
+    tmax = torch.tensor([res["fp32_refine"], res["fp64"], e2e_ms], dtype=torch.float64, device=dev)
+    if ws > 1:
+        import torch.distributed as dist
+
+        dist.all_reduce(tmax, op=dist.ReduceOp.MAX)
+    t_ref, t_64, t_e2e = [float(v) for v in tmax.cpu()]
+    ms_ref, ms_64, ms_e2e = t_ref / args.steps, t_64 / args.steps, t_e2e / args.steps
+
+    # accuracy of the refined solve against the FP64 solve (and the reference below)
+    u32 = outs["fp32_refine"].double()
+    u64 = outs["fp64"]
+    rel_vs_fp64 = float((u32 - u64).norm() / u64.norm())
+
+    if rank == 0:
+        peak, peak_kind = _peak_hbm()
+        spec_bytes = 16.0 * (NX // 2 + 1) * NY * NGLL
+        io_bytes = 8.0 * dof
+        dom = max(acc, key=acc.get)
+        alg = _stage_bytes(dom, spec_bytes, io_bytes)
+        achieved = alg / (acc[dom] * 1e-3) / 1e9
+        traffic = _traffic_from_profiles(dom)
+        line = {
+            "metric": METRIC,
+            "value": ws * dof / (ms_ref * 1e-3) / 1e9,
+            "unit": "GDOF/s",
+            "n_gpus": ws,
+            "steps": args.steps,
+            "warmup": args.warmup,
+            "ms_per_step": ms_ref,
+            "higher_is_better": True,
+            "scaling": "weak",
+            "vs_baseline": None,
+            "dtype": "f32 solves + f64 residuals/FFTs",
+            "data": "synthetic",
+            "config": {"workload": WORKLOAD, "precision": "fp32_refine", "method": pref.info()["method"],
+                       "refine_sweeps": 2, "l2": "256 MB buffer written before every timed solve",
+                       "parallelism": f"replicas x{ws}", "dof_per_solve": dof},
+            "fp64": {"value": ws * dof / (ms_64 * 1e-3) / 1e9, "ms_per_step": ms_64,
+                     "method": plans["fp64"].info()["method"]},
+            "refine_over_fp64": ms_64 / ms_ref,
+            "rel_l2_refine_vs_fp64": rel_vs_fp64,
+            "stage_ms": acc,
+            "roofline": {"kernel": dom, "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)",
+                         "algorithmic_bytes": alg, "traffic": (traffic or {}).get("fp32_refine")},
+            "e2e": {"value": ws * dof / (ms_e2e * 1e-3) / 1e9, "unit": "GDOF/s", "ms_per_step": ms_e2e,
+                    "h2d_bytes_per_step": int(fh.numel() * 8), "d2h_bytes_per_step": int(uh.numel() * 8)},
+            "gpu_launches": launches,
+            "clocks": clk,
+        }
+        if not args.skip_cpu_baseline and ws == 1:
+            line["cpu_baseline"], ref_u = _cpu_baseline(fnp)
+            line["rel_l2_refine_vs_reference"] = float(np.linalg.norm(u32.cpu().numpy() - ref_u) / np.linalg.norm(ref_u))
+            line["rel_l2_fp64_vs_reference"] = float(np.linalg.norm(u64.cpu().numpy() - ref_u) / np.linalg.norm(ref_u))
+        print(json.dumps(line), flush=True)
+    for p in plans.values():
+        p.DestroyPDEPlan()
+    if ws > 1:
+        import torch.distributed as dist
+
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def _cpu_baseline(fnp):
+    """The reference's own FP64 CPU solve (oracle/_ref) of the full workload on
+    one host core, twice; its output is also the error reference."""
+    import numpy as np
+
+    from oracle import oracle as O
+
+    O.build()
+    z = np.zeros((NX, NY))
+    kind = "reference" if O.have_reference() else "port"
+    times = []
+    u = None
+    for _ in range(2):
+        t = time.perf_counter()
+        if kind == "reference":
+            u = O.ref_solve3d(fnp, z, z, xl=DOM[0], xr=DOM[1], yl=DOM[2], yr=DOM[3], zl=DOM[4], zr=DOM[5], lam=LAM)
+        else:
+            u = O.solve3d(fnp, z, z, Lx=DOM[1] - DOM[0], Ly=DOM[3] - DOM[2], Lz=DOM[5] - DOM[4], lam=LAM)
+        times.append(time.perf_counter() - t)
+    t = min(times)
+    return ({"value": NX * NY * NGLL / t / 1e9, "unit": "GDOF/s", "cores": 1, "kind": kind,
+             "sample": "two full SolvePDE calls of the 256x256x65 workload on one core (best)"}, u)
+
+
+def main():
+    args = _args()
+    ws, rank, local = _dist()
+    if args.impl == "reference":
+        run_reference_arm(args, ws, rank)
+    else:
+        run_ours(args, ws, rank, local)
+
+
+if __name__ == "__main__":
+    main()

@@ -126,6 +126,14 @@ int helm_plan_get_grid(helm_plan_t plan, double* nodes, double* D, double* D2);
  * plan runs, and the device bytes it holds. */
 int helm_plan_info(helm_plan_t plan, int* Ns, int* n_operators, int* method, long long* device_bytes);
 
+/* Stage timing: when enabled, helm_solve records CUDA events on its stream
+ * around each of its kernels; helm_plan_stage_times then waits for the last
+ * solve and returns the five stage durations in ms: x-FFT, y-FFT, row solves,
+ * inverse y-FFT, inverse x-FFT (y stages are 0 in 2D).  The reference times
+ * only the whole SolvePDE with a host clock (TestNonPeriodic2D_MPI.cpp:103-131). */
+int helm_plan_set_stage_timing(helm_plan_t plan, int enable);
+int helm_plan_stage_times(helm_plan_t plan, float* ms5);
+
 /* Replaces DestroyPDEPlan() + DestroyFFTPlan(). NULL is accepted. */
 int helm_plan_destroy(helm_plan_t plan);
 

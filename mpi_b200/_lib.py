@@ -33,6 +33,7 @@ EXPORTS = (
     "helm2d_plan_create", "helm3d_plan_create", "helm_plan_set_layout", "helm_plan_set_io_bytes",
     "helm_plan_set_refine_sweeps", "helm_solve", "helm_solve_adjoint", "helm_plan_get_grid",
     "helm_plan_info", "helm_plan_destroy", "helm_status_string", "helm_last_error",
+    "helm_plan_set_stage_timing", "helm_plan_stage_times",
 )
 
 
@@ -73,6 +74,8 @@ def lib() -> ctypes.CDLL:
     L.helm_plan_get_grid.argtypes = [vp, vp, vp, vp]
     L.helm_plan_info.argtypes = [vp, P(i), P(i), P(i), P(ll)]
     L.helm_plan_destroy.argtypes = [vp]
+    L.helm_plan_set_stage_timing.argtypes = [vp, i]
+    L.helm_plan_stage_times.argtypes = [vp, P(ctypes.c_float)]
     L.helm_status_string.argtypes = [i]
     L.helm_status_string.restype = ctypes.c_char_p
     L.helm_last_error.argtypes = []

@@ -1,0 +1,443 @@
+// Fast-diagonalisation row solve for one GLL element (Ns = 1), sm_100a.
+//
+// The interior GLL second-derivative operator D2int (n x n) is centrosymmetric:
+// D2int[i][j] = D2int[n-1-i][n-1-j].  The orthogonal even/odd fold Q
+//   s_k = (f_k + f_{n-1-k}) / sqrt2,  d_k = (f_k - f_{n-1-k}) / sqrt2  (k < m = n/2),
+//   s_m = f_m (odd n)
+// block-diagonalises it, Q D2int Q^T = diag(Ms, Ma), and each half-size block
+// is diagonalised once at plan time, Ms = Vs diag(ls) Vs^-1, Ma = Va diag(la) Va^-1.
+// The solve of (D2int - sigma I) x = f for one spectrum row is then
+//   fold -> Vs^-1 s, Va^-1 d -> scale by 1/(l - sigma) -> Vs (.), Va (.) -> unfold,
+// n^2 multiply-adds per real right-hand side instead of 2 n^2.  The result is the
+// same linear map as the reference's per-wavenumber LU (LU_Decomposition.cpp:78-108
+// called from ConstructFundamentalSolutions, NonPeriodic3D_MPI.cpp:184-232),
+// followed by the same Robin/interface epilogue (NonPeriodic3D_MPI.cpp:328-369,
+// 520-533, 582-587).
+//
+// Layout of the work: a persistent grid of 8-warp CTAs, the transforms staged
+// once per CTA in shared memory, and each warp solving RPW spectrum rows at a
+// time (every matrix load feeds RPW rows).  Lane l owns fold index l + 32 t.
+#include "helm_device.cuh"
+#include "helm_fdm.cuh"
+
+namespace helm {
+
+constexpr int FDM_WARPS = 8;
+
+__device__ __forceinline__ float fshfl(float v, int s) { return __shfl_sync(0xffffffffu, v, s); }
+template <typename T> __device__ __forceinline__ T wsum(T v)
+{
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
+struct FdmSmem {
+    size_t mats, d2, stage, total;
+};
+
+template <typename TS, typename TF, bool REFINE, int RPW>
+__host__ __device__ inline FdmSmem fdm_smem_layout(int ld)
+{
+    FdmSmem L{};
+    size_t o = 0;
+    L.mats = o;
+    o += (size_t)4 * ld * ld * sizeof(TF);  // Ws^T, Vs^T, Wa^T, Va^T (column-major, padded)
+    o = (o + 15) / 16 * 16;
+    L.d2 = o;
+    if (REFINE) o += (size_t)2 * ld * ld * sizeof(double);  // Ms^T, Ma^T
+    o = (o + 15) / 16 * 16;
+    L.stage = o;  // per warp, per row: 2*ld complex of the wider type
+    const size_t cw = 2 * (sizeof(TS) > sizeof(TF) ? sizeof(TS) : sizeof(TF));
+    o += (size_t)FDM_WARPS * RPW * 2 * ld * cw;
+    L.total = (o + 15) / 16 * 16;
+    return L;
+}
+
+// One folded solve: x = (Q^T) diag-solve (Q) applied to the folded input held
+// in registers (ins/ind: fold index lane + 32 t), result folded in xs/xd.
+template <typename TF, int NSS, int RPW>
+__device__ __forceinline__ void fdm_folded_core(const TF* Ws, const TF* Vs, const TF* Wa, const TF* Va, int ld, int ms,
+                                                int ma, const TF (&rs)[RPW][NSS], const TF (&ra)[RPW][NSS],
+                                                TF (&sr)[RPW][NSS], TF (&si)[RPW][NSS], TF (&dr)[RPW][NSS],
+                                                TF (&di)[RPW][NSS], cplx_t<TF>* stg, int lane)
+{
+    using C = cplx_t<TF>;
+    __syncwarp();
+#pragma unroll
+    for (int r = 0; r < RPW; ++r)
+#pragma unroll
+        for (int t = 0; t < NSS; ++t) {
+            stg[(size_t)r * 2 * ld + lane + 32 * t] = mk(sr[r][t], si[r][t]);
+            stg[(size_t)r * 2 * ld + ld + lane + 32 * t] = mk(dr[r][t], di[r][t]);
+        }
+    __syncwarp();
+    TF ar[RPW][NSS], ai[RPW][NSS], br[RPW][NSS], bi[RPW][NSS];
+#pragma unroll
+    for (int r = 0; r < RPW; ++r)
+#pragma unroll
+        for (int t = 0; t < NSS; ++t) { ar[r][t] = ai[r][t] = br[r][t] = bi[r][t] = (TF)0; }
+    // coefficients: c_s = Vs^-1 s, c_a = Va^-1 d
+    for (int k = 0; k < ms; ++k) {
+        TF w[NSS], u[NSS];
+        const bool anti = k < ma;
+#pragma unroll
+        for (int t = 0; t < NSS; ++t) {
+            w[t] = Ws[(size_t)k * ld + lane + 32 * t];
+            u[t] = anti ? Wa[(size_t)k * ld + lane + 32 * t] : (TF)0;
+        }
+#pragma unroll
+        for (int r = 0; r < RPW; ++r) {
+            const C s = stg[(size_t)r * 2 * ld + k];
+            const C d = stg[(size_t)r * 2 * ld + ld + k];
+#pragma unroll
+            for (int t = 0; t < NSS; ++t) {
+                ar[r][t] += w[t] * s.x;
+                ai[r][t] += w[t] * s.y;
+                br[r][t] += u[t] * d.x;
+                bi[r][t] += u[t] * d.y;
+            }
+        }
+    }
+    __syncwarp();
+#pragma unroll
+    for (int r = 0; r < RPW; ++r)
+#pragma unroll
+        for (int t = 0; t < NSS; ++t) {
+            stg[(size_t)r * 2 * ld + lane + 32 * t] = mk(ar[r][t] * rs[r][t], ai[r][t] * rs[r][t]);
+            stg[(size_t)r * 2 * ld + ld + lane + 32 * t] = mk(br[r][t] * ra[r][t], bi[r][t] * ra[r][t]);
+        }
+    __syncwarp();
+#pragma unroll
+    for (int r = 0; r < RPW; ++r)
+#pragma unroll
+        for (int t = 0; t < NSS; ++t) { sr[r][t] = si[r][t] = dr[r][t] = di[r][t] = (TF)0; }
+    // back to the folded grid: xs = Vs c_s, xd = Va c_a
+    for (int j = 0; j < ms; ++j) {
+        TF v[NSS], q[NSS];
+        const bool anti = j < ma;
+#pragma unroll
+        for (int t = 0; t < NSS; ++t) {
+            v[t] = Vs[(size_t)j * ld + lane + 32 * t];
+            q[t] = anti ? Va[(size_t)j * ld + lane + 32 * t] : (TF)0;
+        }
+#pragma unroll
+        for (int r = 0; r < RPW; ++r) {
+            const C cs = stg[(size_t)r * 2 * ld + j];
+            const C ca = stg[(size_t)r * 2 * ld + ld + j];
+#pragma unroll
+            for (int t = 0; t < NSS; ++t) {
+                sr[r][t] += v[t] * cs.x;
+                si[r][t] += v[t] * cs.y;
+                dr[r][t] += q[t] * ca.x;
+                di[r][t] += q[t] * ca.y;
+            }
+        }
+    }
+}
+
+template <typename TS, typename TF, int NSS, int RPW, bool REFINE, bool ADJ>
+__global__ void __launch_bounds__(FDM_WARPS * 32, 2) fdm_fast_kernel(FdmArgs a)
+{
+    using CS = cplx_t<TS>;
+    using CF = cplx_t<TF>;
+    extern __shared__ __align__(16) unsigned char fsm[];
+    const int ld = a.ld, ms = a.ms, ma = a.ma, m = a.m, n = a.n, P = a.P;
+    const FdmSmem Lay = fdm_smem_layout<TS, TF, REFINE, RPW>(ld);
+    TF* Ws = reinterpret_cast<TF*>(fsm + Lay.mats);
+    TF* Vs = Ws + (size_t)ld * ld;
+    TF* Wa = Vs + (size_t)ld * ld;
+    TF* Va = Wa + (size_t)ld * ld;
+    double* Ms = reinterpret_cast<double*>(fsm + Lay.d2);
+    double* Ma = Ms + (size_t)ld * ld;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const size_t cw = 2 * (sizeof(TS) > sizeof(TF) ? sizeof(TS) : sizeof(TF));
+    unsigned char* stg_raw = fsm + Lay.stage + (size_t)warp * RPW * 2 * ld * cw;
+
+    {
+        const TF* src = static_cast<const TF*>(a.mats);
+        for (int e = threadIdx.x; e < 4 * ld * ld; e += blockDim.x) Ws[e] = src[e];
+        if (REFINE)
+            for (int e = threadIdx.x; e < 2 * ld * ld; e += blockDim.x) Ms[e] = a.d2f[e];
+    }
+    __syncthreads();
+
+    CS* spec = static_cast<CS*>(a.spec);
+    const TF r2 = (TF)0.70710678118654752440;
+    const int nrows = a.nrows;
+    const long long npacks = (nrows + RPW - 1) / RPW;
+    const long long gw0 = (long long)blockIdx.x * FDM_WARPS + warp;
+    const long long nw = (long long)gridDim.x * FDM_WARPS;
+
+    for (long long pk = gw0; pk < npacks; pk += nw) {
+        int rowid[RPW], grp[RPW];
+        bool ok[RPW];
+#pragma unroll
+        for (int r = 0; r < RPW; ++r) {
+            const long long rr = pk * RPW + r;
+            ok[r] = rr < nrows;
+            rowid[r] = ok[r] ? a.rows[rr] : a.rows[0];
+            grp[r] = ok[r] ? a.row_grp[rr] : a.row_grp[0];
+        }
+        // ---- load the interior of each row and fold it ----
+        TS fsr[RPW][NSS], fsi[RPW][NSS], fdr[RPW][NSS], fdi[RPW][NSS];
+        {
+            CS* stg = reinterpret_cast<CS*>(stg_raw);
+            __syncwarp();
+#pragma unroll
+            for (int r = 0; r < RPW; ++r) {
+                const CS* row = spec + (long long)rowid[r] * P;
+                for (int i = lane; i < n; i += 32) stg[(size_t)r * 2 * ld + i] = row[1 + i];
+            }
+            __syncwarp();
+#pragma unroll
+            for (int r = 0; r < RPW; ++r)
+#pragma unroll
+                for (int t = 0; t < NSS; ++t) {
+                    const int k = lane + 32 * t;
+                    TS a0 = 0, a1 = 0, b0 = 0, b1 = 0;
+                    if (k < m) {
+                        const CS lo = stg[(size_t)r * 2 * ld + k], hi = stg[(size_t)r * 2 * ld + n - 1 - k];
+                        a0 = (TS)r2 * (lo.x + hi.x); a1 = (TS)r2 * (lo.y + hi.y);
+                        b0 = (TS)r2 * (lo.x - hi.x); b1 = (TS)r2 * (lo.y - hi.y);
+                    } else if (k < ms) {  // middle node of an odd n
+                        const CS mid = stg[(size_t)r * 2 * ld + k];
+                        a0 = mid.x; a1 = mid.y;
+                    }
+                    fsr[r][t] = a0; fsi[r][t] = a1; fdr[r][t] = b0; fdi[r][t] = b1;
+                }
+        }
+        // ---- reciprocal shifts of each row's group ----
+        TF rs[RPW][NSS], ra[RPW][NSS];
+#pragma unroll
+        for (int r = 0; r < RPW; ++r) {
+            const TF* rc = static_cast<const TF*>(a.recip) + (size_t)grp[r] * 2 * ld;
+#pragma unroll
+            for (int t = 0; t < NSS; ++t) {
+                rs[r][t] = rc[lane + 32 * t];
+                ra[r][t] = rc[ld + lane + 32 * t];
+            }
+        }
+        // ---- solve (+ FP64-residual refinement) in folded coordinates ----
+        TF sr[RPW][NSS], si[RPW][NSS], dr[RPW][NSS], di[RPW][NSS];
+#pragma unroll
+        for (int r = 0; r < RPW; ++r)
+#pragma unroll
+            for (int t = 0; t < NSS; ++t) {
+                sr[r][t] = (TF)fsr[r][t]; si[r][t] = (TF)fsi[r][t];
+                dr[r][t] = (TF)fdr[r][t]; di[r][t] = (TF)fdi[r][t];
+            }
+        fdm_folded_core<TF, NSS, RPW>(Ws, Vs, Wa, Va, ld, ms, ma, rs, ra, sr, si, dr, di,
+                                      reinterpret_cast<CF*>(stg_raw), lane);
+        TS xsr[RPW][NSS], xsi[RPW][NSS], xdr[RPW][NSS], xdi[RPW][NSS];
+#pragma unroll
+        for (int r = 0; r < RPW; ++r)
+#pragma unroll
+            for (int t = 0; t < NSS; ++t) {
+                xsr[r][t] = (TS)sr[r][t]; xsi[r][t] = (TS)si[r][t];
+                xdr[r][t] = (TS)dr[r][t]; xdi[r][t] = (TS)di[r][t];
+            }
+        if (REFINE) {
+            CS* stg = reinterpret_cast<CS*>(stg_raw);
+            double sg[RPW];
+#pragma unroll
+            for (int r = 0; r < RPW; ++r) sg[r] = a.sigma[grp[r]];
+            for (int sw = 0; sw < a.sweeps; ++sw) {
+                // r = f - (M x - sigma x) per folded block, FP64
+                __syncwarp();
+#pragma unroll
+                for (int r = 0; r < RPW; ++r)
+#pragma unroll
+                    for (int t = 0; t < NSS; ++t) {
+                        stg[(size_t)r * 2 * ld + lane + 32 * t] = mk(xsr[r][t], xsi[r][t]);
+                        stg[(size_t)r * 2 * ld + ld + lane + 32 * t] = mk(xdr[r][t], xdi[r][t]);
+                    }
+                __syncwarp();
+                TS rsr[RPW][NSS], rsi[RPW][NSS], rdr[RPW][NSS], rdi[RPW][NSS];
+#pragma unroll
+                for (int r = 0; r < RPW; ++r)
+#pragma unroll
+                    for (int t = 0; t < NSS; ++t) {
+                        rsr[r][t] = fsr[r][t] + (TS)sg[r] * xsr[r][t];
+                        rsi[r][t] = fsi[r][t] + (TS)sg[r] * xsi[r][t];
+                        rdr[r][t] = fdr[r][t] + (TS)sg[r] * xdr[r][t];
+                        rdi[r][t] = fdi[r][t] + (TS)sg[r] * xdi[r][t];
+                    }
+                for (int k = 0; k < ms; ++k) {
+                    double w[NSS], u[NSS];
+                    const bool anti = k < ma;
+#pragma unroll
+                    for (int t = 0; t < NSS; ++t) {
+                        w[t] = Ms[(size_t)k * ld + lane + 32 * t];
+                        u[t] = anti ? Ma[(size_t)k * ld + lane + 32 * t] : 0.0;
+                    }
+#pragma unroll
+                    for (int r = 0; r < RPW; ++r) {
+                        const CS xs = stg[(size_t)r * 2 * ld + k];
+                        const CS xd = stg[(size_t)r * 2 * ld + ld + k];
+#pragma unroll
+                        for (int t = 0; t < NSS; ++t) {
+                            rsr[r][t] -= w[t] * xs.x;
+                            rsi[r][t] -= w[t] * xs.y;
+                            rdr[r][t] -= u[t] * xd.x;
+                            rdi[r][t] -= u[t] * xd.y;
+                        }
+                    }
+                }
+#pragma unroll
+                for (int r = 0; r < RPW; ++r)
+#pragma unroll
+                    for (int t = 0; t < NSS; ++t) {
+                        sr[r][t] = (TF)rsr[r][t]; si[r][t] = (TF)rsi[r][t];
+                        dr[r][t] = (TF)rdr[r][t]; di[r][t] = (TF)rdi[r][t];
+                    }
+                fdm_folded_core<TF, NSS, RPW>(Ws, Vs, Wa, Va, ld, ms, ma, rs, ra, sr, si, dr, di,
+                                              reinterpret_cast<CF*>(stg_raw), lane);
+#pragma unroll
+                for (int r = 0; r < RPW; ++r)
+#pragma unroll
+                    for (int t = 0; t < NSS; ++t) {
+                        xsr[r][t] += (TS)sr[r][t]; xsi[r][t] += (TS)si[r][t];
+                        xdr[r][t] += (TS)dr[r][t]; xdi[r][t] += (TS)di[r][t];
+                    }
+            }
+        }
+        // ---- epilogue per row: boundary values, unfold, store ----
+#pragma unroll
+        for (int r = 0; r < RPW; ++r) {
+            if (!ok[r]) continue;  // warp-uniform
+            CS* row = spec + (long long)rowid[r] * P;
+            const int g = grp[r];
+            TS zlr = 0, zli = 0, zrr = 0, zri = 0;   // boundary values of the row
+            TS el = 0, er = 0;                       // weights of the per-group vectors hl / hr
+            TS elr = 0, eli = 0, err_ = 0, eri = 0;
+            const bool bnd = a.hvec != nullptr;
+            if (bnd) {
+                // folded dot products with e0 / eN (forward: D0, DN rows; adjoint: D2 boundary columns)
+                TS p0r = 0, p0i = 0, pNr = 0, pNi = 0;
+#pragma unroll
+                for (int t = 0; t < NSS; ++t) {
+                    const int k = lane + 32 * t;
+                    if (k < ms) {
+                        const TS e0s = (TS)a.e0f[k], eNs = (TS)a.eNf[k];
+                        p0r += e0s * xsr[r][t]; p0i += e0s * xsi[r][t];
+                        pNr += eNs * xsr[r][t]; pNi += eNs * xsi[r][t];
+                    }
+                    if (k < ma) {
+                        const TS e0a = (TS)a.e0f[ld + k], eNa = (TS)a.eNf[ld + k];
+                        p0r += e0a * xdr[r][t]; p0i += e0a * xdi[r][t];
+                        pNr += eNa * xdr[r][t]; pNi += eNa * xdi[r][t];
+                    }
+                }
+                p0r = wsum(p0r); p0i = wsum(p0i); pNr = wsum(pNr); pNi = wsum(pNi);
+                const CS wl = row[0], wr = row[P - 1];
+                const double* sc = a.hscal + (size_t)g * 4;
+                if (!ADJ) {
+                    // Robin ends, one element (NonPeriodic3D_MPI.cpp:334-336, 357-367, 528-529)
+                    const TS b0 = (TS)(-a.al * sc[0] + a.bl), c0 = (TS)(-a.al * sc[1]);
+                    const TS lb = (TS)(a.ar * sc[2]);
+                    const TS bR = (TS)(a.ar * sc[3] + a.br) - (c0 / b0) * lb;
+                    const TS rhr = wl.x + (TS)a.al * p0r, rhi = wl.y + (TS)a.al * p0i;
+                    const TS rRr = wr.x - (TS)a.ar * pNr - (rhr / b0) * lb;
+                    const TS rRi = wr.y - (TS)a.ar * pNi - (rhi / b0) * lb;
+                    zrr = rRr / bR; zri = rRi / bR;
+                    zlr = (rhr - c0 * zrr) / b0; zli = (rhi - c0 * zri) / b0;
+                } else {
+                    const TS m00 = (TS)sc[0], m01 = (TS)sc[1], m10 = (TS)sc[2], m11 = (TS)sc[3];
+                    const TS det = m00 * m11 - m01 * m10;
+                    const TS q0r = wl.x - p0r, q0i = wl.y - p0i, qNr = wr.x - pNr, qNi = wr.y - pNi;
+                    zlr = (m11 * q0r - m01 * qNr) / det; zli = (m11 * q0i - m01 * qNi) / det;
+                    zrr = (m00 * qNr - m10 * q0r) / det; zri = (m00 * qNi - m10 * q0i) / det;
+                }
+                elr = zlr; eli = zli; err_ = zrr; eri = zri;
+                (void)el; (void)er;
+            }
+            const double* hl = bnd ? a.hvec + (size_t)g * 2 * P : nullptr;
+            const double* hr = bnd ? hl + P : nullptr;
+#pragma unroll
+            for (int t = 0; t < NSS; ++t) {
+                const int k = lane + 32 * t;
+                if (k < m) {
+                    TS lo_r = (TS)r2 * (xsr[r][t] + xdr[r][t]), lo_i = (TS)r2 * (xsi[r][t] + xdi[r][t]);
+                    TS hi_r = (TS)r2 * (xsr[r][t] - xdr[r][t]), hi_i = (TS)r2 * (xsi[r][t] - xdi[r][t]);
+                    if (bnd) {
+                        const TS l0 = (TS)hl[1 + k], r0 = (TS)hr[1 + k];
+                        const TS l1 = (TS)hl[n - k], r1 = (TS)hr[n - k];
+                        lo_r += elr * l0 + err_ * r0; lo_i += eli * l0 + eri * r0;
+                        hi_r += elr * l1 + err_ * r1; hi_i += eli * l1 + eri * r1;
+                    }
+                    row[1 + k] = mk(lo_r, lo_i);
+                    row[n - k] = mk(hi_r, hi_i);
+                } else if (k < ms) {
+                    TS mr = xsr[r][t], mi = xsi[r][t];
+                    if (bnd) {
+                        const TS l0 = (TS)hl[1 + k], r0 = (TS)hr[1 + k];
+                        mr += elr * l0 + err_ * r0; mi += eli * l0 + eri * r0;
+                    }
+                    row[1 + k] = mk(mr, mi);
+                }
+            }
+            if (lane == 0) {
+                row[0] = mk(zlr, zli);
+                row[P - 1] = mk(zrr, zri);
+            }
+        }
+    }
+}
+
+template <typename TS, typename TF, int NSS, int RPW, bool REFINE, bool ADJ>
+static int run_fdm(const FdmArgs& a, cudaStream_t s)
+{
+    auto k = fdm_fast_kernel<TS, TF, NSS, RPW, REFINE, ADJ>;
+    const FdmSmem L = fdm_smem_layout<TS, TF, REFINE, RPW>(a.ld);
+    cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L.total);
+    if (e != cudaSuccess) return (int)e;
+    int dev = 0, sms = 148, per = 1;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k, FDM_WARPS * 32, L.total);
+    if (per < 1) per = 1;
+    const long long packs = (a.nrows + RPW - 1) / RPW;
+    long long grid = (packs + FDM_WARPS - 1) / FDM_WARPS;
+    if (grid > (long long)sms * per) grid = (long long)sms * per;
+    if (grid <= 0) return 0;
+    k<<<(unsigned)grid, FDM_WARPS * 32, L.total, s>>>(a);
+    return (int)cudaGetLastError();
+}
+
+template <int NSS>
+static int fdm_dispatch(int prec, const FdmArgs& a, cudaStream_t s)
+{
+    constexpr int RPW = NSS == 1 ? 4 : 2;  // rows per warp: keeps the accumulators in registers
+    if (a.adjoint) {
+        if (prec == 0) return run_fdm<double, double, NSS, RPW, false, true>(a, s);
+        if (prec == 1) return run_fdm<float, float, NSS, RPW, false, true>(a, s);
+        return run_fdm<double, float, NSS, RPW, true, true>(a, s);
+    }
+    if (prec == 0) return run_fdm<double, double, NSS, RPW, false, false>(a, s);
+    if (prec == 1) return run_fdm<float, float, NSS, RPW, false, false>(a, s);
+    return run_fdm<double, float, NSS, RPW, true, false>(a, s);
+}
+
+int launch_fdm_fast(int prec, const FdmArgs& a, cudaStream_t s)
+{
+    switch (a.ld / 32) {
+        case 1: return fdm_dispatch<1>(prec, a, s);
+        case 2: return fdm_dispatch<2>(prec, a, s);
+        default: return (int)cudaErrorInvalidValue;
+    }
+}
+
+size_t fdm_fast_smem_bytes(int prec, int ld)
+{
+    if (ld == 32) {
+        if (prec == 0) return fdm_smem_layout<double, double, false, 4>(ld).total;
+        if (prec == 1) return fdm_smem_layout<float, float, false, 4>(ld).total;
+        return fdm_smem_layout<double, float, true, 4>(ld).total;
+    }
+    if (prec == 0) return fdm_smem_layout<double, double, false, 2>(ld).total;
+    if (prec == 1) return fdm_smem_layout<float, float, false, 2>(ld).total;
+    return fdm_smem_layout<double, float, true, 2>(ld).total;
+}
+
+}  // namespace helm

@@ -1,0 +1,32 @@
+// Arguments of the folded fast-diagonalisation row solve (helm_fdm.cu).
+#pragma once
+#include <cstddef>
+#include <cuda_runtime.h>
+
+namespace helm {
+
+struct FdmArgs {
+    void* spec;          // complex spectrum rows [nrows_total][P]
+    int P, n, m, ms, ma; // GLL points, interior n = P-2, m = n/2, ms = m + n%2, ma = m
+    int ld;              // padded fold length (32 * ceil(ms/32))
+    int nrows;           // rows to solve
+    const int* rows;     // spectrum row of each work item (grouped by shift)
+    const int* row_grp;  // shift group of each work item
+    const void* mats;    // 4 column-major ld x ld blocks: first/second transform of the
+                         // symmetric block, then of the antisymmetric block
+    const double* d2f;   // refinement: the folded blocks of D2int (column-major), 2 x ld*ld
+    const void* recip;   // [groups][2][ld]: 1/(lambda_s - sigma), 1/(lambda_a - sigma)
+    const double* sigma; // [groups]
+    int sweeps;
+    const double* e0f;   // [2][ld] folded weights of the first boundary functional
+    const double* eNf;   // [2][ld] folded weights of the second
+    const double* hvec;  // [groups][2][P] vectors combined with the boundary values (NULL: none)
+    const double* hscal; // [groups][4] scalars of the boundary system
+    double al, bl, ar, br;
+    int adjoint;
+};
+
+int launch_fdm_fast(int prec, const FdmArgs& a, cudaStream_t s);
+size_t fdm_fast_smem_bytes(int prec, int ld);
+
+}  // namespace helm

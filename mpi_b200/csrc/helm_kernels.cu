@@ -403,7 +403,7 @@ __host__ __device__ inline RowSmem row_smem_layout(int n, int ld)
     return L;
 }
 
-template <typename TS, typename TF, int NSLOT, int METHOD, bool REFINE>
+template <typename TS, typename TF, int NSLOT, int METHOD, bool REFINE, bool ADJ = false>
 __global__ void __launch_bounds__(ROW_WARPS * 32) rows_kernel(RowArgs a)
 {
     using CS = cplx_t<TS>;
@@ -515,6 +515,41 @@ __global__ void __launch_bounds__(ROW_WARPS * 32) rows_kernel(RowArgs a)
                         for (int s = 0; s < NSLOT; ++s) { xr[s] += (TS)yr[s]; xi[s] += (TS)yi[s]; }
                     }
                 }
+                if (ADJ) {
+                    // transposed collocation system: boundary unknowns from the 2x2
+                    // system, interior = psi + v0 pl + vN pr (one element)
+                    TS a0r = 0, a0i = 0, aNr = 0, aNi = 0;
+#pragma unroll
+                    for (int s = 0; s < NSLOT; ++s) {
+                        const int i = lane + 32 * s;
+                        if (i < n) {
+                            const TS c0 = (TS)a.d0[1 + i], cN = (TS)a.dN[1 + i];
+                            a0r += c0 * xr[s]; a0i += c0 * xi[s];
+                            aNr += cN * xr[s]; aNi += cN * xi[s];
+                        }
+                    }
+                    a0r = warp_sum(a0r); a0i = warp_sum(a0i);
+                    aNr = warp_sum(aNr); aNi = warp_sum(aNi);
+                    const CS w0 = row[0], wN = row[P - 1];
+                    const double* m = a.homs + grp * 4;
+                    const TS m00 = (TS)m[0], m01 = (TS)m[1], m10 = (TS)m[2], m11 = (TS)m[3];
+                    const TS det = m00 * m11 - m01 * m10;
+                    const TS q0r = w0.x - a0r, q0i = w0.y - a0i, qNr = wN.x - aNr, qNi = wN.y - aNi;
+                    const TS v0r = (m11 * q0r - m01 * qNr) / det, v0i = (m11 * q0i - m01 * qNi) / det;
+                    const TS vNr = (m00 * qNr - m10 * q0r) / det, vNi = (m00 * qNi - m10 * q0i) / det;
+                    const double* pl = a.hom + (size_t)grp * 2 * P;
+                    const double* pr_ = pl + P;
+#pragma unroll
+                    for (int s = 0; s < NSLOT; ++s) {
+                        const int i = lane + 32 * s;
+                        if (i < n) {
+                            const TS l = (TS)pl[1 + i], r = (TS)pr_[1 + i];
+                            row[1 + i] = mk(xr[s] + v0r * l + vNr * r, xi[s] + v0i * l + vNi * r);
+                        }
+                    }
+                    if (lane == 0) { row[0] = mk(v0r, v0i); row[P - 1] = mk(vNr, vNi); }
+                    continue;
+                }
                 if (!hom_active) {
 #pragma unroll
                     for (int s = 0; s < NSLOT; ++s) {
@@ -565,7 +600,7 @@ __global__ void __launch_bounds__(ROW_WARPS * 32) rows_kernel(RowArgs a)
                     }
                 }
             }
-            if (!hom_active) continue;
+            if (ADJ || !hom_active) continue;
             // ---- right end, back sweep, combination ----
             CS* lastrow = spec + (long long)(Ns - 1) * a.elem_stride + rowoff;
             const CS gr = lastrow[P - 1];
@@ -619,10 +654,10 @@ __global__ void __launch_bounds__(ROW_WARPS * 32) rows_kernel(RowArgs a)
     }
 }
 
-template <typename TS, typename TF, int NSLOT, int METHOD, bool REFINE>
+template <typename TS, typename TF, int NSLOT, int METHOD, bool REFINE, bool ADJ = false>
 static int run_rows(const RowArgs& a, cudaStream_t s)
 {
-    auto k = rows_kernel<TS, TF, NSLOT, METHOD, REFINE>;
+    auto k = rows_kernel<TS, TF, NSLOT, METHOD, REFINE, ADJ>;
     const RowSmem L = row_smem_layout<TS, TF, METHOD, REFINE>(a.n, a.ldf);
     cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L.total);
     if (e != cudaSuccess) return (int)e;
@@ -643,6 +678,12 @@ static int run_rows(const RowArgs& a, cudaStream_t s)
 template <int NSLOT>
 static int rows_dispatch_prec(int method, int prec, const RowArgs& a, cudaStream_t s)
 {
+    if (a.adjoint) {  // transposed solve: FDM only, one element
+        if (method != 2 || a.Ns != 1) return (int)cudaErrorInvalidValue;
+        if (prec == 0) return run_rows<double, double, NSLOT, 2, false, true>(a, s);
+        if (prec == 1) return run_rows<float, float, NSLOT, 2, false, true>(a, s);
+        return run_rows<double, float, NSLOT, 2, true, true>(a, s);
+    }
     if (method == 1) {
         if (prec == 0) return run_rows<double, double, NSLOT, 1, false>(a, s);
         if (prec == 1) return run_rows<float, float, NSLOT, 1, false>(a, s);
@@ -651,6 +692,56 @@ static int rows_dispatch_prec(int method, int prec, const RowArgs& a, cudaStream
     if (prec == 0) return run_rows<double, double, NSLOT, 2, false>(a, s);
     if (prec == 1) return run_rows<float, float, NSLOT, 2, false>(a, s);
     return run_rows<double, float, NSLOT, 2, true>(a, s);
+}
+
+// Adjoint output split: the adjoint pipeline leaves v = A^-T ubar in fbar with
+// every GLL slot filled.  One warp per (x, y) column moves slot 0 / P-1 to
+// glbar / grbar (dL/dgl, dL/dgr), zeroes them in fbar (f is never read there),
+// and accumulates lambda_bar += sum over the interior slots of fbar * u.
+__global__ void __launch_bounds__(256) adjoint_finalize_kernel(double* fbar, double* glbar, double* grbar,
+                                                               const double* u, double* lambda_bar, int Nx, int Ny,
+                                                               int P, long long x_stride, long long bc_row)
+{
+    __shared__ double red[8];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const long long ncol = (long long)Nx * Ny;
+    const long long nw = (long long)gridDim.x * 8;
+    double acc = 0.0;
+    for (long long c = (long long)blockIdx.x * 8 + warp; c < ncol; c += nw) {
+        const int i = (int)(c / Ny), j = (int)(c - (long long)(c / Ny) * Ny);
+        double* col = fbar + (long long)i * x_stride + (long long)j * P;
+        const double* uc = u ? u + (long long)i * x_stride + (long long)j * P : nullptr;
+        for (int k = lane; k < P; k += 32) {
+            const double v = col[k];
+            if (k == 0 || k == P - 1) {
+                if (k == 0 && glbar) glbar[(long long)i * bc_row + j] = v;
+                if (k == P - 1 && grbar) grbar[(long long)i * bc_row + j] = v;
+                col[k] = 0.0;
+            } else if (uc) {
+                acc += v * uc[k];
+            }
+        }
+    }
+    if (!lambda_bar) return;
+    acc = warp_sum(acc);
+    if (lane == 0) red[warp] = acc;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double s = 0.0;
+        for (int w = 0; w < 8; ++w) s += red[w];
+        atomicAdd(lambda_bar, s);
+    }
+}
+
+int launch_adjoint_finalize(double* fbar, double* glbar, double* grbar, const double* u, double* lambda_bar, int Nx,
+                            int Ny, int P, long long x_stride, long long bc_row, cudaStream_t s)
+{
+    const long long ncol = (long long)Nx * Ny;
+    long long blocks = (ncol + 7) / 8;
+    if (blocks > 148 * 16) blocks = 148 * 16;
+    adjoint_finalize_kernel<<<(unsigned)blocks, 256, 0, s>>>(fbar, glbar, grbar, u, lambda_bar, Nx, Ny, P, x_stride,
+                                                            bc_row);
+    return (int)cudaGetLastError();
 }
 
 size_t rows_smem_bytes(int method, int prec, int n, int ld)

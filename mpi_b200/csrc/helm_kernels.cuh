@@ -57,6 +57,12 @@ struct RowArgs {
     const double* d2t;         // refinement: column-major interior D2 [n][n]
     int sweeps;
     double al, bl, ar, br;
+    // Adjoint (transposed) solve, Ns = 1, FDM: vinvT / vT then hold the
+    // transposed transforms, d2t the transposed D2, d0 / dN the boundary
+    // columns D2[int][0] / D2[int][N-1], hom the per-group interior vectors
+    // pl = -A^-T r0 and pr = -A^-T rN, homs the 2x2 boundary matrix
+    // [[m00, m01], [m10, m11]] of the transposed system (row-major).
+    int adjoint;
 };
 
 // Launchers (helm_kernels.cu).  Return a cudaError_t.
@@ -66,6 +72,9 @@ int launch_fft(int L, int mode, int dir, int t_double, int io_bytes, const FftAr
                cudaStream_t s);
 // method: 1 = LU, 2 = FDM; prec: 0 = FP64, 1 = FP32, 2 = FP32 with FP64 refinement
 int launch_rows(int method, int prec, const RowArgs& a, cudaStream_t s);
+// Adjoint output split (boundary slots -> glbar/grbar, lambda_bar reduction).
+int launch_adjoint_finalize(double* fbar, double* glbar, double* grbar, const double* u, double* lambda_bar, int Nx,
+                            int Ny, int P, long long x_stride, long long bc_row, cudaStream_t s);
 // Dynamic shared memory rows_kernel needs for this method / precision / size.
 size_t rows_smem_bytes(int method, int prec, int n, int ld);
 constexpr size_t kMaxSmemPerBlock = 232448;  // 227 KB opt-in limit of sm_100

@@ -10,6 +10,7 @@
 // kernels on the caller's stream: x-FFT (R2C) -> y-FFT -> row solves -> inverse
 // y-FFT -> x-FFT (C2R); 2D plans skip the y passes.
 #include "../../include/helm_b200.h"
+#include "helm_fdm.cuh"
 #include "helm_kernels.cuh"
 #include "helm_plan.hpp"
 #include "helm_setup.hpp"
@@ -40,6 +41,8 @@ static const double kRefPi = 3.1415926535897932;
 
 void Plan::release()
 {
+    for (cudaEvent_t& e : ev)
+        if (e) { cudaEventDestroy(e); e = nullptr; }
     for (void* p : allocations) cudaFree(p);
     allocations.clear();
     device_bytes = 0;
@@ -116,6 +119,215 @@ static void build_groups(Plan& p)
         p.grp_start.push_back((int)p.grp_rows.size());
     }
     p.ngroups = (int)p.sigma.size();
+}
+
+// Data of the transposed per-wavenumber system M_sigma^T v = w (one element,
+// FDM): M_sigma has the interior rows D2[k][:] - sigma e_k and the Robin rows
+// (betal - alphal D[0][0], -alphal D[0][int], -alphal D[0][N-1]) and
+// (alphar D[N-1][0], alphar D[N-1][int], betar + alphar D[N-1][N-1]).
+// Eliminating the interior, v_int = psi + v0 pl + vN pr with psi = A^-T w_int,
+// pl = -A^-T r0, pr = -A^-T rN, and (v0, vN) solve a 2x2 system.
+static int setup_adjoint(Plan& p, const std::vector<double>& A0, const std::vector<double>& lam,
+                         const std::vector<double>& V, const std::vector<double>& Vi, int prec_code)
+{
+    const int N = p.N, n = p.n, ld = p.ld, G = p.ngroups;
+    const std::vector<double>& D = p.gll.D;
+    const std::vector<double>& D2 = p.gll.D2;
+    const double al = p.bc.alphal, bl = p.bc.betal, ar = p.bc.alphar, br = p.bc.betar;
+    std::vector<double> r0(n), rN(n), c0(N, 0.0), cN(N, 0.0);
+    for (int i = 0; i < n; ++i) {
+        r0[i] = -al * D[i + 1];
+        rN[i] = ar * D[(N - 1) * N + i + 1];
+        c0[i + 1] = D2[(i + 1) * N];
+        cN[i + 1] = D2[(i + 1) * N + N - 1];
+    }
+    const double a00 = bl - al * D[0], a0N = -al * D[N - 1];
+    const double aN0 = ar * D[(N - 1) * N], aNN = br + ar * D[(N - 1) * N + N - 1];
+    std::vector<double> vr0(n), vrN(n);  // V^T r0, V^T rN
+    for (int j = 0; j < n; ++j) {
+        double s0 = 0, s1 = 0;
+        for (int k = 0; k < n; ++k) { s0 += V[k * n + j] * r0[k]; s1 += V[k * n + j] * rN[k]; }
+        vr0[j] = s0;
+        vrN[j] = s1;
+    }
+    std::vector<double> hom((size_t)G * 2 * N, 0.0), homs((size_t)G * 4);
+    for (int g = 0; g < G; ++g) {
+        double* pl = &hom[(size_t)g * 2 * N];
+        double* pr = pl + N;
+        const double sig = p.sigma[g];
+        for (int i = 0; i < n; ++i) {
+            double s0 = 0, s1 = 0;
+            for (int j = 0; j < n; ++j) {
+                const double rr = 1.0 / (lam[j] - sig);
+                s0 += Vi[j * n + i] * vr0[j] * rr;
+                s1 += Vi[j * n + i] * vrN[j] * rr;
+            }
+            pl[i + 1] = -s0;
+            pr[i + 1] = -s1;
+        }
+        double c0pl = 0, c0pr = 0, cNpl = 0, cNpr = 0;
+        for (int i = 1; i <= n; ++i) {
+            c0pl += c0[i] * pl[i]; c0pr += c0[i] * pr[i];
+            cNpl += cN[i] * pl[i]; cNpr += cN[i] * pr[i];
+        }
+        homs[(size_t)g * 4 + 0] = a00 + c0pl;
+        homs[(size_t)g * 4 + 1] = aN0 + c0pr;
+        homs[(size_t)g * 4 + 2] = a0N + cNpl;
+        homs[(size_t)g * 4 + 3] = aNN + cNpr;
+        const double det = homs[g * 4] * homs[g * 4 + 3] - homs[g * 4 + 1] * homs[g * 4 + 2];
+        if (!(std::fabs(det) > 0.0)) { g_last_error = "singular boundary system of the adjoint"; return HELM_ERR_SINGULAR; }
+    }
+    std::vector<double> vtT((size_t)n * ld, 0.0), vinvtT((size_t)n * ld, 0.0), d2row((size_t)n * ld, 0.0);
+    for (int k = 0; k < n; ++k)
+        for (int i = 0; i < n; ++i) {
+            vtT[(size_t)k * ld + i] = V[k * n + i];
+            vinvtT[(size_t)k * ld + i] = Vi[k * n + i];
+            d2row[(size_t)k * ld + i] = A0[k * n + i];
+        }
+    int st;
+    auto up_mat = [&](const std::vector<double>& h, void** d) -> int {
+        if (prec_code == 0) return p.upload(d, h.data(), h.size() * sizeof(double));
+        std::vector<float> f(h.begin(), h.end());
+        return p.upload(d, f.data(), f.size() * sizeof(float));
+    };
+    if ((st = up_mat(vtT, &p.d_vtT))) return st;
+    if ((st = up_mat(vinvtT, &p.d_vinvtT))) return st;
+    if ((st = p.upload((void**)&p.d_d2row, d2row.data(), d2row.size() * sizeof(double)))) return st;
+    if ((st = p.upload((void**)&p.d_c0, c0.data(), c0.size() * sizeof(double)))) return st;
+    if ((st = p.upload((void**)&p.d_cN, cN.data(), cN.size() * sizeof(double)))) return st;
+    if ((st = p.upload((void**)&p.d_hom_adj, hom.data(), hom.size() * sizeof(double)))) return st;
+    if ((st = p.upload((void**)&p.d_homs_adj, homs.data(), homs.size() * sizeof(double)))) return st;
+    p.adj_ready = true;
+    return HELM_OK;
+}
+
+// Folded fast-diagonalisation data (helm_fdm.cu): the orthogonal even/odd
+// fold Q of the interior nodes block-diagonalises the centrosymmetric D2int,
+// Q D2int Q^T = diag(Ms, Ma); each block gets its own eigen-decomposition.
+static int setup_fast(Plan& p, const std::vector<double>& A0, int prec_code)
+{
+    const int n = p.n, m = n / 2, odd = n % 2, ms = m + odd, ma = m, N = p.N, G = p.ngroups;
+    const int ld = 32 * ((ms + 31) / 32);
+    if (fdm_fast_smem_bytes(prec_code, ld) > kMaxSmemPerBlock || ld > 64) return HELM_OK;  // stay on rows_kernel
+    const double r2 = 0.70710678118654752440;
+    std::vector<double> Q((size_t)n * n, 0.0), T((size_t)n * n, 0.0), Mf((size_t)n * n, 0.0);
+    for (int k = 0; k < m; ++k) {
+        Q[(size_t)k * n + k] = r2;
+        Q[(size_t)k * n + n - 1 - k] = r2;
+        Q[(size_t)(ms + k) * n + k] = r2;
+        Q[(size_t)(ms + k) * n + n - 1 - k] = -r2;
+    }
+    if (odd) Q[(size_t)m * n + m] = 1.0;
+    for (int i = 0; i < n; ++i)  // T = Q A0
+        for (int j = 0; j < n; ++j) {
+            double s = 0;
+            for (int k = 0; k < n; ++k) s += Q[(size_t)i * n + k] * A0[(size_t)k * n + j];
+            T[(size_t)i * n + j] = s;
+        }
+    double amax = 0, off = 0;
+    for (int i = 0; i < n; ++i)  // Mf = T Q^T
+        for (int j = 0; j < n; ++j) {
+            double s = 0;
+            for (int k = 0; k < n; ++k) s += T[(size_t)i * n + k] * Q[(size_t)j * n + k];
+            Mf[(size_t)i * n + j] = s;
+            amax = std::max(amax, std::fabs(s));
+            if ((i < ms) != (j < ms)) off = std::max(off, std::fabs(s));
+        }
+    if (off > 1e-11 * amax) return HELM_OK;  // not centrosymmetric to rounding: keep rows_kernel
+    std::vector<double> Ms((size_t)ms * ms), Ma((size_t)ma * ma);
+    for (int i = 0; i < ms; ++i)
+        for (int j = 0; j < ms; ++j) Ms[(size_t)i * ms + j] = Mf[(size_t)i * n + j];
+    for (int i = 0; i < ma; ++i)
+        for (int j = 0; j < ma; ++j) Ma[(size_t)i * ma + j] = Mf[(size_t)(ms + i) * n + ms + j];
+    std::vector<double> ls(ms), Vs((size_t)ms * ms), Vsi((size_t)ms * ms), la(ma), Va((size_t)ma * ma), Vai((size_t)ma * ma);
+    if (!real_eigen(ms, Ms.data(), ls.data(), Vs.data(), Vsi.data())) return HELM_OK;
+    if (ma > 0 && !real_eigen(ma, Ma.data(), la.data(), Va.data(), Vai.data())) return HELM_OK;
+
+    const size_t L2 = (size_t)ld * ld;
+    std::vector<double> fw(4 * L2, 0.0), fa(4 * L2, 0.0), d2f(2 * L2, 0.0), d2a(2 * L2, 0.0);
+    for (int i = 0; i < ms; ++i)
+        for (int j = 0; j < ms; ++j) {
+            fw[0 * L2 + (size_t)j * ld + i] = Vsi[(size_t)i * ms + j];  // first: Vs^-1, column-major
+            fw[1 * L2 + (size_t)j * ld + i] = Vs[(size_t)i * ms + j];   // second: Vs
+            fa[0 * L2 + (size_t)j * ld + i] = Vs[(size_t)j * ms + i];   // adjoint first: Vs^T
+            fa[1 * L2 + (size_t)j * ld + i] = Vsi[(size_t)j * ms + i];  // adjoint second: Vs^-T
+            d2f[0 * L2 + (size_t)j * ld + i] = Ms[(size_t)i * ms + j];
+            d2a[0 * L2 + (size_t)j * ld + i] = Ms[(size_t)j * ms + i];
+        }
+    for (int i = 0; i < ma; ++i)
+        for (int j = 0; j < ma; ++j) {
+            fw[2 * L2 + (size_t)j * ld + i] = Vai[(size_t)i * ma + j];
+            fw[3 * L2 + (size_t)j * ld + i] = Va[(size_t)i * ma + j];
+            fa[2 * L2 + (size_t)j * ld + i] = Va[(size_t)j * ma + i];
+            fa[3 * L2 + (size_t)j * ld + i] = Vai[(size_t)j * ma + i];
+            d2f[1 * L2 + (size_t)j * ld + i] = Ma[(size_t)i * ma + j];
+            d2a[1 * L2 + (size_t)j * ld + i] = Ma[(size_t)j * ma + i];
+        }
+    std::vector<double> recip((size_t)G * 2 * ld, 0.0);
+    for (int g = 0; g < G; ++g) {
+        const double sg = p.sigma[g];
+        for (int j = 0; j < ms; ++j) {
+            const double d = ls[j] - sg;
+            if (!(std::fabs(d) > 1e-12 * std::max(std::fabs(ls[j]), std::fabs(sg)))) {
+                g_last_error = "shifted GLL operator is singular";
+                return HELM_ERR_SINGULAR;
+            }
+            recip[(size_t)g * 2 * ld + j] = 1.0 / d;
+        }
+        for (int j = 0; j < ma; ++j) {
+            const double d = la[j] - sg;
+            if (!(std::fabs(d) > 1e-12 * std::max(std::fabs(la[j]), std::fabs(sg)))) {
+                g_last_error = "shifted GLL operator is singular";
+                return HELM_ERR_SINGULAR;
+            }
+            recip[(size_t)g * 2 * ld + ld + j] = 1.0 / d;
+        }
+    }
+    // folded boundary functionals: e_f = Q e restricted to the two blocks
+    auto fold = [&](const std::vector<double>& e) {
+        std::vector<double> out(2 * ld, 0.0);
+        for (int i = 0; i < n; ++i) {
+            double s = 0;
+            for (int k = 0; k < n; ++k) s += Q[(size_t)i * n + k] * e[k];
+            if (i < ms) out[i] = s; else out[ld + (i - ms)] = s;
+        }
+        return out;
+    };
+    const std::vector<double>& D = p.gll.D;
+    const std::vector<double>& D2 = p.gll.D2;
+    std::vector<double> e0(n), eN(n), c0(n), cN(n);
+    for (int i = 0; i < n; ++i) {
+        e0[i] = D[i + 1];
+        eN[i] = D[(size_t)(N - 1) * N + i + 1];
+        c0[i] = D2[(size_t)(i + 1) * N];
+        cN[i] = D2[(size_t)(i + 1) * N + N - 1];
+    }
+    std::vector<double> fe0 = fold(e0), feN = fold(eN), fc0 = fold(c0), fcN = fold(cN);
+    std::vector<int> row_grp(p.grp_rows.size());
+    for (int g = 0; g < G; ++g)
+        for (int rr = p.grp_start[g]; rr < p.grp_start[g + 1]; ++rr) row_grp[rr] = g;
+    int st;
+    auto up_t = [&](const std::vector<double>& h, void** d) -> int {
+        if (prec_code == 0) return p.upload(d, h.data(), h.size() * sizeof(double));
+        std::vector<float> f(h.begin(), h.end());
+        return p.upload(d, f.data(), f.size() * sizeof(float));
+    };
+    if ((st = up_t(fw, &p.d_fmats))) return st;
+    if ((st = up_t(fa, &p.d_fmats_adj))) return st;
+    if ((st = up_t(recip, &p.d_frecip))) return st;
+    if ((st = p.upload((void**)&p.d_fd2, d2f.data(), d2f.size() * sizeof(double)))) return st;
+    if ((st = p.upload((void**)&p.d_fd2_adj, d2a.data(), d2a.size() * sizeof(double)))) return st;
+    if ((st = p.upload((void**)&p.d_row_grp, row_grp.data(), row_grp.size() * sizeof(int)))) return st;
+    if ((st = p.upload((void**)&p.d_fe0, fe0.data(), fe0.size() * sizeof(double)))) return st;
+    if ((st = p.upload((void**)&p.d_feN, feN.data(), feN.size() * sizeof(double)))) return st;
+    if ((st = p.upload((void**)&p.d_fc0, fc0.data(), fc0.size() * sizeof(double)))) return st;
+    if ((st = p.upload((void**)&p.d_fcN, fcN.data(), fcN.size() * sizeof(double)))) return st;
+    p.fm = m;
+    p.fms = ms;
+    p.fma = ma;
+    p.fld = ld;
+    p.fast = true;
+    return HELM_OK;
 }
 
 static int setup_plan(Plan& p)
@@ -277,12 +489,16 @@ static int setup_plan(Plan& p)
     p.h_lam = lam;
     p.h_V = V;
     p.h_Vi = Vi;
+    if (!lu && p.Ns == 1) {
+        if ((st = setup_adjoint(p, A0, lam, V, Vi, prec_code))) return st;
+        if ((st = setup_fast(p, A0, prec_code))) return st;
+    }
     return HELM_OK;
 }
 
 static int fft_pass(Plan& p, int L, int mode, int dir, const void* in, void* out, long long in_row, long long out_row,
                     long long in_batch, long long out_batch, int ncols, int nbatch, double scale, const void* tw,
-                    const double* gl, const double* gr, cudaStream_t s)
+                    const double* gl, const double* gr, bool inject, bool io_double, cudaStream_t s)
 {
     FftArgs a{};
     a.in = in;
@@ -298,32 +514,42 @@ static int fft_pass(Plan& p, int L, int mode, int dir, const void* in, void* out
     a.gl = gl;
     a.gr = gr;
     a.bc_row = p.dim == 3 ? p.bc_x_stride : 1;
-    a.P = (mode == FFT_R2C) ? p.N : 0;
+    a.P = (mode == FFT_R2C && inject) ? p.N : 0;
     a.gl_batch = 0;
     a.gr_batch = p.Ns - 1;
     const long long ccols = (mode == FFT_C2C) ? ncols : (ncols + 1) / 2;
     const int td = p.precision != HELM_FP32;
-    const int io = td ? 8 : p.io_bytes;
+    const int io = (td || io_double) ? 8 : p.io_bytes;
     int e = launch_fft(L, mode, dir, td, io, a, ccols * nbatch, s);
     if (e) return set_cuda_error((cudaError_t)e, "fft launch");
     return HELM_OK;
 }
 
-int solve(Plan& p, const void* f, const double* gl, const double* gr, void* u, cudaStream_t s)
+// The five kernels of a solve.  Forward: in = f with gl/gr injected into the
+// GLL boundary slots of the spectrum, out = u.  Adjoint: in = ubar read in
+// every slot, the transposed row solve, out = A^-T ubar in every slot.
+static int run_pipeline(Plan& p, const void* in, const double* gl, const double* gr, void* out, bool adjoint,
+                        cudaStream_t s)
 {
     const int N = p.N;
     const long long cols = (long long)(p.dim == 3 ? p.Ny : 1) * N;  // real columns per x row
     const int nkx = p.Nx / 2 + 1;
     int st;
-    // 1. x: real-to-complex, GLL boundary slots take the boundary data
-    if ((st = fft_pass(p, p.Nx, FFT_R2C, -1, f, p.d_spec, p.x_stride, cols, p.elem_stride, p.elem_spec, (int)cols, p.Ns,
-                       1.0, p.d_tw_x, gl, gr, s)))
+    auto mark = [&](int i) {
+        if (p.stage_timing && !adjoint) cudaEventRecord(p.ev[i], s);
+    };
+    mark(0);
+    // 1. x: real-to-complex (forward: GLL boundary slots take the boundary data)
+    if ((st = fft_pass(p, p.Nx, FFT_R2C, -1, in, p.d_spec, p.x_stride, cols, p.elem_stride, p.elem_spec, (int)cols,
+                       p.Ns, 1.0, p.d_tw_x, gl, gr, !adjoint, adjoint, s)))
         return st;
+    mark(1);
     // 2. y: complex-to-complex along the middle axis
     if (p.dim == 3 &&
         (st = fft_pass(p, p.Ny, FFT_C2C, -1, p.d_spec, p.d_spec, N, N, (long long)p.Ny * N, (long long)p.Ny * N, N,
-                       p.Ns * nkx, 1.0, p.d_tw_y, nullptr, nullptr, s)))
+                       p.Ns * nkx, 1.0, p.d_tw_y, nullptr, nullptr, false, false, s)))
         return st;
+    mark(2);
     // 3. per-wavenumber collocation solves + interface sweep + combination
     RowArgs r{};
     r.spec = p.d_spec;
@@ -339,34 +565,102 @@ int solve(Plan& p, const void* f, const double* gl, const double* gr, void* u, c
     r.perm = p.d_perm;
     r.ldf = p.ld;
     r.fac_stride = (long long)p.n * p.ld;
-    r.vinvT = p.d_vinvT;
-    r.vT = p.d_vT;
     r.lam = p.d_lam;
-    const bool hom = p.Ns > 1 || p.bc.alphal != 0.0 || p.bc.alphar != 0.0 || gl != nullptr || gr != nullptr;
-    r.hom = hom ? p.d_hom : nullptr;
-    r.homs = p.d_homs;
-    r.d0 = p.d_d0;
-    r.dN = p.d_dN;
     r.sigma = p.d_sigma;
-    r.d2t = p.d_d2t;
     r.sweeps = p.sweeps;
     r.al = p.bc.alphal;
     r.bl = p.bc.betal;
     r.ar = p.bc.alphar;
     r.br = p.bc.betar;
+    if (!adjoint) {
+        r.vinvT = p.d_vinvT;
+        r.vT = p.d_vT;
+        const bool hom = p.Ns > 1 || p.bc.alphal != 0.0 || p.bc.alphar != 0.0 || gl != nullptr || gr != nullptr;
+        r.hom = hom ? p.d_hom : nullptr;
+        r.homs = p.d_homs;
+        r.d0 = p.d_d0;
+        r.dN = p.d_dN;
+        r.d2t = p.d_d2t;
+    } else {
+        r.adjoint = 1;
+        r.vinvT = p.d_vtT;
+        r.vT = p.d_vinvtT;
+        r.hom = p.d_hom_adj;
+        r.homs = p.d_homs_adj;
+        r.d0 = p.d_c0;
+        r.dN = p.d_cN;
+        r.d2t = p.d_d2row;
+    }
     const int prec = p.precision == HELM_FP64 ? 0 : (p.precision == HELM_FP32 ? 1 : 2);
-    int e = launch_rows(p.method, prec, r, s);
+    int e;
+    if (p.fast) {
+        FdmArgs fa{};
+        fa.spec = p.d_spec;
+        fa.P = N;
+        fa.n = p.n;
+        fa.m = p.fm;
+        fa.ms = p.fms;
+        fa.ma = p.fma;
+        fa.ld = p.fld;
+        fa.nrows = (int)p.grp_rows.size();
+        fa.rows = p.d_grp_rows;
+        fa.row_grp = p.d_row_grp;
+        fa.mats = adjoint ? p.d_fmats_adj : p.d_fmats;
+        fa.d2f = adjoint ? p.d_fd2_adj : p.d_fd2;
+        fa.recip = p.d_frecip;
+        fa.sigma = p.d_sigma;
+        fa.sweeps = p.sweeps;
+        fa.e0f = adjoint ? p.d_fc0 : p.d_fe0;
+        fa.eNf = adjoint ? p.d_fcN : p.d_feN;
+        fa.hvec = adjoint ? p.d_hom_adj : r.hom;
+        fa.hscal = adjoint ? p.d_homs_adj : p.d_homs;
+        fa.al = p.bc.alphal;
+        fa.bl = p.bc.betal;
+        fa.ar = p.bc.alphar;
+        fa.br = p.bc.betar;
+        fa.adjoint = adjoint ? 1 : 0;
+        e = launch_fdm_fast(prec, fa, s);
+    } else {
+        e = launch_rows(p.method, prec, r, s);
+    }
     if (e) return set_cuda_error((cudaError_t)e, "row-solve launch");
+    mark(3);
     // 4. inverse y
     if (p.dim == 3 &&
         (st = fft_pass(p, p.Ny, FFT_C2C, 1, p.d_spec, p.d_spec, N, N, (long long)p.Ny * N, (long long)p.Ny * N, N,
-                       p.Ns * nkx, 1.0, p.d_tw_y, nullptr, nullptr, s)))
+                       p.Ns * nkx, 1.0, p.d_tw_y, nullptr, nullptr, false, false, s)))
         return st;
+    mark(4);
     // 5. x: complex-to-real, scaled by 1/(Nx Ny) (the reference's /Nx, /Ny)
     const double scale = 1.0 / ((double)p.Nx * (p.dim == 3 ? p.Ny : 1));
-    if ((st = fft_pass(p, p.Nx, FFT_C2R, 1, p.d_spec, u, cols, p.x_stride, p.elem_spec, p.elem_stride, (int)cols, p.Ns,
-                       scale, p.d_tw_x, nullptr, nullptr, s)))
+    if ((st = fft_pass(p, p.Nx, FFT_C2R, 1, p.d_spec, out, cols, p.x_stride, p.elem_spec, p.elem_stride, (int)cols,
+                       p.Ns, scale, p.d_tw_x, nullptr, nullptr, false, adjoint, s)))
         return st;
+    mark(5);
+    return HELM_OK;
+}
+
+int solve(Plan& p, const void* f, const double* gl, const double* gr, void* u, cudaStream_t s)
+{
+    return run_pipeline(p, f, gl, gr, u, false, s);
+}
+
+int solve_adjoint(Plan& p, const double* ubar, double* fbar, double* glbar, double* grbar, const double* u,
+                  double* lambda_bar, cudaStream_t s)
+{
+    if (!p.adj_ready) {
+        g_last_error = "adjoint needs a fast-diagonalisation plan with one GLL element";
+        return HELM_ERR_UNSUPPORTED;
+    }
+    int st = run_pipeline(p, ubar, nullptr, nullptr, fbar, true, s);
+    if (st) return st;
+    if (lambda_bar) {
+        cudaError_t e = cudaMemsetAsync(lambda_bar, 0, sizeof(double), s);
+        if (e != cudaSuccess) return set_cuda_error(e, "cudaMemsetAsync");
+    }
+    int e = launch_adjoint_finalize(fbar, glbar, grbar, lambda_bar ? u : nullptr, lambda_bar, p.Nx,
+                                    p.dim == 3 ? p.Ny : 1, p.N, p.x_stride, p.dim == 3 ? p.bc_x_stride : 1, s);
+    if (e) return set_cuda_error((cudaError_t)e, "adjoint finalize launch");
     return HELM_OK;
 }
 
@@ -487,8 +781,14 @@ int helm_solve(helm_plan_t plan, const void* f, const double* gl, const double* 
 int helm_solve_adjoint(helm_plan_t plan, const double* ubar, double* fbar, double* glbar, double* grbar,
                        const double* u, double* lambda_bar, void* stream)
 {
-    (void)plan; (void)ubar; (void)fbar; (void)glbar; (void)grbar; (void)u; (void)lambda_bar; (void)stream;
-    return HELM_ERR_UNSUPPORTED;
+    if (!plan || !ubar || !fbar || (lambda_bar && !u)) return HELM_ERR_INVALID;
+    Plan& p = *reinterpret_cast<Plan*>(plan);
+    int cur = 0;
+    cudaGetDevice(&cur);
+    if (cur != p.device) cudaSetDevice(p.device);
+    int st = helm::solve_adjoint(p, ubar, fbar, glbar, grbar, u, lambda_bar, static_cast<cudaStream_t>(stream));
+    if (cur != p.device) cudaSetDevice(cur);
+    return st;
 }
 
 int helm_plan_get_grid(helm_plan_t plan, double* nodes, double* D, double* D2)
@@ -509,6 +809,35 @@ int helm_plan_info(helm_plan_t plan, int* Ns, int* n_operators, int* method, lon
     if (n_operators) *n_operators = p.ngroups;
     if (method) *method = p.method;
     if (device_bytes) *device_bytes = p.device_bytes;
+    return HELM_OK;
+}
+
+int helm_plan_set_stage_timing(helm_plan_t plan, int enable)
+{
+    if (!plan) return HELM_ERR_INVALID;
+    Plan& p = *reinterpret_cast<Plan*>(plan);
+    if (enable && !p.ev[0])
+        for (cudaEvent_t& e : p.ev) {
+            cudaError_t err = cudaEventCreate(&e);
+            if (err != cudaSuccess) return helm::set_cuda_error(err, "cudaEventCreate");
+        }
+    p.stage_timing = enable != 0;
+    return HELM_OK;
+}
+
+int helm_plan_stage_times(helm_plan_t plan, float* ms5)
+{
+    if (!plan || !ms5) return HELM_ERR_INVALID;
+    Plan& p = *reinterpret_cast<Plan*>(plan);
+    if (!p.stage_timing) return HELM_ERR_INVALID;
+    cudaError_t err = cudaEventSynchronize(p.ev[5]);
+    if (err != cudaSuccess) return helm::set_cuda_error(err, "cudaEventSynchronize");
+    for (int i = 0; i < 5; ++i) {
+        float t = 0.0f;
+        err = cudaEventElapsedTime(&t, p.ev[i], p.ev[i + 1]);
+        if (err != cudaSuccess) return helm::set_cuda_error(err, "cudaEventElapsedTime");
+        ms5[i] = t;
+    }
     return HELM_OK;
 }
 

@@ -48,6 +48,30 @@ struct Plan {
     double* d_d0 = nullptr;
     double* d_dN = nullptr;
     double* d_d2t = nullptr;
+    // adjoint (transposed) solve data, FDM plans with one element
+    bool adj_ready = false;
+    void* d_vtT = nullptr;        // column-major V^T
+    void* d_vinvtT = nullptr;     // column-major V^-T
+    double* d_d2row = nullptr;    // column-major D2int^T (= row-major D2int)
+    double* d_c0 = nullptr;       // [P] D2[int][0] in the interior slots
+    double* d_cN = nullptr;       // [P] D2[int][N-1]
+    double* d_hom_adj = nullptr;  // [G][2][P] pl, pr
+    double* d_homs_adj = nullptr; // [G][4] 2x2 boundary matrix
+    // folded fast-diagonalisation path (FDM plans with one element)
+    bool fast = false;
+    int fm = 0, fms = 0, fma = 0, fld = 32;
+    void* d_fmats = nullptr;       // forward transforms [4][fld][fld]
+    void* d_fmats_adj = nullptr;   // transposed transforms
+    double* d_fd2 = nullptr;       // folded D2int blocks (refinement)
+    double* d_fd2_adj = nullptr;   // their transposes
+    void* d_frecip = nullptr;      // [G][2][fld] reciprocal shifts
+    int* d_row_grp = nullptr;      // group of each grouped row
+    double* d_fe0 = nullptr;       // folded D[0][int], D[N-1][int]
+    double* d_feN = nullptr;
+    double* d_fc0 = nullptr;       // folded D2[int][0], D2[int][N-1]
+    double* d_fcN = nullptr;
+    bool stage_timing = false;
+    cudaEvent_t ev[6] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
     std::vector<void*> allocations;
     long long device_bytes = 0;
 

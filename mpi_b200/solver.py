@@ -135,6 +135,17 @@ class _PlanBase:
         L.check(st, "helm_solve_adjoint")
         return fbar, lam, glb, grb
 
+    def enable_stage_timing(self, enable: bool = True) -> None:
+        L.check(self._lib.helm_plan_set_stage_timing(self._plan, int(enable)), "helm_plan_set_stage_timing")
+
+    STAGES = ("fft_x", "fft_y", "rows", "ifft_y", "ifft_x")
+
+    def stage_times(self) -> dict:
+        """Durations (ms) of the last solve's kernels, from CUDA events on its stream."""
+        buf = (ctypes.c_float * 5)()
+        L.check(self._lib.helm_plan_stage_times(self._plan, buf), "helm_plan_stage_times")
+        return dict(zip(self.STAGES, [float(v) for v in buf]))
+
     def DestroyPDEPlan(self) -> None:
         if self._plan.value:
             self._lib.helm_plan_destroy(self._plan)

@@ -126,8 +126,10 @@ def test_reference_array_layout_3d(cuda):
     p = _plan3d(g)
     p.set_layout(x_stride=2 * Ny * N, elem_stride=2 * Nx * 2 * Ny * N, bc_x_stride=2 * Ny)
     fd, ud = _dev(F), torch.full((2 * Nx, 2 * Ny, N), 7.0, dtype=torch.float64, device="cuda")
-    st = p._lib.helm_solve(p._plan, fd.data_ptr(), _dev(GL).data_ptr(), _dev(GR).data_ptr(), ud.data_ptr(),
+    gld, grd = _dev(GL), _dev(GR)  # keep the device buffers alive across the asynchronous solve
+    st = p._lib.helm_solve(p._plan, fd.data_ptr(), gld.data_ptr(), grd.data_ptr(), ud.data_ptr(),
                            torch.cuda.current_stream().cuda_stream)
+    torch.cuda.synchronize()
     assert st == 0
     U = ud.cpu().numpy()
     assert max_rel(U[:Nx, :Ny], g["u"]) < 1e-12
