@@ -163,7 +163,7 @@ __global__ void __launch_bounds__(FDM_WARPS * 32, 2) fdm_fast_kernel(FdmArgs a)
     __syncthreads();
 
     CS* spec = static_cast<CS*>(a.spec);
-    const TF r2 = (TF)0.70710678118654752440;
+    const TS r2 = (TS)0.70710678118654752440;  // fold weight, in the storage precision
     const int nrows = a.nrows;
     const long long npacks = (nrows + RPW - 1) / RPW;
     const long long gw0 = (long long)blockIdx.x * FDM_WARPS + warp;
@@ -308,9 +308,7 @@ __global__ void __launch_bounds__(FDM_WARPS * 32, 2) fdm_fast_kernel(FdmArgs a)
             if (!ok[r]) continue;  // warp-uniform
             CS* row = spec + (long long)rowid[r] * P;
             const int g = grp[r];
-            TS zlr = 0, zli = 0, zrr = 0, zri = 0;   // boundary values of the row
-            TS el = 0, er = 0;                       // weights of the per-group vectors hl / hr
-            TS elr = 0, eli = 0, err_ = 0, eri = 0;
+            TS zlr = 0, zli = 0, zrr = 0, zri = 0;   // boundary values of the row (weights of hl / hr)
             const bool bnd = a.hvec != nullptr;
             if (bnd) {
                 // folded dot products with e0 / eN (forward: D0, DN rows; adjoint: D2 boundary columns)
@@ -349,8 +347,6 @@ __global__ void __launch_bounds__(FDM_WARPS * 32, 2) fdm_fast_kernel(FdmArgs a)
                     zlr = (m11 * q0r - m01 * qNr) / det; zli = (m11 * q0i - m01 * qNi) / det;
                     zrr = (m00 * qNr - m10 * q0r) / det; zri = (m00 * qNi - m10 * q0i) / det;
                 }
-                elr = zlr; eli = zli; err_ = zrr; eri = zri;
-                (void)el; (void)er;
             }
             const double* hl = bnd ? a.hvec + (size_t)g * 2 * P : nullptr;
             const double* hr = bnd ? hl + P : nullptr;
@@ -363,8 +359,8 @@ __global__ void __launch_bounds__(FDM_WARPS * 32, 2) fdm_fast_kernel(FdmArgs a)
                     if (bnd) {
                         const TS l0 = (TS)hl[1 + k], r0 = (TS)hr[1 + k];
                         const TS l1 = (TS)hl[n - k], r1 = (TS)hr[n - k];
-                        lo_r += elr * l0 + err_ * r0; lo_i += eli * l0 + eri * r0;
-                        hi_r += elr * l1 + err_ * r1; hi_i += eli * l1 + eri * r1;
+                        lo_r += zlr * l0 + zrr * r0; lo_i += zli * l0 + zri * r0;
+                        hi_r += zlr * l1 + zrr * r1; hi_i += zli * l1 + zri * r1;
                     }
                     row[1 + k] = mk(lo_r, lo_i);
                     row[n - k] = mk(hi_r, hi_i);
@@ -372,7 +368,7 @@ __global__ void __launch_bounds__(FDM_WARPS * 32, 2) fdm_fast_kernel(FdmArgs a)
                     TS mr = xsr[r][t], mi = xsi[r][t];
                     if (bnd) {
                         const TS l0 = (TS)hl[1 + k], r0 = (TS)hr[1 + k];
-                        mr += elr * l0 + err_ * r0; mi += eli * l0 + eri * r0;
+                        mr += zlr * l0 + zrr * r0; mi += zli * l0 + zri * r0;
                     }
                     row[1 + k] = mk(mr, mi);
                 }

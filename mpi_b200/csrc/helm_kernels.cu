@@ -119,7 +119,8 @@ __global__ void __launch_bounds__(FFT_THREADS) fft_kernel(FftArgs a, long long t
         const TIO* in = static_cast<const TIO*>(a.in) + (long long)b * a.in_batch;
         int k0 = -1, k1 = -1, j0 = 0, j1 = 0;  // GLL slot of the two real columns
         if (a.P > 0) { k0 = c0 % a.P; j0 = c0 / a.P; k1 = c1 % a.P; j1 = c1 / a.P; }
-        const bool bnd0 = (k0 == 0 || k0 == a.P - 1), bnd1 = (k1 == 0 || k1 == a.P - 1);
+        const bool bnd0 = a.P > 0 && (k0 == 0 || k0 == a.P - 1);
+        const bool bnd1 = a.P > 0 && (k1 == 0 || k1 == a.P - 1);
         const double* s0 = (k0 == 0) ? (b == a.gl_batch ? a.gl : nullptr) : (b == a.gr_batch ? a.gr : nullptr);
         const double* s1 = (k1 == 0) ? (b == a.gl_batch ? a.gl : nullptr) : (b == a.gr_batch ? a.gr : nullptr);
 #pragma unroll
