@@ -134,6 +134,17 @@ int helm_plan_info(helm_plan_t plan, int* Ns, int* n_operators, int* method, lon
 int helm_plan_set_stage_timing(helm_plan_t plan, int enable);
 int helm_plan_stage_times(helm_plan_t plan, float* ms5);
 
+/* helm_solve with the spectrum workspace taken from a fixed 16 MiB device
+ * array inside this library instead of the plan's buffer; the call allocates
+ * no device memory.  For callers whose memory manager owns the device memory
+ * or whose device footprint must stay fixed after start-up.  Plans whose
+ * spectrum needs more than 16 MiB get HELM_ERR_UNSUPPORTED.  The first call on
+ * a device looks up the array's address and should come before any stream
+ * capture; calls that overlap on the GPU share the array and race.  No
+ * counterpart in the reference. */
+int helm_solve_static_scratch(helm_plan_t plan, const void* f, const double* gl, const double* gr, void* u,
+                              void* stream);
+
 /* Replaces DestroyPDEPlan() + DestroyFFTPlan(). NULL is accepted. */
 int helm_plan_destroy(helm_plan_t plan);
 
