@@ -323,7 +323,7 @@ def run_ours(args, ws, rank, local):
             "dtype": "f32 solves + f64 residuals/FFTs",
             "data": "synthetic",
             "config": {"workload": WORKLOAD, "precision": "fp32_refine", "method": pref.info()["method"],
-                       "refine_sweeps": 2, "l2": "256 MB buffer written before every timed solve",
+                       "refine_sweeps": 1, "l2": "256 MB buffer written before every timed solve",
                        "parallelism": f"replicas x{ws}", "dof_per_solve": dof},
             "fp64": {"value": ws * dof / (ms_64 * 1e-3) / 1e9, "ms_per_step": ms_64,
                      "method": plans["fp64"].info()["method"]},

@@ -96,7 +96,7 @@ int helm_plan_set_layout(helm_plan_t plan, long long x_stride, long long elem_st
  * FP64 and FP32_REFINE plans always read and write double. */
 int helm_plan_set_io_bytes(helm_plan_t plan, int bytes);
 
-/* Number of refinement sweeps of a HELM_FP32_REFINE plan (default 2, 0..8). */
+/* Number of refinement sweeps of a HELM_FP32_REFINE plan (default 1, 0..8). */
 int helm_plan_set_refine_sweeps(helm_plan_t plan, int sweeps);
 
 /* SolvePDE(U, ConstructOperator) (NonPeriodic2D_MPI.cpp:228-474,

@@ -100,4 +100,11 @@ template <> struct Radix<256> { static constexpr int n = 2, r0 = 16, r1 = 16, r2
 template <> struct Radix<512> { static constexpr int n = 3, r0 = 8, r1 = 8, r2 = 8; };
 template <> struct Radix<1024> { static constexpr int n = 3, r0 = 16, r1 = 8, r2 = 8; };
 
+// Schedule with at most radix 8 per pass where it changes anything (half the
+// register tile of the radix-16 passes, so more CTAs fit on an SM).
+template <int L, int SMALL> struct RadixV : Radix<L> {};
+template <> struct RadixV<128, 1> { static constexpr int n = 3, r0 = 8, r1 = 4, r2 = 4; };
+template <> struct RadixV<256, 1> { static constexpr int n = 3, r0 = 8, r1 = 8, r2 = 4; };
+template <int L> constexpr bool has_small_radix() { return L == 128 || L == 256; }
+
 }  // namespace helm

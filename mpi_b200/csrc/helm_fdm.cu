@@ -401,10 +401,9 @@ static int run_fdm(const FdmArgs& a, cudaStream_t s)
     return (int)cudaGetLastError();
 }
 
-template <int NSS>
+template <int NSS, int RPW>
 static int fdm_dispatch(int prec, const FdmArgs& a, cudaStream_t s)
 {
-    constexpr int RPW = NSS == 1 ? 4 : 2;  // rows per warp: keeps the accumulators in registers
     if (a.adjoint) {
         if (prec == 0) return run_fdm<double, double, NSS, RPW, false, true>(a, s);
         if (prec == 1) return run_fdm<float, float, NSS, RPW, false, true>(a, s);
@@ -415,11 +414,13 @@ static int fdm_dispatch(int prec, const FdmArgs& a, cudaStream_t s)
     return run_fdm<double, float, NSS, RPW, true, false>(a, s);
 }
 
-int launch_fdm_fast(int prec, const FdmArgs& a, cudaStream_t s)
+// variant 0: 4 rows per warp (2 for the wide fold); variant 1: half as many.
+// Rows per warp keep the accumulators in registers.
+int launch_fdm_fast(int prec, const FdmArgs& a, cudaStream_t s, int variant)
 {
     switch (a.ld / 32) {
-        case 1: return fdm_dispatch<1>(prec, a, s);
-        case 2: return fdm_dispatch<2>(prec, a, s);
+        case 1: return variant ? fdm_dispatch<1, 2>(prec, a, s) : fdm_dispatch<1, 4>(prec, a, s);
+        case 2: return variant ? fdm_dispatch<2, 1>(prec, a, s) : fdm_dispatch<2, 2>(prec, a, s);
         default: return (int)cudaErrorInvalidValue;
     }
 }

@@ -26,7 +26,7 @@ struct FdmArgs {
     int adjoint;
 };
 
-int launch_fdm_fast(int prec, const FdmArgs& a, cudaStream_t s);
+int launch_fdm_fast(int prec, const FdmArgs& a, cudaStream_t s, int variant = 0);
 size_t fdm_fast_smem_bytes(int prec, int ld);
 
 }  // namespace helm

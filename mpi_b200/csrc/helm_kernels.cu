@@ -14,13 +14,12 @@
 
 namespace helm {
 
-constexpr int FFT_THREADS = 256;
-
-template <typename T, int L>
+template <typename T, int L, int THREADS, int SMALL>
 struct FftShape {
-    static constexpr int R0 = Radix<L>::r0, R1 = Radix<L>::r1, R2 = Radix<L>::r2, NP = Radix<L>::n;
+    using RS = RadixV<L, SMALL>;
+    static constexpr int R0 = RS::r0, R1 = RS::r1, R2 = RS::r2, NP = RS::n;
     static constexpr int TPC = L / R0;          // threads per column
-    static constexpr int CT = FFT_THREADS / TPC;  // columns per tile
+    static constexpr int CT = THREADS / TPC;    // columns per tile
     static constexpr size_t smem = (size_t)L * CT * sizeof(cplx_t<T>);
 };
 
@@ -76,11 +75,11 @@ __device__ __forceinline__ void pass_to_smem(cplx_t<T>* sm, int tc, int cl, cons
         for (int r = 0; r < R; ++r) sm[pass_out_row<R, NS, TPC>(tc, t, r) * CT + cl] = v[t * R + r];
 }
 
-template <typename T, typename TIO, int L, int DIR, int MODE>
-__global__ void __launch_bounds__(FFT_THREADS) fft_kernel(FftArgs a, long long total_cols)
+template <typename T, typename TIO, int L, int DIR, int MODE, int THREADS, int SMALL>
+__global__ void __launch_bounds__(THREADS) fft_kernel(FftArgs a, long long total_cols)
 {
     using C = cplx_t<T>;
-    using S = FftShape<T, L>;
+    using S = FftShape<T, L, THREADS, SMALL>;
     constexpr int R0 = S::R0, R1 = S::R1, R2 = S::R2, NP = S::NP, TPC = S::TPC, CT = S::CT;
     extern __shared__ __align__(16) unsigned char fft_smem[];
     C* sm = reinterpret_cast<C*>(fft_smem);
@@ -202,54 +201,68 @@ __global__ void __launch_bounds__(FFT_THREADS) fft_kernel(FftArgs a, long long t
     }
 }
 
-template <typename T, typename TIO, int L, int DIR, int MODE>
+template <typename T, typename TIO, int L, int DIR, int MODE, int THREADS, int SMALL>
 static int run_fft(const FftArgs& a, long long total_cols, cudaStream_t s)
 {
-    using S = FftShape<T, L>;
-    auto k = fft_kernel<T, TIO, L, DIR, MODE>;
-    static bool attr_done = false;  // per instantiation
-    if (!attr_done) {
-        cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)S::smem);
-        if (e != cudaSuccess) return (int)e;
-        attr_done = true;
-    }
+    using S = FftShape<T, L, THREADS, SMALL>;
+    auto k = fft_kernel<T, TIO, L, DIR, MODE, THREADS, SMALL>;
+    cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)S::smem);
+    if (e != cudaSuccess) return (int)e;
     const long long blocks = (total_cols + S::CT - 1) / S::CT;
     if (blocks <= 0) return 0;
-    k<<<(unsigned)blocks, FFT_THREADS, S::smem, s>>>(a, total_cols);
+    k<<<(unsigned)blocks, THREADS, S::smem, s>>>(a, total_cols);
     return (int)cudaGetLastError();
 }
 
-template <typename T, typename TIO, int L>
+template <typename T, typename TIO, int L, int THREADS, int SMALL>
 static int fft_dispatch_mode(int mode, int dir, const FftArgs& a, long long tc, cudaStream_t s)
 {
-    if (mode == FFT_C2C) return dir < 0 ? run_fft<T, T, L, -1, FFT_C2C>(a, tc, s) : run_fft<T, T, L, 1, FFT_C2C>(a, tc, s);
-    if (mode == FFT_R2C) return run_fft<T, TIO, L, -1, FFT_R2C>(a, tc, s);
-    return run_fft<T, TIO, L, 1, FFT_C2R>(a, tc, s);
+    if (mode == FFT_C2C)
+        return dir < 0 ? run_fft<T, T, L, -1, FFT_C2C, THREADS, SMALL>(a, tc, s)
+                       : run_fft<T, T, L, 1, FFT_C2C, THREADS, SMALL>(a, tc, s);
+    if (mode == FFT_R2C) return run_fft<T, TIO, L, -1, FFT_R2C, THREADS, SMALL>(a, tc, s);
+    return run_fft<T, TIO, L, 1, FFT_C2R, THREADS, SMALL>(a, tc, s);
+}
+
+// Launch variants the autotuner chooses from: bit 0 -> 128-thread CTAs (half the
+// columns per tile), bit 1 -> radix-8 schedule (lengths 128 and 256).
+template <typename T, typename TIO, int L>
+static int fft_dispatch_variant(int variant, int mode, int dir, const FftArgs& a, long long tc, cudaStream_t s)
+{
+    const bool small_cta = (variant & 1) && (L / Radix<L>::r0 <= 128);
+    if constexpr (has_small_radix<L>()) {
+        if (variant & 2) {
+            if (small_cta) return fft_dispatch_mode<T, TIO, L, 128, 1>(mode, dir, a, tc, s);
+            return fft_dispatch_mode<T, TIO, L, 256, 1>(mode, dir, a, tc, s);
+        }
+    }
+    if (small_cta) return fft_dispatch_mode<T, TIO, L, 128, 0>(mode, dir, a, tc, s);
+    return fft_dispatch_mode<T, TIO, L, 256, 0>(mode, dir, a, tc, s);
 }
 
 template <typename T, typename TIO>
-static int fft_dispatch_len(int L, int mode, int dir, const FftArgs& a, long long tc, cudaStream_t s)
+static int fft_dispatch_len(int L, int variant, int mode, int dir, const FftArgs& a, long long tc, cudaStream_t s)
 {
     switch (L) {
-        case 4: return fft_dispatch_mode<T, TIO, 4>(mode, dir, a, tc, s);
-        case 8: return fft_dispatch_mode<T, TIO, 8>(mode, dir, a, tc, s);
-        case 16: return fft_dispatch_mode<T, TIO, 16>(mode, dir, a, tc, s);
-        case 32: return fft_dispatch_mode<T, TIO, 32>(mode, dir, a, tc, s);
-        case 64: return fft_dispatch_mode<T, TIO, 64>(mode, dir, a, tc, s);
-        case 128: return fft_dispatch_mode<T, TIO, 128>(mode, dir, a, tc, s);
-        case 256: return fft_dispatch_mode<T, TIO, 256>(mode, dir, a, tc, s);
-        case 512: return fft_dispatch_mode<T, TIO, 512>(mode, dir, a, tc, s);
-        case 1024: return fft_dispatch_mode<T, TIO, 1024>(mode, dir, a, tc, s);
+        case 4: return fft_dispatch_variant<T, TIO, 4>(variant, mode, dir, a, tc, s);
+        case 8: return fft_dispatch_variant<T, TIO, 8>(variant, mode, dir, a, tc, s);
+        case 16: return fft_dispatch_variant<T, TIO, 16>(variant, mode, dir, a, tc, s);
+        case 32: return fft_dispatch_variant<T, TIO, 32>(variant, mode, dir, a, tc, s);
+        case 64: return fft_dispatch_variant<T, TIO, 64>(variant, mode, dir, a, tc, s);
+        case 128: return fft_dispatch_variant<T, TIO, 128>(variant, mode, dir, a, tc, s);
+        case 256: return fft_dispatch_variant<T, TIO, 256>(variant, mode, dir, a, tc, s);
+        case 512: return fft_dispatch_variant<T, TIO, 512>(variant, mode, dir, a, tc, s);
+        case 1024: return fft_dispatch_variant<T, TIO, 1024>(variant, mode, dir, a, tc, s);
         default: return (int)cudaErrorInvalidValue;
     }
 }
 
 int launch_fft(int L, int mode, int dir, int t_double, int io_bytes, const FftArgs& a, long long total_cols,
-               cudaStream_t s)
+               cudaStream_t s, int variant)
 {
-    if (t_double) return fft_dispatch_len<double, double>(L, mode, dir, a, total_cols, s);
-    if (io_bytes == 8) return fft_dispatch_len<float, double>(L, mode, dir, a, total_cols, s);
-    return fft_dispatch_len<float, float>(L, mode, dir, a, total_cols, s);
+    if (t_double) return fft_dispatch_len<double, double>(L, variant, mode, dir, a, total_cols, s);
+    if (io_bytes == 8) return fft_dispatch_len<float, double>(L, variant, mode, dir, a, total_cols, s);
+    return fft_dispatch_len<float, float>(L, variant, mode, dir, a, total_cols, s);
 }
 
 // ======================================================== row solves ==

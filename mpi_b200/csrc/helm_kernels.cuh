@@ -68,8 +68,9 @@ struct RowArgs {
 // Launchers (helm_kernels.cu).  Return a cudaError_t.
 // T: compute precision (0 = float, 1 = double); io: real element bytes for
 // R2C input / C2R output (4 or 8).
+// variant: launch shape chosen by the plan's autotuner (0: 256-thread CTAs, 1: 128).
 int launch_fft(int L, int mode, int dir, int t_double, int io_bytes, const FftArgs& a, long long total_cols,
-               cudaStream_t s);
+               cudaStream_t s, int variant = 0);
 // method: 1 = LU, 2 = FDM; prec: 0 = FP64, 1 = FP32, 2 = FP32 with FP64 refinement
 int launch_rows(int method, int prec, const RowArgs& a, cudaStream_t s);
 // Adjoint output split (boundary slots -> glbar/grbar, lambda_bar reduction).

@@ -16,9 +16,12 @@
 #include "helm_setup.hpp"
 
 #include <algorithm>
+#include <array>
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 #include <map>
+#include <mutex>
 #include <string>
 #include <thread>
 #include <vector>
@@ -498,7 +501,7 @@ static int setup_plan(Plan& p)
 
 static int fft_pass(Plan& p, int L, int mode, int dir, const void* in, void* out, long long in_row, long long out_row,
                     long long in_batch, long long out_batch, int ncols, int nbatch, double scale, const void* tw,
-                    const double* gl, const double* gr, bool inject, bool io_double, cudaStream_t s)
+                    const double* gl, const double* gr, bool inject, bool io_double, int stage, cudaStream_t s)
 {
     FftArgs a{};
     a.in = in;
@@ -520,7 +523,7 @@ static int fft_pass(Plan& p, int L, int mode, int dir, const void* in, void* out
     const long long ccols = (mode == FFT_C2C) ? ncols : (ncols + 1) / 2;
     const int td = p.precision != HELM_FP32;
     const int io = (td || io_double) ? 8 : p.io_bytes;
-    int e = launch_fft(L, mode, dir, td, io, a, ccols * nbatch, s);
+    int e = launch_fft(L, mode, dir, td, io, a, ccols * nbatch, s, p.fft_var[stage]);
     if (e) return set_cuda_error((cudaError_t)e, "fft launch");
     return HELM_OK;
 }
@@ -541,13 +544,13 @@ static int run_pipeline(Plan& p, const void* in, const double* gl, const double*
     mark(0);
     // 1. x: real-to-complex (forward: GLL boundary slots take the boundary data)
     if ((st = fft_pass(p, p.Nx, FFT_R2C, -1, in, p.d_spec, p.x_stride, cols, p.elem_stride, p.elem_spec, (int)cols,
-                       p.Ns, 1.0, p.d_tw_x, gl, gr, !adjoint, adjoint, s)))
+                       p.Ns, 1.0, p.d_tw_x, gl, gr, !adjoint, adjoint, 0, s)))
         return st;
     mark(1);
     // 2. y: complex-to-complex along the middle axis
     if (p.dim == 3 &&
         (st = fft_pass(p, p.Ny, FFT_C2C, -1, p.d_spec, p.d_spec, N, N, (long long)p.Ny * N, (long long)p.Ny * N, N,
-                       p.Ns * nkx, 1.0, p.d_tw_y, nullptr, nullptr, false, false, s)))
+                       p.Ns * nkx, 1.0, p.d_tw_y, nullptr, nullptr, false, false, 1, s)))
         return st;
     mark(2);
     // 3. per-wavenumber collocation solves + interface sweep + combination
@@ -619,7 +622,7 @@ static int run_pipeline(Plan& p, const void* in, const double* gl, const double*
         fa.ar = p.bc.alphar;
         fa.br = p.bc.betar;
         fa.adjoint = adjoint ? 1 : 0;
-        e = launch_fdm_fast(prec, fa, s);
+        e = launch_fdm_fast(prec, fa, s, p.row_var);
     } else {
         e = launch_rows(p.method, prec, r, s);
     }
@@ -628,15 +631,85 @@ static int run_pipeline(Plan& p, const void* in, const double* gl, const double*
     // 4. inverse y
     if (p.dim == 3 &&
         (st = fft_pass(p, p.Ny, FFT_C2C, 1, p.d_spec, p.d_spec, N, N, (long long)p.Ny * N, (long long)p.Ny * N, N,
-                       p.Ns * nkx, 1.0, p.d_tw_y, nullptr, nullptr, false, false, s)))
+                       p.Ns * nkx, 1.0, p.d_tw_y, nullptr, nullptr, false, false, 2, s)))
         return st;
     mark(4);
     // 5. x: complex-to-real, scaled by 1/(Nx Ny) (the reference's /Nx, /Ny)
     const double scale = 1.0 / ((double)p.Nx * (p.dim == 3 ? p.Ny : 1));
     if ((st = fft_pass(p, p.Nx, FFT_C2R, 1, p.d_spec, out, cols, p.x_stride, p.elem_spec, p.elem_stride, (int)cols,
-                       p.Ns, scale, p.d_tw_x, nullptr, nullptr, false, adjoint, s)))
+                       p.Ns, scale, p.d_tw_x, nullptr, nullptr, false, adjoint, 3, s)))
         return st;
     mark(5);
+    return HELM_OK;
+}
+
+// Autotuner: times every launch variant of the four FFT stages on this plan's
+// own shape (CUDA events around each stage of whole solves on zero input) and
+// keeps the fastest per stage.  Results are cached per shape for the process;
+// HELM_AUTOTUNE=0 in the environment keeps the default variants.
+static std::mutex g_tune_mutex;
+static std::map<std::string, std::array<int, 5>> g_tune_cache;
+
+static int autotune(Plan& p)
+{
+    const char* env = std::getenv("HELM_AUTOTUNE");
+    if (env && env[0] == '0') return HELM_OK;
+    const std::string key = std::to_string(p.dim) + ":" + std::to_string(p.Nx) + ":" + std::to_string(p.Ny) + ":" +
+                            std::to_string(p.N) + ":" + std::to_string(p.Ns) + ":" + std::to_string(p.precision) +
+                            ":" + std::to_string(p.io_bytes) + ":" + std::to_string(p.x_stride);
+    {
+        std::lock_guard<std::mutex> lock(g_tune_mutex);
+        auto it = g_tune_cache.find(key);
+        if (it != g_tune_cache.end()) {
+            for (int i = 0; i < 4; ++i) p.fft_var[i] = it->second[i];
+            p.row_var = it->second[4];
+            return HELM_OK;
+        }
+    }
+    const size_t bytes = (size_t)p.Ns * p.elem_stride * (p.precision == HELM_FP32 ? p.io_bytes : 8);
+    void *f = nullptr, *u = nullptr;
+    if (cudaMalloc(&f, bytes) != cudaSuccess || cudaMalloc(&u, bytes) != cudaSuccess) {
+        cudaGetLastError();
+        if (f) cudaFree(f);
+        return HELM_OK;  // keep the defaults
+    }
+    cudaMemset(f, 0, bytes);
+    const bool had = p.stage_timing;
+    if (!p.ev[0])
+        for (cudaEvent_t& e : p.ev) cudaEventCreate(&e);
+    p.stage_timing = true;
+    // stages: x, y, rows, inverse y, inverse x (event intervals 0..4); the
+    // FFT stages try variants 0..3, the row stage its variants 0..1
+    float best[5] = {1e30f, 1e30f, 1e30f, 1e30f, 1e30f};
+    int pick[5] = {0, 0, 0, 0, 0};
+    for (int v = 0; v < 4; ++v) {
+        for (int i = 0; i < 4; ++i) p.fft_var[i] = v;
+        p.row_var = v & 1;
+        float acc[5] = {0, 0, 0, 0, 0};
+        bool ok = true;
+        for (int rep = 0; rep < 4 && ok; ++rep) {
+            if (solve(p, f, nullptr, nullptr, u, 0)) { ok = false; break; }
+            cudaEventSynchronize(p.ev[5]);
+            if (rep == 0) continue;  // warm-up
+            for (int i = 0; i < 5; ++i) {
+                float t = 0;
+                cudaEventElapsedTime(&t, p.ev[i], p.ev[i + 1]);
+                acc[i] += t;
+            }
+        }
+        if (!ok) { cudaGetLastError(); continue; }
+        for (int i = 0; i < 5; ++i)
+            if (acc[i] < best[i]) { best[i] = acc[i]; pick[i] = (i == 2) ? (v & 1) : v; }
+    }
+    cudaGetLastError();
+    p.stage_timing = had;
+    const int stage_of_fft[4] = {0, 1, 3, 4};
+    for (int i = 0; i < 4; ++i) p.fft_var[i] = pick[stage_of_fft[i]];
+    p.row_var = p.fast ? pick[2] : 0;
+    cudaFree(f);
+    cudaFree(u);
+    std::lock_guard<std::mutex> lock(g_tune_mutex);
+    g_tune_cache[key] = {p.fft_var[0], p.fft_var[1], p.fft_var[2], p.fft_var[3], p.row_var};
     return HELM_OK;
 }
 
@@ -704,6 +777,7 @@ static int create_plan(int dim, int Nx, int Ny, int Ngll_total, int N, double xl
     p->elem_stride = (long long)Nx * cols;
     p->bc_x_stride = p->Ny;
     int st = setup_plan(*p);
+    if (!st) st = autotune(*p);
     if (st) { p->release(); delete p; return st; }
     *out = reinterpret_cast<helm_plan_t>(p);
     return HELM_OK;

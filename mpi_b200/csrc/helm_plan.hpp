@@ -18,7 +18,7 @@ struct Plan {
     helm_robin_t bc{0.0, 1.0, 0.0, 1.0};
     double lambda = 0;
     int precision = HELM_FP64, method = HELM_METHOD_AUTO;
-    int io_bytes = 8, sweeps = 2;
+    int io_bytes = 8, sweeps = 1;
     long long x_stride = 0, elem_stride = 0, bc_x_stride = 0;
     int device = 0;
     GllSetup gll;
@@ -70,6 +70,9 @@ struct Plan {
     double* d_feN = nullptr;
     double* d_fc0 = nullptr;       // folded D2[int][0], D2[int][N-1]
     double* d_fcN = nullptr;
+    // autotuned launch shapes of the four FFT stages (x, y, inverse y, inverse x)
+    int fft_var[4] = {0, 0, 0, 0};
+    int row_var = 0;  // launch variant of the folded row kernel
     bool stage_timing = false;
     cudaEvent_t ev[6] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
     std::vector<void*> allocations;
