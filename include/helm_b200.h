@@ -84,6 +84,20 @@ int helm3d_plan_create(int Nx, int Ny, int Nz, int N, double xl, double xr, doub
                        double zl, double zr, const helm_robin_t* bc, double lambda, int precision,
                        int method, helm_plan_t* plan);
 
+/* Second-order finite-difference variant: the 7-point stencil of the
+ * reference's HypreFDM solver (HelmholtzSolvers/HypreFDM/src/Helmholtz3D_MPI.cpp:
+ * CreatePDEPlan 117-269, SetA 297-410, Setb 424-466) with x and y periodic
+ * (dx = Lx/Nx, dy = Ly/Ny) and Nz interior points in z (dz = Lz/(Nz+1)), solved
+ * directly: FFT in x and y, one Thomas solve along z per wavenumber, inverse
+ * FFT (the reference solves the same system iteratively with HYPRE).  bc gives
+ * the Robin coefficients of the back (z = zl: alphal, betal) and front (z = zr:
+ * alphar, betar) rows, with the reference's one-sided second-order rows.
+ * Arrays: f, u [Nx][Ny][Nz] interior points; gl = back data, gr = front data,
+ * [Nx][Ny].  helm_solve / helm_solve_adjoint / helm_plan_destroy apply.
+ * FP32_REFINE plans compute in FP64. */
+int helm_fd3d_plan_create(int Nx, int Ny, int Nz, double xl, double xr, double yl, double yr, double zl, double zr,
+                          const helm_robin_t* bc, double lambda, int precision, helm_plan_t* plan);
+
 /* Strides (in elements) of f/u and of gl/gr; 0 keeps the compact value.
  *   x_stride    : between consecutive x rows of f and u   (compact: N in 2D, Ny*N in 3D)
  *   elem_stride : between consecutive GLL elements         (compact: Nx*x_stride)

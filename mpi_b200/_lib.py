@@ -33,7 +33,7 @@ EXPORTS = (
     "helm2d_plan_create", "helm3d_plan_create", "helm_plan_set_layout", "helm_plan_set_io_bytes",
     "helm_plan_set_refine_sweeps", "helm_solve", "helm_solve_adjoint", "helm_plan_get_grid",
     "helm_plan_info", "helm_plan_destroy", "helm_status_string", "helm_last_error",
-    "helm_plan_set_stage_timing", "helm_plan_stage_times",
+    "helm_plan_set_stage_timing", "helm_plan_stage_times", "helm_fd3d_plan_create",
 )
 
 
@@ -66,6 +66,7 @@ def lib() -> ctypes.CDLL:
     P = ctypes.POINTER
     L.helm2d_plan_create.argtypes = [i, i, i, d, d, d, d, P(robin_t), d, i, i, P(vp)]
     L.helm3d_plan_create.argtypes = [i, i, i, i, d, d, d, d, d, d, P(robin_t), d, i, i, P(vp)]
+    L.helm_fd3d_plan_create.argtypes = [i, i, i, d, d, d, d, d, d, P(robin_t), d, i, P(vp)]
     L.helm_plan_set_layout.argtypes = [vp, ll, ll, ll]
     L.helm_plan_set_io_bytes.argtypes = [vp, i]
     L.helm_plan_set_refine_sweeps.argtypes = [vp, i]

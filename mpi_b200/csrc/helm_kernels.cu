@@ -127,11 +127,25 @@ __global__ void __launch_bounds__(THREADS) fft_kernel(FftArgs a, long long total
             const long long row = tc + r * TPC;
             T x0 = 0, x1 = 0;
             if (valid) {
-                if (!bnd0) x0 = (T)in[row * a.in_row + c0];
-                else if (s0) x0 = (T)s0[row * a.bc_row + j0];
+                if (!bnd0) {
+                    x0 = (T)in[row * a.in_row + c0];
+                } else if (a.bc_add) {
+                    double v = (double)in[row * a.in_row + c0];
+                    if (s0) v += (k0 == 0 ? a.bc_scale_l : a.bc_scale_r) * s0[row * a.bc_row + j0];
+                    x0 = (T)v;
+                } else if (s0) {
+                    x0 = (T)s0[row * a.bc_row + j0];
+                }
                 if (has1) {
-                    if (!bnd1) x1 = (T)in[row * a.in_row + c1];
-                    else if (s1) x1 = (T)s1[row * a.bc_row + j1];
+                    if (!bnd1) {
+                        x1 = (T)in[row * a.in_row + c1];
+                    } else if (a.bc_add) {
+                        double v = (double)in[row * a.in_row + c1];
+                        if (s1) v += (k1 == 0 ? a.bc_scale_l : a.bc_scale_r) * s1[row * a.bc_row + j1];
+                        x1 = (T)v;
+                    } else if (s1) {
+                        x1 = (T)s1[row * a.bc_row + j1];
+                    }
                 }
             }
             v[r] = mk(x0, x1);
@@ -708,13 +722,18 @@ static int rows_dispatch_prec(int method, int prec, const RowArgs& a, cudaStream
     return run_rows<double, float, NSLOT, 2, true>(a, s);
 }
 
-// Adjoint output split: the adjoint pipeline leaves v = A^-T ubar in fbar with
-// every GLL slot filled.  One warp per (x, y) column moves slot 0 / P-1 to
-// glbar / grbar (dL/dgl, dL/dgr), zeroes them in fbar (f is never read there),
-// and accumulates lambda_bar += sum over the interior slots of fbar * u.
+// Adjoint output split.  The adjoint pipeline leaves v = A^-T ubar in fbar in
+// every slot of the GLL (or z) direction.  One warp per (x, y) column.
+//   GLL plans: slot 0 / P-1 are the boundary equations: they move to glbar /
+//   grbar (dL/dgl, dL/dgr) and are zeroed in fbar (f is never read there);
+//   lambda_bar += sum over the interior slots of fbar * u.
+//   FD plans: every slot is an interior equation; the boundary data entered the
+//   first / last equation with weights scale_l / scale_r, so dL/dg = scale * v
+//   there; lambda_bar sums over every slot.
 __global__ void __launch_bounds__(256) adjoint_finalize_kernel(double* fbar, double* glbar, double* grbar,
                                                                const double* u, double* lambda_bar, int Nx, int Ny,
-                                                               int P, long long x_stride, long long bc_row)
+                                                               int P, long long x_stride, long long bc_row, int fd,
+                                                               double scale_l, double scale_r)
 {
     __shared__ double red[8];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -727,13 +746,11 @@ __global__ void __launch_bounds__(256) adjoint_finalize_kernel(double* fbar, dou
         const double* uc = u ? u + (long long)i * x_stride + (long long)j * P : nullptr;
         for (int k = lane; k < P; k += 32) {
             const double v = col[k];
-            if (k == 0 || k == P - 1) {
-                if (k == 0 && glbar) glbar[(long long)i * bc_row + j] = v;
-                if (k == P - 1 && grbar) grbar[(long long)i * bc_row + j] = v;
-                col[k] = 0.0;
-            } else if (uc) {
-                acc += v * uc[k];
-            }
+            if (k == 0 && glbar) glbar[(long long)i * bc_row + j] = scale_l * v;
+            if (k == P - 1 && grbar) grbar[(long long)i * bc_row + j] = scale_r * v;
+            const bool bslot = (k == 0 || k == P - 1);
+            if (!fd && bslot) col[k] = 0.0;
+            else if (uc) acc += v * uc[k];
         }
     }
     if (!lambda_bar) return;
@@ -748,13 +765,80 @@ __global__ void __launch_bounds__(256) adjoint_finalize_kernel(double* fbar, dou
 }
 
 int launch_adjoint_finalize(double* fbar, double* glbar, double* grbar, const double* u, double* lambda_bar, int Nx,
-                            int Ny, int P, long long x_stride, long long bc_row, cudaStream_t s)
+                            int Ny, int P, long long x_stride, long long bc_row, cudaStream_t s, int fd,
+                            double scale_l, double scale_r)
 {
     const long long ncol = (long long)Nx * Ny;
     long long blocks = (ncol + 7) / 8;
     if (blocks > 148 * 16) blocks = 148 * 16;
     adjoint_finalize_kernel<<<(unsigned)blocks, 256, 0, s>>>(fbar, glbar, grbar, u, lambda_bar, Nx, Ny, P, x_stride,
-                                                            bc_row);
+                                                            bc_row, fd, scale_l, scale_r);
+    return (int)cudaGetLastError();
+}
+
+// Finite-difference variant (HypreFDM stencil, HelmholtzSolvers/HypreFDM/src/
+// Helmholtz3D_MPI.cpp:387-403, periodic x and y turned into the modified
+// wavenumbers mx, my): one Thomas solve along z per complex spectrum row, one
+// thread per row.  The forward sweep writes the modified right-hand side in
+// place and the elimination coefficients to `cprime`; the backward sweep reads
+// both.  Consecutive threads take consecutive rows, so every step's loads fall
+// on lines the previous step brought into L1.
+template <typename T>
+__global__ void __launch_bounds__(128) thomas_kernel(ThomasArgs a)
+{
+    using C = cplx_t<T>;
+    const long long r = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= a.nrows) return;
+    const int Nz = a.Nz;
+    const int kx = (int)(r / a.Ny), ky = (int)(r - (long long)kx * a.Ny);
+    const double d = -2.0 * a.cz1 - a.lambda - a.mx[kx] - a.my[ky];
+    C* x = static_cast<C*>(a.spec) + r * Nz;
+    T* cp = static_cast<T*>(a.cprime) + r * Nz;
+    const T cz = (T)a.cz1;
+    // matrix entries of row k: sub a_k, diagonal b_k, super c_k (transposed: the
+    // sub-diagonal of row k is the super-diagonal of row k-1 and vice versa)
+    auto diag = [&](int k) -> T {
+        double b = d;
+        if (k == 0) b += a.d_first;
+        if (k == Nz - 1) b += a.d_last;
+        return (T)b;
+    };
+    auto sub = [&](int k) -> T {  // k >= 1
+        if (!a.transpose) return (k == Nz - 1) ? (T)a.s_last : cz;
+        return (k - 1 == 0) ? (T)a.s_first : cz;
+    };
+    auto sup = [&](int k) -> T {  // k <= Nz-2
+        if (!a.transpose) return (k == 0) ? (T)a.s_first : cz;
+        return (k + 1 == Nz - 1) ? (T)a.s_last : cz;
+    };
+    T cprev = 0;
+    C dprev = mk((T)0, (T)0);
+    for (int k = 0; k < Nz; ++k) {
+        const T ak = (k > 0) ? sub(k) : (T)0;
+        const T m = (T)1 / (diag(k) - ak * cprev);
+        const T ck = (k < Nz - 1) ? sup(k) * m : (T)0;
+        const C f = x[k];
+        const C dk = mk((f.x - ak * dprev.x) * m, (f.y - ak * dprev.y) * m);
+        x[k] = dk;
+        cp[k] = ck;
+        cprev = ck;
+        dprev = dk;
+    }
+    C xn = dprev;
+    for (int k = Nz - 2; k >= 0; --k) {
+        const C dk = x[k];
+        const T ck = cp[k];
+        xn = mk(dk.x - ck * xn.x, dk.y - ck * xn.y);
+        x[k] = xn;
+    }
+}
+
+int launch_thomas(int prec, const ThomasArgs& a, cudaStream_t s)
+{
+    const long long blocks = (a.nrows + 127) / 128;
+    if (blocks <= 0) return 0;
+    if (prec == 1) thomas_kernel<float><<<(unsigned)blocks, 128, 0, s>>>(a);
+    else thomas_kernel<double><<<(unsigned)blocks, 128, 0, s>>>(a);
     return (int)cudaGetLastError();
 }
 

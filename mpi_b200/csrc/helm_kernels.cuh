@@ -28,6 +28,26 @@ struct FftArgs {
     const double* gr;
     long long bc_row;
     int P, gl_batch, gr_batch;
+    // bc_add = 1: the boundary slots keep the input and add bc_scale_l * gl /
+    // bc_scale_r * gr (finite-difference variant: the Robin rows eliminated
+    // into the first and last interior equations).
+    int bc_add;
+    double bc_scale_l, bc_scale_r;
+};
+
+// Finite-difference variant: one tridiagonal solve along z per spectrum row.
+// Interior rows: cz1 u_{k-1} + (-2 cz1 - lambda - mx[kx] - my[ky]) u_k + cz1 u_{k+1};
+// the first row adds d_first to its diagonal and has super-diagonal s_first,
+// the last row adds d_last and has sub-diagonal s_last.
+struct ThomasArgs {
+    void* spec;           // complex [nrows][Nz], overwritten by the solution
+    void* cprime;         // scratch [nrows][Nz] real: forward-elimination coefficients
+    long long nrows;
+    int Ny, Nz;
+    const double* mx;     // [Nx/2+1] modified x wavenumbers 4 cx1 sin^2(pi kx / Nx)
+    const double* my;     // [Ny]
+    double cz1, lambda, d_first, s_first, d_last, s_last;
+    int transpose;        // solve with the transposed matrix (adjoint)
 };
 
 // Per-wavenumber solve of the spectrum rows, grouped by shift sigma.
@@ -73,9 +93,14 @@ int launch_fft(int L, int mode, int dir, int t_double, int io_bytes, const FftAr
                cudaStream_t s, int variant = 0);
 // method: 1 = LU, 2 = FDM; prec: 0 = FP64, 1 = FP32, 2 = FP32 with FP64 refinement
 int launch_rows(int method, int prec, const RowArgs& a, cudaStream_t s);
-// Adjoint output split (boundary slots -> glbar/grbar, lambda_bar reduction).
+// Adjoint output split.  GLL plans (fd = 0): boundary slots -> glbar/grbar and
+// zeroed, lambda_bar over the interior slots.  FD plans (fd = 1): glbar/grbar =
+// scale_l/scale_r times the first/last slot, nothing zeroed, lambda_bar over
+// every slot.
 int launch_adjoint_finalize(double* fbar, double* glbar, double* grbar, const double* u, double* lambda_bar, int Nx,
-                            int Ny, int P, long long x_stride, long long bc_row, cudaStream_t s);
+                            int Ny, int P, long long x_stride, long long bc_row, cudaStream_t s, int fd = 0,
+                            double scale_l = 1.0, double scale_r = 1.0);
+int launch_thomas(int prec, const ThomasArgs& a, cudaStream_t s);
 // Dynamic shared memory rows_kernel needs for this method / precision / size.
 size_t rows_smem_bytes(int method, int prec, int n, int ld);
 constexpr size_t kMaxSmemPerBlock = 232448;  // 227 KB opt-in limit of sm_100

@@ -520,6 +520,9 @@ static int fft_pass(Plan& p, int L, int mode, int dir, const void* in, void* out
     a.P = (mode == FFT_R2C && inject) ? p.N : 0;
     a.gl_batch = 0;
     a.gr_batch = p.Ns - 1;
+    a.bc_add = p.fd ? 1 : 0;
+    a.bc_scale_l = p.fd_scale_l;
+    a.bc_scale_r = p.fd_scale_r;
     const long long ccols = (mode == FFT_C2C) ? ncols : (ncols + 1) / 2;
     const int td = p.precision != HELM_FP32;
     const int io = (td || io_double) ? 8 : p.io_bytes;
@@ -596,7 +599,24 @@ static int run_pipeline(Plan& p, const void* in, const double* gl, const double*
     }
     const int prec = p.precision == HELM_FP64 ? 0 : (p.precision == HELM_FP32 ? 1 : 2);
     int e;
-    if (p.fast) {
+    if (p.fd) {
+        ThomasArgs ta{};
+        ta.spec = p.d_spec;
+        ta.cprime = p.d_cprime;
+        ta.nrows = p.nrows;
+        ta.Ny = p.Ny;
+        ta.Nz = N;
+        ta.mx = p.d_mx;
+        ta.my = p.d_my;
+        ta.cz1 = p.fd_cz1;
+        ta.lambda = p.lambda;
+        ta.d_first = p.fd_dfirst;
+        ta.s_first = p.fd_sfirst;
+        ta.d_last = p.fd_dlast;
+        ta.s_last = p.fd_slast;
+        ta.transpose = adjoint ? 1 : 0;
+        e = launch_thomas(prec, ta, s);
+    } else if (p.fast) {
         FdmArgs fa{};
         fa.spec = p.d_spec;
         fa.P = N;
@@ -654,7 +674,8 @@ static int autotune(Plan& p)
 {
     const char* env = std::getenv("HELM_AUTOTUNE");
     if (env && env[0] == '0') return HELM_OK;
-    const std::string key = std::to_string(p.dim) + ":" + std::to_string(p.Nx) + ":" + std::to_string(p.Ny) + ":" +
+    const std::string key = std::string(p.fd ? "fd:" : "gll:") + std::to_string(p.dim) + ":" + std::to_string(p.Nx) +
+                            ":" + std::to_string(p.Ny) + ":" +
                             std::to_string(p.N) + ":" + std::to_string(p.Ns) + ":" + std::to_string(p.precision) +
                             ":" + std::to_string(p.io_bytes) + ":" + std::to_string(p.x_stride);
     {
@@ -732,8 +753,98 @@ int solve_adjoint(Plan& p, const double* ubar, double* fbar, double* glbar, doub
         if (e != cudaSuccess) return set_cuda_error(e, "cudaMemsetAsync");
     }
     int e = launch_adjoint_finalize(fbar, glbar, grbar, lambda_bar ? u : nullptr, lambda_bar, p.Nx,
-                                    p.dim == 3 ? p.Ny : 1, p.N, p.x_stride, p.dim == 3 ? p.bc_x_stride : 1, s);
+                                    p.dim == 3 ? p.Ny : 1, p.N, p.x_stride, p.dim == 3 ? p.bc_x_stride : 1, s,
+                                    p.fd ? 1 : 0, p.fd ? p.fd_scale_l : 1.0, p.fd ? p.fd_scale_r : 1.0);
     if (e) return set_cuda_error((cudaError_t)e, "adjoint finalize launch");
+    return HELM_OK;
+}
+
+// Finite-difference variant: the second-order stencil of HypreFDM
+// (HelmholtzSolvers/HypreFDM/src/Helmholtz3D_MPI.cpp:297-410) with periodic x
+// and y (dx = Lx/Nx, dy = Ly/Ny) and Nz interior points in z (dz = Lz/(Nz+1)),
+// one-sided second-order Robin rows at z = zl (back) and z = zr (front).  The
+// Robin rows are eliminated into the first and last interior equations, whose
+// right-hand sides then carry -cz1/a0 * g_back and -cz1/e0 * g_front.
+static int create_fd_plan(int Nx, int Ny, int Nz, double xl, double xr, double yl, double yr, double zl, double zr,
+                          const helm_robin_t* bc, double lambda, int precision, helm_plan_t* out)
+{
+    if (!out) return HELM_ERR_INVALID;
+    *out = nullptr;
+    if (Nz < 2 || Nz > 4096 || Nx < 4 || Ny < 4) { g_last_error = "size out of range"; return HELM_ERR_INVALID; }
+    if (!is_pow2(Nx) || !is_pow2(Ny)) { g_last_error = "N has to be 2^n"; return HELM_ERR_NOT_POW2; }
+    if (Nx > 1024 || Ny > 1024) { g_last_error = "Fourier size beyond 4..1024"; return HELM_ERR_UNSUPPORTED; }
+    if (precision < HELM_FP64 || precision > HELM_FP32_REFINE) return HELM_ERR_INVALID;
+    if (!(xr > xl) || !(yr > yl) || !(zr > zl)) { g_last_error = "empty domain"; return HELM_ERR_INVALID; }
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+        cudaGetLastError();
+        g_last_error = "no CUDA device";
+        return HELM_ERR_NO_DEVICE;
+    }
+    Plan* p = new (std::nothrow) Plan();
+    if (!p) return HELM_ERR_OOM;
+    cudaGetDevice(&p->device);
+    p->fd = true;
+    p->dim = 3;
+    p->Nx = Nx;
+    p->Ny = Ny;
+    p->N = Nz;
+    p->n = Nz;
+    p->Ns = 1;
+    p->xl = xl; p->xr = xr; p->yl = yl; p->yr = yr; p->zl = zl; p->zr = zr;
+    p->Lx = xr - xl;
+    p->Ly = yr - yl;
+    p->Lgll = zr - zl;
+    p->bc = bc ? *bc : helm_robin_t{0.0, 1.0, 0.0, 1.0};
+    p->lambda = lambda;
+    // the FD path computes in FP64 for FP32_REFINE plans (an O(Nz) Thomas solve
+    // has nothing to refine against: it is bound by the same FP64 bytes)
+    p->precision = precision == HELM_FP32 ? HELM_FP32 : HELM_FP64;
+    p->method = HELM_METHOD_LU;
+    p->x_stride = (long long)Ny * Nz;
+    p->elem_stride = (long long)Nx * Ny * Nz;
+    p->bc_x_stride = Ny;
+    const double dx = p->Lx / Nx, dy = p->Ly / Ny, dz = p->Lgll / (Nz + 1);
+    const double cx1 = 1.0 / (dx * dx), cy1 = 1.0 / (dy * dy), cz0 = 1.0 / dz, cz1 = 1.0 / (dz * dz);
+    const double a0 = 1.5 * p->bc.alphal * cz0 + p->bc.betal, a1 = -2.0 * p->bc.alphal * cz0,
+                 a2 = 0.5 * p->bc.alphal * cz0;
+    const double e0 = 1.5 * p->bc.alphar * cz0 + p->bc.betar, e1 = -2.0 * p->bc.alphar * cz0,
+                 e2 = 0.5 * p->bc.alphar * cz0;
+    if (a0 == 0.0 || e0 == 0.0) {
+        delete p;
+        g_last_error = "degenerate Robin row";
+        return HELM_ERR_SINGULAR;
+    }
+    p->fd_cz1 = cz1;
+    p->fd_dfirst = -cz1 * a1 / a0;
+    p->fd_sfirst = cz1 - cz1 * a2 / a0;
+    p->fd_dlast = -cz1 * e1 / e0;
+    p->fd_slast = cz1 - cz1 * e2 / e0;
+    p->fd_scale_l = -cz1 / a0;
+    p->fd_scale_r = -cz1 / e0;
+    const int nkx = Nx / 2 + 1;
+    std::vector<double> mx(nkx), my(Ny);
+    const long double pi = 3.141592653589793238462643383279502884L;
+    for (int k = 0; k < nkx; ++k) { const long double s = std::sin(pi * k / Nx); mx[k] = (double)(4.0L * cx1 * s * s); }
+    for (int k = 0; k < Ny; ++k) { const long double s = std::sin(pi * k / Ny); my[k] = (double)(4.0L * cy1 * s * s); }
+    p->nrows = (long long)nkx * Ny;
+    p->elem_spec = p->nrows * Nz;
+    const bool td = p->precision != HELM_FP32;
+    int st = p->alloc(&p->d_spec, (size_t)p->elem_spec * (td ? 16 : 8));
+    if (!st) st = p->alloc(&p->d_cprime, (size_t)p->elem_spec * (td ? 8 : 4));
+    if (!st) st = p->upload((void**)&p->d_mx, mx.data(), mx.size() * sizeof(double));
+    if (!st) st = p->upload((void**)&p->d_my, my.data(), my.size() * sizeof(double));
+    auto up_tw = [&](int L, void** d) -> int {
+        if (td) { auto t = twiddles<double>(L); return p->upload(d, t.data(), t.size() * sizeof(double)); }
+        auto t = twiddles<float>(L);
+        return p->upload(d, t.data(), t.size() * sizeof(float));
+    };
+    if (!st) st = up_tw(Nx, &p->d_tw_x);
+    if (!st) st = up_tw(Ny, &p->d_tw_y);
+    p->adj_ready = true;
+    if (!st) st = autotune(*p);
+    if (st) { p->release(); delete p; return st; }
+    *out = reinterpret_cast<helm_plan_t>(p);
     return HELM_OK;
 }
 
@@ -794,6 +905,16 @@ int helm2d_plan_create(int Nx, int Ny, int N, double xl, double xr, double yl, d
 {
     try {
         return helm::create_plan(2, Nx, 1, Ny, N, xl, xr, yl, yr, 0.0, 1.0, bc, lambda, precision, method, plan);
+    } catch (...) {
+        return HELM_ERR_OOM;
+    }
+}
+
+int helm_fd3d_plan_create(int Nx, int Ny, int Nz, double xl, double xr, double yl, double yr, double zl, double zr,
+                          const helm_robin_t* bc, double lambda, int precision, helm_plan_t* plan)
+{
+    try {
+        return helm::create_fd_plan(Nx, Ny, Nz, xl, xr, yl, yr, zl, zr, bc, lambda, precision, plan);
     } catch (...) {
         return HELM_ERR_OOM;
     }

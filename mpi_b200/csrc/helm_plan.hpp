@@ -70,6 +70,13 @@ struct Plan {
     double* d_feN = nullptr;
     double* d_fc0 = nullptr;       // folded D2[int][0], D2[int][N-1]
     double* d_fcN = nullptr;
+    // finite-difference variant (FFT in x and y, Thomas along z)
+    bool fd = false;
+    double fd_cz1 = 0, fd_dfirst = 0, fd_sfirst = 0, fd_dlast = 0, fd_slast = 0;
+    double fd_scale_l = 0, fd_scale_r = 0;  // weights of gl / gr in the first / last equation
+    double* d_mx = nullptr;
+    double* d_my = nullptr;
+    void* d_cprime = nullptr;
     // autotuned launch shapes of the four FFT stages (x, y, inverse y, inverse x)
     int fft_var[4] = {0, 0, 0, 0};
     int row_var = 0;  // launch variant of the folded row kernel

@@ -215,6 +215,35 @@ class NonPeriodic3D(_PlanBase):
         return (self.Nx, self.Ny)
 
 
+class Helmholtz3DFD(_PlanBase):
+    """Second-order finite-difference solver on the HypreFDM stencil
+    (HelmholtzSolvers/HypreFDM/src/Helmholtz3D_MPI.cpp, CreatePDEPlan 117-269,
+    SetA 297-410) with x and y periodic and Nz interior points in z, solved
+    directly by FFT + Thomas.  ``bc`` = (alpha_back, beta_back, alpha_front,
+    beta_front) of the one-sided Robin rows at z = zl and z = zr.  Arrays:
+    f, u ``[Nx, Ny, Nz]``; gl (back) and gr (front) ``[Nx, Ny]``."""
+
+    dim = 3
+
+    def __init__(self, Nx: int, Ny: int, Nz: int, xl: float, xr: float, yl: float, yr: float, zl: float, zr: float,
+                 *, Lambda: float, bc: Sequence[float] = (0.0, 1.0, 0.0, 1.0), precision: str = "fp64"):
+        super().__init__()
+        self.Nx, self.Ny, self.N = Nx, Ny, Nz
+        self.Lambda = Lambda
+        self.bc = tuple(float(b) for b in bc)
+        self.precision = precision
+        self.io_dtype = torch.float64
+        r = L.robin_t(*self.bc)
+        L.check(self._lib.helm_fd3d_plan_create(Nx, Ny, Nz, xl, xr, yl, yr, zl, zr, ctypes.byref(r), Lambda,
+                                                _PREC[precision], ctypes.byref(self._plan)), "helm_fd3d_plan_create")
+
+    def _shape(self, Ns):
+        return (Ns, self.Nx, self.Ny, self.N)
+
+    def _bc_shape(self):
+        return (self.Nx, self.Ny)
+
+
 def gdof(Nx: int, Ny: int, N: int, Ns: int = 1) -> int:
     """Degrees of freedom of one solve: grid values of u (Ns elements of N GLL points)."""
     return Nx * Ny * N * Ns

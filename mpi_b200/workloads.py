@@ -119,3 +119,29 @@ def stock_3d(Nx: int = 64, Ny: int = 32, Nz: int = 250, N: int = 10, lam: float 
     gl = (al * 4 * REF_PI * math.sin(0.0) + bl * math.cos(0.0)) * sxy
     gr = (-ar * 4 * REF_PI * math.sin(4 * REF_PI) + br * math.cos(4 * REF_PI)) * sxy
     return np.ascontiguousarray(f), gl, gr, np.ascontiguousarray(u), bc
+
+
+def smooth_field_fd(Nx: int, Ny: int, Nz: int, seed: int, kmax: int = 64) -> np.ndarray:
+    """f[Nx, Ny, Nz] on the interior points of the finite-difference grid:
+    Re of sum c_{kx,ky,l} e^{i(kx x + ky y)} sin(pi l z / Lz), l = 1..Nz, with
+    seeded complex Gaussian c of amplitude (1 + kx^2 + ky^2 + l^2)^-1.5 and zero
+    mean; modes beyond |k| = kmax (amplitude < 4e-6 of the largest) are omitted."""
+    rng = np.random.default_rng(seed)
+    kx = np.fft.fftfreq(Nx, 1.0 / Nx)
+    ky = np.fft.fftfreq(Ny, 1.0 / Ny)
+    L = min(Nz, kmax)
+    l = np.arange(1, L + 1)
+    keepx = np.abs(kx) <= kmax
+    keepy = np.abs(ky) <= kmax
+    planes = np.empty((L, Nx, Ny))
+    for li in range(L):
+        c = np.zeros((Nx, Ny), dtype=np.complex128)
+        sub = (rng.standard_normal((keepx.sum(), keepy.sum())) + 1j * rng.standard_normal((keepx.sum(), keepy.sum())))
+        amp = (1.0 + kx[keepx][:, None] ** 2 + ky[keepy][None, :] ** 2 + l[li] ** 2) ** -1.5
+        c[np.ix_(keepx, keepy)] = sub * amp
+        planes[li] = np.fft.ifft2(c).real * (Nx * Ny)
+    z = np.arange(1, Nz + 1) / (Nz + 1)
+    S = np.sin(np.pi * l[:, None] * z[None, :])  # [L, Nz]
+    f = planes.reshape(L, Nx * Ny).T @ S
+    f -= f.mean()
+    return np.ascontiguousarray(f.reshape(Nx, Ny, Nz))
