@@ -50,6 +50,7 @@ def _args():
     ap.add_argument("--warmup", type=int, default=20)
     ap.add_argument("--impl", choices=("ours", "reference"), default="ours")
     ap.add_argument("--skip-cpu-baseline", action="store_true", help="omit the CPU leg (profiling runs)")
+    ap.add_argument("--skip-side", action="store_true", help="omit the batch / adjoint / finite-difference legs")
     return ap.parse_args()
 
 
@@ -285,6 +286,12 @@ def run_ours(args, ws, rank, local):
         for k, v in pref.stage_times().items():
             acc[k] = acc.get(k, 0.0) + v / nst
     pref.enable_stage_timing(False)
+    side = {}
+    if ws == 1 and not args.skip_side:
+        st, wu = max(3, min(args.steps, 20)), 3
+        side["batch"] = _leg_batch(dev, flush, stream, st, wu, cpu=not args.skip_cpu_baseline)
+        side["adjoint"] = _leg_adjoint(dev, flush, stream, st, wu)
+        side["fd"] = _leg_fd(dev, flush, stream, st, wu)
     clk = clocks.stop()
 
     # max over ranks
@@ -338,6 +345,7 @@ def run_ours(args, ws, rank, local):
             "gpu_launches": launches,
             "clocks": clk,
         }
+        line.update(side)
         if not args.skip_cpu_baseline and ws == 1:
             line["cpu_baseline"], ref_u = _cpu_baseline(fnp)
             line["rel_l2_refine_vs_reference"] = float(np.linalg.norm(u32.cpu().numpy() - ref_u) / np.linalg.norm(ref_u))
@@ -350,6 +358,133 @@ def run_ours(args, ws, rank, local):
 
         dist.barrier()
         dist.destroy_process_group()
+
+
+# ------------------------------------------------------ side workloads --
+# Measured on one GPU beside the headline and reported under their own keys.
+BATCH_WORKLOAD = ("512 independent 2D problems, Nx from {32..512}, GLL order from {16..128}, lambda log-uniform "
+                  "in [1e-2, 1e4], manufactured sin(3x)(1-y^2)e^y f on [0,2pi) x [-1,1], Dirichlet")
+ADJ_WORKLOAD = "3D Fourier 128 x Fourier 128 x GLL 65 (N=64), lambda=5, L = 0.5 ||u - u_obs||^2"
+FD_WORKLOAD = "finite-difference FFT/Thomas, 1024 x 1024 periodic x 256 interior points, Dirichlet, lambda=1"
+
+
+def _ev_ms(fn, flush, stream, steps, warmup):
+    """Mean device ms of fn over `steps` calls (CUDA events on `stream`), the L2
+    flushed before each call."""
+    import torch
+
+    for _ in range(warmup):
+        flush.add_(1.0)
+        fn()
+    torch.cuda.synchronize()
+    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
+    for e0, e1 in evs:
+        flush.add_(1.0)
+        e0.record(stream)
+        fn()
+        e1.record(stream)
+    torch.cuda.synchronize()
+    return sum(e0.elapsed_time(e1) for e0, e1 in evs) / steps
+
+
+def _leg_batch(dev, flush, stream, steps, warmup, cpu):
+    import numpy as np
+    import torch
+
+    from mpi_b200 import BatchNonPeriodic2D
+    from mpi_b200 import workloads as W
+
+    Nx, P, lam, fs, us = W.batch_2d(512, seed=1237)
+    dof = sum(a * b for a, b in zip(Nx, P))
+    res, sol, info = {}, {}, None
+    for prec in ("fp32_refine", "fp64"):
+        b = BatchNonPeriodic2D(Nx, P, lam, 0.0, 2 * math.pi, -1.0, 1.0, precision=prec)
+        f = b.pack([torch.from_numpy(x) for x in fs]).to(dev)
+        u = b.solve(f)
+        res[prec] = _ev_ms(lambda b=b, f=f, u=u: b.solve(f, out=u), flush, stream, steps, warmup)
+        sol[prec] = [x.cpu().numpy() for x in b.unpack(u)]
+        info = b.info()
+        b.destroy()
+
+    def rel(a, c):
+        return float(np.linalg.norm(a - c) / np.linalg.norm(c))
+
+    out = {
+        "workload": BATCH_WORKLOAD, "precision": "fp32_refine", "dof_per_solve": dof,
+        "value": dof / (res["fp32_refine"] * 1e-3) / 1e9, "unit": "GDOF/s", "ms_per_step": res["fp32_refine"],
+        "fp64": {"value": dof / (res["fp64"] * 1e-3) / 1e9, "ms_per_step": res["fp64"]},
+        "max_rel_l2_refine_vs_fp64": max(rel(a, c) for a, c in zip(sol["fp32_refine"], sol["fp64"])),
+        "max_rel_l2_fp64_vs_exact": max(rel(a, c) for a, c in zip(sol["fp64"], us)),
+        "launch": "one cudaGraphLaunch per solve; size classes on concurrent streams inside the graph",
+        "classes": info["classes"], "kernels_per_solve": info["kernels_per_solve"],
+        "l2": "256 MB buffer written before every timed solve",
+    }
+    if cpu:
+        from oracle import oracle as O
+
+        O.build()
+        if O.have_reference():
+            t, errs = 0.0, []
+            for f, la, u in zip(fs, lam, sol["fp32_refine"]):
+                z = np.zeros(f.shape[0])
+                r, ms = O.ref_solve2d(f, z, z, xl=0.0, xr=2 * math.pi, yl=-1.0, yr=1.0, lam=la, return_time=True)
+                t += ms
+                errs.append(rel(u, r))
+            out["cpu_baseline"] = {"value": dof / (t * 1e-3) / 1e9, "unit": "GDOF/s", "cores": 1, "kind": "reference",
+                                   "sample": "the reference's SolvePDE of each of the 512 problems, one core, "
+                                             "its own SolvePDE clock summed"}
+            out["max_rel_l2_refine_vs_reference"] = max(errs)
+    return out
+
+
+def _leg_adjoint(dev, flush, stream, steps, warmup):
+    import torch
+
+    from mpi_b200 import NonPeriodic3D
+    from mpi_b200 import workloads as W
+
+    n, P, la = 128, 65, 5.0
+    f = torch.from_numpy(W.smooth_field_3d(n, n, P, seed=11)).to(dev)
+    uobs = torch.from_numpy(W.smooth_field_3d(n, n, P, seed=12)).to(dev)
+    out = {"workload": ADJ_WORKLOAD}
+    for prec in ("fp32", "fp64"):
+        p = NonPeriodic3D(n, n, P, P, *DOM, Lambda=la, precision=prec)
+        u = p.SolvePDE(f)
+        fwd = _ev_ms(lambda: p.SolvePDE(f, out=u), flush, stream, steps, warmup)
+        ubar = u - uobs
+
+        def both():
+            p.SolvePDE(f, out=u)
+            torch.sub(u, uobs, out=ubar)
+            p.SolveAdjoint(ubar, u=u)
+
+        fb = _ev_ms(both, flush, stream, steps, warmup)
+        out[prec] = {"forward_ms": fwd, "forward_plus_adjoint_ms": fb, "ratio": fb / fwd}
+        p.DestroyPDEPlan()
+    return out
+
+
+def _leg_fd(dev, flush, stream, steps, warmup):
+    import torch
+
+    from mpi_b200 import Helmholtz3DFD
+    from mpi_b200 import workloads as W
+
+    Nx, Ny, Nz = 1024, 1024, 256
+    f = torch.from_numpy(W.smooth_field_fd(Nx, Ny, Nz, seed=1239)).to(dev)
+    dof = Nx * Ny * Nz
+    out = {"workload": FD_WORKLOAD, "dof_per_solve": dof}
+    us = {}
+    for prec in ("fp32", "fp64"):
+        p = Helmholtz3DFD(Nx, Ny, Nz, 0.0, 1.0, 0.0, 1.0, 0.0, 1.0, Lambda=1.0, precision=prec)
+        u = p.SolvePDE(f)
+        fwd = _ev_ms(lambda: p.SolvePDE(f, out=u), flush, stream, steps, warmup)
+        adj = _ev_ms(lambda: p.SolveAdjoint(u), flush, stream, steps, warmup)
+        out[prec] = {"value": dof / (fwd * 1e-3) / 1e9, "unit": "GDOF/s", "forward_ms": fwd, "adjoint_ms": adj}
+        us[prec] = u
+        p.DestroyPDEPlan()
+    out["rel_l2_fp32_vs_fp64"] = float((us["fp32"] - us["fp64"]).norm() / us["fp64"].norm())
+    return out
 
 
 def _cpu_baseline(fnp):

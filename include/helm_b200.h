@@ -159,6 +159,40 @@ int helm_plan_stage_times(helm_plan_t plan, float* ms5);
 int helm_solve_static_scratch(helm_plan_t plan, const void* f, const double* gl, const double* gr, void* u,
                               void* stream);
 
+/* ---- batches of independent 2D problems of uneven sizes ----
+ * No counterpart in the reference, which solves one problem per plan
+ * (NonPeriodic2D_MPI.h:33-37).  Problem p is the 2D problem of
+ * helm2d_plan_create with Nx[p] Fourier modes, one GLL element of N[p] points,
+ * lambda[p], homogeneous Dirichlet rows in y, on the common domain
+ * [xl, xr) x [yl, yr].  f and u are packed: problem p is the compact
+ * [Nx[p]][N[p]] block at element offset sum_{q<p} Nx[q] N[q].  Problems of
+ * one size (Nx, N) share a class whose three kernels cover them all;
+ * helm_batch_solve runs every class as one CUDA graph, the class chains on
+ * concurrent streams, with a single cudaGraphLaunch on `stream`.  The graph is
+ * captured at the first call and again whenever f or u differ from the last
+ * call's.  Calls on one batch whose kernels overlap on the GPU race on its
+ * workspace: serialise them. */
+typedef struct helm_batch_s* helm_batch_t;
+
+int helm2d_batch_create(int nprob, const int* Nx, const int* N, const double* lambda, double xl, double xr,
+                        double yl, double yr, int precision, helm_batch_t* batch);
+
+/* Element offsets of the problems in the packed buffers (host array of nprob,
+ * may be NULL) and the packed length. */
+int helm_batch_offsets(helm_batch_t batch, long long* offsets, long long* total_elems);
+
+/* Size classes, kernel launches inside one solve, device bytes held. */
+int helm_batch_info(helm_batch_t batch, int* n_classes, int* kernels_per_solve, long long* device_bytes);
+
+/* enable = 0: helm_batch_solve launches the class kernels directly on `stream`,
+ * one class after another, instead of through the graph (default 1). */
+int helm_batch_set_graph(helm_batch_t batch, int enable);
+
+/* u = solution of every problem; f, u DEVICE double arrays of the packed length. */
+int helm_batch_solve(helm_batch_t batch, const double* f, double* u, void* stream);
+
+int helm_batch_destroy(helm_batch_t batch);
+
 /* Replaces DestroyPDEPlan() + DestroyFFTPlan(). NULL is accepted. */
 int helm_plan_destroy(helm_plan_t plan);
 

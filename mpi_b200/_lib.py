@@ -34,6 +34,8 @@ EXPORTS = (
     "helm_plan_set_refine_sweeps", "helm_solve", "helm_solve_adjoint", "helm_plan_get_grid",
     "helm_plan_info", "helm_plan_destroy", "helm_status_string", "helm_last_error",
     "helm_plan_set_stage_timing", "helm_plan_stage_times", "helm_fd3d_plan_create",
+    "helm2d_batch_create", "helm_batch_offsets", "helm_batch_info", "helm_batch_set_graph",
+    "helm_batch_solve", "helm_batch_destroy",
 )
 
 
@@ -77,6 +79,12 @@ def lib() -> ctypes.CDLL:
     L.helm_plan_destroy.argtypes = [vp]
     L.helm_plan_set_stage_timing.argtypes = [vp, i]
     L.helm_plan_stage_times.argtypes = [vp, P(ctypes.c_float)]
+    L.helm2d_batch_create.argtypes = [i, P(i), P(i), P(d), d, d, d, d, i, P(vp)]
+    L.helm_batch_offsets.argtypes = [vp, P(ll), P(ll)]
+    L.helm_batch_info.argtypes = [vp, P(i), P(i), P(ll)]
+    L.helm_batch_set_graph.argtypes = [vp, i]
+    L.helm_batch_solve.argtypes = [vp, vp, vp, vp]
+    L.helm_batch_destroy.argtypes = [vp]
     L.helm_status_string.argtypes = [i]
     L.helm_status_string.restype = ctypes.c_char_p
     L.helm_last_error.argtypes = []

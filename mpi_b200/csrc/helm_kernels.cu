@@ -95,12 +95,14 @@ __global__ void __launch_bounds__(THREADS) fft_kernel(FftArgs a, long long total
     const int c = (int)(gg - (long long)b * ccols);
     const int c0 = 2 * c, c1 = 2 * c + 1;  // real columns of an R2C / C2R pair
     const bool has1 = c1 < a.ncols;
+    const long long in_base = a.in_boff ? a.in_boff[b] : (long long)b * a.in_batch;
+    const long long out_base = a.out_boff ? a.out_boff[b] : (long long)b * a.out_batch;
 
     C v[R0];
     // ---------------------------------------------------------- pass 0 --
     if constexpr (MODE == FFT_C2R) {
         // Z_k = A_k + i B_k over the full length from the two half spectra
-        const C* in = static_cast<const C*>(a.in) + (long long)b * a.in_batch;
+        const C* in = static_cast<const C*>(a.in) + in_base;
         for (int k = tc; k <= L / 2; k += TPC) {
             C A = mk((T)0, (T)0), B = mk((T)0, (T)0);
             if (valid) {
@@ -115,7 +117,7 @@ __global__ void __launch_bounds__(THREADS) fft_kernel(FftArgs a, long long total
 #pragma unroll
         for (int r = 0; r < R0; ++r) v[r] = sm[(tc + r * TPC) * CT + cl];
     } else if constexpr (MODE == FFT_R2C) {
-        const TIO* in = static_cast<const TIO*>(a.in) + (long long)b * a.in_batch;
+        const TIO* in = static_cast<const TIO*>(a.in) + in_base;
         int k0 = -1, k1 = -1, j0 = 0, j1 = 0;  // GLL slot of the two real columns
         if (a.P > 0) { k0 = c0 % a.P; j0 = c0 / a.P; k1 = c1 % a.P; j1 = c1 / a.P; }
         const bool bnd0 = a.P > 0 && (k0 == 0 || k0 == a.P - 1);
@@ -151,7 +153,7 @@ __global__ void __launch_bounds__(THREADS) fft_kernel(FftArgs a, long long total
             v[r] = mk(x0, x1);
         }
     } else {
-        const C* in = static_cast<const C*>(a.in) + (long long)b * a.in_batch;
+        const C* in = static_cast<const C*>(a.in) + in_base;
 #pragma unroll
         for (int r = 0; r < R0; ++r) v[r] = valid ? in[(long long)(tc + r * TPC) * a.in_row + c] : mk((T)0, (T)0);
     }
@@ -177,7 +179,7 @@ __global__ void __launch_bounds__(THREADS) fft_kernel(FftArgs a, long long total
     const T sc = (T)a.scale;
     if constexpr (MODE == FFT_C2C) {
         if (valid) {
-            C* out = static_cast<C*>(a.out) + (long long)b * a.out_batch;
+            C* out = static_cast<C*>(a.out) + out_base;
 #pragma unroll
             for (int t = 0; t < R0 / RL; ++t)
 #pragma unroll
@@ -188,7 +190,7 @@ __global__ void __launch_bounds__(THREADS) fft_kernel(FftArgs a, long long total
         }
     } else if constexpr (MODE == FFT_C2R) {
         if (valid) {
-            TIO* out = static_cast<TIO*>(a.out) + (long long)b * a.out_batch;
+            TIO* out = static_cast<TIO*>(a.out) + out_base;
 #pragma unroll
             for (int t = 0; t < R0 / RL; ++t)
 #pragma unroll
@@ -203,7 +205,7 @@ __global__ void __launch_bounds__(THREADS) fft_kernel(FftArgs a, long long total
         pass_to_smem<T, L, RL, NSL, TPC, CT, R0>(sm, tc, cl, v);
         __syncthreads();
         if (valid) {
-            C* out = static_cast<C*>(a.out) + (long long)b * a.out_batch;
+            C* out = static_cast<C*>(a.out) + out_base;
             const T h = (T)0.5 * sc;
             for (int k = tc; k <= L / 2; k += TPC) {
                 const C Z = sm[k * CT + cl];

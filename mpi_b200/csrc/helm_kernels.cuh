@@ -33,6 +33,10 @@ struct FftArgs {
     // into the first and last interior equations).
     int bc_add;
     double bc_scale_l, bc_scale_r;
+    // optional per-batch element offsets of the input / output (batched plans of
+    // independent problems in a packed buffer); NULL: batch * *_batch
+    const long long* in_boff;
+    const long long* out_boff;
 };
 
 // Finite-difference variant: one tridiagonal solve along z per spectrum row.

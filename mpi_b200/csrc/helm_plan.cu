@@ -91,35 +91,40 @@ static std::vector<T> twiddles(int L)
     return t;
 }
 
-// Groups of spectrum rows that share one shifted operator.
+// Groups of spectrum rows that share one shifted operator (per problem of a
+// batched plan: problem b's rows follow problem b-1's in the spectrum).
 static void build_groups(Plan& p)
 {
     const int nkx = p.Nx / 2 + 1;
     const int Nyf = p.dim == 3 ? p.Ny : 1;
     const bool merge = (p.dim == 3) && (p.Lx == p.Ly);  // sigma depends on kx^2+ky^2 only
-    std::map<long long, std::vector<int>> by_key;
-    std::map<long long, std::pair<int, int>> key_pair;
-    for (int kx = 0; kx < nkx; ++kx)
-        for (int ky = 0; ky < Nyf; ++ky) {
-            const int jw = p.dim == 3 ? std::min(ky, p.Ny - ky) : 0;
-            const long long key = merge ? (long long)kx * kx + (long long)jw * jw : (long long)kx * 4096 + jw;
-            by_key[key].push_back(kx * Nyf + ky);
-            if (!key_pair.count(key)) key_pair[key] = {kx, jw};
-        }
     p.grp_start.assign(1, 0);
     p.grp_rows.clear();
     p.grp_iw.clear();
     p.grp_jw.clear();
     p.sigma.clear();
-    for (auto& kv : by_key) {
-        const int iw = key_pair[kv.first].first, jw = key_pair[kv.first].second;
-        double s = p.lambda + 4.0 * kRefPi * kRefPi * iw * iw / (p.Lx * p.Lx);
-        if (p.dim == 3) s = s + 4.0 * kRefPi * kRefPi * jw * jw / (p.Ly * p.Ly);
-        p.sigma.push_back(s);
-        p.grp_iw.push_back(iw);
-        p.grp_jw.push_back(jw);
-        for (int r : kv.second) p.grp_rows.push_back(r);
-        p.grp_start.push_back((int)p.grp_rows.size());
+    for (int b = 0; b < p.batch; ++b) {
+        const double lam = p.batch > 1 ? p.lambdas[b] : p.lambda;
+        const int row0 = b * nkx * Nyf;
+        std::map<long long, std::vector<int>> by_key;
+        std::map<long long, std::pair<int, int>> key_pair;
+        for (int kx = 0; kx < nkx; ++kx)
+            for (int ky = 0; ky < Nyf; ++ky) {
+                const int jw = p.dim == 3 ? std::min(ky, p.Ny - ky) : 0;
+                const long long key = merge ? (long long)kx * kx + (long long)jw * jw : (long long)kx * 4096 + jw;
+                by_key[key].push_back(row0 + kx * Nyf + ky);
+                if (!key_pair.count(key)) key_pair[key] = {kx, jw};
+            }
+        for (auto& kv : by_key) {
+            const int iw = key_pair[kv.first].first, jw = key_pair[kv.first].second;
+            double s = lam + 4.0 * kRefPi * kRefPi * iw * iw / (p.Lx * p.Lx);
+            if (p.dim == 3) s = s + 4.0 * kRefPi * kRefPi * jw * jw / (p.Ly * p.Ly);
+            p.sigma.push_back(s);
+            p.grp_iw.push_back(iw);
+            p.grp_jw.push_back(jw);
+            for (int r : kv.second) p.grp_rows.push_back(r);
+            p.grp_start.push_back((int)p.grp_rows.size());
+        }
     }
     p.ngroups = (int)p.sigma.size();
 }
@@ -354,10 +359,14 @@ static int setup_plan(Plan& p)
     }
     const int prec_code = p.precision == HELM_FP64 ? 0 : (p.precision == HELM_FP32 ? 1 : 2);
     if (p.method == HELM_METHOD_AUTO) p.method = HELM_METHOD_FDM;
-    // the FDM transforms live in shared memory; beyond its capacity use the LU method
-    if (p.method == HELM_METHOD_FDM && rows_smem_bytes(2, prec_code, n, p.ld) > kMaxSmemPerBlock)
+    // one-element plans run the folded FDM kernel, whose half-size transforms fit
+    // shared memory up to 129 points at every precision
+    const int fold_ld = 32 * (((n / 2 + n % 2) + 31) / 32);
+    const bool fold_fits = p.Ns == 1 && fold_ld <= 64 && fdm_fast_smem_bytes(prec_code, fold_ld) <= kMaxSmemPerBlock;
+    // the unfolded FDM transforms live in shared memory; beyond its capacity use the LU method
+    if (p.method == HELM_METHOD_FDM && !fold_fits && rows_smem_bytes(2, prec_code, n, p.ld) > kMaxSmemPerBlock)
         p.method = HELM_METHOD_LU;
-    if (rows_smem_bytes(p.method, prec_code, n, p.ld) > kMaxSmemPerBlock) {
+    if (!(p.method == HELM_METHOD_FDM && fold_fits) && rows_smem_bytes(p.method, prec_code, n, p.ld) > kMaxSmemPerBlock) {
         g_last_error = "GLL size too large for the row-solve kernel at this precision";
         return HELM_ERR_UNSUPPORTED;
     }
@@ -449,7 +458,7 @@ static int setup_plan(Plan& p)
     p.nrows = (long long)nkx * Nyf;
     p.elem_spec = p.nrows * N;
     int st;
-    if ((st = p.alloc(&p.d_spec, (size_t)p.Ns * p.elem_spec * (td ? 16 : 8)))) return st;
+    if ((st = p.alloc(&p.d_spec, (size_t)p.Ns * p.batch * p.elem_spec * (td ? 16 : 8)))) return st;
     auto up_tw = [&](int L, void** d) -> int {
         if (td) { auto t = twiddles<double>(L); return p.upload(d, t.data(), t.size() * sizeof(double)); }
         auto t = twiddles<float>(L);
@@ -493,8 +502,12 @@ static int setup_plan(Plan& p)
     p.h_V = V;
     p.h_Vi = Vi;
     if (!lu && p.Ns == 1) {
-        if ((st = setup_adjoint(p, A0, lam, V, Vi, prec_code))) return st;
+        if (p.packed_elems == 0 && (st = setup_adjoint(p, A0, lam, V, Vi, prec_code))) return st;
         if ((st = setup_fast(p, A0, prec_code))) return st;
+    }
+    if (!p.fast && rows_smem_bytes(p.method, prec_code, n, p.ld) > kMaxSmemPerBlock) {
+        g_last_error = "GLL size too large for the row-solve kernel at this precision";
+        return HELM_ERR_UNSUPPORTED;
     }
     return HELM_OK;
 }
@@ -523,6 +536,9 @@ static int fft_pass(Plan& p, int L, int mode, int dir, const void* in, void* out
     a.bc_add = p.fd ? 1 : 0;
     a.bc_scale_l = p.fd_scale_l;
     a.bc_scale_r = p.fd_scale_r;
+    // batched plans: the caller's packed f (x pass) and u (inverse x pass)
+    a.in_boff = stage == 0 ? p.d_boff : nullptr;
+    a.out_boff = stage == 3 ? p.d_boff : nullptr;
     const long long ccols = (mode == FFT_C2C) ? ncols : (ncols + 1) / 2;
     const int td = p.precision != HELM_FP32;
     const int io = (td || io_double) ? 8 : p.io_bytes;
@@ -547,7 +563,7 @@ static int run_pipeline(Plan& p, const void* in, const double* gl, const double*
     mark(0);
     // 1. x: real-to-complex (forward: GLL boundary slots take the boundary data)
     if ((st = fft_pass(p, p.Nx, FFT_R2C, -1, in, p.d_spec, p.x_stride, cols, p.elem_stride, p.elem_spec, (int)cols,
-                       p.Ns, 1.0, p.d_tw_x, gl, gr, !adjoint, adjoint, 0, s)))
+                       p.Ns * p.batch, 1.0, p.d_tw_x, gl, gr, !adjoint, adjoint, 0, s)))
         return st;
     mark(1);
     // 2. y: complex-to-complex along the middle axis
@@ -657,7 +673,7 @@ static int run_pipeline(Plan& p, const void* in, const double* gl, const double*
     // 5. x: complex-to-real, scaled by 1/(Nx Ny) (the reference's /Nx, /Ny)
     const double scale = 1.0 / ((double)p.Nx * (p.dim == 3 ? p.Ny : 1));
     if ((st = fft_pass(p, p.Nx, FFT_C2R, 1, p.d_spec, out, cols, p.x_stride, p.elem_spec, p.elem_stride, (int)cols,
-                       p.Ns, scale, p.d_tw_x, nullptr, nullptr, false, adjoint, 3, s)))
+                       p.Ns * p.batch, scale, p.d_tw_x, nullptr, nullptr, false, adjoint, 3, s)))
         return st;
     mark(5);
     return HELM_OK;
@@ -677,7 +693,8 @@ static int autotune(Plan& p)
     const std::string key = std::string(p.fd ? "fd:" : "gll:") + std::to_string(p.dim) + ":" + std::to_string(p.Nx) +
                             ":" + std::to_string(p.Ny) + ":" +
                             std::to_string(p.N) + ":" + std::to_string(p.Ns) + ":" + std::to_string(p.precision) +
-                            ":" + std::to_string(p.io_bytes) + ":" + std::to_string(p.x_stride);
+                            ":" + std::to_string(p.io_bytes) + ":" + std::to_string(p.x_stride) + ":" +
+                            std::to_string(p.batch);
     {
         std::lock_guard<std::mutex> lock(g_tune_mutex);
         auto it = g_tune_cache.find(key);
@@ -687,7 +704,8 @@ static int autotune(Plan& p)
             return HELM_OK;
         }
     }
-    const size_t bytes = (size_t)p.Ns * p.elem_stride * (p.precision == HELM_FP32 ? p.io_bytes : 8);
+    const long long elems = std::max((long long)p.Ns * p.elem_stride, p.packed_elems);
+    const size_t bytes = (size_t)elems * (p.precision == HELM_FP32 ? p.io_bytes : 8);
     void *f = nullptr, *u = nullptr;
     if (cudaMalloc(&f, bytes) != cudaSuccess || cudaMalloc(&u, bytes) != cudaSuccess) {
         cudaGetLastError();
@@ -891,6 +909,47 @@ static int create_plan(int dim, int Nx, int Ny, int Ngll_total, int N, double xl
     if (!st) st = autotune(*p);
     if (st) { p->release(); delete p; return st; }
     *out = reinterpret_cast<helm_plan_t>(p);
+    return HELM_OK;
+}
+
+void set_last_error(const char* msg) { g_last_error = msg; }
+
+int create_batch_class(int Nx, int N, double xl, double xr, double yl, double yr, const std::vector<double>& lams,
+                       const std::vector<long long>& offs, long long packed_elems, int precision, Plan** out)
+{
+    *out = nullptr;
+    if (lams.empty() || lams.size() != offs.size()) return HELM_ERR_INVALID;
+    if (N < 3 || N > 129 || Nx < 4) { g_last_error = "size out of range"; return HELM_ERR_INVALID; }
+    if (!is_pow2(Nx)) { g_last_error = "N has to be 2^n"; return HELM_ERR_NOT_POW2; }
+    if (Nx > 1024) { g_last_error = "Fourier size beyond 4..1024"; return HELM_ERR_UNSUPPORTED; }
+    Plan* p = new (std::nothrow) Plan();
+    if (!p) return HELM_ERR_OOM;
+    cudaGetDevice(&p->device);
+    p->dim = 2;
+    p->Nx = Nx;
+    p->Ny = 1;
+    p->N = N;
+    p->Ns = 1;
+    p->xl = xl; p->xr = xr; p->yl = yl; p->yr = yr;
+    p->Lx = xr - xl;
+    p->Ly = yr - yl;
+    p->Lgll = yr - yl;
+    p->bc = helm_robin_t{0.0, 1.0, 0.0, 1.0};
+    p->batch = (int)lams.size();
+    p->lambdas = lams;
+    p->lambda = lams[0];
+    p->precision = precision;
+    p->method = HELM_METHOD_AUTO;
+    p->x_stride = N;
+    p->elem_stride = (long long)Nx * N;
+    p->bc_x_stride = 1;
+    p->packed_elems = packed_elems;
+    int st = setup_plan(*p);
+    if (!st && !p->fast) { g_last_error = "batched plans need the folded fast-diagonalisation path"; st = HELM_ERR_UNSUPPORTED; }
+    if (!st) st = p->upload((void**)&p->d_boff, offs.data(), offs.size() * sizeof(long long));
+    if (!st) st = autotune(*p);
+    if (st) { p->release(); delete p; return st; }
+    *out = p;
     return HELM_OK;
 }
 

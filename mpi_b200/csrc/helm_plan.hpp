@@ -70,6 +70,13 @@ struct Plan {
     double* d_feN = nullptr;
     double* d_fc0 = nullptr;       // folded D2[int][0], D2[int][N-1]
     double* d_fcN = nullptr;
+    // batched independent 2D problems of one size class (helm_batch_*): their
+    // lambdas, and the element offsets of each problem in the caller's packed
+    // f / u buffers
+    int batch = 1;
+    std::vector<double> lambdas;
+    long long* d_boff = nullptr;
+    long long packed_elems = 0;  // length of the caller's packed buffers
     // finite-difference variant (FFT in x and y, Thomas along z)
     bool fd = false;
     double fd_cz1 = 0, fd_dfirst = 0, fd_sfirst = 0, fd_dlast = 0, fd_slast = 0;
@@ -91,5 +98,12 @@ struct Plan {
 };
 
 int solve(Plan& p, const void* f, const double* gl, const double* gr, void* u, cudaStream_t s);
+
+// One size class of a batch: `lams.size()` independent 2D problems with Nx
+// Fourier modes and N GLL points on one domain, homogeneous Dirichlet in y,
+// stored in the caller's packed buffers at element offsets `offs`.
+int create_batch_class(int Nx, int N, double xl, double xr, double yl, double yr, const std::vector<double>& lams,
+                       const std::vector<long long>& offs, long long packed_elems, int precision, Plan** out);
+void set_last_error(const char* msg);
 
 }  // namespace helm

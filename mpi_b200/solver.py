@@ -244,9 +244,74 @@ class Helmholtz3DFD(_PlanBase):
         return (self.Nx, self.Ny)
 
 
+class BatchNonPeriodic2D:
+    """Many independent 2D problems of uneven sizes solved together
+    (helm2d_batch_*).  Problem p has ``Nx[p]`` Fourier modes, one GLL element of
+    ``N[p]`` points, ``lambdas[p]`` and homogeneous Dirichlet rows in y, on the
+    common domain.  ``f`` and ``u`` are packed 1-D float64 tensors: problem p is
+    the ``[Nx[p], N[p]]`` block at ``offsets[p]``; :meth:`pack` / :meth:`unpack`
+    convert from / to per-problem tensors.  One solve is one CUDA graph launch
+    (``graph=False``: the class kernels launched directly)."""
+
+    def __init__(self, Nx: Sequence[int], N: Sequence[int], lambdas: Sequence[float], xl: float, xr: float,
+                 yl: float, yr: float, *, precision: str = "fp64"):
+        self._lib = L.lib()
+        self._batch = ctypes.c_void_p()
+        n = len(Nx)
+        if len(N) != n or len(lambdas) != n:
+            raise ValueError("Nx, N and lambdas need one entry per problem")
+        self.Nx, self.N, self.lambdas = list(Nx), list(N), [float(v) for v in lambdas]
+        self.precision = precision
+        ia = (ctypes.c_int * n)(*self.Nx)
+        na = (ctypes.c_int * n)(*self.N)
+        la = (ctypes.c_double * n)(*self.lambdas)
+        L.check(self._lib.helm2d_batch_create(n, ia, na, la, xl, xr, yl, yr, _PREC[precision],
+                                              ctypes.byref(self._batch)), "helm2d_batch_create")
+        offs = (ctypes.c_longlong * n)()
+        tot = ctypes.c_longlong()
+        L.check(self._lib.helm_batch_offsets(self._batch, offs, ctypes.byref(tot)), "helm_batch_offsets")
+        self.offsets = list(offs)
+        self.total = tot.value
+
+    def info(self) -> dict:
+        nc, nk = ctypes.c_int(), ctypes.c_int()
+        nb = ctypes.c_longlong()
+        L.check(self._lib.helm_batch_info(self._batch, ctypes.byref(nc), ctypes.byref(nk), ctypes.byref(nb)),
+                "helm_batch_info")
+        return {"classes": nc.value, "kernels_per_solve": nk.value, "device_bytes": nb.value}
+
+    def set_graph(self, enable: bool) -> None:
+        L.check(self._lib.helm_batch_set_graph(self._batch, int(bool(enable))), "helm_batch_set_graph")
+
+    def pack(self, fs: Sequence[torch.Tensor]) -> torch.Tensor:
+        return torch.cat([f.reshape(-1).to(torch.float64) for f in fs]).contiguous()
+
+    def unpack(self, u: torch.Tensor):
+        return [u[o:o + a * b].view(a, b) for o, a, b in zip(self.offsets, self.Nx, self.N)]
+
+    def solve(self, f: torch.Tensor, out: Optional[torch.Tensor] = None, stream=None) -> torch.Tensor:
+        if f.dtype != torch.float64 or not f.is_cuda or not f.is_contiguous() or f.numel() != self.total:
+            raise ValueError(f"f must be a contiguous CUDA float64 tensor of {self.total} elements")
+        u = torch.empty_like(f) if out is None else out
+        L.check(self._lib.helm_batch_solve(self._batch, ctypes.c_void_p(f.data_ptr()), ctypes.c_void_p(u.data_ptr()),
+                                           ctypes.c_void_p(_stream_ptr(stream))), "helm_batch_solve")
+        return u
+
+    def destroy(self) -> None:
+        if self._batch:
+            self._lib.helm_batch_destroy(self._batch)
+            self._batch = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.destroy()
+        except Exception:
+            pass
+
+
 def gdof(Nx: int, Ny: int, N: int, Ns: int = 1) -> int:
     """Degrees of freedom of one solve: grid values of u (Ns elements of N GLL points)."""
     return Nx * Ny * N * Ns
 
 
-__all__ = ["NonPeriodic2D", "NonPeriodic3D", "gdof", "math"]
+__all__ = ["BatchNonPeriodic2D", "Helmholtz3DFD", "NonPeriodic2D", "NonPeriodic3D", "gdof", "math"]

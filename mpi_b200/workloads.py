@@ -145,3 +145,25 @@ def smooth_field_fd(Nx: int, Ny: int, Nz: int, seed: int, kmax: int = 64) -> np.
     f = planes.reshape(L, Nx * Ny).T @ S
     f -= f.mean()
     return np.ascontiguousarray(f.reshape(Nx, Ny, Nz))
+
+
+BATCH_NX = (32, 64, 128, 256, 512)
+BATCH_ORDER = (16, 32, 64, 128)  # GLL polynomial orders; N + 1 points
+
+
+def batch_2d(nprob: int = 512, seed: int = 1237):
+    """Uneven batch of independent 2D problems: per problem Nx drawn from
+    {32, 64, 128, 256, 512}, GLL order from {16, 32, 64, 128} (order + 1
+    points), lambda log-uniform in [1e-2, 1e4], and f / u_exact the
+    manufactured sin(3x)(1-y^2)e^y problem of :func:`manufactured_2d` at that
+    size and lambda.  Returns (Nx list, points list, lambda list, f list, u list)."""
+    rng = np.random.default_rng(seed)
+    Nx = [int(v) for v in rng.choice(BATCH_NX, nprob)]
+    P = [int(v) + 1 for v in rng.choice(BATCH_ORDER, nprob)]
+    lam = [float(v) for v in 10.0 ** rng.uniform(-2.0, 4.0, nprob)]
+    fs, us = [], []
+    for nx, p, la in zip(Nx, P, lam):
+        f, u = manufactured_2d(nx, p, la)
+        fs.append(f)
+        us.append(u)
+    return Nx, P, lam, fs, us

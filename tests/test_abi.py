@@ -72,3 +72,26 @@ def test_null_arguments(lib):
 def test_status_strings(lib):
     for s in range(8):
         assert lib.helm_status_string(s)
+
+
+def _create_batch(lib, Nx, N, lam, prec=0, xr=1.0):
+    n = len(Nx)
+    b = ctypes.c_void_p()
+    st = lib.helm2d_batch_create(n, (ctypes.c_int * max(n, 1))(*Nx), (ctypes.c_int * max(n, 1))(*N),
+                                 (ctypes.c_double * max(n, 1))(*lam), 0.0, xr, -1.0, 1.0, prec, ctypes.byref(b))
+    if st == 0:
+        lib.helm_batch_destroy(b)
+    return st
+
+
+def test_batch_rejects_bad_input(lib):
+    assert _create_batch(lib, [], [], []) == L.HELM_ERR_INVALID
+    assert _create_batch(lib, [32, 48], [9, 9], [1.0, 1.0]) == L.HELM_ERR_NOT_POW2
+    assert _create_batch(lib, [32, 2048], [9, 9], [1.0, 1.0]) == L.HELM_ERR_UNSUPPORTED
+    assert _create_batch(lib, [32], [2], [1.0]) == L.HELM_ERR_INVALID
+    assert _create_batch(lib, [32], [130], [1.0]) == L.HELM_ERR_INVALID
+    assert _create_batch(lib, [32], [9], [float("nan")]) == L.HELM_ERR_INVALID
+    assert _create_batch(lib, [32], [9], [1.0], prec=5) == L.HELM_ERR_INVALID
+    assert _create_batch(lib, [32], [9], [1.0], xr=0.0) == L.HELM_ERR_INVALID
+    assert lib.helm_batch_solve(None, None, None, None) == L.HELM_ERR_INVALID
+    assert lib.helm_batch_destroy(None) == L.HELM_OK
