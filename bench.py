@@ -51,7 +51,45 @@ def _args():
     ap.add_argument("--impl", choices=("ours", "reference"), default="ours")
     ap.add_argument("--skip-cpu-baseline", action="store_true", help="omit the CPU leg (profiling runs)")
     ap.add_argument("--skip-side", action="store_true", help="omit the batch / adjoint / finite-difference legs")
+    ap.add_argument("--profile-case", choices=("fp64", "fp32_refine", "fp32", "fd64", "fd32", "batch"),
+                    help="run three untimed solves of one workload and exit (a small case for ncu captures)")
     return ap.parse_args()
+
+
+def profile_case(which: str):
+    """Plan creation (with its autotuning), then three solves: the headline
+    256 x 256 x 65 workload at one precision, a 256 x 256 x 256 finite-difference
+    solve, or the 512-problem batch."""
+    import torch
+
+    from mpi_b200 import workloads as W
+
+    torch.cuda.set_device(0)
+    if which in ("fd64", "fd32"):
+        from mpi_b200 import Helmholtz3DFD
+
+        n = 256
+        f = torch.from_numpy(W.smooth_field_fd(n, n, n, seed=1239)).cuda()
+        p = Helmholtz3DFD(n, n, n, 0.0, 1.0, 0.0, 1.0, 0.0, 1.0, Lambda=1.0,
+                          precision="fp64" if which == "fd64" else "fp32")
+        run = lambda: p.SolvePDE(f)  # noqa: E731
+    elif which == "batch":
+        from mpi_b200 import BatchNonPeriodic2D
+
+        Nx, P, lam, fs, _ = W.batch_2d(512, seed=1237)
+        p = BatchNonPeriodic2D(Nx, P, lam, 0.0, 2 * math.pi, -1.0, 1.0, precision="fp32_refine")
+        f = p.pack([torch.from_numpy(x) for x in fs]).cuda()
+        run = lambda: p.solve(f)  # noqa: E731
+    else:
+        from mpi_b200 import NonPeriodic3D
+
+        f = torch.from_numpy(W.smooth_field_3d(NX, NY, NGLL, seed=SEED)).cuda()
+        p = NonPeriodic3D(NX, NY, NGLL, NGLL, *DOM, Lambda=LAM, precision=which)
+        run = lambda: p.SolvePDE(f)  # noqa: E731
+    for _ in range(3):
+        run()
+    torch.cuda.synchronize()
+    print("profile case done:", which, flush=True)
 
 
 def _dist():
@@ -189,14 +227,15 @@ def _traffic_from_profiles(stage: str):
     """DRAM bytes per launch of a stage's kernel at this workload, from the
     committed ncu summary (profiles/), or None."""
     path = os.path.join(HERE, "profiles", "traffic_256x256x65.txt")
+    out = {}
     try:
         for line in open(path):
             m = re.match(r"^\s*(\w+)\s+(fp64|fp32_refine|fp32)\s+([\d.eE+]+)\s*$", line)
             if m and m.group(1) == stage:
-                return {m.group(2): float(m.group(3))}
+                out[m.group(2)] = float(m.group(3))
     except OSError:
         pass
-    return None
+    return out or None
 
 
 def _stage_bytes(stage: str, spec_bytes: float, io_bytes: float) -> float:
@@ -514,7 +553,9 @@ def _cpu_baseline(fnp):
 def main():
     args = _args()
     ws, rank, local = _dist()
-    if args.impl == "reference":
+    if args.profile_case:
+        profile_case(args.profile_case)
+    elif args.impl == "reference":
         run_reference_arm(args, ws, rank)
     else:
         run_ours(args, ws, rank, local)
