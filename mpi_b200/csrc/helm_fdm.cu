@@ -136,6 +136,95 @@ __device__ __forceinline__ void fdm_folded_core(const TF* Ws, const TF* Vs, cons
     }
 }
 
+// Epilogue of a folded solve for RPW rows: boundary values (Robin / interface
+// data, or the transposed 2x2 system of the adjoint), unfold, store.  x* hold
+// the folded solution, lane l owning fold index l + 32 t.
+template <typename TS, int NSS, int RPW, bool ADJ>
+__device__ __forceinline__ void fdm_store_rows(const FdmArgs& a, cplx_t<TS>* spec, const int (&rowid)[RPW],
+                                               const int (&grp)[RPW], const bool (&ok)[RPW],
+                                               const TS (&xsr)[RPW][NSS], const TS (&xsi)[RPW][NSS],
+                                               const TS (&xdr)[RPW][NSS], const TS (&xdi)[RPW][NSS], int lane)
+{
+    using CS = cplx_t<TS>;
+    const int ld = a.ld, ms = a.ms, ma = a.ma, m = a.m, n = a.n, P = a.P;
+    const TS r2 = (TS)0.70710678118654752440;
+#pragma unroll
+    for (int r = 0; r < RPW; ++r) {
+        if (!ok[r]) continue;  // warp-uniform
+        CS* row = spec + (long long)rowid[r] * P;
+        const int g = grp[r];
+        TS zlr = 0, zli = 0, zrr = 0, zri = 0;   // boundary values of the row (weights of hl / hr)
+        const bool bnd = a.hvec != nullptr;
+        if (bnd) {
+            // folded dot products with e0 / eN (forward: D0, DN rows; adjoint: D2 boundary columns)
+            TS p0r = 0, p0i = 0, pNr = 0, pNi = 0;
+#pragma unroll
+            for (int t = 0; t < NSS; ++t) {
+                const int k = lane + 32 * t;
+                if (k < ms) {
+                    const TS e0s = (TS)a.e0f[k], eNs = (TS)a.eNf[k];
+                    p0r += e0s * xsr[r][t]; p0i += e0s * xsi[r][t];
+                    pNr += eNs * xsr[r][t]; pNi += eNs * xsi[r][t];
+                }
+                if (k < ma) {
+                    const TS e0a = (TS)a.e0f[ld + k], eNa = (TS)a.eNf[ld + k];
+                    p0r += e0a * xdr[r][t]; p0i += e0a * xdi[r][t];
+                    pNr += eNa * xdr[r][t]; pNi += eNa * xdi[r][t];
+                }
+            }
+            p0r = wsum(p0r); p0i = wsum(p0i); pNr = wsum(pNr); pNi = wsum(pNi);
+            const CS wl = row[0], wr = row[P - 1];
+            const double* sc = a.hscal + (size_t)g * 4;
+            if (!ADJ) {
+                // Robin ends, one element (NonPeriodic3D_MPI.cpp:334-336, 357-367, 528-529)
+                const TS b0 = (TS)(-a.al * sc[0] + a.bl), c0 = (TS)(-a.al * sc[1]);
+                const TS lb = (TS)(a.ar * sc[2]);
+                const TS bR = (TS)(a.ar * sc[3] + a.br) - (c0 / b0) * lb;
+                const TS rhr = wl.x + (TS)a.al * p0r, rhi = wl.y + (TS)a.al * p0i;
+                const TS rRr = wr.x - (TS)a.ar * pNr - (rhr / b0) * lb;
+                const TS rRi = wr.y - (TS)a.ar * pNi - (rhi / b0) * lb;
+                zrr = rRr / bR; zri = rRi / bR;
+                zlr = (rhr - c0 * zrr) / b0; zli = (rhi - c0 * zri) / b0;
+            } else {
+                const TS m00 = (TS)sc[0], m01 = (TS)sc[1], m10 = (TS)sc[2], m11 = (TS)sc[3];
+                const TS det = m00 * m11 - m01 * m10;
+                const TS q0r = wl.x - p0r, q0i = wl.y - p0i, qNr = wr.x - pNr, qNi = wr.y - pNi;
+                zlr = (m11 * q0r - m01 * qNr) / det; zli = (m11 * q0i - m01 * qNi) / det;
+                zrr = (m00 * qNr - m10 * q0r) / det; zri = (m00 * qNi - m10 * q0i) / det;
+            }
+        }
+        const double* hl = bnd ? a.hvec + (size_t)g * 2 * P : nullptr;
+        const double* hr = bnd ? hl + P : nullptr;
+#pragma unroll
+        for (int t = 0; t < NSS; ++t) {
+            const int k = lane + 32 * t;
+            if (k < m) {
+                TS lo_r = (TS)r2 * (xsr[r][t] + xdr[r][t]), lo_i = (TS)r2 * (xsi[r][t] + xdi[r][t]);
+                TS hi_r = (TS)r2 * (xsr[r][t] - xdr[r][t]), hi_i = (TS)r2 * (xsi[r][t] - xdi[r][t]);
+                if (bnd) {
+                    const TS l0 = (TS)hl[1 + k], r0 = (TS)hr[1 + k];
+                    const TS l1 = (TS)hl[n - k], r1 = (TS)hr[n - k];
+                    lo_r += zlr * l0 + zrr * r0; lo_i += zli * l0 + zri * r0;
+                    hi_r += zlr * l1 + zrr * r1; hi_i += zli * l1 + zri * r1;
+                }
+                row[1 + k] = mk(lo_r, lo_i);
+                row[n - k] = mk(hi_r, hi_i);
+            } else if (k < ms) {
+                TS mr = xsr[r][t], mi = xsi[r][t];
+                if (bnd) {
+                    const TS l0 = (TS)hl[1 + k], r0 = (TS)hr[1 + k];
+                    mr += zlr * l0 + zrr * r0; mi += zli * l0 + zri * r0;
+                }
+                row[1 + k] = mk(mr, mi);
+            }
+        }
+        if (lane == 0) {
+            row[0] = mk(zlr, zli);
+            row[P - 1] = mk(zrr, zri);
+        }
+    }
+}
+
 template <typename TS, typename TF, int NSS, int RPW, bool REFINE, bool ADJ>
 __global__ void __launch_bounds__(FDM_WARPS * 32, 2) fdm_fast_kernel(FdmArgs a)
 {
@@ -302,82 +391,7 @@ __global__ void __launch_bounds__(FDM_WARPS * 32, 2) fdm_fast_kernel(FdmArgs a)
                     }
             }
         }
-        // ---- epilogue per row: boundary values, unfold, store ----
-#pragma unroll
-        for (int r = 0; r < RPW; ++r) {
-            if (!ok[r]) continue;  // warp-uniform
-            CS* row = spec + (long long)rowid[r] * P;
-            const int g = grp[r];
-            TS zlr = 0, zli = 0, zrr = 0, zri = 0;   // boundary values of the row (weights of hl / hr)
-            const bool bnd = a.hvec != nullptr;
-            if (bnd) {
-                // folded dot products with e0 / eN (forward: D0, DN rows; adjoint: D2 boundary columns)
-                TS p0r = 0, p0i = 0, pNr = 0, pNi = 0;
-#pragma unroll
-                for (int t = 0; t < NSS; ++t) {
-                    const int k = lane + 32 * t;
-                    if (k < ms) {
-                        const TS e0s = (TS)a.e0f[k], eNs = (TS)a.eNf[k];
-                        p0r += e0s * xsr[r][t]; p0i += e0s * xsi[r][t];
-                        pNr += eNs * xsr[r][t]; pNi += eNs * xsi[r][t];
-                    }
-                    if (k < ma) {
-                        const TS e0a = (TS)a.e0f[ld + k], eNa = (TS)a.eNf[ld + k];
-                        p0r += e0a * xdr[r][t]; p0i += e0a * xdi[r][t];
-                        pNr += eNa * xdr[r][t]; pNi += eNa * xdi[r][t];
-                    }
-                }
-                p0r = wsum(p0r); p0i = wsum(p0i); pNr = wsum(pNr); pNi = wsum(pNi);
-                const CS wl = row[0], wr = row[P - 1];
-                const double* sc = a.hscal + (size_t)g * 4;
-                if (!ADJ) {
-                    // Robin ends, one element (NonPeriodic3D_MPI.cpp:334-336, 357-367, 528-529)
-                    const TS b0 = (TS)(-a.al * sc[0] + a.bl), c0 = (TS)(-a.al * sc[1]);
-                    const TS lb = (TS)(a.ar * sc[2]);
-                    const TS bR = (TS)(a.ar * sc[3] + a.br) - (c0 / b0) * lb;
-                    const TS rhr = wl.x + (TS)a.al * p0r, rhi = wl.y + (TS)a.al * p0i;
-                    const TS rRr = wr.x - (TS)a.ar * pNr - (rhr / b0) * lb;
-                    const TS rRi = wr.y - (TS)a.ar * pNi - (rhi / b0) * lb;
-                    zrr = rRr / bR; zri = rRi / bR;
-                    zlr = (rhr - c0 * zrr) / b0; zli = (rhi - c0 * zri) / b0;
-                } else {
-                    const TS m00 = (TS)sc[0], m01 = (TS)sc[1], m10 = (TS)sc[2], m11 = (TS)sc[3];
-                    const TS det = m00 * m11 - m01 * m10;
-                    const TS q0r = wl.x - p0r, q0i = wl.y - p0i, qNr = wr.x - pNr, qNi = wr.y - pNi;
-                    zlr = (m11 * q0r - m01 * qNr) / det; zli = (m11 * q0i - m01 * qNi) / det;
-                    zrr = (m00 * qNr - m10 * q0r) / det; zri = (m00 * qNi - m10 * q0i) / det;
-                }
-            }
-            const double* hl = bnd ? a.hvec + (size_t)g * 2 * P : nullptr;
-            const double* hr = bnd ? hl + P : nullptr;
-#pragma unroll
-            for (int t = 0; t < NSS; ++t) {
-                const int k = lane + 32 * t;
-                if (k < m) {
-                    TS lo_r = (TS)r2 * (xsr[r][t] + xdr[r][t]), lo_i = (TS)r2 * (xsi[r][t] + xdi[r][t]);
-                    TS hi_r = (TS)r2 * (xsr[r][t] - xdr[r][t]), hi_i = (TS)r2 * (xsi[r][t] - xdi[r][t]);
-                    if (bnd) {
-                        const TS l0 = (TS)hl[1 + k], r0 = (TS)hr[1 + k];
-                        const TS l1 = (TS)hl[n - k], r1 = (TS)hr[n - k];
-                        lo_r += zlr * l0 + zrr * r0; lo_i += zli * l0 + zri * r0;
-                        hi_r += zlr * l1 + zrr * r1; hi_i += zli * l1 + zri * r1;
-                    }
-                    row[1 + k] = mk(lo_r, lo_i);
-                    row[n - k] = mk(hi_r, hi_i);
-                } else if (k < ms) {
-                    TS mr = xsr[r][t], mi = xsi[r][t];
-                    if (bnd) {
-                        const TS l0 = (TS)hl[1 + k], r0 = (TS)hr[1 + k];
-                        mr += zlr * l0 + zrr * r0; mi += zli * l0 + zri * r0;
-                    }
-                    row[1 + k] = mk(mr, mi);
-                }
-            }
-            if (lane == 0) {
-                row[0] = mk(zlr, zli);
-                row[P - 1] = mk(zrr, zri);
-            }
-        }
+        fdm_store_rows<TS, NSS, RPW, ADJ>(a, spec, rowid, grp, ok, xsr, xsi, xdr, xdi, lane);
     }
 }
 
@@ -435,6 +449,238 @@ size_t fdm_fast_smem_bytes(int prec, int ld)
     if (prec == 0) return fdm_smem_layout<double, double, false, 2>(ld).total;
     if (prec == 1) return fdm_smem_layout<float, float, false, 2>(ld).total;
     return fdm_smem_layout<double, float, true, 2>(ld).total;
+}
+
+// ======================================== FP64 tensor-core folded solve ==
+//
+// The same folded solve as fdm_fast_kernel for FP64 plans, with both
+// transforms as products on the FP64 tensor cores (mma.sync m8n8k4 .f64):
+// per warp, the folded right-hand sides of RPW = 4 NT spectrum rows form the
+// B operand (ld x 8 NT: column 2 r + c is the real (c = 0) or imaginary part of
+// row r), the transform is the A operand (ld x ld, i = output fold index,
+// k = input fold index), and C accumulates ld x 8 NT in FP64.  The transforms
+// sit in shared memory in A-fragment order, so each fragment is one
+// conflict-free 8-byte load per lane.  Each row is staged in shared memory
+// between the passes (raw interior, scaled coefficients, folded solution) and
+// the epilogue is fdm_store_rows.
+//
+// Fragment layout of m8n8k4 .f64 (g = lane / 4, q = lane % 4):
+//   A[g][q];  B[q][g];  C[g][2 q], C[g][2 q + 1].
+
+__device__ __forceinline__ void dmma_8x8x4(double& c0, double& c1, double a, double b)
+{
+    asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};\n"
+                 : "+d"(c0), "+d"(c1)
+                 : "d"(a), "d"(b));
+}
+
+template <int NSS, int NT, int WARPS>
+struct MmaShape {
+    static constexpr int LD = 32 * NSS;     // padded fold length
+    static constexpr int MT = LD / 8;       // 8-row tiles of the output
+    static constexpr int KS = LD / 4;       // 4-deep steps of the contraction
+    static constexpr int RPW = 4 * NT;      // spectrum rows per warp
+    static constexpr int RSD = 4 * LD + 8;  // doubles per staged row (2 LD complex + pad)
+    static constexpr size_t mats = (size_t)4 * LD * LD;
+    static constexpr size_t smem = (mats + (size_t)WARPS * RPW * RSD) * sizeof(double);
+};
+
+template <int NSS, int NT, int WARPS, bool ADJ>
+__global__ void __launch_bounds__(WARPS * 32) fdm_mma_kernel(FdmArgs a)
+{
+    using S = MmaShape<NSS, NT, WARPS>;
+    constexpr int LD = S::LD, MT = S::MT, KS = S::KS, RPW = S::RPW, RSD = S::RSD;
+    extern __shared__ __align__(16) double dsm[];
+    double* A = dsm;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int g = lane >> 2, q = lane & 3;
+    double* stg = dsm + S::mats + (size_t)warp * RPW * RSD;
+    {
+        const double2* src = reinterpret_cast<const double2*>(a.mma_mats);
+        double2* dst = reinterpret_cast<double2*>(A);
+        for (int e = threadIdx.x; e < (int)(S::mats / 2); e += blockDim.x) dst[e] = src[e];
+    }
+    __syncthreads();
+
+    cplx_t<double>* spec = static_cast<cplx_t<double>*>(a.spec);
+    const int n = a.n, m = a.m, ms = a.ms, P = a.P, nrows = a.nrows;
+    const double r2 = 0.70710678118654752440;
+    const long long npacks = (nrows + RPW - 1) / RPW;
+    const double* As1 = A;                           // first transform, symmetric block
+    const double* As2 = A + (size_t)LD * LD;         // second transform, symmetric block
+    const double* Aa1 = A + (size_t)2 * LD * LD;     // first transform, antisymmetric block
+    const double* Aa2 = A + (size_t)3 * LD * LD;     // second transform, antisymmetric block
+
+    for (long long pk = (long long)blockIdx.x * WARPS + warp; pk < npacks; pk += (long long)gridDim.x * WARPS) {
+        int rowid[RPW], grp[RPW];
+        bool ok[RPW];
+#pragma unroll
+        for (int r = 0; r < RPW; ++r) {
+            const long long rr = pk * RPW + r;
+            ok[r] = rr < nrows;
+            rowid[r] = ok[r] ? a.rows[rr] : a.rows[0];
+            grp[r] = ok[r] ? a.row_grp[rr] : a.row_grp[0];
+        }
+        // ---- stage the interior of each row ----
+        __syncwarp();
+#pragma unroll
+        for (int r = 0; r < RPW; ++r) {
+            const double2* row = reinterpret_cast<const double2*>(spec + (long long)rowid[r] * P);
+            for (int i = lane; i < n; i += 32) *reinterpret_cast<double2*>(stg + r * RSD + 2 * i) = row[1 + i];
+        }
+        __syncwarp();
+        // ---- first transform; B fragments folded on the fly ----
+        double cs[NT][MT][2], ca[NT][MT][2];
+#pragma unroll
+        for (int t = 0; t < NT; ++t)
+#pragma unroll
+            for (int mt = 0; mt < MT; ++mt) cs[t][mt][0] = cs[t][mt][1] = ca[t][mt][0] = ca[t][mt][1] = 0.0;
+#pragma unroll 2
+        for (int kk = 0; kk < KS; ++kk) {
+            const int k = 4 * kk + q;
+            double bs[NT], ba[NT];
+#pragma unroll
+            for (int t = 0; t < NT; ++t) {
+                const double* raw = stg + (4 * t + (g >> 1)) * RSD + (g & 1);
+                double vs = 0.0, va = 0.0;
+                if (k < m) {
+                    const double lo = raw[2 * k], hi = raw[2 * (n - 1 - k)];
+                    vs = r2 * (lo + hi);
+                    va = r2 * (lo - hi);
+                } else if (k < ms) {
+                    vs = raw[2 * k];
+                }
+                bs[t] = vs;
+                ba[t] = va;
+            }
+#pragma unroll
+            for (int mt = 0; mt < MT; ++mt) {
+                const double as = As1[(mt * KS + kk) * 32 + lane];
+                const double aa = Aa1[(mt * KS + kk) * 32 + lane];
+#pragma unroll
+                for (int t = 0; t < NT; ++t) {
+                    dmma_8x8x4(cs[t][mt][0], cs[t][mt][1], as, bs[t]);
+                    dmma_8x8x4(ca[t][mt][0], ca[t][mt][1], aa, ba[t]);
+                }
+            }
+        }
+        // ---- scale by 1 / (lambda_j - sigma) of each row's shift; stage as the next B ----
+        __syncwarp();
+#pragma unroll
+        for (int t = 0; t < NT; ++t) {
+            const int r = 4 * t + q;
+            const long long rr = pk * RPW + r;
+            const int gr = a.row_grp[rr < nrows ? rr : 0];
+            const double* rc = static_cast<const double*>(a.recip) + (size_t)gr * 2 * LD;
+#pragma unroll
+            for (int mt = 0; mt < MT; ++mt) {
+                const int i = mt * 8 + g;
+                const double s = rc[i], u = rc[LD + i];
+                *reinterpret_cast<double2*>(stg + r * RSD + 2 * i) = make_double2(cs[t][mt][0] * s, cs[t][mt][1] * s);
+                *reinterpret_cast<double2*>(stg + r * RSD + 2 * (LD + i)) =
+                    make_double2(ca[t][mt][0] * u, ca[t][mt][1] * u);
+                cs[t][mt][0] = cs[t][mt][1] = ca[t][mt][0] = ca[t][mt][1] = 0.0;
+            }
+        }
+        __syncwarp();
+        // ---- second transform ----
+#pragma unroll 2
+        for (int kk = 0; kk < KS; ++kk) {
+            const int k = 4 * kk + q;
+            double bs[NT], ba[NT];
+#pragma unroll
+            for (int t = 0; t < NT; ++t) {
+                const double* c = stg + (4 * t + (g >> 1)) * RSD + (g & 1);
+                bs[t] = c[2 * k];
+                ba[t] = c[2 * (LD + k)];
+            }
+#pragma unroll
+            for (int mt = 0; mt < MT; ++mt) {
+                const double as = As2[(mt * KS + kk) * 32 + lane];
+                const double aa = Aa2[(mt * KS + kk) * 32 + lane];
+#pragma unroll
+                for (int t = 0; t < NT; ++t) {
+                    dmma_8x8x4(cs[t][mt][0], cs[t][mt][1], as, bs[t]);
+                    dmma_8x8x4(ca[t][mt][0], ca[t][mt][1], aa, ba[t]);
+                }
+            }
+        }
+        __syncwarp();
+#pragma unroll
+        for (int t = 0; t < NT; ++t) {
+            const int r = 4 * t + q;
+#pragma unroll
+            for (int mt = 0; mt < MT; ++mt) {
+                const int i = mt * 8 + g;
+                *reinterpret_cast<double2*>(stg + r * RSD + 2 * i) = make_double2(cs[t][mt][0], cs[t][mt][1]);
+                *reinterpret_cast<double2*>(stg + r * RSD + 2 * (LD + i)) = make_double2(ca[t][mt][0], ca[t][mt][1]);
+            }
+        }
+        __syncwarp();
+        // ---- folded solution to the lane-per-fold-index layout, epilogue ----
+        double xsr[RPW][NSS], xsi[RPW][NSS], xdr[RPW][NSS], xdi[RPW][NSS];
+#pragma unroll
+        for (int r = 0; r < RPW; ++r)
+#pragma unroll
+            for (int t = 0; t < NSS; ++t) {
+                const double2 vs = *reinterpret_cast<const double2*>(stg + r * RSD + 2 * (lane + 32 * t));
+                const double2 vd = *reinterpret_cast<const double2*>(stg + r * RSD + 2 * (LD + lane + 32 * t));
+                xsr[r][t] = vs.x; xsi[r][t] = vs.y;
+                xdr[r][t] = vd.x; xdi[r][t] = vd.y;
+            }
+        fdm_store_rows<double, NSS, RPW, ADJ>(a, spec, rowid, grp, ok, xsr, xsi, xdr, xdi, lane);
+    }
+}
+
+template <int NSS, int NT, int WARPS, bool ADJ>
+static int run_fdm_mma(const FdmArgs& a, cudaStream_t s)
+{
+    using S = MmaShape<NSS, NT, WARPS>;
+    auto k = fdm_mma_kernel<NSS, NT, WARPS, ADJ>;
+    cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)S::smem);
+    if (e != cudaSuccess) return (int)e;
+    int dev = 0, sms = 148, per = 1;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k, WARPS * 32, S::smem);
+    if (per < 1) per = 1;
+    const long long packs = (a.nrows + S::RPW - 1) / S::RPW;
+    long long grid = (packs + WARPS - 1) / WARPS;
+    if (grid > (long long)sms * per) grid = (long long)sms * per;
+    if (grid <= 0) return 0;
+    k<<<(unsigned)grid, WARPS * 32, S::smem, s>>>(a);
+    return (int)cudaGetLastError();
+}
+
+// variant 0: 4 rows per warp; variant 1: 8 rows per warp (each A fragment feeds
+// two products).  ld = 64 keeps 4 warps per CTA so the transforms (128 KB) fit.
+int launch_fdm_mma(const FdmArgs& a, cudaStream_t s, int variant)
+{
+    if (!a.mma_mats || a.ld != 32 * (a.ld / 32)) return (int)cudaErrorInvalidValue;
+    if (a.ld == 32) {
+        if (a.adjoint) return variant ? run_fdm_mma<1, 2, 8, true>(a, s) : run_fdm_mma<1, 1, 8, true>(a, s);
+        return variant ? run_fdm_mma<1, 2, 8, false>(a, s) : run_fdm_mma<1, 1, 8, false>(a, s);
+    }
+    if (a.ld == 64) {
+        if (a.adjoint) return variant ? run_fdm_mma<2, 2, 4, true>(a, s) : run_fdm_mma<2, 1, 4, true>(a, s);
+        return variant ? run_fdm_mma<2, 2, 4, false>(a, s) : run_fdm_mma<2, 1, 4, false>(a, s);
+    }
+    return (int)cudaErrorInvalidValue;
+}
+
+void fdm_mma_swizzle(const double* cm, int ld, double* out)
+{
+    const int MT = ld / 8, KS = ld / 4;
+    for (int b = 0; b < 4; ++b) {
+        const double* M = cm + (size_t)b * ld * ld;      // column-major: A[i][k] = M[k * ld + i]
+        double* O = out + (size_t)b * ld * ld;
+        for (int mt = 0; mt < MT; ++mt)
+            for (int kk = 0; kk < KS; ++kk)
+                for (int l = 0; l < 32; ++l) {
+                    const int i = mt * 8 + (l >> 2), k = kk * 4 + (l & 3);
+                    O[((size_t)mt * KS + kk) * 32 + l] = M[(size_t)k * ld + i];
+                }
+    }
 }
 
 }  // namespace helm

@@ -24,9 +24,17 @@ struct FdmArgs {
     const double* hscal; // [groups][4] scalars of the boundary system
     double al, bl, ar, br;
     int adjoint;
+    // FP64 tensor-core variant: the four transforms of `mats` in mma.sync
+    // m8n8k4 A-fragment order, [4][ld/8][ld/4][32] (NULL: not prepared)
+    const double* mma_mats;
 };
 
 int launch_fdm_fast(int prec, const FdmArgs& a, cudaStream_t s, int variant = 0);
 size_t fdm_fast_smem_bytes(int prec, int ld);
+// FP64 plans: the folded solve with its transforms on the FP64 tensor cores.
+int launch_fdm_mma(const FdmArgs& a, cudaStream_t s, int variant = 0);
+// The transforms `cm` (4 column-major ld x ld blocks) in the A-fragment order
+// launch_fdm_mma reads.
+void fdm_mma_swizzle(const double* cm, int ld, double* out);
 
 }  // namespace helm

@@ -322,6 +322,13 @@ static int setup_fast(Plan& p, const std::vector<double>& A0, int prec_code)
     };
     if ((st = up_t(fw, &p.d_fmats))) return st;
     if ((st = up_t(fa, &p.d_fmats_adj))) return st;
+    if (prec_code == 0) {
+        std::vector<double> sw(4 * L2);
+        fdm_mma_swizzle(fw.data(), ld, sw.data());
+        if ((st = p.upload((void**)&p.d_fmma, sw.data(), sw.size() * sizeof(double)))) return st;
+        fdm_mma_swizzle(fa.data(), ld, sw.data());
+        if ((st = p.upload((void**)&p.d_fmma_adj, sw.data(), sw.size() * sizeof(double)))) return st;
+    }
     if ((st = up_t(recip, &p.d_frecip))) return st;
     if ((st = p.upload((void**)&p.d_fd2, d2f.data(), d2f.size() * sizeof(double)))) return st;
     if ((st = p.upload((void**)&p.d_fd2_adj, d2a.data(), d2a.size() * sizeof(double)))) return st;
@@ -658,7 +665,11 @@ static int run_pipeline(Plan& p, const void* in, const double* gl, const double*
         fa.ar = p.bc.alphar;
         fa.br = p.bc.betar;
         fa.adjoint = adjoint ? 1 : 0;
-        e = launch_fdm_fast(prec, fa, s, p.row_var);
+        fa.mma_mats = adjoint ? p.d_fmma_adj : p.d_fmma;
+        if (prec == 0 && fa.mma_mats)
+            e = launch_fdm_mma(fa, s, p.row_var);
+        else
+            e = launch_fdm_fast(prec, fa, s, p.row_var);
     } else {
         e = launch_rows(p.method, prec, r, s);
     }

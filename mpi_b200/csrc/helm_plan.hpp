@@ -62,6 +62,8 @@ struct Plan {
     int fm = 0, fms = 0, fma = 0, fld = 32;
     void* d_fmats = nullptr;       // forward transforms [4][fld][fld]
     void* d_fmats_adj = nullptr;   // transposed transforms
+    double* d_fmma = nullptr;      // FP64 plans: the transforms in tensor-core fragment order
+    double* d_fmma_adj = nullptr;
     double* d_fd2 = nullptr;       // folded D2int blocks (refinement)
     double* d_fd2_adj = nullptr;   // their transposes
     void* d_frecip = nullptr;      // [G][2][fld] reciprocal shifts
