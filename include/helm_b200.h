@@ -148,6 +148,18 @@ int helm_plan_info(helm_plan_t plan, int* Ns, int* n_operators, int* method, lon
 int helm_plan_set_stage_timing(helm_plan_t plan, int enable);
 int helm_plan_stage_times(helm_plan_t plan, float* ms5);
 
+/* Kernel launch variants of the plan: fft4[i] (0..7) for the x, y, inverse y
+ * and inverse x FFT passes -- bit 0: 128-thread CTAs, bit 1: radix-8 schedule
+ * (lengths 128, 256), bit 2: persistent pipelined pass -- and rows (0..1) for
+ * the row solve (1: half as many rows per warp).  Plan creation times every
+ * variant on the plan's own shape and keeps the fastest per stage (environment
+ * HELM_AUTOTUNE=0: all 0).  Setting them pins the choice, e.g. to reproduce a
+ * run bit for bit.  Every variant computes the same transform; the last bits
+ * of the results may differ between variants.  No counterpart in the
+ * reference, which has one FFT code path. */
+int helm_plan_get_launch_variants(helm_plan_t plan, int* fft4, int* rows);
+int helm_plan_set_launch_variants(helm_plan_t plan, const int* fft4, int rows);
+
 /* helm_solve with the spectrum workspace taken from a fixed 16 MiB device
  * array inside this library instead of the plan's buffer; the call allocates
  * no device memory.  For callers whose memory manager owns the device memory

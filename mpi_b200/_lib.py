@@ -35,7 +35,7 @@ EXPORTS = (
     "helm_plan_info", "helm_plan_destroy", "helm_status_string", "helm_last_error",
     "helm_plan_set_stage_timing", "helm_plan_stage_times", "helm_fd3d_plan_create",
     "helm2d_batch_create", "helm_batch_offsets", "helm_batch_info", "helm_batch_set_graph",
-    "helm_batch_solve", "helm_batch_destroy",
+    "helm_batch_solve", "helm_batch_destroy", "helm_plan_get_launch_variants", "helm_plan_set_launch_variants",
 )
 
 
@@ -85,6 +85,8 @@ def lib() -> ctypes.CDLL:
     L.helm_batch_set_graph.argtypes = [vp, i]
     L.helm_batch_solve.argtypes = [vp, vp, vp, vp]
     L.helm_batch_destroy.argtypes = [vp]
+    L.helm_plan_get_launch_variants.argtypes = [vp, P(i), P(i)]
+    L.helm_plan_set_launch_variants.argtypes = [vp, P(i), i]
     L.helm_status_string.argtypes = [i]
     L.helm_status_string.restype = ctypes.c_char_p
     L.helm_last_error.argtypes = []

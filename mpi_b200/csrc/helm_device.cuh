@@ -107,4 +107,32 @@ template <> struct RadixV<128, 1> { static constexpr int n = 3, r0 = 8, r1 = 4, 
 template <> struct RadixV<256, 1> { static constexpr int n = 3, r0 = 8, r1 = 8, r2 = 4; };
 template <int L> constexpr bool has_small_radix() { return L == 128 || L == 256; }
 
+// Asynchronous global -> shared copies of one element (cp.async; valid = false
+// writes zeros and reads nothing), their commit and wait.
+__device__ __forceinline__ void cp_async_bytes4(void* dst, const void* src, bool valid)
+{
+    const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;\n" ::"r"(d), "l"(src), "r"(valid ? 4 : 0));
+}
+__device__ __forceinline__ void cp_async_bytes8(void* dst, const void* src, bool valid)
+{
+    const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(d), "l"(src), "r"(valid ? 8 : 0));
+}
+__device__ __forceinline__ void cp_async_bytes16(void* dst, const void* src, bool valid)
+{
+    const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(d), "l"(src), "r"(valid ? 16 : 0));
+}
+template <int BYTES>
+__device__ __forceinline__ void cp_async_elem(void* dst, const void* src, bool valid)
+{
+    if constexpr (BYTES == 4) cp_async_bytes4(dst, src, valid);
+    else if constexpr (BYTES == 8) cp_async_bytes8(dst, src, valid);
+    else cp_async_bytes16(dst, src, valid);
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
+__device__ __forceinline__ void cp_async_wait_prev() { asm volatile("cp.async.wait_group 1;\n" ::); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::); }
+
 }  // namespace helm

@@ -482,11 +482,27 @@ struct MmaShape {
     static constexpr int RPW = 4 * NT;      // spectrum rows per warp
     static constexpr int RSD = 4 * LD + 8;  // doubles per staged row (2 LD complex + pad)
     static constexpr size_t mats = (size_t)4 * LD * LD;
-    static constexpr size_t smem = (mats + (size_t)WARPS * RPW * RSD) * sizeof(double);
+    // two staging buffers per warp: the next pack's rows arrive while this one is solved
+    static constexpr size_t smem = (mats + (size_t)WARPS * 2 * RPW * RSD) * sizeof(double);
 };
 
+// Asynchronous copy of the interiors of pack pk's rows into stg (row r at
+// stg + r RSD, complex i at 2 i).
+template <int RPW, int RSD>
+__device__ __forceinline__ void mma_issue_pack(const FdmArgs& a, long long pk, double* stg, int lane)
+{
+    const cplx_t<double>* spec = static_cast<const cplx_t<double>*>(a.spec);
+#pragma unroll
+    for (int r = 0; r < RPW; ++r) {
+        const long long rr = pk * RPW + r;
+        const int rowid = rr < a.nrows ? a.rows[rr] : a.rows[0];
+        const cplx_t<double>* row = spec + (long long)rowid * a.P + 1;
+        for (int i = lane; i < a.n; i += 32) cp_async_bytes16(stg + r * RSD + 2 * i, row + i, true);
+    }
+}
+
 template <int NSS, int NT, int WARPS, bool ADJ>
-__global__ void __launch_bounds__(WARPS * 32) fdm_mma_kernel(FdmArgs a)
+__global__ void __launch_bounds__(WARPS * 32, (NSS == 1 ? 2 : 1)) fdm_mma_kernel(FdmArgs a)
 {
     using S = MmaShape<NSS, NT, WARPS>;
     constexpr int LD = S::LD, MT = S::MT, KS = S::KS, RPW = S::RPW, RSD = S::RSD;
@@ -494,7 +510,7 @@ __global__ void __launch_bounds__(WARPS * 32) fdm_mma_kernel(FdmArgs a)
     double* A = dsm;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int g = lane >> 2, q = lane & 3;
-    double* stg = dsm + S::mats + (size_t)warp * RPW * RSD;
+    double* stg_base = dsm + S::mats + (size_t)warp * 2 * RPW * RSD;
     {
         const double2* src = reinterpret_cast<const double2*>(a.mma_mats);
         double2* dst = reinterpret_cast<double2*>(A);
@@ -511,7 +527,15 @@ __global__ void __launch_bounds__(WARPS * 32) fdm_mma_kernel(FdmArgs a)
     const double* Aa1 = A + (size_t)2 * LD * LD;     // first transform, antisymmetric block
     const double* Aa2 = A + (size_t)3 * LD * LD;     // second transform, antisymmetric block
 
-    for (long long pk = (long long)blockIdx.x * WARPS + warp; pk < npacks; pk += (long long)gridDim.x * WARPS) {
+    const long long pstride = (long long)gridDim.x * WARPS;
+    long long pk = (long long)blockIdx.x * WARPS + warp;
+    int cur = 0;
+    if (pk < npacks) mma_issue_pack<RPW, RSD>(a, pk, stg_base, lane);
+    cp_async_commit();
+    for (; pk < npacks; pk += pstride, cur ^= 1) {
+        double* stg = stg_base + (size_t)cur * RPW * RSD;
+        if (pk + pstride < npacks) mma_issue_pack<RPW, RSD>(a, pk + pstride, stg_base + (size_t)(cur ^ 1) * RPW * RSD, lane);
+        cp_async_commit();
         int rowid[RPW], grp[RPW];
         bool ok[RPW];
 #pragma unroll
@@ -521,13 +545,8 @@ __global__ void __launch_bounds__(WARPS * 32) fdm_mma_kernel(FdmArgs a)
             rowid[r] = ok[r] ? a.rows[rr] : a.rows[0];
             grp[r] = ok[r] ? a.row_grp[rr] : a.row_grp[0];
         }
-        // ---- stage the interior of each row ----
-        __syncwarp();
-#pragma unroll
-        for (int r = 0; r < RPW; ++r) {
-            const double2* row = reinterpret_cast<const double2*>(spec + (long long)rowid[r] * P);
-            for (int i = lane; i < n; i += 32) *reinterpret_cast<double2*>(stg + r * RSD + 2 * i) = row[1 + i];
-        }
+        // ---- the staged interiors of this pack's rows ----
+        cp_async_wait_prev();
         __syncwarp();
         // ---- first transform; B fragments folded on the fly ----
         double cs[NT][MT][2], ca[NT][MT][2];
@@ -629,7 +648,9 @@ __global__ void __launch_bounds__(WARPS * 32) fdm_mma_kernel(FdmArgs a)
                 xdr[r][t] = vd.x; xdi[r][t] = vd.y;
             }
         fdm_store_rows<double, NSS, RPW, ADJ>(a, spec, rowid, grp, ok, xsr, xsi, xdr, xdi, lane);
+        __syncwarp();  // stg is refilled by the copy issued in the next iteration
     }
+    cp_async_wait_all();
 }
 
 template <int NSS, int NT, int WARPS, bool ADJ>
@@ -652,20 +673,230 @@ static int run_fdm_mma(const FdmArgs& a, cudaStream_t s)
     return (int)cudaGetLastError();
 }
 
-// variant 0: 4 rows per warp; variant 1: 8 rows per warp (each A fragment feeds
-// two products).  ld = 64 keeps 4 warps per CTA so the transforms (128 KB) fit.
+// ---- the same solve with the m16n8k8 .f64 shape (sm_90 and later) ----
+// Fragment layout (g = lane / 4, q = lane % 4):
+//   A (16 x 8): a0 = A[g][q], a1 = A[g + 8][q], a2 = A[g][q + 4], a3 = A[g + 8][q + 4]
+//   B (8 x 8):  b0 = B[q][g], b1 = B[q + 4][g]
+//   C (16 x 8): c0, c1 = C[g][2 q], C[g][2 q + 1];  c2, c3 = C[g + 8][2 q], C[g + 8][2 q + 1]
+// One product is 1024 multiply-adds (four times m8n8k4), a fragment of A four
+// consecutive doubles per lane in the stored order.
+__device__ __forceinline__ void dmma_16x8x8(double (&c)[4], const double2& a01, const double2& a23, double b0,
+                                            double b1)
+{
+    asm volatile("mma.sync.aligned.m16n8k8.row.col.f64.f64.f64.f64 {%0, %1, %2, %3}, {%4, %5, %6, %7}, {%8, %9}, "
+                 "{%0, %1, %2, %3};\n"
+                 : "+d"(c[0]), "+d"(c[1]), "+d"(c[2]), "+d"(c[3])
+                 : "d"(a01.x), "d"(a01.y), "d"(a23.x), "d"(a23.y), "d"(b0), "d"(b1));
+}
+
+template <int NSS, int WARPS, bool ADJ>
+__global__ void __launch_bounds__(WARPS * 32, (NSS == 1 ? 2 : 1)) fdm_mma16_kernel(FdmArgs a)
+{
+    using S = MmaShape<NSS, 1, WARPS>;
+    constexpr int LD = S::LD, RPW = S::RPW, RSD = S::RSD;
+    constexpr int MT = LD / 16, KS = LD / 8;
+    extern __shared__ __align__(16) double dsm[];
+    double* A = dsm;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int g = lane >> 2, q = lane & 3;
+    double* stg_base = dsm + S::mats + (size_t)warp * 2 * RPW * RSD;
+    {
+        const double2* src = reinterpret_cast<const double2*>(a.mma16_mats);
+        double2* dst = reinterpret_cast<double2*>(A);
+        for (int e = threadIdx.x; e < (int)(S::mats / 2); e += blockDim.x) dst[e] = src[e];
+    }
+    __syncthreads();
+
+    cplx_t<double>* spec = static_cast<cplx_t<double>*>(a.spec);
+    const int n = a.n, m = a.m, ms = a.ms, nrows = a.nrows;
+    const double r2 = 0.70710678118654752440;
+    const long long npacks = (nrows + RPW - 1) / RPW;
+    // fragment (mt, kk) of transform b: 4 doubles per lane at ((mt KS + kk) 32 + lane) 4
+    const double2* Af = reinterpret_cast<const double2*>(A);
+    constexpr size_t BLK = (size_t)LD * LD / 2;  // double2 per transform
+    const double* rcp = static_cast<const double*>(a.recip);
+
+    const long long pstride = (long long)gridDim.x * WARPS;
+    long long pk = (long long)blockIdx.x * WARPS + warp;
+    int cur = 0;
+    if (pk < npacks) mma_issue_pack<RPW, RSD>(a, pk, stg_base, lane);
+    cp_async_commit();
+    for (; pk < npacks; pk += pstride, cur ^= 1) {
+        double* stg = stg_base + (size_t)cur * RPW * RSD;
+        if (pk + pstride < npacks) mma_issue_pack<RPW, RSD>(a, pk + pstride, stg_base + (size_t)(cur ^ 1) * RPW * RSD, lane);
+        cp_async_commit();
+        int rowid[RPW], grp[RPW];
+        bool ok[RPW];
+#pragma unroll
+        for (int r = 0; r < RPW; ++r) {
+            const long long rr = pk * RPW + r;
+            ok[r] = rr < nrows;
+            rowid[r] = ok[r] ? a.rows[rr] : a.rows[0];
+            grp[r] = ok[r] ? a.row_grp[rr] : a.row_grp[0];
+        }
+        // reciprocal shifts of this lane's accumulator rows (row q), loaded early
+        double rs[MT][2], ra[MT][2];
+        {
+            const int gq = a.row_grp[(pk * RPW + q) < nrows ? pk * RPW + q : 0];
+            const double* rc = rcp + (size_t)gq * 2 * LD;
+#pragma unroll
+            for (int mt = 0; mt < MT; ++mt) {
+                rs[mt][0] = rc[mt * 16 + g];
+                rs[mt][1] = rc[mt * 16 + g + 8];
+                ra[mt][0] = rc[LD + mt * 16 + g];
+                ra[mt][1] = rc[LD + mt * 16 + g + 8];
+            }
+        }
+        cp_async_wait_prev();
+        __syncwarp();
+        // ---- first transform; B fragments folded on the fly ----
+        double cs[MT][4], ca[MT][4];
+#pragma unroll
+        for (int mt = 0; mt < MT; ++mt)
+#pragma unroll
+            for (int j = 0; j < 4; ++j) cs[mt][j] = ca[mt][j] = 0.0;
+        const double* raw = stg + (g >> 1) * RSD + (g & 1);
+#pragma unroll 2
+        for (int kk = 0; kk < KS; ++kk) {
+            double bs[2], ba[2];
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+                const int k = 8 * kk + q + 4 * h;
+                double vs = 0.0, va = 0.0;
+                if (k < m) {
+                    const double lo = raw[2 * k], hi = raw[2 * (n - 1 - k)];
+                    vs = r2 * (lo + hi);
+                    va = r2 * (lo - hi);
+                } else if (k < ms) {
+                    vs = raw[2 * k];
+                }
+                bs[h] = vs;
+                ba[h] = va;
+            }
+#pragma unroll
+            for (int mt = 0; mt < MT; ++mt) {
+                const double2* fs = Af + 0 * BLK + ((size_t)(mt * KS + kk) * 32 + lane) * 2;
+                const double2* fa = Af + 2 * BLK + ((size_t)(mt * KS + kk) * 32 + lane) * 2;
+                dmma_16x8x8(cs[mt], fs[0], fs[1], bs[0], bs[1]);
+                dmma_16x8x8(ca[mt], fa[0], fa[1], ba[0], ba[1]);
+            }
+        }
+        // ---- scale by 1 / (lambda_j - sigma); stage as the next B ----
+        __syncwarp();
+        {
+            double* row = stg + q * RSD;
+#pragma unroll
+            for (int mt = 0; mt < MT; ++mt) {
+                const int i0 = mt * 16 + g, i1 = i0 + 8;
+                *reinterpret_cast<double2*>(row + 2 * i0) = make_double2(cs[mt][0] * rs[mt][0], cs[mt][1] * rs[mt][0]);
+                *reinterpret_cast<double2*>(row + 2 * i1) = make_double2(cs[mt][2] * rs[mt][1], cs[mt][3] * rs[mt][1]);
+                *reinterpret_cast<double2*>(row + 2 * (LD + i0)) =
+                    make_double2(ca[mt][0] * ra[mt][0], ca[mt][1] * ra[mt][0]);
+                *reinterpret_cast<double2*>(row + 2 * (LD + i1)) =
+                    make_double2(ca[mt][2] * ra[mt][1], ca[mt][3] * ra[mt][1]);
+#pragma unroll
+                for (int j = 0; j < 4; ++j) cs[mt][j] = ca[mt][j] = 0.0;
+            }
+        }
+        __syncwarp();
+        // ---- second transform ----
+        const double* cf = stg + (g >> 1) * RSD + (g & 1);
+#pragma unroll 2
+        for (int kk = 0; kk < KS; ++kk) {
+            const int k0 = 8 * kk + q, k1 = k0 + 4;
+            const double bs0 = cf[2 * k0], bs1 = cf[2 * k1];
+            const double ba0 = cf[2 * (LD + k0)], ba1 = cf[2 * (LD + k1)];
+#pragma unroll
+            for (int mt = 0; mt < MT; ++mt) {
+                const double2* fs = Af + 1 * BLK + ((size_t)(mt * KS + kk) * 32 + lane) * 2;
+                const double2* fa = Af + 3 * BLK + ((size_t)(mt * KS + kk) * 32 + lane) * 2;
+                dmma_16x8x8(cs[mt], fs[0], fs[1], bs0, bs1);
+                dmma_16x8x8(ca[mt], fa[0], fa[1], ba0, ba1);
+            }
+        }
+        __syncwarp();
+        {
+            double* row = stg + q * RSD;
+#pragma unroll
+            for (int mt = 0; mt < MT; ++mt) {
+                const int i0 = mt * 16 + g, i1 = i0 + 8;
+                *reinterpret_cast<double2*>(row + 2 * i0) = make_double2(cs[mt][0], cs[mt][1]);
+                *reinterpret_cast<double2*>(row + 2 * i1) = make_double2(cs[mt][2], cs[mt][3]);
+                *reinterpret_cast<double2*>(row + 2 * (LD + i0)) = make_double2(ca[mt][0], ca[mt][1]);
+                *reinterpret_cast<double2*>(row + 2 * (LD + i1)) = make_double2(ca[mt][2], ca[mt][3]);
+            }
+        }
+        __syncwarp();
+        double xsr[RPW][NSS], xsi[RPW][NSS], xdr[RPW][NSS], xdi[RPW][NSS];
+#pragma unroll
+        for (int r = 0; r < RPW; ++r)
+#pragma unroll
+            for (int t = 0; t < NSS; ++t) {
+                const double2 vs = *reinterpret_cast<const double2*>(stg + r * RSD + 2 * (lane + 32 * t));
+                const double2 vd = *reinterpret_cast<const double2*>(stg + r * RSD + 2 * (LD + lane + 32 * t));
+                xsr[r][t] = vs.x; xsi[r][t] = vs.y;
+                xdr[r][t] = vd.x; xdi[r][t] = vd.y;
+            }
+        fdm_store_rows<double, NSS, RPW, ADJ>(a, spec, rowid, grp, ok, xsr, xsi, xdr, xdi, lane);
+        __syncwarp();  // stg is refilled by the copy issued in the next iteration
+    }
+    cp_async_wait_all();
+}
+
+template <int NSS, int WARPS, bool ADJ>
+static int run_fdm_mma16(const FdmArgs& a, cudaStream_t s)
+{
+    using S = MmaShape<NSS, 1, WARPS>;
+    auto k = fdm_mma16_kernel<NSS, WARPS, ADJ>;
+    cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)S::smem);
+    if (e != cudaSuccess) return (int)e;
+    int dev = 0, sms = 148, per = 1;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k, WARPS * 32, S::smem);
+    if (per < 1) per = 1;
+    const long long packs = (a.nrows + S::RPW - 1) / S::RPW;
+    long long grid = (packs + WARPS - 1) / WARPS;
+    if (grid > (long long)sms * per) grid = (long long)sms * per;
+    if (grid <= 0) return 0;
+    k<<<(unsigned)grid, WARPS * 32, S::smem, s>>>(a);
+    return (int)cudaGetLastError();
+}
+
+// variant 0: m16n8k8 products; variant 1: m8n8k4 products.  4 rows per warp;
+// ld = 64 keeps 4 warps per CTA so the transforms (128 KB) fit.
 int launch_fdm_mma(const FdmArgs& a, cudaStream_t s, int variant)
 {
-    if (!a.mma_mats || a.ld != 32 * (a.ld / 32)) return (int)cudaErrorInvalidValue;
+    if (!a.mma_mats || !a.mma16_mats) return (int)cudaErrorInvalidValue;
     if (a.ld == 32) {
-        if (a.adjoint) return variant ? run_fdm_mma<1, 2, 8, true>(a, s) : run_fdm_mma<1, 1, 8, true>(a, s);
-        return variant ? run_fdm_mma<1, 2, 8, false>(a, s) : run_fdm_mma<1, 1, 8, false>(a, s);
+        if (variant == 0) return a.adjoint ? run_fdm_mma16<1, 8, true>(a, s) : run_fdm_mma16<1, 8, false>(a, s);
+        return a.adjoint ? run_fdm_mma<1, 1, 8, true>(a, s) : run_fdm_mma<1, 1, 8, false>(a, s);
     }
     if (a.ld == 64) {
-        if (a.adjoint) return variant ? run_fdm_mma<2, 2, 4, true>(a, s) : run_fdm_mma<2, 1, 4, true>(a, s);
-        return variant ? run_fdm_mma<2, 2, 4, false>(a, s) : run_fdm_mma<2, 1, 4, false>(a, s);
+        if (variant == 0) return a.adjoint ? run_fdm_mma16<2, 4, true>(a, s) : run_fdm_mma16<2, 4, false>(a, s);
+        return a.adjoint ? run_fdm_mma<2, 1, 4, true>(a, s) : run_fdm_mma<2, 1, 4, false>(a, s);
     }
     return (int)cudaErrorInvalidValue;
+}
+
+void fdm_mma16_swizzle(const double* cm, int ld, double* out)
+{
+    const int MT = ld / 16, KS = ld / 8;
+    for (int b = 0; b < 4; ++b) {
+        const double* M = cm + (size_t)b * ld * ld;      // column-major: A[i][k] = M[k * ld + i]
+        double* O = out + (size_t)b * ld * ld;
+        for (int mt = 0; mt < MT; ++mt)
+            for (int kk = 0; kk < KS; ++kk)
+                for (int l = 0; l < 32; ++l) {
+                    const int gg = l >> 2, qq = l & 3;
+                    const int i0 = mt * 16 + gg, i1 = i0 + 8, k0 = kk * 8 + qq, k1 = k0 + 4;
+                    double* o = O + (((size_t)mt * KS + kk) * 32 + l) * 4;
+                    o[0] = M[(size_t)k0 * ld + i0];
+                    o[1] = M[(size_t)k0 * ld + i1];
+                    o[2] = M[(size_t)k1 * ld + i0];
+                    o[3] = M[(size_t)k1 * ld + i1];
+                }
+    }
 }
 
 void fdm_mma_swizzle(const double* cm, int ld, double* out)

@@ -27,6 +27,7 @@ struct FdmArgs {
     // FP64 tensor-core variant: the four transforms of `mats` in mma.sync
     // m8n8k4 A-fragment order, [4][ld/8][ld/4][32] (NULL: not prepared)
     const double* mma_mats;
+    const double* mma16_mats;  // the same transforms in m16n8k8 fragment order, [4][ld/16][ld/8][32][4]
 };
 
 int launch_fdm_fast(int prec, const FdmArgs& a, cudaStream_t s, int variant = 0);
@@ -36,5 +37,6 @@ int launch_fdm_mma(const FdmArgs& a, cudaStream_t s, int variant = 0);
 // The transforms `cm` (4 column-major ld x ld blocks) in the A-fragment order
 // launch_fdm_mma reads.
 void fdm_mma_swizzle(const double* cm, int ld, double* out);
+void fdm_mma16_swizzle(const double* cm, int ld, double* out);
 
 }  // namespace helm

@@ -217,6 +217,266 @@ __global__ void __launch_bounds__(THREADS) fft_kernel(FftArgs a, long long total
     }
 }
 
+// ------------------------------------------------ pipelined FFT pass --
+// The same transforms as fft_kernel from a persistent grid: every CTA walks
+// tiles blockIdx.x, blockIdx.x + gridDim.x, ... and copies the next tile's
+// input into shared memory (cp.async, one copy per element) while it
+// transforms the current one, so the loads of one tile overlap the butterflies
+// and stores of the previous.  Two tile buffers per CTA; the buffer of the
+// current tile doubles as the exchange buffer of its passes.
+
+
+template <typename T, typename TIO, int L, int THREADS, int SMALL>
+struct PipeShape {
+    using S = FftShape<T, L, THREADS, SMALL>;
+    // one tile buffer holds the staged input -- complex values (C2C), pairs of
+    // real inputs (R2C), or the pairs A_k, B_k of rows k <= L/2 (C2R) -- and
+    // then serves as the exchange buffer of the passes
+    static constexpr size_t c2r = (size_t)(L + 2) * S::CT * 2 * sizeof(T);
+    static constexpr size_t r2c = (size_t)L * S::CT * 2 * sizeof(TIO);
+    static constexpr size_t exch = (size_t)L * S::CT * 2 * sizeof(T);
+    static constexpr size_t big = c2r > r2c ? (c2r > exch ? c2r : exch) : (r2c > exch ? r2c : exch);
+    static constexpr size_t buf = (big + 15) / 16 * 16;
+    static constexpr size_t smem = 2 * buf;
+};
+
+// Issue the asynchronous copies of tile `tile` into `stage` (no commit).
+template <typename T, typename TIO, int L, int MODE, int THREADS, int SMALL>
+__device__ __forceinline__ void pipe_issue(const FftArgs& a, long long total_cols, long long tile,
+                                           unsigned char* stage)
+{
+    using C = cplx_t<T>;
+    using S = FftShape<T, L, THREADS, SMALL>;
+    constexpr int R0 = S::R0, TPC = S::TPC, CT = S::CT;
+    const int tc = threadIdx.x / CT;
+    const int cl = threadIdx.x - tc * CT;
+    const long long g = tile * CT + cl;
+    const bool valid = g < total_cols;
+    const int ccols = (MODE == FFT_C2C) ? a.ncols : (a.ncols + 1) >> 1;
+    const long long gg = valid ? g : 0;
+    const int b = (int)(gg / ccols);
+    const int c = (int)(gg - (long long)b * ccols);
+    const long long in_base = a.in_boff ? a.in_boff[b] : (long long)b * a.in_batch;
+    if constexpr (MODE == FFT_C2C) {
+        const C* in = static_cast<const C*>(a.in) + in_base;
+        C* st = reinterpret_cast<C*>(stage);
+#pragma unroll
+        for (int r = 0; r < R0; ++r) {
+            const long long row = tc + r * TPC;
+            cp_async_elem<sizeof(C)>(&st[row * CT + cl], valid ? &in[row * a.in_row + c] : a.in, valid);
+        }
+    } else if constexpr (MODE == FFT_R2C) {
+        const TIO* in = static_cast<const TIO*>(a.in) + in_base;
+        TIO* st = reinterpret_cast<TIO*>(stage);
+        const int c0 = 2 * c, c1 = 2 * c + 1;
+        const bool v1 = valid && c1 < a.ncols;
+#pragma unroll
+        for (int r = 0; r < R0; ++r) {
+            const long long row = tc + r * TPC;
+            cp_async_elem<sizeof(TIO)>(&st[(row * CT + cl) * 2], valid ? &in[row * a.in_row + c0] : a.in, valid);
+            cp_async_elem<sizeof(TIO)>(&st[(row * CT + cl) * 2 + 1], v1 ? &in[row * a.in_row + c1] : a.in, v1);
+        }
+    } else {  // C2R: A_k, B_k for k = 0 .. L/2
+        const C* in = static_cast<const C*>(a.in) + in_base;
+        C* st = reinterpret_cast<C*>(stage);
+        const int c0 = 2 * c, c1 = 2 * c + 1;
+        const bool v1 = valid && c1 < a.ncols;
+        for (int k = tc; k <= L / 2; k += TPC) {
+            cp_async_elem<sizeof(C)>(&st[((long long)k * CT + cl) * 2], valid ? &in[(long long)k * a.in_row + c0] : a.in,
+                                     valid);
+            cp_async_elem<sizeof(C)>(&st[((long long)k * CT + cl) * 2 + 1],
+                                     v1 ? &in[(long long)k * a.in_row + c1] : a.in, v1);
+        }
+    }
+}
+
+template <typename T, typename TIO, int L, int DIR, int MODE, int THREADS, int SMALL>
+__global__ void __launch_bounds__(THREADS) fft_pipe_kernel(FftArgs a, long long total_cols, long long ntiles)
+{
+    using C = cplx_t<T>;
+    using S = FftShape<T, L, THREADS, SMALL>;
+    using PS = PipeShape<T, TIO, L, THREADS, SMALL>;
+    constexpr int R0 = S::R0, R1 = S::R1, R2 = S::R2, NP = S::NP, TPC = S::TPC, CT = S::CT;
+    extern __shared__ __align__(16) unsigned char fft_smem[];
+    const C* tw = static_cast<const C*>(a.tw);
+    const int tc = threadIdx.x / CT;
+    const int cl = threadIdx.x - tc * CT;
+    const int ccols = (MODE == FFT_C2C) ? a.ncols : (a.ncols + 1) >> 1;
+
+    long long tile = blockIdx.x;
+    int cur = 0;
+    if (tile < ntiles) pipe_issue<T, TIO, L, MODE, THREADS, SMALL>(a, total_cols, tile, fft_smem);
+    cp_async_commit();
+    for (; tile < ntiles; tile += gridDim.x, cur ^= 1) {
+        unsigned char* buf = fft_smem + (size_t)cur * PS::buf;
+        const long long next = tile + gridDim.x;
+        if (next < ntiles) pipe_issue<T, TIO, L, MODE, THREADS, SMALL>(a, total_cols, next, fft_smem + (size_t)(cur ^ 1) * PS::buf);
+        cp_async_commit();
+        cp_async_wait_prev();
+        __syncthreads();
+
+        C* sm = reinterpret_cast<C*>(buf);
+        const long long g = tile * CT + cl;
+        const bool valid = g < total_cols;
+        const long long gg = valid ? g : 0;
+        const int b = (int)(gg / ccols);
+        const int c = (int)(gg - (long long)b * ccols);
+        const int c0 = 2 * c, c1 = 2 * c + 1;
+        const bool has1 = c1 < a.ncols;
+        const long long out_base = a.out_boff ? a.out_boff[b] : (long long)b * a.out_batch;
+
+        C v[R0];
+        // ------------------------------------------------ pass 0 input --
+        if constexpr (MODE == FFT_C2R) {
+            constexpr int KPT = (L / 2) / TPC + 1;  // half-spectrum rows per thread (upper bound)
+            C A[KPT], B[KPT];
+#pragma unroll
+            for (int j = 0; j < KPT; ++j) {
+                const int k = tc + j * TPC;
+                if (k <= L / 2) {
+                    A[j] = sm[((size_t)k * CT + cl) * 2];
+                    B[j] = sm[((size_t)k * CT + cl) * 2 + 1];
+                }
+            }
+            __syncthreads();
+#pragma unroll
+            for (int j = 0; j < KPT; ++j) {
+                const int k = tc + j * TPC;
+                if (k <= L / 2) {
+                    C Aj = A[j], Bj = B[j];
+                    if (k == 0 || k == L / 2) { Aj.y = 0; Bj.y = 0; }
+                    sm[k * CT + cl] = mk(Aj.x - Bj.y, Aj.y + Bj.x);
+                    if (k != 0 && k != L / 2) sm[(L - k) * CT + cl] = mk(Aj.x + Bj.y, Bj.x - Aj.y);
+                }
+            }
+            __syncthreads();
+#pragma unroll
+            for (int r = 0; r < R0; ++r) v[r] = sm[(tc + r * TPC) * CT + cl];
+            __syncthreads();
+        } else if constexpr (MODE == FFT_R2C) {
+            const TIO* st = reinterpret_cast<const TIO*>(buf);
+            int k0 = -1, k1 = -1, j0 = 0, j1 = 0;
+            if (a.P > 0) { k0 = c0 % a.P; j0 = c0 / a.P; k1 = c1 % a.P; j1 = c1 / a.P; }
+            const bool bnd0 = a.P > 0 && (k0 == 0 || k0 == a.P - 1);
+            const bool bnd1 = a.P > 0 && (k1 == 0 || k1 == a.P - 1);
+            const double* s0 = (k0 == 0) ? (b == a.gl_batch ? a.gl : nullptr) : (b == a.gr_batch ? a.gr : nullptr);
+            const double* s1 = (k1 == 0) ? (b == a.gl_batch ? a.gl : nullptr) : (b == a.gr_batch ? a.gr : nullptr);
+#pragma unroll
+            for (int r = 0; r < R0; ++r) {
+                const long long row = tc + r * TPC;
+                const TIO i0 = st[(row * CT + cl) * 2], i1 = st[(row * CT + cl) * 2 + 1];
+                T x0 = (T)i0, x1 = (T)i1;
+                if (bnd0) {
+                    if (a.bc_add) {
+                        double vv = (double)i0;
+                        if (s0) vv += (k0 == 0 ? a.bc_scale_l : a.bc_scale_r) * s0[row * a.bc_row + j0];
+                        x0 = (T)vv;
+                    } else {
+                        x0 = s0 ? (T)s0[row * a.bc_row + j0] : (T)0;
+                    }
+                }
+                if (has1 && bnd1) {
+                    if (a.bc_add) {
+                        double vv = (double)i1;
+                        if (s1) vv += (k1 == 0 ? a.bc_scale_l : a.bc_scale_r) * s1[row * a.bc_row + j1];
+                        x1 = (T)vv;
+                    } else {
+                        x1 = s1 ? (T)s1[row * a.bc_row + j1] : (T)0;
+                    }
+                }
+                if (!valid) { x0 = 0; x1 = 0; }
+                v[r] = mk(x0, x1);
+            }
+            __syncthreads();  // the stage is the exchange buffer from here on
+        } else {
+#pragma unroll
+            for (int r = 0; r < R0; ++r) v[r] = sm[(tc + r * TPC) * CT + cl];
+            __syncthreads();
+        }
+        dft_reg<R0, DIR, T>(v);
+
+        // ------------------------------------------------ later passes --
+        if constexpr (NP >= 2) {
+            pass_to_smem<T, L, R0, 1, TPC, CT, R0>(sm, tc, cl, v);
+            __syncthreads();
+            pass_from_smem<T, L, R1, R0, DIR, TPC, CT, R0>(sm, tw, tc, cl, v);
+        }
+        if constexpr (NP >= 3) {
+            __syncthreads();
+            pass_to_smem<T, L, R1, R0, TPC, CT, R0>(sm, tc, cl, v);
+            __syncthreads();
+            pass_from_smem<T, L, R2, R0 * R1, DIR, TPC, CT, R0>(sm, tw, tc, cl, v);
+        }
+        constexpr int RL = (NP == 1) ? R0 : (NP == 2 ? R1 : R2);
+        constexpr int NSL = L / RL;
+
+        // ------------------------------------------------------ output --
+        const T sc = (T)a.scale;
+        if constexpr (MODE == FFT_C2C) {
+            if (valid) {
+                C* out = static_cast<C*>(a.out) + out_base;
+#pragma unroll
+                for (int t = 0; t < R0 / RL; ++t)
+#pragma unroll
+                    for (int r = 0; r < RL; ++r) {
+                        const int row = pass_out_row<RL, NSL, TPC>(tc, t, r);
+                        out[(long long)row * a.out_row + c] = cscale(v[t * RL + r], sc);
+                    }
+            }
+        } else if constexpr (MODE == FFT_C2R) {
+            if (valid) {
+                TIO* out = static_cast<TIO*>(a.out) + out_base;
+#pragma unroll
+                for (int t = 0; t < R0 / RL; ++t)
+#pragma unroll
+                    for (int r = 0; r < RL; ++r) {
+                        const long long row = pass_out_row<RL, NSL, TPC>(tc, t, r);
+                        out[row * a.out_row + c0] = (TIO)(v[t * RL + r].x * sc);
+                        if (has1) out[row * a.out_row + c1] = (TIO)(v[t * RL + r].y * sc);
+                    }
+            }
+        } else {
+            __syncthreads();
+            pass_to_smem<T, L, RL, NSL, TPC, CT, R0>(sm, tc, cl, v);
+            __syncthreads();
+            if (valid) {
+                C* out = static_cast<C*>(a.out) + out_base;
+                const T h = (T)0.5 * sc;
+                for (int k = tc; k <= L / 2; k += TPC) {
+                    const C Z = sm[k * CT + cl];
+                    const C Zm = sm[((L - k) & (L - 1)) * CT + cl];
+                    out[(long long)k * a.out_row + c0] = mk((Z.x + Zm.x) * h, (Z.y - Zm.y) * h);
+                    if (has1) out[(long long)k * a.out_row + c1] = mk((Z.y + Zm.y) * h, (Zm.x - Z.x) * h);
+                }
+            }
+        }
+        __syncthreads();  // this buffer is refilled two tiles later
+    }
+    asm volatile("cp.async.wait_all;\n" ::);
+}
+
+template <typename T, typename TIO, int L, int DIR, int MODE, int THREADS, int SMALL>
+static int run_fft_pipe(const FftArgs& a, long long total_cols, cudaStream_t s)
+{
+    using S = FftShape<T, L, THREADS, SMALL>;
+    using PS = PipeShape<T, TIO, L, THREADS, SMALL>;
+    auto k = fft_pipe_kernel<T, TIO, L, DIR, MODE, THREADS, SMALL>;
+    if (PS::smem > kMaxSmemPerBlock) return (int)cudaErrorInvalidValue;
+    cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)PS::smem);
+    if (e != cudaSuccess) return (int)e;
+    const long long tiles = (total_cols + S::CT - 1) / S::CT;
+    if (tiles <= 0) return 0;
+    int dev = 0, sms = 148, per = 1;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k, THREADS, PS::smem);
+    if (per < 1) per = 1;
+    long long grid = (long long)sms * per;
+    if (grid > tiles) grid = tiles;
+    k<<<(unsigned)grid, THREADS, PS::smem, s>>>(a, total_cols, tiles);
+    return (int)cudaGetLastError();
+}
+
 template <typename T, typename TIO, int L, int DIR, int MODE, int THREADS, int SMALL>
 static int run_fft(const FftArgs& a, long long total_cols, cudaStream_t s)
 {
@@ -231,8 +491,15 @@ static int run_fft(const FftArgs& a, long long total_cols, cudaStream_t s)
 }
 
 template <typename T, typename TIO, int L, int THREADS, int SMALL>
-static int fft_dispatch_mode(int mode, int dir, const FftArgs& a, long long tc, cudaStream_t s)
+static int fft_dispatch_mode(int mode, int dir, const FftArgs& a, long long tc, cudaStream_t s, bool pipe)
 {
+    if (pipe) {
+        if (mode == FFT_C2C)
+            return dir < 0 ? run_fft_pipe<T, T, L, -1, FFT_C2C, THREADS, SMALL>(a, tc, s)
+                           : run_fft_pipe<T, T, L, 1, FFT_C2C, THREADS, SMALL>(a, tc, s);
+        if (mode == FFT_R2C) return run_fft_pipe<T, TIO, L, -1, FFT_R2C, THREADS, SMALL>(a, tc, s);
+        return run_fft_pipe<T, TIO, L, 1, FFT_C2R, THREADS, SMALL>(a, tc, s);
+    }
     if (mode == FFT_C2C)
         return dir < 0 ? run_fft<T, T, L, -1, FFT_C2C, THREADS, SMALL>(a, tc, s)
                        : run_fft<T, T, L, 1, FFT_C2C, THREADS, SMALL>(a, tc, s);
@@ -241,19 +508,21 @@ static int fft_dispatch_mode(int mode, int dir, const FftArgs& a, long long tc, 
 }
 
 // Launch variants the autotuner chooses from: bit 0 -> 128-thread CTAs (half the
-// columns per tile), bit 1 -> radix-8 schedule (lengths 128 and 256).
+// columns per tile), bit 1 -> radix-8 schedule (lengths 128 and 256), bit 2 ->
+// the persistent pipelined kernel.
 template <typename T, typename TIO, int L>
 static int fft_dispatch_variant(int variant, int mode, int dir, const FftArgs& a, long long tc, cudaStream_t s)
 {
     const bool small_cta = (variant & 1) && (L / Radix<L>::r0 <= 128);
+    const bool pipe = (variant & 4) != 0;
     if constexpr (has_small_radix<L>()) {
         if (variant & 2) {
-            if (small_cta) return fft_dispatch_mode<T, TIO, L, 128, 1>(mode, dir, a, tc, s);
-            return fft_dispatch_mode<T, TIO, L, 256, 1>(mode, dir, a, tc, s);
+            if (small_cta) return fft_dispatch_mode<T, TIO, L, 128, 1>(mode, dir, a, tc, s, pipe);
+            return fft_dispatch_mode<T, TIO, L, 256, 1>(mode, dir, a, tc, s, pipe);
         }
     }
-    if (small_cta) return fft_dispatch_mode<T, TIO, L, 128, 0>(mode, dir, a, tc, s);
-    return fft_dispatch_mode<T, TIO, L, 256, 0>(mode, dir, a, tc, s);
+    if (small_cta) return fft_dispatch_mode<T, TIO, L, 128, 0>(mode, dir, a, tc, s, pipe);
+    return fft_dispatch_mode<T, TIO, L, 256, 0>(mode, dir, a, tc, s, pipe);
 }
 
 template <typename T, typename TIO>
@@ -835,13 +1104,242 @@ __global__ void __launch_bounds__(128) thomas_kernel(ThomasArgs a)
     }
 }
 
-int launch_thomas(int prec, const ThomasArgs& a, cudaStream_t s)
+// The same tridiagonal solves, one warp per spectrum row (Nz <= 32 M).  Lane p
+// owns rows z = p M .. p M + M - 1 (rows beyond Nz are identity rows).  The row
+// is read once and written once, both coalesced through a per-warp shared
+// buffer; no elimination coefficients go to memory:
+//   1. each lane eliminates its interior rows (a Thomas solve of size M - 2
+//      with three right-hand sides), leaving two equations that couple its
+//      first and last unknowns to the neighbouring lanes' last and first ones;
+//   2. the 64 reduced equations (a tridiagonal system in the order first_0,
+//      last_0, first_1, ...) are solved by parallel cyclic reduction over warp
+//      shuffles, six steps;
+//   3. each lane recovers its interior unknowns from its first and last.
+// The matrix is diagonally dominant (|diag| >= 2 cz1 + lambda + mx + my), so
+// neither elimination pivots.
+template <typename T>
+struct TriEq {
+    T a, b, c;
+    cplx_t<T> d;
+};
+
+template <typename T>
+__device__ __forceinline__ TriEq<T> tri_shfl_up(const TriEq<T>& e, int k)
 {
+    TriEq<T> o;
+    o.a = __shfl_up_sync(0xffffffffu, e.a, k);
+    o.b = __shfl_up_sync(0xffffffffu, e.b, k);
+    o.c = __shfl_up_sync(0xffffffffu, e.c, k);
+    o.d.x = __shfl_up_sync(0xffffffffu, e.d.x, k);
+    o.d.y = __shfl_up_sync(0xffffffffu, e.d.y, k);
+    return o;
+}
+template <typename T>
+__device__ __forceinline__ TriEq<T> tri_shfl_down(const TriEq<T>& e, int k)
+{
+    TriEq<T> o;
+    o.a = __shfl_down_sync(0xffffffffu, e.a, k);
+    o.b = __shfl_down_sync(0xffffffffu, e.b, k);
+    o.c = __shfl_down_sync(0xffffffffu, e.c, k);
+    o.d.x = __shfl_down_sync(0xffffffffu, e.d.x, k);
+    o.d.y = __shfl_down_sync(0xffffffffu, e.d.y, k);
+    return o;
+}
+// One cyclic-reduction update of equation e with its neighbours lo (index - s)
+// and hi (index + s), whose b fields hold the reciprocal of their diagonal.
+template <typename T>
+__device__ __forceinline__ TriEq<T> tri_reduce(const TriEq<T>& e, const TriEq<T>& lo, const TriEq<T>& hi)
+{
+    const T k1 = e.a * lo.b, k2 = e.c * hi.b;
+    TriEq<T> o;
+    o.a = -lo.a * k1;
+    o.c = -hi.c * k2;
+    o.b = e.b - lo.c * k1 - hi.a * k2;
+    o.d = mk(e.d.x - lo.d.x * k1 - hi.d.x * k2, e.d.y - lo.d.y * k1 - hi.d.y * k2);
+    return o;
+}
+
+constexpr int TRI_WARPS = 4;
+
+// Copies row r of the spectrum into the lane-chunked buffer sb (asynchronous,
+// coalesced: step j moves elements 32 j .. 32 j + 31); elements >= Nz read 0.
+template <typename T, int M>
+__device__ __forceinline__ void tri_issue_row(const ThomasArgs& a, long long r, cplx_t<T>* sb, int lane)
+{
+    using C = cplx_t<T>;
+    const C* x = static_cast<const C*>(a.spec) + r * a.Nz;
+#pragma unroll
+    for (int j = 0; j < M; ++j) {
+        const int e = j * 32 + lane;
+        const bool ok = e < a.Nz;
+        cp_async_elem<sizeof(C)>(&sb[(e / M) * (M + 1) + e % M], ok ? (const void*)&x[e] : a.spec, ok);
+    }
+}
+
+template <typename T, int M>
+__global__ void __launch_bounds__(TRI_WARPS * 32, (M <= 8 ? 4 : 2)) thomas_warp_kernel(ThomasArgs a)
+{
+    using C = cplx_t<T>;
+    extern __shared__ __align__(16) unsigned char tri_smem[];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    C* bufs = reinterpret_cast<C*>(tri_smem) + (size_t)warp * 2 * 32 * (M + 1);
+    const int Nz = a.Nz;
+    const T cz = (T)a.cz1;
+    const TriEq<T> ident{(T)0, (T)1, (T)0, mk((T)0, (T)0)};
+    const long long stride = (long long)gridDim.x * TRI_WARPS;
+    long long r = (long long)blockIdx.x * TRI_WARPS + warp;
+    int cur = 0;
+    if (r < a.nrows) tri_issue_row<T, M>(a, r, bufs, lane);
+    cp_async_commit();
+    for (; r < a.nrows; r += stride, cur ^= 1) {
+        C* sb = bufs + (size_t)cur * 32 * (M + 1);
+        if (r + stride < a.nrows) tri_issue_row<T, M>(a, r + stride, bufs + (size_t)(cur ^ 1) * 32 * (M + 1), lane);
+        cp_async_commit();
+        cp_async_wait_prev();
+        __syncwarp();
+        C* x = static_cast<C*>(a.spec) + r * Nz;
+        const int kx = (int)(r / a.Ny), ky = (int)(r - (long long)kx * a.Ny);
+        const double dg = -2.0 * a.cz1 - a.lambda - a.mx[kx] - a.my[ky];
+        C dv[M];
+#pragma unroll
+        for (int i = 0; i < M; ++i) dv[i] = sb[lane * (M + 1) + i];
+        // row k: sub (k >= 1), diagonal, super (k <= Nz - 2); transposed, the sub of
+        // row k is the super of row k - 1 and the super of row k the sub of row k + 1.
+        // Rows k >= Nz are identity rows.
+        auto sub = [&](int k) -> T {
+            if (k == 0 || k >= Nz) return (T)0;
+            if (!a.transpose) return (k == Nz - 1) ? (T)a.s_last : cz;
+            return (k == 1) ? (T)a.s_first : cz;
+        };
+        auto sup = [&](int k) -> T {
+            if (k >= Nz - 1) return (T)0;
+            if (!a.transpose) return (k == 0) ? (T)a.s_first : cz;
+            return (k + 2 == Nz) ? (T)a.s_last : cz;
+        };
+        auto dia = [&](int k) -> T {
+            if (k >= Nz) return (T)1;
+            double b = dg;
+            if (k == 0) b += a.d_first;
+            if (k == Nz - 1) b += a.d_last;
+            return (T)b;
+        };
+        const int k0 = lane * M;
+        // ---- 1. eliminate the lane's interior rows ----
+        TriEq<T> e0, e1;
+        C y[M > 2 ? M - 2 : 1];
+        T v[M > 2 ? M - 2 : 1], w[M > 2 ? M - 2 : 1];
+        if constexpr (M == 2) {
+            e0 = TriEq<T>{sub(k0), dia(k0), sup(k0), dv[0]};
+            e1 = TriEq<T>{sub(k0 + 1), dia(k0 + 1), sup(k0 + 1), dv[1]};
+        } else {
+            constexpr int NI = M - 2;
+            T cp[NI];
+#pragma unroll
+            for (int j = 0; j < NI; ++j) {
+                const int k = k0 + j + 1;
+                const T al = (j > 0) ? sub(k) : (T)0;
+                const T den = (j > 0) ? dia(k) - al * cp[j - 1] : dia(k);
+                const T m = (T)1 / den;
+                cp[j] = (j < NI - 1) ? sup(k) * m : (T)0;
+                const C yp = (j > 0) ? y[j - 1] : mk((T)0, (T)0);
+                y[j] = mk((dv[j + 1].x - al * yp.x) * m, (dv[j + 1].y - al * yp.y) * m);
+                v[j] = (((j == 0) ? sub(k) : (T)0) - ((j > 0) ? al * v[j - 1] : (T)0)) * m;
+                w[j] = (((j == NI - 1) ? sup(k) : (T)0) - ((j > 0) ? al * w[j - 1] : (T)0)) * m;
+            }
+#pragma unroll
+            for (int j = NI - 2; j >= 0; --j) {
+                y[j] = mk(y[j].x - cp[j] * y[j + 1].x, y[j].y - cp[j] * y[j + 1].y);
+                v[j] -= cp[j] * v[j + 1];
+                w[j] -= cp[j] * w[j + 1];
+            }
+            const T c0 = sup(k0), aM = sub(k0 + M - 1);
+            e0 = TriEq<T>{sub(k0), dia(k0) - c0 * v[0], -c0 * w[0],
+                          mk(dv[0].x - c0 * y[0].x, dv[0].y - c0 * y[0].y)};
+            e1 = TriEq<T>{-aM * v[NI - 1], dia(k0 + M - 1) - aM * w[NI - 1], sup(k0 + M - 1),
+                          mk(dv[M - 1].x - aM * y[NI - 1].x, dv[M - 1].y - aM * y[NI - 1].y)};
+        }
+        // ---- 2. cyclic reduction of the 64 reduced equations (2 lane, 2 lane + 1) ----
+        {
+            // stride 1: e0's lower neighbour is lane - 1's e1, e1's upper one lane + 1's e0
+            const TriEq<T> r0{e0.a, (T)1 / e0.b, e0.c, e0.d}, r1{e1.a, (T)1 / e1.b, e1.c, e1.d};
+            TriEq<T> lo = tri_shfl_up(r1, 1), hi = tri_shfl_down(r0, 1);
+            if (lane == 0) lo = ident;
+            if (lane == 31) hi = ident;
+            const TriEq<T> n0 = tri_reduce(e0, lo, r1);
+            const TriEq<T> n1 = tri_reduce(e1, r0, hi);
+            e0 = n0;
+            e1 = n1;
+        }
+#pragma unroll
+        for (int k = 1; k < 32; k <<= 1) {  // strides 2, 4, .., 32 of the reduced index
+            const TriEq<T> r0{e0.a, (T)1 / e0.b, e0.c, e0.d}, r1{e1.a, (T)1 / e1.b, e1.c, e1.d};
+            TriEq<T> l0 = tri_shfl_up(r0, k), h0 = tri_shfl_down(r0, k);
+            TriEq<T> l1 = tri_shfl_up(r1, k), h1 = tri_shfl_down(r1, k);
+            if (lane < k) { l0 = ident; l1 = ident; }
+            if (lane + k > 31) { h0 = ident; h1 = ident; }
+            const TriEq<T> n0 = tri_reduce(e0, l0, h0);
+            const TriEq<T> n1 = tri_reduce(e1, l1, h1);
+            e0 = n0;
+            e1 = n1;
+        }
+        const C xs = mk(e0.d.x / e0.b, e0.d.y / e0.b);
+        const C xe = mk(e1.d.x / e1.b, e1.d.y / e1.b);
+        // ---- 3. interior unknowns, coalesced store ----
+        __syncwarp();
+        sb[lane * (M + 1)] = xs;
+        sb[lane * (M + 1) + M - 1] = xe;
+        if constexpr (M > 2) {
+#pragma unroll
+            for (int j = 0; j < M - 2; ++j)
+                sb[lane * (M + 1) + j + 1] =
+                    mk(y[j].x - xs.x * v[j] - xe.x * w[j], y[j].y - xs.y * v[j] - xe.y * w[j]);
+        }
+        __syncwarp();
+#pragma unroll
+        for (int j = 0; j < M; ++j) {
+            const int e = j * 32 + lane;
+            if (e < Nz) x[e] = sb[(e / M) * (M + 1) + e % M];
+        }
+        __syncwarp();  // sb is refilled by the copy issued in the next iteration
+    }
+    asm volatile("cp.async.wait_all;\n" ::);
+}
+
+template <typename T, int M>
+static int run_thomas_warp(const ThomasArgs& a, cudaStream_t s)
+{
+    auto k = thomas_warp_kernel<T, M>;
+    const size_t smem = (size_t)TRI_WARPS * 2 * 32 * (M + 1) * sizeof(cplx_t<T>);
+    cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return (int)e;
+    int dev = 0, sms = 148, per = 1;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k, TRI_WARPS * 32, smem);
+    if (per < 1) per = 1;
+    long long grid = (a.nrows + TRI_WARPS - 1) / TRI_WARPS;
+    if (grid > (long long)sms * per) grid = (long long)sms * per;
+    if (grid <= 0) return 0;
+    k<<<(unsigned)grid, TRI_WARPS * 32, smem, s>>>(a);
+    return (int)cudaGetLastError();
+}
+
+template <typename T>
+static int thomas_dispatch(const ThomasArgs& a, cudaStream_t s)
+{
+    if (a.Nz <= 64) return run_thomas_warp<T, 2>(a, s);
+    if (a.Nz <= 128) return run_thomas_warp<T, 4>(a, s);
+    if (a.Nz <= 256) return run_thomas_warp<T, 8>(a, s);
+    if (a.Nz <= 512) return run_thomas_warp<T, 16>(a, s);
     const long long blocks = (a.nrows + 127) / 128;
     if (blocks <= 0) return 0;
-    if (prec == 1) thomas_kernel<float><<<(unsigned)blocks, 128, 0, s>>>(a);
-    else thomas_kernel<double><<<(unsigned)blocks, 128, 0, s>>>(a);
+    thomas_kernel<T><<<(unsigned)blocks, 128, 0, s>>>(a);
     return (int)cudaGetLastError();
+}
+
+int launch_thomas(int prec, const ThomasArgs& a, cudaStream_t s)
+{
+    return prec == 1 ? thomas_dispatch<float>(a, s) : thomas_dispatch<double>(a, s);
 }
 
 size_t rows_smem_bytes(int method, int prec, int n, int ld)

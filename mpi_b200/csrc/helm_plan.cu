@@ -328,6 +328,10 @@ static int setup_fast(Plan& p, const std::vector<double>& A0, int prec_code)
         if ((st = p.upload((void**)&p.d_fmma, sw.data(), sw.size() * sizeof(double)))) return st;
         fdm_mma_swizzle(fa.data(), ld, sw.data());
         if ((st = p.upload((void**)&p.d_fmma_adj, sw.data(), sw.size() * sizeof(double)))) return st;
+        fdm_mma16_swizzle(fw.data(), ld, sw.data());
+        if ((st = p.upload((void**)&p.d_fmma16, sw.data(), sw.size() * sizeof(double)))) return st;
+        fdm_mma16_swizzle(fa.data(), ld, sw.data());
+        if ((st = p.upload((void**)&p.d_fmma16_adj, sw.data(), sw.size() * sizeof(double)))) return st;
     }
     if ((st = up_t(recip, &p.d_frecip))) return st;
     if ((st = p.upload((void**)&p.d_fd2, d2f.data(), d2f.size() * sizeof(double)))) return st;
@@ -666,6 +670,7 @@ static int run_pipeline(Plan& p, const void* in, const double* gl, const double*
         fa.br = p.bc.betar;
         fa.adjoint = adjoint ? 1 : 0;
         fa.mma_mats = adjoint ? p.d_fmma_adj : p.d_fmma;
+        fa.mma16_mats = adjoint ? p.d_fmma16_adj : p.d_fmma16;
         if (prec == 0 && fa.mma_mats)
             e = launch_fdm_mma(fa, s, p.row_var);
         else
@@ -729,10 +734,10 @@ static int autotune(Plan& p)
         for (cudaEvent_t& e : p.ev) cudaEventCreate(&e);
     p.stage_timing = true;
     // stages: x, y, rows, inverse y, inverse x (event intervals 0..4); the
-    // FFT stages try variants 0..3, the row stage its variants 0..1
+    // FFT stages try variants 0..7, the row stage its variants 0..1
     float best[5] = {1e30f, 1e30f, 1e30f, 1e30f, 1e30f};
     int pick[5] = {0, 0, 0, 0, 0};
-    for (int v = 0; v < 4; ++v) {
+    for (int v = 0; v < 8; ++v) {
         for (int i = 0; i < 4; ++i) p.fft_var[i] = v;
         p.row_var = v & 1;
         float acc[5] = {0, 0, 0, 0, 0};
@@ -1103,6 +1108,27 @@ int helm_plan_stage_times(helm_plan_t plan, float* ms5)
         if (err != cudaSuccess) return helm::set_cuda_error(err, "cudaEventElapsedTime");
         ms5[i] = t;
     }
+    return HELM_OK;
+}
+
+int helm_plan_get_launch_variants(helm_plan_t plan, int* fft4, int* rows)
+{
+    if (!plan) return HELM_ERR_INVALID;
+    const Plan& p = *reinterpret_cast<const Plan*>(plan);
+    if (fft4)
+        for (int i = 0; i < 4; ++i) fft4[i] = p.fft_var[i];
+    if (rows) *rows = p.row_var;
+    return HELM_OK;
+}
+
+int helm_plan_set_launch_variants(helm_plan_t plan, const int* fft4, int rows)
+{
+    if (!plan || !fft4 || rows < 0 || rows > 1) return HELM_ERR_INVALID;
+    for (int i = 0; i < 4; ++i)
+        if (fft4[i] < 0 || fft4[i] > 7) return HELM_ERR_INVALID;
+    Plan& p = *reinterpret_cast<Plan*>(plan);
+    for (int i = 0; i < 4; ++i) p.fft_var[i] = fft4[i];
+    p.row_var = rows;
     return HELM_OK;
 }
 

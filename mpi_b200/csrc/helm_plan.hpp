@@ -64,6 +64,8 @@ struct Plan {
     void* d_fmats_adj = nullptr;   // transposed transforms
     double* d_fmma = nullptr;      // FP64 plans: the transforms in tensor-core fragment order
     double* d_fmma_adj = nullptr;
+    double* d_fmma16 = nullptr;    // the same in m16n8k8 fragment order
+    double* d_fmma16_adj = nullptr;
     double* d_fd2 = nullptr;       // folded D2int blocks (refinement)
     double* d_fd2_adj = nullptr;   // their transposes
     void* d_frecip = nullptr;      // [G][2][fld] reciprocal shifts

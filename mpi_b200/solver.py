@@ -146,6 +146,19 @@ class _PlanBase:
         L.check(self._lib.helm_plan_stage_times(self._plan, buf), "helm_plan_stage_times")
         return dict(zip(self.STAGES, [float(v) for v in buf]))
 
+    def launch_variants(self) -> dict:
+        """The autotuned (or pinned) kernel variants: FFT passes (x, y,
+        inverse y, inverse x) and the row solve."""
+        f4 = (ctypes.c_int * 4)()
+        rv = ctypes.c_int()
+        L.check(self._lib.helm_plan_get_launch_variants(self._plan, f4, ctypes.byref(rv)),
+                "helm_plan_get_launch_variants")
+        return {"fft": list(f4), "rows": rv.value}
+
+    def set_launch_variants(self, fft: Sequence[int], rows: int) -> None:
+        f4 = (ctypes.c_int * 4)(*fft)
+        L.check(self._lib.helm_plan_set_launch_variants(self._plan, f4, int(rows)), "helm_plan_set_launch_variants")
+
     def DestroyPDEPlan(self) -> None:
         if self._plan.value:
             self._lib.helm_plan_destroy(self._plan)
