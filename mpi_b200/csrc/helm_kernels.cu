@@ -75,6 +75,43 @@ __device__ __forceinline__ void pass_to_smem(cplx_t<T>* sm, int tc, int cl, cons
         for (int r = 0; r < R; ++r) sm[pass_out_row<R, NS, TPC>(tc, t, r) * CT + cl] = v[t * R + r];
 }
 
+// One real output value of a C2R pass at (row, column c) of the output tile;
+// in an adjoint pass (a.adj_mode) it is also split into the boundary
+// cotangents and accumulated into the lambda sum.
+template <typename TIO>
+__device__ __forceinline__ void c2r_put(const FftArgs& a, TIO* out, long long out_base, long long row, int c,
+                                        double v, double& acc)
+{
+    const long long idx = row * a.out_row + c;
+    if (a.adj_mode) {
+        const int k = c % a.adj_P, j = c / a.adj_P;
+        const bool first = k == 0, last = k == a.adj_P - 1;
+        if (first && a.gbar_l) a.gbar_l[row * a.bc_row + j] = a.adj_scale_l * v;
+        if (last && a.gbar_r) a.gbar_r[row * a.bc_row + j] = a.adj_scale_r * v;
+        if (a.adj_mode == 1 && (first || last)) {
+            out[idx] = (TIO)0;
+            return;
+        }
+        if (a.lam_u) acc += v * a.lam_u[out_base + idx];
+    }
+    out[idx] = (TIO)v;
+}
+
+// Adds every thread's acc into *a.lam_out (one atomic per CTA); all threads call.
+__device__ __forceinline__ void c2r_lambda_sum(const FftArgs& a, double acc)
+{
+    __shared__ double red[32];
+    for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+    __syncthreads();
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = acc;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double sum = 0.0;
+        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) sum += red[w];
+        atomicAdd(a.lam_out, sum);
+    }
+}
+
 template <typename T, typename TIO, int L, int DIR, int MODE, int THREADS, int SMALL>
 __global__ void __launch_bounds__(THREADS) fft_kernel(FftArgs a, long long total_cols)
 {
@@ -189,6 +226,7 @@ __global__ void __launch_bounds__(THREADS) fft_kernel(FftArgs a, long long total
                 }
         }
     } else if constexpr (MODE == FFT_C2R) {
+        double acc = 0.0;
         if (valid) {
             TIO* out = static_cast<TIO*>(a.out) + out_base;
 #pragma unroll
@@ -196,10 +234,11 @@ __global__ void __launch_bounds__(THREADS) fft_kernel(FftArgs a, long long total
 #pragma unroll
                 for (int r = 0; r < RL; ++r) {
                     const long long row = pass_out_row<RL, NSL, TPC>(tc, t, r);
-                    out[row * a.out_row + c0] = (TIO)(v[t * RL + r].x * sc);
-                    if (has1) out[row * a.out_row + c1] = (TIO)(v[t * RL + r].y * sc);
+                    c2r_put(a, out, out_base, row, c0, (double)(v[t * RL + r].x * sc), acc);
+                    if (has1) c2r_put(a, out, out_base, row, c1, (double)(v[t * RL + r].y * sc), acc);
                 }
         }
+        if (a.lam_out) c2r_lambda_sum(a, acc);
     } else {  // R2C: separate the two real columns' spectra, keep k = 0 .. L/2
         __syncthreads();
         pass_to_smem<T, L, RL, NSL, TPC, CT, R0>(sm, tc, cl, v);
@@ -305,6 +344,7 @@ __global__ void __launch_bounds__(THREADS) fft_pipe_kernel(FftArgs a, long long 
 
     long long tile = blockIdx.x;
     int cur = 0;
+    double lam_acc = 0.0;  // adjoint C2R: this thread's share of the lambda sum
     if (tile < ntiles) pipe_issue<T, TIO, L, MODE, THREADS, SMALL>(a, total_cols, tile, fft_smem);
     cp_async_commit();
     for (; tile < ntiles; tile += gridDim.x, cur ^= 1) {
@@ -431,8 +471,8 @@ __global__ void __launch_bounds__(THREADS) fft_pipe_kernel(FftArgs a, long long 
 #pragma unroll
                     for (int r = 0; r < RL; ++r) {
                         const long long row = pass_out_row<RL, NSL, TPC>(tc, t, r);
-                        out[row * a.out_row + c0] = (TIO)(v[t * RL + r].x * sc);
-                        if (has1) out[row * a.out_row + c1] = (TIO)(v[t * RL + r].y * sc);
+                        c2r_put(a, out, out_base, row, c0, (double)(v[t * RL + r].x * sc), lam_acc);
+                        if (has1) c2r_put(a, out, out_base, row, c1, (double)(v[t * RL + r].y * sc), lam_acc);
                     }
             }
         } else {
@@ -453,6 +493,8 @@ __global__ void __launch_bounds__(THREADS) fft_pipe_kernel(FftArgs a, long long 
         __syncthreads();  // this buffer is refilled two tiles later
     }
     asm volatile("cp.async.wait_all;\n" ::);
+    if constexpr (MODE == FFT_C2R)
+        if (a.lam_out) c2r_lambda_sum(a, lam_acc);
 }
 
 template <typename T, typename TIO, int L, int DIR, int MODE, int THREADS, int SMALL>
@@ -991,60 +1033,6 @@ static int rows_dispatch_prec(int method, int prec, const RowArgs& a, cudaStream
     if (prec == 0) return run_rows<double, double, NSLOT, 2, false>(a, s);
     if (prec == 1) return run_rows<float, float, NSLOT, 2, false>(a, s);
     return run_rows<double, float, NSLOT, 2, true>(a, s);
-}
-
-// Adjoint output split.  The adjoint pipeline leaves v = A^-T ubar in fbar in
-// every slot of the GLL (or z) direction.  One warp per (x, y) column.
-//   GLL plans: slot 0 / P-1 are the boundary equations: they move to glbar /
-//   grbar (dL/dgl, dL/dgr) and are zeroed in fbar (f is never read there);
-//   lambda_bar += sum over the interior slots of fbar * u.
-//   FD plans: every slot is an interior equation; the boundary data entered the
-//   first / last equation with weights scale_l / scale_r, so dL/dg = scale * v
-//   there; lambda_bar sums over every slot.
-__global__ void __launch_bounds__(256) adjoint_finalize_kernel(double* fbar, double* glbar, double* grbar,
-                                                               const double* u, double* lambda_bar, int Nx, int Ny,
-                                                               int P, long long x_stride, long long bc_row, int fd,
-                                                               double scale_l, double scale_r)
-{
-    __shared__ double red[8];
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const long long ncol = (long long)Nx * Ny;
-    const long long nw = (long long)gridDim.x * 8;
-    double acc = 0.0;
-    for (long long c = (long long)blockIdx.x * 8 + warp; c < ncol; c += nw) {
-        const int i = (int)(c / Ny), j = (int)(c - (long long)(c / Ny) * Ny);
-        double* col = fbar + (long long)i * x_stride + (long long)j * P;
-        const double* uc = u ? u + (long long)i * x_stride + (long long)j * P : nullptr;
-        for (int k = lane; k < P; k += 32) {
-            const double v = col[k];
-            if (k == 0 && glbar) glbar[(long long)i * bc_row + j] = scale_l * v;
-            if (k == P - 1 && grbar) grbar[(long long)i * bc_row + j] = scale_r * v;
-            const bool bslot = (k == 0 || k == P - 1);
-            if (!fd && bslot) col[k] = 0.0;
-            else if (uc) acc += v * uc[k];
-        }
-    }
-    if (!lambda_bar) return;
-    acc = warp_sum(acc);
-    if (lane == 0) red[warp] = acc;
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        double s = 0.0;
-        for (int w = 0; w < 8; ++w) s += red[w];
-        atomicAdd(lambda_bar, s);
-    }
-}
-
-int launch_adjoint_finalize(double* fbar, double* glbar, double* grbar, const double* u, double* lambda_bar, int Nx,
-                            int Ny, int P, long long x_stride, long long bc_row, cudaStream_t s, int fd,
-                            double scale_l, double scale_r)
-{
-    const long long ncol = (long long)Nx * Ny;
-    long long blocks = (ncol + 7) / 8;
-    if (blocks > 148 * 16) blocks = 148 * 16;
-    adjoint_finalize_kernel<<<(unsigned)blocks, 256, 0, s>>>(fbar, glbar, grbar, u, lambda_bar, Nx, Ny, P, x_stride,
-                                                            bc_row, fd, scale_l, scale_r);
-    return (int)cudaGetLastError();
 }
 
 // Finite-difference variant (HypreFDM stencil, HelmholtzSolvers/HypreFDM/src/

@@ -37,6 +37,17 @@ struct FftArgs {
     // independent problems in a packed buffer); NULL: batch * *_batch
     const long long* in_boff;
     const long long* out_boff;
+    // C2R of the adjoint solve (adj_mode != 0): the output is fbar; its GLL
+    // boundary slots k = 0 / adj_P - 1 also go to gbar_l / gbar_r (times
+    // adj_scale_l / adj_scale_r, index row * bc_row + col / adj_P); mode 1 (GLL)
+    // stores 0 in those slots of fbar, mode 2 (finite differences) keeps them;
+    // lam_out += sum of fbar * lam_u over the slots fbar keeps (lam_u NULL: no sum)
+    int adj_mode, adj_P;
+    double adj_scale_l, adj_scale_r;
+    double* gbar_l;
+    double* gbar_r;
+    const double* lam_u;
+    double* lam_out;
 };
 
 // Finite-difference variant: one tridiagonal solve along z per spectrum row.
@@ -97,13 +108,6 @@ int launch_fft(int L, int mode, int dir, int t_double, int io_bytes, const FftAr
                cudaStream_t s, int variant = 0);
 // method: 1 = LU, 2 = FDM; prec: 0 = FP64, 1 = FP32, 2 = FP32 with FP64 refinement
 int launch_rows(int method, int prec, const RowArgs& a, cudaStream_t s);
-// Adjoint output split.  GLL plans (fd = 0): boundary slots -> glbar/grbar and
-// zeroed, lambda_bar over the interior slots.  FD plans (fd = 1): glbar/grbar =
-// scale_l/scale_r times the first/last slot, nothing zeroed, lambda_bar over
-// every slot.
-int launch_adjoint_finalize(double* fbar, double* glbar, double* grbar, const double* u, double* lambda_bar, int Nx,
-                            int Ny, int P, long long x_stride, long long bc_row, cudaStream_t s, int fd = 0,
-                            double scale_l = 1.0, double scale_r = 1.0);
 int launch_thomas(int prec, const ThomasArgs& a, cudaStream_t s);
 // Dynamic shared memory rows_kernel needs for this method / precision / size.
 size_t rows_smem_bytes(int method, int prec, int n, int ld);

@@ -523,11 +523,30 @@ static int setup_plan(Plan& p)
     return HELM_OK;
 }
 
+// Outputs of the adjoint solve that its last (C2R) pass writes besides fbar.
+struct AdjOut {
+    double* glbar;
+    double* grbar;
+    const double* u;       // forward solution (lambda sum), or NULL
+    double* lambda_bar;    // device scalar, zeroed before the pass, or NULL
+};
+
 static int fft_pass(Plan& p, int L, int mode, int dir, const void* in, void* out, long long in_row, long long out_row,
                     long long in_batch, long long out_batch, int ncols, int nbatch, double scale, const void* tw,
-                    const double* gl, const double* gr, bool inject, bool io_double, int stage, cudaStream_t s)
+                    const double* gl, const double* gr, bool inject, bool io_double, int stage, cudaStream_t s,
+                    const AdjOut* adj = nullptr)
 {
     FftArgs a{};
+    if (adj && mode == FFT_C2R) {
+        a.adj_mode = p.fd ? 2 : 1;
+        a.adj_P = p.N;
+        a.adj_scale_l = p.fd ? p.fd_scale_l : 1.0;
+        a.adj_scale_r = p.fd ? p.fd_scale_r : 1.0;
+        a.gbar_l = adj->glbar;
+        a.gbar_r = adj->grbar;
+        a.lam_u = adj->lambda_bar ? adj->u : nullptr;
+        a.lam_out = adj->lambda_bar;
+    }
     a.in = in;
     a.out = out;
     a.in_row = in_row;
@@ -562,7 +581,7 @@ static int fft_pass(Plan& p, int L, int mode, int dir, const void* in, void* out
 // GLL boundary slots of the spectrum, out = u.  Adjoint: in = ubar read in
 // every slot, the transposed row solve, out = A^-T ubar in every slot.
 static int run_pipeline(Plan& p, const void* in, const double* gl, const double* gr, void* out, bool adjoint,
-                        cudaStream_t s)
+                        cudaStream_t s, const AdjOut* adj = nullptr)
 {
     const int N = p.N;
     const long long cols = (long long)(p.dim == 3 ? p.Ny : 1) * N;  // real columns per x row
@@ -689,7 +708,7 @@ static int run_pipeline(Plan& p, const void* in, const double* gl, const double*
     // 5. x: complex-to-real, scaled by 1/(Nx Ny) (the reference's /Nx, /Ny)
     const double scale = 1.0 / ((double)p.Nx * (p.dim == 3 ? p.Ny : 1));
     if ((st = fft_pass(p, p.Nx, FFT_C2R, 1, p.d_spec, out, cols, p.x_stride, p.elem_spec, p.elem_stride, (int)cols,
-                       p.Ns * p.batch, scale, p.d_tw_x, nullptr, nullptr, false, adjoint, 3, s)))
+                       p.Ns * p.batch, scale, p.d_tw_x, nullptr, nullptr, false, adjoint, 3, s, adj)))
         return st;
     mark(5);
     return HELM_OK;
@@ -780,17 +799,17 @@ int solve_adjoint(Plan& p, const double* ubar, double* fbar, double* glbar, doub
         g_last_error = "adjoint needs a fast-diagonalisation plan with one GLL element";
         return HELM_ERR_UNSUPPORTED;
     }
-    int st = run_pipeline(p, ubar, nullptr, nullptr, fbar, true, s);
-    if (st) return st;
+    if (lambda_bar && !u) {
+        g_last_error = "lambda_bar needs the forward solution u";
+        return HELM_ERR_INVALID;
+    }
     if (lambda_bar) {
         cudaError_t e = cudaMemsetAsync(lambda_bar, 0, sizeof(double), s);
         if (e != cudaSuccess) return set_cuda_error(e, "cudaMemsetAsync");
     }
-    int e = launch_adjoint_finalize(fbar, glbar, grbar, lambda_bar ? u : nullptr, lambda_bar, p.Nx,
-                                    p.dim == 3 ? p.Ny : 1, p.N, p.x_stride, p.dim == 3 ? p.bc_x_stride : 1, s,
-                                    p.fd ? 1 : 0, p.fd ? p.fd_scale_l : 1.0, p.fd ? p.fd_scale_r : 1.0);
-    if (e) return set_cuda_error((cudaError_t)e, "adjoint finalize launch");
-    return HELM_OK;
+    // the last pass writes fbar, splits off glbar / grbar and sums fbar * u
+    const AdjOut adj{glbar, grbar, u, lambda_bar};
+    return run_pipeline(p, ubar, nullptr, nullptr, fbar, true, s, &adj);
 }
 
 // Finite-difference variant: the second-order stencil of HypreFDM
