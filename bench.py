@@ -362,7 +362,7 @@ def run_ours(args, ws, rank, local):
     if ws == 1 and not args.skip_side:
         st, wu = max(3, min(args.steps, 20)), 3
         side["batch"] = _leg_batch(dev, flush, stream, st, wu, cpu=not args.skip_cpu_baseline)
-        side["adjoint"] = _leg_adjoint(dev, flush, stream, st, wu)
+        side["adjoint"] = _leg_adjoint(dev, flush, stream, max(st, 50), wu)
         side["fd"] = _leg_fd(dev, flush, stream, st, wu)
     clk = clocks.stop()
 

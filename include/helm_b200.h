@@ -140,7 +140,7 @@ int helm_plan_get_grid(helm_plan_t plan, double* nodes, double* D, double* D2);
  * plan runs, and the device bytes it holds. */
 int helm_plan_info(helm_plan_t plan, int* Ns, int* n_operators, int* method, long long* device_bytes);
 
-/* Stage timing: when enabled, helm_solve records CUDA events on its stream
+/* Stage timing: when enabled, helm_solve and helm_solve_adjoint record CUDA events on their stream
  * around each of its kernels; helm_plan_stage_times then waits for the last
  * solve and returns the five stage durations in ms: x-FFT, y-FFT, row solves,
  * inverse y-FFT, inverse x-FFT (y stages are 0 in 2D).  The reference times

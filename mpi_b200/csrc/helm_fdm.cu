@@ -193,15 +193,18 @@ __device__ __forceinline__ void fdm_store_rows(const FdmArgs& a, cplx_t<TS>* spe
                 zrr = (m00 * qNr - m10 * q0r) / det; zri = (m00 * qNi - m10 * q0i) / det;
             }
         }
-        const double* hl = bnd ? a.hvec + (size_t)g * 2 * P : nullptr;
-        const double* hr = bnd ? hl + P : nullptr;
+        // the interior correction zl hl + zr hr (skipped when hl = hr = 0: the
+        // transposed system of Dirichlet ends)
+        const bool hadd = bnd && !a.hzero;
+        const double* hl = hadd ? a.hvec + (size_t)g * 2 * P : nullptr;
+        const double* hr = hadd ? hl + P : nullptr;
 #pragma unroll
         for (int t = 0; t < NSS; ++t) {
             const int k = lane + 32 * t;
             if (k < m) {
                 TS lo_r = (TS)r2 * (xsr[r][t] + xdr[r][t]), lo_i = (TS)r2 * (xsi[r][t] + xdi[r][t]);
                 TS hi_r = (TS)r2 * (xsr[r][t] - xdr[r][t]), hi_i = (TS)r2 * (xsi[r][t] - xdi[r][t]);
-                if (bnd) {
+                if (hadd) {
                     const TS l0 = (TS)hl[1 + k], r0 = (TS)hr[1 + k];
                     const TS l1 = (TS)hl[n - k], r1 = (TS)hr[n - k];
                     lo_r += zlr * l0 + zrr * r0; lo_i += zli * l0 + zri * r0;
@@ -211,7 +214,7 @@ __device__ __forceinline__ void fdm_store_rows(const FdmArgs& a, cplx_t<TS>* spe
                 row[n - k] = mk(hi_r, hi_i);
             } else if (k < ms) {
                 TS mr = xsr[r][t], mi = xsi[r][t];
-                if (bnd) {
+                if (hadd) {
                     const TS l0 = (TS)hl[1 + k], r0 = (TS)hr[1 + k];
                     mr += zlr * l0 + zrr * r0; mi += zli * l0 + zri * r0;
                 }

@@ -22,6 +22,7 @@ struct FdmArgs {
     const double* eNf;   // [2][ld] folded weights of the second
     const double* hvec;  // [groups][2][P] vectors combined with the boundary values (NULL: none)
     const double* hscal; // [groups][4] scalars of the boundary system
+    int hzero;           // hvec is zero: skip its reads (boundary values still computed)
     double al, bl, ar, br;
     int adjoint;
     // FP64 tensor-core variant: the four transforms of `mats` in mma.sync

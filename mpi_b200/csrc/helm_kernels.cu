@@ -75,26 +75,60 @@ __device__ __forceinline__ void pass_to_smem(cplx_t<T>* sm, int tc, int cl, cons
         for (int r = 0; r < R; ++r) sm[pass_out_row<R, NS, TPC>(tc, t, r) * CT + cl] = v[t * R + r];
 }
 
-// One real output value of a C2R pass at (row, column c) of the output tile;
-// in an adjoint pass (a.adj_mode) it is also split into the boundary
-// cotangents and accumulated into the lambda sum.
-template <typename TIO>
-__device__ __forceinline__ void c2r_put(const FftArgs& a, TIO* out, long long out_base, long long row, int c,
-                                        double v, double& acc)
+// The real outputs of one thread of a C2R pass: columns c0 (and c1 when has1)
+// at the rows of its last-pass items v[t RL + r], scaled by sc.  In an adjoint
+// pass (a.adj_mode) the GLL boundary slots also go to the boundary cotangents
+// and acc gathers the lambda sum; the forward solution values it needs are
+// loaded for a whole group of RL rows before any store of that group.
+template <typename T, typename TIO, int R0, int RL, int NSL, int TPC>
+__device__ __forceinline__ void c2r_store(const FftArgs& a, TIO* out, long long out_base, int tc, int c0, int c1,
+                                          bool has1, const cplx_t<T> (&v)[R0], T sc, double& acc)
 {
-    const long long idx = row * a.out_row + c;
-    if (a.adj_mode) {
-        const int k = c % a.adj_P, j = c / a.adj_P;
-        const bool first = k == 0, last = k == a.adj_P - 1;
-        if (first && a.gbar_l) a.gbar_l[row * a.bc_row + j] = a.adj_scale_l * v;
-        if (last && a.gbar_r) a.gbar_r[row * a.bc_row + j] = a.adj_scale_r * v;
-        if (a.adj_mode == 1 && (first || last)) {
-            out[idx] = (TIO)0;
-            return;
-        }
-        if (a.lam_u) acc += v * a.lam_u[out_base + idx];
+    if (!a.adj_mode) {
+#pragma unroll
+        for (int t = 0; t < R0 / RL; ++t)
+#pragma unroll
+            for (int r = 0; r < RL; ++r) {
+                const long long row = pass_out_row<RL, NSL, TPC>(tc, t, r);
+                out[row * a.out_row + c0] = (TIO)(v[t * RL + r].x * sc);
+                if (has1) out[row * a.out_row + c1] = (TIO)(v[t * RL + r].y * sc);
+            }
+        return;
     }
-    out[idx] = (TIO)v;
+    const int P = a.adj_P;
+    const int k0 = c0 % P, j0 = c0 / P, k1 = c1 % P, j1 = c1 / P;
+    const bool b0 = k0 == 0 || k0 == P - 1, b1 = k1 == 0 || k1 == P - 1;
+    const bool zero0 = a.adj_mode == 1 && b0, zero1 = a.adj_mode == 1 && b1;
+    const double* u = a.lam_u ? a.lam_u + out_base : nullptr;
+#pragma unroll
+    for (int t = 0; t < R0 / RL; ++t) {
+        double u0[RL], u1[RL];
+#pragma unroll
+        for (int r = 0; r < RL; ++r) {
+            const long long row = pass_out_row<RL, NSL, TPC>(tc, t, r);
+            u0[r] = (u && !zero0) ? u[row * a.out_row + c0] : 0.0;
+            u1[r] = (u && has1 && !zero1) ? u[row * a.out_row + c1] : 0.0;
+        }
+#pragma unroll
+        for (int r = 0; r < RL; ++r) {
+            const long long row = pass_out_row<RL, NSL, TPC>(tc, t, r);
+            const double x0 = (double)(v[t * RL + r].x * sc), x1 = (double)(v[t * RL + r].y * sc);
+            if (b0) {
+                if (k0 == 0 && a.gbar_l) a.gbar_l[row * a.bc_row + j0] = a.adj_scale_l * x0;
+                if (k0 == P - 1 && a.gbar_r) a.gbar_r[row * a.bc_row + j0] = a.adj_scale_r * x0;
+            }
+            out[row * a.out_row + c0] = zero0 ? (TIO)0 : (TIO)x0;
+            acc += x0 * u0[r];
+            if (has1) {
+                if (b1) {
+                    if (k1 == 0 && a.gbar_l) a.gbar_l[row * a.bc_row + j1] = a.adj_scale_l * x1;
+                    if (k1 == P - 1 && a.gbar_r) a.gbar_r[row * a.bc_row + j1] = a.adj_scale_r * x1;
+                }
+                out[row * a.out_row + c1] = zero1 ? (TIO)0 : (TIO)x1;
+                acc += x1 * u1[r];
+            }
+        }
+    }
 }
 
 // Adds every thread's acc into *a.lam_out (one atomic per CTA); all threads call.
@@ -115,6 +149,7 @@ __device__ __forceinline__ void c2r_lambda_sum(const FftArgs& a, double acc)
 template <typename T, typename TIO, int L, int DIR, int MODE, int THREADS, int SMALL>
 __global__ void __launch_bounds__(THREADS) fft_kernel(FftArgs a, long long total_cols)
 {
+    if (a.zero_out && blockIdx.x == 0 && threadIdx.x == 0) *a.zero_out = 0.0;
     using C = cplx_t<T>;
     using S = FftShape<T, L, THREADS, SMALL>;
     constexpr int R0 = S::R0, R1 = S::R1, R2 = S::R2, NP = S::NP, TPC = S::TPC, CT = S::CT;
@@ -227,17 +262,9 @@ __global__ void __launch_bounds__(THREADS) fft_kernel(FftArgs a, long long total
         }
     } else if constexpr (MODE == FFT_C2R) {
         double acc = 0.0;
-        if (valid) {
-            TIO* out = static_cast<TIO*>(a.out) + out_base;
-#pragma unroll
-            for (int t = 0; t < R0 / RL; ++t)
-#pragma unroll
-                for (int r = 0; r < RL; ++r) {
-                    const long long row = pass_out_row<RL, NSL, TPC>(tc, t, r);
-                    c2r_put(a, out, out_base, row, c0, (double)(v[t * RL + r].x * sc), acc);
-                    if (has1) c2r_put(a, out, out_base, row, c1, (double)(v[t * RL + r].y * sc), acc);
-                }
-        }
+        if (valid)
+            c2r_store<T, TIO, R0, RL, NSL, TPC>(a, static_cast<TIO*>(a.out) + out_base, out_base, tc, c0, c1, has1, v,
+                                                sc, acc);
         if (a.lam_out) c2r_lambda_sum(a, acc);
     } else {  // R2C: separate the two real columns' spectra, keep k = 0 .. L/2
         __syncthreads();
@@ -332,6 +359,7 @@ __device__ __forceinline__ void pipe_issue(const FftArgs& a, long long total_col
 template <typename T, typename TIO, int L, int DIR, int MODE, int THREADS, int SMALL>
 __global__ void __launch_bounds__(THREADS) fft_pipe_kernel(FftArgs a, long long total_cols, long long ntiles)
 {
+    if (a.zero_out && blockIdx.x == 0 && threadIdx.x == 0) *a.zero_out = 0.0;
     using C = cplx_t<T>;
     using S = FftShape<T, L, THREADS, SMALL>;
     using PS = PipeShape<T, TIO, L, THREADS, SMALL>;
@@ -464,17 +492,9 @@ __global__ void __launch_bounds__(THREADS) fft_pipe_kernel(FftArgs a, long long 
                     }
             }
         } else if constexpr (MODE == FFT_C2R) {
-            if (valid) {
-                TIO* out = static_cast<TIO*>(a.out) + out_base;
-#pragma unroll
-                for (int t = 0; t < R0 / RL; ++t)
-#pragma unroll
-                    for (int r = 0; r < RL; ++r) {
-                        const long long row = pass_out_row<RL, NSL, TPC>(tc, t, r);
-                        c2r_put(a, out, out_base, row, c0, (double)(v[t * RL + r].x * sc), lam_acc);
-                        if (has1) c2r_put(a, out, out_base, row, c1, (double)(v[t * RL + r].y * sc), lam_acc);
-                    }
-            }
+            if (valid)
+                c2r_store<T, TIO, R0, RL, NSL, TPC>(a, static_cast<TIO*>(a.out) + out_base, out_base, tc, c0, c1, has1,
+                                                    v, sc, lam_acc);
         } else {
             __syncthreads();
             pass_to_smem<T, L, RL, NSL, TPC, CT, R0>(sm, tc, cl, v);

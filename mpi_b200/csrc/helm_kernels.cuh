@@ -48,6 +48,9 @@ struct FftArgs {
     double* gbar_r;
     const double* lam_u;
     double* lam_out;
+    // when set, the pass writes 0 to *zero_out first (the lambda sum of the same
+    // solve's last pass starts from it; no separate memset)
+    double* zero_out;
 };
 
 // Finite-difference variant: one tridiagonal solve along z per spectrum row.

@@ -547,6 +547,7 @@ static int fft_pass(Plan& p, int L, int mode, int dir, const void* in, void* out
         a.lam_u = adj->lambda_bar ? adj->u : nullptr;
         a.lam_out = adj->lambda_bar;
     }
+    if (adj && stage == 0) a.zero_out = adj->lambda_bar;
     a.in = in;
     a.out = out;
     a.in_row = in_row;
@@ -588,12 +589,12 @@ static int run_pipeline(Plan& p, const void* in, const double* gl, const double*
     const int nkx = p.Nx / 2 + 1;
     int st;
     auto mark = [&](int i) {
-        if (p.stage_timing && !adjoint) cudaEventRecord(p.ev[i], s);
+        if (p.stage_timing) cudaEventRecord(p.ev[i], s);
     };
     mark(0);
     // 1. x: real-to-complex (forward: GLL boundary slots take the boundary data)
     if ((st = fft_pass(p, p.Nx, FFT_R2C, -1, in, p.d_spec, p.x_stride, cols, p.elem_stride, p.elem_spec, (int)cols,
-                       p.Ns * p.batch, 1.0, p.d_tw_x, gl, gr, !adjoint, adjoint, 0, s)))
+                       p.Ns * p.batch, 1.0, p.d_tw_x, gl, gr, !adjoint, adjoint, 0, s, adj)))
         return st;
     mark(1);
     // 2. y: complex-to-complex along the middle axis
@@ -683,6 +684,9 @@ static int run_pipeline(Plan& p, const void* in, const double* gl, const double*
         fa.eNf = adjoint ? p.d_fcN : p.d_feN;
         fa.hvec = adjoint ? p.d_hom_adj : r.hom;
         fa.hscal = adjoint ? p.d_homs_adj : p.d_homs;
+        // the transposed system's pl, pr are -A^-T of the Robin rows' interior
+        // entries, which vanish for Dirichlet ends
+        fa.hzero = (adjoint && p.bc.alphal == 0.0 && p.bc.alphar == 0.0) ? 1 : 0;
         fa.al = p.bc.alphal;
         fa.bl = p.bc.betal;
         fa.ar = p.bc.alphar;
@@ -803,11 +807,8 @@ int solve_adjoint(Plan& p, const double* ubar, double* fbar, double* glbar, doub
         g_last_error = "lambda_bar needs the forward solution u";
         return HELM_ERR_INVALID;
     }
-    if (lambda_bar) {
-        cudaError_t e = cudaMemsetAsync(lambda_bar, 0, sizeof(double), s);
-        if (e != cudaSuccess) return set_cuda_error(e, "cudaMemsetAsync");
-    }
-    // the last pass writes fbar, splits off glbar / grbar and sums fbar * u
+    // the first pass zeroes lambda_bar; the last writes fbar, splits off glbar /
+    // grbar and sums fbar * u into lambda_bar
     const AdjOut adj{glbar, grbar, u, lambda_bar};
     return run_pipeline(p, ubar, nullptr, nullptr, fbar, true, s, &adj);
 }
