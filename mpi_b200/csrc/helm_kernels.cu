@@ -80,11 +80,11 @@ __device__ __forceinline__ void pass_to_smem(cplx_t<T>* sm, int tc, int cl, cons
 // pass (a.adj_mode) the GLL boundary slots also go to the boundary cotangents
 // and acc gathers the lambda sum; the forward solution values it needs are
 // loaded for a whole group of RL rows before any store of that group.
-template <typename T, typename TIO, int R0, int RL, int NSL, int TPC>
+template <bool ADJ, typename T, typename TIO, int R0, int RL, int NSL, int TPC>
 __device__ __forceinline__ void c2r_store(const FftArgs& a, TIO* out, long long out_base, int tc, int c0, int c1,
                                           bool has1, const cplx_t<T> (&v)[R0], T sc, double& acc)
 {
-    if (!a.adj_mode) {
+    if constexpr (!ADJ) {
 #pragma unroll
         for (int t = 0; t < R0 / RL; ++t)
 #pragma unroll
@@ -94,7 +94,7 @@ __device__ __forceinline__ void c2r_store(const FftArgs& a, TIO* out, long long 
                 if (has1) out[row * a.out_row + c1] = (TIO)(v[t * RL + r].y * sc);
             }
         return;
-    }
+    } else {
     const int P = a.adj_P;
     const int k0 = c0 % P, j0 = c0 / P, k1 = c1 % P, j1 = c1 / P;
     const bool b0 = k0 == 0 || k0 == P - 1, b1 = k1 == 0 || k1 == P - 1;
@@ -128,6 +128,7 @@ __device__ __forceinline__ void c2r_store(const FftArgs& a, TIO* out, long long 
                 acc += x1 * u1[r];
             }
         }
+    }
     }
 }
 
@@ -172,7 +173,7 @@ __global__ void __launch_bounds__(THREADS) fft_kernel(FftArgs a, long long total
 
     C v[R0];
     // ---------------------------------------------------------- pass 0 --
-    if constexpr (MODE == FFT_C2R) {
+    if constexpr (MODE == FFT_C2R || MODE == FFT_C2R_ADJ) {
         // Z_k = A_k + i B_k over the full length from the two half spectra
         const C* in = static_cast<const C*>(a.in) + in_base;
         for (int k = tc; k <= L / 2; k += TPC) {
@@ -233,7 +234,7 @@ __global__ void __launch_bounds__(THREADS) fft_kernel(FftArgs a, long long total
 
     // --------------------------------------------------- later passes --
     if constexpr (NP >= 2) {
-        if constexpr (MODE == FFT_C2R) __syncthreads();  // pass 0 read shared memory
+        if constexpr (MODE == FFT_C2R || MODE == FFT_C2R_ADJ) __syncthreads();  // pass 0 read shared memory
         pass_to_smem<T, L, R0, 1, TPC, CT, R0>(sm, tc, cl, v);
         __syncthreads();
         pass_from_smem<T, L, R1, R0, DIR, TPC, CT, R0>(sm, tw, tc, cl, v);
@@ -260,12 +261,13 @@ __global__ void __launch_bounds__(THREADS) fft_kernel(FftArgs a, long long total
                     out[(long long)row * a.out_row + c] = cscale(v[t * RL + r], sc);
                 }
         }
-    } else if constexpr (MODE == FFT_C2R) {
+    } else if constexpr (MODE == FFT_C2R || MODE == FFT_C2R_ADJ) {
         double acc = 0.0;
         if (valid)
-            c2r_store<T, TIO, R0, RL, NSL, TPC>(a, static_cast<TIO*>(a.out) + out_base, out_base, tc, c0, c1, has1, v,
+            c2r_store<MODE == FFT_C2R_ADJ, T, TIO, R0, RL, NSL, TPC>(a, static_cast<TIO*>(a.out) + out_base, out_base, tc, c0, c1, has1, v,
                                                 sc, acc);
-        if (a.lam_out) c2r_lambda_sum(a, acc);
+        if constexpr (MODE == FFT_C2R_ADJ)
+            if (a.lam_out) c2r_lambda_sum(a, acc);
     } else {  // R2C: separate the two real columns' spectra, keep k = 0 .. L/2
         __syncthreads();
         pass_to_smem<T, L, RL, NSL, TPC, CT, R0>(sm, tc, cl, v);
@@ -395,7 +397,7 @@ __global__ void __launch_bounds__(THREADS) fft_pipe_kernel(FftArgs a, long long 
 
         C v[R0];
         // ------------------------------------------------ pass 0 input --
-        if constexpr (MODE == FFT_C2R) {
+        if constexpr (MODE == FFT_C2R || MODE == FFT_C2R_ADJ) {
             constexpr int KPT = (L / 2) / TPC + 1;  // half-spectrum rows per thread (upper bound)
             C A[KPT], B[KPT];
 #pragma unroll
@@ -491,9 +493,9 @@ __global__ void __launch_bounds__(THREADS) fft_pipe_kernel(FftArgs a, long long 
                         out[(long long)row * a.out_row + c] = cscale(v[t * RL + r], sc);
                     }
             }
-        } else if constexpr (MODE == FFT_C2R) {
+        } else if constexpr (MODE == FFT_C2R || MODE == FFT_C2R_ADJ) {
             if (valid)
-                c2r_store<T, TIO, R0, RL, NSL, TPC>(a, static_cast<TIO*>(a.out) + out_base, out_base, tc, c0, c1, has1,
+                c2r_store<MODE == FFT_C2R_ADJ, T, TIO, R0, RL, NSL, TPC>(a, static_cast<TIO*>(a.out) + out_base, out_base, tc, c0, c1, has1,
                                                     v, sc, lam_acc);
         } else {
             __syncthreads();
@@ -513,7 +515,7 @@ __global__ void __launch_bounds__(THREADS) fft_pipe_kernel(FftArgs a, long long 
         __syncthreads();  // this buffer is refilled two tiles later
     }
     asm volatile("cp.async.wait_all;\n" ::);
-    if constexpr (MODE == FFT_C2R)
+    if constexpr (MODE == FFT_C2R_ADJ)
         if (a.lam_out) c2r_lambda_sum(a, lam_acc);
 }
 
@@ -560,12 +562,20 @@ static int fft_dispatch_mode(int mode, int dir, const FftArgs& a, long long tc, 
             return dir < 0 ? run_fft_pipe<T, T, L, -1, FFT_C2C, THREADS, SMALL>(a, tc, s)
                            : run_fft_pipe<T, T, L, 1, FFT_C2C, THREADS, SMALL>(a, tc, s);
         if (mode == FFT_R2C) return run_fft_pipe<T, TIO, L, -1, FFT_R2C, THREADS, SMALL>(a, tc, s);
+        if (mode == FFT_C2R_ADJ) {
+            if constexpr (sizeof(TIO) == 8) return run_fft_pipe<T, TIO, L, 1, FFT_C2R_ADJ, THREADS, SMALL>(a, tc, s);
+            return (int)cudaErrorInvalidValue;  // adjoint outputs are double
+        }
         return run_fft_pipe<T, TIO, L, 1, FFT_C2R, THREADS, SMALL>(a, tc, s);
     }
     if (mode == FFT_C2C)
         return dir < 0 ? run_fft<T, T, L, -1, FFT_C2C, THREADS, SMALL>(a, tc, s)
                        : run_fft<T, T, L, 1, FFT_C2C, THREADS, SMALL>(a, tc, s);
     if (mode == FFT_R2C) return run_fft<T, TIO, L, -1, FFT_R2C, THREADS, SMALL>(a, tc, s);
+    if (mode == FFT_C2R_ADJ) {
+        if constexpr (sizeof(TIO) == 8) return run_fft<T, TIO, L, 1, FFT_C2R_ADJ, THREADS, SMALL>(a, tc, s);
+        return (int)cudaErrorInvalidValue;
+    }
     return run_fft<T, TIO, L, 1, FFT_C2R, THREADS, SMALL>(a, tc, s);
 }
 

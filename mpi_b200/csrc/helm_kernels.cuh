@@ -6,7 +6,9 @@
 
 namespace helm {
 
-enum FftMode { FFT_C2C = 0, FFT_R2C = 1, FFT_C2R = 2 };
+// FFT_C2R_ADJ: the C2R pass of an adjoint solve (FftArgs adj_* fields), a
+// separate instantiation so the forward C2R carries none of its code.
+enum FftMode { FFT_C2C = 0, FFT_R2C = 1, FFT_C2R = 2, FFT_C2R_ADJ = 3 };
 
 // One batched FFT along a strided axis.  The transform index is the row; the
 // data of one row are `ncols` contiguous columns; batches are `*_batch` apart.

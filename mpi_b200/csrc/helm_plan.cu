@@ -573,7 +573,8 @@ static int fft_pass(Plan& p, int L, int mode, int dir, const void* in, void* out
     const long long ccols = (mode == FFT_C2C) ? ncols : (ncols + 1) / 2;
     const int td = p.precision != HELM_FP32;
     const int io = (td || io_double) ? 8 : p.io_bytes;
-    int e = launch_fft(L, mode, dir, td, io, a, ccols * nbatch, s, p.fft_var[stage]);
+    const int kmode = a.adj_mode ? (int)FFT_C2R_ADJ : mode;
+    int e = launch_fft(L, kmode, dir, td, io, a, ccols * nbatch, s, p.fft_var[stage]);
     if (e) return set_cuda_error((cudaError_t)e, "fft launch");
     return HELM_OK;
 }
