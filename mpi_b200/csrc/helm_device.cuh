@@ -2,6 +2,7 @@
 // float2/double2, in-register power-of-2 DFTs, and one Stockham pass of a
 // batched strided-axis FFT held in shared memory.
 #pragma once
+#include <cstdlib>
 #include <cuda_runtime.h>
 #include <cstdint>
 
@@ -134,5 +135,44 @@ __device__ __forceinline__ void cp_async_elem(void* dst, const void* src, bool v
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
 __device__ __forceinline__ void cp_async_wait_prev() { asm volatile("cp.async.wait_group 1;\n" ::); }
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::); }
+
+// Programmatic dependent launch.  Every kernel of a solve is launched with the
+// programmatic-serialization attribute, so it may be scheduled while the
+// previous kernel in the stream is still finishing; pdl_enter() then waits
+// (griddepcontrol.wait) until that kernel has completed and its writes are
+// visible, and lets the next kernel in the stream be scheduled in turn.  Call
+// it before the first read of anything an earlier kernel wrote.
+__device__ __forceinline__ void pdl_enter()
+{
+    asm volatile("griddepcontrol.wait;\n" ::: "memory");
+    asm volatile("griddepcontrol.launch_dependents;\n" ::: "memory");
+}
+
+// Host side: launch `k` with the programmatic-serialization attribute
+// (environment HELM_PDL=0: ordinary launches).  Returns the launch status.
+inline bool pdl_enabled()
+{
+    static const bool on = [] {
+        const char* e = std::getenv("HELM_PDL");
+        return !(e && e[0] == '0');
+    }();
+    return on;
+}
+
+template <typename... KArgs, typename... Args>
+inline cudaError_t launch_k(void (*k)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t s, Args... args)
+{
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = grid;
+    cfg.blockDim = block;
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = s;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = pdl_enabled() ? 1 : 0;
+    return cudaLaunchKernelEx(&cfg, k, ((KArgs)args)...);
+}
 
 }  // namespace helm

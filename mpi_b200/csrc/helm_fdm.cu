@@ -252,6 +252,7 @@ __global__ void __launch_bounds__(FDM_WARPS * 32, 2) fdm_fast_kernel(FdmArgs a)
         if (REFINE)
             for (int e = threadIdx.x; e < 2 * ld * ld; e += blockDim.x) Ms[e] = a.d2f[e];
     }
+    pdl_enter();  // the constants above are plan data; the spectrum comes from the previous pass
     __syncthreads();
 
     CS* spec = static_cast<CS*>(a.spec);
@@ -414,8 +415,7 @@ static int run_fdm(const FdmArgs& a, cudaStream_t s)
     long long grid = (packs + FDM_WARPS - 1) / FDM_WARPS;
     if (grid > (long long)sms * per) grid = (long long)sms * per;
     if (grid <= 0) return 0;
-    k<<<(unsigned)grid, FDM_WARPS * 32, L.total, s>>>(a);
-    return (int)cudaGetLastError();
+    return (int)launch_k(k, dim3((unsigned)grid), dim3(FDM_WARPS * 32), L.total, s, a);
 }
 
 template <int NSS, int RPW>
@@ -519,6 +519,7 @@ __global__ void __launch_bounds__(WARPS * 32, (NSS == 1 ? 2 : 1)) fdm_mma_kernel
         double2* dst = reinterpret_cast<double2*>(A);
         for (int e = threadIdx.x; e < (int)(S::mats / 2); e += blockDim.x) dst[e] = src[e];
     }
+    pdl_enter();
     __syncthreads();
 
     cplx_t<double>* spec = static_cast<cplx_t<double>*>(a.spec);
@@ -672,8 +673,7 @@ static int run_fdm_mma(const FdmArgs& a, cudaStream_t s)
     long long grid = (packs + WARPS - 1) / WARPS;
     if (grid > (long long)sms * per) grid = (long long)sms * per;
     if (grid <= 0) return 0;
-    k<<<(unsigned)grid, WARPS * 32, S::smem, s>>>(a);
-    return (int)cudaGetLastError();
+    return (int)launch_k(k, dim3((unsigned)grid), dim3(WARPS * 32), S::smem, s, a);
 }
 
 // ---- the same solve with the m16n8k8 .f64 shape (sm_90 and later) ----
@@ -708,6 +708,7 @@ __global__ void __launch_bounds__(WARPS * 32, (NSS == 1 ? 2 : 1)) fdm_mma16_kern
         double2* dst = reinterpret_cast<double2*>(A);
         for (int e = threadIdx.x; e < (int)(S::mats / 2); e += blockDim.x) dst[e] = src[e];
     }
+    pdl_enter();
     __syncthreads();
 
     cplx_t<double>* spec = static_cast<cplx_t<double>*>(a.spec);
@@ -862,8 +863,7 @@ static int run_fdm_mma16(const FdmArgs& a, cudaStream_t s)
     long long grid = (packs + WARPS - 1) / WARPS;
     if (grid > (long long)sms * per) grid = (long long)sms * per;
     if (grid <= 0) return 0;
-    k<<<(unsigned)grid, WARPS * 32, S::smem, s>>>(a);
-    return (int)cudaGetLastError();
+    return (int)launch_k(k, dim3((unsigned)grid), dim3(WARPS * 32), S::smem, s, a);
 }
 
 // variant 0: m16n8k8 products; variant 1: m8n8k4 products.  4 rows per warp;

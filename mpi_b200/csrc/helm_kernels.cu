@@ -150,6 +150,7 @@ __device__ __forceinline__ void c2r_lambda_sum(const FftArgs& a, double acc)
 template <typename T, typename TIO, int L, int DIR, int MODE, int THREADS, int SMALL>
 __global__ void __launch_bounds__(THREADS) fft_kernel(FftArgs a, long long total_cols)
 {
+    pdl_enter();
     if (a.zero_out && blockIdx.x == 0 && threadIdx.x == 0) *a.zero_out = 0.0;
     using C = cplx_t<T>;
     using S = FftShape<T, L, THREADS, SMALL>;
@@ -361,6 +362,7 @@ __device__ __forceinline__ void pipe_issue(const FftArgs& a, long long total_col
 template <typename T, typename TIO, int L, int DIR, int MODE, int THREADS, int SMALL>
 __global__ void __launch_bounds__(THREADS) fft_pipe_kernel(FftArgs a, long long total_cols, long long ntiles)
 {
+    pdl_enter();
     if (a.zero_out && blockIdx.x == 0 && threadIdx.x == 0) *a.zero_out = 0.0;
     using C = cplx_t<T>;
     using S = FftShape<T, L, THREADS, SMALL>;
@@ -537,8 +539,7 @@ static int run_fft_pipe(const FftArgs& a, long long total_cols, cudaStream_t s)
     if (per < 1) per = 1;
     long long grid = (long long)sms * per;
     if (grid > tiles) grid = tiles;
-    k<<<(unsigned)grid, THREADS, PS::smem, s>>>(a, total_cols, tiles);
-    return (int)cudaGetLastError();
+    return (int)launch_k(k, dim3((unsigned)grid), dim3(THREADS), PS::smem, s, a, total_cols, tiles);
 }
 
 template <typename T, typename TIO, int L, int DIR, int MODE, int THREADS, int SMALL>
@@ -550,8 +551,7 @@ static int run_fft(const FftArgs& a, long long total_cols, cudaStream_t s)
     if (e != cudaSuccess) return (int)e;
     const long long blocks = (total_cols + S::CT - 1) / S::CT;
     if (blocks <= 0) return 0;
-    k<<<(unsigned)blocks, THREADS, S::smem, s>>>(a, total_cols);
-    return (int)cudaGetLastError();
+    return (int)launch_k(k, dim3((unsigned)blocks), dim3(THREADS), S::smem, s, a, total_cols);
 }
 
 template <typename T, typename TIO, int L, int THREADS, int SMALL>
@@ -777,6 +777,7 @@ __host__ __device__ inline RowSmem row_smem_layout(int n, int ld)
 template <typename TS, typename TF, int NSLOT, int METHOD, bool REFINE, bool ADJ = false>
 __global__ void __launch_bounds__(ROW_WARPS * 32) rows_kernel(RowArgs a)
 {
+    pdl_enter();
     using CS = cplx_t<TS>;
     using CF = cplx_t<TF>;
     extern __shared__ __align__(16) unsigned char row_smem[];
@@ -1042,8 +1043,7 @@ static int run_rows(const RowArgs& a, cudaStream_t s)
         grid = a.ngroups < sms * per ? a.ngroups : sms * per;
     }
     if (grid <= 0) return 0;
-    k<<<grid, ROW_WARPS * 32, L.total, s>>>(a);
-    return (int)cudaGetLastError();
+    return (int)launch_k(k, dim3(grid), dim3(ROW_WARPS * 32), L.total, s, a);
 }
 
 template <int NSLOT>
@@ -1075,6 +1075,7 @@ static int rows_dispatch_prec(int method, int prec, const RowArgs& a, cudaStream
 template <typename T>
 __global__ void __launch_bounds__(128) thomas_kernel(ThomasArgs a)
 {
+    pdl_enter();
     using C = cplx_t<T>;
     const long long r = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (r >= a.nrows) return;
@@ -1197,6 +1198,7 @@ __device__ __forceinline__ void tri_issue_row(const ThomasArgs& a, long long r, 
 template <typename T, int M>
 __global__ void __launch_bounds__(TRI_WARPS * 32, (M <= 8 ? 4 : 2)) thomas_warp_kernel(ThomasArgs a)
 {
+    pdl_enter();
     using C = cplx_t<T>;
     extern __shared__ __align__(16) unsigned char tri_smem[];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -1338,8 +1340,7 @@ static int run_thomas_warp(const ThomasArgs& a, cudaStream_t s)
     long long grid = (a.nrows + TRI_WARPS - 1) / TRI_WARPS;
     if (grid > (long long)sms * per) grid = (long long)sms * per;
     if (grid <= 0) return 0;
-    k<<<(unsigned)grid, TRI_WARPS * 32, smem, s>>>(a);
-    return (int)cudaGetLastError();
+    return (int)launch_k(k, dim3((unsigned)grid), dim3(TRI_WARPS * 32), smem, s, a);
 }
 
 template <typename T>
@@ -1351,8 +1352,7 @@ static int thomas_dispatch(const ThomasArgs& a, cudaStream_t s)
     if (a.Nz <= 512) return run_thomas_warp<T, 16>(a, s);
     const long long blocks = (a.nrows + 127) / 128;
     if (blocks <= 0) return 0;
-    thomas_kernel<T><<<(unsigned)blocks, 128, 0, s>>>(a);
-    return (int)cudaGetLastError();
+    return (int)launch_k(thomas_kernel<T>, dim3((unsigned)blocks), dim3(128), 0, s, a);
 }
 
 int launch_thomas(int prec, const ThomasArgs& a, cudaStream_t s)
