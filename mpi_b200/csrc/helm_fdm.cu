@@ -20,6 +20,9 @@
 #include "helm_device.cuh"
 #include "helm_fdm.cuh"
 
+#include <cstdint>
+#include <cstring>
+
 namespace helm {
 
 constexpr int FDM_WARPS = 8;
@@ -887,6 +890,371 @@ void fdm_mma16_swizzle(const double* cm, int ld, double* out)
     const int MT = ld / 16, KS = ld / 8;
     for (int b = 0; b < 4; ++b) {
         const double* M = cm + (size_t)b * ld * ld;      // column-major: A[i][k] = M[k * ld + i]
+        double* O = out + (size_t)b * ld * ld;
+        for (int mt = 0; mt < MT; ++mt)
+            for (int kk = 0; kk < KS; ++kk)
+                for (int l = 0; l < 32; ++l) {
+                    const int gg = l >> 2, qq = l & 3;
+                    const int i0 = mt * 16 + gg, i1 = i0 + 8, k0 = kk * 8 + qq, k1 = k0 + 4;
+                    double* o = O + (((size_t)mt * KS + kk) * 32 + l) * 4;
+                    o[0] = M[(size_t)k0 * ld + i0];
+                    o[1] = M[(size_t)k0 * ld + i1];
+                    o[2] = M[(size_t)k1 * ld + i0];
+                    o[3] = M[(size_t)k1 * ld + i1];
+                }
+    }
+}
+
+// ============================== refined solve on the tensor cores ==
+//
+// The HELM_FP32_REFINE row solve for folds of up to 32 (GLL up to 65 points):
+//   x  = S(f)                 S: the folded solve with FP32-accurate products
+//   r  = f - (M x - sigma x)  M: the folded blocks of D2int, FP64 tensor cores
+//   x += S(r)
+// S's two transforms run as three TF32 products each (hi*hi + hi*lo + lo*hi
+// with a = hi + lo split at the 10-bit TF32 mantissa; the transforms are split
+// once at plan time, the right-hand sides on the fly), accumulated in FP32 --
+// the accuracy of an FP32 product at the TF32 tensor rate.  The FP64 residual
+// uses mma.sync m16n8k8 .f64.  One warp solves 4 spectrum rows (8 columns:
+// re / im) at a time; the TF32 fragment layout of m16n8k8 is that of the f64
+// shape (g = lane / 4, q = lane % 4):
+//   A: a0 = A[g][q], a1 = A[g + 8][q], a2 = A[g][q + 4], a3 = A[g + 8][q + 4]
+//   B: b0 = B[q][g], b1 = B[q + 4][g]
+//   C: C[g][2q], C[g][2q + 1], C[g + 8][2q], C[g + 8][2q + 1]
+// Per warp a single staging region of 8 columns x 68 doubles holds, in turn,
+// the raw rows, the FP32 exchanges between transforms, and the FP64 iterates.
+
+__device__ __forceinline__ uint32_t to_tf32(float x)
+{
+    uint32_t r;
+    asm("cvt.rna.tf32.f32 %0, %1;\n" : "=r"(r) : "f"(x));
+    return r;
+}
+
+__device__ __forceinline__ void mma_tf32(float (&c)[4], const float4& a, uint32_t b0, uint32_t b1)
+{
+    asm volatile("mma.sync.aligned.m16n8k8.row.col.f32.tf32.tf32.f32 {%0, %1, %2, %3}, {%4, %5, %6, %7}, "
+                 "{%8, %9}, {%0, %1, %2, %3};\n"
+                 : "+f"(c[0]), "+f"(c[1]), "+f"(c[2]), "+f"(c[3])
+                 : "r"(__float_as_uint(a.x)), "r"(__float_as_uint(a.y)), "r"(__float_as_uint(a.z)),
+                   "r"(__float_as_uint(a.w)), "r"(b0), "r"(b1));
+}
+
+// c += A (hi + lo) * B (b = bh + bl), three TF32 products.
+__device__ __forceinline__ void mma_3xtf32(float (&c)[4], const float4& ah, const float4& al, float b0, float b1)
+{
+    const uint32_t h0 = to_tf32(b0), h1 = to_tf32(b1);
+    const uint32_t l0 = to_tf32(b0 - __uint_as_float(h0)), l1 = to_tf32(b1 - __uint_as_float(h1));
+    mma_tf32(c, al, h0, h1);
+    mma_tf32(c, ah, l0, l1);
+    mma_tf32(c, ah, h0, h1);
+}
+
+constexpr int TC_WARPS = 8, TC_LD = 32, TC_MT = 2, TC_KS = 4, TC_S = 68;
+constexpr size_t TC_TF32_FLOATS = (size_t)4 * 2 * TC_LD * TC_LD;  // 4 transforms x (hi, lo)
+constexpr size_t TC_M_DOUBLES = (size_t)2 * TC_LD * TC_LD;        // Ms, Ma
+constexpr size_t TC_SMEM = TC_TF32_FLOATS * 4 + TC_M_DOUBLES * 8 + (size_t)TC_WARPS * 8 * TC_S * 8;
+
+// One folded solve S on B columns read by `bread(blk, k)` (the lane's B element
+// at fold index k of block blk, as float); result x in C layout (FP32).
+template <typename BRead>
+__device__ __forceinline__ void tc_solve(const float4* Tf, const float (&rs)[TC_MT][2], const float (&ra)[TC_MT][2],
+                                         float* X, int g, int q, BRead bread, float (&xs)[TC_MT][4],
+                                         float (&xa)[TC_MT][4])
+{
+    const int lane = g * 4 + q;
+    constexpr size_t BLKF = (size_t)2 * TC_LD * TC_LD / 4;  // float4 per transform (hi + lo)
+    float cs[TC_MT][4], ca[TC_MT][4];
+#pragma unroll
+    for (int mt = 0; mt < TC_MT; ++mt)
+#pragma unroll
+        for (int j = 0; j < 4; ++j) cs[mt][j] = ca[mt][j] = 0.f;
+#pragma unroll
+    for (int kk = 0; kk < TC_KS; ++kk) {
+        const float bs0 = bread(0, 8 * kk + q), bs1 = bread(0, 8 * kk + q + 4);
+        const float ba0 = bread(1, 8 * kk + q), ba1 = bread(1, 8 * kk + q + 4);
+#pragma unroll
+        for (int mt = 0; mt < TC_MT; ++mt) {
+            const size_t f = (size_t)(mt * TC_KS + kk) * 32 + lane;
+            mma_3xtf32(cs[mt], Tf[0 * BLKF + f], Tf[0 * BLKF + BLKF / 2 + f], bs0, bs1);  // Ws
+            mma_3xtf32(ca[mt], Tf[2 * BLKF + f], Tf[2 * BLKF + BLKF / 2 + f], ba0, ba1);  // Wa
+        }
+    }
+    // scale by 1 / (lambda_j - sigma) and stage as the next B (column 2q + j)
+    __syncwarp();
+#pragma unroll
+    for (int mt = 0; mt < TC_MT; ++mt)
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+            const int i = mt * 16 + g + 8 * h;
+#pragma unroll
+            for (int j = 0; j < 2; ++j) {
+                X[(2 * q + j) * TC_S + i] = cs[mt][2 * h + j] * rs[mt][h];
+                X[(2 * q + j) * TC_S + TC_LD + i] = ca[mt][2 * h + j] * ra[mt][h];
+            }
+        }
+    __syncwarp();
+#pragma unroll
+    for (int mt = 0; mt < TC_MT; ++mt)
+#pragma unroll
+        for (int j = 0; j < 4; ++j) xs[mt][j] = xa[mt][j] = 0.f;
+    const float* col = X + g * TC_S;
+#pragma unroll
+    for (int kk = 0; kk < TC_KS; ++kk) {
+        const int k0 = 8 * kk + q, k1 = k0 + 4;
+        const float bs0 = col[k0], bs1 = col[k1], ba0 = col[TC_LD + k0], ba1 = col[TC_LD + k1];
+#pragma unroll
+        for (int mt = 0; mt < TC_MT; ++mt) {
+            const size_t f = (size_t)(mt * TC_KS + kk) * 32 + lane;
+            mma_3xtf32(xs[mt], Tf[1 * BLKF + f], Tf[1 * BLKF + BLKF / 2 + f], bs0, bs1);  // Vs
+            mma_3xtf32(xa[mt], Tf[3 * BLKF + f], Tf[3 * BLKF + BLKF / 2 + f], ba0, ba1);  // Va
+        }
+    }
+    __syncwarp();  // X is free again
+}
+
+template <bool ADJ>
+__global__ void __launch_bounds__(TC_WARPS * 32, 2) fdm_tc_refine_kernel(FdmArgs a)
+{
+    extern __shared__ __align__(16) unsigned char tsm[];
+    float4* Tf = reinterpret_cast<float4*>(tsm);
+    double* Md = reinterpret_cast<double*>(tsm + TC_TF32_FLOATS * 4);
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int g = lane >> 2, q = lane & 3;
+    double* Xd = reinterpret_cast<double*>(tsm + TC_TF32_FLOATS * 4 + TC_M_DOUBLES * 8) + (size_t)warp * 8 * TC_S;
+    float* Xf = reinterpret_cast<float*>(Xd);
+    {
+        const float4* src = static_cast<const float4*>(a.tc_mats);
+        for (int e = threadIdx.x; e < (int)(TC_TF32_FLOATS / 4); e += blockDim.x) Tf[e] = src[e];
+        const double2* msrc = reinterpret_cast<const double2*>(a.tc_m);
+        double2* mdst = reinterpret_cast<double2*>(Md);
+        for (int e = threadIdx.x; e < (int)(TC_M_DOUBLES / 2); e += blockDim.x) mdst[e] = msrc[e];
+    }
+    pdl_enter();
+    __syncthreads();
+
+    cplx_t<double>* spec = static_cast<cplx_t<double>*>(a.spec);
+    const int n = a.n, m = a.m, ms = a.ms, P = a.P, nrows = a.nrows;
+    const double r2 = 0.70710678118654752440;
+    constexpr int RPW = 4, RR = 136;  // raw row r at Xd + r RR (complex i at 2 i)
+    const long long npacks = (nrows + RPW - 1) / RPW;
+    const float* rcp = static_cast<const float*>(a.recip);
+    const double2* Mf = reinterpret_cast<const double2*>(Md);
+    constexpr size_t MBLK = (size_t)TC_LD * TC_LD / 2;  // double2 per block
+
+    for (long long pk = (long long)blockIdx.x * TC_WARPS + warp; pk < npacks; pk += (long long)gridDim.x * TC_WARPS) {
+        int rowid[RPW], grp[RPW];
+        bool ok[RPW];
+#pragma unroll
+        for (int r = 0; r < RPW; ++r) {
+            const long long rr = pk * RPW + r;
+            ok[r] = rr < nrows;
+            rowid[r] = ok[r] ? a.rows[rr] : a.rows[0];
+            grp[r] = ok[r] ? a.row_grp[rr] : a.row_grp[0];
+        }
+        // this lane's C-layout row is q: its shift and reciprocal shifts
+        const int gq = a.row_grp[(pk * RPW + q) < nrows ? pk * RPW + q : 0];
+        const double sig = a.sigma[gq];
+        float rs[TC_MT][2], ra[TC_MT][2];
+#pragma unroll
+        for (int mt = 0; mt < TC_MT; ++mt)
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+                rs[mt][h] = rcp[(size_t)gq * 2 * TC_LD + mt * 16 + g + 8 * h];
+                ra[mt][h] = rcp[(size_t)gq * 2 * TC_LD + TC_LD + mt * 16 + g + 8 * h];
+            }
+        // ---- raw interiors of the 4 rows ----
+        __syncwarp();
+#pragma unroll
+        for (int r = 0; r < RPW; ++r) {
+            const double2* row = reinterpret_cast<const double2*>(spec + (long long)rowid[r] * P);
+            for (int i = lane; i < n; i += 32) *reinterpret_cast<double2*>(Xd + r * RR + 2 * i) = row[1 + i];
+        }
+        __syncwarp();
+        // folded right-hand side at (fold index k, block blk) of column `col` (row col / 2, part col % 2)
+        auto fold_at = [&](int col, int blk, int k) -> double {
+            const double* raw = Xd + (col >> 1) * RR + (col & 1);
+            if (k < m) {
+                const double lo = raw[2 * k], hi = raw[2 * (n - 1 - k)];
+                return blk == 0 ? r2 * (lo + hi) : r2 * (lo - hi);
+            }
+            return (blk == 0 && k < ms) ? raw[2 * k] : 0.0;
+        };
+        // f in C layout (kept for the residual): [blk][mt][h][j]
+        double fc[2][TC_MT][2][2];
+#pragma unroll
+        for (int blk = 0; blk < 2; ++blk)
+#pragma unroll
+            for (int mt = 0; mt < TC_MT; ++mt)
+#pragma unroll
+                for (int h = 0; h < 2; ++h)
+#pragma unroll
+                    for (int j = 0; j < 2; ++j) fc[blk][mt][h][j] = fold_at(2 * q + j, blk, mt * 16 + g + 8 * h);
+        // ---- x = S(f) ----
+        float xs[TC_MT][4], xa[TC_MT][4];
+        {
+            float bsave[2][TC_KS][2];  // the lane's B elements of f, read before X is reused
+#pragma unroll
+            for (int blk = 0; blk < 2; ++blk)
+#pragma unroll
+                for (int kk = 0; kk < TC_KS; ++kk) {
+                    bsave[blk][kk][0] = (float)fold_at(g, blk, 8 * kk + q);
+                    bsave[blk][kk][1] = (float)fold_at(g, blk, 8 * kk + q + 4);
+                }
+            __syncwarp();
+            tc_solve(Tf, rs, ra, Xf, g, q,
+                     [&](int blk, int k) { return bsave[blk][k >> 3][((k & 7) >= 4) ? 1 : 0]; }, xs, xa);
+        }
+        // ---- r = f - (M x - sigma x), FP64 ----
+#pragma unroll
+        for (int mt = 0; mt < TC_MT; ++mt)
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+                const int i = mt * 16 + g + 8 * h;
+#pragma unroll
+                for (int j = 0; j < 2; ++j) {
+                    Xd[(2 * q + j) * TC_S + i] = (double)xs[mt][2 * h + j];
+                    Xd[(2 * q + j) * TC_S + TC_LD + i] = (double)xa[mt][2 * h + j];
+                }
+            }
+        __syncwarp();
+        double ys[TC_MT][4], ya[TC_MT][4];
+#pragma unroll
+        for (int mt = 0; mt < TC_MT; ++mt)
+#pragma unroll
+            for (int j = 0; j < 4; ++j) ys[mt][j] = ya[mt][j] = 0.0;
+        {
+            const double* col = Xd + g * TC_S;
+#pragma unroll
+            for (int kk = 0; kk < TC_KS; ++kk) {
+                const int k0 = 8 * kk + q, k1 = k0 + 4;
+                const double bs0 = col[k0], bs1 = col[k1], ba0 = col[TC_LD + k0], ba1 = col[TC_LD + k1];
+#pragma unroll
+                for (int mt = 0; mt < TC_MT; ++mt) {
+                    const size_t f = ((size_t)(mt * TC_KS + kk) * 32 + lane) * 2;
+                    dmma_16x8x8(ys[mt], Mf[f], Mf[f + 1], bs0, bs1);
+                    dmma_16x8x8(ya[mt], Mf[MBLK + f], Mf[MBLK + f + 1], ba0, ba1);
+                }
+            }
+        }
+        __syncwarp();  // Xd is reused for the residual below
+        float resf[2][TC_KS][2];
+        {
+            // residual in C layout, staged as FP32 columns, then read back as B elements
+#pragma unroll
+            for (int mt = 0; mt < TC_MT; ++mt)
+#pragma unroll
+                for (int h = 0; h < 2; ++h) {
+                    const int i = mt * 16 + g + 8 * h;
+#pragma unroll
+                    for (int j = 0; j < 2; ++j) {
+                        const double rsv = fc[0][mt][h][j] - ys[mt][2 * h + j] + sig * (double)xs[mt][2 * h + j];
+                        const double rav = fc[1][mt][h][j] - ya[mt][2 * h + j] + sig * (double)xa[mt][2 * h + j];
+                        Xf[(2 * q + j) * TC_S + i] = (float)rsv;
+                        Xf[(2 * q + j) * TC_S + TC_LD + i] = (float)rav;
+                    }
+                }
+            __syncwarp();
+            const float* col = Xf + g * TC_S;
+#pragma unroll
+            for (int kk = 0; kk < TC_KS; ++kk) {
+                resf[0][kk][0] = col[8 * kk + q];
+                resf[0][kk][1] = col[8 * kk + q + 4];
+                resf[1][kk][0] = col[TC_LD + 8 * kk + q];
+                resf[1][kk][1] = col[TC_LD + 8 * kk + q + 4];
+            }
+            __syncwarp();
+        }
+        // ---- x += S(r) ----
+        float ds[TC_MT][4], da[TC_MT][4];
+        tc_solve(Tf, rs, ra, Xf, g, q,
+                 [&](int blk, int k) { return resf[blk][k >> 3][((k & 7) >= 4) ? 1 : 0]; }, ds, da);
+#pragma unroll
+        for (int mt = 0; mt < TC_MT; ++mt)
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+                const int i = mt * 16 + g + 8 * h;
+#pragma unroll
+                for (int j = 0; j < 2; ++j) {
+                    Xd[(2 * q + j) * TC_S + i] = (double)xs[mt][2 * h + j] + (double)ds[mt][2 * h + j];
+                    Xd[(2 * q + j) * TC_S + TC_LD + i] = (double)xa[mt][2 * h + j] + (double)da[mt][2 * h + j];
+                }
+            }
+        __syncwarp();
+        double xsr[RPW][1], xsi[RPW][1], xdr[RPW][1], xdi[RPW][1];
+#pragma unroll
+        for (int r = 0; r < RPW; ++r) {
+            xsr[r][0] = Xd[(2 * r) * TC_S + lane];
+            xsi[r][0] = Xd[(2 * r + 1) * TC_S + lane];
+            xdr[r][0] = Xd[(2 * r) * TC_S + TC_LD + lane];
+            xdi[r][0] = Xd[(2 * r + 1) * TC_S + TC_LD + lane];
+        }
+        fdm_store_rows<double, 1, RPW, ADJ>(a, spec, rowid, grp, ok, xsr, xsi, xdr, xdi, lane);
+        __syncwarp();
+    }
+}
+
+int launch_fdm_tc_refine(const FdmArgs& a, cudaStream_t s)
+{
+    if (a.ld != TC_LD || !a.tc_mats || !a.tc_m || a.sweeps != 1) return (int)cudaErrorInvalidValue;
+    auto k = a.adjoint ? fdm_tc_refine_kernel<true> : fdm_tc_refine_kernel<false>;
+    cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TC_SMEM);
+    if (e != cudaSuccess) return (int)e;
+    int dev = 0, sms = 148, per = 1;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k, TC_WARPS * 32, TC_SMEM);
+    if (per < 1) per = 1;
+    const long long packs = (a.nrows + 3) / 4;
+    long long grid = (packs + TC_WARPS - 1) / TC_WARPS;
+    if (grid > (long long)sms * per) grid = (long long)sms * per;
+    if (grid <= 0) return 0;
+    return (int)launch_k(k, dim3((unsigned)grid), dim3(TC_WARPS * 32), TC_SMEM, s, a);
+}
+
+// The four transforms (column-major ld x ld, A[i][k] = cm[k ld + i]) split into
+// TF32 hi + lo, in the m16n8k8 A-fragment order: [4][hi, lo][ld/16][ld/8][32][4].
+static float tf32_round(double v)
+{
+    // round to nearest (ties away from zero) at 10 mantissa bits, like cvt.rna.tf32.f32
+    float f = (float)v;
+    uint32_t u;
+    std::memcpy(&u, &f, 4);
+    if ((u & 0x7f800000u) != 0x7f800000u) u = (u + 0x1000u) & 0xffffe000u;
+    std::memcpy(&f, &u, 4);
+    return f;
+}
+
+void fdm_tc_swizzle(const double* cm, int ld, float* out)
+{
+    const int MT = ld / 16, KS = ld / 8;
+    for (int b = 0; b < 4; ++b) {
+        const double* M = cm + (size_t)b * ld * ld;
+        for (int part = 0; part < 2; ++part) {
+            float* O = out + ((size_t)b * 2 + part) * ld * ld;
+            for (int mt = 0; mt < MT; ++mt)
+                for (int kk = 0; kk < KS; ++kk)
+                    for (int l = 0; l < 32; ++l) {
+                        const int gg = l >> 2, qq = l & 3;
+                        const int i0 = mt * 16 + gg, i1 = i0 + 8, k0 = kk * 8 + qq, k1 = k0 + 4;
+                        const double v[4] = {M[(size_t)k0 * ld + i0], M[(size_t)k0 * ld + i1], M[(size_t)k1 * ld + i0],
+                                             M[(size_t)k1 * ld + i1]};
+                        float* o = O + (((size_t)mt * KS + kk) * 32 + l) * 4;
+                        for (int e = 0; e < 4; ++e) {
+                            const float hi = tf32_round(v[e]);
+                            o[e] = part == 0 ? hi : tf32_round(v[e] - (double)hi);
+                        }
+                    }
+        }
+    }
+}
+
+// Two FP64 column-major blocks in the m16n8k8 .f64 A-fragment order.
+void fdm_m16_swizzle2(const double* cm, int ld, double* out)
+{
+    const int MT = ld / 16, KS = ld / 8;
+    for (int b = 0; b < 2; ++b) {
+        const double* M = cm + (size_t)b * ld * ld;
         double* O = out + (size_t)b * ld * ld;
         for (int mt = 0; mt < MT; ++mt)
             for (int kk = 0; kk < KS; ++kk)

@@ -29,6 +29,10 @@ struct FdmArgs {
     // m8n8k4 A-fragment order, [4][ld/8][ld/4][32] (NULL: not prepared)
     const double* mma_mats;
     const double* mma16_mats;  // the same transforms in m16n8k8 fragment order, [4][ld/16][ld/8][32][4]
+    // refined plans with ld = 32: the transforms split into TF32 hi + lo, and the
+    // folded D2int blocks in f64 fragment order (launch_fdm_tc_refine)
+    const void* tc_mats;
+    const double* tc_m;
 };
 
 int launch_fdm_fast(int prec, const FdmArgs& a, cudaStream_t s, int variant = 0);
@@ -39,5 +43,10 @@ int launch_fdm_mma(const FdmArgs& a, cudaStream_t s, int variant = 0);
 // launch_fdm_mma reads.
 void fdm_mma_swizzle(const double* cm, int ld, double* out);
 void fdm_mma16_swizzle(const double* cm, int ld, double* out);
+// Refined plans (ld = 32, one sweep): FP32-accurate solves as three TF32
+// tensor products, FP64 residual on the FP64 tensor cores.
+int launch_fdm_tc_refine(const FdmArgs& a, cudaStream_t s);
+void fdm_tc_swizzle(const double* cm, int ld, float* out);    // [4][2][ld/16][ld/8][32][4]
+void fdm_m16_swizzle2(const double* cm, int ld, double* out);  // [2][ld/16][ld/8][32][4]
 
 }  // namespace helm

@@ -322,6 +322,18 @@ static int setup_fast(Plan& p, const std::vector<double>& A0, int prec_code)
     };
     if ((st = up_t(fw, &p.d_fmats))) return st;
     if ((st = up_t(fa, &p.d_fmats_adj))) return st;
+    if (prec_code == 2 && ld == 32) {
+        std::vector<float> tf(8 * L2);
+        fdm_tc_swizzle(fw.data(), ld, tf.data());
+        if ((st = p.upload((void**)&p.d_ftc, tf.data(), tf.size() * sizeof(float)))) return st;
+        fdm_tc_swizzle(fa.data(), ld, tf.data());
+        if ((st = p.upload((void**)&p.d_ftc_adj, tf.data(), tf.size() * sizeof(float)))) return st;
+        std::vector<double> mm(2 * L2);
+        fdm_m16_swizzle2(d2f.data(), ld, mm.data());
+        if ((st = p.upload((void**)&p.d_ftcm, mm.data(), mm.size() * sizeof(double)))) return st;
+        fdm_m16_swizzle2(d2a.data(), ld, mm.data());
+        if ((st = p.upload((void**)&p.d_ftcm_adj, mm.data(), mm.size() * sizeof(double)))) return st;
+    }
     if (prec_code == 0) {
         std::vector<double> sw(4 * L2);
         fdm_mma_swizzle(fw.data(), ld, sw.data());
@@ -695,8 +707,12 @@ static int run_pipeline(Plan& p, const void* in, const double* gl, const double*
         fa.adjoint = adjoint ? 1 : 0;
         fa.mma_mats = adjoint ? p.d_fmma_adj : p.d_fmma;
         fa.mma16_mats = adjoint ? p.d_fmma16_adj : p.d_fmma16;
+        fa.tc_mats = adjoint ? (const void*)p.d_ftc_adj : (const void*)p.d_ftc;
+        fa.tc_m = adjoint ? p.d_ftcm_adj : p.d_ftcm;
         if (prec == 0 && fa.mma_mats)
             e = launch_fdm_mma(fa, s, p.row_var);
+        else if (prec == 2 && fa.tc_mats && p.sweeps == 1 && p.row_var == 0)
+            e = launch_fdm_tc_refine(fa, s);
         else
             e = launch_fdm_fast(prec, fa, s, p.row_var);
     } else {

@@ -66,6 +66,10 @@ struct Plan {
     double* d_fmma_adj = nullptr;
     double* d_fmma16 = nullptr;    // the same in m16n8k8 fragment order
     double* d_fmma16_adj = nullptr;
+    float* d_ftc = nullptr;        // refined plans: TF32 hi/lo transforms (tensor-core refine)
+    float* d_ftc_adj = nullptr;
+    double* d_ftcm = nullptr;      // folded D2int blocks, f64 fragment order
+    double* d_ftcm_adj = nullptr;
     double* d_fd2 = nullptr;       // folded D2int blocks (refinement)
     double* d_fd2_adj = nullptr;   // their transposes
     void* d_frecip = nullptr;      // [G][2][fld] reciprocal shifts
