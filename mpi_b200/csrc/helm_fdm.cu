@@ -940,20 +940,34 @@ __device__ __forceinline__ void mma_tf32(float (&c)[4], const float4& a, uint32_
                    "r"(__float_as_uint(a.w)), "r"(b0), "r"(b1));
 }
 
-// c += A (hi + lo) * B (b = bh + bl), three TF32 products.
-__device__ __forceinline__ void mma_3xtf32(float (&c)[4], const float4& ah, const float4& al, float b0, float b1)
+// A B fragment split at the TF32 mantissa: b = hi + lo.
+struct Tf32Split {
+    uint32_t h0, h1, l0, l1;
+};
+__device__ __forceinline__ Tf32Split tf32_split(float b0, float b1)
 {
-    const uint32_t h0 = to_tf32(b0), h1 = to_tf32(b1);
-    const uint32_t l0 = to_tf32(b0 - __uint_as_float(h0)), l1 = to_tf32(b1 - __uint_as_float(h1));
-    mma_tf32(c, al, h0, h1);
-    mma_tf32(c, ah, l0, l1);
-    mma_tf32(c, ah, h0, h1);
+    Tf32Split t;
+    t.h0 = to_tf32(b0);
+    t.h1 = to_tf32(b1);
+    t.l0 = to_tf32(b0 - __uint_as_float(t.h0));
+    t.l1 = to_tf32(b1 - __uint_as_float(t.h1));
+    return t;
 }
 
-constexpr int TC_WARPS = 8, TC_LD = 32, TC_MT = 2, TC_KS = 4, TC_S = 68;
+// c += A (hi + lo) * B (hi + lo), three TF32 products (lo * lo dropped).
+__device__ __forceinline__ void mma_3xtf32(float (&c)[4], const float4& ah, const float4& al, const Tf32Split& b)
+{
+    mma_tf32(c, al, b.h0, b.h1);
+    mma_tf32(c, ah, b.l0, b.l1);
+    mma_tf32(c, ah, b.h0, b.h1);
+}
+
+constexpr int TC_WARPS = 16, TC_LD = 32, TC_MT = 2, TC_KS = 4, TC_S = 68;
 constexpr size_t TC_TF32_FLOATS = (size_t)4 * 2 * TC_LD * TC_LD;  // 4 transforms x (hi, lo)
 constexpr size_t TC_M_DOUBLES = (size_t)2 * TC_LD * TC_LD;        // Ms, Ma
-constexpr size_t TC_SMEM = TC_TF32_FLOATS * 4 + TC_M_DOUBLES * 8 + (size_t)TC_WARPS * 8 * TC_S * 8;
+// per warp two staging regions of 8 columns x 68 doubles: the current pack and the next one arriving
+constexpr size_t TC_REG = (size_t)8 * TC_S;  // doubles
+constexpr size_t TC_SMEM = TC_TF32_FLOATS * 4 + TC_M_DOUBLES * 8 + (size_t)TC_WARPS * 2 * TC_REG * 8;
 
 // One folded solve S on B columns read by `bread(blk, k)` (the lane's B element
 // at fold index k of block blk, as float); result x in C layout (FP32).
@@ -971,13 +985,13 @@ __device__ __forceinline__ void tc_solve(const float4* Tf, const float (&rs)[TC_
         for (int j = 0; j < 4; ++j) cs[mt][j] = ca[mt][j] = 0.f;
 #pragma unroll
     for (int kk = 0; kk < TC_KS; ++kk) {
-        const float bs0 = bread(0, 8 * kk + q), bs1 = bread(0, 8 * kk + q + 4);
-        const float ba0 = bread(1, 8 * kk + q), ba1 = bread(1, 8 * kk + q + 4);
+        const Tf32Split bs = tf32_split(bread(0, 8 * kk + q), bread(0, 8 * kk + q + 4));
+        const Tf32Split ba = tf32_split(bread(1, 8 * kk + q), bread(1, 8 * kk + q + 4));
 #pragma unroll
         for (int mt = 0; mt < TC_MT; ++mt) {
             const size_t f = (size_t)(mt * TC_KS + kk) * 32 + lane;
-            mma_3xtf32(cs[mt], Tf[0 * BLKF + f], Tf[0 * BLKF + BLKF / 2 + f], bs0, bs1);  // Ws
-            mma_3xtf32(ca[mt], Tf[2 * BLKF + f], Tf[2 * BLKF + BLKF / 2 + f], ba0, ba1);  // Wa
+            mma_3xtf32(cs[mt], Tf[0 * BLKF + f], Tf[0 * BLKF + BLKF / 2 + f], bs);  // Ws
+            mma_3xtf32(ca[mt], Tf[2 * BLKF + f], Tf[2 * BLKF + BLKF / 2 + f], ba);  // Wa
         }
     }
     // scale by 1 / (lambda_j - sigma) and stage as the next B (column 2q + j)
@@ -1002,27 +1016,27 @@ __device__ __forceinline__ void tc_solve(const float4* Tf, const float (&rs)[TC_
 #pragma unroll
     for (int kk = 0; kk < TC_KS; ++kk) {
         const int k0 = 8 * kk + q, k1 = k0 + 4;
-        const float bs0 = col[k0], bs1 = col[k1], ba0 = col[TC_LD + k0], ba1 = col[TC_LD + k1];
+        const Tf32Split bs = tf32_split(col[k0], col[k1]);
+        const Tf32Split ba = tf32_split(col[TC_LD + k0], col[TC_LD + k1]);
 #pragma unroll
         for (int mt = 0; mt < TC_MT; ++mt) {
             const size_t f = (size_t)(mt * TC_KS + kk) * 32 + lane;
-            mma_3xtf32(xs[mt], Tf[1 * BLKF + f], Tf[1 * BLKF + BLKF / 2 + f], bs0, bs1);  // Vs
-            mma_3xtf32(xa[mt], Tf[3 * BLKF + f], Tf[3 * BLKF + BLKF / 2 + f], ba0, ba1);  // Va
+            mma_3xtf32(xs[mt], Tf[1 * BLKF + f], Tf[1 * BLKF + BLKF / 2 + f], bs);  // Vs
+            mma_3xtf32(xa[mt], Tf[3 * BLKF + f], Tf[3 * BLKF + BLKF / 2 + f], ba);  // Va
         }
     }
     __syncwarp();  // X is free again
 }
 
 template <bool ADJ>
-__global__ void __launch_bounds__(TC_WARPS * 32, 2) fdm_tc_refine_kernel(FdmArgs a)
+__global__ void __launch_bounds__(TC_WARPS * 32, 1) fdm_tc_refine_kernel(FdmArgs a)
 {
     extern __shared__ __align__(16) unsigned char tsm[];
     float4* Tf = reinterpret_cast<float4*>(tsm);
     double* Md = reinterpret_cast<double*>(tsm + TC_TF32_FLOATS * 4);
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int g = lane >> 2, q = lane & 3;
-    double* Xd = reinterpret_cast<double*>(tsm + TC_TF32_FLOATS * 4 + TC_M_DOUBLES * 8) + (size_t)warp * 8 * TC_S;
-    float* Xf = reinterpret_cast<float*>(Xd);
+    double* regions = reinterpret_cast<double*>(tsm + TC_TF32_FLOATS * 4 + TC_M_DOUBLES * 8) + (size_t)warp * 2 * TC_REG;
     {
         const float4* src = static_cast<const float4*>(a.tc_mats);
         for (int e = threadIdx.x; e < (int)(TC_TF32_FLOATS / 4); e += blockDim.x) Tf[e] = src[e];
@@ -1039,10 +1053,20 @@ __global__ void __launch_bounds__(TC_WARPS * 32, 2) fdm_tc_refine_kernel(FdmArgs
     constexpr int RPW = 4, RR = 136;  // raw row r at Xd + r RR (complex i at 2 i)
     const long long npacks = (nrows + RPW - 1) / RPW;
     const float* rcp = static_cast<const float*>(a.recip);
+    // M fragments in two planes per block: (a0, a1) of every lane, then (a2, a3)
     const double2* Mf = reinterpret_cast<const double2*>(Md);
-    constexpr size_t MBLK = (size_t)TC_LD * TC_LD / 2;  // double2 per block
+    constexpr size_t MPLANE = (size_t)TC_LD * TC_LD / 4;  // double2 per plane
 
-    for (long long pk = (long long)blockIdx.x * TC_WARPS + warp; pk < npacks; pk += (long long)gridDim.x * TC_WARPS) {
+    const long long pstride = (long long)gridDim.x * TC_WARPS;
+    long long pk = (long long)blockIdx.x * TC_WARPS + warp;
+    int cur = 0;
+    if (pk < npacks) mma_issue_pack<RPW, RR>(a, pk, regions, lane);
+    cp_async_commit();
+    for (; pk < npacks; pk += pstride, cur ^= 1) {
+        double* Xd = regions + (size_t)cur * TC_REG;
+        float* Xf = reinterpret_cast<float*>(Xd);
+        if (pk + pstride < npacks) mma_issue_pack<RPW, RR>(a, pk + pstride, regions + (size_t)(cur ^ 1) * TC_REG, lane);
+        cp_async_commit();
         int rowid[RPW], grp[RPW];
         bool ok[RPW];
 #pragma unroll
@@ -1063,13 +1087,8 @@ __global__ void __launch_bounds__(TC_WARPS * 32, 2) fdm_tc_refine_kernel(FdmArgs
                 rs[mt][h] = rcp[(size_t)gq * 2 * TC_LD + mt * 16 + g + 8 * h];
                 ra[mt][h] = rcp[(size_t)gq * 2 * TC_LD + TC_LD + mt * 16 + g + 8 * h];
             }
-        // ---- raw interiors of the 4 rows ----
-        __syncwarp();
-#pragma unroll
-        for (int r = 0; r < RPW; ++r) {
-            const double2* row = reinterpret_cast<const double2*>(spec + (long long)rowid[r] * P);
-            for (int i = lane; i < n; i += 32) *reinterpret_cast<double2*>(Xd + r * RR + 2 * i) = row[1 + i];
-        }
+        // ---- raw interiors of the 4 rows (copied during the previous pack) ----
+        cp_async_wait_prev();
         __syncwarp();
         // folded right-hand side at (fold index k, block blk) of column `col` (row col / 2, part col % 2)
         auto fold_at = [&](int col, int blk, int k) -> double {
@@ -1131,9 +1150,9 @@ __global__ void __launch_bounds__(TC_WARPS * 32, 2) fdm_tc_refine_kernel(FdmArgs
                 const double bs0 = col[k0], bs1 = col[k1], ba0 = col[TC_LD + k0], ba1 = col[TC_LD + k1];
 #pragma unroll
                 for (int mt = 0; mt < TC_MT; ++mt) {
-                    const size_t f = ((size_t)(mt * TC_KS + kk) * 32 + lane) * 2;
-                    dmma_16x8x8(ys[mt], Mf[f], Mf[f + 1], bs0, bs1);
-                    dmma_16x8x8(ya[mt], Mf[MBLK + f], Mf[MBLK + f + 1], ba0, ba1);
+                    const size_t f = (size_t)(mt * TC_KS + kk) * 32 + lane;
+                    dmma_16x8x8(ys[mt], Mf[f], Mf[MPLANE + f], bs0, bs1);
+                    dmma_16x8x8(ya[mt], Mf[2 * MPLANE + f], Mf[3 * MPLANE + f], ba0, ba1);
                 }
             }
         }
@@ -1190,8 +1209,9 @@ __global__ void __launch_bounds__(TC_WARPS * 32, 2) fdm_tc_refine_kernel(FdmArgs
             xdi[r][0] = Xd[(2 * r + 1) * TC_S + TC_LD + lane];
         }
         fdm_store_rows<double, 1, RPW, ADJ>(a, spec, rowid, grp, ok, xsr, xsi, xdr, xdi, lane);
-        __syncwarp();
+        __syncwarp();  // this region is refilled by the copy issued in the next iteration
     }
+    cp_async_wait_all();
 }
 
 int launch_fdm_tc_refine(const FdmArgs& a, cudaStream_t s)
@@ -1249,10 +1269,13 @@ void fdm_tc_swizzle(const double* cm, int ld, float* out)
     }
 }
 
-// Two FP64 column-major blocks in the m16n8k8 .f64 A-fragment order.
+// Two FP64 column-major blocks in the m16n8k8 .f64 A-fragment order, each block
+// as two planes [2][ld/16][ld/8][32][2]: (a0, a1) of every lane, then (a2, a3),
+// so that a warp's 16-byte loads of one plane are contiguous.
 void fdm_m16_swizzle2(const double* cm, int ld, double* out)
 {
     const int MT = ld / 16, KS = ld / 8;
+    const size_t plane = (size_t)ld * ld / 2;
     for (int b = 0; b < 2; ++b) {
         const double* M = cm + (size_t)b * ld * ld;
         double* O = out + (size_t)b * ld * ld;
@@ -1261,11 +1284,11 @@ void fdm_m16_swizzle2(const double* cm, int ld, double* out)
                 for (int l = 0; l < 32; ++l) {
                     const int gg = l >> 2, qq = l & 3;
                     const int i0 = mt * 16 + gg, i1 = i0 + 8, k0 = kk * 8 + qq, k1 = k0 + 4;
-                    double* o = O + (((size_t)mt * KS + kk) * 32 + l) * 4;
-                    o[0] = M[(size_t)k0 * ld + i0];
-                    o[1] = M[(size_t)k0 * ld + i1];
-                    o[2] = M[(size_t)k1 * ld + i0];
-                    o[3] = M[(size_t)k1 * ld + i1];
+                    const size_t f = (((size_t)mt * KS + kk) * 32 + l) * 2;
+                    O[f] = M[(size_t)k0 * ld + i0];
+                    O[f + 1] = M[(size_t)k0 * ld + i1];
+                    O[plane + f] = M[(size_t)k1 * ld + i0];
+                    O[plane + f + 1] = M[(size_t)k1 * ld + i1];
                 }
     }
 }

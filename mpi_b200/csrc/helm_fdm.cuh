@@ -47,6 +47,6 @@ void fdm_mma16_swizzle(const double* cm, int ld, double* out);
 // tensor products, FP64 residual on the FP64 tensor cores.
 int launch_fdm_tc_refine(const FdmArgs& a, cudaStream_t s);
 void fdm_tc_swizzle(const double* cm, int ld, float* out);    // [4][2][ld/16][ld/8][32][4]
-void fdm_m16_swizzle2(const double* cm, int ld, double* out);  // [2][ld/16][ld/8][32][4]
+void fdm_m16_swizzle2(const double* cm, int ld, double* out);  // [2 blocks][2 planes][ld/16][ld/8][32][2]
 
 }  // namespace helm
