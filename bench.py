@@ -217,6 +217,24 @@ def run_reference_arm(args, ws, rank):
 
 
 # ------------------------------------------------------------------- ours --
+def rank_max(times, ws, device):
+    """Element-wise max of per-rank timings over the process group (the replica
+    whose GPU finished last sets the job time); the input list when ws == 1."""
+    import torch
+
+    t = torch.tensor([float(v) for v in times], dtype=torch.float64, device=device)
+    if ws > 1:
+        import torch.distributed as dist
+
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return [float(v) for v in t.cpu()]
+
+
+def job_gdofs(dof_per_rank, ws, ms_per_step):
+    """Whole-job throughput of ws replicas, each solving dof_per_rank per step."""
+    return ws * dof_per_rank / (ms_per_step * 1e-3) / 1e9
+
+
 def _peak_hbm():
     try:
         with open(os.path.join(HERE, "MEASURED_PEAKS.json")) as fh:
@@ -363,16 +381,11 @@ def run_ours(args, ws, rank, local):
         st, wu = max(3, min(args.steps, 20)), 3
         side["batch"] = _leg_batch(dev, flush, stream, st, wu, cpu=not args.skip_cpu_baseline)
         side["adjoint"] = _leg_adjoint(dev, flush, stream, max(st, 50), wu)
-        side["fd"] = _leg_fd(dev, flush, stream, st, wu)
+        side["fd"] = _leg_fd(dev, flush, stream, st, wu, cpu=not args.skip_cpu_baseline)
     clk = clocks.stop()
 
     # max over ranks
-    tmax = torch.tensor([res["fp32_refine"], res["fp64"], e2e_ms], dtype=torch.float64, device=dev)
-    if ws > 1:
-        import torch.distributed as dist
-
-        dist.all_reduce(tmax, op=dist.ReduceOp.MAX)
-    t_ref, t_64, t_e2e = [float(v) for v in tmax.cpu()]
+    t_ref, t_64, t_e2e = rank_max([res["fp32_refine"], res["fp64"], e2e_ms], ws, dev)
     ms_ref, ms_64, ms_e2e = t_ref / args.steps, t_64 / args.steps, t_e2e / args.steps
 
     # accuracy of the refined solve against the FP64 solve (and the reference below)
@@ -390,7 +403,7 @@ def run_ours(args, ws, rank, local):
         traffic = _traffic_from_profiles(dom)
         line = {
             "metric": METRIC,
-            "value": ws * dof / (ms_ref * 1e-3) / 1e9,
+            "value": job_gdofs(dof, ws, ms_ref),
             "unit": "GDOF/s",
             "n_gpus": ws,
             "steps": args.steps,
@@ -508,7 +521,42 @@ def _leg_batch(dev, flush, stream, steps, warmup, cpu):
                                    "sample": "the reference's SolvePDE of each of the 512 problems, one core, "
                                              "its own SolvePDE clock summed"}
             out["max_rel_l2_refine_vs_reference"] = max(errs)
+            # the same 512 reference solves spread over the host's cores (spawned
+            # processes, one share each; wall time of the pool's map, pool warm)
+            import multiprocessing as mp
+
+            cores = max(1, min(os.cpu_count() or 1, 64))
+            if cores > 1:
+                shares = [list(range(i, len(Nx), cores)) for i in range(cores)]
+                with mp.get_context("spawn").Pool(cores, initializer=_ref_worker_init) as pool:
+                    pool.map(_ref_batch_share, [[0]] * cores)
+                    t0 = time.perf_counter()
+                    pool.map(_ref_batch_share, shares)
+                    wall = time.perf_counter() - t0
+                out["cpu_baseline_all_cores"] = {"value": dof / wall / 1e9, "unit": "GDOF/s", "cores": cores,
+                                                 "kind": "reference",
+                                                 "sample": "the 512 reference SolvePDE calls split over the cores, "
+                                                           "wall time"}
     return out
+
+
+_REF_CACHE = {}
+
+
+def _ref_batch_share(idx):
+    """The reference's plan + SolvePDE for the listed problems of the 512-problem batch."""
+    import numpy as np
+
+    from mpi_b200 import workloads as W
+    from oracle import oracle as O
+
+    if "batch" not in _REF_CACHE:  # generated once per worker (the warm-up map)
+        _REF_CACHE["batch"] = W.batch_2d(512, seed=1237)
+    Nx, P, lam, fs, _ = _REF_CACHE["batch"]
+    for i in idx:
+        z = np.zeros(fs[i].shape[0])
+        O.ref_solve2d(fs[i], z, z, xl=0.0, xr=2 * math.pi, yl=-1.0, yr=1.0, lam=lam[i])
+    return len(idx)
 
 
 def _leg_adjoint(dev, flush, stream, steps, warmup):
@@ -538,7 +586,7 @@ def _leg_adjoint(dev, flush, stream, steps, warmup):
     return out
 
 
-def _leg_fd(dev, flush, stream, steps, warmup):
+def _leg_fd(dev, flush, stream, steps, warmup, cpu=False):
     import torch
 
     from mpi_b200 import Helmholtz3DFD
@@ -558,6 +606,23 @@ def _leg_fd(dev, flush, stream, steps, warmup):
         us[prec] = u
         p.DestroyPDEPlan()
     out["rel_l2_fp32_vs_fp64"] = float((us["fp32"] - us["fp64"]).norm() / us["fp64"].norm())
+    if cpu:
+        # no reference implementation of a direct FD solve exists (HypreFDM is
+        # iterative and needs HYPRE): the C restatement on one core, 256 x 256 x 256
+        import numpy as np
+
+        from oracle import oracle as O
+
+        O.build()
+        n = 256
+        fs = W.smooth_field_fd(n, n, Nz, seed=1239)
+        z = np.zeros((n, n))
+        t0 = time.perf_counter()
+        O.fd3d_solve(fs, z, z, Lx=1.0, Ly=1.0, Lz=1.0, lam=1.0)
+        t = time.perf_counter() - t0
+        out["cpu_baseline"] = {"value": n * n * Nz / t / 1e9, "unit": "GDOF/s", "cores": 1, "kind": "port",
+                               "sample": "the C restatement's FFT/tridiagonal solve of 256 x 256 x 256 (the "
+                                         "workload's z size, 1/16 of its x-y plane), one core"}
     return out
 
 
