@@ -153,17 +153,28 @@ class ClockSampler:
 
 # ------------------------------------------------------------- reference --
 def _ref_worker_init():
+    # one thread per worker process (the reference is single-threaded; numpy's
+    # BLAS would otherwise start a pool per process)
+    for v in ("OMP_NUM_THREADS", "OPENBLAS_NUM_THREADS", "MKL_NUM_THREADS"):
+        os.environ[v] = "1"
     sys.path.insert(0, HERE)
 
 
+_REF_CACHE = {}
+
+
 def _ref_solve_slab(ny: int):
-    """One reference SolvePDE of the 256 x ny x 65 slab of the workload (seeded)."""
+    """One reference SolvePDE of the 256 x ny x 65 slab of the workload (seeded;
+    the input is generated once per worker process)."""
     import numpy as np
 
     from mpi_b200 import workloads as W
     from oracle import oracle as O
 
-    f = W.smooth_field_3d(NX, ny, NGLL, seed=SEED)
+    key = ("slab", ny)
+    if key not in _REF_CACHE:
+        _REF_CACHE[key] = W.smooth_field_3d(NX, ny, NGLL, seed=SEED)
+    f = _REF_CACHE[key]
     z = np.zeros((NX, ny))
     t = time.perf_counter()
     if O.have_reference():
@@ -217,6 +228,15 @@ def run_reference_arm(args, ws, rank):
 
 
 # ------------------------------------------------------------------- ours --
+_T0 = time.perf_counter()
+
+
+def _log(msg):
+    """Progress with elapsed wall time, on stderr (the JSON line goes to stdout)."""
+    sys.stderr.write(f"[bench {time.perf_counter() - _T0:7.1f} s] {msg}\n")
+    sys.stderr.flush()
+
+
 def rank_max(times, ws, device):
     """Element-wise max of per-rank timings over the process group (the replica
     whose GPU finished last sets the job time); the input list when ws == 1."""
@@ -379,9 +399,13 @@ def run_ours(args, ws, rank, local):
     side = {}
     if ws == 1 and not args.skip_side:
         st, wu = max(3, min(args.steps, 20)), 3
+        _log("headline done")
         side["batch"] = _leg_batch(dev, flush, stream, st, wu, cpu=not args.skip_cpu_baseline)
+        _log("batch leg done")
         side["adjoint"] = _leg_adjoint(dev, flush, stream, max(st, 50), wu)
+        _log("adjoint leg done")
         side["fd"] = _leg_fd(dev, flush, stream, st, wu, cpu=not args.skip_cpu_baseline)
+        _log("fd leg done")
     clk = clocks.stop()
 
     # max over ranks
@@ -435,6 +459,7 @@ def run_ours(args, ws, rank, local):
         line.update(side)
         if not args.skip_cpu_baseline and ws == 1:
             line["cpu_baseline"], ref_u = _cpu_baseline(fnp)
+            _log("cpu baseline done")
             line["rel_l2_refine_vs_reference"] = float(np.linalg.norm(u32.cpu().numpy() - ref_u) / np.linalg.norm(ref_u))
             line["rel_l2_fp64_vs_reference"] = float(np.linalg.norm(u64.cpu().numpy() - ref_u) / np.linalg.norm(ref_u))
         print(json.dumps(line), flush=True)
@@ -538,9 +563,6 @@ def _leg_batch(dev, flush, stream, steps, warmup, cpu):
                                                  "sample": "the 512 reference SolvePDE calls split over the cores, "
                                                            "wall time"}
     return out
-
-
-_REF_CACHE = {}
 
 
 def _ref_batch_share(idx):
