@@ -150,8 +150,11 @@ int helm_plan_stage_times(helm_plan_t plan, float* ms5);
 
 /* Kernel launch variants of the plan: fft4[i] (0..7) for the x, y, inverse y
  * and inverse x FFT passes -- bit 0: 128-thread CTAs, bit 1: radix-8 schedule
- * (lengths 128, 256), bit 2: persistent pipelined pass -- and rows (0..1) for
- * the row solve (1: half as many rows per warp).  Plan creation times every
+ * (lengths 128, 256), bit 2: persistent pipelined pass -- and rows (0..2) for
+ * the row solve (1: the second kernel shape; 2: FP64 3D plans with one element,
+ * at most 65 GLL points and Ny in {64, 128, 256} only -- the y pass, the row
+ * solve and the inverse y pass fused into one kernel per kx slab, the two y
+ * entries of fft4 then unused).  Plan creation times every
  * variant on the plan's own shape and keeps the fastest per stage (environment
  * HELM_AUTOTUNE=0: all 0).  Setting them pins the choice, e.g. to reproduce a
  * run bit for bit.  Every variant computes the same transform; the last bits

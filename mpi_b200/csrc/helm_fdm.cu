@@ -20,6 +20,7 @@
 #include "helm_device.cuh"
 #include "helm_fdm.cuh"
 
+#include <cooperative_groups.h>
 #include <cstdint>
 #include <cstring>
 
@@ -142,11 +143,11 @@ __device__ __forceinline__ void fdm_folded_core(const TF* Ws, const TF* Vs, cons
 // Epilogue of a folded solve for RPW rows: boundary values (Robin / interface
 // data, or the transposed 2x2 system of the adjoint), unfold, store.  x* hold
 // the folded solution, lane l owning fold index l + 32 t.
-template <typename TS, int NSS, int RPW, bool ADJ>
-__device__ __forceinline__ void fdm_store_rows(const FdmArgs& a, cplx_t<TS>* spec, const int (&rowid)[RPW],
-                                               const int (&grp)[RPW], const bool (&ok)[RPW],
-                                               const TS (&xsr)[RPW][NSS], const TS (&xsi)[RPW][NSS],
-                                               const TS (&xdr)[RPW][NSS], const TS (&xdi)[RPW][NSS], int lane)
+template <typename TS, int NSS, int RPW, bool ADJ, typename RowOf>
+__device__ __forceinline__ void fdm_store_rows_at(const FdmArgs& a, RowOf row_of, const int (&grp)[RPW],
+                                                  const bool (&ok)[RPW], const TS (&xsr)[RPW][NSS],
+                                                  const TS (&xsi)[RPW][NSS], const TS (&xdr)[RPW][NSS],
+                                                  const TS (&xdi)[RPW][NSS], int lane)
 {
     using CS = cplx_t<TS>;
     const int ld = a.ld, ms = a.ms, ma = a.ma, m = a.m, n = a.n, P = a.P;
@@ -154,7 +155,7 @@ __device__ __forceinline__ void fdm_store_rows(const FdmArgs& a, cplx_t<TS>* spe
 #pragma unroll
     for (int r = 0; r < RPW; ++r) {
         if (!ok[r]) continue;  // warp-uniform
-        CS* row = spec + (long long)rowid[r] * P;
+        const auto row = row_of(r);
         const int g = grp[r];
         TS zlr = 0, zli = 0, zrr = 0, zri = 0;   // boundary values of the row (weights of hl / hr)
         const bool bnd = a.hvec != nullptr;
@@ -176,7 +177,7 @@ __device__ __forceinline__ void fdm_store_rows(const FdmArgs& a, cplx_t<TS>* spe
                 }
             }
             p0r = wsum(p0r); p0i = wsum(p0i); pNr = wsum(pNr); pNi = wsum(pNi);
-            const CS wl = row[0], wr = row[P - 1];
+            const CS wl = row.get(0), wr = row.get(P - 1);
             const double* sc = a.hscal + (size_t)g * 4;
             if (!ADJ) {
                 // Robin ends, one element (NonPeriodic3D_MPI.cpp:334-336, 357-367, 528-529)
@@ -213,22 +214,41 @@ __device__ __forceinline__ void fdm_store_rows(const FdmArgs& a, cplx_t<TS>* spe
                     lo_r += zlr * l0 + zrr * r0; lo_i += zli * l0 + zri * r0;
                     hi_r += zlr * l1 + zrr * r1; hi_i += zli * l1 + zri * r1;
                 }
-                row[1 + k] = mk(lo_r, lo_i);
-                row[n - k] = mk(hi_r, hi_i);
+                row.put(1 + k, mk(lo_r, lo_i));
+                row.put(n - k, mk(hi_r, hi_i));
             } else if (k < ms) {
                 TS mr = xsr[r][t], mi = xsi[r][t];
                 if (hadd) {
                     const TS l0 = (TS)hl[1 + k], r0 = (TS)hr[1 + k];
                     mr += zlr * l0 + zrr * r0; mi += zli * l0 + zri * r0;
                 }
-                row[1 + k] = mk(mr, mi);
+                row.put(1 + k, mk(mr, mi));
             }
         }
         if (lane == 0) {
-            row[0] = mk(zlr, zli);
-            row[P - 1] = mk(zrr, zri);
+            row.put(0, mk(zlr, zli));
+            row.put(P - 1, mk(zrr, zri));
         }
     }
+}
+
+// One spectrum row in global memory (complex values at GLL slots 0 .. P-1).
+template <typename CS>
+struct GlobalRow {
+    CS* p;
+    __device__ __forceinline__ CS get(int k) const { return p[k]; }
+    __device__ __forceinline__ void put(int k, CS v) const { p[k] = v; }
+};
+
+template <typename TS, int NSS, int RPW, bool ADJ>
+__device__ __forceinline__ void fdm_store_rows(const FdmArgs& a, cplx_t<TS>* spec, const int (&rowid)[RPW],
+                                               const int (&grp)[RPW], const bool (&ok)[RPW],
+                                               const TS (&xsr)[RPW][NSS], const TS (&xsi)[RPW][NSS],
+                                               const TS (&xdr)[RPW][NSS], const TS (&xdi)[RPW][NSS], int lane)
+{
+    fdm_store_rows_at<TS, NSS, RPW, ADJ>(
+        a, [&](int r) { return GlobalRow<cplx_t<TS>>{spec + (long long)rowid[r] * a.P}; }, grp, ok, xsr, xsi, xdr, xdi,
+        lane);
 }
 
 template <typename TS, typename TF, int NSS, int RPW, bool REFINE, bool ADJ>
@@ -507,6 +527,109 @@ __device__ __forceinline__ void mma_issue_pack(const FdmArgs& a, long long pk, d
     }
 }
 
+// The folded FP64 solve of RPW = 4 NT rows staged in stg (row r's interior at
+// stg + r RSD, complex i at 2 i), both transforms on the FP64 tensor cores
+// (mma.sync m8n8k4).  On return stg holds the folded solution: row r's
+// symmetric block at stg + r RSD + 2 i, its antisymmetric block at + 2 (LD + i).
+// gq[t]: shift group of row 4 t + (lane % 4).
+template <int NT, int MT, int KS, int RSD, int LD>
+__device__ __forceinline__ void mma_fold_solve(const double* A, const double* recip, double* stg, const int (&gq)[NT],
+                                               int n, int m, int ms, int lane)
+{
+    const int g = lane >> 2, q = lane & 3;
+    const double r2 = 0.70710678118654752440;
+    const double* As1 = A;                           // first transform, symmetric block
+    const double* As2 = A + (size_t)LD * LD;         // second transform, symmetric block
+    const double* Aa1 = A + (size_t)2 * LD * LD;     // first transform, antisymmetric block
+    const double* Aa2 = A + (size_t)3 * LD * LD;     // second transform, antisymmetric block
+    // ---- first transform; B fragments folded on the fly ----
+    double cs[NT][MT][2], ca[NT][MT][2];
+#pragma unroll
+    for (int t = 0; t < NT; ++t)
+#pragma unroll
+        for (int mt = 0; mt < MT; ++mt) cs[t][mt][0] = cs[t][mt][1] = ca[t][mt][0] = ca[t][mt][1] = 0.0;
+#pragma unroll 2
+    for (int kk = 0; kk < KS; ++kk) {
+        const int k = 4 * kk + q;
+        double bs[NT], ba[NT];
+#pragma unroll
+        for (int t = 0; t < NT; ++t) {
+            const double* raw = stg + (4 * t + (g >> 1)) * RSD + (g & 1);
+            double vs = 0.0, va = 0.0;
+            if (k < m) {
+                const double lo = raw[2 * k], hi = raw[2 * (n - 1 - k)];
+                vs = r2 * (lo + hi);
+                va = r2 * (lo - hi);
+            } else if (k < ms) {
+                vs = raw[2 * k];
+            }
+            bs[t] = vs;
+            ba[t] = va;
+        }
+#pragma unroll
+        for (int mt = 0; mt < MT; ++mt) {
+            const double as = As1[(mt * KS + kk) * 32 + lane];
+            const double aa = Aa1[(mt * KS + kk) * 32 + lane];
+#pragma unroll
+            for (int t = 0; t < NT; ++t) {
+                dmma_8x8x4(cs[t][mt][0], cs[t][mt][1], as, bs[t]);
+                dmma_8x8x4(ca[t][mt][0], ca[t][mt][1], aa, ba[t]);
+            }
+        }
+    }
+    // ---- scale by 1 / (lambda_j - sigma) of each row's shift; stage as the next B ----
+    __syncwarp();
+#pragma unroll
+    for (int t = 0; t < NT; ++t) {
+        const int r = 4 * t + q;
+        const double* rc = recip + (size_t)gq[t] * 2 * LD;
+#pragma unroll
+        for (int mt = 0; mt < MT; ++mt) {
+            const int i = mt * 8 + g;
+            const double s = rc[i], u = rc[LD + i];
+            *reinterpret_cast<double2*>(stg + r * RSD + 2 * i) = make_double2(cs[t][mt][0] * s, cs[t][mt][1] * s);
+            *reinterpret_cast<double2*>(stg + r * RSD + 2 * (LD + i)) =
+                make_double2(ca[t][mt][0] * u, ca[t][mt][1] * u);
+            cs[t][mt][0] = cs[t][mt][1] = ca[t][mt][0] = ca[t][mt][1] = 0.0;
+        }
+    }
+    __syncwarp();
+    // ---- second transform ----
+#pragma unroll 2
+    for (int kk = 0; kk < KS; ++kk) {
+        const int k = 4 * kk + q;
+        double bs[NT], ba[NT];
+#pragma unroll
+        for (int t = 0; t < NT; ++t) {
+            const double* c = stg + (4 * t + (g >> 1)) * RSD + (g & 1);
+            bs[t] = c[2 * k];
+            ba[t] = c[2 * (LD + k)];
+        }
+#pragma unroll
+        for (int mt = 0; mt < MT; ++mt) {
+            const double as = As2[(mt * KS + kk) * 32 + lane];
+            const double aa = Aa2[(mt * KS + kk) * 32 + lane];
+#pragma unroll
+            for (int t = 0; t < NT; ++t) {
+                dmma_8x8x4(cs[t][mt][0], cs[t][mt][1], as, bs[t]);
+                dmma_8x8x4(ca[t][mt][0], ca[t][mt][1], aa, ba[t]);
+            }
+        }
+    }
+    __syncwarp();
+#pragma unroll
+    for (int t = 0; t < NT; ++t) {
+        const int r = 4 * t + q;
+#pragma unroll
+        for (int mt = 0; mt < MT; ++mt) {
+            const int i = mt * 8 + g;
+            *reinterpret_cast<double2*>(stg + r * RSD + 2 * i) = make_double2(cs[t][mt][0], cs[t][mt][1]);
+            *reinterpret_cast<double2*>(stg + r * RSD + 2 * (LD + i)) = make_double2(ca[t][mt][0], ca[t][mt][1]);
+        }
+    }
+    __syncwarp();
+}
+
 template <int NSS, int NT, int WARPS, bool ADJ>
 __global__ void __launch_bounds__(WARPS * 32, (NSS == 1 ? 2 : 1)) fdm_mma_kernel(FdmArgs a)
 {
@@ -515,7 +638,7 @@ __global__ void __launch_bounds__(WARPS * 32, (NSS == 1 ? 2 : 1)) fdm_mma_kernel
     extern __shared__ __align__(16) double dsm[];
     double* A = dsm;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const int g = lane >> 2, q = lane & 3;
+    const int q = lane & 3;
     double* stg_base = dsm + S::mats + (size_t)warp * 2 * RPW * RSD;
     {
         const double2* src = reinterpret_cast<const double2*>(a.mma_mats);
@@ -526,13 +649,8 @@ __global__ void __launch_bounds__(WARPS * 32, (NSS == 1 ? 2 : 1)) fdm_mma_kernel
     __syncthreads();
 
     cplx_t<double>* spec = static_cast<cplx_t<double>*>(a.spec);
-    const int n = a.n, m = a.m, ms = a.ms, P = a.P, nrows = a.nrows;
-    const double r2 = 0.70710678118654752440;
+    const int n = a.n, m = a.m, ms = a.ms, nrows = a.nrows;
     const long long npacks = (nrows + RPW - 1) / RPW;
-    const double* As1 = A;                           // first transform, symmetric block
-    const double* As2 = A + (size_t)LD * LD;         // second transform, symmetric block
-    const double* Aa1 = A + (size_t)2 * LD * LD;     // first transform, antisymmetric block
-    const double* Aa2 = A + (size_t)3 * LD * LD;     // second transform, antisymmetric block
 
     const long long pstride = (long long)gridDim.x * WARPS;
     long long pk = (long long)blockIdx.x * WARPS + warp;
@@ -555,94 +673,13 @@ __global__ void __launch_bounds__(WARPS * 32, (NSS == 1 ? 2 : 1)) fdm_mma_kernel
         // ---- the staged interiors of this pack's rows ----
         cp_async_wait_prev();
         __syncwarp();
-        // ---- first transform; B fragments folded on the fly ----
-        double cs[NT][MT][2], ca[NT][MT][2];
-#pragma unroll
-        for (int t = 0; t < NT; ++t)
-#pragma unroll
-            for (int mt = 0; mt < MT; ++mt) cs[t][mt][0] = cs[t][mt][1] = ca[t][mt][0] = ca[t][mt][1] = 0.0;
-#pragma unroll 2
-        for (int kk = 0; kk < KS; ++kk) {
-            const int k = 4 * kk + q;
-            double bs[NT], ba[NT];
-#pragma unroll
-            for (int t = 0; t < NT; ++t) {
-                const double* raw = stg + (4 * t + (g >> 1)) * RSD + (g & 1);
-                double vs = 0.0, va = 0.0;
-                if (k < m) {
-                    const double lo = raw[2 * k], hi = raw[2 * (n - 1 - k)];
-                    vs = r2 * (lo + hi);
-                    va = r2 * (lo - hi);
-                } else if (k < ms) {
-                    vs = raw[2 * k];
-                }
-                bs[t] = vs;
-                ba[t] = va;
-            }
-#pragma unroll
-            for (int mt = 0; mt < MT; ++mt) {
-                const double as = As1[(mt * KS + kk) * 32 + lane];
-                const double aa = Aa1[(mt * KS + kk) * 32 + lane];
-#pragma unroll
-                for (int t = 0; t < NT; ++t) {
-                    dmma_8x8x4(cs[t][mt][0], cs[t][mt][1], as, bs[t]);
-                    dmma_8x8x4(ca[t][mt][0], ca[t][mt][1], aa, ba[t]);
-                }
-            }
-        }
-        // ---- scale by 1 / (lambda_j - sigma) of each row's shift; stage as the next B ----
-        __syncwarp();
+        int gq[NT];
 #pragma unroll
         for (int t = 0; t < NT; ++t) {
-            const int r = 4 * t + q;
-            const long long rr = pk * RPW + r;
-            const int gr = a.row_grp[rr < nrows ? rr : 0];
-            const double* rc = static_cast<const double*>(a.recip) + (size_t)gr * 2 * LD;
-#pragma unroll
-            for (int mt = 0; mt < MT; ++mt) {
-                const int i = mt * 8 + g;
-                const double s = rc[i], u = rc[LD + i];
-                *reinterpret_cast<double2*>(stg + r * RSD + 2 * i) = make_double2(cs[t][mt][0] * s, cs[t][mt][1] * s);
-                *reinterpret_cast<double2*>(stg + r * RSD + 2 * (LD + i)) =
-                    make_double2(ca[t][mt][0] * u, ca[t][mt][1] * u);
-                cs[t][mt][0] = cs[t][mt][1] = ca[t][mt][0] = ca[t][mt][1] = 0.0;
-            }
+            const long long rr = pk * RPW + 4 * t + q;
+            gq[t] = a.row_grp[rr < nrows ? rr : 0];
         }
-        __syncwarp();
-        // ---- second transform ----
-#pragma unroll 2
-        for (int kk = 0; kk < KS; ++kk) {
-            const int k = 4 * kk + q;
-            double bs[NT], ba[NT];
-#pragma unroll
-            for (int t = 0; t < NT; ++t) {
-                const double* c = stg + (4 * t + (g >> 1)) * RSD + (g & 1);
-                bs[t] = c[2 * k];
-                ba[t] = c[2 * (LD + k)];
-            }
-#pragma unroll
-            for (int mt = 0; mt < MT; ++mt) {
-                const double as = As2[(mt * KS + kk) * 32 + lane];
-                const double aa = Aa2[(mt * KS + kk) * 32 + lane];
-#pragma unroll
-                for (int t = 0; t < NT; ++t) {
-                    dmma_8x8x4(cs[t][mt][0], cs[t][mt][1], as, bs[t]);
-                    dmma_8x8x4(ca[t][mt][0], ca[t][mt][1], aa, ba[t]);
-                }
-            }
-        }
-        __syncwarp();
-#pragma unroll
-        for (int t = 0; t < NT; ++t) {
-            const int r = 4 * t + q;
-#pragma unroll
-            for (int mt = 0; mt < MT; ++mt) {
-                const int i = mt * 8 + g;
-                *reinterpret_cast<double2*>(stg + r * RSD + 2 * i) = make_double2(cs[t][mt][0], cs[t][mt][1]);
-                *reinterpret_cast<double2*>(stg + r * RSD + 2 * (LD + i)) = make_double2(ca[t][mt][0], ca[t][mt][1]);
-            }
-        }
-        __syncwarp();
+        mma_fold_solve<NT, MT, KS, RSD, LD>(A, static_cast<const double*>(a.recip), stg, gq, n, m, ms, lane);
         // ---- folded solution to the lane-per-fold-index layout, epilogue ----
         double xsr[RPW][NSS], xsi[RPW][NSS], xdr[RPW][NSS], xdi[RPW][NSS];
 #pragma unroll
@@ -903,6 +940,223 @@ void fdm_mma16_swizzle(const double* cm, int ld, double* out)
                     o[3] = M[(size_t)k1 * ld + i1];
                 }
     }
+}
+
+// ============== fused y-FFT + row solve + inverse y-FFT, one slab per cluster ==
+//
+// For 3D FP64 plans with one GLL element and up to 65 points: the spectrum
+// rows of one kx (a slab [Ny][P] complex, 266 KB at Ny = 256, P = 65) live in
+// the shared memory of a cluster of two CTAs, CTA c holding the GLL columns
+// [c H0, ...) of every ky.  Each CTA transforms its columns along y in shared
+// memory, the pair meets at a cluster barrier, each CTA solves half of the ky
+// rows -- gathering a row's two halves through distributed shared memory,
+// solving it with mma_fold_solve and writing the result back to both halves --
+// and after a second barrier each CTA transforms its columns back and stores
+// them.  The spectrum crosses the memory system once instead of three times
+// (y pass, row solve, inverse y pass), and two launches disappear.
+
+struct SlabArgs {
+    int H0, HS;            // columns of CTA 0; shared-memory row stride of a half (complex)
+    const void* tw;        // y twiddles exp(-2 pi i e / Ny), FP64 complex
+    const int* grp_of_row; // shift group of each spectrum row kx Ny + ky
+};
+
+template <int R, int NS, int TPC>
+__device__ __forceinline__ int slab_out_row(int tc, int t, int r)
+{
+    const int j = tc + t * TPC;
+    return (j / NS) * NS * R + (j % NS) + r * NS;
+}
+
+template <int L, int R, int NS, int TPC, int R0>
+__device__ __forceinline__ void slab_to_smem(cplx_t<double>* sm, int hs, int tc, int col, const cplx_t<double> (&v)[R0])
+{
+#pragma unroll
+    for (int t = 0; t < R0 / R; ++t)
+#pragma unroll
+        for (int r = 0; r < R; ++r) sm[slab_out_row<R, NS, TPC>(tc, t, r) * hs + col] = v[t * R + r];
+}
+
+template <int L, int R, int NS, int DIR, int TPC, int R0>
+__device__ __forceinline__ void slab_from_smem(const cplx_t<double>* sm, int hs, const cplx_t<double>* tw, int tc,
+                                               int col, cplx_t<double> (&v)[R0])
+{
+    using C = cplx_t<double>;
+#pragma unroll
+    for (int t = 0; t < R0 / R; ++t) {
+        const int j = tc + t * TPC, jm = j % NS;
+        C w8[R];
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+            C x = sm[(j + r * (L / R)) * hs + col];
+            if (NS > 1 && r > 0) {
+                const C w = tw[r * jm * (L / (NS * R))];
+                x = (DIR < 0) ? cmul(x, w) : cmulc(x, w);
+            }
+            w8[r] = x;
+        }
+        dft_reg<R, DIR, double>(w8);
+#pragma unroll
+        for (int r = 0; r < R; ++r) v[t * R + r] = w8[r];
+    }
+}
+
+// One length-L FFT (direction DIR, unscaled) of each of the ncol columns of the
+// [L][hs] complex array sm, in place; all THREADS threads of the CTA call it.
+template <int L, int DIR, int THREADS>
+__device__ __forceinline__ void slab_fft(cplx_t<double>* sm, int hs, int ncol, const cplx_t<double>* tw)
+{
+    using C = cplx_t<double>;
+    using RS = Radix<L>;
+    constexpr int R0 = RS::r0, R1 = RS::r1, R2 = RS::r2, NP = RS::n, TPC = L / R0, CPR = THREADS / TPC;
+    constexpr int RL = (NP == 1) ? R0 : (NP == 2 ? R1 : R2);
+    const int tc = threadIdx.x / CPR, cl = threadIdx.x - tc * CPR;
+    for (int c0 = 0; c0 < ncol; c0 += CPR) {
+        const int col = c0 + cl;
+        const bool on = col < ncol;
+        C v[R0];
+#pragma unroll
+        for (int r = 0; r < R0; ++r) v[r] = on ? sm[(tc + r * TPC) * hs + col] : mk(0.0, 0.0);
+        dft_reg<R0, DIR, double>(v);
+        if constexpr (NP >= 2) {
+            __syncthreads();
+            if (on) slab_to_smem<L, R0, 1, TPC, R0>(sm, hs, tc, col, v);
+            __syncthreads();
+            if (on) slab_from_smem<L, R1, R0, DIR, TPC, R0>(sm, hs, tw, tc, col, v);
+        }
+        if constexpr (NP >= 3) {
+            __syncthreads();
+            if (on) slab_to_smem<L, R1, R0, TPC, R0>(sm, hs, tc, col, v);
+            __syncthreads();
+            if (on) slab_from_smem<L, R2, R0 * R1, DIR, TPC, R0>(sm, hs, tw, tc, col, v);
+        }
+        __syncthreads();
+        if (on) slab_to_smem<L, RL, L / RL, TPC, R0>(sm, hs, tc, col, v);
+        __syncthreads();
+    }
+}
+
+// A spectrum row split over the two halves of a slab (slots k < h in a, the rest in b).
+struct SlabRow {
+    cplx_t<double>* a;
+    cplx_t<double>* b;
+    int h;
+    __device__ __forceinline__ cplx_t<double> get(int k) const { return k < h ? a[k] : b[k - h]; }
+    __device__ __forceinline__ void put(int k, cplx_t<double> v) const
+    {
+        if (k < h) a[k] = v;
+        else b[k - h] = v;
+    }
+};
+
+constexpr int SLAB_WARPS = 8, SLAB_LD = 32, SLAB_RSD = 4 * SLAB_LD + 8;
+
+inline size_t slab_smem_bytes(int L, int HS)
+{
+    return ((size_t)4 * SLAB_LD * SLAB_LD + (size_t)2 * L * HS + (size_t)SLAB_WARPS * 4 * SLAB_RSD) * sizeof(double);
+}
+
+template <int L, bool ADJ>
+__global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(SLAB_WARPS * 32, 1) slab_kernel(FdmArgs a, SlabArgs sa)
+{
+    namespace cg = cooperative_groups;
+    using C = cplx_t<double>;
+    constexpr int RPW = 4, LD = SLAB_LD, MT = LD / 8, KS = LD / 4, RSD = SLAB_RSD;
+    extern __shared__ __align__(16) double dsm[];
+    double* A = dsm;
+    C* slab = reinterpret_cast<C*>(dsm + 4 * LD * LD);
+    const int HS = sa.HS, H0 = sa.H0, P = a.P, n = a.n, m = a.m, ms = a.ms;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, q = lane & 3;
+    double* stg = dsm + 4 * LD * LD + (size_t)2 * L * HS + (size_t)warp * RPW * RSD;
+    {
+        const double2* src = reinterpret_cast<const double2*>(a.mma_mats);
+        double2* dst = reinterpret_cast<double2*>(A);
+        for (int e = threadIdx.x; e < 2 * LD * LD; e += blockDim.x) dst[e] = src[e];
+    }
+    pdl_enter();
+    cg::cluster_group cluster = cg::this_cluster();
+    const int c = (int)cluster.block_rank();
+    const int kx = blockIdx.x >> 1;
+    const int z0 = c ? H0 : 0, nz = c ? P - H0 : H0;
+    C* spec = static_cast<C*>(a.spec) + (long long)kx * L * P;
+    const C* tw = static_cast<const C*>(sa.tw);
+    for (int e = threadIdx.x; e < L * nz; e += blockDim.x) {
+        const int ky = e / nz, zc = e - ky * nz;
+        cp_async_bytes16(&slab[ky * HS + zc], &spec[(long long)ky * P + z0 + zc], true);
+    }
+    cp_async_commit();
+    cp_async_wait_all();
+    __syncthreads();
+    slab_fft<L, -1, SLAB_WARPS * 32>(slab, HS, nz, tw);
+    cluster.sync();
+
+    // ---- rows ky in [c L/2, (c+1) L/2), 4 per warp at a time ----
+    C* s0 = cluster.map_shared_rank(slab, 0);
+    C* s1 = cluster.map_shared_rank(slab, 1);
+    const int ky0 = c * (L / 2);
+    for (int pk = warp; pk < (L / 2) / RPW; pk += SLAB_WARPS) {
+        const int kyb = ky0 + pk * RPW;
+        __syncwarp();
+#pragma unroll
+        for (int r = 0; r < RPW; ++r) {
+            const SlabRow row{s0 + (kyb + r) * HS, s1 + (kyb + r) * HS, H0};
+            for (int i = lane; i < n; i += 32) *reinterpret_cast<C*>(stg + r * RSD + 2 * i) = row.get(i + 1);
+        }
+        __syncwarp();
+        int gq[1] = {sa.grp_of_row[(long long)kx * L + kyb + q]};
+        mma_fold_solve<1, MT, KS, RSD, LD>(A, static_cast<const double*>(a.recip), stg, gq, n, m, ms, lane);
+        double xsr[RPW][1], xsi[RPW][1], xdr[RPW][1], xdi[RPW][1];
+        int grp[RPW];
+        bool ok[RPW];
+#pragma unroll
+        for (int r = 0; r < RPW; ++r) {
+            const double2 vs = *reinterpret_cast<const double2*>(stg + r * RSD + 2 * lane);
+            const double2 vd = *reinterpret_cast<const double2*>(stg + r * RSD + 2 * (LD + lane));
+            xsr[r][0] = vs.x; xsi[r][0] = vs.y;
+            xdr[r][0] = vd.x; xdi[r][0] = vd.y;
+            grp[r] = sa.grp_of_row[(long long)kx * L + kyb + r];
+            ok[r] = true;
+        }
+        fdm_store_rows_at<double, 1, RPW, ADJ>(
+            a, [&](int r) { return SlabRow{s0 + (kyb + r) * HS, s1 + (kyb + r) * HS, H0}; }, grp, ok, xsr, xsi, xdr,
+            xdi, lane);
+    }
+    cluster.sync();
+    slab_fft<L, 1, SLAB_WARPS * 32>(slab, HS, nz, tw);
+    for (int e = threadIdx.x; e < L * nz; e += blockDim.x) {
+        const int ky = e / nz, zc = e - ky * nz;
+        spec[(long long)ky * P + z0 + zc] = slab[ky * HS + zc];
+    }
+}
+
+template <int L>
+static int run_slab(const FdmArgs& a, const SlabArgs& sa, int nkx, cudaStream_t s)
+{
+    auto k = a.adjoint ? slab_kernel<L, true> : slab_kernel<L, false>;
+    const size_t smem = slab_smem_bytes(L, sa.HS);
+    cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return (int)e;
+    return (int)launch_k(k, dim3(2 * nkx), dim3(SLAB_WARPS * 32), smem, s, a, sa);
+}
+
+int launch_slab(const FdmArgs& a, int Ny, int H0, int HS, const void* tw, const int* grp_of_row, int nkx,
+                cudaStream_t s)
+{
+    if (a.ld != SLAB_LD || !a.mma_mats) return (int)cudaErrorInvalidValue;
+    const SlabArgs sa{H0, HS, tw, grp_of_row};
+    switch (Ny) {
+        case 64: return run_slab<64>(a, sa, nkx, s);
+        case 128: return run_slab<128>(a, sa, nkx, s);
+        case 256: return run_slab<256>(a, sa, nkx, s);
+        default: return (int)cudaErrorInvalidValue;
+    }
+}
+
+bool slab_fits(int Ny, int P, int ld)
+{
+    if (ld != SLAB_LD || (Ny != 64 && Ny != 128 && Ny != 256)) return false;
+    const int H0 = (P + 1) / 2, HS = H0 | 1;
+    return slab_smem_bytes(Ny, HS) <= 232448;
 }
 
 // ============================== refined solve on the tensor cores ==

@@ -46,6 +46,13 @@ void fdm_mma16_swizzle(const double* cm, int ld, double* out);
 // Refined plans (ld = 32, one sweep): FP32-accurate solves as three TF32
 // tensor products, FP64 residual on the FP64 tensor cores.
 int launch_fdm_tc_refine(const FdmArgs& a, cudaStream_t s);
+// FP64 3D plans with Ns = 1, ld = 32 and Ny in {64, 128, 256}: y-FFT, row solve
+// and inverse y-FFT fused per kx slab in a cluster of two CTAs.  H0 = (P + 1) / 2
+// GLL columns in the first CTA; HS its shared-memory row stride (odd);
+// grp_of_row: the shift group of each spectrum row.
+int launch_slab(const FdmArgs& a, int Ny, int H0, int HS, const void* tw, const int* grp_of_row, int nkx,
+                cudaStream_t s);
+bool slab_fits(int Ny, int P, int ld);
 void fdm_tc_swizzle(const double* cm, int ld, float* out);    // [4][2][ld/16][ld/8][32][4]
 void fdm_m16_swizzle2(const double* cm, int ld, double* out);  // [2 blocks][2 planes][ld/16][ld/8][32][2]
 

@@ -349,6 +349,13 @@ static int setup_fast(Plan& p, const std::vector<double>& A0, int prec_code)
     if ((st = p.upload((void**)&p.d_fd2, d2f.data(), d2f.size() * sizeof(double)))) return st;
     if ((st = p.upload((void**)&p.d_fd2_adj, d2a.data(), d2a.size() * sizeof(double)))) return st;
     if ((st = p.upload((void**)&p.d_row_grp, row_grp.data(), row_grp.size() * sizeof(int)))) return st;
+    if (prec_code == 0 && p.dim == 3 && p.batch == 1 && slab_fits(p.Ny, N, ld)) {
+        std::vector<int> gor((size_t)p.nrows, 0);
+        for (int g = 0; g < G; ++g)
+            for (int rr = p.grp_start[g]; rr < p.grp_start[g + 1]; ++rr) gor[p.grp_rows[rr]] = g;
+        if ((st = p.upload((void**)&p.d_grp_of_row, gor.data(), gor.size() * sizeof(int)))) return st;
+        p.slab_ok = true;
+    }
     if ((st = p.upload((void**)&p.d_fe0, fe0.data(), fe0.size() * sizeof(double)))) return st;
     if ((st = p.upload((void**)&p.d_feN, feN.data(), feN.size() * sizeof(double)))) return st;
     if ((st = p.upload((void**)&p.d_fc0, fc0.data(), fc0.size() * sizeof(double)))) return st;
@@ -610,8 +617,10 @@ static int run_pipeline(Plan& p, const void* in, const double* gl, const double*
                        p.Ns * p.batch, 1.0, p.d_tw_x, gl, gr, !adjoint, adjoint, 0, s, adj)))
         return st;
     mark(1);
+    // FP64 3D plans may run stages 2-4 as one fused kernel per kx slab
+    const bool slab = p.row_var == 2 && p.slab_ok && p.fast && p.precision == HELM_FP64;
     // 2. y: complex-to-complex along the middle axis
-    if (p.dim == 3 &&
+    if (p.dim == 3 && !slab &&
         (st = fft_pass(p, p.Ny, FFT_C2C, -1, p.d_spec, p.d_spec, N, N, (long long)p.Ny * N, (long long)p.Ny * N, N,
                        p.Ns * nkx, 1.0, p.d_tw_y, nullptr, nullptr, false, false, 1, s)))
         return st;
@@ -709,7 +718,9 @@ static int run_pipeline(Plan& p, const void* in, const double* gl, const double*
         fa.mma16_mats = adjoint ? p.d_fmma16_adj : p.d_fmma16;
         fa.tc_mats = adjoint ? (const void*)p.d_ftc_adj : (const void*)p.d_ftc;
         fa.tc_m = adjoint ? p.d_ftcm_adj : p.d_ftcm;
-        if (prec == 0 && fa.mma_mats)
+        if (slab)
+            e = launch_slab(fa, p.Ny, (N + 1) / 2, ((N + 1) / 2) | 1, p.d_tw_y, p.d_grp_of_row, nkx, s);
+        else if (prec == 0 && fa.mma_mats)
             e = launch_fdm_mma(fa, s, p.row_var);
         else if (prec == 2 && fa.tc_mats && p.sweeps == 1 && p.row_var == 0)
             e = launch_fdm_tc_refine(fa, s);
@@ -721,7 +732,7 @@ static int run_pipeline(Plan& p, const void* in, const double* gl, const double*
     if (e) return set_cuda_error((cudaError_t)e, "row-solve launch");
     mark(3);
     // 4. inverse y
-    if (p.dim == 3 &&
+    if (p.dim == 3 && !slab &&
         (st = fft_pass(p, p.Ny, FFT_C2C, 1, p.d_spec, p.d_spec, N, N, (long long)p.Ny * N, (long long)p.Ny * N, N,
                        p.Ns * nkx, 1.0, p.d_tw_y, nullptr, nullptr, false, false, 2, s)))
         return st;
@@ -740,7 +751,7 @@ static int run_pipeline(Plan& p, const void* in, const double* gl, const double*
 // keeps the fastest per stage.  Results are cached per shape for the process;
 // HELM_AUTOTUNE=0 in the environment keeps the default variants.
 static std::mutex g_tune_mutex;
-static std::map<std::string, std::array<int, 5>> g_tune_cache;
+static std::map<std::string, std::array<int, 5>> g_tune_cache;  // 4 FFT variants, row variant
 
 static int autotune(Plan& p)
 {
@@ -801,6 +812,25 @@ static int autotune(Plan& p)
     const int stage_of_fft[4] = {0, 1, 3, 4};
     for (int i = 0; i < 4; ++i) p.fft_var[i] = pick[stage_of_fft[i]];
     p.row_var = p.fast ? pick[2] : 0;
+    if (p.slab_ok) {
+        // the fused slab kernel (row variant 2) against the separate passes, whole solves
+        float tot[2] = {0.f, 0.f};
+        const int rv[2] = {p.row_var, 2};
+        bool ok = true;
+        for (int rep = 0; rep < 5 && ok; ++rep)
+            for (int k = 0; k < 2 && ok; ++k) {
+                p.row_var = rv[k];
+                p.stage_timing = true;
+                if (solve(p, f, nullptr, nullptr, u, 0)) { ok = false; break; }
+                cudaEventSynchronize(p.ev[5]);
+                float t = 0;
+                cudaEventElapsedTime(&t, p.ev[0], p.ev[5]);
+                if (rep > 0) tot[k] += t;
+            }
+        p.stage_timing = had;
+        cudaGetLastError();
+        p.row_var = (ok && tot[1] < tot[0]) ? 2 : rv[0];
+    }
     cudaFree(f);
     cudaFree(u);
     std::lock_guard<std::mutex> lock(g_tune_mutex);
@@ -1160,10 +1190,14 @@ int helm_plan_get_launch_variants(helm_plan_t plan, int* fft4, int* rows)
 
 int helm_plan_set_launch_variants(helm_plan_t plan, const int* fft4, int rows)
 {
-    if (!plan || !fft4 || rows < 0 || rows > 1) return HELM_ERR_INVALID;
+    if (!plan || !fft4 || rows < 0 || rows > 2) return HELM_ERR_INVALID;
     for (int i = 0; i < 4; ++i)
         if (fft4[i] < 0 || fft4[i] > 7) return HELM_ERR_INVALID;
     Plan& p = *reinterpret_cast<Plan*>(plan);
+    if (rows == 2 && !p.slab_ok) {
+        helm::set_last_error("the fused slab kernel needs an FP64 3D plan with one element, at most 65 points, Ny in {64, 128, 256}");
+        return HELM_ERR_UNSUPPORTED;
+    }
     for (int i = 0; i < 4; ++i) p.fft_var[i] = fft4[i];
     p.row_var = rows;
     return HELM_OK;

@@ -94,7 +94,9 @@ struct Plan {
     void* d_cprime = nullptr;
     // autotuned launch shapes of the four FFT stages (x, y, inverse y, inverse x)
     int fft_var[4] = {0, 0, 0, 0};
-    int row_var = 0;  // launch variant of the folded row kernel
+    int row_var = 0;  // launch variant of the folded row kernel; 2: fused y-FFT / rows / inverse y (slab)
+    bool slab_ok = false;          // FP64 3D plans whose kx slab fits a two-CTA cluster
+    int* d_grp_of_row = nullptr;   // shift group of each spectrum row (slab kernel)
     bool stage_timing = false;
     cudaEvent_t ev[6] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
     std::vector<void*> allocations;

@@ -175,18 +175,21 @@ def test_linearity_full_size(cuda):
 @pytest.mark.parametrize("N", [33, 65, 129])
 @pytest.mark.parametrize("precision", ["fp64", "fp32_refine"])
 def test_every_launch_variant(cuda, N, precision):
-    """Every FFT launch variant (0..7) and both row-solve variants compute the
-    same solve: each pinned combination against the oracle (Robin ends, so the
+    """Every FFT launch variant (0..7) and every row-solve variant (including the
+    fused y-FFT / row / inverse-y slab kernel of FP64 plans) compute the same
+    solve: each pinned combination against the oracle (Robin ends, so the
     boundary epilogue runs too)."""
     rng = np.random.default_rng(N)
-    Nx, Ny, lam, bc = 16, 32, 3.0, (0.4, 1.0, 0.3, 2.0)
+    Nx, Ny, lam, bc = 16, 64, 3.0, (0.4, 1.0, 0.3, 2.0)
     f = rng.standard_normal((Nx, Ny, N))
     gl, gr = rng.standard_normal((Nx, Ny)), rng.standard_normal((Nx, Ny))
     ref = O.solve3d(f, gl, gr, Lx=1.0, Ly=1.5, Lz=2.0, lam=lam, bc=bc)
     p = NonPeriodic3D(Nx, Ny, N, N, 0.0, 1.0, 0.0, 1.5, 0.0, 2.0, Lambda=lam, bc=bc, precision=precision)
     fd, gld, grd = _dev(f), _dev(gl), _dev(gr)
+    # row variant 2 (the fused slab kernel) exists for FP64 plans with <= 65 points
+    rows = (0, 1, 2) if (precision == "fp64" and N <= 65) else (0, 1)
     for fv in range(8):
-        for rv in (0, 1):
+        for rv in rows:
             p.set_launch_variants([fv] * 4, rv)
             u = p.SolvePDE(fd, gld, grd).cpu().numpy()
             err = max_rel(u, ref) if precision == "fp64" else rel_l2(u, ref)
