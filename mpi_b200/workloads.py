@@ -121,6 +121,30 @@ def stock_3d(Nx: int = 64, Ny: int = 32, Nz: int = 250, N: int = 10, lam: float 
     return np.ascontiguousarray(f), gl, gr, np.ascontiguousarray(u), bc
 
 
+def stock_periodic_2d(Nx: int = 512, Ny: int = 512, N: int = 10, lam: float = 1.0):
+    """The reference's Periodic2D test on [0,1]^2 (periodic in both directions):
+    exact u = sin(8 pi x) cos(6 pi y).  Returns (f[Ns,Nx,N], u_exact)."""
+    Ns = math.ceil(Ny / N)
+    x = np.arange(Nx) / Nx
+    y = element_nodes(N, Ns, 1.0)
+    sx = np.sin(8 * REF_PI * x)
+    u = sx[None, :, None] * np.cos(6 * REF_PI * y)[:, None, :]
+    f = -(64 * REF_PI**2 + 36 * REF_PI**2 + lam) * u
+    return np.ascontiguousarray(f), np.ascontiguousarray(u)
+
+
+def stock_periodic_3d(Nx: int = 64, Ny: int = 32, Nz: int = 250, N: int = 10, lam: float = 1.0):
+    """The reference's Periodic3D test on [0,1]^3: u = sin(8 pi x) cos(6 pi y) cos(4 pi z)."""
+    Ns = math.ceil(Nz / N)
+    x = np.arange(Nx) / Nx
+    y = np.arange(Ny) / Ny
+    z = element_nodes(N, Ns, 1.0)
+    sxy = np.sin(8 * REF_PI * x)[:, None] * np.cos(6 * REF_PI * y)[None, :]
+    u = sxy[None, :, :, None] * np.cos(4 * REF_PI * z)[:, None, None, :]
+    f = -(64 * REF_PI**2 + 36 * REF_PI**2 + 16 * REF_PI**2 + lam) * u
+    return np.ascontiguousarray(f), np.ascontiguousarray(u)
+
+
 def smooth_field_fd(Nx: int, Ny: int, Nz: int, seed: int, kmax: int = 64) -> np.ndarray:
     """f[Nx, Ny, Nz] on the interior points of the finite-difference grid:
     Re of sum c_{kx,ky,l} e^{i(kx x + ky y)} sin(pi l z / Lz), l = 1..Nz, with

@@ -262,6 +262,83 @@ static void orc_row_solve(int N, int Ns, const double* Op, const int* piv, const
             U[jj * es + j] = phi[(size_t)jj * N + j] + zl[jj] * ul[j] + zr[jj] * ur[j];
 }
 
+/* The same row set for the solver that is periodic in the GLL direction: the
+ * particular solutions, then the cyclic interface sweep with its rank-one
+ * correction, then the combination (Periodic2D_MPI.cpp:176-223; the size == 1
+ * paths :257-283 forward, :411-444 backward, :459-461 combine).  One element:
+ * u(0) = u(L) = zeta with matching slopes.  Several: a tridiagonal sweep whose
+ * first diagonal is shifted, a second right-hand side rhs1 for the shift, and
+ * alpha = -(zl + zr) / (1 + el + er) at the last element. */
+static void orc_row_solve_periodic(int N, int Ns, const double* Op, const int* piv, const double* D,
+                                   const double* ul, const double* ur, const double* F, long es,
+                                   double* U, double* work)
+{
+    int n = N - 2;
+    double* phi = work;                    /* [Ns][N] */
+    double* b = phi + (size_t)Ns * N;      /* [Ns] each */
+    double* c = b + Ns;
+    double* r0 = c + Ns;
+    double* r1 = r0 + Ns;
+    double* zl = r1 + Ns;
+    double* zr = zl + Ns;
+    double* el = zr + Ns;
+    double* er = el + Ns;
+    const double* D0 = D;
+    const double* DN = D + (size_t)(N - 1) * N;
+    for (int jj = 0; jj < Ns; ++jj) {
+        double* p = phi + (size_t)jj * N;
+        p[0] = 0.0;
+        p[N - 1] = 0.0;
+        for (int j = 0; j < n; ++j) p[j + 1] = F[jj * es + j + 1];
+        orc_lu_solve(n, Op, piv, p + 1);
+    }
+    double d0ul = orc_dot(N, D0, ul), d0ur = orc_dot(N, D0, ur), dNul = orc_dot(N, DN, ul), dNur = orc_dot(N, DN, ur);
+    if (Ns == 1) {
+        double bb = (d0ul + d0ur) - (dNul + dNur);
+        double z = (orc_dot(N, DN, phi) - orc_dot(N, D0, phi)) / bb;
+        zl[0] = z;
+        zr[0] = z;
+    } else {
+        const double* plast = phi + (size_t)(Ns - 1) * N;
+        b[0] = dNur - dNul - d0ul;
+        c[0] = -d0ur;
+        r0[0] = orc_dot(N, D0, phi) - orc_dot(N, DN, plast);
+        r1[0] = dNul;
+        for (int jj = 1; jj < Ns; ++jj) {
+            const double* pj = phi + (size_t)jj * N;
+            const double* pp = phi + (size_t)(jj - 1) * N;
+            r0[jj] = orc_dot(N, D0, pj) - orc_dot(N, DN, pp) - (r0[jj - 1] / b[jj - 1]) * dNul;
+            if (jj < Ns - 1) {
+                b[jj] = dNur - d0ul - (c[jj - 1] / b[jj - 1]) * dNul;
+                c[jj] = -d0ur;
+                r1[jj] = -(r1[jj - 1] / b[jj - 1]) * dNul;
+            } else {
+                b[jj] = dNur - d0ul + d0ur - (c[jj - 1] / b[jj - 1]) * dNul;
+                c[jj] = 0.0;
+                r1[jj] = -d0ur - (r1[jj - 1] / b[jj - 1]) * dNul;
+            }
+        }
+        zl[Ns - 1] = r0[Ns - 1] / b[Ns - 1];
+        el[Ns - 1] = r1[Ns - 1] / b[Ns - 1];
+        for (int jj = Ns - 2; jj >= 0; --jj) {
+            zr[jj] = zl[jj + 1];
+            er[jj] = el[jj + 1];
+            zl[jj] = (r0[jj] - c[jj] * zr[jj]) / b[jj];
+            el[jj] = (r1[jj] - c[jj] * er[jj]) / b[jj];
+        }
+        zr[Ns - 1] = zl[0];
+        er[Ns - 1] = el[0];
+        double alpha = -(zl[Ns - 1] + zr[Ns - 1]) / (1.0 + el[Ns - 1] + er[Ns - 1]);
+        for (int jj = 0; jj < Ns; ++jj) {
+            zl[jj] += alpha * el[jj];
+            zr[jj] += alpha * er[jj];
+        }
+    }
+    for (int jj = 0; jj < Ns; ++jj)
+        for (int j = 0; j < N; ++j)
+            U[jj * es + j] = phi[(size_t)jj * N + j] + zl[jj] * ul[j] + zr[jj] * ur[j];
+}
+
 /* Build Dyy_int - sigma I, factor it, and form the homogeneous solutions
  * (the ConstructOperator callback of TestNonPeriodic2D_MPI.cpp:67-74 plus
  * NonPeriodic2D_MPI.cpp:194-213).  Returns the LU status. */
@@ -280,11 +357,12 @@ static int orc_operator(int N, const double* D2, double sigma, double* Op, int* 
     return 0;
 }
 
-/* 2D solve (SolvePDE, NonPeriodic2D_MPI.cpp:228-474).  Returns 0 on success,
- * 2 for a non-power-of-2 Nx, 3 for a singular operator. */
-int orc_solve2d(int Nx, int N, int Ns, double Lx, double Ly,
-                double al, double bl, double ar, double br, double lam,
-                const double* f, const double* gl, const double* gr, double* u)
+/* 2D solve (SolvePDE, NonPeriodic2D_MPI.cpp:228-474; periodic in y:
+ * Periodic2D_MPI.cpp:228-469).  Returns 0 on success, 2 for a non-power-of-2
+ * Nx, 3 for a singular operator. */
+static int orc_solve2d_impl(int Nx, int N, int Ns, double Lx, double Ly,
+                            double al, double bl, double ar, double br, double lam,
+                            const double* f, const double* gl, const double* gr, double* u, int periodic)
 {
     if (!orc_is_pow2(Nx)) return 2;
     size_t es = (size_t)Nx * N; /* element stride */
@@ -300,7 +378,7 @@ int orc_solve2d(int Nx, int N, int Ns, double Lx, double Ly,
     double* Op = malloc(sizeof(double) * N * N);
     int* piv = malloc(sizeof(int) * N);
     double* ul = malloc(sizeof(double) * N), *ur = malloc(sizeof(double) * N);
-    double* work = malloc(sizeof(double) * (Ns * (N + 5) + 8));
+    double* work = malloc(sizeof(double) * (Ns * (N + 9) + 8));
     double* Fa = malloc(sizeof(double) * Ns * N), *Ua = malloc(sizeof(double) * Ns * N);
     int status = 0;
     orc_gll_setup(N, Ns, Ly, y, D, D2);
@@ -319,8 +397,11 @@ int orc_solve2d(int Nx, int N, int Ns, double Lx, double Ly,
             const double* F = part ? Fi : Fr;
             double* U = part ? Ui : Ur;
             for (int jj = 0; jj < Ns; ++jj) memcpy(Fa + jj * N, F + jj * es + (size_t)m * N, sizeof(double) * N);
-            orc_row_solve(N, Ns, Op, piv, D, ul, ur, al, bl, ar, br, Fa, N,
-                          part ? Gli[m] : Glr[m], part ? Gri[m] : Grr[m], Ua, work);
+            if (periodic)
+                orc_row_solve_periodic(N, Ns, Op, piv, D, ul, ur, Fa, N, Ua, work);
+            else
+                orc_row_solve(N, Ns, Op, piv, D, ul, ur, al, bl, ar, br, Fa, N,
+                              part ? Gli[m] : Glr[m], part ? Gri[m] : Grr[m], Ua, work);
             for (int jj = 0; jj < Ns; ++jj) memcpy(U + jj * es + (size_t)m * N, Ua + jj * N, sizeof(double) * N);
         }
     }
@@ -334,11 +415,28 @@ done:
     return status;
 }
 
-/* 3D solve (SolvePDE, NonPeriodic3D_MPI.cpp:237-591): 2D DFT over (x, y), one
- * operator per (|kx|, |ky|), inverse DFT. */
-int orc_solve3d(int Nx, int Ny, int N, int Ns, double Lx, double Ly, double Lz,
+int orc_solve2d(int Nx, int N, int Ns, double Lx, double Ly,
                 double al, double bl, double ar, double br, double lam,
                 const double* f, const double* gl, const double* gr, double* u)
+{
+    return orc_solve2d_impl(Nx, N, Ns, Lx, Ly, al, bl, ar, br, lam, f, gl, gr, u, 0);
+}
+
+/* Periodic in y (Periodic2D_MPI.cpp SolvePDE): no boundary data. */
+int orc_psolve2d(int Nx, int N, int Ns, double Lx, double Ly, double lam, const double* f, double* u)
+{
+    double* z = calloc(Nx, sizeof(double));
+    int st = orc_solve2d_impl(Nx, N, Ns, Lx, Ly, 0.0, 1.0, 0.0, 1.0, lam, f, z, z, u, 1);
+    free(z);
+    return st;
+}
+
+/* 3D solve (SolvePDE, NonPeriodic3D_MPI.cpp:237-591; periodic in z:
+ * Periodic3D_MPI.cpp:233-866): 2D DFT over (x, y), one operator per
+ * (|kx|, |ky|), inverse DFT. */
+static int orc_solve3d_impl(int Nx, int Ny, int N, int Ns, double Lx, double Ly, double Lz,
+                            double al, double bl, double ar, double br, double lam,
+                            const double* f, const double* gl, const double* gr, double* u, int periodic)
 {
     if (!orc_is_pow2(Nx) || !orc_is_pow2(Ny)) return 2;
     size_t plane = (size_t)Ny * N, es = (size_t)Nx * plane;
@@ -355,7 +453,7 @@ int orc_solve3d(int Nx, int Ny, int N, int Ns, double Lx, double Ly, double Lz,
     double* Op = malloc(sizeof(double) * N * N);
     int* piv = malloc(sizeof(int) * N);
     double* ul = malloc(sizeof(double) * N), *ur = malloc(sizeof(double) * N);
-    double* work = malloc(sizeof(double) * (Ns * (N + 5) + 8));
+    double* work = malloc(sizeof(double) * (Ns * (N + 9) + 8));
     double* Fa = malloc(sizeof(double) * Ns * N), *Ua = malloc(sizeof(double) * Ns * N);
     int status = 0;
     orc_gll_setup(N, Ns, Lz, z, D, D2);
@@ -384,8 +482,11 @@ int orc_solve3d(int Nx, int Ny, int N, int Ns, double Lx, double Ly, double Lz,
                         const double* F = part ? Fi : Fr;
                         double* U = part ? Ui : Ur;
                         for (int kk = 0; kk < Ns; ++kk) memcpy(Fa + kk * N, F + kk * es + off, sizeof(double) * N);
-                        orc_row_solve(N, Ns, Op, piv, D, ul, ur, al, bl, ar, br, Fa, N,
-                                      part ? Gli[boff] : Glr[boff], part ? Gri[boff] : Grr[boff], Ua, work);
+                        if (periodic)
+                            orc_row_solve_periodic(N, Ns, Op, piv, D, ul, ur, Fa, N, Ua, work);
+                        else
+                            orc_row_solve(N, Ns, Op, piv, D, ul, ur, al, bl, ar, br, Fa, N,
+                                          part ? Gli[boff] : Glr[boff], part ? Gri[boff] : Grr[boff], Ua, work);
                         for (int kk = 0; kk < Ns; ++kk) memcpy(U + kk * es + off, Ua + kk * N, sizeof(double) * N);
                     }
                 }
@@ -403,6 +504,23 @@ done:
     free(Glr); free(Gli); free(Grr); free(Gri); free(Op); free(piv); free(ul); free(ur);
     free(work); free(Fa); free(Ua);
     return status;
+}
+
+int orc_solve3d(int Nx, int Ny, int N, int Ns, double Lx, double Ly, double Lz,
+                double al, double bl, double ar, double br, double lam,
+                const double* f, const double* gl, const double* gr, double* u)
+{
+    return orc_solve3d_impl(Nx, Ny, N, Ns, Lx, Ly, Lz, al, bl, ar, br, lam, f, gl, gr, u, 0);
+}
+
+/* Periodic in z (Periodic3D_MPI.cpp SolvePDE): no boundary data. */
+int orc_psolve3d(int Nx, int Ny, int N, int Ns, double Lx, double Ly, double Lz, double lam,
+                 const double* f, double* u)
+{
+    double* z = calloc((size_t)Nx * Ny, sizeof(double));
+    int st = orc_solve3d_impl(Nx, Ny, N, Ns, Lx, Ly, Lz, 0.0, 1.0, 0.0, 1.0, lam, f, z, z, u, 1);
+    free(z);
+    return st;
 }
 
 /* The collocation residual of a 3D solution, computed directly in FP64:

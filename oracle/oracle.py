@@ -5,9 +5,11 @@ Two libraries, both built by ``oracle/Makefile``:
 * ``liboracle.so`` -- the plain-C restatement (``helm_oracle.c``) of the
   reference's DirectPseudoSpectral solve and of the HypreFDM stencil solved by
   FFT/Thomas.  Always buildable (gcc only).
-* ``_ref/libref2d.so`` / ``_ref/libref3d.so`` -- the reference's own C++
-  sources compiled unchanged, wrapped by ``ref_driver2d.cpp`` /
-  ``ref_driver3d.cpp``.  Present only where the reference tree was available
+* ``_ref/libref2d.so`` / ``_ref/libref3d.so`` (and ``libref2dp.so`` /
+  ``libref3dp.so``, the solvers periodic in the GLL direction) -- the
+  reference's own C++ sources compiled unchanged, wrapped by
+  ``ref_driver2d.cpp`` / ``ref_driver3d.cpp`` / ``ref_driver2dp.cpp`` /
+  ``ref_driver3dp.cpp``.  Present only where the reference tree was available
   at build time; :func:`have_reference` says whether they were built.
 
 Only ``tests/``, ``__graft_entry__.smoke`` and the CPU-baseline leg of
@@ -29,6 +31,7 @@ _P = ctypes.POINTER(ctypes.c_double)
 _lib = None
 _ref2d = None
 _ref3d = None
+_refp = {}
 
 
 def build(quiet: bool = True) -> None:
@@ -60,6 +63,10 @@ def lib():
         _lib.orc_solve2d.argtypes = [_I, _I, _I] + [_D] * 7 + [_P] * 4
         _lib.orc_solve3d.restype = _I
         _lib.orc_solve3d.argtypes = [_I, _I, _I, _I] + [_D] * 8 + [_P] * 4
+        _lib.orc_psolve2d.restype = _I
+        _lib.orc_psolve2d.argtypes = [_I, _I, _I] + [_D] * 3 + [_P] * 2
+        _lib.orc_psolve3d.restype = _I
+        _lib.orc_psolve3d.argtypes = [_I, _I, _I, _I] + [_D] * 4 + [_P] * 2
         _lib.orc_residual3d.restype = _D
         _lib.orc_residual3d.argtypes = [_I, _I, _I] + [_D] * 8 + [_P] * 5
         _lib.orc_fd3d_solve.restype = _I
@@ -76,7 +83,8 @@ def lib():
 
 
 def have_reference() -> bool:
-    return all(os.path.exists(os.path.join(_HERE, "_ref", n)) for n in ("libref2d.so", "libref3d.so"))
+    return all(os.path.exists(os.path.join(_HERE, "_ref", n))
+               for n in ("libref2d.so", "libref3d.so", "libref2dp.so", "libref3dp.so"))
 
 
 def _ref(which: int):
@@ -92,6 +100,19 @@ def _ref(which: int):
         _ref3d.oracle_ref3d_solve.restype = _I
         _ref3d.oracle_ref3d_solve.argtypes = [_I] * 4 + [_D] * 11 + [_P] * 6
     return _ref3d
+
+
+def _ref_periodic(which: int):
+    if which not in _refp:
+        lib_ = ctypes.CDLL(os.path.join(_HERE, "_ref", f"libref{which}dp.so"))
+        if which == 2:
+            lib_.oracle_ref2dp_solve.restype = _I
+            lib_.oracle_ref2dp_solve.argtypes = [_I] * 3 + [_D] * 5 + [_P] * 4
+        else:
+            lib_.oracle_ref3dp_solve.restype = _I
+            lib_.oracle_ref3dp_solve.argtypes = [_I] * 4 + [_D] * 7 + [_P] * 4
+        _refp[which] = lib_
+    return _refp[which]
 
 
 # ------------------------------------------------------------------ grid --
@@ -131,6 +152,34 @@ def solve3d(f, gl, gr, *, Lx, Ly, Lz, lam, bc=(0.0, 1.0, 0.0, 1.0)):
     st = lib().orc_solve3d(Nx, Ny, N, Ns, Lx, Ly, Lz, *bc, lam, _p(f), _p(_c64(gl)), _p(_c64(gr)), _p(u))
     if st:
         raise RuntimeError(f"orc_solve3d status {st}")
+    return u[0] if squeeze else u
+
+
+def psolve2d(f, *, Lx, Ly, lam):
+    """Periodic in the GLL direction.  f: [Ns, Nx, N] or [Nx, N]."""
+    f = _c64(f)
+    squeeze = f.ndim == 2
+    if squeeze:
+        f = f[None]
+    Ns, Nx, N = f.shape
+    u = np.zeros_like(f)
+    st = lib().orc_psolve2d(Nx, N, Ns, Lx, Ly, lam, _p(f), _p(u))
+    if st:
+        raise RuntimeError(f"orc_psolve2d status {st}")
+    return u[0] if squeeze else u
+
+
+def psolve3d(f, *, Lx, Ly, Lz, lam):
+    """Periodic in the GLL direction.  f: [Ns, Nx, Ny, N] or [Nx, Ny, N]."""
+    f = _c64(f)
+    squeeze = f.ndim == 3
+    if squeeze:
+        f = f[None]
+    Ns, Nx, Ny, N = f.shape
+    u = np.zeros_like(f)
+    st = lib().orc_psolve3d(Nx, Ny, N, Ns, Lx, Ly, Lz, lam, _p(f), _p(u))
+    if st:
+        raise RuntimeError(f"orc_psolve3d status {st}")
     return u[0] if squeeze else u
 
 
@@ -189,6 +238,41 @@ def ref_solve3d(f, gl, gr, *, xl, xr, yl, yr, zl, zr, lam, bc=(0.0, 1.0, 0.0, 1.
     ms = np.zeros(1)
     ns = _ref(3).oracle_ref3d_solve(Nx, Ny, Ns * N, N, xl, xr, yl, yr, zl, zr, *bc, lam,
                                     _p(f), _p(_c64(gl)), _p(_c64(gr)), _p(u), _p(z), _p(ms))
+    if ns != Ns:
+        raise RuntimeError(f"reference chose Ns={ns}, expected {Ns}")
+    out = u[0] if squeeze else u
+    return (out, ms[0]) if return_time else out
+
+
+def ref_psolve2d(f, *, xl, xr, yl, yr, lam, return_time=False):
+    """The reference's own Periodic2D SolvePDE.  f: [Ns, Nx, N] or [Nx, N]."""
+    f = _c64(f)
+    squeeze = f.ndim == 2
+    if squeeze:
+        f = f[None]
+    Ns, Nx, N = f.shape
+    u = np.zeros_like(f)
+    y = np.zeros(Ns * (N - 1) + 1)
+    ms = np.zeros(1)
+    ns = _ref_periodic(2).oracle_ref2dp_solve(Nx, Ns * N, N, xl, xr, yl, yr, lam, _p(f), _p(u), _p(y), _p(ms))
+    if ns != Ns:
+        raise RuntimeError(f"reference chose Ns={ns}, expected {Ns}")
+    out = u[0] if squeeze else u
+    return (out, ms[0]) if return_time else out
+
+
+def ref_psolve3d(f, *, xl, xr, yl, yr, zl, zr, lam, return_time=False):
+    """The reference's own Periodic3D SolvePDE.  f: [Ns, Nx, Ny, N] or [Nx, Ny, N]."""
+    f = _c64(f)
+    squeeze = f.ndim == 3
+    if squeeze:
+        f = f[None]
+    Ns, Nx, Ny, N = f.shape
+    u = np.zeros_like(f)
+    z = np.zeros(Ns * (N - 1) + 1)
+    ms = np.zeros(1)
+    ns = _ref_periodic(3).oracle_ref3dp_solve(Nx, Ny, Ns * N, N, xl, xr, yl, yr, zl, zr, lam,
+                                              _p(f), _p(u), _p(z), _p(ms))
     if ns != Ns:
         raise RuntimeError(f"reference chose Ns={ns}, expected {Ns}")
     out = u[0] if squeeze else u

@@ -63,6 +63,25 @@ def main():
     out["smooth_3d"] = dict(f=f, u=u, Nx=Nx, Ny=Ny, N=N, Ns=1, dom=[0.0, 2 * math.pi, 0.0, 2 * math.pi, 0.0, 2.0],
                             lam=10.0, bc=[0.0, 1.0, 0.0, 1.0])
 
+    # solvers periodic in the GLL direction (Periodic2D_MPI.cpp, Periodic3D_MPI.cpp)
+    prng = np.random.default_rng(20240602)
+    Nx, N, Ns = 16, 9, 1
+    f = prng.standard_normal((Ns, Nx, N))
+    u = O.ref_psolve2d(f, xl=0.0, xr=1.3, yl=0.0, yr=0.8, lam=1.5)
+    out["periodic_2d"] = dict(f=f, u=u, Nx=Nx, N=N, Ns=Ns, dom=[0.0, 1.3, 0.0, 0.8], lam=1.5)
+    Nx, N, Ns = 16, 8, 4
+    f = prng.standard_normal((Ns, Nx, N))
+    u = O.ref_psolve2d(f, xl=0.0, xr=2.0, yl=0.0, yr=3.0, lam=0.6)
+    out["periodic_2d_ns4"] = dict(f=f, u=u, Nx=Nx, N=N, Ns=Ns, dom=[0.0, 2.0, 0.0, 3.0], lam=0.6)
+    Nx, Ny, N, Ns = 8, 16, 9, 1
+    f = prng.standard_normal((Ns, Nx, Ny, N))
+    u = O.ref_psolve3d(f, xl=0.0, xr=1.3, yl=0.0, yr=0.7, zl=0.0, zr=0.9, lam=2.0)
+    out["periodic_3d"] = dict(f=f, u=u, Nx=Nx, Ny=Ny, N=N, Ns=Ns, dom=[0.0, 1.3, 0.0, 0.7, 0.0, 0.9], lam=2.0)
+    Nx, Ny, N, Ns = 8, 4, 7, 3
+    f = prng.standard_normal((Ns, Nx, Ny, N))
+    u = O.ref_psolve3d(f, xl=0.0, xr=1.0, yl=0.0, yr=2.0, zl=0.0, zr=1.5, lam=0.5)
+    out["periodic_3d_ns3"] = dict(f=f, u=u, Nx=Nx, Ny=Ny, N=N, Ns=Ns, dom=[0.0, 1.0, 0.0, 2.0, 0.0, 1.5], lam=0.5)
+
     for name, d in out.items():
         np.savez_compressed(os.path.join(HERE, name + ".npz"), **{k: np.asarray(v) for k, v in d.items()})
         print(name, {k: np.asarray(v).shape for k, v in d.items()})

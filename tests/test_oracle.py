@@ -61,6 +61,50 @@ def test_reference_stock_3d_known_answer():
     assert np.abs(u - ue).max() < 1e-12
 
 
+@pytest.mark.parametrize("name", ["periodic_2d", "periodic_2d_ns4"])
+def test_periodic_restatement_matches_golden_2d(name):
+    g = golden(name)
+    xl, xr, yl, yr = g["dom"]
+    u = O.psolve2d(g["f"], Lx=xr - xl, Ly=yr - yl, lam=float(g["lam"]))
+    assert max_rel(u, g["u"]) < 1e-12
+
+
+@pytest.mark.parametrize("name", ["periodic_3d", "periodic_3d_ns3"])
+def test_periodic_restatement_matches_golden_3d(name):
+    g = golden(name)
+    xl, xr, yl, yr, zl, zr = g["dom"]
+    u = O.psolve3d(g["f"], Lx=xr - xl, Ly=yr - yl, Lz=zr - zl, lam=float(g["lam"]))
+    assert max_rel(u, g["u"]) < 1e-12
+
+
+def test_reference_stock_periodic_2d_known_answer():
+    """TestPeriodic2D_MPI.cpp: 512 x 512, N = 10 (Ns = 52), periodic in y."""
+    f, ue = W.stock_periodic_2d()
+    u = O.psolve2d(f, Lx=1.0, Ly=1.0, lam=1.0)
+    assert np.abs(u - ue).max() < 1e-11
+
+
+def test_reference_stock_periodic_3d_known_answer():
+    """TestPeriodic3D_MPI.cpp: 64 x 32 x 250, N = 10 (Ns = 25), periodic in z."""
+    f, ue = W.stock_periodic_3d()
+    u = O.psolve3d(f, Lx=1.0, Ly=1.0, Lz=1.0, lam=1.0)
+    assert np.abs(u - ue).max() < 1e-11
+
+
+@pytest.mark.skipif(not O.have_reference(), reason="reference sources were not available at build time")
+def test_periodic_restatement_matches_reference_random():
+    rng = np.random.default_rng(6)
+    for Ns, N, Nx in [(1, 17, 16), (2, 9, 8), (5, 10, 32)]:
+        f = rng.standard_normal((Ns, Nx, N))
+        a = O.psolve2d(f, Lx=2 * math.pi, Ly=2.0, lam=1.5)
+        b = O.ref_psolve2d(f, xl=0.0, xr=2 * math.pi, yl=0.0, yr=2.0, lam=1.5)
+        assert max_rel(a, b) < 1e-11
+    f = rng.standard_normal((4, 4, 8, 8))
+    a = O.psolve3d(f, Lx=1.0, Ly=2.0, Lz=3.0, lam=0.7)
+    b = O.ref_psolve3d(f, xl=0.0, xr=1.0, yl=0.0, yr=2.0, zl=0.0, zr=3.0, lam=0.7)
+    assert max_rel(a, b) < 1e-11
+
+
 def test_collocation_residual_3d():
     g = golden("robin_3d")
     xl, xr, yl, yr, zl, zr = g["dom"]
