@@ -84,6 +84,23 @@ int helm3d_plan_create(int Nx, int Ny, int Nz, int N, double xl, double xr, doub
                        double zl, double zr, const helm_robin_t* bc, double lambda, int precision,
                        int method, helm_plan_t* plan);
 
+/* Solvers periodic in the GLL direction as well: replaces the CreatePDEPlan of
+ * Periodic2D_MPI.h:31 (and Periodic3D_MPI.h:31 for helm3d_periodic_plan_create)
+ * with the ConstructOperator of TestPeriodic2D_MPI.cpp:44-51
+ * (TestPeriodic3D_MPI.cpp:46-54).  The GLL elements close on themselves: u and
+ * its slope are continuous from the last element's right end into the first
+ * element's left end (one element: u(0) = u(L), u'(0) = u'(L)), solved by the
+ * reference's cyclic interface sweep with its rank-one correction
+ * (Periodic2D_MPI.cpp:257-565).  helm_solve takes gl = gr = NULL; the GLL
+ * boundary slots of f are not read.  helm_solve_adjoint (Ns = 1) takes
+ * glbar = grbar = NULL.  Same size limits as helm2d_plan_create /
+ * helm3d_plan_create; lambda > 0 (lambda = 0 leaves the constant mode singular,
+ * HELM_ERR_SINGULAR). */
+int helm2d_periodic_plan_create(int Nx, int Ny, int N, double xl, double xr, double yl, double yr, double lambda,
+                                int precision, int method, helm_plan_t* plan);
+int helm3d_periodic_plan_create(int Nx, int Ny, int Nz, int N, double xl, double xr, double yl, double yr,
+                                double zl, double zr, double lambda, int precision, int method, helm_plan_t* plan);
+
 /* Second-order finite-difference variant: the 7-point stencil of the
  * reference's HypreFDM solver (HelmholtzSolvers/HypreFDM/src/Helmholtz3D_MPI.cpp:
  * CreatePDEPlan 117-269, SetA 297-410, Setb 424-466) with x and y periodic

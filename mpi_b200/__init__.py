@@ -5,7 +5,8 @@ sweep, inverse FFT) as CUDA kernels behind a C ABI (include/helm_b200.h).
 The solver classes load on first use, so that `mpi_b200.workloads` (numpy only)
 imports without torch, e.g. in CPU worker processes."""
 
-_SOLVER_NAMES = ("BatchNonPeriodic2D", "Helmholtz3DFD", "NonPeriodic2D", "NonPeriodic3D", "gdof")
+_SOLVER_NAMES = ("BatchNonPeriodic2D", "Helmholtz3DFD", "NonPeriodic2D", "NonPeriodic3D", "Periodic2D", "Periodic3D",
+                 "gdof")
 
 __all__ = list(_SOLVER_NAMES)
 

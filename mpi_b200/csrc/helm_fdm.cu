@@ -179,7 +179,18 @@ __device__ __forceinline__ void fdm_store_rows_at(const FdmArgs& a, RowOf row_of
             p0r = wsum(p0r); p0i = wsum(p0i); pNr = wsum(pNr); pNi = wsum(pNi);
             const CS wl = row.get(0), wr = row.get(P - 1);
             const double* sc = a.hscal + (size_t)g * 4;
-            if (!ADJ) {
+            if (a.periodic) {
+                // periodic, one element (Periodic3D_MPI.cpp:322-333, 661-662): forward
+                // zeta = (DN - D0).phi / b; adjoint mu = (w0 + wN - c0.s - cN.s) / b,
+                // the same b = (D0 - DN).(ul + ur)
+                const TS bb = (TS)((sc[0] + sc[1]) - (sc[2] + sc[3]));
+                if (!ADJ) {
+                    zlr = (pNr - p0r) / bb; zli = (pNi - p0i) / bb;
+                } else {
+                    zlr = ((wl.x - p0r) + (wr.x - pNr)) / bb; zli = ((wl.y - p0i) + (wr.y - pNi)) / bb;
+                }
+                zrr = zlr; zri = zli;
+            } else if (!ADJ) {
                 // Robin ends, one element (NonPeriodic3D_MPI.cpp:334-336, 357-367, 528-529)
                 const TS b0 = (TS)(-a.al * sc[0] + a.bl), c0 = (TS)(-a.al * sc[1]);
                 const TS lb = (TS)(a.ar * sc[2]);

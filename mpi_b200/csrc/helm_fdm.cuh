@@ -25,6 +25,10 @@ struct FdmArgs {
     int hzero;           // hvec is zero: skip its reads (boundary values still computed)
     double al, bl, ar, br;
     int adjoint;
+    // periodic in the GLL direction (one element): u(0) = u(L) = zeta with
+    // matching slopes; hscal then holds D0.ul, D0.ur, DN.ul, DN.ur in both
+    // directions, and the adjoint's hvec the interior vectors A^-T (DN - D0), 0
+    int periodic;
     // FP64 tensor-core variant: the four transforms of `mats` in mma.sync
     // m8n8k4 A-fragment order, [4][ld/8][ld/4][32] (NULL: not prepared)
     const double* mma_mats;

@@ -905,10 +905,18 @@ __global__ void __launch_bounds__(ROW_WARPS * 32) rows_kernel(RowArgs a)
                     const CS w0 = row[0], wN = row[P - 1];
                     const double* m = a.homs + grp * 4;
                     const TS m00 = (TS)m[0], m01 = (TS)m[1], m10 = (TS)m[2], m11 = (TS)m[3];
-                    const TS det = m00 * m11 - m01 * m10;
                     const TS q0r = w0.x - a0r, q0i = w0.y - a0i, qNr = wN.x - aNr, qNi = wN.y - aNi;
-                    const TS v0r = (m11 * q0r - m01 * qNr) / det, v0i = (m11 * q0i - m01 * qNi) / det;
-                    const TS vNr = (m00 * qNr - m10 * q0r) / det, vNi = (m00 * qNi - m10 * q0i) / det;
+                    TS v0r, v0i, vNr, vNi;
+                    if (a.periodic) {
+                        // periodic: mu = (q0 + qN) / b with the forward b = (D0 - DN).(ul + ur)
+                        const TS bb = (TS)((m[0] + m[1]) - (m[2] + m[3]));
+                        v0r = (q0r + qNr) / bb; v0i = (q0i + qNi) / bb;
+                        vNr = v0r; vNi = v0i;
+                    } else {
+                        const TS det = m00 * m11 - m01 * m10;
+                        v0r = (m11 * q0r - m01 * qNr) / det; v0i = (m11 * q0i - m01 * qNi) / det;
+                        vNr = (m00 * qNr - m10 * q0r) / det; vNi = (m00 * qNi - m10 * q0i) / det;
+                    }
                     const double* pl = a.hom + (size_t)grp * 2 * P;
                     const double* pr_ = pl + P;
 #pragma unroll
@@ -944,6 +952,21 @@ __global__ void __launch_bounds__(ROW_WARPS * 32) rows_kernel(RowArgs a)
                 }
                 d0r = warp_sum(a0r); d0i = warp_sum(a0i);
                 dNr = warp_sum(aNr); dNi = warp_sum(aNi);
+                if (a.periodic) {
+                    // the cyclic sweep needs every element's end slopes first
+                    if (Ns > 1) {
+                        if (lane == 0) {
+                            sNs[jj * 6 + 0] = d0r; sNs[jj * 6 + 1] = d0i;
+                            sNs[jj * 6 + 2] = dNr; sNs[jj * 6 + 3] = dNi;
+                        }
+#pragma unroll
+                        for (int s = 0; s < NSLOT; ++s) {
+                            const int i = lane + 32 * s;
+                            if (i < n) row[1 + i] = mk(xr[s], xi[s]);
+                        }
+                    }
+                    continue;
+                }
                 // ---- forward sweep of the interface system ----
                 TS bj, cj;
                 if (jj == 0) {
@@ -973,6 +996,99 @@ __global__ void __launch_bounds__(ROW_WARPS * 32) rows_kernel(RowArgs a)
                 }
             }
             if (ADJ || !hom_active) continue;
+            if (a.periodic) {
+                if (Ns == 1) {
+                    // u(0) = u(L) = zeta, slopes equal (Periodic2D_MPI.cpp:262-266, 524-531)
+                    const TS bb = (TS)((d0ul + d0ur) - (dNul + dNur));
+                    const TS zr_ = (dNr - d0r) / bb, zi_ = (dNi - d0i) / bb;
+                    CS* row = spec + rowoff;
+#pragma unroll
+                    for (int s = 0; s < NSLOT; ++s) {
+                        const int i = lane + 32 * s;
+                        if (i < n) {
+                            const TS l = (TS)ul[1 + i], r = (TS)ur[1 + i];
+                            row[1 + i] = mk(xr[s] + zr_ * l + zr_ * r, xi[s] + zi_ * l + zi_ * r);
+                        }
+                    }
+                    if (lane == 0) { row[0] = mk(zr_, zi_); row[P - 1] = mk(zr_, zi_); }
+                    continue;
+                }
+                // cyclic interface sweep with the rank-one correction (Periodic2D_MPI.cpp:
+                // forward 268-293, backward 533-565): slot jj of sNs holds rhs0 (then
+                // zeta_l) in [0, 1], b in [2], c in [3], rhs1 (then eta_l) in [4]
+                __syncwarp();
+                if (lane == 0) {
+                    const TS D0ul = (TS)d0ul, D0ur = (TS)d0ur, DNul = (TS)dNul, DNur = (TS)dNur;
+                    TS pNr = sNs[(Ns - 1) * 6 + 2], pNi = sNs[(Ns - 1) * 6 + 3];  // DN.phi of the element before
+                    TS bp = 0, cp = 0, q0r = 0, q0i = 0, q1 = 0;
+                    for (int jj = 0; jj < Ns; ++jj) {
+                        const TS e0r = sNs[jj * 6 + 0], e0i = sNs[jj * 6 + 1];
+                        const TS eNr = sNs[jj * 6 + 2], eNi = sNs[jj * 6 + 3];
+                        TS bj, cj;
+                        if (jj == 0) {
+                            bj = DNur - DNul - D0ul;
+                            cj = -D0ur;
+                            q0r = e0r - pNr; q0i = e0i - pNi;
+                            q1 = DNul;
+                        } else {
+                            q0r = e0r - pNr - (q0r / bp) * DNul;
+                            q0i = e0i - pNi - (q0i / bp) * DNul;
+                            if (jj < Ns - 1) {
+                                bj = DNur - D0ul - (cp / bp) * DNul;
+                                cj = -D0ur;
+                                q1 = -(q1 / bp) * DNul;
+                            } else {
+                                bj = DNur - D0ul + D0ur - (cp / bp) * DNul;
+                                cj = 0;
+                                q1 = -D0ur - (q1 / bp) * DNul;
+                            }
+                        }
+                        sNs[jj * 6 + 0] = q0r; sNs[jj * 6 + 1] = q0i;
+                        sNs[jj * 6 + 2] = bj;  sNs[jj * 6 + 3] = cj;
+                        sNs[jj * 6 + 4] = q1;
+                        bp = bj; cp = cj; pNr = eNr; pNi = eNi;
+                    }
+                    // back sweep: zeta_r(jj) = zeta_l(jj + 1), eta likewise
+                    TS zlr = q0r / bp, zli = q0i / bp, el = q1 / bp;
+                    sNs[(Ns - 1) * 6 + 0] = zlr; sNs[(Ns - 1) * 6 + 1] = zli; sNs[(Ns - 1) * 6 + 4] = el;
+                    const TS zlastr = zlr, zlasti = zli, elast = el;
+                    for (int jj = Ns - 2; jj >= 0; --jj) {
+                        const TS bj = sNs[jj * 6 + 2], cj = sNs[jj * 6 + 3];
+                        zlr = (sNs[jj * 6 + 0] - cj * zlr) / bj;
+                        zli = (sNs[jj * 6 + 1] - cj * zli) / bj;
+                        el = (sNs[jj * 6 + 4] - cj * el) / bj;
+                        sNs[jj * 6 + 0] = zlr; sNs[jj * 6 + 1] = zli; sNs[jj * 6 + 4] = el;
+                    }
+                    // alpha = -(zeta_l + zeta_r) / (1 + eta_l + eta_r) of the last element,
+                    // whose right values are the first element's left ones
+                    const TS den = (TS)1 + elast + el;
+                    const TS alr = -(zlastr + zlr) / den, ali = -(zlasti + zli) / den;
+                    for (int jj = 0; jj < Ns; ++jj) {
+                        const TS e = sNs[jj * 6 + 4];
+                        sNs[jj * 6 + 0] += alr * e;
+                        sNs[jj * 6 + 1] += ali * e;
+                    }
+                }
+                __syncwarp();
+                for (int jj = 0; jj < Ns; ++jj) {
+                    CS* row = spec + (long long)jj * a.elem_stride + rowoff;
+                    const int jn = (jj + 1 == Ns) ? 0 : jj + 1;
+                    const TS zl_r = sNs[jj * 6 + 0], zl_i = sNs[jj * 6 + 1];
+                    const TS zrr = sNs[jn * 6 + 0], zri = sNs[jn * 6 + 1];
+#pragma unroll
+                    for (int s = 0; s < NSLOT; ++s) {
+                        const int i = lane + 32 * s;
+                        if (i < n) {
+                            const CS x = row[1 + i];
+                            const TS l = (TS)ul[1 + i], r = (TS)ur[1 + i];
+                            row[1 + i] = mk(x.x + zl_r * l + zrr * r, x.y + zl_i * l + zri * r);
+                        }
+                    }
+                    if (lane == 0) { row[0] = mk(zl_r, zl_i); row[P - 1] = mk(zrr, zri); }
+                }
+                __syncwarp();
+                continue;
+            }
             // ---- right end, back sweep, combination ----
             CS* lastrow = spec + (long long)(Ns - 1) * a.elem_stride + rowoff;
             const CS gr = lastrow[P - 1];

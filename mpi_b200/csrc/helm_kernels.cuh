@@ -103,6 +103,12 @@ struct RowArgs {
     // pl = -A^-T r0 and pr = -A^-T rN, homs the 2x2 boundary matrix
     // [[m00, m01], [m10, m11]] of the transposed system (row-major).
     int adjoint;
+    // periodic in the GLL direction: the interface system is cyclic (u and its
+    // slope continuous across the last element's right end into the first
+    // element's left end); hom / homs are the forward ul, ur / D0.ul, D0.ur,
+    // DN.ul, DN.ur in both directions, and the adjoint (one element) reads
+    // pl = A^-T (DN - D0), pr = 0
+    int periodic;
 };
 
 // Launchers (helm_kernels.cu).  Return a cudaError_t.

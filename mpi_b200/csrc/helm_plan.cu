@@ -135,8 +135,15 @@ static void build_groups(Plan& p)
 // (alphar D[N-1][0], alphar D[N-1][int], betar + alphar D[N-1][N-1]).
 // Eliminating the interior, v_int = psi + v0 pl + vN pr with psi = A^-T w_int,
 // pl = -A^-T r0, pr = -A^-T rN, and (v0, vN) solve a 2x2 system.
+//
+// Periodic plans: the forward map is u_int = A^-1 f_int + zeta h_int, u_0 =
+// u_{N-1} = zeta with zeta = (DN - D0).phi / b and b = (D0 - DN).(ul + ur), so
+// the transpose is fbar_int = psi + mu A^-T (DN - D0), mu = (w_0 + w_{N-1} -
+// c0.psi - cN.psi) / b: pl = A^-T (DN - D0) (r0 = D0 - DN), pr = 0, and the
+// boundary scalars stay the forward D0.ul, D0.ur, DN.ul, DN.ur (`fwd_homs`).
 static int setup_adjoint(Plan& p, const std::vector<double>& A0, const std::vector<double>& lam,
-                         const std::vector<double>& V, const std::vector<double>& Vi, int prec_code)
+                         const std::vector<double>& V, const std::vector<double>& Vi, int prec_code,
+                         const std::vector<double>& fwd_homs)
 {
     const int N = p.N, n = p.n, ld = p.ld, G = p.ngroups;
     const std::vector<double>& D = p.gll.D;
@@ -144,8 +151,8 @@ static int setup_adjoint(Plan& p, const std::vector<double>& A0, const std::vect
     const double al = p.bc.alphal, bl = p.bc.betal, ar = p.bc.alphar, br = p.bc.betar;
     std::vector<double> r0(n), rN(n), c0(N, 0.0), cN(N, 0.0);
     for (int i = 0; i < n; ++i) {
-        r0[i] = -al * D[i + 1];
-        rN[i] = ar * D[(N - 1) * N + i + 1];
+        r0[i] = p.periodic ? D[i + 1] - D[(N - 1) * N + i + 1] : -al * D[i + 1];
+        rN[i] = p.periodic ? 0.0 : ar * D[(N - 1) * N + i + 1];
         c0[i + 1] = D2[(i + 1) * N];
         cN[i + 1] = D2[(i + 1) * N + N - 1];
     }
@@ -177,6 +184,10 @@ static int setup_adjoint(Plan& p, const std::vector<double>& A0, const std::vect
         for (int i = 1; i <= n; ++i) {
             c0pl += c0[i] * pl[i]; c0pr += c0[i] * pr[i];
             cNpl += cN[i] * pl[i]; cNpr += cN[i] * pr[i];
+        }
+        if (p.periodic) {
+            for (int q = 0; q < 4; ++q) homs[(size_t)g * 4 + q] = fwd_homs[(size_t)g * 4 + q];
+            continue;
         }
         homs[(size_t)g * 4 + 0] = a00 + c0pl;
         homs[(size_t)g * 4 + 1] = aN0 + c0pr;
@@ -480,6 +491,44 @@ static int setup_plan(Plan& p)
     for (auto& t : th) t.join();
     for (int g = 0; g < G; ++g)
         if (bad[g]) { g_last_error = "shifted GLL operator is singular"; return HELM_ERR_SINGULAR; }
+    if (p.periodic) {
+        // the real coefficients of the cyclic interface sweep (the kernels' divisors)
+        // must not vanish: lambda = 0 leaves the constant mode without an equation
+        for (int g = 0; g < G; ++g) {
+            const double* h = &homs[(size_t)g * 4];
+            const double d0ul = h[0], d0ur = h[1], dNul = h[2], dNur = h[3];
+            const double tol = 1e-12 * (std::fabs(d0ul) + std::fabs(d0ur) + std::fabs(dNul) + std::fabs(dNur));
+            bool ok = true;
+            if (p.Ns == 1) {
+                ok = std::fabs((d0ul + d0ur) - (dNul + dNur)) > tol;
+            } else {
+                std::vector<double> b(p.Ns), c(p.Ns), r1(p.Ns);
+                for (int jj = 0; jj < p.Ns && ok; ++jj) {
+                    if (jj == 0) { b[0] = dNur - dNul - d0ul; c[0] = -d0ur; r1[0] = dNul; }
+                    else if (jj < p.Ns - 1) {
+                        b[jj] = dNur - d0ul - (c[jj - 1] / b[jj - 1]) * dNul;
+                        c[jj] = -d0ur;
+                        r1[jj] = -(r1[jj - 1] / b[jj - 1]) * dNul;
+                    } else {
+                        b[jj] = dNur - d0ul + d0ur - (c[jj - 1] / b[jj - 1]) * dNul;
+                        c[jj] = 0.0;
+                        r1[jj] = -d0ur - (r1[jj - 1] / b[jj - 1]) * dNul;
+                    }
+                    ok = std::fabs(b[jj]) > tol;
+                }
+                if (ok) {
+                    double el = r1[p.Ns - 1] / b[p.Ns - 1];
+                    const double elast = el;
+                    for (int jj = p.Ns - 2; jj >= 0; --jj) el = (r1[jj] - c[jj] * el) / b[jj];
+                    ok = std::fabs(1.0 + elast + el) > 1e-12 * (1.0 + std::fabs(elast) + std::fabs(el));
+                }
+            }
+            if (!ok) {
+                g_last_error = "periodic interface system is singular (lambda = 0 leaves the constant mode free)";
+                return HELM_ERR_SINGULAR;
+            }
+        }
+    }
 
     // ---- device uploads ----
     const bool td = p.precision != HELM_FP32;           // spectrum / FFT precision is double
@@ -532,7 +581,7 @@ static int setup_plan(Plan& p)
     p.h_V = V;
     p.h_Vi = Vi;
     if (!lu && p.Ns == 1) {
-        if (p.packed_elems == 0 && (st = setup_adjoint(p, A0, lam, V, Vi, prec_code))) return st;
+        if (p.packed_elems == 0 && (st = setup_adjoint(p, A0, lam, V, Vi, prec_code, homs))) return st;
         if ((st = setup_fast(p, A0, prec_code))) return st;
     }
     if (!p.fast && rows_smem_bytes(p.method, prec_code, n, p.ld) > kMaxSmemPerBlock) {
@@ -650,7 +699,8 @@ static int run_pipeline(Plan& p, const void* in, const double* gl, const double*
     if (!adjoint) {
         r.vinvT = p.d_vinvT;
         r.vT = p.d_vT;
-        const bool hom = p.Ns > 1 || p.bc.alphal != 0.0 || p.bc.alphar != 0.0 || gl != nullptr || gr != nullptr;
+        const bool hom = p.Ns > 1 || p.periodic || p.bc.alphal != 0.0 || p.bc.alphar != 0.0 || gl != nullptr ||
+                         gr != nullptr;
         r.hom = hom ? p.d_hom : nullptr;
         r.homs = p.d_homs;
         r.d0 = p.d_d0;
@@ -666,6 +716,7 @@ static int run_pipeline(Plan& p, const void* in, const double* gl, const double*
         r.dN = p.d_cN;
         r.d2t = p.d_d2row;
     }
+    r.periodic = p.periodic ? 1 : 0;
     const int prec = p.precision == HELM_FP64 ? 0 : (p.precision == HELM_FP32 ? 1 : 2);
     int e;
     if (p.fd) {
@@ -708,7 +759,8 @@ static int run_pipeline(Plan& p, const void* in, const double* gl, const double*
         fa.hscal = adjoint ? p.d_homs_adj : p.d_homs;
         // the transposed system's pl, pr are -A^-T of the Robin rows' interior
         // entries, which vanish for Dirichlet ends
-        fa.hzero = (adjoint && p.bc.alphal == 0.0 && p.bc.alphar == 0.0) ? 1 : 0;
+        fa.hzero = (adjoint && !p.periodic && p.bc.alphal == 0.0 && p.bc.alphar == 0.0) ? 1 : 0;
+        fa.periodic = p.periodic ? 1 : 0;
         fa.al = p.bc.alphal;
         fa.bl = p.bc.betal;
         fa.ar = p.bc.alphar;
@@ -951,7 +1003,7 @@ static int create_fd_plan(int Nx, int Ny, int Nz, double xl, double xr, double y
 
 static int create_plan(int dim, int Nx, int Ny, int Ngll_total, int N, double xl, double xr, double yl, double yr,
                        double zl, double zr, const helm_robin_t* bc, double lambda, int precision, int method,
-                       helm_plan_t* out)
+                       helm_plan_t* out, bool periodic = false)
 {
     if (!out) return HELM_ERR_INVALID;
     *out = nullptr;
@@ -981,6 +1033,8 @@ static int create_plan(int dim, int Nx, int Ny, int Ngll_total, int N, double xl
     p->Ly = yr - yl;
     p->Lgll = dim == 3 ? zr - zl : yr - yl;
     p->bc = bc ? *bc : helm_robin_t{0.0, 1.0, 0.0, 1.0};
+    p->periodic = periodic;
+    if (periodic) p->bc = helm_robin_t{0.0, 1.0, 0.0, 1.0};  // unused: no boundary rows
     p->lambda = lambda;
     p->precision = precision;
     p->method = method;
@@ -1072,6 +1126,28 @@ int helm3d_plan_create(int Nx, int Ny, int Nz, int N, double xl, double xr, doub
     }
 }
 
+int helm2d_periodic_plan_create(int Nx, int Ny, int N, double xl, double xr, double yl, double yr, double lambda,
+                                int precision, int method, helm_plan_t* plan)
+{
+    try {
+        return helm::create_plan(2, Nx, 1, Ny, N, xl, xr, yl, yr, 0.0, 1.0, nullptr, lambda, precision, method, plan,
+                                 true);
+    } catch (...) {
+        return HELM_ERR_OOM;
+    }
+}
+
+int helm3d_periodic_plan_create(int Nx, int Ny, int Nz, int N, double xl, double xr, double yl, double yr, double zl,
+                                double zr, double lambda, int precision, int method, helm_plan_t* plan)
+{
+    try {
+        return helm::create_plan(3, Nx, Ny, Nz, N, xl, xr, yl, yr, zl, zr, nullptr, lambda, precision, method, plan,
+                                 true);
+    } catch (...) {
+        return HELM_ERR_OOM;
+    }
+}
+
 int helm_plan_set_layout(helm_plan_t plan, long long x_stride, long long elem_stride, long long bc_x_stride)
 {
     if (!plan) return HELM_ERR_INVALID;
@@ -1107,6 +1183,10 @@ int helm_solve(helm_plan_t plan, const void* f, const double* gl, const double* 
 {
     if (!plan || !f || !u) return HELM_ERR_INVALID;
     Plan& p = *reinterpret_cast<Plan*>(plan);
+    if (p.periodic && (gl || gr)) {
+        helm::set_last_error("a plan periodic in the GLL direction takes no boundary data");
+        return HELM_ERR_INVALID;
+    }
     int cur = 0;
     cudaGetDevice(&cur);
     if (cur != p.device) cudaSetDevice(p.device);
@@ -1120,6 +1200,10 @@ int helm_solve_adjoint(helm_plan_t plan, const double* ubar, double* fbar, doubl
 {
     if (!plan || !ubar || !fbar || (lambda_bar && !u)) return HELM_ERR_INVALID;
     Plan& p = *reinterpret_cast<Plan*>(plan);
+    if (p.periodic && (glbar || grbar)) {
+        helm::set_last_error("a plan periodic in the GLL direction has no boundary data to differentiate");
+        return HELM_ERR_INVALID;
+    }
     int cur = 0;
     cudaGetDevice(&cur);
     if (cur != p.device) cudaSetDevice(p.device);

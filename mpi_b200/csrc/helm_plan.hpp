@@ -16,6 +16,7 @@ struct Plan {
     double xl = 0, xr = 1, yl = 0, yr = 1, zl = 0, zr = 1;
     double Lx = 1, Ly = 1, Lgll = 1;
     helm_robin_t bc{0.0, 1.0, 0.0, 1.0};
+    bool periodic = false;       // periodic in the GLL direction (no boundary data)
     double lambda = 0;
     int precision = HELM_FP64, method = HELM_METHOD_AUTO;
     int io_bytes = 8, sweeps = 1;

@@ -11,6 +11,8 @@ in the reference's index order (GLL index fastest):
 
 * ``NonPeriodic2D``: f, u ``[Ns, Nx, N]`` (or ``[Nx, N]`` when Ns == 1), gl/gr ``[Nx]``
 * ``NonPeriodic3D``: f, u ``[Ns, Nx, Ny, N]`` (or ``[Nx, Ny, N]``), gl/gr ``[Nx, Ny]``
+* ``Periodic2D`` / ``Periodic3D`` (periodic in the GLL direction too,
+  Periodic2D_MPI.h / Periodic3D_MPI.h): the same f, u shapes and no boundary data
 
 Errors raise :class:`mpi_b200._lib.HelmError` with the C status code (the
 reference prints a message and exits).
@@ -226,6 +228,58 @@ class NonPeriodic3D(_PlanBase):
 
     def _bc_shape(self):
         return (self.Nx, self.Ny)
+
+
+class _PeriodicMixin:
+    """The GLL direction is periodic: no boundary data in or out."""
+
+    def SolvePDE(self, f, gl=None, gr=None, out=None, stream=None):
+        if gl is not None or gr is not None:
+            raise ValueError("a solver periodic in the GLL direction takes no boundary data")
+        return _PlanBase.SolvePDE(self, f, None, None, out=out, stream=stream)
+
+    solve = SolvePDE
+
+    def SolveAdjoint(self, ubar, u=None, want_bc: bool = False, stream=None):
+        if want_bc:
+            raise ValueError("a solver periodic in the GLL direction has no boundary data")
+        return _PlanBase.SolveAdjoint(self, ubar, u=u, want_bc=False, stream=stream)
+
+
+class Periodic2D(_PeriodicMixin, NonPeriodic2D):
+    """2D Fourier (x) x GLL (y) solver periodic in y as well: CreatePDEPlan(Nx,
+    Ny, N, xl, xr, yl, yr) of Periodic2D_MPI.cpp:36-125 with Lambda, solved by
+    the cyclic interface sweep of Periodic2D_MPI.cpp:257-565."""
+
+    def __init__(self, Nx: int, Ny: int, N: int, xl: float, xr: float, yl: float, yr: float, *, Lambda: float,
+                 precision: str = "fp64", method: str = "auto"):
+        _PlanBase.__init__(self)
+        self.Nx, self.N = Nx, N
+        self.xl, self.xr, self.yl, self.yr = xl, xr, yl, yr
+        self.Lambda = Lambda
+        self.bc = None
+        self.precision = precision
+        self.io_dtype = torch.float64
+        L.check(self._lib.helm2d_periodic_plan_create(Nx, Ny, N, xl, xr, yl, yr, Lambda, _PREC[precision],
+                                                      _METHOD[method], ctypes.byref(self._plan)),
+                "helm2d_periodic_plan_create")
+
+
+class Periodic3D(_PeriodicMixin, NonPeriodic3D):
+    """3D Fourier (x, y) x GLL (z) solver periodic in z as well: CreatePDEPlan(Nx,
+    Ny, Nz, N, xl, xr, yl, yr, zl, zr) of Periodic3D_MPI.cpp:36-133."""
+
+    def __init__(self, Nx: int, Ny: int, Nz: int, N: int, xl: float, xr: float, yl: float, yr: float, zl: float,
+                 zr: float, *, Lambda: float, precision: str = "fp64", method: str = "auto"):
+        _PlanBase.__init__(self)
+        self.Nx, self.Ny, self.N = Nx, Ny, N
+        self.Lambda = Lambda
+        self.bc = None
+        self.precision = precision
+        self.io_dtype = torch.float64
+        L.check(self._lib.helm3d_periodic_plan_create(Nx, Ny, Nz, N, xl, xr, yl, yr, zl, zr, Lambda,
+                                                      _PREC[precision], _METHOD[method], ctypes.byref(self._plan)),
+                "helm3d_periodic_plan_create")
 
 
 class Helmholtz3DFD(_PlanBase):

@@ -265,7 +265,7 @@ static void orc_row_solve(int N, int Ns, const double* Op, const int* piv, const
 /* The same row set for the solver that is periodic in the GLL direction: the
  * particular solutions, then the cyclic interface sweep with its rank-one
  * correction, then the combination (Periodic2D_MPI.cpp:176-223; the size == 1
- * paths :257-283 forward, :411-444 backward, :459-461 combine).  One element:
+ * paths of Step 3 :257-295, Step 4 :521-565 and Step 5 :682-686).  One element:
  * u(0) = u(L) = zeta with matching slopes.  Several: a tridiagonal sweep whose
  * first diagonal is shifted, a second right-hand side rhs1 for the shift, and
  * alpha = -(zl + zr) / (1 + el + er) at the last element. */

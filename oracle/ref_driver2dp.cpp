@@ -2,9 +2,9 @@
 // reference's own 2D solver that is periodic in the GLL direction
 // (Periodic2D_MPI.cpp, compiled unchanged by oracle/Makefile).
 //
-// Follows the reference's test driver TestPeriodic2D_MPI.cpp:86-120:
+// Follows the reference's test driver TestPeriodic2D_MPI.cpp:71-89:
 // CreatePDEPlan -> CreateFFTPlan -> fill rhsPDE -> SolvePDE with the
-// shifted-Laplacian ConstructOperator (TestPeriodic2D_MPI.cpp:46-53) -> read U.
+// shifted-Laplacian ConstructOperator (TestPeriodic2D_MPI.cpp:44-51) -> read U.
 #include "Periodic2D_MPI.h"
 #include <chrono>
 

@@ -2,8 +2,8 @@
 // reference's own 3D solver that is periodic in the GLL direction
 // (Periodic3D_MPI.cpp, compiled unchanged by oracle/Makefile).
 //
-// Follows TestPeriodic3D_MPI.cpp:72-105 with the ConstructOperator of
-// TestPeriodic3D_MPI.cpp:45-53.
+// Follows TestPeriodic3D_MPI.cpp:73-93 with the ConstructOperator of
+// TestPeriodic3D_MPI.cpp:46-54.
 #include "Periodic3D_MPI.h"
 #include <chrono>
 
