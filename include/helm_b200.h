@@ -148,6 +148,28 @@ int helm_solve(helm_plan_t plan, const void* f, const double* gl, const double* 
 int helm_solve_adjoint(helm_plan_t plan, const double* ubar, double* fbar, double* glbar, double* grbar,
                        const double* u, double* lambda_bar, void* stream);
 
+/* Derivative along the GLL direction, element by element: du = Dy u (order 1)
+ * or Dyy u (order 2) with the plan's scaled matrices (helm_plan_get_grid), at
+ * every node of every Fourier row.  Replaces FirstDerivativeY /
+ * SecondDerivativeY of the 2D solvers (NonPeriodic2D_MPI.cpp:497-542,
+ * Periodic2D_MPI.cpp:714-763) and FirstDerivativeZ / SecondDerivativeZ of the 3D
+ * ones (NonPeriodic3D_MPI.cpp:632-683, Periodic3D_MPI.cpp:905-957).  u, du: the
+ * plan's layout and io type (helm_plan_set_layout / helm_plan_set_io_bytes),
+ * device pointers; du may equal u.  Not for finite-difference plans. */
+int helm_gll_derivative(helm_plan_t plan, int order, const void* u, void* du, void* stream);
+
+/* Spectral derivative along a Fourier direction: axis 0 = x, axis 1 = y (3D
+ * plans) of a real field in the plan's layout: forward FFT along the axis,
+ * multiplication by (2 pi i K / L)^order with K = k below L/2 and K = -L/2 at
+ * the Nyquist index, inverse FFT, real part.  Replaces FirstDerivativeFourierX
+ * / FirstDerivativeFourierY and SecondDerivativeFourierX / ...Y
+ * (Fourier_Quadrature.cpp:1387-1834) on the solver's arrays (the reference's
+ * solver-level FirstDerivativeX of NonPeriodic2D_MPI.cpp:479-483 is an empty
+ * stub).  Every GLL node is differentiated, boundary slots included; du must
+ * not overlap u.  Uses the plan's spectrum scratch: do not run it concurrently
+ * with a solve of the same plan on another stream. */
+int helm_fourier_derivative(helm_plan_t plan, int axis, int order, const void* u, void* du, void* stream);
+
 /* Node coordinates: 2D y[Ns*(N-1)+1] / 3D z[...], and the scaled first and
  * second GLL derivative matrices D[N*N], D2[N*N] (row-major), host pointers,
  * any may be NULL.  The reference's globals y/z, Dy/Dz, Dyy/Dzz. */

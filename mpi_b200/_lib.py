@@ -36,7 +36,7 @@ EXPORTS = (
     "helm_plan_set_stage_timing", "helm_plan_stage_times", "helm_fd3d_plan_create",
     "helm2d_batch_create", "helm_batch_offsets", "helm_batch_info", "helm_batch_set_graph",
     "helm_batch_solve", "helm_batch_destroy", "helm_plan_get_launch_variants", "helm_plan_set_launch_variants",
-    "helm2d_periodic_plan_create", "helm3d_periodic_plan_create",
+    "helm2d_periodic_plan_create", "helm3d_periodic_plan_create", "helm_gll_derivative", "helm_fourier_derivative",
 )
 
 
@@ -70,6 +70,8 @@ def lib() -> ctypes.CDLL:
     L.helm2d_plan_create.argtypes = [i, i, i, d, d, d, d, P(robin_t), d, i, i, P(vp)]
     L.helm3d_plan_create.argtypes = [i, i, i, i, d, d, d, d, d, d, P(robin_t), d, i, i, P(vp)]
     L.helm_fd3d_plan_create.argtypes = [i, i, i, d, d, d, d, d, d, P(robin_t), d, i, P(vp)]
+    L.helm_gll_derivative.argtypes = [vp, i, vp, vp, vp]
+    L.helm_fourier_derivative.argtypes = [vp, i, i, vp, vp, vp]
     L.helm2d_periodic_plan_create.argtypes = [i, i, i, d, d, d, d, d, i, i, P(vp)]
     L.helm3d_periodic_plan_create.argtypes = [i, i, i, i, d, d, d, d, d, d, d, i, i, P(vp)]
     L.helm_plan_set_layout.argtypes = [vp, ll, ll, ll]

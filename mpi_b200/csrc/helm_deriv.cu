@@ -1,0 +1,395 @@
+// Derivative along the GLL direction (sm_100a): du = M u for every row of P
+// values, M the plan's scaled first- or second-derivative matrix.  Replaces the
+// reference's per-element loops FirstDerivativeY / SecondDerivativeY
+// (NonPeriodic2D_MPI.cpp:497-542, Periodic2D_MPI.cpp:714-763) and
+// FirstDerivativeZ / SecondDerivativeZ (NonPeriodic3D_MPI.cpp:632-683,
+// Periodic3D_MPI.cpp:905-957).
+//
+// The GLL derivative matrices are anti-centrosymmetric (first) or
+// centrosymmetric (second), so with the fold s_k = u_k + u_{P-1-k},
+// a_k = u_k - u_{P-1-k} (k < h = P/2; s_h = u_h for odd P) every output pair
+// comes from two half-size products:
+//     sigma_j = sum_k E[j][k] s_k,   E[j][k] = (M[j][k] + M[j][P-1-k]) / 2  (E[j][h] = M[j][h])
+//     alpha_j = sum_k F[j][k] a_k,   F[j][k] = (M[j][k] - M[j][P-1-k]) / 2
+//     du_j = sigma_j + alpha_j,      du_{P-1-j} = -/+ (sigma_j - alpha_j)  (first / second)
+// which halves the multiply-adds of the dense product.
+//
+// FP64 arrays run both products on the FP64 tensor cores (gll_deriv_mma_kernel);
+// FP32 arrays run them on the CUDA cores, one lane per row (gll_deriv_kernel).
+// Each warp owns 32 rows of a tile in shared memory (raw rows, then their
+// folded halves) and never waits on another warp.  The raw rows of
+// the warp's next tile are copied in by cp.async while it folds, multiplies and
+// stores the current one; E and F are built once per CTA and read as
+// broadcasts.  HBM-bound: 2 P values (read + write) per row.
+#include "helm_device.cuh"
+#include "helm_kernels.cuh"
+
+namespace helm {
+
+constexpr int GD_JB = 8;   // outputs per register block
+
+struct GdLayout {
+    int h, odd, hs, hsp, hap, hsr, rs, os;
+    size_t ef_bytes, warp_bytes;
+};
+
+template <typename T>
+static GdLayout gd_layout(int P)
+{
+    GdLayout L{};
+    L.h = P / 2;
+    L.odd = P & 1;
+    L.hs = L.h + L.odd;
+    L.hsp = (L.hs + 1) & ~1;                 // k loops run in pairs (16-byte loads)
+    L.hap = (L.h + 1) & ~1;
+    L.hsr = (L.hs + GD_JB - 1) / GD_JB * GD_JB;  // E / F rows padded to whole register blocks
+    L.rs = L.hsp + L.hap;                    // folded row stride: = 2 mod 4 elements, so the
+    while ((L.rs & 3) != 2) ++L.rs;          //   per-lane 16-byte loads of 8 rows hit distinct banks
+    L.os = P | 1;                            // raw row stride: odd
+    L.ef_bytes = (size_t)L.hsr * (L.hsp + L.hap) * sizeof(T);
+    L.warp_bytes = (size_t)32 * (L.rs + 2 * L.os) * sizeof(T);  // folded rows + two raw buffers
+    return L;
+}
+
+__device__ __forceinline__ long long gd_row_offset(const GllDerivArgs& a, long long R)
+{
+    const long long per_elem = (long long)a.nx * a.rows_per_x;
+    const long long e = R / per_elem;
+    const long long rem = R - e * per_elem;
+    const long long i = rem / a.rows_per_x;
+    const long long j = rem - i * a.rows_per_x;
+    return e * a.elem_stride + i * a.x_stride + j * a.P;
+}
+
+template <typename T>
+__global__ void gll_deriv_kernel(GllDerivArgs a, GdLayout L)
+{
+    pdl_enter();
+    using V2 = typename std::conditional<sizeof(T) == 8, double2, float2>::type;
+    extern __shared__ __align__(16) unsigned char gd_smem[];
+    const int P = a.P, h = L.h, hs = L.hs, hsp = L.hsp, hap = L.hap;
+    T* E = reinterpret_cast<T*>(gd_smem);                 // [hsr][hsp]
+    T* F = E + (size_t)L.hsr * hsp;                       // [hsr][hap]
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    T* fin = reinterpret_cast<T*>(gd_smem + L.ef_bytes + (size_t)warp * L.warp_bytes);  // [32][rs]
+    T* raw = fin + (size_t)32 * L.rs;                                                    // [2][32][os]
+
+    for (int e = threadIdx.x; e < L.hsr * hsp; e += blockDim.x) {
+        const int j = e / hsp, k = e - j * hsp;
+        double v = 0.0;
+        if (j < hs) {
+            if (k < h) v = 0.5 * (a.M[j * P + k] + a.M[j * P + P - 1 - k]);
+            else if (k == h && L.odd) v = a.M[j * P + h];
+        }
+        E[e] = (T)v;
+    }
+    for (int e = threadIdx.x; e < L.hsr * hap; e += blockDim.x) {
+        const int j = e / hap, k = e - j * hap;
+        double v = 0.0;
+        if (j < hs && k < h) v = 0.5 * (a.M[j * P + k] - a.M[j * P + P - 1 - k]);
+        F[e] = (T)v;
+    }
+    __syncthreads();
+
+    const T* in = static_cast<const T*>(a.in);
+    T* out = static_cast<T*>(a.out);
+    const T sgn = a.order == 1 ? (T)-1 : (T)1;
+    const long long tiles = (a.nrows + 31) / 32;
+    const long long wstride = (long long)gridDim.x * (blockDim.x >> 5);
+    // raw rows of tile t land in raw[buf] by cp.async, issued one tile ahead
+    auto issue = [&](long long t, T* dst) {
+        const long long R0 = t * 32;
+        const int nr = (int)min(32LL, a.nrows - R0);
+        const long long my = lane < nr ? gd_row_offset(a, R0 + lane) : 0;
+        for (int r = 0; r < nr; ++r) {
+            const long long off = __shfl_sync(0xffffffffu, my, r);
+            for (int k = lane; k < P; k += 32) cp_async_elem<sizeof(T)>(dst + r * L.os + k, in + off + k, true);
+        }
+        cp_async_commit();
+    };
+    long long t = (long long)blockIdx.x * (blockDim.x >> 5) + warp;
+    int buf = 0;
+    if (t < tiles) issue(t, raw);
+    for (; t < tiles; t += wstride, buf ^= 1) {
+        T* cur = raw + (size_t)buf * 32 * L.os;
+        const long long R0 = t * 32;
+        const int nr = (int)min(32LL, a.nrows - R0);
+        if (t + wstride < tiles) {
+            issue(t + wstride, raw + (size_t)(buf ^ 1) * 32 * L.os);
+            cp_async_wait_prev();
+        } else {
+            cp_async_wait_all();
+        }
+        __syncwarp();
+        // fold
+        for (int r = 0; r < nr; ++r) {
+            const T* u = cur + r * L.os;
+            T* f = fin + r * L.rs;
+            for (int k = lane; k < hsp; k += 32) {
+                T s = 0;
+                if (k < h) s = u[k] + u[P - 1 - k];
+                else if (k == h && L.odd) s = u[h];
+                f[k] = s;
+            }
+            for (int k = lane; k < hap; k += 32) f[hsp + k] = (k < h) ? u[k] - u[P - 1 - k] : (T)0;
+        }
+        __syncwarp();
+        // lane = row: half-size products in register blocks of GD_JB outputs
+        if (lane < nr) {
+            const T* fs = fin + lane * L.rs;
+            const T* fa = fs + hsp;
+            T* o = cur + lane * L.os;  // the raw row is folded already: reuse it for the output
+            for (int jb = 0; jb < hs; jb += GD_JB) {
+                T sg[GD_JB], al[GD_JB];
+#pragma unroll
+                for (int q = 0; q < GD_JB; ++q) { sg[q] = 0; al[q] = 0; }
+                for (int k = 0; k < hsp; k += 2) {
+                    const V2 x = *reinterpret_cast<const V2*>(fs + k);
+#pragma unroll
+                    for (int q = 0; q < GD_JB; ++q) {
+                        const V2 m = *reinterpret_cast<const V2*>(E + (size_t)(jb + q) * hsp + k);
+                        sg[q] = fma(m.x, x.x, sg[q]);
+                        sg[q] = fma(m.y, x.y, sg[q]);
+                    }
+                }
+                for (int k = 0; k < hap; k += 2) {
+                    const V2 x = *reinterpret_cast<const V2*>(fa + k);
+#pragma unroll
+                    for (int q = 0; q < GD_JB; ++q) {
+                        const V2 m = *reinterpret_cast<const V2*>(F + (size_t)(jb + q) * hap + k);
+                        al[q] = fma(m.x, x.x, al[q]);
+                        al[q] = fma(m.y, x.y, al[q]);
+                    }
+                }
+#pragma unroll
+                for (int q = 0; q < GD_JB; ++q) {
+                    const int j = jb + q;
+                    if (j < h) {
+                        o[j] = sg[q] + al[q];
+                        o[P - 1 - j] = sgn * (sg[q] - al[q]);
+                    } else if (j == h && L.odd) {
+                        o[j] = sg[q] + al[q];
+                    }
+                }
+            }
+        }
+        __syncwarp();
+        const long long my = lane < nr ? gd_row_offset(a, R0 + lane) : 0;
+        for (int r = 0; r < nr; ++r) {
+            const long long off = __shfl_sync(0xffffffffu, my, r);
+            for (int k = lane; k < P; k += 32) out[off + k] = cur[r * L.os + k];
+        }
+        __syncwarp();
+    }
+}
+
+// ---------------------------------------------------------------------------
+// FP64 arrays: the two half-size products on the FP64 tensor cores.  Per warp
+// tile of 32 rows (four 8-row m-tiles), sigma = S E^T and alpha = A F^T as
+// m8n8k4 products.  The warp loads its rows as mirrored pairs (u_k, u_{P-1-k})
+// straight into the folded layout in shared memory, all 32 lanes busy; the A
+// operand is read from there, the B operands (E^T, F^T) sit in shared memory in
+// fragment order (one 8-byte word per lane, two wavefronts per warp load), and
+// the outputs go from the accumulators straight to global memory.
+struct GdMmaLayout {
+    int h, odd, hs, ks, ka, nt, rs, w;  // k-steps of the s and a halves, n-tiles, row stride, fold width
+    size_t b_bytes, warp_bytes;
+};
+
+static GdMmaLayout gd_mma_layout(int P)
+{
+    GdMmaLayout L{};
+    L.h = P / 2;
+    L.odd = P & 1;
+    L.hs = L.h + L.odd;
+    L.ks = (L.hs + 3) / 4;
+    L.ka = (L.h + 3) / 4;
+    L.nt = (L.hs + 7) / 8;
+    L.w = 4 * std::max(L.ks, L.ka);
+    L.rs = 4 * (L.ks + L.ka);           // folded row [s | a]; = 4 mod 16 doubles, so an
+    while ((L.rs & 15) != 4) ++L.rs;    //   A fragment (8 rows x 4) is two conflict-free wavefronts
+    L.b_bytes = (size_t)(L.ks + L.ka) * L.nt * 32 * sizeof(double);
+    L.warp_bytes = (size_t)32 * L.rs * sizeof(double);
+    return L;
+}
+
+template <int NT>
+__global__ void gll_deriv_mma_kernel(GllDerivArgs a, GdMmaLayout L)
+{
+    pdl_enter();
+    extern __shared__ __align__(16) unsigned char gm_smem[];
+    const int P = a.P, h = L.h, hs = L.hs;
+    double* BE = reinterpret_cast<double*>(gm_smem);   // [ks][NT][32]
+    double* BF = BE + (size_t)L.ks * NT * 32;          // [ka][NT][32]
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, g = lane >> 2, q = lane & 3;
+    double* fold = reinterpret_cast<double*>(gm_smem + L.b_bytes + (size_t)warp * L.warp_bytes);  // [32][rs]
+
+    // B fragments: BE[k][t][l] = E[8t + l/4][4k + l%4], BF likewise with F
+    for (int e = threadIdx.x; e < L.ks * NT * 32; e += blockDim.x) {
+        const int l = e & 31, t = (e >> 5) % NT, k = (e >> 5) / NT;
+        const int j = 8 * t + (l >> 2), kk = 4 * k + (l & 3);
+        double v = 0.0;
+        if (j < hs) {
+            if (kk < h) v = 0.5 * (a.M[j * P + kk] + a.M[j * P + P - 1 - kk]);
+            else if (kk == h && L.odd) v = a.M[j * P + h];
+        }
+        BE[e] = v;
+    }
+    for (int e = threadIdx.x; e < L.ka * NT * 32; e += blockDim.x) {
+        const int l = e & 31, t = (e >> 5) % NT, k = (e >> 5) / NT;
+        const int j = 8 * t + (l >> 2), kk = 4 * k + (l & 3);
+        double v = 0.0;
+        if (j < hs && kk < h) v = 0.5 * (a.M[j * P + kk] - a.M[j * P + P - 1 - kk]);
+        BF[e] = v;
+    }
+    __syncthreads();
+
+    const double* in = static_cast<const double*>(a.in);
+    double* out = static_cast<double*>(a.out);
+    const double sgn = a.order == 1 ? -1.0 : 1.0;
+    const int sw = 4 * L.ks, aw = 4 * L.ka, W = L.w;
+    const long long tiles = (a.nrows + 31) / 32;
+    const long long wstride = (long long)gridDim.x * (blockDim.x >> 5);
+    for (long long t = (long long)blockIdx.x * (blockDim.x >> 5) + warp; t < tiles; t += wstride) {
+        const long long R0 = t * 32;
+        const int nr = (int)min(32LL, a.nrows - R0);
+        const long long my = lane < nr ? gd_row_offset(a, R0 + lane) : 0;  // row offsets, by lane
+        // fold while loading: item (r, k), k < W: s_k at [k], a_k at [sw + k]
+        __syncwarp();
+        int r = 0, k = lane;
+        while (k >= W) { k -= W; ++r; }
+#pragma unroll 4
+        for (int e = lane; e < 32 * W; e += 32) {
+            const long long off = __shfl_sync(0xffffffffu, my, r);
+            double s_ = 0.0, a_ = 0.0;
+            if (r < nr) {
+                if (k < h) {
+                    const double x = in[off + k], y = in[off + P - 1 - k];
+                    s_ = x + y;
+                    a_ = x - y;
+                } else if (k == h && L.odd) {
+                    s_ = in[off + h];
+                }
+            }
+            double* f = fold + r * L.rs;
+            if (k < sw) f[k] = s_;
+            if (k < aw) f[sw + k] = a_;
+            k += 32;
+            while (k >= W) { k -= W; ++r; }
+        }
+        __syncwarp();
+#pragma unroll 1
+        for (int mt = 0; mt < 4; ++mt) {
+            if (8 * mt >= nr) break;
+            double cs[NT][2], ca[NT][2];
+#pragma unroll
+            for (int n = 0; n < NT; ++n) { cs[n][0] = cs[n][1] = 0.0; ca[n][0] = ca[n][1] = 0.0; }
+            const double* arow = fold + (8 * mt + g) * L.rs + q;
+#pragma unroll 2
+            for (int kk = 0; kk < L.ks; ++kk) {
+                const double av = arow[4 * kk];
+                const double* b = BE + ((size_t)kk * NT) * 32 + lane;
+#pragma unroll
+                for (int n = 0; n < NT; ++n) dmma_8x8x4(cs[n][0], cs[n][1], av, b[n * 32]);
+            }
+#pragma unroll 2
+            for (int kk = 0; kk < L.ka; ++kk) {
+                const double av = arow[sw + 4 * kk];
+                const double* b = BF + ((size_t)kk * NT) * 32 + lane;
+#pragma unroll
+                for (int n = 0; n < NT; ++n) dmma_8x8x4(ca[n][0], ca[n][1], av, b[n * 32]);
+            }
+            // du_j = sigma + alpha, du_{P-1-j} = sgn (sigma - alpha), straight to global memory
+            const int row = 8 * mt + g;
+            const long long off = __shfl_sync(0xffffffffu, my, row);
+            if (row < nr) {
+                double* o = out + off;
+#pragma unroll
+                for (int n = 0; n < NT; ++n)
+#pragma unroll
+                    for (int e2 = 0; e2 < 2; ++e2) {
+                        const int j = 8 * n + 2 * q + e2;
+                        const double sg = cs[n][e2], al = ca[n][e2];
+                        if (j < h) {
+                            o[j] = sg + al;
+                            o[P - 1 - j] = sgn * (sg - al);
+                        } else if (j == h && L.odd) {
+                            o[j] = sg + al;
+                        }
+                    }
+            }
+        }
+    }
+}
+
+template <int NT>
+static int run_gll_deriv_mma(const GllDerivArgs& a, cudaStream_t s)
+{
+    const GdMmaLayout L = gd_mma_layout(a.P);
+    int warps = (int)((kMaxSmemPerBlock - L.b_bytes) / L.warp_bytes);
+    if (warps > 16) warps = 16;
+    if (warps < 1) return (int)cudaErrorInvalidValue;
+    const size_t smem = L.b_bytes + (size_t)warps * L.warp_bytes;
+    auto k = gll_deriv_mma_kernel<NT>;
+    cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return (int)e;
+    int dev = 0, sms = 148, per = 1;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k, warps * 32, smem);
+    if (per < 1) per = 1;
+    const long long tiles = (a.nrows + 31) / 32;
+    long long grid = (long long)sms * per;
+    const long long need = (tiles + warps - 1) / warps;
+    if (grid > need) grid = need;
+    if (grid < 1) return 0;
+    return (int)launch_k(k, dim3((unsigned)grid), dim3(warps * 32), smem, s, a, L);
+}
+
+static int launch_gll_deriv_mma(const GllDerivArgs& a, cudaStream_t s)
+{
+    switch ((a.P / 2 + (a.P & 1) + 7) / 8) {
+        case 1: return run_gll_deriv_mma<1>(a, s);
+        case 2: return run_gll_deriv_mma<2>(a, s);
+        case 3: return run_gll_deriv_mma<3>(a, s);
+        case 4: return run_gll_deriv_mma<4>(a, s);
+        case 5: return run_gll_deriv_mma<5>(a, s);
+        case 6: return run_gll_deriv_mma<6>(a, s);
+        case 7: return run_gll_deriv_mma<7>(a, s);
+        case 8: return run_gll_deriv_mma<8>(a, s);
+        case 9: return run_gll_deriv_mma<9>(a, s);
+        default: return (int)cudaErrorInvalidValue;
+    }
+}
+
+template <typename T>
+static int run_gll_deriv(const GllDerivArgs& a, cudaStream_t s)
+{
+    const GdLayout L = gd_layout<T>(a.P);
+    int warps = (int)((kMaxSmemPerBlock - L.ef_bytes) / L.warp_bytes);
+    if (warps > 8) warps = 8;
+    if (warps < 1) return (int)cudaErrorInvalidValue;
+    const size_t smem = L.ef_bytes + (size_t)warps * L.warp_bytes;
+    auto k = gll_deriv_kernel<T>;
+    cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return (int)e;
+    int dev = 0, sms = 148, per = 1;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k, warps * 32, smem);
+    if (per < 1) per = 1;
+    const long long tiles = (a.nrows + 31) / 32;
+    long long grid = (long long)sms * per;
+    const long long need = (tiles + warps - 1) / warps;
+    if (grid > need) grid = need;
+    if (grid < 1) return 0;
+    return (int)launch_k(k, dim3((unsigned)grid), dim3(warps * 32), smem, s, a, L);
+}
+
+int launch_gll_deriv(int io_double, const GllDerivArgs& a, cudaStream_t s)
+{
+    if (a.P < 2 || a.P > 129 || (a.order != 1 && a.order != 2)) return (int)cudaErrorInvalidValue;
+    return io_double ? launch_gll_deriv_mma(a, s) : run_gll_deriv<float>(a, s);
+}
+
+}  // namespace helm

@@ -136,6 +136,15 @@ __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commi
 __device__ __forceinline__ void cp_async_wait_prev() { asm volatile("cp.async.wait_group 1;\n" ::); }
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::); }
 
+// One FP64 tensor-core product C += A B of m8n8k4 (g = lane / 4, q = lane % 4):
+// A[g][q], B[q][g], C[g][2 q] and C[g][2 q + 1] per lane.
+__device__ __forceinline__ void dmma_8x8x4(double& c0, double& c1, double a, double b)
+{
+    asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};\n"
+                 : "+d"(c0), "+d"(c1)
+                 : "d"(a), "d"(b));
+}
+
 // Programmatic dependent launch.  Every kernel of a solve is launched with the
 // programmatic-serialization attribute, so it may be scheduled while the
 // previous kernel in the stream is still finishing; pdl_enter() then waits

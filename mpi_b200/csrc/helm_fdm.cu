@@ -504,12 +504,7 @@ size_t fdm_fast_smem_bytes(int prec, int ld)
 // Fragment layout of m8n8k4 .f64 (g = lane / 4, q = lane % 4):
 //   A[g][q];  B[q][g];  C[g][2 q], C[g][2 q + 1].
 
-__device__ __forceinline__ void dmma_8x8x4(double& c0, double& c1, double a, double b)
-{
-    asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};\n"
-                 : "+d"(c0), "+d"(c1)
-                 : "d"(a), "d"(b));
-}
+// dmma_8x8x4: helm_device.cuh
 
 template <int NSS, int NT, int WARPS>
 struct MmaShape {

@@ -147,6 +147,28 @@ __device__ __forceinline__ void c2r_lambda_sum(const FftArgs& a, double acc)
     }
 }
 
+// Spectral derivative on the C2R load: multiply half-spectrum row k of both
+// real columns by (i w K)^order, K = k below L/2 and K = k - L = -L/2 at L/2
+// (FirstDerivativeFourierX / SecondDerivativeFourierX, Fourier_Quadrature.cpp:
+// 1400-1407, 1630-1637).  The caller then drops the imaginary parts at k = 0
+// and L/2, as the reference's real part of the inverse transform does.
+template <typename T, int L>
+__device__ __forceinline__ void deriv_mul(const FftArgs& a, int k, cplx_t<T>& A, cplx_t<T>& B)
+{
+    if (!a.deriv_order) return;
+    const double K = (k < L / 2) ? (double)k : (double)(k - L);
+    const double wk = a.deriv_w * K;
+    if (a.deriv_order == 1) {
+        const T m = (T)wk;
+        A = mk(-m * A.y, m * A.x);
+        B = mk(-m * B.y, m * B.x);
+    } else {
+        const T m = (T)(-wk * wk);
+        A = mk(m * A.x, m * A.y);
+        B = mk(m * B.x, m * B.y);
+    }
+}
+
 template <typename T, typename TIO, int L, int DIR, int MODE, int THREADS, int SMALL>
 __global__ void __launch_bounds__(THREADS) fft_kernel(FftArgs a, long long total_cols)
 {
@@ -183,6 +205,7 @@ __global__ void __launch_bounds__(THREADS) fft_kernel(FftArgs a, long long total
                 A = in[(long long)k * a.in_row + c0];
                 if (has1) B = in[(long long)k * a.in_row + c1];
             }
+            deriv_mul<T, L>(a, k, A, B);
             if (k == 0 || k == L / 2) { A.y = 0; B.y = 0; }
             sm[k * CT + cl] = mk(A.x - B.y, A.y + B.x);
             if (k != 0 && k != L / 2) sm[(L - k) * CT + cl] = mk(A.x + B.y, B.x - A.y);
@@ -416,6 +439,7 @@ __global__ void __launch_bounds__(THREADS) fft_pipe_kernel(FftArgs a, long long 
                 const int k = tc + j * TPC;
                 if (k <= L / 2) {
                     C Aj = A[j], Bj = B[j];
+                    deriv_mul<T, L>(a, k, Aj, Bj);
                     if (k == 0 || k == L / 2) { Aj.y = 0; Bj.y = 0; }
                     sm[k * CT + cl] = mk(Aj.x - Bj.y, Aj.y + Bj.x);
                     if (k != 0 && k != L / 2) sm[(L - k) * CT + cl] = mk(Aj.x + Bj.y, Bj.x - Aj.y);

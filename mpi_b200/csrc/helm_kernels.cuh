@@ -53,6 +53,11 @@ struct FftArgs {
     // when set, the pass writes 0 to *zero_out first (the lambda sum of the same
     // solve's last pass starts from it; no separate memset)
     double* zero_out;
+    // C2R only: spectral derivative, the half-spectrum row k is multiplied by
+    // (i deriv_w K)^deriv_order on load, K = k below L/2 and -L/2 at L/2
+    // (0: no derivative)
+    int deriv_order;
+    double deriv_w;
 };
 
 // Finite-difference variant: one tridiagonal solve along z per spectrum row.
@@ -110,6 +115,21 @@ struct RowArgs {
     // pl = A^-T (DN - D0), pr = 0
     int periodic;
 };
+
+// Derivative along the GLL direction of every row of P values: du = M u with
+// M the plan's scaled first (order 1, anti-centrosymmetric) or second (order 2,
+// centrosymmetric) derivative matrix, applied through its even/odd fold.
+struct GllDerivArgs {
+    const void* in;
+    void* out;
+    const double* M;        // [P][P] row-major, FP64
+    int P, order;
+    long long nrows;        // rows of P values
+    int rows_per_x;         // rows in one x row (Ny in 3D, 1 in 2D)
+    int nx;                 // x rows per element
+    long long x_stride, elem_stride;  // in elements of the io type
+};
+int launch_gll_deriv(int io_double, const GllDerivArgs& a, cudaStream_t s);
 
 // Launchers (helm_kernels.cu).  Return a cudaError_t.
 // T: compute precision (0 = float, 1 = double); io: real element bytes for

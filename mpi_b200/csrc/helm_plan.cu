@@ -537,7 +537,10 @@ static int setup_plan(Plan& p)
     p.nrows = (long long)nkx * Nyf;
     p.elem_spec = p.nrows * N;
     int st;
-    if ((st = p.alloc(&p.d_spec, (size_t)p.Ns * p.batch * p.elem_spec * (td ? 16 : 8)))) return st;
+    // the spectrum scratch also holds the half spectra of a derivative along y
+    // (Nx x (Ny/2+1) rows per element), larger than the solve's when Nx > Ny
+    const long long spec_elems = std::max(p.elem_spec, p.dim == 3 ? (long long)p.Nx * (p.Ny / 2 + 1) * N : 0LL);
+    if ((st = p.alloc(&p.d_spec, (size_t)p.Ns * p.batch * spec_elems * (td ? 16 : 8)))) return st;
     auto up_tw = [&](int L, void** d) -> int {
         if (td) { auto t = twiddles<double>(L); return p.upload(d, t.data(), t.size() * sizeof(double)); }
         auto t = twiddles<float>(L);
@@ -552,6 +555,8 @@ static int setup_plan(Plan& p)
     if ((st = p.upload((void**)&p.d_homs, homs.data(), homs.size() * sizeof(double)))) return st;
     if ((st = p.upload((void**)&p.d_d0, D.data(), N * sizeof(double)))) return st;
     if ((st = p.upload((void**)&p.d_dN, D.data() + (size_t)(N - 1) * N, N * sizeof(double)))) return st;
+    if ((st = p.upload((void**)&p.d_Dfull, D.data(), (size_t)N * N * sizeof(double)))) return st;
+    if ((st = p.upload((void**)&p.d_D2full, D2.data(), (size_t)N * N * sizeof(double)))) return st;
     // refinement: interior D2 column-major with leading dimension ld
     std::vector<double> d2t((size_t)n * ld, 0.0);
     for (int k = 0; k < n; ++k)
@@ -602,9 +607,11 @@ struct AdjOut {
 static int fft_pass(Plan& p, int L, int mode, int dir, const void* in, void* out, long long in_row, long long out_row,
                     long long in_batch, long long out_batch, int ncols, int nbatch, double scale, const void* tw,
                     const double* gl, const double* gr, bool inject, bool io_double, int stage, cudaStream_t s,
-                    const AdjOut* adj = nullptr)
+                    const AdjOut* adj = nullptr, int deriv_order = 0, double deriv_w = 0.0)
 {
     FftArgs a{};
+    a.deriv_order = deriv_order;
+    a.deriv_w = deriv_w;
     if (adj && mode == FFT_C2R) {
         a.adj_mode = p.fd ? 2 : 1;
         a.adj_P = p.N;
@@ -912,6 +919,72 @@ int solve_adjoint(Plan& p, const double* ubar, double* fbar, double* glbar, doub
     return run_pipeline(p, ubar, nullptr, nullptr, fbar, true, s, &adj);
 }
 
+// du = M u along the GLL index of every row (helm_deriv.cu).
+int gll_derivative(Plan& p, int order, const void* u, void* du, cudaStream_t s)
+{
+    if (p.fd || p.batch > 1 || !p.d_Dfull) {
+        g_last_error = "GLL derivative needs a Fourier x GLL plan";
+        return HELM_ERR_UNSUPPORTED;
+    }
+    GllDerivArgs a{};
+    a.in = u;
+    a.out = du;
+    a.M = order == 1 ? p.d_Dfull : p.d_D2full;
+    a.P = p.N;
+    a.order = order;
+    a.nx = p.Nx;
+    a.rows_per_x = p.dim == 3 ? p.Ny : 1;
+    a.nrows = (long long)p.Ns * p.Nx * a.rows_per_x;
+    a.x_stride = p.x_stride;
+    a.elem_stride = p.elem_stride;
+    const int io_double = (p.precision != HELM_FP32 || p.io_bytes == 8) ? 1 : 0;
+    const int e = launch_gll_deriv(io_double, a, s);
+    if (e) return set_cuda_error((cudaError_t)e, "GLL derivative launch");
+    return HELM_OK;
+}
+
+// Spectral derivative along x (axis 0) or y (axis 1, 3D): a real-to-complex
+// pass along the axis into the spectrum scratch, then the complex-to-real pass
+// back with the multiplier (i 2 pi K / L)^order applied on its load.
+int fourier_derivative(Plan& p, int axis, int order, const void* u, void* du, cudaStream_t s)
+{
+    if (p.batch > 1) { g_last_error = "derivative of a batched plan"; return HELM_ERR_UNSUPPORTED; }
+    const int N = p.N;
+    const bool tdbl = p.precision != HELM_FP32;
+    const size_t celem = tdbl ? 16 : 8;
+    int st;
+    if (axis == 0) {
+        const long long cols = (long long)(p.dim == 3 ? p.Ny : 1) * N;
+        const double w = 2.0 * kRefPi / p.Lx;
+        if ((st = fft_pass(p, p.Nx, FFT_R2C, -1, u, p.d_spec, p.x_stride, cols, p.elem_stride, p.elem_spec, (int)cols,
+                           p.Ns, 1.0, p.d_tw_x, nullptr, nullptr, false, false, 0, s)))
+            return st;
+        return fft_pass(p, p.Nx, FFT_C2R, 1, p.d_spec, du, cols, p.x_stride, p.elem_spec, p.elem_stride, (int)cols,
+                        p.Ns, 1.0 / p.Nx, p.d_tw_x, nullptr, nullptr, false, false, 3, s, nullptr, order, w);
+    }
+    if (axis != 1 || p.dim != 3) {
+        g_last_error = "axis must be 0 (x) or, for 3D plans, 1 (y)";
+        return HELM_ERR_INVALID;
+    }
+    // y rows of one element are uniform batches when elements are packed back to back
+    const double w = 2.0 * kRefPi / p.Ly;
+    const long long hspec = (long long)(p.Ny / 2 + 1) * N;  // one x row's half spectrum
+    const bool uniform = p.elem_stride == (long long)p.Nx * p.x_stride;
+    const int nb = uniform ? p.Ns * p.Nx : p.Nx;
+    for (int e = 0; e < (uniform ? 1 : p.Ns); ++e) {
+        const char* ue = static_cast<const char*>(u) + (size_t)e * p.elem_stride * (tdbl || p.io_bytes == 8 ? 8 : 4);
+        char* de = static_cast<char*>(du) + (size_t)e * p.elem_stride * (tdbl || p.io_bytes == 8 ? 8 : 4);
+        char* sp = static_cast<char*>(p.d_spec) + (size_t)e * p.Nx * hspec * celem;
+        if ((st = fft_pass(p, p.Ny, FFT_R2C, -1, ue, sp, N, N, p.x_stride, hspec, N, nb, 1.0, p.d_tw_y, nullptr,
+                           nullptr, false, false, 0, s)))
+            return st;
+        if ((st = fft_pass(p, p.Ny, FFT_C2R, 1, sp, de, N, N, hspec, p.x_stride, N, nb, 1.0 / p.Ny, p.d_tw_y, nullptr,
+                           nullptr, false, false, 3, s, nullptr, order, w)))
+            return st;
+    }
+    return HELM_OK;
+}
+
 // Finite-difference variant: the second-order stencil of HypreFDM
 // (HelmholtzSolvers/HypreFDM/src/Helmholtz3D_MPI.cpp:297-410) with periodic x
 // and y (dx = Lx/Nx, dy = Ly/Ny) and Nz interior points in z (dz = Lz/(Nz+1)),
@@ -1208,6 +1281,30 @@ int helm_solve_adjoint(helm_plan_t plan, const double* ubar, double* fbar, doubl
     cudaGetDevice(&cur);
     if (cur != p.device) cudaSetDevice(p.device);
     int st = helm::solve_adjoint(p, ubar, fbar, glbar, grbar, u, lambda_bar, static_cast<cudaStream_t>(stream));
+    if (cur != p.device) cudaSetDevice(cur);
+    return st;
+}
+
+int helm_gll_derivative(helm_plan_t plan, int order, const void* u, void* du, void* stream)
+{
+    if (!plan || !u || !du || (order != 1 && order != 2)) return HELM_ERR_INVALID;
+    Plan& p = *reinterpret_cast<Plan*>(plan);
+    int cur = 0;
+    cudaGetDevice(&cur);
+    if (cur != p.device) cudaSetDevice(p.device);
+    int st = helm::gll_derivative(p, order, u, du, static_cast<cudaStream_t>(stream));
+    if (cur != p.device) cudaSetDevice(cur);
+    return st;
+}
+
+int helm_fourier_derivative(helm_plan_t plan, int axis, int order, const void* u, void* du, void* stream)
+{
+    if (!plan || !u || !du || (order != 1 && order != 2)) return HELM_ERR_INVALID;
+    Plan& p = *reinterpret_cast<Plan*>(plan);
+    int cur = 0;
+    cudaGetDevice(&cur);
+    if (cur != p.device) cudaSetDevice(p.device);
+    int st = helm::fourier_derivative(p, axis, order, u, du, static_cast<cudaStream_t>(stream));
     if (cur != p.device) cudaSetDevice(cur);
     return st;
 }

@@ -49,6 +49,8 @@ struct Plan {
     double* d_d0 = nullptr;
     double* d_dN = nullptr;
     double* d_d2t = nullptr;
+    double* d_Dfull = nullptr;   // [N][N] scaled first-derivative matrix (derivative helpers)
+    double* d_D2full = nullptr;  // [N][N] second-derivative matrix
     // adjoint (transposed) solve data, FDM plans with one element
     bool adj_ready = false;
     void* d_vtT = nullptr;        // column-major V^T

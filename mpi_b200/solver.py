@@ -137,6 +137,54 @@ class _PlanBase:
         L.check(st, "helm_solve_adjoint")
         return fbar, lam, glb, grb
 
+    # ------------------------------------------------------- derivatives --
+    def _derivative(self, axis: int, order: int, u: torch.Tensor, out: Optional[torch.Tensor], stream) -> torch.Tensor:
+        """axis: Fourier axes first (x; y in 3D), then the GLL axis."""
+        ns = self.Ns
+        full = self._shape(ns)
+        uv = u.unsqueeze(0) if (u.dim() == len(full) - 1 and ns == 1) else u
+        if tuple(uv.shape) != full or not u.is_cuda or u.dtype != self.io_dtype or not u.is_contiguous():
+            raise ValueError(f"u must be a contiguous CUDA {self.io_dtype} tensor of shape {full}")
+        if out is None:
+            out = torch.empty_like(u)
+        elif tuple(out.shape) != tuple(u.shape) or out.dtype != u.dtype or not out.is_contiguous():
+            raise ValueError("out does not match u")
+        if axis == self.dim - 1:
+            st = self._lib.helm_gll_derivative(self._plan, order, u.data_ptr(), out.data_ptr(), _stream_ptr(stream))
+            L.check(st, "helm_gll_derivative")
+        else:
+            if out.data_ptr() == u.data_ptr():
+                raise ValueError("a Fourier derivative cannot run in place")
+            st = self._lib.helm_fourier_derivative(self._plan, axis, order, u.data_ptr(), out.data_ptr(),
+                                                   _stream_ptr(stream))
+            L.check(st, "helm_fourier_derivative")
+        return out
+
+    def FirstDerivativeX(self, u, out=None, stream=None):
+        """Spectral d/dx (Fourier_Quadrature.cpp FirstDerivativeFourierX)."""
+        return self._derivative(0, 1, u, out, stream)
+
+    def SecondDerivativeX(self, u, out=None, stream=None):
+        return self._derivative(0, 2, u, out, stream)
+
+    def FirstDerivativeY(self, u, out=None, stream=None):
+        """2D: GLL d/dy per element (NonPeriodic2D_MPI.cpp:497-519); 3D: spectral d/dy."""
+        return self._derivative(1, 1, u, out, stream)
+
+    def SecondDerivativeY(self, u, out=None, stream=None):
+        return self._derivative(1, 2, u, out, stream)
+
+    def FirstDerivativeZ(self, u, out=None, stream=None):
+        """3D: GLL d/dz per element (NonPeriodic3D_MPI.cpp:632-656)."""
+        if self.dim != 3:
+            raise ValueError("a 2D plan has no z direction")
+        return self._derivative(2, 1, u, out, stream)
+
+    def SecondDerivativeZ(self, u, out=None, stream=None):
+        if self.dim != 3:
+            raise ValueError("a 2D plan has no z direction")
+        return self._derivative(2, 2, u, out, stream)
+
     def enable_stage_timing(self, enable: bool = True) -> None:
         L.check(self._lib.helm_plan_set_stage_timing(self._plan, int(enable)), "helm_plan_set_stage_timing")
 

@@ -523,6 +523,63 @@ int orc_psolve3d(int Nx, int Ny, int N, int Ns, double Lx, double Ly, double Lz,
     return st;
 }
 
+/* ------------------------------------------------ derivative helpers -- */
+
+/* du = M u for `nrows` rows of N values, M the scaled first (order 1) or
+ * second (order 2) GLL derivative matrix of one element of length L/Ns
+ * (FirstDerivativeY / SecondDerivativeY, NonPeriodic2D_MPI.cpp:497-542;
+ * FirstDerivativeZ / SecondDerivativeZ, NonPeriodic3D_MPI.cpp:632-683). */
+void orc_gll_deriv(int N, int Ns, double L, int order, long nrows, const double* u, double* du)
+{
+    double* y = malloc(sizeof(double) * (Ns * (N - 1) + 1));
+    double* D = malloc(sizeof(double) * N * N);
+    double* D2 = malloc(sizeof(double) * N * N);
+    orc_gll_setup(N, Ns, L, y, D, D2);
+    const double* M = order == 1 ? D : D2;
+    for (long r = 0; r < nrows; ++r)
+        for (int j = 0; j < N; ++j) {
+            double a = 0.0;
+            for (int k = 0; k < N; ++k) a += M[j * N + k] * u[r * N + k];
+            du[r * N + j] = a;
+        }
+    free(y); free(D); free(D2);
+}
+
+/* Spectral derivative of the real array u[n0][n1][n2] along axis 0 or 1:
+ * forward DFT, multiply by 2 pi K (order 1, times i) or -4 pi^2 K^2 (order 2)
+ * with K = k for k < n/2 and k - n otherwise, inverse DFT (/n), real part,
+ * divided by L^order (FirstDerivativeFourierX..Y / SecondDerivativeFourierX..Y,
+ * Fourier_Quadrature.cpp:1387-1834). */
+void orc_fourier_deriv(int n0, int n1, int n2, int axis, int order, double L, const double* u, double* du)
+{
+    int n = axis == 0 ? n0 : n1;
+    long st = axis == 0 ? (long)n1 * n2 : n2;
+    double* re = malloc(sizeof(double) * n);
+    double* im = malloc(sizeof(double) * n);
+    int outer = axis == 0 ? 1 : n0, inner = axis == 0 ? n1 * n2 : n2;
+    for (int o = 0; o < outer; ++o)
+        for (int c = 0; c < inner; ++c) {
+            long base = (axis == 0 ? 0 : (long)o * n1 * n2) + c;
+            for (int i = 0; i < n; ++i) { re[i] = u[base + i * st]; im[i] = 0.0; }
+            orc_fft(n, re, im, 1, -1);
+            for (int i = 0; i < n; ++i) {
+                double K = (i < n / 2) ? (double)i : (double)(i - n);
+                if (order == 1) {
+                    double t = re[i];
+                    re[i] = -2.0 * ORC_PI * K * im[i];
+                    im[i] = 2.0 * ORC_PI * K * t;
+                } else {
+                    re[i] *= -4.0 * ORC_PI * ORC_PI * K * K;
+                    im[i] *= -4.0 * ORC_PI * ORC_PI * K * K;
+                }
+            }
+            orc_fft(n, re, im, 1, +1);
+            double sc = (order == 1 ? L : L * L) * n;
+            for (int i = 0; i < n; ++i) du[base + i * st] = re[i] / sc;
+        }
+    free(re); free(im);
+}
+
 /* The collocation residual of a 3D solution, computed directly in FP64:
  * interior GLL rows  r = f - (u_xx + u_yy + D2 u - lambda u)  (spectral x/y
  * derivatives), boundary rows r = g - (Robin operator) u, for Ns = 1.

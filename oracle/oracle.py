@@ -63,6 +63,10 @@ def lib():
         _lib.orc_solve2d.argtypes = [_I, _I, _I] + [_D] * 7 + [_P] * 4
         _lib.orc_solve3d.restype = _I
         _lib.orc_solve3d.argtypes = [_I, _I, _I, _I] + [_D] * 8 + [_P] * 4
+        _lib.orc_gll_deriv.restype = None
+        _lib.orc_gll_deriv.argtypes = [_I, _I, _D, _I, ctypes.c_long, _P, _P]
+        _lib.orc_fourier_deriv.restype = None
+        _lib.orc_fourier_deriv.argtypes = [_I] * 5 + [_D, _P, _P]
         _lib.orc_psolve2d.restype = _I
         _lib.orc_psolve2d.argtypes = [_I, _I, _I] + [_D] * 3 + [_P] * 2
         _lib.orc_psolve3d.restype = _I
@@ -183,6 +187,24 @@ def psolve3d(f, *, Lx, Ly, Lz, lam):
     return u[0] if squeeze else u
 
 
+def gll_deriv(u, *, N, Ns, L, order):
+    """du = D u (order 1) or D2 u (order 2) along the last axis (length N) of u,
+    with the element matrices of an Ns-element GLL grid of total length L."""
+    u = _c64(u)
+    du = np.zeros_like(u)
+    lib().orc_gll_deriv(N, Ns, L, order, u.size // N, _p(u), _p(du))
+    return du
+
+
+def fourier_deriv(u, *, axis, order, L):
+    """Spectral derivative of a real [n0, n1(, n2)] array along axis 0 or 1."""
+    u = _c64(u)
+    shp = u.shape + (1,) * (3 - u.ndim)
+    du = np.zeros_like(u)
+    lib().orc_fourier_deriv(shp[0], shp[1], shp[2], axis, order, L, _p(u), _p(du))
+    return du
+
+
 def residual3d(u, f, gl, gr, *, Lx, Ly, Lz, lam, bc=(0.0, 1.0, 0.0, 1.0)):
     """Max-abs collocation residual (FP64) of a single-element 3D solution."""
     u = _c64(u)
@@ -277,3 +299,54 @@ def ref_psolve3d(f, *, xl, xr, yl, yr, zl, zr, lam, return_time=False):
         raise RuntimeError(f"reference chose Ns={ns}, expected {Ns}")
     out = u[0] if squeeze else u
     return (out, ms[0]) if return_time else out
+
+
+def _ref_deriv(which: int):
+    lib_ = _ref(which)
+    if not hasattr(lib_, "_deriv_ready"):
+        if which == 2:
+            lib_.oracle_ref2d_deriv_y.restype = _I
+            lib_.oracle_ref2d_deriv_y.argtypes = [_I] * 3 + [_D] * 2 + [_I] + [_P] * 2
+            lib_.oracle_ref_fourier_deriv_2d.restype = None
+            lib_.oracle_ref_fourier_deriv_2d.argtypes = [_I] * 4 + [_D] + [_P] * 2
+        else:
+            lib_.oracle_ref3d_deriv_z.restype = _I
+            lib_.oracle_ref3d_deriv_z.argtypes = [_I] * 4 + [_D] * 2 + [_I] + [_P] * 2
+            lib_.oracle_ref_fourier_deriv_3d.restype = None
+            lib_.oracle_ref_fourier_deriv_3d.argtypes = [_I] * 5 + [_D] + [_P] * 2
+        lib_._deriv_ready = True
+    return lib_
+
+
+def ref_gll_deriv_2d(u, *, yl, yr, order):
+    """The reference's NonPeriodic2D FirstDerivativeY / SecondDerivativeY.  u: [Ns, Nx, N]."""
+    u = _c64(u)
+    Ns, Nx, N = u.shape
+    du = np.zeros_like(u)
+    ns = _ref_deriv(2).oracle_ref2d_deriv_y(Nx, Ns * N, N, yl, yr, order, _p(u), _p(du))
+    if ns != Ns:
+        raise RuntimeError(f"reference chose Ns={ns}, expected {Ns}")
+    return du
+
+
+def ref_gll_deriv_3d(u, *, zl, zr, order):
+    """The reference's NonPeriodic3D FirstDerivativeZ / SecondDerivativeZ.  u: [Ns, Nx, Ny, N]."""
+    u = _c64(u)
+    Ns, Nx, Ny, N = u.shape
+    du = np.zeros_like(u)
+    ns = _ref_deriv(3).oracle_ref3d_deriv_z(Nx, Ny, Ns * N, N, zl, zr, order, _p(u), _p(du))
+    if ns != Ns:
+        raise RuntimeError(f"reference chose Ns={ns}, expected {Ns}")
+    return du
+
+
+def ref_fourier_deriv(u, *, axis, order, L):
+    """The reference's FirstDerivativeFourierX/Y, SecondDerivativeFourierX/Y on a
+    real [n0, n1] or [n0, n1, n2] array (Fourier_Quadrature.cpp:1387-1834)."""
+    u = _c64(u)
+    du = np.zeros_like(u)
+    if u.ndim == 2:
+        _ref_deriv(2).oracle_ref_fourier_deriv_2d(u.shape[0], u.shape[1], axis, order, L, _p(u), _p(du))
+    else:
+        _ref_deriv(3).oracle_ref_fourier_deriv_3d(u.shape[0], u.shape[1], u.shape[2], axis, order, L, _p(u), _p(du))
+    return du

@@ -61,3 +61,51 @@ extern "C" int oracle_ref2d_solve(int nx, int ny, int n,
     DestroyPDEPlan();
     return ns;
 }
+
+// The reference's GLL derivative of a 2D field, FirstDerivativeY / SecondDerivativeY
+// (NonPeriodic2D_MPI.cpp:497-542) on the plan's grid.  u, du: [Ns][Nx][N].
+extern "C" int oracle_ref2d_deriv_y(int nx, int ny, int n, double yl_, double yr_, int order, const double* u,
+                                    double* du)
+{
+    Rank = 0;
+    size = 1;
+    CreatePDEPlan(nx, ny, n, 0.0, 1.0, yl_, yr_);
+    FieldVariable* V = new FieldVariable[Ns];
+    FieldVariable* W = new FieldVariable[Ns];
+    for (int jj = 0; jj < Ns; ++jj) { Allocate(V[jj].phi, NX, N); Allocate(W[jj].phi, NX, N); }
+    for (int jj = 0; jj < Ns; ++jj)
+        for (int i = 0; i < Nx; ++i)
+            for (int j = 0; j < N; ++j) V[jj].phi[i][j] = u[((size_t)jj * Nx + i) * N + j];
+    if (order == 1) FirstDerivativeY(W, V); else SecondDerivativeY(W, V);
+    for (int jj = 0; jj < Ns; ++jj)
+        for (int i = 0; i < Nx; ++i)
+            for (int j = 0; j < N; ++j) du[((size_t)jj * Nx + i) * N + j] = W[jj].phi[i][j];
+    int ns = Ns;
+    for (int jj = 0; jj < Ns; ++jj) { Deallocate(V[jj].phi, NX, N); Deallocate(W[jj].phi, NX, N); }
+    delete[] V;
+    delete[] W;
+    DestroyPDEPlan();
+    return ns;
+}
+
+// The reference's spectral derivatives of a real [n0][n1] array
+// (FirstDerivativeFourierX / Y, SecondDerivativeFourierX / Y, Fourier_Quadrature.cpp:1420-1716).
+extern "C" void oracle_ref_fourier_deriv_2d(int n0, int n1, int axis, int order, double L, const double* u, double* du)
+{
+    CreateFFTPlan(n0 > n1 ? n0 : n1);
+    double **F, **G;
+    Allocate(F, n0, n1);
+    Allocate(G, n0, n1);
+    for (int i = 0; i < n0; ++i)
+        for (int j = 0; j < n1; ++j) F[i][j] = u[(size_t)i * n1 + j];
+    if (axis == 0) {
+        if (order == 1) FirstDerivativeFourierX(G, F, n0, n1, L); else SecondDerivativeFourierX(G, F, n0, n1, L);
+    } else {
+        if (order == 1) FirstDerivativeFourierY(G, F, n0, n1, L); else SecondDerivativeFourierY(G, F, n0, n1, L);
+    }
+    for (int i = 0; i < n0; ++i)
+        for (int j = 0; j < n1; ++j) du[(size_t)i * n1 + j] = G[i][j];
+    Deallocate(F, n0, n1);
+    Deallocate(G, n0, n1);
+    DestroyFFTPlan(n0 > n1 ? n0 : n1);
+}

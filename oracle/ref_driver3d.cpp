@@ -63,3 +63,56 @@ extern "C" int oracle_ref3d_solve(int nx, int ny, int nz, int n,
     DestroyPDEPlan();
     return ns;
 }
+
+// The reference's GLL derivative of a 3D field, FirstDerivativeZ / SecondDerivativeZ
+// (NonPeriodic3D_MPI.cpp:632-683).  u, du: [Ns][Nx][Ny][N].
+extern "C" int oracle_ref3d_deriv_z(int nx, int ny, int nz, int n, double zl_, double zr_, int order,
+                                    const double* u, double* du)
+{
+    Rank = 0;
+    size = 1;
+    CreatePDEPlan(nx, ny, nz, n, 0.0, 1.0, 0.0, 1.0, zl_, zr_);
+    FieldVariable* V = new FieldVariable[Ns];
+    FieldVariable* W = new FieldVariable[Ns];
+    for (int kk = 0; kk < Ns; ++kk) { Allocate(V[kk].phi, 2 * Nx, NY, N); Allocate(W[kk].phi, 2 * Nx, NY, N); }
+    for (int kk = 0; kk < Ns; ++kk)
+        for (int i = 0; i < Nx; ++i)
+            for (int j = 0; j < Ny; ++j)
+                for (int k = 0; k < N; ++k) V[kk].phi[i][j][k] = u[(((size_t)kk * Nx + i) * Ny + j) * N + k];
+    if (order == 1) FirstDerivativeZ(W, V); else SecondDerivativeZ(W, V);
+    for (int kk = 0; kk < Ns; ++kk)
+        for (int i = 0; i < Nx; ++i)
+            for (int j = 0; j < Ny; ++j)
+                for (int k = 0; k < N; ++k) du[(((size_t)kk * Nx + i) * Ny + j) * N + k] = W[kk].phi[i][j][k];
+    int ns = Ns;
+    for (int kk = 0; kk < Ns; ++kk) { Deallocate(V[kk].phi, 2 * Nx, NY, N); Deallocate(W[kk].phi, 2 * Nx, NY, N); }
+    delete[] V;
+    delete[] W;
+    DestroyPDEPlan();
+    return ns;
+}
+
+// The reference's spectral derivatives of a real [n0][n1][n2] array along x or y
+// (Fourier_Quadrature.cpp:1494-1575, 1721-1800).
+extern "C" void oracle_ref_fourier_deriv_3d(int n0, int n1, int n2, int axis, int order, double L, const double* u,
+                                            double* du)
+{
+    CreateFFTPlan(n0 > n1 ? n0 : n1);
+    double ***F, ***G;
+    Allocate(F, n0, n1, n2);
+    Allocate(G, n0, n1, n2);
+    for (int i = 0; i < n0; ++i)
+        for (int j = 0; j < n1; ++j)
+            for (int k = 0; k < n2; ++k) F[i][j][k] = u[((size_t)i * n1 + j) * n2 + k];
+    if (axis == 0) {
+        if (order == 1) FirstDerivativeFourierX(G, F, n0, n1, n2, L); else SecondDerivativeFourierX(G, F, n0, n1, n2, L);
+    } else {
+        if (order == 1) FirstDerivativeFourierY(G, F, n0, n1, n2, L); else SecondDerivativeFourierY(G, F, n0, n1, n2, L);
+    }
+    for (int i = 0; i < n0; ++i)
+        for (int j = 0; j < n1; ++j)
+            for (int k = 0; k < n2; ++k) du[((size_t)i * n1 + j) * n2 + k] = G[i][j][k];
+    Deallocate(F, n0, n1, n2);
+    Deallocate(G, n0, n1, n2);
+    DestroyFFTPlan(n0 > n1 ? n0 : n1);
+}

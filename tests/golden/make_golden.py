@@ -82,6 +82,21 @@ def main():
     u = O.ref_psolve3d(f, xl=0.0, xr=1.0, yl=0.0, yr=2.0, zl=0.0, zr=1.5, lam=0.5)
     out["periodic_3d_ns3"] = dict(f=f, u=u, Nx=Nx, Ny=Ny, N=N, Ns=Ns, dom=[0.0, 1.0, 0.0, 2.0, 0.0, 1.5], lam=0.5)
 
+    # derivative helpers: the reference's spectral derivatives and GLL derivatives
+    drng = np.random.default_rng(20240603)
+    u2 = drng.standard_normal((16, 9))
+    u3 = drng.standard_normal((8, 16, 5))
+    ug2 = drng.standard_normal((3, 8, 9))
+    ug3 = drng.standard_normal((2, 4, 8, 7))
+    d = dict(u2=u2, u3=u3, ug2=ug2, ug3=ug3, L2=1.3, L3x=0.7, L3y=2.1, yl=-1.0, yr=1.0, zl=0.0, zr=1.5)
+    for order in (1, 2):
+        d[f"fx2_{order}"] = O.ref_fourier_deriv(u2, axis=0, order=order, L=1.3)
+        d[f"fx3_{order}"] = O.ref_fourier_deriv(u3, axis=0, order=order, L=0.7)
+        d[f"fy3_{order}"] = O.ref_fourier_deriv(u3, axis=1, order=order, L=2.1)
+        d[f"gy2_{order}"] = O.ref_gll_deriv_2d(ug2, yl=-1.0, yr=1.0, order=order)
+        d[f"gz3_{order}"] = O.ref_gll_deriv_3d(ug3, zl=0.0, zr=1.5, order=order)
+    out["derivatives"] = d
+
     for name, d in out.items():
         np.savez_compressed(os.path.join(HERE, name + ".npz"), **{k: np.asarray(v) for k, v in d.items()})
         print(name, {k: np.asarray(v).shape for k, v in d.items()})

@@ -105,6 +105,19 @@ def test_periodic_restatement_matches_reference_random():
     assert max_rel(a, b) < 1e-11
 
 
+@pytest.mark.parametrize("order", [1, 2])
+def test_derivative_restatement_matches_golden(order):
+    """Spectral (Fourier_Quadrature.cpp:1387-1834) and GLL (NonPeriodic2D_MPI.cpp:497-542,
+    NonPeriodic3D_MPI.cpp:632-683) derivatives of the reference on seeded arrays."""
+    g = golden("derivatives")
+    L2, L3x, L3y = float(g["L2"]), float(g["L3x"]), float(g["L3y"])
+    assert max_rel(O.fourier_deriv(g["u2"], axis=0, order=order, L=L2), g[f"fx2_{order}"]) < 1e-13
+    assert max_rel(O.fourier_deriv(g["u3"], axis=0, order=order, L=L3x), g[f"fx3_{order}"]) < 1e-13
+    assert max_rel(O.fourier_deriv(g["u3"], axis=1, order=order, L=L3y), g[f"fy3_{order}"]) < 1e-13
+    assert max_rel(O.gll_deriv(g["ug2"], N=9, Ns=3, L=2.0, order=order), g[f"gy2_{order}"]) < 1e-13
+    assert max_rel(O.gll_deriv(g["ug3"], N=7, Ns=2, L=1.5, order=order), g[f"gz3_{order}"]) < 1e-13
+
+
 def test_collocation_residual_3d():
     g = golden("robin_3d")
     xl, xr, yl, yr, zl, zr = g["dom"]
