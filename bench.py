@@ -52,7 +52,7 @@ def _args():
     ap.add_argument("--warmup", type=int, default=20)
     ap.add_argument("--impl", choices=("ours", "reference"), default="ours")
     ap.add_argument("--skip-cpu-baseline", action="store_true", help="omit the CPU leg (profiling runs)")
-    ap.add_argument("--skip-side", action="store_true", help="omit the batch / adjoint / finite-difference legs")
+    ap.add_argument("--skip-side", action="store_true", help="omit the batch / adjoint / finite-difference / periodic / derivative legs")
     ap.add_argument("--profile-case", choices=("fp64", "fp32_refine", "fp32", "fd64", "fd32", "batch"),
                     help="run three untimed solves of one workload and exit (a small case for ncu captures)")
     return ap.parse_args()
@@ -406,6 +406,10 @@ def run_ours(args, ws, rank, local):
         _log("adjoint leg done")
         side["fd"] = _leg_fd(dev, flush, stream, st, wu, cpu=not args.skip_cpu_baseline)
         _log("fd leg done")
+        side["periodic"] = _leg_periodic(dev, flush, stream, st, wu, cpu=not args.skip_cpu_baseline)
+        _log("periodic leg done")
+        side["derivatives"] = _leg_derivatives(dev, flush, stream, st, wu)
+        _log("derivatives leg done")
     clk = clocks.stop()
 
     # max over ranks
@@ -478,6 +482,10 @@ BATCH_WORKLOAD = ("512 independent 2D problems, Nx from {32..512}, GLL order fro
                   "in [1e-2, 1e4], manufactured sin(3x)(1-y^2)e^y f on [0,2pi) x [-1,1], Dirichlet")
 ADJ_WORKLOAD = "3D Fourier 128 x Fourier 128 x GLL 65 (N=64), lambda=5, L = 0.5 ||u - u_obs||^2"
 FD_WORKLOAD = "finite-difference FFT/Thomas, 1024 x 1024 periodic x 256 interior points, Dirichlet, lambda=1"
+PER_WORKLOAD = ("3D Helmholtz periodic in all three directions, Fourier 256 x Fourier 256 x GLL 65 (N=64, one "
+                "element), lambda=10, seeded smooth field; plus the reference's stock Periodic3D test "
+                "(64 x 32 x 250, N=10: 25 elements, cyclic interface sweep)")
+DER_WORKLOAD = "derivatives of a 256 x 256 x 65 FP64 field on the GLL grid of the headline plan"
 
 
 def _ev_ms(fn, flush, stream, steps, warmup):
@@ -645,6 +653,76 @@ def _leg_fd(dev, flush, stream, steps, warmup, cpu=False):
         out["cpu_baseline"] = {"value": n * n * Nz / t / 1e9, "unit": "GDOF/s", "cores": 1, "kind": "port",
                                "sample": "the C restatement's FFT/tridiagonal solve of 256 x 256 x 256 (the "
                                          "workload's z size, 1/16 of its x-y plane), one core"}
+    return out
+
+
+def _leg_periodic(dev, flush, stream, steps, warmup, cpu=False):
+    import numpy as np
+    import torch
+
+    from mpi_b200 import Periodic3D
+    from mpi_b200 import workloads as W
+
+    f = torch.from_numpy(W.smooth_field_3d(NX, NY, NGLL, seed=SEED)).to(dev)
+    dof = NX * NY * NGLL
+    out = {"workload": PER_WORKLOAD, "dof_per_solve": dof}
+    us = {}
+    for prec in ("fp64", "fp32_refine"):
+        p = Periodic3D(NX, NY, NGLL, NGLL, *DOM, Lambda=LAM, precision=prec)
+        u = p.SolvePDE(f)
+        ms = _ev_ms(lambda: p.SolvePDE(f, out=u), flush, stream, steps, warmup)
+        out[prec] = {"value": dof / (ms * 1e-3) / 1e9, "unit": "GDOF/s", "ms_per_solve": ms}
+        us[prec] = u
+        p.DestroyPDEPlan()
+    out["rel_l2_refine_vs_fp64"] = float((us["fp32_refine"] - us["fp64"]).norm() / us["fp64"].norm())
+    fs, ue = W.stock_periodic_3d()
+    ps = Periodic3D(64, 32, 250, 10, 0.0, 1.0, 0.0, 1.0, 0.0, 1.0, Lambda=1.0)
+    fsd = torch.from_numpy(fs).to(dev)
+    us_ = ps.SolvePDE(fsd)
+    ms = _ev_ms(lambda: ps.SolvePDE(fsd, out=us_), flush, stream, steps, warmup)
+    out["stock_periodic_3d"] = {"value": fs.size / (ms * 1e-3) / 1e9, "unit": "GDOF/s", "ms_per_solve": ms,
+                                "max_err_vs_exact": float(np.abs(us_.cpu().numpy() - ue).max())}
+    ps.DestroyPDEPlan()
+    if cpu:
+        from oracle import oracle as O
+
+        O.build()
+        n = 64
+        fsmall = W.smooth_field_3d(n, n, NGLL, seed=SEED)
+        kind = "reference" if O.have_reference() else "port"
+        t0 = time.perf_counter()
+        if kind == "reference":
+            O.ref_psolve3d(fsmall, xl=DOM[0], xr=DOM[1], yl=DOM[2], yr=DOM[3], zl=DOM[4], zr=DOM[5], lam=LAM)
+        else:
+            O.psolve3d(fsmall, Lx=DOM[1] - DOM[0], Ly=DOM[3] - DOM[2], Lz=DOM[5] - DOM[4], lam=LAM)
+        t = time.perf_counter() - t0
+        out["cpu_baseline"] = {"value": n * n * NGLL / t / 1e9, "unit": "GDOF/s", "cores": 1, "kind": kind,
+                               "sample": "the reference's Periodic3D SolvePDE of 64 x 64 x 65 (1/16 of the "
+                                         "workload's x-y plane), one core"}
+    return out
+
+
+def _leg_derivatives(dev, flush, stream, steps, warmup):
+    """GLL-direction and spectral derivatives at the headline shape; HBM roofline
+    with algorithmic bytes = one read and one write of the field per call."""
+    import torch
+
+    from mpi_b200 import NonPeriodic3D
+
+    p = NonPeriodic3D(NX, NY, NGLL, NGLL, *DOM, Lambda=LAM)
+    u = torch.randn(NX, NY, NGLL, dtype=torch.float64, device=dev)
+    du = torch.empty_like(u)
+    peak, src = _peak_hbm()
+    nbytes = 2 * u.numel() * 8
+    out = {"workload": DER_WORKLOAD, "algorithmic_bytes": nbytes, "peak_gbs": peak, "peak_source": src}
+    for name, axis in (("d_dz_gll", "Z"), ("d_dx_fourier", "X"), ("d_dy_fourier", "Y")):
+        for order in (1, 2):
+            fn = getattr(p, ("First" if order == 1 else "Second") + "Derivative" + axis)
+            ms = _ev_ms(lambda: fn(u, out=du), flush, stream, steps, warmup)
+            gbs = nbytes / (ms * 1e-3) / 1e9
+            out[f"{name}_{order}"] = {"ms": ms, "achieved_gbs": gbs, "frac": gbs / peak,
+                                      "launches": 1 if axis == "Z" else 2}
+    p.DestroyPDEPlan()
     return out
 
 
