@@ -170,6 +170,19 @@ int helm_gll_derivative(helm_plan_t plan, int order, const void* u, void* du, vo
  * with a solve of the same plan on another stream. */
 int helm_fourier_derivative(helm_plan_t plan, int axis, int order, const void* u, void* du, void* stream);
 
+/* Output writers (host code; u is a HOST array in the plan's compact layout):
+ * the reference's WriteFile (NonPeriodic2D_MPI.cpp:571-650,
+ * NonPeriodic3D_MPI.cpp:713-795, and the Periodic twins) in the same text
+ * format -- fixed notation, 8 decimals, tab-separated, x fastest, then y, then
+ * the GLL node of each element (element boundaries twice).  helm_write_tecplot
+ * writes the TECPLOT branch (columns X, Y, [Z,] U, Exact; `exact` may be NULL
+ * for zeros, 2D plans get z = 0); helm_write_vtk the VISIT branch (legacy VTK
+ * structured grid, scalar Phi).  The reference picks the file name from its
+ * rank ("Output/Solution-%04d.tec"); here the caller passes `path`. */
+int helm_write_tecplot(helm_plan_t plan, const double* u, double (*exact)(double x, double y, double z),
+                       const char* path);
+int helm_write_vtk(helm_plan_t plan, const double* u, const char* path);
+
 /* Node coordinates: 2D y[Ns*(N-1)+1] / 3D z[...], and the scaled first and
  * second GLL derivative matrices D[N*N], D2[N*N] (row-major), host pointers,
  * any may be NULL.  The reference's globals y/z, Dy/Dz, Dyy/Dzz. */

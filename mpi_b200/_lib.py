@@ -37,7 +37,11 @@ EXPORTS = (
     "helm2d_batch_create", "helm_batch_offsets", "helm_batch_info", "helm_batch_set_graph",
     "helm_batch_solve", "helm_batch_destroy", "helm_plan_get_launch_variants", "helm_plan_set_launch_variants",
     "helm2d_periodic_plan_create", "helm3d_periodic_plan_create", "helm_gll_derivative", "helm_fourier_derivative",
+    "helm_write_tecplot", "helm_write_vtk",
 )
+
+# exact-solution callback of helm_write_tecplot: double exact(double x, double y, double z)
+EXACT_FN = ctypes.CFUNCTYPE(ctypes.c_double, ctypes.c_double, ctypes.c_double, ctypes.c_double)
 
 
 class HelmError(RuntimeError):
@@ -71,6 +75,8 @@ def lib() -> ctypes.CDLL:
     L.helm3d_plan_create.argtypes = [i, i, i, i, d, d, d, d, d, d, P(robin_t), d, i, i, P(vp)]
     L.helm_fd3d_plan_create.argtypes = [i, i, i, d, d, d, d, d, d, P(robin_t), d, i, P(vp)]
     L.helm_gll_derivative.argtypes = [vp, i, vp, vp, vp]
+    L.helm_write_tecplot.argtypes = [vp, vp, EXACT_FN, ctypes.c_char_p]
+    L.helm_write_vtk.argtypes = [vp, vp, ctypes.c_char_p]
     L.helm_fourier_derivative.argtypes = [vp, i, i, vp, vp, vp]
     L.helm2d_periodic_plan_create.argtypes = [i, i, i, d, d, d, d, d, i, i, P(vp)]
     L.helm3d_periodic_plan_create.argtypes = [i, i, i, i, d, d, d, d, d, d, d, i, i, P(vp)]

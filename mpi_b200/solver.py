@@ -185,6 +185,22 @@ class _PlanBase:
             raise ValueError("a 2D plan has no z direction")
         return self._derivative(2, 2, u, out, stream)
 
+    # ------------------------------------------------------------ output --
+    def WriteFile(self, u, path: str, exact=None, fmt: str = "tecplot") -> None:
+        """The reference's WriteFile: u (any device, the plan's shape) written to
+        `path` as a Tecplot point file (fmt "tecplot", with exact(x, y, z) beside
+        it; 2D plans get z = 0) or a legacy-VTK structured grid (fmt "vtk")."""
+        full = self._shape(self.Ns)
+        uh = u.detach().to("cpu", torch.float64).contiguous().reshape(full)
+        if fmt == "tecplot":
+            cb = L.EXACT_FN(exact) if exact is not None else L.EXACT_FN()
+            st = self._lib.helm_write_tecplot(self._plan, uh.data_ptr(), cb, path.encode())
+        elif fmt == "vtk":
+            st = self._lib.helm_write_vtk(self._plan, uh.data_ptr(), path.encode())
+        else:
+            raise ValueError("fmt must be 'tecplot' or 'vtk'")
+        L.check(st, "helm_write_" + fmt)
+
     def enable_stage_timing(self, enable: bool = True) -> None:
         L.check(self._lib.helm_plan_set_stage_timing(self._plan, int(enable)), "helm_plan_set_stage_timing")
 

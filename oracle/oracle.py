@@ -350,3 +350,30 @@ def ref_fourier_deriv(u, *, axis, order, L):
     else:
         _ref_deriv(3).oracle_ref_fourier_deriv_3d(u.shape[0], u.shape[1], u.shape[2], axis, order, L, _p(u), _p(du))
     return du
+
+
+def ref_write_tecplot(u, dom, workdir):
+    """The reference's WriteFile (TECPLOT) of u ([Ns, Nx, N] or [Ns, Nx, Ny, N]) on
+    the domain `dom`; returns the text of Output/Solution-0000.tec written under
+    `workdir` (exact = sin(x) cos(y) [* z])."""
+    u = _c64(u)
+    os.makedirs(os.path.join(workdir, "Output"), exist_ok=True)
+    cwd = os.getcwd()
+    os.chdir(workdir)
+    try:
+        if u.ndim == 3:
+            Ns, Nx, N = u.shape
+            lib_ = _ref(2)
+            lib_.oracle_ref2d_write.restype = _I
+            lib_.oracle_ref2d_write.argtypes = [_I] * 3 + [_D] * 4 + [_P]
+            lib_.oracle_ref2d_write(Nx, Ns * N, N, *dom, _p(u))
+        else:
+            Ns, Nx, Ny, N = u.shape
+            lib_ = _ref(3)
+            lib_.oracle_ref3d_write.restype = _I
+            lib_.oracle_ref3d_write.argtypes = [_I] * 4 + [_D] * 6 + [_P]
+            lib_.oracle_ref3d_write(Nx, Ny, Ns * N, N, *dom, _p(u))
+        with open(os.path.join("Output", "Solution-0000.tec")) as fh:
+            return fh.read()
+    finally:
+        os.chdir(cwd)

@@ -109,3 +109,26 @@ extern "C" void oracle_ref_fourier_deriv_2d(int n0, int n1, int axis, int order,
     Deallocate(G, n0, n1);
     DestroyFFTPlan(n0 > n1 ? n0 : n1);
 }
+
+// The reference's WriteFile (NonPeriodic2D_MPI.cpp:571-598, TECPLOT branch) of u
+// [Ns][Nx][N] with exact(x, y) = sin(x) cos(y); writes Output/Solution-0000.tec
+// under the current directory.
+static double oracle_exact_2d(const double x, const double y) { return sin(x) * cos(y); }
+extern "C" int oracle_ref2d_write(int nx, int ny, int n, double xl_, double xr_, double yl_, double yr_,
+                                  const double* u)
+{
+    Rank = 0;
+    size = 1;
+    CreatePDEPlan(nx, ny, n, xl_, xr_, yl_, yr_);
+    FieldVariable* V = new FieldVariable[Ns];
+    for (int jj = 0; jj < Ns; ++jj) Allocate(V[jj].phi, NX, N);
+    for (int jj = 0; jj < Ns; ++jj)
+        for (int i = 0; i < Nx; ++i)
+            for (int j = 0; j < N; ++j) V[jj].phi[i][j] = u[((size_t)jj * Nx + i) * N + j];
+    WriteFile(V, oracle_exact_2d);
+    int ns = Ns;
+    for (int jj = 0; jj < Ns; ++jj) Deallocate(V[jj].phi, NX, N);
+    delete[] V;
+    DestroyPDEPlan();
+    return ns;
+}

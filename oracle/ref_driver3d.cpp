@@ -116,3 +116,27 @@ extern "C" void oracle_ref_fourier_deriv_3d(int n0, int n1, int n2, int axis, in
     Deallocate(G, n0, n1, n2);
     DestroyFFTPlan(n0 > n1 ? n0 : n1);
 }
+
+// The reference's WriteFile (NonPeriodic3D_MPI.cpp:713-741, TECPLOT branch) of u
+// [Ns][Nx][Ny][N] with exact(x, y, z) = sin(x) cos(y) z; writes
+// Output/Solution-0000.tec under the current directory.
+static double oracle_exact_3d(const double x, const double y, const double zz) { return sin(x) * cos(y) * zz; }
+extern "C" int oracle_ref3d_write(int nx, int ny, int nz, int n, double xl_, double xr_, double yl_, double yr_,
+                                  double zl_, double zr_, const double* u)
+{
+    Rank = 0;
+    size = 1;
+    CreatePDEPlan(nx, ny, nz, n, xl_, xr_, yl_, yr_, zl_, zr_);
+    FieldVariable* V = new FieldVariable[Ns];
+    for (int kk = 0; kk < Ns; ++kk) Allocate(V[kk].phi, 2 * Nx, NY, N);
+    for (int kk = 0; kk < Ns; ++kk)
+        for (int i = 0; i < Nx; ++i)
+            for (int j = 0; j < Ny; ++j)
+                for (int k = 0; k < N; ++k) V[kk].phi[i][j][k] = u[(((size_t)kk * Nx + i) * Ny + j) * N + k];
+    WriteFile(V, oracle_exact_3d);
+    int ns = Ns;
+    for (int kk = 0; kk < Ns; ++kk) Deallocate(V[kk].phi, 2 * Nx, NY, N);
+    delete[] V;
+    DestroyPDEPlan();
+    return ns;
+}

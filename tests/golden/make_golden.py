@@ -97,6 +97,20 @@ def main():
         d[f"gz3_{order}"] = O.ref_gll_deriv_3d(ug3, zl=0.0, zr=1.5, order=order)
     out["derivatives"] = d
 
+    # the reference's Tecplot writer (WriteFile) on seeded small fields
+    import tempfile
+    wrng = np.random.default_rng(20240604)
+    u2 = wrng.standard_normal((2, 8, 5))
+    u3 = wrng.standard_normal((2, 4, 4, 4))
+    with tempfile.TemporaryDirectory() as td:
+        t2 = O.ref_write_tecplot(u2, (0.5, 2.0, -1.0, 1.0), td)
+        t3 = O.ref_write_tecplot(u3, (0.0, 1.0, 0.5, 1.5, 0.0, 2.0), td)
+    with open(os.path.join(HERE, "writer_2d.tec"), "w") as fh:
+        fh.write(t2)
+    with open(os.path.join(HERE, "writer_3d.tec"), "w") as fh:
+        fh.write(t3)
+    out["writer_fields"] = dict(u2=u2, u3=u3, dom2=[0.5, 2.0, -1.0, 1.0], dom3=[0.0, 1.0, 0.5, 1.5, 0.0, 2.0])
+
     for name, d in out.items():
         np.savez_compressed(os.path.join(HERE, name + ".npz"), **{k: np.asarray(v) for k, v in d.items()})
         print(name, {k: np.asarray(v).shape for k, v in d.items()})
