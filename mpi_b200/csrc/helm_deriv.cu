@@ -185,14 +185,17 @@ __global__ void gll_deriv_kernel(GllDerivArgs a, GdLayout L)
 
 // ---------------------------------------------------------------------------
 // FP64 arrays: the two half-size products on the FP64 tensor cores.  Per warp
-// tile of 32 rows (four 8-row m-tiles), sigma = S E^T and alpha = A F^T as
-// m8n8k4 products.  The warp loads its rows as mirrored pairs (u_k, u_{P-1-k})
-// straight into the folded layout in shared memory, all 32 lanes busy; the A
-// operand is read from there, the B operands (E^T, F^T) sit in shared memory in
-// fragment order (one 8-byte word per lane, two wavefronts per warp load), and
-// the outputs go from the accumulators straight to global memory.
+// tile of 16 rows (two 8-row m-tiles), sigma = S E^T and alpha = A F^T as
+// m8n8k4 products.  The raw rows arrive in shared memory by cp.async one tile
+// ahead (two buffers per warp); the A operand (folded rows) is built on the fly
+// from the mirrored pair (u_k, u_{P-1-k}) of the staged row, the B operands
+// (E^T, F^T) sit in shared memory in fragment order (one 8-byte word per lane,
+// two wavefronts per warp load), and the outputs go from the accumulators
+// straight to global memory.
+constexpr int GM_ROWS = 16;  // rows per warp tile
+
 struct GdMmaLayout {
-    int h, odd, hs, ks, ka, nt, rs, w;  // k-steps of the s and a halves, n-tiles, row stride, fold width
+    int h, odd, hs, ks, ka, nt, rs;  // k-steps of the s and a halves, n-tiles, staged row stride
     size_t b_bytes, warp_bytes;
 };
 
@@ -205,11 +208,10 @@ static GdMmaLayout gd_mma_layout(int P)
     L.ks = (L.hs + 3) / 4;
     L.ka = (L.h + 3) / 4;
     L.nt = (L.hs + 7) / 8;
-    L.w = 4 * std::max(L.ks, L.ka);
-    L.rs = 4 * (L.ks + L.ka);           // folded row [s | a]; = 4 mod 16 doubles, so an
-    while ((L.rs & 15) != 4) ++L.rs;    //   A fragment (8 rows x 4) is two conflict-free wavefronts
+    L.rs = P;                           // staged row stride: = 4 mod 16 doubles, so an A fragment
+    while ((L.rs & 15) != 4) ++L.rs;    //   (8 rows x 4, and its mirror) is two conflict-free wavefronts
     L.b_bytes = (size_t)(L.ks + L.ka) * L.nt * 32 * sizeof(double);
-    L.warp_bytes = (size_t)32 * L.rs * sizeof(double);
+    L.warp_bytes = (size_t)2 * GM_ROWS * L.rs * sizeof(double);
     return L;
 }
 
@@ -222,7 +224,7 @@ __global__ void gll_deriv_mma_kernel(GllDerivArgs a, GdMmaLayout L)
     double* BE = reinterpret_cast<double*>(gm_smem);   // [ks][NT][32]
     double* BF = BE + (size_t)L.ks * NT * 32;          // [ka][NT][32]
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, g = lane >> 2, q = lane & 3;
-    double* fold = reinterpret_cast<double*>(gm_smem + L.b_bytes + (size_t)warp * L.warp_bytes);  // [32][rs]
+    double* stage = reinterpret_cast<double*>(gm_smem + L.b_bytes + (size_t)warp * L.warp_bytes);  // [2][16][rs]
 
     // B fragments: BE[k][t][l] = E[8t + l/4][4k + l%4], BF likewise with F
     for (int e = threadIdx.x; e < L.ks * NT * 32; e += blockDim.x) {
@@ -247,57 +249,67 @@ __global__ void gll_deriv_mma_kernel(GllDerivArgs a, GdMmaLayout L)
     const double* in = static_cast<const double*>(a.in);
     double* out = static_cast<double*>(a.out);
     const double sgn = a.order == 1 ? -1.0 : 1.0;
-    const int sw = 4 * L.ks, aw = 4 * L.ka, W = L.w;
-    const long long tiles = (a.nrows + 31) / 32;
+    const long long tiles = (a.nrows + GM_ROWS - 1) / GM_ROWS;
     const long long wstride = (long long)gridDim.x * (blockDim.x >> 5);
-    for (long long t = (long long)blockIdx.x * (blockDim.x >> 5) + warp; t < tiles; t += wstride) {
-        const long long R0 = t * 32;
-        const int nr = (int)min(32LL, a.nrows - R0);
-        const long long my = lane < nr ? gd_row_offset(a, R0 + lane) : 0;  // row offsets, by lane
-        // fold while loading: item (r, k), k < W: s_k at [k], a_k at [sw + k]
-        __syncwarp();
+    // cp.async of tile t's rows into dst (row r at dst + r rs), all lanes busy
+    auto issue = [&](long long t, double* dst) {
+        const long long R0 = t * GM_ROWS;
+        const int nr = (int)min((long long)GM_ROWS, a.nrows - R0);
+        const long long my = lane < nr ? gd_row_offset(a, R0 + lane) : 0;
+        // element e = base + lane sits at (r, k) = divmod(e, P), kept incrementally;
+        // every lane runs the same trips (the shuffle needs the whole warp)
         int r = 0, k = lane;
-        while (k >= W) { k -= W; ++r; }
-#pragma unroll 4
-        for (int e = lane; e < 32 * W; e += 32) {
-            const long long off = __shfl_sync(0xffffffffu, my, r);
-            double s_ = 0.0, a_ = 0.0;
-            if (r < nr) {
-                if (k < h) {
-                    const double x = in[off + k], y = in[off + P - 1 - k];
-                    s_ = x + y;
-                    a_ = x - y;
-                } else if (k == h && L.odd) {
-                    s_ = in[off + h];
-                }
-            }
-            double* f = fold + r * L.rs;
-            if (k < sw) f[k] = s_;
-            if (k < aw) f[sw + k] = a_;
+        while (k >= P) { k -= P; ++r; }
+        for (int base = 0; base < GM_ROWS * P; base += 32) {
+            const long long off = __shfl_sync(0xffffffffu, my, r < 31 ? r : 31);
+            if (base + lane < GM_ROWS * P && r < nr) cp_async_elem<8>(dst + r * L.rs + k, in + off + k, true);
             k += 32;
-            while (k >= W) { k -= W; ++r; }
+            while (k >= P) { k -= P; ++r; }
+        }
+        cp_async_commit();
+    };
+    long long t = (long long)blockIdx.x * (blockDim.x >> 5) + warp;
+    int buf = 0;
+    if (t < tiles) issue(t, stage);
+    for (; t < tiles; t += wstride, buf ^= 1) {
+        const double* cur = stage + (size_t)buf * GM_ROWS * L.rs;
+        const long long R0 = t * GM_ROWS;
+        const int nr = (int)min((long long)GM_ROWS, a.nrows - R0);
+        const long long my = lane < nr ? gd_row_offset(a, R0 + lane) : 0;
+        if (t + wstride < tiles) {
+            issue(t + wstride, stage + (size_t)(buf ^ 1) * GM_ROWS * L.rs);
+            cp_async_wait_prev();
+        } else {
+            cp_async_wait_all();
         }
         __syncwarp();
 #pragma unroll 1
-        for (int mt = 0; mt < 4; ++mt) {
+        for (int mt = 0; mt < GM_ROWS / 8; ++mt) {
             if (8 * mt >= nr) break;
             double cs[NT][2], ca[NT][2];
 #pragma unroll
             for (int n = 0; n < NT; ++n) { cs[n][0] = cs[n][1] = 0.0; ca[n][0] = ca[n][1] = 0.0; }
-            const double* arow = fold + (8 * mt + g) * L.rs + q;
+            const double* u = cur + (8 * mt + g) * L.rs;
 #pragma unroll 2
             for (int kk = 0; kk < L.ks; ++kk) {
-                const double av = arow[4 * kk];
-                const double* b = BE + ((size_t)kk * NT) * 32 + lane;
+                const int k = 4 * kk + q;
+                // A fragments of both halves from one mirrored pair
+                double sv = 0.0, av = 0.0;
+                if (k < h) {
+                    const double x = u[k], y = u[P - 1 - k];
+                    sv = x + y;
+                    av = x - y;
+                } else if (k == h && L.odd) {
+                    sv = u[h];
+                }
+                const double* bs = BE + ((size_t)kk * NT) * 32 + lane;
 #pragma unroll
-                for (int n = 0; n < NT; ++n) dmma_8x8x4(cs[n][0], cs[n][1], av, b[n * 32]);
-            }
-#pragma unroll 2
-            for (int kk = 0; kk < L.ka; ++kk) {
-                const double av = arow[sw + 4 * kk];
-                const double* b = BF + ((size_t)kk * NT) * 32 + lane;
+                for (int n = 0; n < NT; ++n) dmma_8x8x4(cs[n][0], cs[n][1], sv, bs[n * 32]);
+                if (kk < L.ka) {
+                    const double* ba = BF + ((size_t)kk * NT) * 32 + lane;
 #pragma unroll
-                for (int n = 0; n < NT; ++n) dmma_8x8x4(ca[n][0], ca[n][1], av, b[n * 32]);
+                    for (int n = 0; n < NT; ++n) dmma_8x8x4(ca[n][0], ca[n][1], av, ba[n * 32]);
+                }
             }
             // du_j = sigma + alpha, du_{P-1-j} = sgn (sigma - alpha), straight to global memory
             const int row = 8 * mt + g;
@@ -319,6 +331,7 @@ __global__ void gll_deriv_mma_kernel(GllDerivArgs a, GdMmaLayout L)
                     }
             }
         }
+        __syncwarp();  // this buffer is refilled by the copy issued in the next iteration
     }
 }
 
@@ -338,7 +351,7 @@ static int run_gll_deriv_mma(const GllDerivArgs& a, cudaStream_t s)
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k, warps * 32, smem);
     if (per < 1) per = 1;
-    const long long tiles = (a.nrows + 31) / 32;
+    const long long tiles = (a.nrows + GM_ROWS - 1) / GM_ROWS;
     long long grid = (long long)sms * per;
     const long long need = (tiles + warps - 1) / warps;
     if (grid > need) grid = need;
