@@ -53,7 +53,7 @@ def _args():
     ap.add_argument("--impl", choices=("ours", "reference"), default="ours")
     ap.add_argument("--skip-cpu-baseline", action="store_true", help="omit the CPU leg (profiling runs)")
     ap.add_argument("--skip-side", action="store_true", help="omit the batch / adjoint / finite-difference / periodic / derivative legs")
-    ap.add_argument("--profile-case", choices=("fp64", "fp32_refine", "fp32", "fd64", "fd32", "batch"),
+    ap.add_argument("--profile-case", choices=("fp64", "fp32_refine", "fp32", "fd64", "fd32", "batch", "deriv"),
                     help="run three untimed solves of one workload and exit (a small case for ncu captures)")
     return ap.parse_args()
 
@@ -61,7 +61,8 @@ def _args():
 def profile_case(which: str):
     """Plan creation (with its autotuning), then three solves: the headline
     256 x 256 x 65 workload at one precision, a 256 x 256 x 256 finite-difference
-    solve, or the 512-problem batch."""
+    solve, or the 512-problem batch; or ("deriv") three GLL derivatives of a
+    128 x 128 x 65 FP64 field."""
     import torch
 
     from mpi_b200 import workloads as W
@@ -75,6 +76,13 @@ def profile_case(which: str):
         p = Helmholtz3DFD(n, n, n, 0.0, 1.0, 0.0, 1.0, 0.0, 1.0, Lambda=1.0,
                           precision="fp64" if which == "fd64" else "fp32")
         run = lambda: p.SolvePDE(f)  # noqa: E731
+    elif which == "deriv":
+        from mpi_b200 import NonPeriodic3D
+
+        p = NonPeriodic3D(128, 128, NGLL, NGLL, *DOM, Lambda=1.0)
+        f = torch.randn(128, 128, NGLL, dtype=torch.float64, device="cuda")
+        o = torch.empty_like(f)
+        run = lambda: p.FirstDerivativeZ(f, out=o)  # noqa: E731
     elif which == "batch":
         from mpi_b200 import BatchNonPeriodic2D
 
@@ -385,6 +393,30 @@ def run_ours(args, ws, rank, local):
     e2e_ms = e0.elapsed_time(e1)
     e2e_ok = bool(torch.equal(uds[(args.steps - 1) & 1].cpu(), uh))
 
+    # the PCIe bound of e2e: the same pipelined H2D / D2H traffic with no solve
+    def copy_run(n):
+        for i in range(n):
+            b = i & 1
+            with torch.cuda.stream(s_in):
+                if i >= 2:
+                    s_in.wait_event(ev["out"][b])
+                fds[b].copy_(fh, non_blocking=True)
+                ev["in"][b].record(s_in)
+            with torch.cuda.stream(s_out):
+                s_out.wait_event(ev["in"][b])
+                uh.copy_(fds[b], non_blocking=True)
+                ev["out"][b].record(s_out)
+        stream.wait_stream(s_in)
+        stream.wait_stream(s_out)
+
+    copy_run(3)
+    barrier()
+    e0.record(stream)
+    copy_run(args.steps)
+    e1.record(stream)
+    barrier()
+    copy_ms = e0.elapsed_time(e1) / args.steps
+
     # per-stage device time of the refined solve (events on its stream)
     pref = plans["fp32_refine"]
     pref.enable_stage_timing(True)
@@ -450,13 +482,18 @@ def run_ours(args, ws, rank, local):
             "refine_over_fp64": ms_64 / ms_ref,
             "rel_l2_refine_vs_fp64": rel_vs_fp64,
             "stage_ms": acc,
+            "stage_hbm_frac": {k: _stage_bytes(k, spec_bytes, io_bytes) / (v * 1e-3) / 1e9 / peak
+                               for k, v in acc.items() if v > 0},
             "roofline": {"kernel": dom, "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)",
                          "algorithmic_bytes": alg, "traffic": (traffic or {}).get("fp32_refine")},
             "e2e": {"value": ws * dof / (ms_e2e * 1e-3) / 1e9, "unit": "GDOF/s", "ms_per_step": ms_e2e,
                     "pipelined": "H2D of step i+1 and D2H of step i-1 overlap the solve of step i",
                     "last_result_read_back": e2e_ok,
-                    "h2d_bytes_per_step": int(fh.numel() * 8), "d2h_bytes_per_step": int(uh.numel() * 8)},
+                    "h2d_bytes_per_step": int(fh.numel() * 8), "d2h_bytes_per_step": int(uh.numel() * 8),
+                    "copy_only_ms_per_step": copy_ms,
+                    "frac_of_copy_bound": copy_ms / ms_e2e,
+                    "bound": "pcie: the same pinned H2D + D2H per step with no solve"},
             "gpu_launches": launches,
             "clocks": clk,
         }
@@ -627,12 +664,28 @@ def _leg_fd(dev, flush, stream, steps, warmup, cpu=False):
     dof = Nx * Ny * Nz
     out = {"workload": FD_WORKLOAD, "dof_per_solve": dof}
     us = {}
+    peak, _ = _peak_hbm()
     for prec in ("fp32", "fp64"):
         p = Helmholtz3DFD(Nx, Ny, Nz, 0.0, 1.0, 0.0, 1.0, 0.0, 1.0, Lambda=1.0, precision=prec)
         u = p.SolvePDE(f)
         fwd = _ev_ms(lambda: p.SolvePDE(f, out=u), flush, stream, steps, warmup)
         adj = _ev_ms(lambda: p.SolveAdjoint(u), flush, stream, steps, warmup)
         out[prec] = {"value": dof / (fwd * 1e-3) / 1e9, "unit": "GDOF/s", "forward_ms": fwd, "adjoint_ms": adj}
+        # per-pass HBM fraction at this size: algorithmic bytes = input + output of each pass
+        p.enable_stage_timing(True)
+        st = {}
+        for _ in range(3):
+            flush.add_(1.0)
+            p.SolvePDE(f, out=u)
+            for k, v in p.stage_times().items():
+                st[k] = st.get(k, 0.0) + v / 3
+        p.enable_stage_timing(False)
+        eb = 8 if prec == "fp64" else 4
+        real_b, spec_b = dof * eb, (Nx // 2 + 1) * Ny * Nz * 2 * eb
+        pass_bytes = {"fft_x": real_b + spec_b, "fft_y": 2 * spec_b, "rows": 2 * spec_b, "ifft_y": 2 * spec_b,
+                      "ifft_x": spec_b + real_b}
+        out[prec]["stage_ms"] = st
+        out[prec]["stage_hbm_frac"] = {k: pass_bytes[k] / (st[k] * 1e-3) / 1e9 / peak for k in st if st[k] > 0}
         us[prec] = u
         p.DestroyPDEPlan()
     out["rel_l2_fp32_vs_fp64"] = float((us["fp32"] - us["fp64"]).norm() / us["fp64"].norm())

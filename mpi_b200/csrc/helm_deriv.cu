@@ -107,7 +107,7 @@ __global__ void gll_deriv_kernel(GllDerivArgs a, GdLayout L)
         }
         cp_async_commit();
     };
-    long long t = (long long)blockIdx.x * (blockDim.x >> 5) + warp;
+    long long t = (long long)warp * gridDim.x + blockIdx.x;  // warp-major: small jobs still reach every SM
     int buf = 0;
     if (t < tiles) issue(t, raw);
     for (; t < tiles; t += wstride, buf ^= 1) {
@@ -268,7 +268,7 @@ __global__ void gll_deriv_mma_kernel(GllDerivArgs a, GdMmaLayout L)
         }
         cp_async_commit();
     };
-    long long t = (long long)blockIdx.x * (blockDim.x >> 5) + warp;
+    long long t = (long long)warp * gridDim.x + blockIdx.x;  // warp-major: small jobs still reach every SM
     int buf = 0;
     if (t < tiles) issue(t, stage);
     for (; t < tiles; t += wstride, buf ^= 1) {
@@ -353,8 +353,7 @@ static int run_gll_deriv_mma(const GllDerivArgs& a, cudaStream_t s)
     if (per < 1) per = 1;
     const long long tiles = (a.nrows + GM_ROWS - 1) / GM_ROWS;
     long long grid = (long long)sms * per;
-    const long long need = (tiles + warps - 1) / warps;
-    if (grid > need) grid = need;
+    if (grid > tiles) grid = tiles;
     if (grid < 1) return 0;
     return (int)launch_k(k, dim3((unsigned)grid), dim3(warps * 32), smem, s, a, L);
 }
@@ -393,8 +392,7 @@ static int run_gll_deriv(const GllDerivArgs& a, cudaStream_t s)
     if (per < 1) per = 1;
     const long long tiles = (a.nrows + 31) / 32;
     long long grid = (long long)sms * per;
-    const long long need = (tiles + warps - 1) / warps;
-    if (grid > need) grid = need;
+    if (grid > tiles) grid = tiles;
     if (grid < 1) return 0;
     return (int)launch_k(k, dim3((unsigned)grid), dim3(warps * 32), smem, s, a, L);
 }

@@ -1308,7 +1308,7 @@ __global__ void __launch_bounds__(TC_WARPS * 32, 1) fdm_tc_refine_kernel(FdmArgs
     __syncthreads();
 
     cplx_t<double>* spec = static_cast<cplx_t<double>*>(a.spec);
-    const int n = a.n, m = a.m, ms = a.ms, P = a.P, nrows = a.nrows;
+    const int n = a.n, m = a.m, ms = a.ms, nrows = a.nrows;
     const double r2 = 0.70710678118654752440;
     constexpr int RPW = 4, RR = 136;  // raw row r at Xd + r RR (complex i at 2 i)
     const long long npacks = (nrows + RPW - 1) / RPW;
