@@ -14,6 +14,7 @@ import torch
 
 from mpi_b200 import NonPeriodic2D, NonPeriodic3D
 from mpi_b200 import workloads as W
+from mpi_b200._lib import HelmError
 from oracle import oracle as O
 from tests.helpers import golden, max_rel, rel_l2
 
@@ -194,3 +195,32 @@ def test_every_launch_variant(cuda, N, precision):
             u = p.SolvePDE(fd, gld, grd).cpu().numpy()
             err = max_rel(u, ref) if precision == "fp64" else rel_l2(u, ref)
             assert err < TOL[precision], (fv, rv, err)
+
+
+@pytest.mark.parametrize("precision", ["fp64", "fp32_refine"])
+def test_maximum_sizes(cuda, precision):
+    """The largest sizes the plan accepts: Nx = 1024 Fourier modes with N = 129 GLL
+    points (2D), 64 elements (2D, Robin ends), and a 1024 x 8 x 17 3D plan; one
+    past each limit is rejected."""
+    rng = np.random.default_rng(17)
+    tol = 1e-12 if precision == "fp64" else 1e-10
+    f = rng.standard_normal((1024, 129))
+    p = NonPeriodic2D(1024, 129, 129, 0.0, 2 * math.pi, -1.0, 1.0, Lambda=2.0, precision=precision)
+    u = p.SolvePDE(_dev(f)).cpu().numpy()
+    ref = O.solve2d(f, np.zeros(1024), np.zeros(1024), Lx=2 * math.pi, Ly=2.0, lam=2.0)
+    assert rel_l2(u, ref) < tol
+    bc = (0.4, 1.0, 0.3, 2.0)
+    f = rng.standard_normal((64, 32, 6))
+    gl, gr = rng.standard_normal(32), rng.standard_normal(32)
+    p = NonPeriodic2D(32, 64 * 6, 6, 0.0, 1.0, 0.0, 3.0, Lambda=1.5, bc=bc, precision=precision)
+    assert p.Ns == 64
+    u = p.SolvePDE(_dev(f), _dev(gl), _dev(gr)).cpu().numpy()
+    assert rel_l2(u, O.solve2d(f, gl, gr, Lx=1.0, Ly=3.0, lam=1.5, bc=bc)) < tol
+    f = rng.standard_normal((1024, 8, 17))
+    p = NonPeriodic3D(1024, 8, 17, 17, 0.0, 1.0, 0.0, 1.0, 0.0, 1.0, Lambda=1.0, precision=precision)
+    u = p.SolvePDE(_dev(f)).cpu().numpy()
+    z = np.zeros((1024, 8))
+    assert rel_l2(u, O.solve3d(f, z, z, Lx=1.0, Ly=1.0, Lz=1.0, lam=1.0)) < tol
+    for args in ((2048, 33, 33), (64, 130, 130), (64, 65 * 6, 6)):
+        with pytest.raises(HelmError):
+            NonPeriodic2D(*args, 0.0, 1.0, 0.0, 1.0, Lambda=1.0, precision=precision)
