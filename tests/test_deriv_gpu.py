@@ -106,3 +106,31 @@ def test_derivative_rejects_bad_axis(cuda):
     from mpi_b200._lib import HelmError
     with pytest.raises(HelmError):
         p._derivative(1, 3, u, None, None)
+
+
+def test_derivatives_in_the_reference_array_layout(cuda):
+    """Padded reference arrays (U.phi[2Nx][2Ny][N] per element, two elements): the
+    derivatives read and write only the solution rows, per element, through the
+    plan's strides; the padding is left untouched."""
+    rng = np.random.default_rng(23)
+    Nx, Ny, N, Ns = 8, 16, 9, 2
+    u = rng.standard_normal((Ns, Nx, Ny, N))
+    p = NonPeriodic3D(Nx, Ny, Ns * N, N, 0.0, 1.0, 0.0, 2.0, 0.0, 3.0, Lambda=1.0)
+    p.set_layout(x_stride=2 * Ny * N, elem_stride=2 * Nx * 2 * Ny * N, bc_x_stride=2 * Ny)
+    U = np.zeros((Ns, 2 * Nx, 2 * Ny, N))
+    U[:, :Nx, :Ny] = u
+    ud = _dev(U)
+    stream = torch.cuda.current_stream().cuda_stream
+    cases = [(lambda o: p._lib.helm_fourier_derivative(p._plan, 0, 1, ud.data_ptr(), o.data_ptr(), stream),
+              np.stack([O.fourier_deriv(u[e], axis=0, order=1, L=1.0) for e in range(Ns)])),
+             (lambda o: p._lib.helm_fourier_derivative(p._plan, 1, 2, ud.data_ptr(), o.data_ptr(), stream),
+              np.stack([O.fourier_deriv(u[e], axis=1, order=2, L=2.0) for e in range(Ns)])),
+             (lambda o: p._lib.helm_gll_derivative(p._plan, 1, ud.data_ptr(), o.data_ptr(), stream),
+              O.gll_deriv(u, N=N, Ns=Ns, L=3.0, order=1))]
+    for run, ref in cases:
+        od = torch.full(U.shape, 5.0, dtype=torch.float64, device="cuda")
+        assert run(od) == 0
+        torch.cuda.synchronize()
+        D = od.cpu().numpy()
+        assert max_rel(D[:, :Nx, :Ny], ref) < 1e-12
+        assert np.all(D[:, Nx:] == 5.0) and np.all(D[:, :, Ny:] == 5.0)
