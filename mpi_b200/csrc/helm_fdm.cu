@@ -732,7 +732,7 @@ static int run_fdm_mma(const FdmArgs& a, cudaStream_t s)
 __device__ __forceinline__ void dmma_16x8x8(double (&c)[4], const double2& a01, const double2& a23, double b0,
                                             double b1)
 {
-    asm volatile("mma.sync.aligned.m16n8k8.row.col.f64.f64.f64.f64 {%0, %1, %2, %3}, {%4, %5, %6, %7}, {%8, %9}, "
+    asm("mma.sync.aligned.m16n8k8.row.col.f64.f64.f64.f64 {%0, %1, %2, %3}, {%4, %5, %6, %7}, {%8, %9}, "
                  "{%0, %1, %2, %3};\n"
                  : "+d"(c[0]), "+d"(c[1]), "+d"(c[2]), "+d"(c[3])
                  : "d"(a01.x), "d"(a01.y), "d"(a23.x), "d"(a23.y), "d"(b0), "d"(b1));
@@ -1193,7 +1193,7 @@ __device__ __forceinline__ uint32_t to_tf32(float x)
 
 __device__ __forceinline__ void mma_tf32(float (&c)[4], const float4& a, uint32_t b0, uint32_t b1)
 {
-    asm volatile("mma.sync.aligned.m16n8k8.row.col.f32.tf32.tf32.f32 {%0, %1, %2, %3}, {%4, %5, %6, %7}, "
+    asm("mma.sync.aligned.m16n8k8.row.col.f32.tf32.tf32.f32 {%0, %1, %2, %3}, {%4, %5, %6, %7}, "
                  "{%8, %9}, {%0, %1, %2, %3};\n"
                  : "+f"(c[0]), "+f"(c[1]), "+f"(c[2]), "+f"(c[3])
                  : "r"(__float_as_uint(a.x)), "r"(__float_as_uint(a.y)), "r"(__float_as_uint(a.z)),
@@ -1229,8 +1229,10 @@ constexpr size_t TC_M_DOUBLES = (size_t)2 * TC_LD * TC_LD;        // Ms, Ma
 constexpr size_t TC_REG = (size_t)8 * TC_S;  // doubles
 constexpr size_t TC_SMEM = TC_TF32_FLOATS * 4 + TC_M_DOUBLES * 8 + (size_t)TC_WARPS * 2 * TC_REG * 8;
 
-// One folded solve S on B columns read by `bread(blk, k)` (the lane's B element
-// at fold index k of block blk, as float); result x in C layout (FP32).
+// One folded solve S on B columns read by `bread(blk, kk, hf)` (the lane's B
+// element of block blk at fold index 8 kk + q + 4 hf, as float; kk and hf are
+// compile-time after unrolling, so register arrays stay in registers); result x
+// in C layout (FP32).
 template <typename BRead>
 __device__ __forceinline__ void tc_solve(const float4* Tf, const float (&rs)[TC_MT][2], const float (&ra)[TC_MT][2],
                                          float* X, int g, int q, BRead bread, float (&xs)[TC_MT][4],
@@ -1245,8 +1247,8 @@ __device__ __forceinline__ void tc_solve(const float4* Tf, const float (&rs)[TC_
         for (int j = 0; j < 4; ++j) cs[mt][j] = ca[mt][j] = 0.f;
 #pragma unroll
     for (int kk = 0; kk < TC_KS; ++kk) {
-        const Tf32Split bs = tf32_split(bread(0, 8 * kk + q), bread(0, 8 * kk + q + 4));
-        const Tf32Split ba = tf32_split(bread(1, 8 * kk + q), bread(1, 8 * kk + q + 4));
+        const Tf32Split bs = tf32_split(bread(0, kk, 0), bread(0, kk, 1));
+        const Tf32Split ba = tf32_split(bread(1, kk, 0), bread(1, kk, 1));
 #pragma unroll
         for (int mt = 0; mt < TC_MT; ++mt) {
             const size_t f = (size_t)(mt * TC_KS + kk) * 32 + lane;
@@ -1382,7 +1384,7 @@ __global__ void __launch_bounds__(TC_WARPS * 32, 1) fdm_tc_refine_kernel(FdmArgs
                 }
             __syncwarp();
             tc_solve(Tf, rs, ra, Xf, g, q,
-                     [&](int blk, int k) { return bsave[blk][k >> 3][((k & 7) >= 4) ? 1 : 0]; }, xs, xa);
+                     [&](int blk, int kk, int hf) { return bsave[blk][kk][hf]; }, xs, xa);
         }
         // ---- r = f - (M x - sigma x), FP64 ----
 #pragma unroll
@@ -1447,7 +1449,7 @@ __global__ void __launch_bounds__(TC_WARPS * 32, 1) fdm_tc_refine_kernel(FdmArgs
         // ---- x += S(r) ----
         float ds[TC_MT][4], da[TC_MT][4];
         tc_solve(Tf, rs, ra, Xf, g, q,
-                 [&](int blk, int k) { return resf[blk][k >> 3][((k & 7) >= 4) ? 1 : 0]; }, ds, da);
+                 [&](int blk, int kk, int hf) { return resf[blk][kk][hf]; }, ds, da);
 #pragma unroll
         for (int mt = 0; mt < TC_MT; ++mt)
 #pragma unroll
