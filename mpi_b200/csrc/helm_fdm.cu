@@ -1222,7 +1222,7 @@ __device__ __forceinline__ void mma_3xtf32(float (&c)[4], const float4& ah, cons
     mma_tf32(c, ah, b.h0, b.h1);
 }
 
-constexpr int TC_WARPS = 16, TC_LD = 32, TC_MT = 2, TC_KS = 4, TC_S = 68;
+constexpr int TC_WARPS = 12, TC_LD = 32, TC_MT = 2, TC_KS = 4, TC_S = 68;
 constexpr size_t TC_TF32_FLOATS = (size_t)4 * 2 * TC_LD * TC_LD;  // 4 transforms x (hi, lo)
 constexpr size_t TC_M_DOUBLES = (size_t)2 * TC_LD * TC_LD;        // Ms, Ma
 // per warp two staging regions of 8 columns x 68 doubles: the current pack and the next one arriving
