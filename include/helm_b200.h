@@ -200,9 +200,11 @@ int helm_plan_info(helm_plan_t plan, int* Ns, int* n_operators, int* method, lon
 int helm_plan_set_stage_timing(helm_plan_t plan, int enable);
 int helm_plan_stage_times(helm_plan_t plan, float* ms5);
 
-/* Kernel launch variants of the plan: fft4[i] (0..7) for the x, y, inverse y
+/* Kernel launch variants of the plan: fft4[i] (0..15) for the x, y, inverse y
  * and inverse x FFT passes -- bit 0: 128-thread CTAs, bit 1: radix-8 schedule
- * (lengths 128, 256), bit 2: persistent pipelined pass -- and rows (0..2) for
+ * (lengths 128, 256), bit 2: persistent pipelined pass, bit 3: 512-thread CTAs
+ * for passes of length 512 or 1024 (ignored for shorter ones; with bit 2 the
+ * tile exceeds shared memory and the solve fails with HELM_ERR_CUDA) -- and rows (0..2) for
  * the row solve (1: the second kernel shape; 2: FP64 3D plans with one element,
  * at most 65 GLL points and Ny in {64, 128, 256} only -- the y pass, the row
  * solve and the inverse y pass fused into one kernel per kx slab, the two y

@@ -605,12 +605,17 @@ static int fft_dispatch_mode(int mode, int dir, const FftArgs& a, long long tc, 
 
 // Launch variants the autotuner chooses from: bit 0 -> 128-thread CTAs (half the
 // columns per tile), bit 1 -> radix-8 schedule (lengths 128 and 256), bit 2 ->
-// the persistent pipelined kernel.
+// the persistent pipelined kernel, bit 3 -> 512-thread CTAs for lengths 512 and
+// 1024 (twice the columns per tile: 128-byte runs of each row instead of 64 on
+// the strided x pass; bit 0 is then ignored).
 template <typename T, typename TIO, int L>
 static int fft_dispatch_variant(int variant, int mode, int dir, const FftArgs& a, long long tc, cudaStream_t s)
 {
-    const bool small_cta = (variant & 1) && (L / Radix<L>::r0 <= 128);
+    const bool small_cta = !(variant & 8) && (variant & 1) && (L / Radix<L>::r0 <= 128);
     const bool pipe = (variant & 4) != 0;
+    if constexpr (L >= 512) {
+        if (variant & 8) return fft_dispatch_mode<T, TIO, L, 512, 0>(mode, dir, a, tc, s, pipe);
+    }
     if constexpr (has_small_radix<L>()) {
         if (variant & 2) {
             if (small_cta) return fft_dispatch_mode<T, TIO, L, 128, 1>(mode, dir, a, tc, s, pipe);

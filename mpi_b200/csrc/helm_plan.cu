@@ -844,10 +844,12 @@ static int autotune(Plan& p)
         for (cudaEvent_t& e : p.ev) cudaEventCreate(&e);
     p.stage_timing = true;
     // stages: x, y, rows, inverse y, inverse x (event intervals 0..4); the
-    // FFT stages try variants 0..7, the row stage its variants 0..1
+    // FFT stages try variants 0..7 (and 8..15, the 512-thread CTAs, when a pass is
+    // 512 or 1024 long), the row stage its variants 0..1
     float best[5] = {1e30f, 1e30f, 1e30f, 1e30f, 1e30f};
     int pick[5] = {0, 0, 0, 0, 0};
-    for (int v = 0; v < 8; ++v) {
+    const int nvar = (p.Nx >= 512 || (p.dim == 3 && p.Ny >= 512)) ? 16 : 8;
+    for (int v = 0; v < nvar; ++v) {
         for (int i = 0; i < 4; ++i) p.fft_var[i] = v;
         p.row_var = v & 1;
         float acc[5] = {0, 0, 0, 0, 0};
@@ -1373,7 +1375,7 @@ int helm_plan_set_launch_variants(helm_plan_t plan, const int* fft4, int rows)
 {
     if (!plan || !fft4 || rows < 0 || rows > 2) return HELM_ERR_INVALID;
     for (int i = 0; i < 4; ++i)
-        if (fft4[i] < 0 || fft4[i] > 7) return HELM_ERR_INVALID;
+        if (fft4[i] < 0 || fft4[i] > 15) return HELM_ERR_INVALID;
     Plan& p = *reinterpret_cast<Plan*>(plan);
     if (rows == 2 && !p.slab_ok) {
         helm::set_last_error("the fused slab kernel needs an FP64 3D plan with one element, at most 65 points, Ny in {64, 128, 256}");

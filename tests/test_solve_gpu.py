@@ -224,3 +224,24 @@ def test_maximum_sizes(cuda, precision):
     for args in ((2048, 33, 33), (64, 130, 130), (64, 65 * 6, 6)):
         with pytest.raises(HelmError):
             NonPeriodic2D(*args, 0.0, 1.0, 0.0, 1.0, Lambda=1.0, precision=precision)
+
+
+@pytest.mark.parametrize("precision", ["fp64", "fp32"])
+def test_long_pass_launch_variants(cuda, precision):
+    """FFT variants 8..11 (512-thread CTAs, lengths 512 and 1024) against the
+    oracle on 2D plans with Nx = 512 and 1024; 12..15 (pipelined, too large a
+    tile) fail cleanly and leave the plan usable."""
+    rng = np.random.default_rng(5)
+    for Nx in (512, 1024):
+        f = rng.standard_normal((Nx, 17))
+        ref = O.solve2d(f, np.zeros(Nx), np.zeros(Nx), Lx=1.0, Ly=2.0, lam=1.0)
+        p = NonPeriodic2D(Nx, 17, 17, 0.0, 1.0, -1.0, 1.0, Lambda=1.0, precision=precision)
+        for fv in range(8, 16):
+            p.set_launch_variants([fv] * 4, 0)
+            try:
+                u = p.SolvePDE(_dev(f)).cpu().numpy()
+            except HelmError as e:
+                assert fv & 4 and e.status == 5, (Nx, fv, e)
+                continue
+            err = max_rel(u, ref) if precision == "fp64" else rel_l2(u, ref)
+            assert err < TOL[precision], (Nx, fv, err)
