@@ -148,6 +148,14 @@ int helm_solve(helm_plan_t plan, const void* f, const double* gl, const double* 
 int helm_solve_adjoint(helm_plan_t plan, const double* ubar, double* fbar, double* glbar, double* grbar,
                        const double* u, double* lambda_bar, void* stream);
 
+/* The adjoint of the least-squares loss L = 1/2 ||u - u_obs||^2 in one call:
+ * helm_solve_adjoint with ubar = u - u_obs, formed as the first pass loads its
+ * input (no ubar array, no separate kernel); u must be the forward solution of
+ * the same plan (it is also the u of dL/dlambda).  Outputs as helm_solve_adjoint.
+ * No counterpart in the reference, which has no gradients. */
+int helm_solve_adjoint_misfit(helm_plan_t plan, const double* u, const double* u_obs, double* fbar, double* glbar,
+                              double* grbar, double* lambda_bar, void* stream);
+
 /* Derivative along the GLL direction, element by element: du = Dy u (order 1)
  * or Dyy u (order 2) with the plan's scaled matrices (helm_plan_get_grid), at
  * every node of every Fourier row.  Replaces FirstDerivativeY /

@@ -37,7 +37,7 @@ EXPORTS = (
     "helm2d_batch_create", "helm_batch_offsets", "helm_batch_info", "helm_batch_set_graph",
     "helm_batch_solve", "helm_batch_destroy", "helm_plan_get_launch_variants", "helm_plan_set_launch_variants",
     "helm2d_periodic_plan_create", "helm3d_periodic_plan_create", "helm_gll_derivative", "helm_fourier_derivative",
-    "helm_write_tecplot", "helm_write_vtk",
+    "helm_write_tecplot", "helm_write_vtk", "helm_solve_adjoint_misfit",
 )
 
 # exact-solution callback of helm_write_tecplot: double exact(double x, double y, double z)
@@ -77,6 +77,7 @@ def lib() -> ctypes.CDLL:
     L.helm_gll_derivative.argtypes = [vp, i, vp, vp, vp]
     L.helm_write_tecplot.argtypes = [vp, vp, EXACT_FN, ctypes.c_char_p]
     L.helm_write_vtk.argtypes = [vp, vp, ctypes.c_char_p]
+    L.helm_solve_adjoint_misfit.argtypes = [vp, vp, vp, vp, vp, vp, vp, vp]
     L.helm_fourier_derivative.argtypes = [vp, i, i, vp, vp, vp]
     L.helm2d_periodic_plan_create.argtypes = [i, i, i, d, d, d, d, d, i, i, P(vp)]
     L.helm3d_periodic_plan_create.argtypes = [i, i, i, i, d, d, d, d, d, d, d, i, i, P(vp)]

@@ -215,6 +215,7 @@ __global__ void __launch_bounds__(THREADS) fft_kernel(FftArgs a, long long total
         for (int r = 0; r < R0; ++r) v[r] = sm[(tc + r * TPC) * CT + cl];
     } else if constexpr (MODE == FFT_R2C) {
         const TIO* in = static_cast<const TIO*>(a.in) + in_base;
+        const TIO* sub = a.in_sub ? static_cast<const TIO*>(a.in_sub) + in_base : nullptr;
         int k0 = -1, k1 = -1, j0 = 0, j1 = 0;  // GLL slot of the two real columns
         if (a.P > 0) { k0 = c0 % a.P; j0 = c0 / a.P; k1 = c1 % a.P; j1 = c1 / a.P; }
         const bool bnd0 = a.P > 0 && (k0 == 0 || k0 == a.P - 1);
@@ -227,7 +228,8 @@ __global__ void __launch_bounds__(THREADS) fft_kernel(FftArgs a, long long total
             T x0 = 0, x1 = 0;
             if (valid) {
                 if (!bnd0) {
-                    x0 = (T)in[row * a.in_row + c0];
+                    x0 = sub ? (T)((double)in[row * a.in_row + c0] - (double)sub[row * a.in_row + c0])
+                             : (T)in[row * a.in_row + c0];
                 } else if (a.bc_add) {
                     double v = (double)in[row * a.in_row + c0];
                     if (s0) v += (k0 == 0 ? a.bc_scale_l : a.bc_scale_r) * s0[row * a.bc_row + j0];
@@ -237,7 +239,8 @@ __global__ void __launch_bounds__(THREADS) fft_kernel(FftArgs a, long long total
                 }
                 if (has1) {
                     if (!bnd1) {
-                        x1 = (T)in[row * a.in_row + c1];
+                        x1 = sub ? (T)((double)in[row * a.in_row + c1] - (double)sub[row * a.in_row + c1])
+                                 : (T)in[row * a.in_row + c1];
                     } else if (a.bc_add) {
                         double v = (double)in[row * a.in_row + c1];
                         if (s1) v += (k1 == 0 ? a.bc_scale_l : a.bc_scale_r) * s1[row * a.bc_row + j1];

@@ -58,6 +58,10 @@ struct FftArgs {
     // (0: no derivative)
     int deriv_order;
     double deriv_w;
+    // R2C only (non-pipelined kernel): when set, the transformed input is
+    // in - in_sub, same layout and type as in (the data misfit u - u_obs of the
+    // adjoint of a least-squares loss, formed as it is loaded)
+    const void* in_sub;
 };
 
 // Finite-difference variant: one tridiagonal solve along z per spectrum row.

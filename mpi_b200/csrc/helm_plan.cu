@@ -602,6 +602,7 @@ struct AdjOut {
     double* grbar;
     const double* u;       // forward solution (lambda sum), or NULL
     double* lambda_bar;    // device scalar, zeroed before the pass, or NULL
+    const double* sub;     // the first pass reads ubar - sub (data misfit), or NULL
 };
 
 static int fft_pass(Plan& p, int L, int mode, int dir, const void* in, void* out, long long in_row, long long out_row,
@@ -612,6 +613,9 @@ static int fft_pass(Plan& p, int L, int mode, int dir, const void* in, void* out
     FftArgs a{};
     a.deriv_order = deriv_order;
     a.deriv_w = deriv_w;
+    // the misfit subtrahend is read by the non-pipelined R2C kernel only
+    const bool sub = adj && adj->sub && mode == FFT_R2C && stage == 0;
+    a.in_sub = sub ? adj->sub : nullptr;
     if (adj && mode == FFT_C2R) {
         a.adj_mode = p.fd ? 2 : 1;
         a.adj_P = p.N;
@@ -649,7 +653,7 @@ static int fft_pass(Plan& p, int L, int mode, int dir, const void* in, void* out
     const int td = p.precision != HELM_FP32;
     const int io = (td || io_double) ? 8 : p.io_bytes;
     const int kmode = a.adj_mode ? (int)FFT_C2R_ADJ : mode;
-    int e = launch_fft(L, kmode, dir, td, io, a, ccols * nbatch, s, p.fft_var[stage]);
+    int e = launch_fft(L, kmode, dir, td, io, a, ccols * nbatch, s, sub ? (p.fft_var[stage] & ~4) : p.fft_var[stage]);
     if (e) return set_cuda_error((cudaError_t)e, "fft launch");
     return HELM_OK;
 }
@@ -905,7 +909,7 @@ int solve(Plan& p, const void* f, const double* gl, const double* gr, void* u, c
 }
 
 int solve_adjoint(Plan& p, const double* ubar, double* fbar, double* glbar, double* grbar, const double* u,
-                  double* lambda_bar, cudaStream_t s)
+                  double* lambda_bar, cudaStream_t s, const double* sub = nullptr)
 {
     if (!p.adj_ready) {
         g_last_error = "adjoint needs a fast-diagonalisation plan with one GLL element";
@@ -917,7 +921,7 @@ int solve_adjoint(Plan& p, const double* ubar, double* fbar, double* glbar, doub
     }
     // the first pass zeroes lambda_bar; the last writes fbar, splits off glbar /
     // grbar and sums fbar * u into lambda_bar
-    const AdjOut adj{glbar, grbar, u, lambda_bar};
+    const AdjOut adj{glbar, grbar, u, lambda_bar, sub};
     return run_pipeline(p, ubar, nullptr, nullptr, fbar, true, s, &adj);
 }
 
@@ -1307,6 +1311,23 @@ int helm_fourier_derivative(helm_plan_t plan, int axis, int order, const void* u
     cudaGetDevice(&cur);
     if (cur != p.device) cudaSetDevice(p.device);
     int st = helm::fourier_derivative(p, axis, order, u, du, static_cast<cudaStream_t>(stream));
+    if (cur != p.device) cudaSetDevice(cur);
+    return st;
+}
+
+int helm_solve_adjoint_misfit(helm_plan_t plan, const double* u, const double* u_obs, double* fbar, double* glbar,
+                              double* grbar, double* lambda_bar, void* stream)
+{
+    if (!plan || !u || !u_obs || !fbar) return HELM_ERR_INVALID;
+    Plan& p = *reinterpret_cast<Plan*>(plan);
+    if (p.periodic && (glbar || grbar)) {
+        helm::set_last_error("a plan periodic in the GLL direction has no boundary data to differentiate");
+        return HELM_ERR_INVALID;
+    }
+    int cur = 0;
+    cudaGetDevice(&cur);
+    if (cur != p.device) cudaSetDevice(p.device);
+    int st = helm::solve_adjoint(p, u, fbar, glbar, grbar, u, lambda_bar, static_cast<cudaStream_t>(stream), u_obs);
     if (cur != p.device) cudaSetDevice(cur);
     return st;
 }

@@ -201,6 +201,23 @@ class _PlanBase:
             raise ValueError("fmt must be 'tecplot' or 'vtk'")
         L.check(st, "helm_write_" + fmt)
 
+    def SolveAdjointMisfit(self, u: torch.Tensor, u_obs: torch.Tensor, want_bc: bool = False, stream=None):
+        """(fbar, lambda_bar, glbar, grbar) of L = 1/2 ||u - u_obs||^2, u the forward
+        solution: SolveAdjoint with ubar = u - u_obs formed inside the adjoint's
+        first pass (no ubar tensor)."""
+        if u.shape != u_obs.shape or u.dtype != torch.float64 or u_obs.dtype != torch.float64:
+            raise ValueError("u and u_obs must be float64 tensors of one shape")
+        fbar = torch.empty_like(u)
+        lam = torch.zeros(1, dtype=torch.float64, device=u.device)
+        glb = torch.empty(self._bc_shape(), dtype=torch.float64, device=u.device) if want_bc else None
+        grb = torch.empty(self._bc_shape(), dtype=torch.float64, device=u.device) if want_bc else None
+        st = self._lib.helm_solve_adjoint_misfit(self._plan, u.data_ptr(), u_obs.data_ptr(), fbar.data_ptr(),
+                                                 glb.data_ptr() if glb is not None else None,
+                                                 grb.data_ptr() if grb is not None else None, lam.data_ptr(),
+                                                 _stream_ptr(stream))
+        L.check(st, "helm_solve_adjoint_misfit")
+        return fbar, lam, glb, grb
+
     def enable_stage_timing(self, enable: bool = True) -> None:
         L.check(self._lib.helm_plan_set_stage_timing(self._plan, int(enable)), "helm_plan_set_stage_timing")
 

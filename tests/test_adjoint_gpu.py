@@ -148,3 +148,35 @@ def test_adjoint_slab_variant(cuda, bc):
         outs.append([x.cpu().numpy() for x in (u, fb, lb, glb, grb)])
     for a, b in zip(outs[0], outs[1]):
         assert rel_l2(b, a) < 1e-12
+
+
+@pytest.mark.parametrize("kind", ["fp64", "fp32_refine", "fp32", "fd", "periodic"])
+def test_misfit_adjoint_matches_explicit_ubar(cuda, kind):
+    """helm_solve_adjoint_misfit (ubar = u - u_obs formed in the first pass) gives the
+    gradients of helm_solve_adjoint on an explicit ubar."""
+    from mpi_b200 import Helmholtz3DFD, Periodic3D
+
+    rng = np.random.default_rng(31)
+    bc = (0.4, 1.0, 0.3, 2.0)
+    if kind == "fd":
+        p = Helmholtz3DFD(16, 8, 12, 0.0, 1.0, 0.0, 2.0, 0.0, 1.5, Lambda=1.0, bc=bc)
+        shape, want_bc = (16, 8, 12), True
+    elif kind == "periodic":
+        p = Periodic3D(16, 8, 17, 17, 0.0, 1.0, 0.0, 2.0, 0.0, 1.5, Lambda=1.0)
+        shape, want_bc = (16, 8, 17), False
+    else:
+        p = NonPeriodic3D(16, 8, 17, 17, 0.0, 1.0, 0.0, 2.0, 0.0, 1.5, Lambda=1.0, bc=bc, precision=kind)
+        shape, want_bc = (16, 8, 17), True
+    f = _dev(rng.standard_normal(shape))
+    uobs = _dev(rng.standard_normal(shape))
+    u = p.SolvePDE(f).double()
+    if kind == "fp32":
+        uobs = uobs.float().double()
+    a = p.SolveAdjoint((u - uobs).contiguous(), u=u, want_bc=want_bc)
+    b = p.SolveAdjointMisfit(u, uobs, want_bc=want_bc)
+    tol = 1e-5 if kind == "fp32" else 1e-13
+    assert rel_l2(b[0].cpu().numpy(), a[0].cpu().numpy()) < tol
+    assert abs(b[1].item() - a[1].item()) <= tol * abs(a[1].item())
+    if want_bc:
+        for x, y in zip(b[2:], a[2:]):
+            assert rel_l2(x.cpu().numpy(), y.cpu().numpy()) < tol
