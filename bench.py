@@ -286,11 +286,50 @@ def _traffic_from_profiles(stage: str):
     return out or None
 
 
-def _stage_bytes(stage: str, spec_bytes: float, io_bytes: float) -> float:
-    """Algorithmic HBM bytes of one launch of each stage (inputs read once,
-    outputs written once)."""
-    return {"fft_x": io_bytes + spec_bytes, "fft_y": 2 * spec_bytes, "rows": 2 * spec_bytes,
-            "ifft_y": 2 * spec_bytes, "ifft_x": spec_bytes + io_bytes}[stage]
+def _stage_model(eig: bool, spec_bytes: float, io_bytes: float) -> dict:
+    """Kernel, algorithmic HBM bytes (inputs read once, outputs written once) and
+    FP64 flops of each timed stage of the headline solve.  Five-kernel pipeline:
+    x FFT, y FFT, row solves, inverse y, inverse x.  Eigen-basis pipeline: the
+    GLL transform + x FFT (stage event 0-1), the y convolution (1-2) and the
+    inverse (4-5); the coefficient spectrum holds 64 complex values per row."""
+    nkx = NX // 2 + 1
+    if not eig:
+        rows_flops = 2.0 * nkx * NY * 2 * (NGLL - 2) ** 2  # folded transforms: n^2 MAC per real row
+        fft_x = 2.5 * NGLL * NY * NX * math.log2(NX)       # R2C: 5 N log2 N per complex pair of columns
+        fft_y = 5.0 * nkx * NGLL * NY * math.log2(NY)
+        return {"fft_x": {"kernel": "fft_x", "bytes": io_bytes + spec_bytes, "flops": fft_x},
+                "fft_y": {"kernel": "fft_y", "bytes": 2 * spec_bytes, "flops": fft_y},
+                "rows": {"kernel": "rows", "bytes": 2 * spec_bytes, "flops": rows_flops},
+                "ifft_y": {"kernel": "ifft_y", "bytes": 2 * spec_bytes, "flops": fft_y},
+                "ifft_x": {"kernel": "ifft_x", "bytes": spec_bytes + io_bytes, "flops": fft_x}}
+    s_bytes = 16.0 * nkx * NY * 64
+    gll = 2.0 * NX * NY * 2 * 32 * 32                     # two 32 x 32 folded products per real row
+    fft_x = 5.0 * 32 * NY * NX * math.log2(NX)           # 32 complex column pairs per plane
+    fft_y = 2 * 5.0 * nkx * 64 * NY * math.log2(NY)      # forward and inverse
+    return {"fft_x": {"kernel": "eig_fwd_kernel", "bytes": io_bytes + s_bytes, "flops": gll + fft_x},
+            "fft_y": {"kernel": "eig_conv_kernel", "bytes": 2 * s_bytes, "flops": fft_y},
+            "ifft_x": {"kernel": "eig_inv_kernel", "bytes": s_bytes + io_bytes, "flops": gll + fft_x}}
+
+
+def _fp64_peak(dev) -> float:
+    """Dense FP64 throughput of this GPU (TFLOP/s): torch.matmul float64 4096^3
+    (cuBLAS DGEMM), best of 5, CUDA events."""
+    import torch
+
+    n = 4096
+    a = torch.randn(n, n, dtype=torch.float64, device=dev)
+    b = torch.randn(n, n, dtype=torch.float64, device=dev)
+    c = torch.empty_like(a)
+    torch.matmul(a, b, out=c)
+    best = 1e30
+    for _ in range(5):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        torch.matmul(a, b, out=c)
+        e1.record()
+        torch.cuda.synchronize()
+        best = min(best, e0.elapsed_time(e1))
+    return 2.0 * n ** 3 / (best * 1e-3) / 1e12
 
 
 def run_ours(args, ws, rank, local):
@@ -309,10 +348,19 @@ def run_ours(args, ws, rank, local):
     fnp = W.smooth_field_3d(NX, NY, NGLL, seed=SEED)
     f = torch.from_numpy(fnp).to(dev)
     dof = NX * NY * NGLL
-    plans = {
-        "fp32_refine": NonPeriodic3D(NX, NY, NGLL, NGLL, *DOM, Lambda=LAM, precision="fp32_refine"),
-        "fp64": NonPeriodic3D(NX, NY, NGLL, NGLL, *DOM, Lambda=LAM, precision="fp64"),
-    }
+    # plan creation: host setup (GLL grid, eigen-decompositions, per-shift data),
+    # uploads and, the first time a shape is seen in the process, the autotuner
+    plans, plan_ms = {}, {}
+    for prec in ("fp32_refine", "fp64"):
+        t0 = time.perf_counter()
+        plans[prec] = NonPeriodic3D(NX, NY, NGLL, NGLL, *DOM, Lambda=LAM, precision=prec)
+        torch.cuda.synchronize()
+        plan_ms[prec + "_with_autotune"] = 1e3 * (time.perf_counter() - t0)
+    t0 = time.perf_counter()
+    NonPeriodic3D(NX, NY, NGLL, NGLL, *DOM, Lambda=LAM, precision="fp64").DestroyPDEPlan()
+    torch.cuda.synchronize()
+    plan_ms["fp64_autotune_cached"] = 1e3 * (time.perf_counter() - t0)
+    fp64_peak = _fp64_peak(dev)
     outs = {k: p.SolvePDE(f) for k, p in plans.items()}
     torch.cuda.synchronize()
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
@@ -344,11 +392,11 @@ def run_ours(args, ws, rank, local):
         return sum(e0.elapsed_time(e1) for e0, e1 in evs)
 
     res = {}
-    launches = 0
     for name, p in plans.items():
         total_ms = timed(lambda p=p, name=name: p.SolvePDE(f, out=outs[name]))
         res[name] = total_ms
-    launches = 5 * args.steps  # five kernels per 3D solve, refined plan in the headline
+    kernels = {k: p.kernels() for k, p in plans.items()}
+    launches = len(kernels["fp32_refine"].split()) * args.steps  # the headline's timed solves
 
     # end to end through the public API: every step copies its f from pinned host
     # memory (H2D), solves, and reads its u back (D2H).  Steps are pipelined the
@@ -373,7 +421,6 @@ def run_ours(args, ws, rank, local):
             stream.wait_event(ev["in"][b])
             if i >= 2:
                 stream.wait_event(ev["out"][b])  # D2H i - 2 has read uds[b]
-            flush.add_(1.0)
             plans["fp32_refine"].SolvePDE(fds[b], out=uds[b], stream=stream)
             ev["solved"][b].record(stream)
             with torch.cuda.stream(s_out):
@@ -457,10 +504,15 @@ def run_ours(args, ws, rank, local):
         peak, peak_kind = _peak_hbm()
         spec_bytes = 16.0 * (NX // 2 + 1) * NY * NGLL
         io_bytes = 8.0 * dof
+        eig = kernels["fp32_refine"].startswith("eig_")
+        stages = _stage_model(eig, spec_bytes, io_bytes)
+        acc = {stages[k]["kernel"]: v for k, v in acc.items() if k in stages}
         dom = max(acc, key=acc.get)
-        alg = _stage_bytes(dom, spec_bytes, io_bytes)
+        alg = {v["kernel"]: v["bytes"] for v in stages.values()}[dom]
+        flops = {v["kernel"]: v["flops"] for v in stages.values()}[dom]
         achieved = alg / (acc[dom] * 1e-3) / 1e9
         traffic = _traffic_from_profiles(dom)
+        refine_fp64 = "fdm_tc_refine_kernel" not in kernels["fp32_refine"]
         line = {
             "metric": METRIC,
             "value": job_gdofs(dof, ws, ms_ref),
@@ -472,21 +524,30 @@ def run_ours(args, ws, rank, local):
             "higher_is_better": True,
             "scaling": "weak",
             "vs_baseline": None,
-            "dtype": "f32 solves + f64 residuals/FFTs",
+            "dtype": "f64" if refine_fp64 else "f32 solves + f64 residuals/FFTs",
             "data": "synthetic",
             "config": {"workload": WORKLOAD, "precision": "fp32_refine", "method": pref.info()["method"],
                        "refine_sweeps": 1, "l2": "256 MB buffer written before every timed solve",
-                       "parallelism": f"replicas x{ws}", "dof_per_solve": dof},
+                       "parallelism": f"replicas x{ws}", "dof_per_solve": dof,
+                       "kernels": kernels["fp32_refine"],
+                       "rows_kernel": ("FP64 arithmetic (the autotuner picked an FP64 path for the refined plan: "
+                                       "faster than its FP32 tensor-core refinement kernel at this shape)"
+                                       if refine_fp64 else "FP32 tensor-core solves + FP64 residual sweep")},
             "fp64": {"value": ws * dof / (ms_64 * 1e-3) / 1e9, "ms_per_step": ms_64,
-                     "method": plans["fp64"].info()["method"]},
+                     "method": plans["fp64"].info()["method"], "kernels": kernels["fp64"]},
             "refine_over_fp64": ms_64 / ms_ref,
             "rel_l2_refine_vs_fp64": rel_vs_fp64,
+            "plan_ms": plan_ms,
             "stage_ms": acc,
-            "stage_hbm_frac": {k: _stage_bytes(k, spec_bytes, io_bytes) / (v * 1e-3) / 1e9 / peak
-                               for k, v in acc.items() if v > 0},
+            "stage_hbm_frac": {k: {v["kernel"]: v["bytes"] for v in stages.values()}[k] / (t * 1e-3) / 1e9 / peak
+                               for k, t in acc.items() if t > 0},
             "roofline": {"kernel": dom, "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)",
-                         "algorithmic_bytes": alg, "traffic": (traffic or {}).get("fp32_refine")},
+                         "algorithmic_bytes": alg, "traffic": (traffic or {}).get("fp32_refine"),
+                         "compute": {"flops": flops, "achieved_tflops": flops / (acc[dom] * 1e-3) / 1e12,
+                                     "fp64_peak_tflops": fp64_peak,
+                                     "frac": flops / (acc[dom] * 1e-3) / 1e12 / fp64_peak,
+                                     "peak_source": "measured here: torch.matmul float64 4096^3, best of 5"}},
             "e2e": {"value": ws * dof / (ms_e2e * 1e-3) / 1e9, "unit": "GDOF/s", "ms_per_step": ms_e2e,
                     "pipelined": "H2D of step i+1 and D2H of step i-1 overlap the solve of step i",
                     "last_result_read_back": e2e_ok,

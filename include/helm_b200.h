@@ -212,18 +212,40 @@ int helm_plan_stage_times(helm_plan_t plan, float* ms5);
  * and inverse x FFT passes -- bit 0: 128-thread CTAs, bit 1: radix-8 schedule
  * (lengths 128, 256), bit 2: persistent pipelined pass, bit 3: 512-thread CTAs
  * for passes of length 512 or 1024 (ignored for shorter ones; with bit 2 the
- * tile exceeds shared memory and the solve fails with HELM_ERR_CUDA) -- and rows (0..2) for
- * the row solve (1: the second kernel shape; 2: FP64 3D plans with one element,
- * at most 65 GLL points and Ny in {64, 128, 256} only -- the y pass, the row
- * solve and the inverse y pass fused into one kernel per kx slab, the two y
- * entries of fft4 then unused).  Plan creation times every
- * variant on the plan's own shape and keeps the fastest per stage (environment
- * HELM_AUTOTUNE=0: all 0).  Setting them pins the choice, e.g. to reproduce a
- * run bit for bit.  Every variant computes the same transform; the last bits
- * of the results may differ between variants.  No counterpart in the
- * reference, which has one FFT code path. */
+ * tile exceeds shared memory and the solve fails with HELM_ERR_CUDA) -- and rows (0..4) for
+ * the row solve: 0, 1 the two kernel shapes of the plan's precision; 2 (FP64 and
+ * refined 3D plans with one element, at most 65 GLL points and Ny in {64, 128,
+ * 256}) the y pass, the row solve and the inverse y pass fused into one kernel
+ * per kx slab, the two y entries of fft4 then unused; 3 (refined plans with one
+ * element) the FP64 tensor-core row kernel on the refined plan's FP64 spectrum;
+ * 4 (FP64 and refined plans with one element, Dirichlet ends, at most 66 GLL
+ * points, Nx in {8, ..., 256}, Ny in {4, ..., 512}, powers of 2) the eigen-basis
+ * pipeline of the whole forward solve -- GLL eigen-transform fused with the x
+ * FFT, the y FFT, diagonal scaling and inverse y FFT in one pass, and the
+ * inverse of the first pass: three kernels in 3D, one in 2D, fft4 unused
+ * (adjoint solves of such a plan run variant 0, or 3 when refined).  Plan
+ * creation times every variant on the plan's own shape and keeps the fastest
+ * (environment HELM_AUTOTUNE=0: all 0, rows 4 where it applies).  Setting them
+ * pins the choice, e.g. to reproduce a run bit for bit.  Every variant
+ * computes the same solve; the last bits of the results may differ between
+ * variants.  No counterpart in the reference, which has one code path. */
 int helm_plan_get_launch_variants(helm_plan_t plan, int* fft4, int* rows);
 int helm_plan_set_launch_variants(helm_plan_t plan, const int* fft4, int rows);
+
+/* The kernels a forward helm_solve of the plan launches, as a short
+ * space-separated list of kernel names in launch order (for reports: which
+ * row kernel ran, e.g. whether a refined plan ran its FP32 tensor-core kernel or
+ * the FP64 one).  The string stays valid until the plan is destroyed or its
+ * variants change.  No counterpart in the reference. */
+const char* helm_plan_kernels(helm_plan_t plan);
+
+/* Test hook for the out-of-memory paths (host-side fault injection): with
+ * n >= 0 the n-th device allocation made by plan creation from now on (0: the
+ * next) fails as a failed cudaMalloc would -- the call returns HELM_ERR_OOM
+ * after freeing what it had allocated -- and the hook disarms itself; n < 0
+ * disarms it.  The reference exits on allocation failure (General.h:320-392,
+ * no status); this hook has no counterpart there. */
+int helm_debug_fail_alloc(long long n);
 
 /* helm_solve with the spectrum workspace taken from a fixed 16 MiB device
  * array inside this library instead of the plan's buffer; the call allocates

@@ -37,7 +37,8 @@ EXPORTS = (
     "helm2d_batch_create", "helm_batch_offsets", "helm_batch_info", "helm_batch_set_graph",
     "helm_batch_solve", "helm_batch_destroy", "helm_plan_get_launch_variants", "helm_plan_set_launch_variants",
     "helm2d_periodic_plan_create", "helm3d_periodic_plan_create", "helm_gll_derivative", "helm_fourier_derivative",
-    "helm_write_tecplot", "helm_write_vtk", "helm_solve_adjoint_misfit",
+    "helm_write_tecplot", "helm_write_vtk", "helm_solve_adjoint_misfit", "helm_solve_static_scratch",
+    "helm_plan_kernels", "helm_debug_fail_alloc",
 )
 
 # exact-solution callback of helm_write_tecplot: double exact(double x, double y, double z)
@@ -103,10 +104,13 @@ def lib() -> ctypes.CDLL:
     L.helm_status_string.restype = ctypes.c_char_p
     L.helm_last_error.argtypes = []
     L.helm_last_error.restype = ctypes.c_char_p
+    L.helm_debug_fail_alloc.argtypes = [ctypes.c_longlong]
+    L.helm_plan_kernels.argtypes = [ctypes.c_void_p]
+    L.helm_plan_kernels.restype = ctypes.c_char_p
     for name in EXPORTS:
         f = getattr(L, name)
         if f.restype is None or f.restype is ctypes.c_int:
-            if name not in ("helm_status_string", "helm_last_error"):
+            if name not in ("helm_status_string", "helm_last_error", "helm_plan_kernels"):
                 f.restype = ctypes.c_int
     _lib = L
     return L

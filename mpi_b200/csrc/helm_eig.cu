@@ -1,0 +1,577 @@
+// Eigen-basis pipeline of the one-element solve with Dirichlet ends, FP64,
+// sm_100a.
+//
+// The per-wavenumber solve of the reference (ConstructFundamentalSolutions +
+// LUSolve, DPS/src/NonPeriodic3D_MPI.cpp:184-232, with the Dirichlet ends of
+// the interface step :328-369 and the combination :582-587) is, for every
+// spectrum row (kx, ky),
+//     u_int = (D2int - sigma(kx, ky) I)^-1 (f_int + zl bl + zr br),
+//     u(0) = zl = gl / beta_l,  u(N-1) = zr = gr / beta_r,
+// with bl, br minus the boundary columns of D2.  D2int = V diag(mu) V^-1 (the
+// folded blocks of helm_fdm.cu), so the solve is V^-1 along the GLL index, a
+// diagonal scaling by 1 / (mu_j - sigma), and V along the GLL index.  V and
+// V^-1 act on the GLL index only and commute with the Fourier transforms along
+// x and y, which act on the other two.  The solve therefore runs as
+//   pass 1 (one CTA per y plane): load f[x][y][:] for all x, fold, apply V^-1
+//          (plus the boundary columns times zl, zr) on the FP64 tensor cores,
+//          real-to-complex FFT along x, store the coefficient spectrum
+//          S[kx][y][64];
+//   pass 2 (one CTA per kx and 16 coefficients): FFT along y, scale by
+//          1 / (mu_j - sigma) / (Nx Ny), inverse FFT along y, in place;
+//   pass 3 (one CTA per y plane): complex-to-real FFT along x, apply V on the
+//          tensor cores, unfold, write u[x][y][:] with the boundary values.
+// f is read once, u written once, and S crosses the memory system four times
+// (34 MB each at 256 x 256 x 65): three launches instead of five.  A 2D problem
+// is one plane: its whole solve is one CTA, one launch.
+#include "helm_device.cuh"
+#include "helm_eig.cuh"
+#include "helm_kernels.cuh"
+
+namespace helm {
+
+namespace {
+
+constexpr int EP_PITCH = 68;     // doubles per row of a plane in shared memory (P <= 66, 64 slots, 4 of pad)
+constexpr int EP_HS = EP_PITCH / 2;
+constexpr int EP_FRAG = 4 * 8 * 32;  // doubles of one fold's transform in fragment order
+constexpr double kR2 = 0.70710678118654752440;
+
+template <int L>
+struct EpShape {
+    static constexpr int WARPS = (L / 8 < 16) ? L / 8 : 16;
+    static constexpr int THREADS = 32 * WARPS;
+    static constexpr int RW = L / WARPS;  // rows of the plane per warp
+    static constexpr int MTW = RW / 8;    // 8-row tiles per warp
+    static_assert(MTW >= 1 && RW % 8 == 0, "plane rows per warp");
+    // plane, then the transforms it applies (2 folds, or all 4 for the fused 2D solve)
+    static constexpr size_t smem(int nmats) { return ((size_t)L * EP_PITCH + (size_t)nmats * EP_FRAG) * sizeof(double); }
+};
+
+__device__ __forceinline__ void copy_mats(double* dst, const double* src, int blk0, int blk1)
+{
+    const double2* s0 = reinterpret_cast<const double2*>(src + (size_t)blk0 * EP_FRAG);
+    const double2* s1 = reinterpret_cast<const double2*>(src + (size_t)blk1 * EP_FRAG);
+    double2* d = reinterpret_cast<double2*>(dst);
+    for (int e = threadIdx.x; e < EP_FRAG; e += blockDim.x) d[e] = (e < EP_FRAG / 2) ? s0[e] : s1[e - EP_FRAG / 2];
+}
+
+// Loads plane y of f (rows x = 0..L-1, GLL slots 1..P-2) into buf and the
+// scaled boundary values zl, zr into slots 0 and P-1.
+template <int L>
+__device__ __forceinline__ void load_plane(const EigArgs& a, const double* f, const double* gl, const double* gr,
+                                           long long yoff, long long bc_off, double* buf)
+{
+    const int P = a.P;
+    for (int e = threadIdx.x; e < L * P; e += blockDim.x) {
+        const int x = e / P, k = e - x * P;
+        double* d = buf + x * EP_PITCH + k;
+        const double* s = f + (long long)x * a.x_stride + yoff + k;
+        if (k == 0) *d = gl ? gl[(long long)x * a.bc_x_stride + bc_off] * a.ibl : 0.0;
+        else if (k == P - 1) *d = gr ? gr[(long long)x * a.bc_x_stride + bc_off] * a.ibr : 0.0;
+        else cp_async_bytes8(d, s, true);
+    }
+    cp_async_commit();
+    cp_async_wait_all();
+    if (a.sub) {  // adjoint of a least-squares misfit: ubar = u - u_obs at the interior slots
+        __syncthreads();
+        for (int e = threadIdx.x; e < L * P; e += blockDim.x) {
+            const int x = e / P, k = e - x * P;
+            if (k > 0 && k < P - 1) buf[x * EP_PITCH + k] -= a.sub[(long long)x * a.x_stride + yoff + k];
+        }
+    }
+}
+
+// First transform of the warp's rows (8 MTW rows at `rows`): coefficients of
+// the folded interior plus the boundary columns, written back over the rows as
+// slots 0..31 (symmetric fold) and 32..63 (antisymmetric fold).
+template <int MTW>
+__device__ __forceinline__ void first_transform(const EigArgs& a, double* rows, const double* Ms, const double* Ma,
+                                                const double* hbc, int lane)
+{
+    const int g = lane >> 2, q = lane & 3;
+    const int n = a.n, m = a.m, ms = a.ms, P = a.P;
+    double cs[MTW][4][2], ca[MTW][4][2];
+#pragma unroll
+    for (int mt = 0; mt < MTW; ++mt)
+#pragma unroll
+        for (int nt = 0; nt < 4; ++nt) cs[mt][nt][0] = cs[mt][nt][1] = ca[mt][nt][0] = ca[mt][nt][1] = 0.0;
+#pragma unroll 2
+    for (int kk = 0; kk < 8; ++kk) {
+        const int k = 4 * kk + q;
+        double as[MTW], aa[MTW];
+#pragma unroll
+        for (int mt = 0; mt < MTW; ++mt) {
+            const double* row = rows + (mt * 8 + g) * EP_PITCH;
+            double vs = 0.0, va = 0.0;
+            if (k < m) {
+                const double lo = row[1 + k], hi = row[n - k];
+                vs = kR2 * (lo + hi);
+                va = kR2 * (lo - hi);
+            } else if (k < ms) {
+                vs = row[1 + k];
+            }
+            as[mt] = vs;
+            aa[mt] = va;
+        }
+#pragma unroll
+        for (int nt = 0; nt < 4; ++nt) {
+            const double bs = Ms[(nt * 8 + kk) * 32 + lane], ba = Ma[(nt * 8 + kk) * 32 + lane];
+#pragma unroll
+            for (int mt = 0; mt < MTW; ++mt) {
+                dmma_8x8x4(cs[mt][nt][0], cs[mt][nt][1], as[mt], bs);
+                dmma_8x8x4(ca[mt][nt][0], ca[mt][nt][1], aa[mt], ba);
+            }
+        }
+    }
+    double zl[MTW], zr[MTW];
+#pragma unroll
+    for (int mt = 0; mt < MTW; ++mt) {
+        const double* row = rows + (mt * 8 + g) * EP_PITCH;
+        zl[mt] = row[0];
+        zr[mt] = row[P - 1];
+    }
+    __syncwarp();
+#pragma unroll
+    for (int nt = 0; nt < 4; ++nt)
+#pragma unroll
+        for (int j = 0; j < 2; ++j) {
+            const int i = nt * 8 + 2 * q + j;
+            const double hsl = hbc[i], hsr = hbc[32 + i], hal = hbc[64 + i], har = hbc[96 + i];
+#pragma unroll
+            for (int mt = 0; mt < MTW; ++mt) {
+                cs[mt][nt][j] += zl[mt] * hsl + zr[mt] * hsr;
+                ca[mt][nt][j] += zl[mt] * hal + zr[mt] * har;
+            }
+        }
+#pragma unroll
+    for (int mt = 0; mt < MTW; ++mt) {
+        double* row = rows + (mt * 8 + g) * EP_PITCH;
+#pragma unroll
+        for (int nt = 0; nt < 4; ++nt) {
+            *reinterpret_cast<double2*>(row + nt * 8 + 2 * q) = make_double2(cs[mt][nt][0], cs[mt][nt][1]);
+            *reinterpret_cast<double2*>(row + 32 + nt * 8 + 2 * q) = make_double2(ca[mt][nt][0], ca[mt][nt][1]);
+        }
+    }
+    __syncwarp();
+}
+
+// Second transform of the warp's rows (coefficients in slots 0..63), unfolded
+// into GLL slots 1..P-2 of the same rows; slots 0 and P-1 keep the boundary
+// values the caller puts there.
+template <int MTW>
+__device__ __forceinline__ void second_transform(const EigArgs& a, double* rows, const double* Ms, const double* Ma,
+                                                 int lane)
+{
+    const int g = lane >> 2, q = lane & 3;
+    const int n = a.n, m = a.m, ms = a.ms;
+    double cs[MTW][4][2], ca[MTW][4][2];
+#pragma unroll
+    for (int mt = 0; mt < MTW; ++mt)
+#pragma unroll
+        for (int nt = 0; nt < 4; ++nt) cs[mt][nt][0] = cs[mt][nt][1] = ca[mt][nt][0] = ca[mt][nt][1] = 0.0;
+#pragma unroll 2
+    for (int kk = 0; kk < 8; ++kk) {
+        const int k = 4 * kk + q;
+        double as[MTW], aa[MTW];
+#pragma unroll
+        for (int mt = 0; mt < MTW; ++mt) {
+            const double* row = rows + (mt * 8 + g) * EP_PITCH;
+            as[mt] = row[k];
+            aa[mt] = row[32 + k];
+        }
+#pragma unroll
+        for (int nt = 0; nt < 4; ++nt) {
+            const double bs = Ms[(nt * 8 + kk) * 32 + lane], ba = Ma[(nt * 8 + kk) * 32 + lane];
+#pragma unroll
+            for (int mt = 0; mt < MTW; ++mt) {
+                dmma_8x8x4(cs[mt][nt][0], cs[mt][nt][1], as[mt], bs);
+                dmma_8x8x4(ca[mt][nt][0], ca[mt][nt][1], aa[mt], ba);
+            }
+        }
+    }
+    __syncwarp();
+#pragma unroll
+    for (int mt = 0; mt < MTW; ++mt) {
+        double* row = rows + (mt * 8 + g) * EP_PITCH;
+#pragma unroll
+        for (int nt = 0; nt < 4; ++nt)
+#pragma unroll
+            for (int j = 0; j < 2; ++j) {
+                const int i = nt * 8 + 2 * q + j;
+                const double s = cs[mt][nt][j], d = ca[mt][nt][j];
+                if (i < m) {
+                    row[1 + i] = kR2 * (s + d);
+                    row[n - i] = kR2 * (s - d);
+                } else if (i < ms) {
+                    row[1 + i] = s;
+                }
+            }
+    }
+    __syncwarp();
+}
+
+// Real-to-complex split of the 32 column pairs of the transformed plane into
+// the half spectrum X (slot 2c) and Y (slot 2c+1) of row kx; emit(kx, c, X, Y).
+template <int L, typename Emit>
+__device__ __forceinline__ void r2c_split(const double2* z, int warp, int lane, Emit emit)
+{
+    for (int kx = warp; kx <= L / 2; kx += EpShape<L>::WARPS) {
+        const double2 zk = z[kx * EP_HS + lane], zm = z[((L - kx) & (L - 1)) * EP_HS + lane];
+        const double2 X = make_double2(0.5 * (zk.x + zm.x), 0.5 * (zk.y - zm.y));
+        const double2 Y = make_double2(0.5 * (zk.y + zm.y), 0.5 * (zm.x - zk.x));
+        emit(kx, lane, X, Y);
+    }
+}
+
+// Complex-to-real assembly: full-length Z[k] = X_k + i Y_k from the half
+// spectra of the 32 column pairs (imaginary parts dropped at k = 0 and L/2, as
+// the real part of the reference's inverse transform does); fetch(kx, c, X, Y).
+template <int L, typename Fetch>
+__device__ __forceinline__ void c2r_assemble(double2* z, int warp, int lane, Fetch fetch)
+{
+    for (int kx = warp; kx <= L / 2; kx += EpShape<L>::WARPS) {
+        double2 X, Y;
+        fetch(kx, lane, X, Y);
+        if (kx == 0 || kx == L / 2) { X.y = 0.0; Y.y = 0.0; }
+        z[kx * EP_HS + lane] = make_double2(X.x - Y.y, X.y + Y.x);
+        if (kx > 0 && kx < L / 2) z[(L - kx) * EP_HS + lane] = make_double2(X.x + Y.y, Y.x - X.y);
+    }
+}
+
+// ------------------------------------------------------------------ pass 1 --
+template <int L>
+__global__ void __launch_bounds__(EpShape<L>::THREADS, 1) eig_fwd_kernel(EigArgs a)
+{
+    using S = EpShape<L>;
+    extern __shared__ __align__(16) double esm[];
+    double* buf = esm;
+    double* Mt = esm + (size_t)L * EP_PITCH;
+    copy_mats(Mt, a.mats, 0, 2);
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int y = blockIdx.x;
+    pdl_enter();
+    if (a.lam_out && blockIdx.x == 0 && threadIdx.x == 0) *a.lam_out = 0.0;
+    load_plane<L>(a, a.f, a.adjoint ? nullptr : a.gl, a.adjoint ? nullptr : a.gr, (long long)y * a.P, y, buf);
+    __syncthreads();
+    first_transform<S::MTW>(a, buf + warp * S::RW * EP_PITCH, Mt, Mt + EP_FRAG, a.hbc, lane);
+    __syncthreads();
+    double2* z = reinterpret_cast<double2*>(buf);
+    slab_fft<L, -1, S::THREADS>(z, EP_HS, 32, static_cast<const double2*>(a.tw_x));
+    double2* Sg = reinterpret_cast<double2*>(a.S);
+    const long long Ny = a.Ny;
+    r2c_split<L>(z, warp, lane, [&](int kx, int c, double2 X, double2 Y) {
+        double2* row = Sg + ((long long)kx * Ny + y) * EIG_SLOTS;
+        row[2 * c] = X;
+        row[2 * c + 1] = Y;
+    });
+}
+
+// ------------------------------------------------------------------ pass 2 --
+template <int NY, int CT>
+__global__ void __launch_bounds__(256) eig_conv_kernel(EigArgs a)
+{
+    extern __shared__ __align__(16) double esm[];
+    double2* sm = reinterpret_cast<double2*>(esm);
+    constexpr int TILES = EIG_SLOTS / CT;
+    const int kx = blockIdx.x / TILES, j0 = (blockIdx.x - kx * TILES) * CT;
+    double2* Sg = reinterpret_cast<double2*>(a.S) + (long long)kx * NY * EIG_SLOTS + j0;
+    pdl_enter();
+    for (int e = threadIdx.x; e < NY * CT; e += blockDim.x) {
+        const int ky = e / CT, c = e - ky * CT;
+        cp_async_bytes16(&sm[ky * CT + c], &Sg[(long long)ky * EIG_SLOTS + c], true);
+    }
+    cp_async_commit();
+    cp_async_wait_all();
+    __syncthreads();
+    const double2* tw = static_cast<const double2*>(a.tw_y);
+    slab_fft<NY, -1, 256>(sm, CT, CT, tw);
+    const double* rc = a.recip;
+    for (int e = threadIdx.x; e < NY * CT; e += blockDim.x) {
+        const int ky = e / CT, c = e - ky * CT;
+        const double r = rc[(long long)a.grp_of_row[kx * NY + ky] * EIG_SLOTS + j0 + c] * a.scale;
+        const double2 v = sm[ky * CT + c];
+        sm[ky * CT + c] = make_double2(v.x * r, v.y * r);
+    }
+    __syncthreads();
+    slab_fft<NY, 1, 256>(sm, CT, CT, tw);
+    for (int e = threadIdx.x; e < NY * CT; e += blockDim.x) {
+        const int ky = e / CT, c = e - ky * CT;
+        Sg[(long long)ky * EIG_SLOTS + c] = sm[ky * CT + c];
+    }
+}
+
+// Adjoint: the boundary terms of the transposed map for the warp's rows,
+// b_l . fbar_int = hsl . cs + hal . ca (and the same with the right-hand
+// vectors), from the coefficients in slots 0..63 before the second transform.
+template <int L>
+__device__ __forceinline__ void adjoint_boundary_dots(const EigArgs& a, const double* rows, int lane, double* dl,
+                                                      double* dr)
+{
+    using S = EpShape<L>;
+    const double hs0 = a.hbc[lane], hs1 = a.hbc[EIG_LD + lane], ha0 = a.hbc[2 * EIG_LD + lane],
+                 ha1 = a.hbc[3 * EIG_LD + lane];
+    for (int r = 0; r < S::RW; ++r) {
+        const double cs = rows[r * EP_PITCH + lane], ca = rows[r * EP_PITCH + 32 + lane];
+        double vl = hs0 * cs + ha0 * ca, vr = hs1 * cs + ha1 * ca;
+        for (int o = 16; o > 0; o >>= 1) {
+            vl += __shfl_xor_sync(0xffffffffu, vl, o);
+            vr += __shfl_xor_sync(0xffffffffu, vr, o);
+        }
+        if (lane == r) { *dl = vl; *dr = vr; }
+    }
+}
+
+// Adjoint: writes the warp's rows of fbar (boundary slots 0), the boundary
+// cotangents gbar = (ubar_boundary + dot) / beta, and returns this lane's share
+// of sum(fbar u).
+template <int L>
+__device__ __forceinline__ double store_adjoint_rows(const EigArgs& a, double* fbar, const double* ubar,
+                                                     long long yoff, long long bc_off, double* rows, int x0, int lane,
+                                                     double dl, double dr)
+{
+    using S = EpShape<L>;
+    const int P = a.P;
+    if (lane < S::RW) {
+        const long long x = x0 + lane;
+        const long long o = x * a.x_stride + yoff;
+        if (a.gbar_l) {
+            const double u0 = ubar[o] - (a.sub ? a.sub[o] : 0.0);
+            a.gbar_l[x * a.bc_x_stride + bc_off] = (u0 + dl) * a.ibl;
+        }
+        if (a.gbar_r) {
+            const double uN = ubar[o + P - 1] - (a.sub ? a.sub[o + P - 1] : 0.0);
+            a.gbar_r[x * a.bc_x_stride + bc_off] = (uN + dr) * a.ibr;
+        }
+        rows[lane * EP_PITCH] = 0.0;
+        rows[lane * EP_PITCH + P - 1] = 0.0;
+    }
+    __syncwarp();
+    double acc = 0.0;
+    for (int r = 0; r < S::RW; ++r) {
+        const long long o = (long long)(x0 + r) * a.x_stride + yoff;
+        for (int k = lane; k < P; k += 32) {
+            const double v = rows[r * EP_PITCH + k];
+            fbar[o + k] = v;
+            if (a.lam_u) acc += v * a.lam_u[o + k];
+        }
+    }
+    return acc;
+}
+
+// Adds every thread's acc into *a.lam_out, one atomic per CTA (all threads call).
+__device__ __forceinline__ void eig_lambda_sum(const EigArgs& a, double acc)
+{
+    __shared__ double red[32];
+    for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+    __syncthreads();
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = acc;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double sum = 0.0;
+        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) sum += red[w];
+        atomicAdd(a.lam_out, sum);
+    }
+}
+
+// ------------------------------------------------------------------ pass 3 --
+// Writes the warp's rows of plane y: boundary slots from gl, gr, then the rows.
+template <int L>
+__device__ __forceinline__ void store_plane_rows(const EigArgs& a, double* u, const double* gl, const double* gr,
+                                                 long long yoff, long long bc_off, double* rows, int x0, int lane)
+{
+    using S = EpShape<L>;
+    const int P = a.P;
+    if (lane < S::RW) {
+        const long long x = x0 + lane;
+        rows[lane * EP_PITCH] = gl ? gl[x * a.bc_x_stride + bc_off] * a.ibl : 0.0;
+        rows[lane * EP_PITCH + P - 1] = gr ? gr[x * a.bc_x_stride + bc_off] * a.ibr : 0.0;
+    }
+    __syncwarp();
+    for (int r = 0; r < S::RW; ++r) {
+        double* dst = u + (long long)(x0 + r) * a.x_stride + yoff;
+        for (int k = lane; k < P; k += 32) dst[k] = rows[r * EP_PITCH + k];
+    }
+}
+
+template <int L>
+__global__ void __launch_bounds__(EpShape<L>::THREADS, 1) eig_inv_kernel(EigArgs a)
+{
+    using S = EpShape<L>;
+    extern __shared__ __align__(16) double esm[];
+    double* buf = esm;
+    double* Mt = esm + (size_t)L * EP_PITCH;
+    copy_mats(Mt, a.mats, 1, 3);
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int y = blockIdx.x;
+    double2* z = reinterpret_cast<double2*>(buf);
+    const double2* Sg = reinterpret_cast<const double2*>(a.S);
+    const long long Ny = a.Ny;
+    pdl_enter();
+    c2r_assemble<L>(z, warp, lane, [&](int kx, int c, double2& X, double2& Y) {
+        const double2* row = Sg + ((long long)kx * Ny + y) * EIG_SLOTS;
+        X = row[2 * c];
+        Y = row[2 * c + 1];
+    });
+    __syncthreads();
+    slab_fft<L, 1, S::THREADS>(z, EP_HS, 32, static_cast<const double2*>(a.tw_x));
+    double* rows = buf + warp * S::RW * EP_PITCH;
+    if (!a.adjoint) {
+        second_transform<S::MTW>(a, rows, Mt, Mt + EP_FRAG, lane);
+        store_plane_rows<L>(a, a.u, a.gl, a.gr, (long long)y * a.P, y, rows, warp * S::RW, lane);
+        return;
+    }
+    double dl = 0.0, dr = 0.0;
+    adjoint_boundary_dots<L>(a, rows, lane, &dl, &dr);
+    __syncwarp();
+    second_transform<S::MTW>(a, rows, Mt, Mt + EP_FRAG, lane);
+    const double acc =
+        store_adjoint_rows<L>(a, a.u, a.f, (long long)y * a.P, y, rows, warp * S::RW, lane, dl, dr);
+    if (a.lam_out) eig_lambda_sum(a, acc);
+}
+
+// --------------------------------------------------------- fused 2D solve --
+// One CTA per problem: the whole pipeline on one plane, the diagonal scaling
+// applied to the half spectrum in shared memory between the two FFTs.
+template <int L>
+__global__ void __launch_bounds__(EpShape<L>::THREADS, 1) eig_solve2d_kernel(EigArgs a)
+{
+    using S = EpShape<L>;
+    extern __shared__ __align__(16) double esm[];
+    double* buf = esm;
+    double* M1 = esm + (size_t)L * EP_PITCH;
+    double* M2 = M1 + 2 * EP_FRAG;
+    copy_mats(M1, a.mats, 0, 2);
+    copy_mats(M2, a.mats, 1, 3);
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int b = blockIdx.x;
+    const long long off = a.boff ? a.boff[b] : 0;
+    // batched problems have no boundary data (homogeneous Dirichlet rows);
+    // adjoint solves read none
+    const double* gl = (a.boff || a.adjoint) ? nullptr : a.gl;
+    const double* gr = (a.boff || a.adjoint) ? nullptr : a.gr;
+    pdl_enter();
+    if (a.lam_out && threadIdx.x == 0) *a.lam_out = 0.0;
+    load_plane<L>(a, a.f + off, gl, gr, 0, 0, buf);
+    __syncthreads();
+    double* rows = buf + warp * S::RW * EP_PITCH;
+    first_transform<S::MTW>(a, rows, M1, M1 + EP_FRAG, a.hbc, lane);
+    __syncthreads();
+    double2* z = reinterpret_cast<double2*>(buf);
+    const double2* tw = static_cast<const double2*>(a.tw_x);
+    slab_fft<L, -1, S::THREADS>(z, EP_HS, 32, tw);
+    // split, scale and reassemble each pair of rows (kx, L - kx) in place
+    for (int kx = warp; kx <= L / 2; kx += S::WARPS) {
+        const int km = (L - kx) & (L - 1);
+        const double2 zk = z[kx * EP_HS + lane], zm = z[km * EP_HS + lane];
+        double2 X = make_double2(0.5 * (zk.x + zm.x), 0.5 * (zk.y - zm.y));
+        double2 Y = make_double2(0.5 * (zk.y + zm.y), 0.5 * (zm.x - zk.x));
+        const double* rc = a.recip + (long long)a.grp_of_row[(long long)b * (L / 2 + 1) + kx] * EIG_SLOTS;
+        const double r0 = rc[2 * lane] * a.scale, r1 = rc[2 * lane + 1] * a.scale;
+        X = make_double2(X.x * r0, X.y * r0);
+        Y = make_double2(Y.x * r1, Y.y * r1);
+        if (kx == 0 || kx == L / 2) { X.y = 0.0; Y.y = 0.0; }
+        z[kx * EP_HS + lane] = make_double2(X.x - Y.y, X.y + Y.x);
+        if (kx > 0 && kx < L / 2) z[km * EP_HS + lane] = make_double2(X.x + Y.y, Y.x - X.y);
+    }
+    __syncthreads();
+    slab_fft<L, 1, S::THREADS>(z, EP_HS, 32, tw);
+    if (!a.adjoint) {
+        second_transform<S::MTW>(a, rows, M2, M2 + EP_FRAG, lane);
+        store_plane_rows<L>(a, a.u + off, gl, gr, 0, 0, rows, warp * S::RW, lane);
+        return;
+    }
+    double dl = 0.0, dr = 0.0;
+    adjoint_boundary_dots<L>(a, rows, lane, &dl, &dr);
+    __syncwarp();
+    second_transform<S::MTW>(a, rows, M2, M2 + EP_FRAG, lane);
+    const double acc = store_adjoint_rows<L>(a, a.u, a.f, 0, 0, rows, warp * S::RW, lane, dl, dr);
+    if (a.lam_out) eig_lambda_sum(a, acc);
+}
+
+template <typename K>
+cudaError_t prep(K k, size_t smem)
+{
+    return cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+}
+
+template <int L>
+int run_3d(int pass, const EigArgs& a, cudaStream_t s)
+{
+    using S = EpShape<L>;
+    cudaError_t e;
+    const size_t sm1 = S::smem(2);
+    if (pass == 0) {
+        if ((e = prep(eig_fwd_kernel<L>, sm1)) != cudaSuccess) return (int)e;
+        return (int)launch_k(eig_fwd_kernel<L>, dim3(a.Ny), dim3(S::THREADS), sm1, s, a);
+    }
+    if (pass == 2) {
+        if ((e = prep(eig_inv_kernel<L>, sm1)) != cudaSuccess) return (int)e;
+        return (int)launch_k(eig_inv_kernel<L>, dim3(a.Ny), dim3(S::THREADS), sm1, s, a);
+    }
+    const int nkx = L / 2 + 1;
+    switch (a.Ny) {
+#define HELM_EIG_CONV(NY, CT)                                                                                   \
+    case NY: {                                                                                                  \
+        const size_t sm2 = (size_t)NY * CT * sizeof(double2);                                                   \
+        if ((e = prep(eig_conv_kernel<NY, CT>, sm2)) != cudaSuccess) return (int)e;                             \
+        return (int)launch_k(eig_conv_kernel<NY, CT>, dim3(nkx * (EIG_SLOTS / CT)), dim3(256), sm2, s, a);      \
+    }
+        HELM_EIG_CONV(4, 16)
+        HELM_EIG_CONV(8, 16)
+        HELM_EIG_CONV(16, 16)
+        HELM_EIG_CONV(32, 16)
+        HELM_EIG_CONV(64, 16)
+        HELM_EIG_CONV(128, 16)
+        HELM_EIG_CONV(256, 16)
+        HELM_EIG_CONV(512, 8)
+#undef HELM_EIG_CONV
+        default: return (int)cudaErrorInvalidValue;
+    }
+}
+
+template <int L>
+int run_2d(const EigArgs& a, int nprob, cudaStream_t s)
+{
+    using S = EpShape<L>;
+    const size_t sm = S::smem(4);
+    cudaError_t e = prep(eig_solve2d_kernel<L>, sm);
+    if (e != cudaSuccess) return (int)e;
+    return (int)launch_k(eig_solve2d_kernel<L>, dim3(nprob), dim3(S::THREADS), sm, s, a);
+}
+
+}  // namespace
+
+bool eig_shape_ok(int dim, int Nx, int Ny, int P)
+{
+    if (P < 4 || P > 2 * EIG_LD + 2) return false;
+    if (Nx < 8 || Nx > 256 || (Nx & (Nx - 1))) return false;
+    if (dim == 2) return true;
+    return Ny >= 4 && Ny <= 512 && !(Ny & (Ny - 1));
+}
+
+int launch_eig_pass(int pass, int dim, int Nx, const EigArgs& a, int nprob, cudaStream_t s)
+{
+    if (dim == 3) {
+        switch (Nx) {
+            case 8: return run_3d<8>(pass, a, s);
+            case 16: return run_3d<16>(pass, a, s);
+            case 32: return run_3d<32>(pass, a, s);
+            case 64: return run_3d<64>(pass, a, s);
+            case 128: return run_3d<128>(pass, a, s);
+            case 256: return run_3d<256>(pass, a, s);
+            default: return (int)cudaErrorInvalidValue;
+        }
+    }
+    if (pass != 0) return 0;
+    switch (Nx) {
+        case 8: return run_2d<8>(a, nprob, s);
+        case 16: return run_2d<16>(a, nprob, s);
+        case 32: return run_2d<32>(a, nprob, s);
+        case 64: return run_2d<64>(a, nprob, s);
+        case 128: return run_2d<128>(a, nprob, s);
+        case 256: return run_2d<256>(a, nprob, s);
+        default: return (int)cudaErrorInvalidValue;
+    }
+}
+
+}  // namespace helm

@@ -967,81 +967,6 @@ struct SlabArgs {
     const int* grp_of_row; // shift group of each spectrum row kx Ny + ky
 };
 
-template <int R, int NS, int TPC>
-__device__ __forceinline__ int slab_out_row(int tc, int t, int r)
-{
-    const int j = tc + t * TPC;
-    return (j / NS) * NS * R + (j % NS) + r * NS;
-}
-
-template <int L, int R, int NS, int TPC, int R0>
-__device__ __forceinline__ void slab_to_smem(cplx_t<double>* sm, int hs, int tc, int col, const cplx_t<double> (&v)[R0])
-{
-#pragma unroll
-    for (int t = 0; t < R0 / R; ++t)
-#pragma unroll
-        for (int r = 0; r < R; ++r) sm[slab_out_row<R, NS, TPC>(tc, t, r) * hs + col] = v[t * R + r];
-}
-
-template <int L, int R, int NS, int DIR, int TPC, int R0>
-__device__ __forceinline__ void slab_from_smem(const cplx_t<double>* sm, int hs, const cplx_t<double>* tw, int tc,
-                                               int col, cplx_t<double> (&v)[R0])
-{
-    using C = cplx_t<double>;
-#pragma unroll
-    for (int t = 0; t < R0 / R; ++t) {
-        const int j = tc + t * TPC, jm = j % NS;
-        C w8[R];
-#pragma unroll
-        for (int r = 0; r < R; ++r) {
-            C x = sm[(j + r * (L / R)) * hs + col];
-            if (NS > 1 && r > 0) {
-                const C w = tw[r * jm * (L / (NS * R))];
-                x = (DIR < 0) ? cmul(x, w) : cmulc(x, w);
-            }
-            w8[r] = x;
-        }
-        dft_reg<R, DIR, double>(w8);
-#pragma unroll
-        for (int r = 0; r < R; ++r) v[t * R + r] = w8[r];
-    }
-}
-
-// One length-L FFT (direction DIR, unscaled) of each of the ncol columns of the
-// [L][hs] complex array sm, in place; all THREADS threads of the CTA call it.
-template <int L, int DIR, int THREADS>
-__device__ __forceinline__ void slab_fft(cplx_t<double>* sm, int hs, int ncol, const cplx_t<double>* tw)
-{
-    using C = cplx_t<double>;
-    using RS = Radix<L>;
-    constexpr int R0 = RS::r0, R1 = RS::r1, R2 = RS::r2, NP = RS::n, TPC = L / R0, CPR = THREADS / TPC;
-    constexpr int RL = (NP == 1) ? R0 : (NP == 2 ? R1 : R2);
-    const int tc = threadIdx.x / CPR, cl = threadIdx.x - tc * CPR;
-    for (int c0 = 0; c0 < ncol; c0 += CPR) {
-        const int col = c0 + cl;
-        const bool on = col < ncol;
-        C v[R0];
-#pragma unroll
-        for (int r = 0; r < R0; ++r) v[r] = on ? sm[(tc + r * TPC) * hs + col] : mk(0.0, 0.0);
-        dft_reg<R0, DIR, double>(v);
-        if constexpr (NP >= 2) {
-            __syncthreads();
-            if (on) slab_to_smem<L, R0, 1, TPC, R0>(sm, hs, tc, col, v);
-            __syncthreads();
-            if (on) slab_from_smem<L, R1, R0, DIR, TPC, R0>(sm, hs, tw, tc, col, v);
-        }
-        if constexpr (NP >= 3) {
-            __syncthreads();
-            if (on) slab_to_smem<L, R1, R0, TPC, R0>(sm, hs, tc, col, v);
-            __syncthreads();
-            if (on) slab_from_smem<L, R2, R0 * R1, DIR, TPC, R0>(sm, hs, tw, tc, col, v);
-        }
-        __syncthreads();
-        if (on) slab_to_smem<L, RL, L / RL, TPC, R0>(sm, hs, tc, col, v);
-        __syncthreads();
-    }
-}
-
 // A spectrum row split over the two halves of a slab (slots k < h in a, the rest in b).
 struct SlabRow {
     cplx_t<double>* a;

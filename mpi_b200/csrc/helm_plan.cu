@@ -13,10 +13,12 @@
 #include "helm_fdm.cuh"
 #include "helm_kernels.cuh"
 #include "helm_plan.hpp"
+#include "helm_eig.cuh"
 #include "helm_setup.hpp"
 
 #include <algorithm>
 #include <array>
+#include <atomic>
 #include <cmath>
 #include <cstdlib>
 #include <cstring>
@@ -51,10 +53,19 @@ void Plan::release()
     device_bytes = 0;
 }
 
+// Host-side fault injection for tests of the out-of-memory paths: while armed
+// with n >= 0, the n-th device allocation of a plan from then on (0: the next)
+// fails as a cudaMalloc failure would, and the hook disarms itself.
+static std::atomic<long long> g_alloc_fault{-1};
+
 int Plan::alloc(void** p, size_t bytes)
 {
     *p = nullptr;
     if (bytes == 0) return HELM_OK;
+    if (g_alloc_fault.load() >= 0 && g_alloc_fault.fetch_sub(1) == 0) {
+        g_last_error = "device allocation failure injected by helm_debug_fail_alloc";
+        return HELM_ERR_OOM;
+    }
     cudaError_t e = cudaMalloc(p, bytes);
     if (e != cudaSuccess) {
         *p = nullptr;
@@ -345,7 +356,9 @@ static int setup_fast(Plan& p, const std::vector<double>& A0, int prec_code)
         fdm_m16_swizzle2(d2a.data(), ld, mm.data());
         if ((st = p.upload((void**)&p.d_ftcm_adj, mm.data(), mm.size() * sizeof(double)))) return st;
     }
-    if (prec_code == 0) {
+    // FP64 tensor-core transforms: FP64 plans, and refined plans (whose FP64
+    // spectrum the FP64 row kernel and the eigen-basis pipeline can also solve)
+    if (prec_code == 0 || prec_code == 2) {
         std::vector<double> sw(4 * L2);
         fdm_mma_swizzle(fw.data(), ld, sw.data());
         if ((st = p.upload((void**)&p.d_fmma, sw.data(), sw.size() * sizeof(double)))) return st;
@@ -357,15 +370,43 @@ static int setup_fast(Plan& p, const std::vector<double>& A0, int prec_code)
         if ((st = p.upload((void**)&p.d_fmma16_adj, sw.data(), sw.size() * sizeof(double)))) return st;
     }
     if ((st = up_t(recip, &p.d_frecip))) return st;
+    if (prec_code == 2 && (st = p.upload((void**)&p.d_frecip64, recip.data(), recip.size() * sizeof(double)))) return st;
+    if (prec_code == 0) p.d_frecip64 = static_cast<double*>(p.d_frecip);
     if ((st = p.upload((void**)&p.d_fd2, d2f.data(), d2f.size() * sizeof(double)))) return st;
     if ((st = p.upload((void**)&p.d_fd2_adj, d2a.data(), d2a.size() * sizeof(double)))) return st;
     if ((st = p.upload((void**)&p.d_row_grp, row_grp.data(), row_grp.size() * sizeof(int)))) return st;
-    if (prec_code == 0 && p.dim == 3 && p.batch == 1 && slab_fits(p.Ny, N, ld)) {
-        std::vector<int> gor((size_t)p.nrows, 0);
+    const bool slab = prec_code != 1 && p.dim == 3 && p.batch == 1 && slab_fits(p.Ny, N, ld);
+    const bool eig = p.eig_cand && ld == EIG_LD && prec_code != 1;
+    if (slab || eig) {
+        std::vector<int> gor((size_t)p.nrows * p.batch, 0);
         for (int g = 0; g < G; ++g)
             for (int rr = p.grp_start[g]; rr < p.grp_start[g + 1]; ++rr) gor[p.grp_rows[rr]] = g;
         if ((st = p.upload((void**)&p.d_grp_of_row, gor.data(), gor.size() * sizeof(int)))) return st;
-        p.slab_ok = true;
+        p.slab_ok = slab;
+    }
+    if (eig) {
+        // first transform of the folded boundary columns bl = -D2[int][0],
+        // br = -D2[int][N-1]: the coefficients that zl = gl / beta_l and
+        // zr = gr / beta_r add to each row's
+        std::vector<double> bl(n), br(n);
+        for (int i = 0; i < n; ++i) {
+            bl[i] = -D2[(size_t)(i + 1) * N];
+            br[i] = -D2[(size_t)(i + 1) * N + N - 1];
+        }
+        const std::vector<double> fbl = fold(bl), fbr = fold(br);
+        std::vector<double> hbc(4 * EIG_LD, 0.0);
+        for (int i = 0; i < ms; ++i)
+            for (int j = 0; j < ms; ++j) {
+                hbc[i] += Vsi[(size_t)i * ms + j] * fbl[j];
+                hbc[EIG_LD + i] += Vsi[(size_t)i * ms + j] * fbr[j];
+            }
+        for (int i = 0; i < ma; ++i)
+            for (int j = 0; j < ma; ++j) {
+                hbc[2 * EIG_LD + i] += Vai[(size_t)i * ma + j] * fbl[ld + j];
+                hbc[3 * EIG_LD + i] += Vai[(size_t)i * ma + j] * fbr[ld + j];
+            }
+        if ((st = p.upload((void**)&p.d_hbc, hbc.data(), hbc.size() * sizeof(double)))) return st;
+        p.eig_ok = true;
     }
     if ((st = p.upload((void**)&p.d_fe0, fe0.data(), fe0.size() * sizeof(double)))) return st;
     if ((st = p.upload((void**)&p.d_feN, feN.data(), feN.size() * sizeof(double)))) return st;
@@ -538,9 +579,15 @@ static int setup_plan(Plan& p)
     p.elem_spec = p.nrows * N;
     int st;
     // the spectrum scratch also holds the half spectra of a derivative along y
-    // (Nx x (Ny/2+1) rows per element), larger than the solve's when Nx > Ny
-    const long long spec_elems = std::max(p.elem_spec, p.dim == 3 ? (long long)p.Nx * (p.Ny / 2 + 1) * N : 0LL);
-    if ((st = p.alloc(&p.d_spec, (size_t)p.Ns * p.batch * spec_elems * (td ? 16 : 8)))) return st;
+    // (Nx x (Ny/2+1) rows per element), larger than the solve's when Nx > Ny,
+    // and the coefficient spectrum of the eigen-basis pipeline (64 per row)
+    p.eig_cand = p.Ns == 1 && !p.periodic && !p.fd && p.bc.alphal == 0.0 && p.bc.alphar == 0.0 &&
+                 p.precision != HELM_FP32 && p.method == HELM_METHOD_FDM && (p.batch == 1 || p.dim == 2) &&
+                 eig_shape_ok(p.dim, p.Nx, p.Ny, N);
+    long long spec_elems = std::max(p.elem_spec, p.dim == 3 ? (long long)p.Nx * (p.Ny / 2 + 1) * N : 0LL);
+    if (p.eig_cand && p.dim == 3) spec_elems = std::max(spec_elems, p.nrows * (long long)EIG_SLOTS);
+    p.spec_bytes = (size_t)p.Ns * p.batch * spec_elems * (td ? 16 : 8);
+    if ((st = p.alloc(&p.d_spec, p.spec_bytes))) return st;
     auto up_tw = [&](int L, void** d) -> int {
         if (td) { auto t = twiddles<double>(L); return p.upload(d, t.data(), t.size() * sizeof(double)); }
         auto t = twiddles<float>(L);
@@ -662,9 +709,11 @@ static int fft_pass(Plan& p, int L, int mode, int dir, const void* in, void* out
 // GLL boundary slots of the spectrum, out = u.  Adjoint: in = ubar read in
 // every slot, the transposed row solve, out = A^-T ubar in every slot.
 static int run_pipeline(Plan& p, const void* in, const double* gl, const double* gr, void* out, bool adjoint,
-                        cudaStream_t s, const AdjOut* adj = nullptr)
+                        cudaStream_t s, const AdjOut* adj = nullptr, const Workspace* ws = nullptr)
 {
     const int N = p.N;
+    void* const spec = ws ? ws->spec : p.d_spec;
+    void* const cprime = ws ? ws->cprime : p.d_cprime;
     const long long cols = (long long)(p.dim == 3 ? p.Ny : 1) * N;  // real columns per x row
     const int nkx = p.Nx / 2 + 1;
     int st;
@@ -672,22 +721,75 @@ static int run_pipeline(Plan& p, const void* in, const double* gl, const double*
         if (p.stage_timing) cudaEventRecord(p.ev[i], s);
     };
     mark(0);
+    // row variant in effect: the eigen-basis pipeline covers forward solves
+    int rv = p.row_var;
+    if (rv == 4 && (!p.eig_ok || (adjoint && !p.d_fmma_adj))) rv = p.precision == HELM_FP64 ? 0 : 3;
+    if (rv == 3 && (p.precision != HELM_FP32_REFINE || !p.d_fmma)) rv = 0;
+    if (rv == 4) {
+        // three launches (3D) or one (2D): GLL transform + x FFT, y convolution,
+        // inverse; stage events 1 and 4 bracket the middle pass
+        EigArgs ea{};
+        ea.f = static_cast<const double*>(in);
+        ea.u = static_cast<double*>(out);
+        ea.S = static_cast<double*>(spec);
+        ea.gl = gl;
+        ea.gr = gr;
+        ea.ibl = 1.0 / p.bc.betal;
+        ea.ibr = 1.0 / p.bc.betar;
+        ea.x_stride = p.x_stride;
+        ea.bc_x_stride = p.dim == 3 ? p.bc_x_stride : 1;
+        ea.Ny = p.dim == 3 ? p.Ny : 1;
+        ea.P = N;
+        ea.n = p.n;
+        ea.m = p.fm;
+        ea.ms = p.fms;
+        ea.mats = adjoint ? p.d_fmma_adj : p.d_fmma;
+        if (adjoint) {
+            ea.adjoint = 1;
+            ea.sub = adj ? adj->sub : nullptr;
+            ea.gbar_l = adj ? adj->glbar : nullptr;
+            ea.gbar_r = adj ? adj->grbar : nullptr;
+            ea.lam_out = adj ? adj->lambda_bar : nullptr;
+            ea.lam_u = ea.lam_out ? adj->u : nullptr;
+        }
+        ea.hbc = p.d_hbc;
+        ea.recip = p.d_frecip64;
+        ea.grp_of_row = p.d_grp_of_row;
+        ea.tw_x = p.d_tw_x;
+        ea.tw_y = p.d_tw_y;
+        ea.scale = 1.0 / ((double)p.Nx * (p.dim == 3 ? p.Ny : 1));
+        ea.boff = p.d_boff;  // size-class plans of a batch: the packed offsets (one problem or more)
+        int e = launch_eig_pass(0, p.dim, p.Nx, ea, p.batch, s);
+        if (e) return set_cuda_error((cudaError_t)e, "eigen-basis pass 1");
+        mark(1);
+        if (p.dim == 3 && (e = launch_eig_pass(1, p.dim, p.Nx, ea, 1, s)))
+            return set_cuda_error((cudaError_t)e, "eigen-basis pass 2");
+        mark(2);
+        mark(3);
+        mark(4);
+        if (p.dim == 3 && (e = launch_eig_pass(2, p.dim, p.Nx, ea, 1, s)))
+            return set_cuda_error((cudaError_t)e, "eigen-basis pass 3");
+        mark(5);
+        return HELM_OK;
+    }
     // 1. x: real-to-complex (forward: GLL boundary slots take the boundary data)
-    if ((st = fft_pass(p, p.Nx, FFT_R2C, -1, in, p.d_spec, p.x_stride, cols, p.elem_stride, p.elem_spec, (int)cols,
+    if ((st = fft_pass(p, p.Nx, FFT_R2C, -1, in, spec, p.x_stride, cols, p.elem_stride, p.elem_spec, (int)cols,
                        p.Ns * p.batch, 1.0, p.d_tw_x, gl, gr, !adjoint, adjoint, 0, s, adj)))
         return st;
     mark(1);
-    // FP64 3D plans may run stages 2-4 as one fused kernel per kx slab
-    const bool slab = p.row_var == 2 && p.slab_ok && p.fast && p.precision == HELM_FP64;
+    // FP64 and refined 3D plans may run stages 2-4 as one fused kernel per kx slab
+    const bool slab = rv == 2 && p.slab_ok && p.fast && p.precision != HELM_FP32;
+    // the FP64 tensor-core row kernels (FP64 plans; refined plans with variant 2, 3)
+    const bool rows64 = p.precision == HELM_FP64 || slab || rv == 3;
     // 2. y: complex-to-complex along the middle axis
     if (p.dim == 3 && !slab &&
-        (st = fft_pass(p, p.Ny, FFT_C2C, -1, p.d_spec, p.d_spec, N, N, (long long)p.Ny * N, (long long)p.Ny * N, N,
+        (st = fft_pass(p, p.Ny, FFT_C2C, -1, spec, spec, N, N, (long long)p.Ny * N, (long long)p.Ny * N, N,
                        p.Ns * nkx, 1.0, p.d_tw_y, nullptr, nullptr, false, false, 1, s)))
         return st;
     mark(2);
     // 3. per-wavenumber collocation solves + interface sweep + combination
     RowArgs r{};
-    r.spec = p.d_spec;
+    r.spec = spec;
     r.elem_stride = p.elem_spec;
     r.P = N;
     r.n = p.n;
@@ -732,8 +834,8 @@ static int run_pipeline(Plan& p, const void* in, const double* gl, const double*
     int e;
     if (p.fd) {
         ThomasArgs ta{};
-        ta.spec = p.d_spec;
-        ta.cprime = p.d_cprime;
+        ta.spec = spec;
+        ta.cprime = cprime;
         ta.nrows = p.nrows;
         ta.Ny = p.Ny;
         ta.Nz = N;
@@ -749,7 +851,7 @@ static int run_pipeline(Plan& p, const void* in, const double* gl, const double*
         e = launch_thomas(prec, ta, s);
     } else if (p.fast) {
         FdmArgs fa{};
-        fa.spec = p.d_spec;
+        fa.spec = spec;
         fa.P = N;
         fa.n = p.n;
         fa.m = p.fm;
@@ -761,7 +863,7 @@ static int run_pipeline(Plan& p, const void* in, const double* gl, const double*
         fa.row_grp = p.d_row_grp;
         fa.mats = adjoint ? p.d_fmats_adj : p.d_fmats;
         fa.d2f = adjoint ? p.d_fd2_adj : p.d_fd2;
-        fa.recip = p.d_frecip;
+        fa.recip = rows64 ? (const void*)p.d_frecip64 : p.d_frecip;
         fa.sigma = p.d_sigma;
         fa.sweeps = p.sweeps;
         fa.e0f = adjoint ? p.d_fc0 : p.d_fe0;
@@ -783,12 +885,12 @@ static int run_pipeline(Plan& p, const void* in, const double* gl, const double*
         fa.tc_m = adjoint ? p.d_ftcm_adj : p.d_ftcm;
         if (slab)
             e = launch_slab(fa, p.Ny, (N + 1) / 2, ((N + 1) / 2) | 1, p.d_tw_y, p.d_grp_of_row, nkx, s);
-        else if (prec == 0 && fa.mma_mats)
-            e = launch_fdm_mma(fa, s, p.row_var);
-        else if (prec == 2 && fa.tc_mats && p.sweeps == 1 && p.row_var == 0)
+        else if (rows64 && fa.mma_mats)
+            e = launch_fdm_mma(fa, s, rv == 3 ? 0 : rv & 1);
+        else if (prec == 2 && fa.tc_mats && p.sweeps == 1 && rv == 0)
             e = launch_fdm_tc_refine(fa, s);
         else
-            e = launch_fdm_fast(prec, fa, s, p.row_var);
+            e = launch_fdm_fast(prec, fa, s, rv & 1);
     } else {
         e = launch_rows(p.method, prec, r, s);
     }
@@ -796,35 +898,64 @@ static int run_pipeline(Plan& p, const void* in, const double* gl, const double*
     mark(3);
     // 4. inverse y
     if (p.dim == 3 && !slab &&
-        (st = fft_pass(p, p.Ny, FFT_C2C, 1, p.d_spec, p.d_spec, N, N, (long long)p.Ny * N, (long long)p.Ny * N, N,
+        (st = fft_pass(p, p.Ny, FFT_C2C, 1, spec, spec, N, N, (long long)p.Ny * N, (long long)p.Ny * N, N,
                        p.Ns * nkx, 1.0, p.d_tw_y, nullptr, nullptr, false, false, 2, s)))
         return st;
     mark(4);
     // 5. x: complex-to-real, scaled by 1/(Nx Ny) (the reference's /Nx, /Ny)
     const double scale = 1.0 / ((double)p.Nx * (p.dim == 3 ? p.Ny : 1));
-    if ((st = fft_pass(p, p.Nx, FFT_C2R, 1, p.d_spec, out, cols, p.x_stride, p.elem_spec, p.elem_stride, (int)cols,
+    if ((st = fft_pass(p, p.Nx, FFT_C2R, 1, spec, out, cols, p.x_stride, p.elem_spec, p.elem_stride, (int)cols,
                        p.Ns * p.batch, scale, p.d_tw_x, nullptr, nullptr, false, adjoint, 3, s, adj)))
         return st;
     mark(5);
     return HELM_OK;
 }
 
-// Autotuner: times every launch variant of the four FFT stages on this plan's
-// own shape (CUDA events around each stage of whole solves on zero input) and
-// keeps the fastest per stage.  Results are cached per shape for the process;
-// HELM_AUTOTUNE=0 in the environment keeps the default variants.
+// Autotuner, at plan creation, on the plan's own shape (zero input, CUDA
+// events around each stage of whole solves):
+//   1. the FFT launch variants 0..7 (and 8..15, the 512-thread CTAs, when a pass
+//      is 512 or 1024 long), with the row variant held at its default, the
+//      fastest kept per FFT stage;
+//   2. with those FFT variants, each row variant of the plan's precision
+//      (refined plans: the FP32 tensor-core kernels and the FP64 tensor-core
+//      kernel), the fastest row stage kept;
+//   3. whole solves of the fused alternatives (the slab kernel, the eigen-basis
+//      pipeline) against the result of 1 and 2, the fastest kept.
+// Results are cached per shape for the process; HELM_AUTOTUNE=0 in the
+// environment keeps the default variants.
 static std::mutex g_tune_mutex;
 static std::map<std::string, std::array<int, 5>> g_tune_cache;  // 4 FFT variants, row variant
+
+// Mean event times of the five stages over `reps` solves after one warm-up.
+static bool time_stages(Plan& p, const void* f, void* u, int reps, float (&ms)[5])
+{
+    for (float& t : ms) t = 0.f;
+    for (int rep = 0; rep <= reps; ++rep) {
+        if (solve(p, f, nullptr, nullptr, u, 0)) return false;
+        if (cudaEventSynchronize(p.ev[5]) != cudaSuccess) return false;
+        if (rep == 0) continue;
+        for (int i = 0; i < 5; ++i) {
+            float t = 0;
+            cudaEventElapsedTime(&t, p.ev[i], p.ev[i + 1]);
+            ms[i] += t / reps;
+        }
+    }
+    return true;
+}
 
 static int autotune(Plan& p)
 {
     const char* env = std::getenv("HELM_AUTOTUNE");
-    if (env && env[0] == '0') return HELM_OK;
+    if (env && env[0] == '0') {
+        if (p.eig_ok) p.row_var = 4;
+        return HELM_OK;
+    }
     const std::string key = std::string(p.fd ? "fd:" : "gll:") + std::to_string(p.dim) + ":" + std::to_string(p.Nx) +
                             ":" + std::to_string(p.Ny) + ":" +
                             std::to_string(p.N) + ":" + std::to_string(p.Ns) + ":" + std::to_string(p.precision) +
                             ":" + std::to_string(p.io_bytes) + ":" + std::to_string(p.x_stride) + ":" +
-                            std::to_string(p.batch);
+                            std::to_string(p.batch) + ":" + std::to_string(p.periodic) + ":" +
+                            std::to_string(p.eig_ok) + ":" + std::to_string(p.sweeps);
     {
         std::lock_guard<std::mutex> lock(g_tune_mutex);
         auto it = g_tune_cache.find(key);
@@ -840,6 +971,7 @@ static int autotune(Plan& p)
     if (cudaMalloc(&f, bytes) != cudaSuccess || cudaMalloc(&u, bytes) != cudaSuccess) {
         cudaGetLastError();
         if (f) cudaFree(f);
+        if (p.eig_ok) p.row_var = 4;
         return HELM_OK;  // keep the defaults
     }
     cudaMemset(f, 0, bytes);
@@ -847,55 +979,64 @@ static int autotune(Plan& p)
     if (!p.ev[0])
         for (cudaEvent_t& e : p.ev) cudaEventCreate(&e);
     p.stage_timing = true;
-    // stages: x, y, rows, inverse y, inverse x (event intervals 0..4); the
-    // FFT stages try variants 0..7 (and 8..15, the 512-thread CTAs, when a pass is
-    // 512 or 1024 long), the row stage its variants 0..1
+    // 1. FFT variants, row variant 0
     float best[5] = {1e30f, 1e30f, 1e30f, 1e30f, 1e30f};
     int pick[5] = {0, 0, 0, 0, 0};
     const int nvar = (p.Nx >= 512 || (p.dim == 3 && p.Ny >= 512)) ? 16 : 8;
+    p.row_var = 0;
+    float ms[5];
     for (int v = 0; v < nvar; ++v) {
         for (int i = 0; i < 4; ++i) p.fft_var[i] = v;
-        p.row_var = v & 1;
-        float acc[5] = {0, 0, 0, 0, 0};
-        bool ok = true;
-        for (int rep = 0; rep < 4 && ok; ++rep) {
-            if (solve(p, f, nullptr, nullptr, u, 0)) { ok = false; break; }
-            cudaEventSynchronize(p.ev[5]);
-            if (rep == 0) continue;  // warm-up
-            for (int i = 0; i < 5; ++i) {
-                float t = 0;
-                cudaEventElapsedTime(&t, p.ev[i], p.ev[i + 1]);
-                acc[i] += t;
-            }
-        }
-        if (!ok) { cudaGetLastError(); continue; }
+        if (!time_stages(p, f, u, 3, ms)) { cudaGetLastError(); continue; }
         for (int i = 0; i < 5; ++i)
-            if (acc[i] < best[i]) { best[i] = acc[i]; pick[i] = (i == 2) ? (v & 1) : v; }
+            if (i != 2 && ms[i] < best[i]) { best[i] = ms[i]; pick[i] = v; }
     }
     cudaGetLastError();
-    p.stage_timing = had;
     const int stage_of_fft[4] = {0, 1, 3, 4};
     for (int i = 0; i < 4; ++i) p.fft_var[i] = pick[stage_of_fft[i]];
-    p.row_var = p.fast ? pick[2] : 0;
-    if (p.slab_ok) {
-        // the fused slab kernel (row variant 2) against the separate passes, whole solves
-        float tot[2] = {0.f, 0.f};
-        const int rv[2] = {p.row_var, 2};
+    // 2. row variants with the chosen FFT variants
+    std::vector<int> rows_cand;
+    if (p.fast) {
+        rows_cand = {0, 1};
+        if (p.precision == HELM_FP32_REFINE && p.d_fmma) rows_cand.push_back(3);
+    } else {
+        rows_cand = {0};
+    }
+    float best_rows = 1e30f;
+    int best_rv = 0;
+    for (int rv : rows_cand) {
+        p.row_var = rv;
+        if (!time_stages(p, f, u, 3, ms)) { cudaGetLastError(); continue; }
+        if (ms[2] < best_rows) { best_rows = ms[2]; best_rv = rv; }
+    }
+    cudaGetLastError();
+    p.row_var = best_rv;
+    // 3. fused alternatives, whole solves
+    std::vector<int> whole = {p.row_var};
+    if (p.slab_ok) whole.push_back(2);
+    if (p.eig_ok) whole.push_back(4);
+    if (whole.size() > 1) {
+        std::vector<float> tot(whole.size(), 0.f);
         bool ok = true;
-        for (int rep = 0; rep < 5 && ok; ++rep)
-            for (int k = 0; k < 2 && ok; ++k) {
-                p.row_var = rv[k];
-                p.stage_timing = true;
-                if (solve(p, f, nullptr, nullptr, u, 0)) { ok = false; break; }
-                cudaEventSynchronize(p.ev[5]);
+        for (int rep = 0; rep < 6 && ok; ++rep)
+            for (size_t k = 0; k < whole.size() && ok; ++k) {
+                p.row_var = whole[k];
+                if (solve(p, f, nullptr, nullptr, u, 0) || cudaEventSynchronize(p.ev[5]) != cudaSuccess) {
+                    ok = false;
+                    break;
+                }
                 float t = 0;
                 cudaEventElapsedTime(&t, p.ev[0], p.ev[5]);
                 if (rep > 0) tot[k] += t;
             }
-        p.stage_timing = had;
         cudaGetLastError();
-        p.row_var = (ok && tot[1] < tot[0]) ? 2 : rv[0];
+        size_t bk = 0;
+        if (ok)
+            for (size_t k = 1; k < whole.size(); ++k)
+                if (tot[k] < tot[bk]) bk = k;
+        p.row_var = whole[bk];
     }
+    p.stage_timing = had;
     cudaFree(f);
     cudaFree(u);
     std::lock_guard<std::mutex> lock(g_tune_mutex);
@@ -903,9 +1044,25 @@ static int autotune(Plan& p)
     return HELM_OK;
 }
 
-int solve(Plan& p, const void* f, const double* gl, const double* gr, void* u, cudaStream_t s)
+int solve(Plan& p, const void* f, const double* gl, const double* gr, void* u, cudaStream_t s, const Workspace* ws)
 {
-    return run_pipeline(p, f, gl, gr, u, false, s);
+    return run_pipeline(p, f, gl, gr, u, false, s, nullptr, ws);
+}
+
+size_t spec_bytes(const Plan& p) { return p.spec_bytes; }
+size_t cprime_bytes(const Plan& p) { return p.d_cprime ? p.cprime_bytes : 0; }
+
+int check_solve_args(const Plan& p, const void* f, const double* gl, const double* gr, const void* u)
+{
+    if (!f || !u) {
+        g_last_error = "f and u must be device pointers";
+        return HELM_ERR_INVALID;
+    }
+    if (p.periodic && (gl || gr)) {
+        g_last_error = "a plan periodic in the GLL direction takes no boundary data";
+        return HELM_ERR_INVALID;
+    }
+    return HELM_OK;
 }
 
 int solve_adjoint(Plan& p, const double* ubar, double* fbar, double* glbar, double* grbar, const double* u,
@@ -1062,8 +1219,11 @@ static int create_fd_plan(int Nx, int Ny, int Nz, double xl, double xr, double y
     p->nrows = (long long)nkx * Ny;
     p->elem_spec = p->nrows * Nz;
     const bool td = p->precision != HELM_FP32;
-    int st = p->alloc(&p->d_spec, (size_t)p->elem_spec * (td ? 16 : 8));
-    if (!st) st = p->alloc(&p->d_cprime, (size_t)p->elem_spec * (td ? 8 : 4));
+    p->spec_bytes = (size_t)p->elem_spec * (td ? 16 : 8);
+    int st = p->alloc(&p->d_spec, p->spec_bytes);
+    // elimination scratch of the thread-per-row tridiagonal kernel (Nz > 512 only)
+    p->cprime_bytes = (size_t)p->elem_spec * (td ? 8 : 4);
+    if (!st && Nz > 512) st = p->alloc(&p->d_cprime, p->cprime_bytes);
     if (!st) st = p->upload((void**)&p->d_mx, mx.data(), mx.size() * sizeof(double));
     if (!st) st = p->upload((void**)&p->d_my, my.data(), my.size() * sizeof(double));
     auto up_tw = [&](int L, void** d) -> int {
@@ -1260,12 +1420,9 @@ int helm_plan_set_refine_sweeps(helm_plan_t plan, int sweeps)
 
 int helm_solve(helm_plan_t plan, const void* f, const double* gl, const double* gr, void* u, void* stream)
 {
-    if (!plan || !f || !u) return HELM_ERR_INVALID;
+    if (!plan) return HELM_ERR_INVALID;
     Plan& p = *reinterpret_cast<Plan*>(plan);
-    if (p.periodic && (gl || gr)) {
-        helm::set_last_error("a plan periodic in the GLL direction takes no boundary data");
-        return HELM_ERR_INVALID;
-    }
+    if (int st = helm::check_solve_args(p, f, gl, gr, u)) return st;
     int cur = 0;
     cudaGetDevice(&cur);
     if (cur != p.device) cudaSetDevice(p.device);
@@ -1394,17 +1551,62 @@ int helm_plan_get_launch_variants(helm_plan_t plan, int* fft4, int* rows)
 
 int helm_plan_set_launch_variants(helm_plan_t plan, const int* fft4, int rows)
 {
-    if (!plan || !fft4 || rows < 0 || rows > 2) return HELM_ERR_INVALID;
+    if (!plan || !fft4 || rows < 0 || rows > 4) return HELM_ERR_INVALID;
     for (int i = 0; i < 4; ++i)
         if (fft4[i] < 0 || fft4[i] > 15) return HELM_ERR_INVALID;
     Plan& p = *reinterpret_cast<Plan*>(plan);
     if (rows == 2 && !p.slab_ok) {
-        helm::set_last_error("the fused slab kernel needs an FP64 3D plan with one element, at most 65 points, Ny in {64, 128, 256}");
+        helm::set_last_error("the fused slab kernel needs an FP64 or refined 3D plan with one element, at most 65 points, Ny in {64, 128, 256}");
+        return HELM_ERR_UNSUPPORTED;
+    }
+    if (rows == 3 && (p.precision != HELM_FP32_REFINE || !p.d_fmma)) {
+        helm::set_last_error("row variant 3 (FP64 tensor-core rows) is for refined plans with one element");
+        return HELM_ERR_UNSUPPORTED;
+    }
+    if (rows == 4 && !p.eig_ok) {
+        helm::set_last_error("the eigen-basis pipeline needs an FP64 or refined plan with one element, Dirichlet ends, "
+                             "at most 66 points, Nx in {8..256} and Ny in {4..512}");
         return HELM_ERR_UNSUPPORTED;
     }
     for (int i = 0; i < 4; ++i) p.fft_var[i] = fft4[i];
     p.row_var = rows;
     return HELM_OK;
+}
+
+int helm_debug_fail_alloc(long long n)
+{
+    helm::g_alloc_fault.store(n < 0 ? -1 : n);
+    return HELM_OK;
+}
+
+const char* helm_plan_kernels(helm_plan_t plan)
+{
+    if (!plan) return "";
+    Plan& p = *reinterpret_cast<Plan*>(plan);
+    int rv = p.row_var;
+    if (rv == 4 && !p.eig_ok) rv = p.precision == HELM_FP64 ? 0 : 3;
+    if (rv == 3 && (p.precision != HELM_FP32_REFINE || !p.d_fmma)) rv = 0;
+    std::string k;
+    if (rv == 4) {
+        k = p.dim == 3 ? "eig_fwd_kernel eig_conv_kernel eig_inv_kernel" : "eig_solve2d_kernel";
+    } else {
+        const bool slab = rv == 2 && p.slab_ok && p.fast && p.precision != HELM_FP32;
+        std::string rows;
+        if (p.fd) rows = p.N <= 512 ? "thomas_warp_kernel" : "thomas_kernel";
+        else if (!p.fast) rows = "rows_kernel";
+        else if (slab) rows = "slab_kernel";
+        else if ((p.precision == HELM_FP64 || rv == 3) && p.d_fmma) rows = (rv == 3 || rv == 0) ? "fdm_mma16_kernel" : "fdm_mma_kernel";
+        else if (p.precision == HELM_FP32_REFINE && p.d_ftc && p.sweeps == 1 && rv == 0) rows = "fdm_tc_refine_kernel";
+        else rows = "fdm_fast_kernel";
+        const std::string fft = p.fft_var[0] & 4 ? "fft_pipe_kernel" : "fft_kernel";
+        k = fft + "(x)";
+        if (p.dim == 3 && !slab) k += " fft_kernel(y)";
+        k += " " + rows;
+        if (p.dim == 3 && !slab) k += " fft_kernel(y-inv)";
+        k += std::string(" ") + (p.fft_var[3] & 4 ? "fft_pipe_kernel" : "fft_kernel") + "(x-inv)";
+    }
+    p.kernel_names = k;
+    return p.kernel_names.c_str();
 }
 
 int helm_plan_destroy(helm_plan_t plan)

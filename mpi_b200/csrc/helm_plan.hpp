@@ -2,6 +2,7 @@
 #pragma once
 #include <cuda_runtime.h>
 #include <cstdint>
+#include <string>
 #include <vector>
 
 #include "../../include/helm_b200.h"
@@ -33,6 +34,7 @@ struct Plan {
 
     // device memory
     void* d_spec = nullptr;
+    size_t spec_bytes = 0, cprime_bytes = 0;
     void* d_tw_x = nullptr;
     void* d_tw_y = nullptr;
     int* d_grp_start = nullptr;
@@ -97,11 +99,21 @@ struct Plan {
     void* d_cprime = nullptr;
     // autotuned launch shapes of the four FFT stages (x, y, inverse y, inverse x)
     int fft_var[4] = {0, 0, 0, 0};
-    int row_var = 0;  // launch variant of the folded row kernel; 2: fused y-FFT / rows / inverse y (slab)
+    // row-solve variant: 0, 1 launch shapes of the plan precision's folded kernel;
+    // 2 fused y-FFT / rows / inverse y (slab, FP64 arithmetic); 3 refined plans:
+    // the FP64 tensor-core row kernel; 4 the eigen-basis pipeline (whole solve)
+    int row_var = 0;
     bool slab_ok = false;          // FP64 3D plans whose kx slab fits a two-CTA cluster
+    // eigen-basis pipeline (helm_eig.cu; row variant 4): one element, Dirichlet
+    // ends, FP64 arithmetic (FP64 and refined plans)
+    bool eig_cand = false;         // shape and boundary conditions allow it
+    bool eig_ok = false;           // its data are on the device
+    double* d_hbc = nullptr;       // [4][32] first transform of the folded boundary columns
+    double* d_frecip64 = nullptr;  // FP64 reciprocal shifts (refined plans; FP64 plans use d_frecip)
     int* d_grp_of_row = nullptr;   // shift group of each spectrum row (slab kernel)
     bool stage_timing = false;
     cudaEvent_t ev[6] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
+    std::string kernel_names;       // helm_plan_kernels
     std::vector<void*> allocations;
     long long device_bytes = 0;
 
@@ -110,7 +122,24 @@ struct Plan {
     void release();
 };
 
-int solve(Plan& p, const void* f, const double* gl, const double* gr, void* u, cudaStream_t s);
+// Scratch that one solve writes: the spectrum workspace and, for
+// finite-difference plans whose Nz exceeds the one-warp tridiagonal kernel, the
+// forward-elimination coefficients.  A solve given no workspace uses the plan's
+// own buffers; the plan itself is never modified by a solve.
+struct Workspace {
+    void* spec = nullptr;
+    void* cprime = nullptr;
+};
+
+// Bytes of spectrum and elimination scratch a solve of this plan writes.
+size_t spec_bytes(const Plan& p);
+size_t cprime_bytes(const Plan& p);
+
+// Argument checks shared by every solve entry point (status, last error set).
+int check_solve_args(const Plan& p, const void* f, const double* gl, const double* gr, const void* u);
+
+int solve(Plan& p, const void* f, const double* gl, const double* gr, void* u, cudaStream_t s,
+          const Workspace* ws = nullptr);
 
 // One size class of a batch: `lams.size()` independent 2D problems with Nx
 // Fourier modes and N GLL points on one domain, homogeneous Dirichlet in y,

@@ -242,6 +242,10 @@ class _PlanBase:
         f4 = (ctypes.c_int * 4)(*fft)
         L.check(self._lib.helm_plan_set_launch_variants(self._plan, f4, int(rows)), "helm_plan_set_launch_variants")
 
+    def kernels(self) -> str:
+        """Names of the kernels a forward solve launches, in launch order."""
+        return self._lib.helm_plan_kernels(self._plan).decode()
+
     def DestroyPDEPlan(self) -> None:
         if self._plan.value:
             self._lib.helm_plan_destroy(self._plan)

@@ -34,12 +34,18 @@ _ref3d = None
 _refp = {}
 
 
+def reference_root() -> str:
+    """The reference checkout: $REF_ROOT, else a sibling of this repository
+    (``<repo>/../reference``)."""
+    return os.environ.get("REF_ROOT", os.path.abspath(os.path.join(_HERE, "..", "..", "reference")))
+
+
 def build(quiet: bool = True) -> None:
     """Compile the C restatement (and the reference wrappers when the reference
     sources are present on this machine)."""
     out = subprocess.DEVNULL if quiet else None
     subprocess.run(["make", "-s", "-C", _HERE], check=True, stdout=out)
-    ref_root = os.environ.get("REF_ROOT", "/root/reference")
+    ref_root = reference_root()
     if os.path.isdir(os.path.join(ref_root, "HelmholtzSolvers", "DirectPseudoSpectral")):
         subprocess.run(["make", "-s", "-C", _HERE, "ref", f"REF_ROOT={ref_root}"], check=True, stdout=out)
 
