@@ -101,6 +101,59 @@ int helm2d_periodic_plan_create(int Nx, int Ny, int N, double xl, double xr, dou
 int helm3d_periodic_plan_create(int Nx, int Ny, int Nz, int N, double xl, double xr, double yl, double yr,
                                 double zl, double zr, double lambda, int precision, int method, helm_plan_t* plan);
 
+/* User operator of a wavenumber pair, the replacement of the reference's
+ * ConstructOperator callback (SolvePDE(FieldVariable U[], void
+ * (*ConstructOperator)(const int)), NonPeriodic2D_MPI.h:37; (const int, const
+ * int) in NonPeriodic3D_MPI.h:37; the periodic twins Periodic2D_MPI.h:35,
+ * Periodic3D_MPI.h:35).  The reference calls it once per |iw| (2D) or per
+ * (|iw|, |jw|) pair (3D) inside every SolvePDE (NonPeriodic2D_MPI.cpp:239-241,
+ * NonPeriodic3D_MPI.cpp:248-253), and the callback fills the interior operator
+ * Operator[N-2][N-2] (TestNonPeriodic2D_MPI.cpp:67-74).  Here the callback
+ * writes that n x n operator (n = N - 2 interior GLL points) row-major into
+ * `op` with leading dimension `ld`, for iw = 0 .. Nx/2 and (3D) jw = 0 .. Ny/2
+ * (2D: jw = 0); `user` is passed through.  The operator of -iw (and -jw) is
+ * taken to be the same, as the reference's loop over |iw| assumes. */
+typedef void (*helm_operator_fn)(int iw, int jw, double* op, int ld, void* user);
+
+/* Replaces the plan's shifted operators D2int - sigma I by the callback's, one
+ * per wavenumber pair: the callback runs now, once per pair, on the calling
+ * thread (serially), each operator is LU-factored in FP64 with the
+ * reference's scaled partial pivoting, and later solves use those factors
+ * (the LU method; the boundary columns, interface sweep and Robin rows stay
+ * the GLL ones).  Rebuilds the plan in place: its handle, layout, I/O width
+ * and refinement count are kept, the launch variants are re-tuned.  FP64 and
+ * FP32 plans (refined plans have no residual for a foreign operator:
+ * HELM_ERR_UNSUPPORTED), non-periodic or periodic, not finite-difference
+ * plans.  A singular operator gives HELM_ERR_SINGULAR and leaves the plan as
+ * it was.  Adjoint solves of such a plan are HELM_ERR_UNSUPPORTED. */
+int helm_plan_set_operator_callback(helm_plan_t plan, helm_operator_fn op, void* user);
+
+/* The GLL grid of one direction as the reference's CreatePDEPlan builds it
+ * (NonPeriodic2D_MPI.cpp:88-123): nodes[Ns*(N-1)+1] of Ns elements of length
+ * L/Ns placed from 0, the first-derivative matrix D[N][N] scaled by 2Ns/L
+ * (FirstDerivativeMatrix, GLLQuadrature.cpp:198-213) and D2 = D D scaled by
+ * 4Ns^2/L^2 (SecondDerivativeMatrix, GLLQuadrature.cpp:250-262).  Host only:
+ * no device, no plan.  Any pointer may be NULL. */
+int helm_gll_grid(int N, int Ns, double L, double* nodes, double* D, double* D2);
+
+/* FP64 LU with scaled partial pivoting of a dense row-major n x n matrix in
+ * place -- the pivot rule of the reference's LUDecomposition
+ * (LU_Decomposition.cpp:7-72) -- stored as P A = L U (unit L below the
+ * diagonal, U on and above it; perm[i] = the original row of position i) with
+ * the determinant (may be NULL); HELM_ERR_SINGULAR below a scaled pivot of
+ * 1e-12.  helm_lu_solve solves A x = b with those factors, b overwritten
+ * (LUSolve, LU_Decomposition.cpp:78-108).  Host only. */
+int helm_lu_factor(int n, double* A, int* perm, double* determinant);
+int helm_lu_solve(int n, const double* LU, const int* perm, double* b);
+
+/* max |a - b| over the solution points of a (single-problem) plan's arrays --
+ * every element, x row and GLL node of the plan's layout, the 3D y index
+ * included -- reduced on the device into *result (a DEVICE double, written on
+ * `stream`; a NaN anywhere gives NaN).  The device form of the reference's
+ * ComputeError (NonPeriodic2D_MPI.cpp:547-566, NonPeriodic3D_MPI.cpp:688-708),
+ * which takes a = the solution and b = the exact values. */
+int helm_max_abs_diff(helm_plan_t plan, const double* a, const double* b, double* result, void* stream);
+
 /* Second-order finite-difference variant: the 7-point stencil of the
  * reference's HypreFDM solver (HelmholtzSolvers/HypreFDM/src/Helmholtz3D_MPI.cpp:
  * CreatePDEPlan 117-269, SetA 297-410, Setb 424-466) with x and y periodic
@@ -208,11 +261,18 @@ int helm_plan_info(helm_plan_t plan, int* Ns, int* n_operators, int* method, lon
 int helm_plan_set_stage_timing(helm_plan_t plan, int enable);
 int helm_plan_stage_times(helm_plan_t plan, float* ms5);
 
+/* Device status of the plan's TMA-pipelined kernels (row variant 5): 0, or the
+ * code of the first wait on a tile copy that ran out of its iteration limit
+ * (the kernel then skipped its remaining work, so that solve's output is not
+ * valid).  Waits for the device; reset != 0 clears the word afterwards.  Plans
+ * without those kernels report 0.  No counterpart in the reference. */
+int helm_plan_device_status(helm_plan_t plan, int* code, int reset);
+
 /* Kernel launch variants of the plan: fft4[i] (0..15) for the x, y, inverse y
  * and inverse x FFT passes -- bit 0: 128-thread CTAs, bit 1: radix-8 schedule
  * (lengths 128, 256), bit 2: persistent pipelined pass, bit 3: 512-thread CTAs
  * for passes of length 512 or 1024 (ignored for shorter ones; with bit 2 the
- * tile exceeds shared memory and the solve fails with HELM_ERR_CUDA) -- and rows (0..4) for
+ * tile exceeds shared memory and the solve fails with HELM_ERR_CUDA) -- and rows (0..5) for
  * the row solve: 0, 1 the two kernel shapes of the plan's precision; 2 (FP64 and
  * refined 3D plans with one element, at most 65 GLL points and Ny in {64, 128,
  * 256}) the y pass, the row solve and the inverse y pass fused into one kernel
@@ -222,10 +282,13 @@ int helm_plan_stage_times(helm_plan_t plan, float* ms5);
  * points, Nx in {8, ..., 256}, Ny in {4, ..., 512}, powers of 2) the eigen-basis
  * pipeline of the whole forward solve -- GLL eigen-transform fused with the x
  * FFT, the y FFT, diagonal scaling and inverse y FFT in one pass, and the
- * inverse of the first pass: three kernels in 3D, one in 2D, fft4 unused
- * (adjoint solves of such a plan run variant 0, or 3 when refined).  Plan
+ * inverse of the first pass: three kernels in 3D, one in 2D, fft4 unused;
+ * adjoint solves run the transposed pipeline; 5 (3D plans that take 4) the
+ * same pipeline with two CTAs per y plane in its first and last passes, one per
+ * GLL fold (2D plans: the same as 4).  Plan
  * creation times every variant on the plan's own shape and keeps the fastest
- * (environment HELM_AUTOTUNE=0: all 0, rows 4 where it applies).  Setting them
+ * (environment HELM_AUTOTUNE=0: all 0, rows 5 in 3D and 4 in 2D where they
+ * apply).  Setting them
  * pins the choice, e.g. to reproduce a run bit for bit.  Every variant
  * computes the same solve; the last bits of the results may differ between
  * variants.  No counterpart in the reference, which has one code path. */

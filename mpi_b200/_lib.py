@@ -38,8 +38,13 @@ EXPORTS = (
     "helm_batch_solve", "helm_batch_destroy", "helm_plan_get_launch_variants", "helm_plan_set_launch_variants",
     "helm2d_periodic_plan_create", "helm3d_periodic_plan_create", "helm_gll_derivative", "helm_fourier_derivative",
     "helm_write_tecplot", "helm_write_vtk", "helm_solve_adjoint_misfit", "helm_solve_static_scratch",
-    "helm_plan_kernels", "helm_debug_fail_alloc",
+    "helm_plan_kernels", "helm_debug_fail_alloc", "helm_plan_device_status", "helm_plan_set_operator_callback",
+    "helm_gll_grid", "helm_lu_factor", "helm_lu_solve", "helm_max_abs_diff",
 )
+
+# operator callback of helm_plan_set_operator_callback: void op(int iw, int jw, double* op, int ld, void* user)
+OPERATOR_FN = ctypes.CFUNCTYPE(None, ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_double), ctypes.c_int,
+                               ctypes.c_void_p)
 
 # exact-solution callback of helm_write_tecplot: double exact(double x, double y, double z)
 EXACT_FN = ctypes.CFUNCTYPE(ctypes.c_double, ctypes.c_double, ctypes.c_double, ctypes.c_double)
@@ -92,6 +97,12 @@ def lib() -> ctypes.CDLL:
     L.helm_plan_destroy.argtypes = [vp]
     L.helm_plan_set_stage_timing.argtypes = [vp, i]
     L.helm_plan_stage_times.argtypes = [vp, P(ctypes.c_float)]
+    L.helm_plan_device_status.argtypes = [vp, P(ctypes.c_int), ctypes.c_int]
+    L.helm_plan_set_operator_callback.argtypes = [vp, OPERATOR_FN, vp]
+    L.helm_gll_grid.argtypes = [i, i, d, vp, vp, vp]
+    L.helm_lu_factor.argtypes = [i, vp, vp, vp]
+    L.helm_lu_solve.argtypes = [i, vp, vp, vp]
+    L.helm_max_abs_diff.argtypes = [vp, vp, vp, vp, vp]
     L.helm2d_batch_create.argtypes = [i, P(i), P(i), P(d), d, d, d, d, i, P(vp)]
     L.helm_batch_offsets.argtypes = [vp, P(ll), P(ll)]
     L.helm_batch_info.argtypes = [vp, P(i), P(i), P(ll)]

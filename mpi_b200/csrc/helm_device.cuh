@@ -150,11 +150,21 @@ __device__ __forceinline__ void slab_from_smem(const cplx_t<double>* sm, int hs,
     }
 }
 
+// Barrier of the threads that share a slab FFT: the whole CTA (BAR = 0), or
+// named barrier BAR of the first THREADS threads (warp-specialised kernels
+// whose other warps do not take part).
+template <int BAR, int THREADS>
+__device__ __forceinline__ void slab_sync()
+{
+    if constexpr (BAR == 0) __syncthreads();
+    else asm volatile("bar.sync %0, %1;\n" ::"n"(BAR), "n"(THREADS) : "memory");
+}
+
 // One length-L FFT (direction DIR, unscaled) of each of the ncol columns of the
-// [L][hs] complex array sm in shared memory, in place; all THREADS threads of
-// the CTA call it (it synchronises the CTA).  tw: the length-L twiddle table
-// exp(-2 pi i e / L).
-template <int L, int DIR, int THREADS>
+// [L][hs] complex array sm in shared memory, in place; threads 0 .. THREADS-1
+// call it (it synchronises them through slab_sync<BAR, THREADS>).  tw: the
+// length-L twiddle table exp(-2 pi i e / L).
+template <int L, int DIR, int THREADS, int BAR = 0>
 __device__ __forceinline__ void slab_fft(cplx_t<double>* sm, int hs, int ncol, const cplx_t<double>* tw)
 {
     using C = cplx_t<double>;
@@ -170,20 +180,20 @@ __device__ __forceinline__ void slab_fft(cplx_t<double>* sm, int hs, int ncol, c
         for (int r = 0; r < R0; ++r) v[r] = on ? sm[(tc + r * TPC) * hs + col] : mk(0.0, 0.0);
         dft_reg<R0, DIR, double>(v);
         if constexpr (NP >= 2) {
-            __syncthreads();
+            slab_sync<BAR, THREADS>();
             if (on) slab_to_smem<L, R0, 1, TPC, R0>(sm, hs, tc, col, v);
-            __syncthreads();
+            slab_sync<BAR, THREADS>();
             if (on) slab_from_smem<L, R1, R0, DIR, TPC, R0>(sm, hs, tw, tc, col, v);
         }
         if constexpr (NP >= 3) {
-            __syncthreads();
+            slab_sync<BAR, THREADS>();
             if (on) slab_to_smem<L, R1, R0, TPC, R0>(sm, hs, tc, col, v);
-            __syncthreads();
+            slab_sync<BAR, THREADS>();
             if (on) slab_from_smem<L, R2, R0 * R1, DIR, TPC, R0>(sm, hs, tw, tc, col, v);
         }
-        __syncthreads();
+        slab_sync<BAR, THREADS>();
         if (on) slab_to_smem<L, RL, L / RL, TPC, R0>(sm, hs, tc, col, v);
-        __syncthreads();
+        slab_sync<BAR, THREADS>();
     }
 }
 

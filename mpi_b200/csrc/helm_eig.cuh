@@ -40,7 +40,18 @@ struct EigArgs {
     double* gbar_r;
     const double* lam_u;
     double* lam_out;
+    // 3D: the persistent TMA-pipelined passes (row variant 5), with one CTA
+    // per SM (nsm), nkx = Nx / 2 + 1 spectrum rows along x, and a device
+    // status word that a wait which ran out sets (NULL: not recorded)
+    int tma;
+    int nsm;
+    int nkx;
+    int* err;
 };
+
+// Whether the TMA-pipelined passes take these arrays: f (and u_obs, when
+// given) start on a 16-byte boundary and their x rows keep that alignment.
+bool eig_tma_ok(const EigArgs& a);
 
 // Whether the pipeline covers a plan of this shape (FP64 arithmetic).
 bool eig_shape_ok(int dim, int Nx, int Ny, int P);

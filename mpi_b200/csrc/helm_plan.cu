@@ -108,7 +108,8 @@ static void build_groups(Plan& p)
 {
     const int nkx = p.Nx / 2 + 1;
     const int Nyf = p.dim == 3 ? p.Ny : 1;
-    const bool merge = (p.dim == 3) && (p.Lx == p.Ly);  // sigma depends on kx^2+ky^2 only
+    // sigma depends on kx^2+ky^2 only; a user operator may tell (kx, ky) pairs apart
+    const bool merge = (p.dim == 3) && (p.Lx == p.Ly) && !p.op_cb;
     p.grp_start.assign(1, 0);
     p.grp_rows.clear();
     p.grp_iw.clear();
@@ -406,6 +407,15 @@ static int setup_fast(Plan& p, const std::vector<double>& A0, int prec_code)
                 hbc[3 * EIG_LD + i] += Vai[(size_t)i * ma + j] * fbr[ld + j];
             }
         if ((st = p.upload((void**)&p.d_hbc, hbc.data(), hbc.size() * sizeof(double)))) return st;
+        if (p.dim == 3) {
+            const int zero = 0;
+            if ((st = p.upload((void**)&p.d_status, &zero, sizeof(int)))) return st;
+            int nsm = 0;
+            if (cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, p.device) == cudaSuccess && nsm > 0)
+                p.nsm = nsm;
+            else
+                cudaGetLastError();
+        }
         p.eig_ok = true;
     }
     if ((st = p.upload((void**)&p.d_fe0, fe0.data(), fe0.size() * sizeof(double)))) return st;
@@ -441,6 +451,14 @@ static int setup_plan(Plan& p)
     }
     const int prec_code = p.precision == HELM_FP64 ? 0 : (p.precision == HELM_FP32 ? 1 : 2);
     if (p.method == HELM_METHOD_AUTO) p.method = HELM_METHOD_FDM;
+    // user operators: one LU factor per wavenumber pair, harvested here serially
+    // (the callback may use global state, as the reference's does)
+    std::vector<double> user_ops;
+    if (p.op_cb) {
+        p.method = HELM_METHOD_LU;
+        user_ops.assign((size_t)G * n * n, 0.0);
+        for (int g = 0; g < G; ++g) p.op_cb(p.grp_iw[g], p.grp_jw[g], &user_ops[(size_t)g * n * n], n, p.op_user);
+    }
     // one-element plans run the folded FDM kernel, whose half-size transforms fit
     // shared memory up to 129 points at every precision
     const int fold_ld = 32 * (((n / 2 + n % 2) + 31) / 32);
@@ -482,8 +500,12 @@ static int setup_plan(Plan& p)
             double* ul = &hom[(size_t)g * 2 * N];
             double* ur = ul + N;
             if (lu) {
-                A = A0;
-                for (int i = 0; i < n; ++i) A[i * n + i] -= sig;
+                if (p.op_cb) {
+                    A.assign(user_ops.begin() + (size_t)g * n * n, user_ops.begin() + (size_t)(g + 1) * n * n);
+                } else {
+                    A = A0;
+                    for (int i = 0; i < n; ++i) A[i * n + i] -= sig;
+                }
                 if (!lu_factor(n, A.data(), pv.data())) { bad[g] = 1; continue; }
                 // column k: U above the diagonal, L below it (the kernel masks by
                 // position), the diagonal as 1/U_kk in dinv
@@ -723,9 +745,10 @@ static int run_pipeline(Plan& p, const void* in, const double* gl, const double*
     mark(0);
     // row variant in effect: the eigen-basis pipeline covers forward solves
     int rv = p.row_var;
-    if (rv == 4 && (!p.eig_ok || (adjoint && !p.d_fmma_adj))) rv = p.precision == HELM_FP64 ? 0 : 3;
+    if (rv == 5 && p.dim != 3) rv = 4;  // 2D: one fused kernel either way
+    if ((rv == 4 || rv == 5) && (!p.eig_ok || (adjoint && !p.d_fmma_adj))) rv = p.precision == HELM_FP64 ? 0 : 3;
     if (rv == 3 && (p.precision != HELM_FP32_REFINE || !p.d_fmma)) rv = 0;
-    if (rv == 4) {
+    if (rv == 4 || rv == 5) {
         // three launches (3D) or one (2D): GLL transform + x FFT, y convolution,
         // inverse; stage events 1 and 4 bracket the middle pass
         EigArgs ea{};
@@ -759,6 +782,10 @@ static int run_pipeline(Plan& p, const void* in, const double* gl, const double*
         ea.tw_y = p.d_tw_y;
         ea.scale = 1.0 / ((double)p.Nx * (p.dim == 3 ? p.Ny : 1));
         ea.boff = p.d_boff;  // size-class plans of a batch: the packed offsets (one problem or more)
+        ea.nsm = p.nsm;
+        ea.nkx = p.Nx / 2 + 1;
+        ea.err = p.d_status;
+        ea.tma = (rv == 5 && p.dim == 3 && eig_tma_ok(ea)) ? 1 : 0;
         int e = launch_eig_pass(0, p.dim, p.Nx, ea, p.batch, s);
         if (e) return set_cuda_error((cudaError_t)e, "eigen-basis pass 1");
         mark(1);
@@ -947,7 +974,7 @@ static int autotune(Plan& p)
 {
     const char* env = std::getenv("HELM_AUTOTUNE");
     if (env && env[0] == '0') {
-        if (p.eig_ok) p.row_var = 4;
+        if (p.eig_ok) p.row_var = p.dim == 3 ? 5 : 4;
         return HELM_OK;
     }
     const std::string key = std::string(p.fd ? "fd:" : "gll:") + std::to_string(p.dim) + ":" + std::to_string(p.Nx) +
@@ -955,7 +982,8 @@ static int autotune(Plan& p)
                             std::to_string(p.N) + ":" + std::to_string(p.Ns) + ":" + std::to_string(p.precision) +
                             ":" + std::to_string(p.io_bytes) + ":" + std::to_string(p.x_stride) + ":" +
                             std::to_string(p.batch) + ":" + std::to_string(p.periodic) + ":" +
-                            std::to_string(p.eig_ok) + ":" + std::to_string(p.sweeps);
+                            std::to_string(p.eig_ok) + ":" + std::to_string(p.sweeps) + ":" +
+                            std::to_string(p.method);
     {
         std::lock_guard<std::mutex> lock(g_tune_mutex);
         auto it = g_tune_cache.find(key);
@@ -971,7 +999,7 @@ static int autotune(Plan& p)
     if (cudaMalloc(&f, bytes) != cudaSuccess || cudaMalloc(&u, bytes) != cudaSuccess) {
         cudaGetLastError();
         if (f) cudaFree(f);
-        if (p.eig_ok) p.row_var = 4;
+        if (p.eig_ok) p.row_var = p.dim == 3 ? 5 : 4;
         return HELM_OK;  // keep the defaults
     }
     cudaMemset(f, 0, bytes);
@@ -1015,6 +1043,7 @@ static int autotune(Plan& p)
     std::vector<int> whole = {p.row_var};
     if (p.slab_ok) whole.push_back(2);
     if (p.eig_ok) whole.push_back(4);
+    if (p.eig_ok && p.dim == 3) whole.push_back(5);
     if (whole.size() > 1) {
         std::vector<float> tot(whole.size(), 0.f);
         bool ok = true;
@@ -1242,7 +1271,8 @@ static int create_fd_plan(int Nx, int Ny, int Nz, double xl, double xr, double y
 
 static int create_plan(int dim, int Nx, int Ny, int Ngll_total, int N, double xl, double xr, double yl, double yr,
                        double zl, double zr, const helm_robin_t* bc, double lambda, int precision, int method,
-                       helm_plan_t* out, bool periodic = false)
+                       helm_plan_t* out, bool periodic = false, helm_operator_fn op = nullptr,
+                       void* op_user = nullptr)
 {
     if (!out) return HELM_ERR_INVALID;
     *out = nullptr;
@@ -1277,6 +1307,8 @@ static int create_plan(int dim, int Nx, int Ny, int Ngll_total, int N, double xl
     p->lambda = lambda;
     p->precision = precision;
     p->method = method;
+    p->op_cb = op;
+    p->op_user = op_user;
     const long long cols = (long long)p->Ny * N;
     p->x_stride = cols;
     p->elem_stride = (long long)Nx * cols;
@@ -1510,6 +1542,23 @@ int helm_plan_info(helm_plan_t plan, int* Ns, int* n_operators, int* method, lon
     return HELM_OK;
 }
 
+int helm_plan_device_status(helm_plan_t plan, int* code, int reset)
+{
+    if (!plan || !code) return HELM_ERR_INVALID;
+    Plan& p = *reinterpret_cast<Plan*>(plan);
+    *code = 0;
+    if (!p.d_status) return HELM_OK;
+    int cur = 0;
+    cudaGetDevice(&cur);
+    if (cur != p.device) cudaSetDevice(p.device);
+    cudaError_t e = cudaDeviceSynchronize();
+    if (e == cudaSuccess) e = cudaMemcpy(code, p.d_status, sizeof(int), cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess && reset) e = cudaMemset(p.d_status, 0, sizeof(int));
+    if (cur != p.device) cudaSetDevice(cur);
+    if (e != cudaSuccess) return helm::set_cuda_error(e, "device status");
+    return HELM_OK;
+}
+
 int helm_plan_set_stage_timing(helm_plan_t plan, int enable)
 {
     if (!plan) return HELM_ERR_INVALID;
@@ -1551,7 +1600,7 @@ int helm_plan_get_launch_variants(helm_plan_t plan, int* fft4, int* rows)
 
 int helm_plan_set_launch_variants(helm_plan_t plan, const int* fft4, int rows)
 {
-    if (!plan || !fft4 || rows < 0 || rows > 4) return HELM_ERR_INVALID;
+    if (!plan || !fft4 || rows < 0 || rows > 5) return HELM_ERR_INVALID;
     for (int i = 0; i < 4; ++i)
         if (fft4[i] < 0 || fft4[i] > 15) return HELM_ERR_INVALID;
     Plan& p = *reinterpret_cast<Plan*>(plan);
@@ -1563,7 +1612,7 @@ int helm_plan_set_launch_variants(helm_plan_t plan, const int* fft4, int rows)
         helm::set_last_error("row variant 3 (FP64 tensor-core rows) is for refined plans with one element");
         return HELM_ERR_UNSUPPORTED;
     }
-    if (rows == 4 && !p.eig_ok) {
+    if ((rows == 4 || rows == 5) && !p.eig_ok) {
         helm::set_last_error("the eigen-basis pipeline needs an FP64 or refined plan with one element, Dirichlet ends, "
                              "at most 66 points, Nx in {8..256} and Ny in {4..512}");
         return HELM_ERR_UNSUPPORTED;
@@ -1571,6 +1620,36 @@ int helm_plan_set_launch_variants(helm_plan_t plan, const int* fft4, int rows)
     for (int i = 0; i < 4; ++i) p.fft_var[i] = fft4[i];
     p.row_var = rows;
     return HELM_OK;
+}
+
+int helm_plan_set_operator_callback(helm_plan_t plan, helm_operator_fn op, void* user)
+{
+    if (!plan || !op) return HELM_ERR_INVALID;
+    Plan& p = *reinterpret_cast<Plan*>(plan);
+    if (p.fd || p.batch > 1) {
+        helm::set_last_error("operator callbacks apply to the GLL plans (not finite-difference or batch plans)");
+        return HELM_ERR_UNSUPPORTED;
+    }
+    if (p.precision == HELM_FP32_REFINE) {
+        helm::set_last_error("a refined plan has no FP64 residual for a user operator: use an FP64 or FP32 plan");
+        return HELM_ERR_UNSUPPORTED;
+    }
+    int cur = 0;
+    cudaGetDevice(&cur);
+    if (cur != p.device) cudaSetDevice(p.device);
+    helm_plan_t fresh = nullptr;
+    const int st = helm::create_plan(p.dim, p.Nx, p.Ny, p.Ns * p.N, p.N, p.xl, p.xr, p.yl, p.yr, p.zl, p.zr, &p.bc,
+                                     p.lambda, p.precision, HELM_METHOD_LU, &fresh, p.periodic, op, user);
+    if (cur != p.device) cudaSetDevice(cur);
+    if (st) return st;
+    Plan& q = *reinterpret_cast<Plan*>(fresh);
+    q.x_stride = p.x_stride;
+    q.elem_stride = p.elem_stride;
+    q.bc_x_stride = p.bc_x_stride;
+    q.io_bytes = p.io_bytes;
+    q.sweeps = p.sweeps;
+    std::swap(p, q);
+    return helm_plan_destroy(fresh);  // frees the old plan's contents
 }
 
 int helm_debug_fail_alloc(long long n)
@@ -1584,10 +1663,14 @@ const char* helm_plan_kernels(helm_plan_t plan)
     if (!plan) return "";
     Plan& p = *reinterpret_cast<Plan*>(plan);
     int rv = p.row_var;
-    if (rv == 4 && !p.eig_ok) rv = p.precision == HELM_FP64 ? 0 : 3;
+    if (rv == 5 && p.dim != 3) rv = 4;
+    if ((rv == 4 || rv == 5) && !p.eig_ok) rv = p.precision == HELM_FP64 ? 0 : 3;
     if (rv == 3 && (p.precision != HELM_FP32_REFINE || !p.d_fmma)) rv = 0;
     std::string k;
-    if (rv == 4) {
+    if (rv == 5) {
+        // (arrays whose alignment the tensor maps cannot take run variant 4's kernels)
+        k = "eig_fwd_tma_kernel eig_conv_tma_kernel eig_inv_tma_kernel";
+    } else if (rv == 4) {
         k = p.dim == 3 ? "eig_fwd_kernel eig_conv_kernel eig_inv_kernel" : "eig_solve2d_kernel";
     } else {
         const bool slab = rv == 2 && p.slab_ok && p.fast && p.precision != HELM_FP32;

@@ -18,6 +18,10 @@ struct Plan {
     double Lx = 1, Ly = 1, Lgll = 1;
     helm_robin_t bc{0.0, 1.0, 0.0, 1.0};
     bool periodic = false;       // periodic in the GLL direction (no boundary data)
+    // user operators (helm_plan_set_operator_callback): per wavenumber pair, in
+    // place of D2int - sigma I; the plan then runs the LU method
+    helm_operator_fn op_cb = nullptr;
+    void* op_user = nullptr;
     double lambda = 0;
     int precision = HELM_FP64, method = HELM_METHOD_AUTO;
     int io_bytes = 8, sweeps = 1;
@@ -101,7 +105,8 @@ struct Plan {
     int fft_var[4] = {0, 0, 0, 0};
     // row-solve variant: 0, 1 launch shapes of the plan precision's folded kernel;
     // 2 fused y-FFT / rows / inverse y (slab, FP64 arithmetic); 3 refined plans:
-    // the FP64 tensor-core row kernel; 4 the eigen-basis pipeline (whole solve)
+    // the FP64 tensor-core row kernel; 4 the eigen-basis pipeline (whole solve);
+    // 5 its 3D passes as persistent TMA-pipelined kernels
     int row_var = 0;
     bool slab_ok = false;          // FP64 3D plans whose kx slab fits a two-CTA cluster
     // eigen-basis pipeline (helm_eig.cu; row variant 4): one element, Dirichlet
@@ -111,6 +116,11 @@ struct Plan {
     double* d_hbc = nullptr;       // [4][32] first transform of the folded boundary columns
     double* d_frecip64 = nullptr;  // FP64 reciprocal shifts (refined plans; FP64 plans use d_frecip)
     int* d_grp_of_row = nullptr;   // shift group of each spectrum row (slab kernel)
+    // row variant 5 (the TMA-pipelined eigen-basis passes): the device's SM
+    // count (one persistent CTA each) and a device status word that a bounded
+    // wait which ran out sets to a nonzero code (helm_plan_device_status)
+    int nsm = 148;
+    int* d_status = nullptr;
     bool stage_timing = false;
     cudaEvent_t ev[6] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
     std::string kernel_names;       // helm_plan_kernels

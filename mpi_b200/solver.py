@@ -80,6 +80,31 @@ class _PlanBase:
     def set_refine_sweeps(self, sweeps: int) -> None:
         L.check(self._lib.helm_plan_set_refine_sweeps(self._plan, sweeps), "helm_plan_set_refine_sweeps")
 
+    def SetOperator(self, construct_operator) -> None:
+        """The reference's ConstructOperator callback (SolvePDE(U,
+        ConstructOperator), NonPeriodic2D_MPI.h:37 / NonPeriodic3D_MPI.h:37):
+        ``construct_operator(iw, jw)`` returns the (N-2) x (N-2) interior
+        operator of the wavenumber pair (|iw|, |jw|) (2D: jw = 0) as an array.
+        It is called once per pair now; later solves use those operators."""
+        import numpy as np
+
+        err = []
+
+        def cb(iw, jw, op, ld, user):
+            try:
+                a = np.asarray(construct_operator(iw, jw), dtype=np.float64)
+                n = a.shape[0]
+                dst = np.ctypeslib.as_array(op, shape=(n * ld,)).reshape(n, ld)
+                dst[:, :n] = a
+            except Exception as e:  # an exception cannot cross the C callback
+                err.append(e)
+
+        fn = L.OPERATOR_FN(cb)
+        st = self._lib.helm_plan_set_operator_callback(self._plan, fn, None)
+        if err:
+            raise err[0]
+        L.check(st, "helm_plan_set_operator_callback")
+
     def set_io_bytes(self, nbytes: int) -> None:
         L.check(self._lib.helm_plan_set_io_bytes(self._plan, nbytes), "helm_plan_set_io_bytes")
         self.io_dtype = torch.float32 if nbytes == 4 else torch.float64
@@ -241,6 +266,14 @@ class _PlanBase:
     def set_launch_variants(self, fft: Sequence[int], rows: int) -> None:
         f4 = (ctypes.c_int * 4)(*fft)
         L.check(self._lib.helm_plan_set_launch_variants(self._plan, f4, int(rows)), "helm_plan_set_launch_variants")
+
+    def device_status(self, reset: bool = True) -> int:
+        """0, or the code of a tile-copy wait of the TMA-pipelined kernels that ran
+        out of its iteration limit (waits for the device)."""
+        code = ctypes.c_int()
+        L.check(self._lib.helm_plan_device_status(self._plan, ctypes.byref(code), int(reset)),
+                "helm_plan_device_status")
+        return code.value
 
     def kernels(self) -> str:
         """Names of the kernels a forward solve launches, in launch order."""

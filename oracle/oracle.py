@@ -272,6 +272,20 @@ def ref_solve3d(f, gl, gr, *, xl, xr, yl, yr, zl, zr, lam, bc=(0.0, 1.0, 0.0, 1.
     return (out, ms[0]) if return_time else out
 
 
+def ref_set_cdiag(dim: int, c=None):
+    """Extra diagonal c_i (interior GLL nodes) that the reference drivers'
+    ConstructOperator subtracts from the stock operator; None restores it."""
+    lib_ = _ref(dim)
+    fn = lib_.oracle_ref2d_set_cdiag if dim == 2 else lib_.oracle_ref3d_set_cdiag
+    fn.restype = None
+    fn.argtypes = [_P, _I]
+    if c is None:
+        fn(None, 0)
+    else:
+        c = _c64(c)
+        fn(_p(c), int(c.size))
+
+
 def ref_psolve2d(f, *, xl, xr, yl, yr, lam, return_time=False):
     """The reference's own Periodic2D SolvePDE.  f: [Ns, Nx, N] or [Nx, N]."""
     f = _c64(f)

@@ -8,6 +8,15 @@
 // shifted-Laplacian ConstructOperator (TestNonPeriodic2D_MPI.cpp:67-74) -> read U.
 #include "NonPeriodic2D_MPI.h"
 #include <chrono>
+#include <vector>
+
+// Extra diagonal of a user operator (empty: the stock operator), set by
+// oracle_ref2d_set_cdiag: the callback below then builds
+// Dyy_int - diag(lambda + (2 pi iw / Lx)^2 + c_i), the kind of operator a
+// caller's own ConstructOperator passes (a coefficient varying along y).
+static std::vector<double> g_cdiag;
+
+extern "C" void oracle_ref2d_set_cdiag(const double* c, int n) { g_cdiag.assign(c, c + (c ? n : 0)); }
 
 // The operator the reference's tests pass to SolvePDE: Dyy on the interior
 // nodes minus (lambda + (2 pi iw / Lx)^2) on the diagonal, LU-factored in place.
@@ -16,6 +25,8 @@ static void oracle_construct_operator_2d(const int iw)
     for (int i = 0; i < N - 2; ++i)
         for (int j = 0; j < N - 2; ++j)
             Operator[i][j] = Dyy[i + 1][j + 1] - (i == j ? (Lambda + 4.0 * PI * PI * iw * iw / (Lx * Lx)) : 0.0);
+    if (!g_cdiag.empty())
+        for (int i = 0; i < N - 2; ++i) Operator[i][i] -= g_cdiag[i];
     LUDecomposition(Operator, npivot, determinant, N - 2);
 }
 

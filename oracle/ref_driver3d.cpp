@@ -6,6 +6,13 @@
 // TestNonPeriodic3D_MPI.cpp:71-79.
 #include "NonPeriodic3D_MPI.h"
 #include <chrono>
+#include <vector>
+
+// Extra diagonal of a user operator (empty: the stock operator); see
+// oracle_ref2d_set_cdiag.
+static std::vector<double> g_cdiag;
+
+extern "C" void oracle_ref3d_set_cdiag(const double* c, int n) { g_cdiag.assign(c, c + (c ? n : 0)); }
 
 static void oracle_construct_operator_3d(const int iw, const int jw)
 {
@@ -13,6 +20,8 @@ static void oracle_construct_operator_3d(const int iw, const int jw)
         for (int j = 0; j < N - 2; ++j)
             Operator[i][j] = Dzz[i + 1][j + 1] -
                 (i == j ? (Lambda + 4.0 * PI * PI * iw * iw / (Lx * Lx) + 4.0 * PI * PI * jw * jw / (Ly * Ly)) : 0.0);
+    if (!g_cdiag.empty())
+        for (int i = 0; i < N - 2; ++i) Operator[i][i] -= g_cdiag[i];
     LUDecomposition(Operator, npivot, determinant, N - 2);
 }
 

@@ -5,7 +5,7 @@ oracle/Makefile into oracle/_ref) on small seeded problems and stores inputs and
 outputs as compressed .npz files.  Needs the reference tree at build time; the
 committed .npz files are what the tests read.
 
-    python tests/golden/make_golden.py
+    python tests/golden/make_golden.py [fixture names]
 """
 import math
 import os
@@ -111,7 +111,32 @@ def main():
         fh.write(t3)
     out["writer_fields"] = dict(u2=u2, u3=u3, dom2=[0.5, 2.0, -1.0, 1.0], dom3=[0.0, 1.0, 0.5, 1.5, 0.0, 2.0])
 
+    # a caller's own operator through SolvePDE's ConstructOperator callback: the
+    # stock operator minus a coefficient c(y) varying along the GLL direction
+    # (Dyy_int - diag(lambda + k^2 + c_i)), 2D with two Robin elements, 3D with
+    # one element and Lx = Ly
+    orng = np.random.default_rng(20240605)
+    d = {}
+    Nx, N, Ns = 16, 9, 2
+    c2 = 1.0 + orng.random(N - 2)
+    f = orng.standard_normal((Ns, Nx, N)); gl = orng.standard_normal(Nx); gr = orng.standard_normal(Nx)
+    O.ref_set_cdiag(2, c2)
+    u = O.ref_solve2d(f, gl, gr, xl=0.0, xr=1.2, yl=0.0, yr=0.8, lam=1.5, bc=(1.0, 0.5, 0.7, 2.0))
+    O.ref_set_cdiag(2, None)
+    d.update(f2=f, gl2=gl, gr2=gr, u2=u, c2=c2, dom2=[0.0, 1.2, 0.0, 0.8], lam2=1.5, bc2=[1.0, 0.5, 0.7, 2.0])
+    Nx, Ny, N = 8, 8, 9
+    c3 = 2.0 * orng.random(N - 2)
+    f = orng.standard_normal((Nx, Ny, N)); gl = orng.standard_normal((Nx, Ny)); gr = orng.standard_normal((Nx, Ny))
+    O.ref_set_cdiag(3, c3)
+    u = O.ref_solve3d(f, gl, gr, xl=0.0, xr=1.0, yl=0.0, yr=1.0, zl=0.0, zr=1.5, lam=0.5)
+    O.ref_set_cdiag(3, None)
+    d.update(f3=f, gl3=gl, gr3=gr, u3=u, c3=c3, dom3=[0.0, 1.0, 0.0, 1.0, 0.0, 1.5], lam3=0.5)
+    out["user_operator"] = d
+
+    only = sys.argv[1:]  # optional: names of the fixtures to (re)write
     for name, d in out.items():
+        if only and name not in only:
+            continue
         np.savez_compressed(os.path.join(HERE, name + ".npz"), **{k: np.asarray(v) for k, v in d.items()})
         print(name, {k: np.asarray(v).shape for k, v in d.items()})
 

@@ -25,6 +25,15 @@ from tests.helpers import golden, max_rel, rel_l2
 pytestmark = pytest.mark.gpu
 
 BC_DIR = (0.0, 0.5, 0.0, 2.0)  # Dirichlet ends with beta_l = 0.5, beta_r = 2
+# 3D row variants of the pipeline: 4 = one CTA per y plane and pass, 5 = the
+# persistent TMA-pipelined passes (one CTA per SM, a producer warp moving tiles)
+KERNELS3 = {4: "eig_fwd_kernel eig_conv_kernel eig_inv_kernel",
+            5: "eig_fwd_tma_kernel eig_conv_tma_kernel eig_inv_tma_kernel"}
+
+
+def _status_ok(p):
+    """No bounded wait of the TMA kernels ran out (device status word 0)."""
+    assert p.device_status() == 0
 
 
 def _dev(a):
@@ -36,18 +45,19 @@ def _pin(p, rows):
     assert p.launch_variants()["rows"] == rows
 
 
+@pytest.mark.parametrize("rv", [4, 5])
 @pytest.mark.parametrize("precision", ["fp64", "fp32_refine"])
 @pytest.mark.parametrize("Nx,Ny,N", [(8, 4, 5), (16, 8, 9), (32, 16, 17), (64, 32, 33), (128, 64, 65),
-                                     (32, 512, 9), (256, 16, 66), (16, 128, 40)])
-def test_eig_3d_vs_oracle(cuda, Nx, Ny, N, precision):
+                                     (32, 512, 9), (256, 16, 66), (16, 128, 40), (256, 8, 64)])
+def test_eig_3d_vs_oracle(cuda, Nx, Ny, N, precision, rv):
     rng = np.random.default_rng(Nx * 1000 + Ny + N)
     f = rng.standard_normal((Nx, Ny, N))
     gl, gr = rng.standard_normal((Nx, Ny)), rng.standard_normal((Nx, Ny))
     lam = 3.0
     ref = O.solve3d(f, gl, gr, Lx=1.3, Ly=0.7, Lz=0.9, lam=lam, bc=BC_DIR)
     p = NonPeriodic3D(Nx, Ny, N, N, 0.0, 1.3, 0.0, 0.7, 0.0, 0.9, Lambda=lam, bc=BC_DIR, precision=precision)
-    _pin(p, 4)
-    assert p.kernels() == "eig_fwd_kernel eig_conv_kernel eig_inv_kernel"
+    _pin(p, rv)
+    assert p.kernels() == KERNELS3[rv]
     fd, gld, grd = _dev(f), _dev(gl), _dev(gr)
     for _ in range(2):  # the spectrum scratch is reused: two solves in a row
         u = p.SolvePDE(fd, gld, grd).cpu().numpy()
@@ -55,6 +65,7 @@ def test_eig_3d_vs_oracle(cuda, Nx, Ny, N, precision):
     # without boundary data: homogeneous Dirichlet rows
     ref0 = O.solve3d(f, 0 * gl, 0 * gr, Lx=1.3, Ly=0.7, Lz=0.9, lam=lam, bc=BC_DIR)
     assert max_rel(p.SolvePDE(fd).cpu().numpy(), ref0) < 1e-12
+    _status_ok(p)
 
 
 @pytest.mark.parametrize("precision", ["fp64", "fp32_refine"])
@@ -83,29 +94,33 @@ def test_eig_config1_golden_and_exact(cuda):
     assert np.abs(u - g["u_exact"]).max() < 1e-13
 
 
-def test_eig_golden_3d(cuda):
+@pytest.mark.parametrize("rv", [4, 5])
+def test_eig_golden_3d(cuda, rv):
     g = golden("smooth_3d")
     xl, xr, yl, yr, zl, zr = [float(v) for v in g["dom"]]
     assert float(g["bc"][0]) == 0.0 and float(g["bc"][2]) == 0.0
     p = NonPeriodic3D(16, 16, 17, 17, xl, xr, yl, yr, zl, zr, Lambda=float(g["lam"]), bc=tuple(g["bc"]))
-    _pin(p, 4)
+    _pin(p, rv)
     assert max_rel(p.SolvePDE(_dev(g["f"])).cpu().numpy(), g["u"]) < 1e-12
 
 
+@pytest.mark.parametrize("rv", [4, 5])
 @pytest.mark.parametrize("precision", ["fp64", "fp32_refine"])
-def test_eig_full_size_vs_oracle(cuda, precision):
+def test_eig_full_size_vs_oracle(cuda, precision, rv):
     """256 x 256 x 65, lambda 10 (the headline workload) with the pipeline pinned."""
     Nx, N = 256, 65
     f = W.smooth_field_3d(Nx, Nx, N, seed=1236)
     z = np.zeros((Nx, Nx))
     ref = O.solve3d(f, z, z, Lx=2 * math.pi, Ly=2 * math.pi, Lz=2.0, lam=10.0)
     p = NonPeriodic3D(Nx, Nx, N, N, 0.0, 2 * math.pi, 0.0, 2 * math.pi, 0.0, 2.0, Lambda=10.0, precision=precision)
-    _pin(p, 4)
+    _pin(p, rv)
     u = p.SolvePDE(_dev(f)).cpu().numpy()
     assert rel_l2(u, ref) < 1e-12
+    _status_ok(p)
 
 
-def test_eig_reference_layout(cuda):
+@pytest.mark.parametrize("rv", [4, 5])
+def test_eig_reference_layout(cuda, rv):
     """The reference's padded arrays rhsPDE[2Nx][2Ny][N], leftBC[2Nx][2Ny]:
     results in the [Nx][Ny] corner, padding untouched."""
     rng = np.random.default_rng(5)
@@ -116,7 +131,7 @@ def test_eig_reference_layout(cuda):
     GL = np.zeros((2 * Nx, 2 * Ny)); GL[:Nx, :Ny] = gl
     GR = np.zeros((2 * Nx, 2 * Ny)); GR[:Nx, :Ny] = gr
     p = NonPeriodic3D(Nx, Ny, N, N, 0.0, 1.0, 0.0, 2.0, 0.0, 1.5, Lambda=2.0, bc=BC_DIR)
-    _pin(p, 4)
+    _pin(p, rv)
     p.set_layout(x_stride=2 * Ny * N, elem_stride=2 * Nx * 2 * Ny * N, bc_x_stride=2 * Ny)
     fd, gld, grd = _dev(F), _dev(GL), _dev(GR)
     ud = torch.full((2 * Nx, 2 * Ny, N), 7.0, dtype=torch.float64, device="cuda")
@@ -133,8 +148,9 @@ def test_eig_declines_other_plans(cuda):
     """Robin ends, several elements and periodic plans have no eigen-basis
     pipeline: pinning it is an error, and the autotuned plan runs another path."""
     p = NonPeriodic3D(32, 16, 17, 17, 0.0, 1.0, 0.0, 1.0, 0.0, 1.0, Lambda=1.0, bc=(0.4, 1.0, 0.3, 2.0))
-    with pytest.raises(HelmError):
-        _pin(p, 4)
+    for rv in (4, 5):
+        with pytest.raises(HelmError):
+            _pin(p, rv)
     assert "eig" not in p.kernels()
     p = NonPeriodic3D(32, 16, 34, 17, 0.0, 1.0, 0.0, 1.0, 0.0, 1.0, Lambda=1.0)  # two elements
     with pytest.raises(HelmError):
@@ -147,11 +163,12 @@ def test_eig_declines_other_plans(cuda):
         _pin(p, 4)
 
 
-@pytest.mark.parametrize("dim,shape", [(3, (8, 4, 5)), (3, (32, 16, 17)), (3, (128, 64, 65)), (2, (64, 33)),
-                                       (2, (256, 66))])
+@pytest.mark.parametrize("dim,shape,rv", [(3, (8, 4, 5), 4), (3, (32, 16, 17), 4), (3, (128, 64, 65), 4),
+                                          (3, (8, 4, 5), 5), (3, (32, 16, 17), 5), (3, (128, 64, 65), 5),
+                                          (3, (256, 8, 66), 5), (2, (64, 33), 4), (2, (256, 66), 4)])
 @pytest.mark.parametrize("precision", ["fp64", "fp32_refine"])
-def test_eig_adjoint_matches_row_kernel_adjoint(cuda, dim, shape, precision):
-    """The transposed pipeline (row variant 4) against the transposed row-kernel
+def test_eig_adjoint_matches_row_kernel_adjoint(cuda, dim, shape, rv, precision):
+    """The transposed pipeline (row variants 4 and 5) against the transposed row-kernel
     pipeline (variant 0; checked against dense adjoint maps in
     test_adjoint_gpu.py): fbar, the boundary cotangents (beta != 1) and
     lambda_bar, plain and in the misfit form."""
@@ -166,20 +183,21 @@ def test_eig_adjoint_matches_row_kernel_adjoint(cuda, dim, shape, precision):
     ubar = _dev(rng.standard_normal(shape))
     uobs = _dev(rng.standard_normal(shape))
     out = {}
-    for rv in (0, 4):
-        _pin(p, rv)
+    for v in (0, rv):
+        _pin(p, v)
         u = p.SolvePDE(f)
         fb, lb, glb, grb = p.SolveAdjoint(ubar, u=u, want_bc=True)
         mfb, mlb, mglb, mgrb = p.SolveAdjointMisfit(u, uobs, want_bc=True)
         torch.cuda.synchronize()
-        out[rv] = [t.cpu().numpy() for t in (u, fb, lb, glb, grb, mfb, mlb, mglb, mgrb)]
+        out[v] = [t.cpu().numpy() for t in (u, fb, lb, glb, grb, mfb, mlb, mglb, mgrb)]
     names = ("u", "fbar", "lambda_bar", "glbar", "grbar", "misfit fbar", "misfit lambda_bar", "misfit glbar",
              "misfit grbar")
     tol = 1e-12 if precision == "fp64" else 1e-10
-    for nm, a, b in zip(names, out[4], out[0]):
+    for nm, a, b in zip(names, out[rv], out[0]):
         assert max_rel(a, b) < tol, (nm, max_rel(a, b))
+    _status_ok(p)
     # boundary slots of fbar are zero (f is read at interior nodes only)
-    assert np.all(out[4][1][..., 0] == 0.0) and np.all(out[4][1][..., -1] == 0.0)
+    assert np.all(out[rv][1][..., 0] == 0.0) and np.all(out[rv][1][..., -1] == 0.0)
 
 
 @pytest.mark.parametrize("N", [17, 65])
