@@ -327,13 +327,19 @@ int helm_solve_static_scratch(helm_plan_t plan, const void* f, const double* gl,
  * helm2d_plan_create with Nx[p] Fourier modes, one GLL element of N[p] points,
  * lambda[p], homogeneous Dirichlet rows in y, on the common domain
  * [xl, xr) x [yl, yr].  f and u are packed: problem p is the compact
- * [Nx[p]][N[p]] block at element offset sum_{q<p} Nx[q] N[q].  Problems of
- * one size (Nx, N) share a class whose three kernels cover them all;
- * helm_batch_solve runs every class as one CUDA graph, the class chains on
- * concurrent streams, with a single cudaGraphLaunch on `stream`.  The graph is
- * captured at the first call and again whenever f or u differ from the last
- * call's.  Calls on one batch whose kernels overlap on the GPU race on its
- * workspace: serialise them. */
+ * [Nx[p]][N[p]] block at element offset sum_{q<p} Nx[q] N[q].
+ * FP64 and refined batches whose problems all have Nx in 8 .. 512 and 4 .. 129
+ * GLL points run as ONE persistent kernel launch (after one memset of its work
+ * queue): every problem is solved in the eigen basis of its GLL operator, cut
+ * into row, column and row items that persistent CTAs take from one ordered
+ * queue (FP64 arithmetic; a refined batch computes in FP64 throughout).
+ * Other batches (FP32, or sizes outside that range) group their problems into
+ * size classes (Nx, N), three kernels per class covering all its problems.
+ * helm_batch_solve runs the solve as one CUDA graph with a single
+ * cudaGraphLaunch on `stream` (the size classes on concurrent streams inside
+ * it).  The graph is captured at the first call and again whenever f or u
+ * differ from the last call's.  Calls on one batch whose kernels overlap on the
+ * GPU race on its workspace: serialise them. */
 typedef struct helm_batch_s* helm_batch_t;
 
 int helm2d_batch_create(int nprob, const int* Nx, const int* N, const double* lambda, double xl, double xr,
@@ -343,11 +349,17 @@ int helm2d_batch_create(int nprob, const int* Nx, const int* N, const double* la
  * may be NULL) and the packed length. */
 int helm_batch_offsets(helm_batch_t batch, long long* offsets, long long* total_elems);
 
-/* Size classes, kernel launches inside one solve, device bytes held. */
+/* Distinct problem sizes (Nx, N), kernel launches inside one solve (1 for the
+ * persistent launch), device bytes held. */
 int helm_batch_info(helm_batch_t batch, int* n_classes, int* kernels_per_solve, long long* device_bytes);
 
-/* enable = 0: helm_batch_solve launches the class kernels directly on `stream`,
- * one class after another, instead of through the graph (default 1). */
+/* Status word of the persistent batch kernel: 0, or 7 when a wait of an item
+ * for the items it depends on ran out of its iteration limit (that solve's
+ * output is not valid).  Waits for the device; reset != 0 clears it. */
+int helm_batch_device_status(helm_batch_t batch, int* code, int reset);
+
+/* enable = 0: helm_batch_solve launches its kernels directly on `stream`
+ * (the classes one after another) instead of through the graph (default 1). */
 int helm_batch_set_graph(helm_batch_t batch, int enable);
 
 /* u = solution of every problem; f, u DEVICE double arrays of the packed length. */

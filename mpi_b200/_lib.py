@@ -39,7 +39,7 @@ EXPORTS = (
     "helm2d_periodic_plan_create", "helm3d_periodic_plan_create", "helm_gll_derivative", "helm_fourier_derivative",
     "helm_write_tecplot", "helm_write_vtk", "helm_solve_adjoint_misfit", "helm_solve_static_scratch",
     "helm_plan_kernels", "helm_debug_fail_alloc", "helm_plan_device_status", "helm_plan_set_operator_callback",
-    "helm_gll_grid", "helm_lu_factor", "helm_lu_solve", "helm_max_abs_diff",
+    "helm_gll_grid", "helm_lu_factor", "helm_lu_solve", "helm_max_abs_diff", "helm_batch_device_status",
 )
 
 # operator callback of helm_plan_set_operator_callback: void op(int iw, int jw, double* op, int ld, void* user)
@@ -103,6 +103,7 @@ def lib() -> ctypes.CDLL:
     L.helm_lu_factor.argtypes = [i, vp, vp, vp]
     L.helm_lu_solve.argtypes = [i, vp, vp, vp]
     L.helm_max_abs_diff.argtypes = [vp, vp, vp, vp, vp]
+    L.helm_batch_device_status.argtypes = [vp, P(ctypes.c_int), ctypes.c_int]
     L.helm2d_batch_create.argtypes = [i, P(i), P(i), P(d), d, d, d, d, i, P(vp)]
     L.helm_batch_offsets.argtypes = [vp, P(ll), P(ll)]
     L.helm_batch_info.argtypes = [vp, P(i), P(i), P(ll)]

@@ -23,12 +23,17 @@
 #include <vector>
 
 #include "../../include/helm_b200.h"
+#include "helm_batch_eig.cuh"
 #include "helm_plan.hpp"
 
 namespace helm {
 
 struct Batch {
     int nprob = 0, device = 0, precision = HELM_FP64;
+    // FP64 and refined batches within its range: one persistent launch
+    // (helm_batch_eig.cu) in place of the size classes
+    BatchEig* be = nullptr;
+    int n_sizes = 0;  // distinct (Nx, N) of the batch
     std::vector<long long> offs;  // element offset of each problem in the packed buffers
     long long total = 0;          // elements of the packed buffers
     std::vector<Plan*> classes;
@@ -45,6 +50,8 @@ struct Batch {
 
     void release()
     {
+        batch_eig_destroy(be);
+        be = nullptr;
         if (exec) cudaGraphExecDestroy(exec);
         if (graph) cudaGraphDestroy(graph);
         exec = nullptr;
@@ -76,6 +83,7 @@ static int cuda_status(cudaError_t e, const char* what)
 // and joined back into `origin`.
 static int launch_classes(Batch& b, const void* f, void* u)
 {
+    if (b.be) return batch_eig_solve(b.be, static_cast<const double*>(f), static_cast<double*>(u), b.origin);
     cudaError_t e = cudaEventRecord(b.fork, b.origin);
     if (e != cudaSuccess) return cuda_status(e, "cudaEventRecord");
     for (size_t c = 0; c < b.classes.size(); ++c) {
@@ -183,8 +191,13 @@ int helm2d_batch_create(int nprob, const int* Nx, const int* N, const double* la
         }
         members[it->second].push_back(i);
     }
+    b->n_sizes = (int)cls_key.size();
     int st = HELM_OK;
-    for (size_t c = 0; c < cls_key.size() && !st; ++c) {
+    if (precision != HELM_FP32) {
+        st = helm::batch_eig_create(nprob, Nx, N, lambda, xl, xr, yl, yr, b->offs.data(), b->device, &b->be);
+        if (st == HELM_ERR_UNSUPPORTED) st = HELM_OK;  // outside its range: the size classes below
+    }
+    for (size_t c = 0; c < cls_key.size() && !st && !b->be; ++c) {
         std::vector<double> lams;
         std::vector<long long> offs;
         for (int i : members[c]) {
@@ -237,10 +250,10 @@ int helm_batch_info(helm_batch_t batch, int* n_classes, int* kernels_per_solve, 
 {
     if (!batch) return HELM_ERR_INVALID;
     Batch* b = reinterpret_cast<Batch*>(batch);
-    if (n_classes) *n_classes = (int)b->classes.size();
-    if (kernels_per_solve) *kernels_per_solve = 3 * (int)b->classes.size();
+    if (n_classes) *n_classes = b->n_sizes;
+    if (kernels_per_solve) *kernels_per_solve = b->be ? 1 : 3 * (int)b->classes.size();
     if (device_bytes) {
-        long long s = 0;
+        long long s = b->be ? helm::batch_eig_device_bytes(b->be) : 0;
         for (const helm::Plan* p : b->classes) s += p->device_bytes;
         *device_bytes = s;
     }
@@ -267,6 +280,7 @@ int helm_batch_solve(helm_batch_t batch, const double* f, double* u, void* strea
     if (cur != b->device) cudaSetDevice(b->device);
     int st = HELM_OK;
     if (!b->use_graph) {
+        if (b->be) st = helm::batch_eig_solve(b->be, f, u, s);
         for (helm::Plan* p : b->classes)
             if ((st = helm::solve(*p, f, nullptr, nullptr, u, s))) break;
     } else {
@@ -278,6 +292,23 @@ int helm_batch_solve(helm_batch_t batch, const double* f, double* u, void* strea
     }
     if (cur != b->device) cudaSetDevice(cur);
     return st;
+}
+
+int helm_batch_device_status(helm_batch_t batch, int* code, int reset)
+{
+    if (!batch || !code) return HELM_ERR_INVALID;
+    Batch* b = reinterpret_cast<Batch*>(batch);
+    *code = 0;
+    if (!b->be) return HELM_OK;
+    int cur = 0;
+    cudaGetDevice(&cur);
+    if (cur != b->device) cudaSetDevice(b->device);
+    int* d = helm::batch_eig_status(b->be);
+    cudaError_t e = cudaDeviceSynchronize();
+    if (e == cudaSuccess) e = cudaMemcpy(code, d, sizeof(int), cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess && reset) e = cudaMemset(d, 0, sizeof(int));
+    if (cur != b->device) cudaSetDevice(cur);
+    return e == cudaSuccess ? HELM_OK : helm::cuda_status(e, "device status");
 }
 
 int helm_batch_destroy(helm_batch_t batch)

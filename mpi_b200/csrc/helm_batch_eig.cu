@@ -1,0 +1,544 @@
+// Batches of independent 2D problems (helm2d_batch_*) in one persistent
+// launch, FP64, sm_100a.
+//
+// Each problem (Nx Fourier modes, P GLL points, its own lambda, homogeneous
+// Dirichlet ends) is solved in the eigen basis of its interior GLL operator,
+// as the reference solves each one with per-wavenumber LU
+// (DPS/src/NonPeriodic2D_MPI.cpp:228-474, one CreatePDEPlan / SolvePDE per
+// problem): u_int = V (x-FFT^-1 diag(1/(mu_j - sigma(kx))) x-FFT) V^-1 f_int,
+// with V, V^-1 the folded transforms of helm_fdm.cu.  The work is cut into
+// three kinds of items that persistent CTAs take from one ordered queue:
+//   1. (problem, 32 x rows): fold and first transform of f's rows on the FP64
+//      tensor cores -> the problem's coefficient rows C[x][2 ld] (scratch);
+//   2. (problem, 16 coefficient column pairs): x FFT, scaling by
+//      1 / ((mu_j - sigma) Nx), inverse x FFT, in place in C;
+//   3. (problem, 32 x rows): second transform, unfold -> u rows.
+// A kind-2 item waits until every kind-1 item of its problem is done, a kind-3
+// item until every kind-2 item is (per-problem counters, bounded waits).  The
+// queue holds every kind-1 item before any kind-2 item before any kind-3 item,
+// so a CTA only waits for items that running CTAs have already taken: the
+// launch needs no co-residency guarantee.  Big problems spread over many CTAs
+// (a 512 x 129 problem is 16 + 4 + 16 items), small ones cost one item each.
+// The coefficient scratch (sum of Nx * 2 ld doubles) mostly stays in L2.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <map>
+#include <new>
+#include <numeric>
+#include <string>
+#include <vector>
+
+#include "../../include/helm_b200.h"
+#include "helm_batch_eig.cuh"
+#include "helm_device.cuh"
+#include "helm_plan.hpp"
+#include "helm_setup.hpp"
+
+namespace helm {
+
+namespace {
+
+constexpr int BE_THREADS = 512;
+constexpr int BE_ROWS = 32;       // x rows of a kind-1 / kind-3 item
+constexpr int BE_HS = 17;         // double2 per row of a kind-2 tile (16 columns + 1 of pad)
+constexpr long long BE_WAIT_LIMIT = 1ll << 24;
+constexpr double kBePi = 3.1415926535897932;  // the reference's PI (General.h:14)
+
+struct BeProblem {
+    long long off;   // element offset of f / u in the packed buffers
+    long long coff;  // offset (doubles) of the coefficient rows in the scratch
+    double lam;
+    int nx, cls, nchunk, ngroup;
+};
+
+struct BeClass {
+    int P, n, m, ms, ma, ld, pitch;  // pitch: doubles per staged f row
+    const double* first;             // m8n8k4 B fragments [2][ld/8][ld/4][32] of Vs^-1 | Va^-1
+    const double* second;            // of Vs | Va
+    const double* mu;                // [2 ld]: ms symmetric then ma antisymmetric eigenvalues
+};
+
+struct BeArgs {
+    const double* f;
+    double* u;
+    double* C;
+    const BeProblem* prob;
+    const BeClass* cls;
+    const int* items;
+    int nitems;
+    int* head;                // queue position
+    int* done1;               // kind-1 items finished, per problem
+    int* done2;               // kind-2 items finished, per problem
+    int* err;                 // status word: 7 when a dependency wait ran out
+    const double2* tw[10];    // exp(-2 pi i e / 2^k), k = 3 .. 9
+    double Lx;
+};
+
+__device__ __forceinline__ int ld_acquire(const int* p)
+{
+    int v;
+    asm volatile("ld.acquire.gpu.global.s32 %0, [%1];\n" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+
+// Kind 1: rows x0 .. x0+R-1 of problem pr -> coefficient rows.
+template <int LD>
+__device__ void be_rows_in(const BeArgs& a, const BeProblem& pr, const BeClass& c, int idx, double* sm)
+{
+    constexpr int NT = LD / 8, KK = LD / 4, NTW = (NT + 1) / 2;
+    const int R = pr.nx < BE_ROWS ? pr.nx : BE_ROWS, x0 = idx * BE_ROWS, P = c.P, pitch = c.pitch;
+    double* st = sm;  // [R][pitch]; the boundary slots stay zero (homogeneous Dirichlet)
+    const double* f = a.f + pr.off + (long long)x0 * P;
+    for (int e = threadIdx.x; e < R * P; e += BE_THREADS) {
+        const int r = e / P, k = e - r * P;
+        st[r * pitch + k] = (k > 0 && k < P - 1) ? __ldg(f + e) : 0.0;
+    }
+    __syncthreads();
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, g = lane >> 2, q = lane & 3;
+    const int mt = warp & 3, fold = (warp >> 2) & 1, nt0 = warp >> 3;
+    if (mt * 8 < R && nt0 < NT) {
+        double acc[NTW][2];
+#pragma unroll
+        for (int t = 0; t < NTW; ++t) acc[t][0] = acc[t][1] = 0.0;
+        const double* row = st + (mt * 8 + g) * pitch;
+        const double* B = c.first + (size_t)fold * NT * KK * 32;
+#pragma unroll
+        for (int kk = 0; kk < KK; ++kk) {
+            const double av = fold_value(row, nullptr, 4 * kk + q, fold, c.n, c.m, c.ms);
+#pragma unroll
+            for (int t = 0; t < NTW; ++t) {
+                const int nt = nt0 + 2 * t;
+                if (nt < NT) dmma_8x8x4(acc[t][0], acc[t][1], av, __ldg(B + (nt * KK + kk) * 32 + lane));
+            }
+        }
+        double* crow = a.C + pr.coff + (long long)(x0 + mt * 8 + g) * 2 * LD + fold * LD;
+#pragma unroll
+        for (int t = 0; t < NTW; ++t) {
+            const int nt = nt0 + 2 * t;
+            if (nt < NT) *reinterpret_cast<double2*>(crow + nt * 8 + 2 * q) = make_double2(acc[t][0], acc[t][1]);
+        }
+    }
+}
+
+// 1 / ((mu_j - sigma) Nx) of real coefficient column j (zero on padding slots).
+__device__ __forceinline__ double be_recip(const BeClass& c, int j, double sig, double scale)
+{
+    const int ld = c.ld;
+    const bool live = j < ld ? j < c.ms : (j - ld) < c.ma;
+    if (!live) return 0.0;
+    return scale / (c.mu[j < ld ? j : c.ms + (j - ld)] - sig);
+}
+
+// Kind 2: column pairs [16 idx, 16 idx + CT) of problem pr, along x.
+template <int L>
+__device__ void be_columns(const BeArgs& a, const BeProblem& pr, const BeClass& c, int idx, double* sm)
+{
+    constexpr int LOG2 = L == 8 ? 3 : L == 16 ? 4 : L == 32 ? 5 : L == 64 ? 6 : L == 128 ? 7 : L == 256 ? 8 : 9;
+    const int ld2 = 2 * c.ld, CT = c.ld < 16 ? c.ld : 16, col0 = idx * 2 * CT;
+    double2* z = reinterpret_cast<double2*>(sm);  // [L][BE_HS]
+    double* Cb = a.C + pr.coff;
+    for (int e = threadIdx.x; e < L * CT; e += BE_THREADS) {
+        const int x = e / CT, cc = e - x * CT;
+        z[x * BE_HS + cc] = __ldcg(reinterpret_cast<const double2*>(Cb + (long long)x * ld2 + col0 + 2 * cc));
+    }
+    __syncthreads();
+    const double2* tw = a.tw[LOG2];
+    slab_fft<L, -1, BE_THREADS>(z, BE_HS, CT, tw);
+    // real-to-complex split of each column pair, scaling, and the assembly of
+    // the full-length spectrum for the inverse (imaginary parts dropped at
+    // kx = 0 and L / 2)
+    const double scale = 1.0 / L;
+    for (int e = threadIdx.x; e < (L / 2 + 1) * CT; e += BE_THREADS) {
+        const int kx = e / CT, cc = e - kx * CT, km = (L - kx) & (L - 1);
+        const double2 zk = z[kx * BE_HS + cc], zm = z[km * BE_HS + cc];
+        double2 X = make_double2(0.5 * (zk.x + zm.x), 0.5 * (zk.y - zm.y));
+        double2 Y = make_double2(0.5 * (zk.y + zm.y), 0.5 * (zm.x - zk.x));
+        const double sig = pr.lam + 4.0 * kBePi * kBePi * kx * kx / (a.Lx * a.Lx);
+        const double r0 = be_recip(c, col0 + 2 * cc, sig, scale), r1 = be_recip(c, col0 + 2 * cc + 1, sig, scale);
+        X = make_double2(X.x * r0, X.y * r0);
+        Y = make_double2(Y.x * r1, Y.y * r1);
+        if (kx == 0 || kx == L / 2) { X.y = 0.0; Y.y = 0.0; }
+        z[kx * BE_HS + cc] = make_double2(X.x - Y.y, X.y + Y.x);
+        if (kx > 0 && kx < L / 2) z[km * BE_HS + cc] = make_double2(X.x + Y.y, Y.x - X.y);
+    }
+    __syncthreads();
+    slab_fft<L, 1, BE_THREADS>(z, BE_HS, CT, tw);
+    for (int e = threadIdx.x; e < L * CT; e += BE_THREADS) {
+        const int x = e / CT, cc = e - x * CT;
+        __stcg(reinterpret_cast<double2*>(Cb + (long long)x * ld2 + col0 + 2 * cc), z[x * BE_HS + cc]);
+    }
+}
+
+// Kind 3: coefficient rows x0 .. x0+R-1 -> second transform, unfold -> u rows.
+template <int LD>
+__device__ void be_rows_out(const BeArgs& a, const BeProblem& pr, const BeClass& c, int idx, double* sm)
+{
+    constexpr int NT = LD / 8, KK = LD / 4, NTW = (NT + 1) / 2, PITCH = 2 * LD + 4;
+    const int R = pr.nx < BE_ROWS ? pr.nx : BE_ROWS, x0 = idx * BE_ROWS, P = c.P;
+    double* cin = sm;                   // [R][PITCH] coefficients
+    double* vout = sm + R * PITCH;      // [R][PITCH] transformed values: s | d
+    const double* Cb = a.C + pr.coff + (long long)x0 * 2 * LD;
+    for (int e = threadIdx.x; e < R * LD; e += BE_THREADS) {
+        const int r = e / LD, j2 = 2 * (e - r * LD);
+        *reinterpret_cast<double2*>(cin + r * PITCH + j2) =
+            __ldcg(reinterpret_cast<const double2*>(Cb + (long long)r * 2 * LD + j2));
+    }
+    __syncthreads();
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, g = lane >> 2, q = lane & 3;
+    const int mt = warp & 3, fold = (warp >> 2) & 1, nt0 = warp >> 3;
+    if (mt * 8 < R && nt0 < NT) {
+        double acc[NTW][2];
+#pragma unroll
+        for (int t = 0; t < NTW; ++t) acc[t][0] = acc[t][1] = 0.0;
+        const double* row = cin + (mt * 8 + g) * PITCH + fold * LD;
+        const double* B = c.second + (size_t)fold * NT * KK * 32;
+#pragma unroll
+        for (int kk = 0; kk < KK; ++kk) {
+            const double av = row[4 * kk + q];
+#pragma unroll
+            for (int t = 0; t < NTW; ++t) {
+                const int nt = nt0 + 2 * t;
+                if (nt < NT) dmma_8x8x4(acc[t][0], acc[t][1], av, __ldg(B + (nt * KK + kk) * 32 + lane));
+            }
+        }
+        double* orow = vout + (mt * 8 + g) * PITCH + fold * LD;
+#pragma unroll
+        for (int t = 0; t < NTW; ++t) {
+            const int nt = nt0 + 2 * t;
+            if (nt < NT) *reinterpret_cast<double2*>(orow + nt * 8 + 2 * q) = make_double2(acc[t][0], acc[t][1]);
+        }
+    }
+    __syncthreads();
+    const int n = c.n, m = c.m, ms = c.ms;
+    double* u = a.u + pr.off + (long long)x0 * P;
+    for (int e = threadIdx.x; e < R * P; e += BE_THREADS) {
+        const int r = e / P, k = e - r * P;
+        const double* s = vout + r * PITCH;
+        double v = 0.0;
+        if (k > 0 && k < P - 1) {
+            const int j = k - 1;
+            if (j < m) v = kR2 * (s[j] + s[LD + j]);
+            else if (j < ms) v = s[j];
+            else v = kR2 * (s[n - 1 - j] - s[LD + n - 1 - j]);
+        }
+        u[e] = v;
+    }
+}
+
+__global__ void __launch_bounds__(BE_THREADS, 1) batch_eig_kernel(BeArgs a)
+{
+    extern __shared__ __align__(16) double bsm[];
+    __shared__ int s_item, s_ok;
+    pdl_enter();
+    for (;;) {
+        if (threadIdx.x == 0) s_item = atomicAdd(a.head, 1);
+        __syncthreads();
+        const int it = s_item;
+        if (it >= a.nitems) break;
+        const int code = a.items[it];
+        const int kind = code >> 28, b = (code >> 12) & 0xffff, idx = code & 0xfff;
+        const BeProblem pr = a.prob[b];
+        const BeClass c = a.cls[pr.cls];
+        if (kind > 1) {
+            // wait for the items this one depends on (taken earlier from the queue)
+            if (threadIdx.x == 0) {
+                const int* cnt = kind == 2 ? &a.done1[b] : &a.done2[b];
+                const int need = kind == 2 ? pr.nchunk : pr.ngroup;
+                int ok = 1;
+                for (long long w = 0; ld_acquire(cnt) < need; ++w) {
+                    if (w >= BE_WAIT_LIMIT) {
+                        ok = 0;
+                        atomicExch(a.err, 7);
+                        break;
+                    }
+                    __nanosleep(64);
+                }
+                s_ok = ok;
+            }
+            __syncthreads();
+        } else if (threadIdx.x == 0) {
+            s_ok = 1;
+        }
+        __syncthreads();
+        if (s_ok) {
+            if (kind == 1 || kind == 3) {
+                switch (c.ld) {
+                    case 8: kind == 1 ? be_rows_in<8>(a, pr, c, idx, bsm) : be_rows_out<8>(a, pr, c, idx, bsm); break;
+                    case 16: kind == 1 ? be_rows_in<16>(a, pr, c, idx, bsm) : be_rows_out<16>(a, pr, c, idx, bsm); break;
+                    case 32: kind == 1 ? be_rows_in<32>(a, pr, c, idx, bsm) : be_rows_out<32>(a, pr, c, idx, bsm); break;
+                    default: kind == 1 ? be_rows_in<64>(a, pr, c, idx, bsm) : be_rows_out<64>(a, pr, c, idx, bsm); break;
+                }
+            } else {
+                switch (pr.nx) {
+                    case 8: be_columns<8>(a, pr, c, idx, bsm); break;
+                    case 16: be_columns<16>(a, pr, c, idx, bsm); break;
+                    case 32: be_columns<32>(a, pr, c, idx, bsm); break;
+                    case 64: be_columns<64>(a, pr, c, idx, bsm); break;
+                    case 128: be_columns<128>(a, pr, c, idx, bsm); break;
+                    case 256: be_columns<256>(a, pr, c, idx, bsm); break;
+                    default: be_columns<512>(a, pr, c, idx, bsm); break;
+                }
+            }
+        }
+        // publish: every thread's writes before the counter moves
+        __threadfence();
+        __syncthreads();
+        if (threadIdx.x == 0 && kind < 3) atomicAdd(kind == 1 ? &a.done1[b] : &a.done2[b], 1);
+    }
+}
+
+// m8n8k4 B fragments of an ld x ld block M (row-major, out = M in): lane l of
+// (nt, kk) holds M[8 nt + l / 4][4 kk + l % 4].
+void swizzle_b(const std::vector<double>& M, int dim, int ld, double* out)
+{
+    const int NT = ld / 8, KK = ld / 4;
+    for (int nt = 0; nt < NT; ++nt)
+        for (int kk = 0; kk < KK; ++kk)
+            for (int l = 0; l < 32; ++l) {
+                const int i = nt * 8 + (l >> 2), k = kk * 4 + (l & 3);
+                out[((size_t)nt * KK + kk) * 32 + l] = (i < dim && k < dim) ? M[(size_t)i * dim + k] : 0.0;
+            }
+}
+
+}  // namespace
+
+struct BatchEig {
+    int device = 0, nprob = 0, nitems = 0, nsm = 148;
+    size_t smem = 0;
+    BeArgs args{};
+    int* d_counters = nullptr;  // head, done1[nprob], done2[nprob]
+    size_t counter_bytes = 0;
+    std::vector<void*> allocs;
+    long long bytes = 0;
+
+    int alloc(void** p, size_t n)
+    {
+        if (cudaMalloc(p, n) != cudaSuccess) {
+            cudaGetLastError();
+            *p = nullptr;
+            set_last_error("cudaMalloc failed for the batch tables");
+            return HELM_ERR_OOM;
+        }
+        allocs.push_back(*p);
+        bytes += (long long)n;
+        return HELM_OK;
+    }
+    int upload(void** p, const void* h, size_t n)
+    {
+        if (int st = alloc(p, n)) return st;
+        if (cudaMemcpy(*p, h, n, cudaMemcpyHostToDevice) != cudaSuccess) {
+            cudaGetLastError();
+            set_last_error("cudaMemcpy failed for the batch tables");
+            return HELM_ERR_CUDA;
+        }
+        return HELM_OK;
+    }
+    void release()
+    {
+        for (void* p : allocs) cudaFree(p);
+        allocs.clear();
+    }
+};
+
+int batch_eig_create(int nprob, const int* Nx, const int* N, const double* lambda, double xl, double xr, double yl,
+                     double yr, const long long* offs, int device, BatchEig** out)
+{
+    *out = nullptr;
+    if (nprob > 0xffff) {
+        set_last_error("more problems than the one-launch batch takes");
+        return HELM_ERR_UNSUPPORTED;
+    }
+    for (int i = 0; i < nprob; ++i)
+        if (Nx[i] < 8 || Nx[i] > 512 || N[i] < 4 || N[i] > 129) {
+            set_last_error("problem outside the one-launch batch range (Nx 8..512, 4..129 GLL points)");
+            return HELM_ERR_UNSUPPORTED;
+        }
+    const double Lx = xr - xl, Ly = yr - yl;
+    BatchEig* be = new (std::nothrow) BatchEig();
+    if (!be) return HELM_ERR_OOM;
+    be->device = device;
+    be->nprob = nprob;
+    int st = HELM_OK;
+    // one class per GLL size: folded eigen-decomposition and its fragments
+    std::map<int, int> cls_of;
+    std::vector<BeClass> cls;
+    std::vector<FoldedEigen> eig;
+    for (int i = 0; i < nprob && !st; ++i) {
+        if (cls_of.count(N[i])) continue;
+        const int P = N[i], n = P - 2;
+        const GllSetup gll = build_gll_setup(P, 1, Ly);
+        std::vector<double> A0((size_t)n * n);
+        for (int r = 0; r < n; ++r)
+            for (int q = 0; q < n; ++q) A0[(size_t)r * n + q] = gll.D2[(size_t)(r + 1) * P + q + 1];
+        FoldedEigen fe;
+        if (!fold_eigen(n, A0, fe)) {
+            set_last_error("no eigen-decomposition of the GLL operator for the one-launch batch");
+            st = HELM_ERR_UNSUPPORTED;
+            break;
+        }
+        BeClass c{};
+        c.P = P;
+        c.n = n;
+        c.m = fe.m;
+        c.ms = fe.ms;
+        c.ma = fe.ma;
+        c.ld = fe.ms <= 8 ? 8 : fe.ms <= 16 ? 16 : fe.ms <= 32 ? 32 : 64;
+        c.pitch = 4 + 16 * ((P + 11) / 16);  // >= P, = 4 mod 16: conflict-free fragment loads
+        const int ld = c.ld;
+        const size_t frag = (size_t)ld * ld;
+        std::vector<double> first(2 * frag), second(2 * frag), mu(2 * (size_t)ld, 0.0);
+        swizzle_b(fe.Vsi, fe.ms, ld, first.data());
+        swizzle_b(fe.Vai, fe.ma, ld, first.data() + frag);
+        swizzle_b(fe.Vs, fe.ms, ld, second.data());
+        swizzle_b(fe.Va, fe.ma, ld, second.data() + frag);
+        for (int j = 0; j < fe.ms; ++j) mu[j] = fe.ls[j];
+        for (int j = 0; j < fe.ma; ++j) mu[fe.ms + j] = fe.la[j];
+        void *d1 = nullptr, *d2 = nullptr, *d3 = nullptr;
+        if ((st = be->upload(&d1, first.data(), first.size() * sizeof(double)))) break;
+        if ((st = be->upload(&d2, second.data(), second.size() * sizeof(double)))) break;
+        if ((st = be->upload(&d3, mu.data(), mu.size() * sizeof(double)))) break;
+        c.first = static_cast<const double*>(d1);
+        c.second = static_cast<const double*>(d2);
+        c.mu = static_cast<const double*>(d3);
+        cls_of[P] = (int)cls.size();
+        cls.push_back(c);
+        eig.push_back(std::move(fe));
+    }
+    // problems: scratch offsets, item counts, and the singularity check of the
+    // class path (a shift too close to an eigenvalue)
+    std::vector<BeProblem> prob(nprob);
+    long long coff = 0;
+    size_t smem = 0;
+    for (int i = 0; i < nprob && !st; ++i) {
+        const int ci = cls_of[N[i]];
+        const BeClass& c = cls[ci];
+        const FoldedEigen& fe = eig[ci];
+        for (int kx = 0; kx <= Nx[i] / 2 && !st; ++kx) {
+            const double sig = lambda[i] + 4.0 * kBePi * kBePi * kx * kx / (Lx * Lx);
+            for (double l : fe.ls)
+                if (!(std::fabs(l - sig) > 1e-12 * std::max(std::fabs(l), std::fabs(sig)))) st = HELM_ERR_SINGULAR;
+            for (double l : fe.la)
+                if (!(std::fabs(l - sig) > 1e-12 * std::max(std::fabs(l), std::fabs(sig)))) st = HELM_ERR_SINGULAR;
+        }
+        if (st) {
+            set_last_error("shifted GLL operator is singular");
+            break;
+        }
+        BeProblem& p = prob[i];
+        p.off = offs[i];
+        p.coff = coff;
+        p.lam = lambda[i];
+        p.nx = Nx[i];
+        p.cls = ci;
+        p.nchunk = (Nx[i] + BE_ROWS - 1) / BE_ROWS;
+        p.ngroup = c.ld <= 16 ? 1 : c.ld / 16;
+        coff += (long long)Nx[i] * 2 * c.ld;
+        const int R = std::min(Nx[i], BE_ROWS);
+        smem = std::max(smem, (size_t)R * c.pitch * sizeof(double));
+        smem = std::max(smem, (size_t)2 * R * (2 * c.ld + 4) * sizeof(double));
+        smem = std::max(smem, (size_t)Nx[i] * BE_HS * sizeof(double2));
+    }
+    if (st) {
+        be->release();
+        delete be;
+        return st;
+    }
+    // the ordered queue: every kind-1 item, then every kind-2, then every
+    // kind-3, problems in order of decreasing work so the big ones start first
+    std::vector<int> order(nprob);
+    std::iota(order.begin(), order.end(), 0);
+    std::stable_sort(order.begin(), order.end(), [&](int x, int y) {
+        const long long cx = (long long)prob[x].nx * cls[prob[x].cls].ld * cls[prob[x].cls].ld;
+        const long long cy = (long long)prob[y].nx * cls[prob[y].cls].ld * cls[prob[y].cls].ld;
+        return cx > cy;
+    });
+    std::vector<int> items;
+    for (int kind = 1; kind <= 3; ++kind)
+        for (int b : order) {
+            const int cnt = kind == 2 ? prob[b].ngroup : prob[b].nchunk;
+            for (int k = 0; k < cnt; ++k) items.push_back((kind << 28) | (b << 12) | k);
+        }
+    BeArgs& a = be->args;
+    void *dp = nullptr, *dc = nullptr, *di = nullptr, *dC = nullptr, *dcnt = nullptr, *derr = nullptr;
+    if (!st) st = be->upload(&dp, prob.data(), prob.size() * sizeof(BeProblem));
+    if (!st) st = be->upload(&dc, cls.data(), cls.size() * sizeof(BeClass));
+    if (!st) st = be->upload(&di, items.data(), items.size() * sizeof(int));
+    if (!st) st = be->alloc(&dC, (size_t)coff * sizeof(double));
+    be->counter_bytes = (1 + 2 * (size_t)nprob) * sizeof(int);
+    if (!st) st = be->alloc(&dcnt, be->counter_bytes);
+    const int zero = 0;
+    if (!st) st = be->upload(&derr, &zero, sizeof(int));
+    for (int k = 3; k <= 9 && !st; ++k) {
+        const int L = 1 << k;
+        std::vector<double> tw(2 * (size_t)L);
+        for (int e = 0; e < L; ++e) {
+            const long double ang = -2.0L * 3.14159265358979323846264338327950288L * e / L;
+            tw[2 * e] = (double)std::cos(ang);
+            tw[2 * e + 1] = (double)std::sin(ang);
+        }
+        void* d = nullptr;
+        if (!(st = be->upload(&d, tw.data(), tw.size() * sizeof(double)))) a.tw[k] = static_cast<const double2*>(d);
+    }
+    if (st) {
+        be->release();
+        delete be;
+        return st;
+    }
+    a.prob = static_cast<const BeProblem*>(dp);
+    a.cls = static_cast<const BeClass*>(dc);
+    a.items = static_cast<const int*>(di);
+    a.nitems = (int)items.size();
+    a.C = static_cast<double*>(dC);
+    be->d_counters = static_cast<int*>(dcnt);
+    a.head = be->d_counters;
+    a.done1 = be->d_counters + 1;
+    a.done2 = be->d_counters + 1 + nprob;
+    a.err = static_cast<int*>(derr);
+    a.Lx = Lx;
+    be->nitems = a.nitems;
+    be->smem = smem;
+    int nsm = 0;
+    if (cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, device) == cudaSuccess && nsm > 0) be->nsm = nsm;
+    cudaGetLastError();
+    if (cudaFuncSetAttribute(batch_eig_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess) {
+        cudaGetLastError();
+        be->release();
+        delete be;
+        set_last_error("the one-launch batch kernel does not get its shared memory");
+        return HELM_ERR_UNSUPPORTED;
+    }
+    *out = be;
+    return HELM_OK;
+}
+
+int batch_eig_solve(BatchEig* be, const double* f, double* u, cudaStream_t s)
+{
+    BeArgs a = be->args;
+    a.f = f;
+    a.u = u;
+    cudaError_t e = cudaMemsetAsync(be->d_counters, 0, be->counter_bytes, s);
+    if (e == cudaSuccess) {
+        const int grid = std::min(be->nsm, be->nitems);
+        e = launch_k(batch_eig_kernel, dim3(grid), dim3(BE_THREADS), be->smem, s, a);
+    }
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        set_last_error(cudaGetErrorString(e));
+        return HELM_ERR_CUDA;
+    }
+    return HELM_OK;
+}
+
+long long batch_eig_device_bytes(const BatchEig* be) { return be->bytes; }
+int* batch_eig_status(BatchEig* be) { return be->args.err; }
+
+void batch_eig_destroy(BatchEig* be)
+{
+    if (!be) return;
+    be->release();
+    delete be;
+}
+
+}  // namespace helm

@@ -234,6 +234,28 @@ __device__ __forceinline__ void dmma_8x8x4(double& c0, double& c1, double a, dou
                  : "d"(a), "d"(b));
 }
 
+// 1 / sqrt 2, the weight of the orthogonal even/odd fold of the GLL interior.
+constexpr double kR2 = 0.70710678118654752440;
+
+// Value of fold `fold` at interior index k of a staged row (interior element
+// j at row[1 + j]; rs: the same row of a field to subtract, or NULL):
+// (u_{1+k} + u_{n-k}) / sqrt 2 (symmetric fold) or (u_{1+k} - u_{n-k}) /
+// sqrt 2 (antisymmetric) for k < m, the middle element for the symmetric fold
+// at k = m when n is odd, zero beyond (padding slots).
+__device__ __forceinline__ double fold_value(const double* row, const double* rs, int k, int fold, int n, int m, int ms)
+{
+    if (k < m) {
+        double lo = row[1 + k], hi = row[n - k];
+        if (rs) {
+            lo -= rs[1 + k];
+            hi -= rs[n - k];
+        }
+        return fold ? kR2 * (lo - hi) : kR2 * (lo + hi);
+    }
+    if (!fold && k < ms) return rs ? row[1 + k] - rs[1 + k] : row[1 + k];
+    return 0.0;
+}
+
 // Programmatic dependent launch.  Every kernel of a solve is launched with the
 // programmatic-serialization attribute, so it may be scheduled while the
 // previous kernel in the stream is still finishing; pdl_enter() then waits

@@ -37,7 +37,6 @@ namespace {
 constexpr int EP_PITCH = 68;     // doubles per row of a plane in shared memory (P <= 66, 64 slots, 4 of pad)
 constexpr int EP_HS = EP_PITCH / 2;
 constexpr int EP_FRAG = 4 * 8 * 32;  // doubles of one fold's transform in fragment order
-constexpr double kR2 = 0.70710678118654752440;
 
 template <int L>
 struct EpShape {
@@ -489,25 +488,6 @@ __global__ void __launch_bounds__(EpShape<L>::THREADS, 1) eig_solve2d_kernel(Eig
     second_transform<S::MTW>(a, rows, M2, M2 + EP_FRAG, lane);
     const double acc = store_adjoint_rows<L>(a, a.u, a.f, 0, 0, rows, warp * S::RW, lane, dl, dr);
     if (a.lam_out) eig_lambda_sum(a, acc);
-}
-
-// Value of fold `fold` at interior index k of a staged row (interior element
-// j at row[1 + j]; rs: the same row of u_obs to subtract, or NULL):
-// (u_{1+k} + u_{n-k}) / sqrt 2 (symmetric) or (u_{1+k} - u_{n-k}) / sqrt 2
-// (antisymmetric) for k < m, the middle element for the symmetric fold at
-// k = m when n is odd, zero beyond.
-__device__ __forceinline__ double fold_value(const double* row, const double* rs, int k, int fold, int n, int m, int ms)
-{
-    if (k < m) {
-        double lo = row[1 + k], hi = row[n - k];
-        if (rs) {
-            lo -= rs[1 + k];
-            hi -= rs[n - k];
-        }
-        return fold ? kR2 * (lo - hi) : kR2 * (lo + hi);
-    }
-    if (!fold && k < ms) return rs ? row[1 + k] - rs[1 + k] : row[1 + k];
-    return 0.0;
 }
 
 // Tensor maps of one solve (kernel parameter, built on the host per call).

@@ -90,8 +90,15 @@ __device__ __forceinline__ void c2r_store(const FftArgs& a, TIO* out, long long 
 #pragma unroll
             for (int r = 0; r < RL; ++r) {
                 const long long row = pass_out_row<RL, NSL, TPC>(tc, t, r);
-                out[row * a.out_row + c0] = (TIO)(v[t * RL + r].x * sc);
-                if (has1) out[row * a.out_row + c1] = (TIO)(v[t * RL + r].y * sc);
+                TIO* o0 = out + row * a.out_row + c0;
+                const TIO x0 = (TIO)(v[t * RL + r].x * sc), x1 = (TIO)(v[t * RL + r].y * sc);
+                if (a.accumulate) {
+                    *o0 += x0;
+                    if (has1) o0[c1 - c0] += x1;
+                } else {
+                    *o0 = x0;
+                    if (has1) o0[c1 - c0] = x1;
+                }
             }
         return;
     } else {

@@ -62,6 +62,9 @@ struct FftArgs {
     // in - in_sub, same layout and type as in (the data misfit u - u_obs of the
     // adjoint of a least-squares loss, formed as it is loaded)
     const void* in_sub;
+    // C2R only (forward): add the result to out instead of storing it (the
+    // correction of a refinement sweep accumulated into the solution)
+    int accumulate;
 };
 
 // Finite-difference variant: one tridiagonal solve along z per spectrum row.

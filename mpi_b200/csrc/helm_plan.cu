@@ -240,39 +240,10 @@ static int setup_fast(Plan& p, const std::vector<double>& A0, int prec_code)
     const int n = p.n, m = n / 2, odd = n % 2, ms = m + odd, ma = m, N = p.N, G = p.ngroups;
     const int ld = 32 * ((ms + 31) / 32);
     if (fdm_fast_smem_bytes(prec_code, ld) > kMaxSmemPerBlock || ld > 64) return HELM_OK;  // stay on rows_kernel
-    const double r2 = 0.70710678118654752440;
-    std::vector<double> Q((size_t)n * n, 0.0), T((size_t)n * n, 0.0), Mf((size_t)n * n, 0.0);
-    for (int k = 0; k < m; ++k) {
-        Q[(size_t)k * n + k] = r2;
-        Q[(size_t)k * n + n - 1 - k] = r2;
-        Q[(size_t)(ms + k) * n + k] = r2;
-        Q[(size_t)(ms + k) * n + n - 1 - k] = -r2;
-    }
-    if (odd) Q[(size_t)m * n + m] = 1.0;
-    for (int i = 0; i < n; ++i)  // T = Q A0
-        for (int j = 0; j < n; ++j) {
-            double s = 0;
-            for (int k = 0; k < n; ++k) s += Q[(size_t)i * n + k] * A0[(size_t)k * n + j];
-            T[(size_t)i * n + j] = s;
-        }
-    double amax = 0, off = 0;
-    for (int i = 0; i < n; ++i)  // Mf = T Q^T
-        for (int j = 0; j < n; ++j) {
-            double s = 0;
-            for (int k = 0; k < n; ++k) s += T[(size_t)i * n + k] * Q[(size_t)j * n + k];
-            Mf[(size_t)i * n + j] = s;
-            amax = std::max(amax, std::fabs(s));
-            if ((i < ms) != (j < ms)) off = std::max(off, std::fabs(s));
-        }
-    if (off > 1e-11 * amax) return HELM_OK;  // not centrosymmetric to rounding: keep rows_kernel
-    std::vector<double> Ms((size_t)ms * ms), Ma((size_t)ma * ma);
-    for (int i = 0; i < ms; ++i)
-        for (int j = 0; j < ms; ++j) Ms[(size_t)i * ms + j] = Mf[(size_t)i * n + j];
-    for (int i = 0; i < ma; ++i)
-        for (int j = 0; j < ma; ++j) Ma[(size_t)i * ma + j] = Mf[(size_t)(ms + i) * n + ms + j];
-    std::vector<double> ls(ms), Vs((size_t)ms * ms), Vsi((size_t)ms * ms), la(ma), Va((size_t)ma * ma), Vai((size_t)ma * ma);
-    if (!real_eigen(ms, Ms.data(), ls.data(), Vs.data(), Vsi.data())) return HELM_OK;
-    if (ma > 0 && !real_eigen(ma, Ma.data(), la.data(), Va.data(), Vai.data())) return HELM_OK;
+    FoldedEigen fe;
+    if (!fold_eigen(n, A0, fe)) return HELM_OK;  // not centrosymmetric to rounding, or no decomposition: rows_kernel
+    const std::vector<double>&Q = fe.Q, &Ms = fe.Ms, &Ma = fe.Ma, &ls = fe.ls, &Vs = fe.Vs, &Vsi = fe.Vsi,
+                               &la = fe.la, &Va = fe.Va, &Vai = fe.Vai;
 
     const size_t L2 = (size_t)ld * ld;
     std::vector<double> fw(4 * L2, 0.0), fa(4 * L2, 0.0), d2f(2 * L2, 0.0), d2a(2 * L2, 0.0);

@@ -341,3 +341,58 @@ GllSetup build_gll_setup(int N, int Ns, double L)
 }
 
 }  // namespace helm
+
+namespace helm {
+
+bool fold_eigen(int n, const std::vector<double>& A0, FoldedEigen& fe)
+{
+    const int m = n / 2, odd = n % 2, ms = m + odd, ma = m;
+    const double r2 = 0.70710678118654752440;
+    fe.n = n;
+    fe.m = m;
+    fe.ms = ms;
+    fe.ma = ma;
+    fe.Q.assign((size_t)n * n, 0.0);
+    std::vector<double>& Q = fe.Q;
+    for (int k = 0; k < m; ++k) {
+        Q[(size_t)k * n + k] = r2;
+        Q[(size_t)k * n + n - 1 - k] = r2;
+        Q[(size_t)(ms + k) * n + k] = r2;
+        Q[(size_t)(ms + k) * n + n - 1 - k] = -r2;
+    }
+    if (odd) Q[(size_t)m * n + m] = 1.0;
+    std::vector<double> T((size_t)n * n, 0.0), Mf((size_t)n * n, 0.0);
+    for (int i = 0; i < n; ++i)  // T = Q A0
+        for (int j = 0; j < n; ++j) {
+            double s = 0;
+            for (int k = 0; k < n; ++k) s += Q[(size_t)i * n + k] * A0[(size_t)k * n + j];
+            T[(size_t)i * n + j] = s;
+        }
+    double amax = 0, off = 0;
+    for (int i = 0; i < n; ++i)  // Mf = T Q^T
+        for (int j = 0; j < n; ++j) {
+            double s = 0;
+            for (int k = 0; k < n; ++k) s += T[(size_t)i * n + k] * Q[(size_t)j * n + k];
+            Mf[(size_t)i * n + j] = s;
+            amax = std::max(amax, std::fabs(s));
+            if ((i < ms) != (j < ms)) off = std::max(off, std::fabs(s));
+        }
+    if (off > 1e-11 * amax) return false;
+    fe.Ms.assign((size_t)ms * ms, 0.0);
+    fe.Ma.assign((size_t)ma * ma, 0.0);
+    for (int i = 0; i < ms; ++i)
+        for (int j = 0; j < ms; ++j) fe.Ms[(size_t)i * ms + j] = Mf[(size_t)i * n + j];
+    for (int i = 0; i < ma; ++i)
+        for (int j = 0; j < ma; ++j) fe.Ma[(size_t)i * ma + j] = Mf[(size_t)(ms + i) * n + ms + j];
+    fe.ls.assign(ms, 0.0);
+    fe.Vs.assign((size_t)ms * ms, 0.0);
+    fe.Vsi.assign((size_t)ms * ms, 0.0);
+    fe.la.assign(ma, 0.0);
+    fe.Va.assign((size_t)ma * ma, 0.0);
+    fe.Vai.assign((size_t)ma * ma, 0.0);
+    if (!real_eigen(ms, fe.Ms.data(), fe.ls.data(), fe.Vs.data(), fe.Vsi.data())) return false;
+    if (ma > 0 && !real_eigen(ma, fe.Ma.data(), fe.la.data(), fe.Va.data(), fe.Vai.data())) return false;
+    return true;
+}
+
+}  // namespace helm

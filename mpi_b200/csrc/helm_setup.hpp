@@ -38,6 +38,19 @@ void lu_solve(int n, const double* LU, const int* perm, double* b);
 // Returns false if it does not converge or the residual check fails.
 bool real_eigen(int n, const double* A, double* lam, double* V, double* Vinv);
 
+// The orthogonal even/odd fold of the n interior GLL nodes and the
+// eigen-decompositions of the two blocks it makes of a centrosymmetric n x n
+// operator A0 (the interior GLL second derivative): Q A0 Q^T = diag(Ms, Ma),
+// Ms = Vs diag(ls) Vs^-1 (ms = ceil(n/2)), Ma = Va diag(la) Va^-1 (ma = n/2).
+// Row k < m of Q is (e_k + e_{n-1-k}) / sqrt 2, row ms + k is
+// (e_k - e_{n-1-k}) / sqrt 2, and row m is e_m when n is odd.
+struct FoldedEigen {
+    int n = 0, m = 0, ms = 0, ma = 0;
+    std::vector<double> Q, Ms, Ma, ls, Vs, Vsi, la, Va, Vai;
+};
+// False when A0 is not centrosymmetric to rounding or a decomposition fails.
+bool fold_eigen(int n, const std::vector<double>& A0, FoldedEigen& fe);
+
 // Grid and operators of one plan, FP64, built by build_gll_setup.
 struct GllSetup {
     int N = 0, Ns = 1;

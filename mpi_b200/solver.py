@@ -436,7 +436,9 @@ class BatchNonPeriodic2D:
     common domain.  ``f`` and ``u`` are packed 1-D float64 tensors: problem p is
     the ``[Nx[p], N[p]]`` block at ``offsets[p]``; :meth:`pack` / :meth:`unpack`
     convert from / to per-problem tensors.  One solve is one CUDA graph launch
-    (``graph=False``: the class kernels launched directly)."""
+    holding one persistent kernel (FP64 and refined batches of Nx 8..512 and
+    4..129 GLL points) or the size classes' kernels (``graph=False``: launched
+    directly)."""
 
     def __init__(self, Nx: Sequence[int], N: Sequence[int], lambdas: Sequence[float], xl: float, xr: float,
                  yl: float, yr: float, *, precision: str = "fp64"):
@@ -467,6 +469,13 @@ class BatchNonPeriodic2D:
 
     def set_graph(self, enable: bool) -> None:
         L.check(self._lib.helm_batch_set_graph(self._batch, int(bool(enable))), "helm_batch_set_graph")
+
+    def device_status(self, reset: bool = True) -> int:
+        """0, or 7 when a dependency wait of the persistent kernel ran out."""
+        code = ctypes.c_int()
+        L.check(self._lib.helm_batch_device_status(self._batch, ctypes.byref(code), int(reset)),
+                "helm_batch_device_status")
+        return code.value
 
     def pack(self, fs: Sequence[torch.Tensor]) -> torch.Tensor:
         return torch.cat([f.reshape(-1).to(torch.float64) for f in fs]).contiguous()

@@ -48,6 +48,8 @@ def build(quiet: bool = True) -> None:
     ref_root = reference_root()
     if os.path.isdir(os.path.join(ref_root, "HelmholtzSolvers", "DirectPseudoSpectral")):
         subprocess.run(["make", "-s", "-C", _HERE, "ref", f"REF_ROOT={ref_root}"], check=True, stdout=out)
+        if os.path.exists(os.path.join(_HERE, "..", "mpi_b200", "libhelm_b200.so")):
+            subprocess.run(["make", "-s", "-C", _HERE, "shim", f"REF_ROOT={ref_root}"], check=True, stdout=out)
 
 
 def _p(a: np.ndarray):

@@ -85,13 +85,35 @@ def test_batch_on_side_stream(cuda):
     assert torch.equal(u, ref)
 
 
+def test_batch_one_launch_and_fallback(cuda):
+    """FP64 / refined batches in range run as one persistent kernel launch;
+    FP32 batches and batches with a problem outside its range (Nx = 1024) run
+    the size classes (three kernels each); both match single-problem plans."""
+    Nx, P, lam, fs = _small_batch(seed=13, n=8)
+    b, us = _solve_batch(Nx, P, lam, fs, "fp64")
+    assert b.info()["kernels_per_solve"] == 1
+    assert b.device_status() == 0
+    b32, _ = _solve_batch(Nx, P, lam, fs, "fp32")
+    assert b32.info()["kernels_per_solve"] == 3 * len(set(zip(Nx, P)))
+    Nx2, P2, lam2 = Nx + [1024], P + [9], lam + [3.0]
+    fs2 = fs + [np.random.default_rng(1).standard_normal((1024, 9))]
+    b2, us2 = _solve_batch(Nx2, P2, lam2, fs2, "fp64")
+    assert b2.info()["kernels_per_solve"] == 3 * len(set(zip(Nx2, P2)))
+    for u, v in zip(us, us2):
+        assert max_rel(u, v) < 1e-13
+    pl = NonPeriodic2D(1024, 9, 9, 0.0, TWO_PI, -1.0, 1.0, Lambda=3.0)
+    assert max_rel(us2[-1], pl.SolvePDE(torch.from_numpy(fs2[-1]).cuda()).cpu().numpy()) < 1e-13
+
+
 def test_batch_full_size_512(cuda):
     """512 problems, Nx in {32..512}, GLL order in {16..128}, lambda log-uniform in
     [1e-2, 1e4], the manufactured 2D problem: FP32 + refinement against FP64 per
     problem, both against the exact solution, and a sample against the oracle."""
     Nx, P, lam, fs, us_exact = W.batch_2d(512, seed=1237)
-    _, u64 = _solve_batch(Nx, P, lam, fs, "fp64")
-    _, u32r = _solve_batch(Nx, P, lam, fs, "fp32_refine")
+    b64, u64 = _solve_batch(Nx, P, lam, fs, "fp64")
+    b32r, u32r = _solve_batch(Nx, P, lam, fs, "fp32_refine")
+    assert b64.info()["kernels_per_solve"] == 1 and b32r.info()["kernels_per_solve"] == 1
+    assert b64.device_status() == 0 and b32r.device_status() == 0
     worst = max(rel_l2(a, b) for a, b in zip(u32r, u64))
     assert worst < 1e-10, worst
     assert max(rel_l2(a, e) for a, e in zip(u64, us_exact)) < 1e-11
