@@ -164,7 +164,13 @@ int helm_max_abs_diff(helm_plan_t plan, const double* a, const double* b, double
  * alphar, betar) rows, with the reference's one-sided second-order rows.
  * Arrays: f, u [Nx][Ny][Nz] interior points; gl = back data, gr = front data,
  * [Nx][Ny].  helm_solve / helm_solve_adjoint / helm_plan_destroy apply.
- * FP32_REFINE plans compute in FP64. */
+ * HELM_FP32_REFINE plans solve in FP32 (FP32 spectrum and tridiagonal solves,
+ * FP64 arrays in and out) and refine: per sweep (2 by default,
+ * helm_plan_set_refine_sweeps) the residual f - A_h u of the stencil in FP64
+ * and an FP32 solve of its correction, added to u; the adjoint refines the same
+ * way with the transposed stencil (fbar, the boundary cotangents and
+ * lambda_bar).  Each sweep multiplies the error by about the FP32 solve's
+ * relative error. */
 int helm_fd3d_plan_create(int Nx, int Ny, int Nz, double xl, double xr, double yl, double yr, double zl, double zr,
                           const helm_robin_t* bc, double lambda, int precision, helm_plan_t* plan);
 
@@ -261,18 +267,19 @@ int helm_plan_info(helm_plan_t plan, int* Ns, int* n_operators, int* method, lon
 int helm_plan_set_stage_timing(helm_plan_t plan, int enable);
 int helm_plan_stage_times(helm_plan_t plan, float* ms5);
 
-/* Device status of the plan's TMA-pipelined kernels (row variant 5): 0, or the
- * code of the first wait on a tile copy that ran out of its iteration limit
- * (the kernel then skipped its remaining work, so that solve's output is not
- * valid).  Waits for the device; reset != 0 clears the word afterwards.  Plans
- * without those kernels report 0.  No counterpart in the reference. */
+/* Device status of the plan's tensor-memory-accelerator tile copies (the
+ * first pass of the 3D eigen-basis pipeline): 0, or the code of a wait on a
+ * copy that ran out of its iteration limit (the kernel then skipped that work,
+ * so that solve's output is not valid).  Waits for the device; reset != 0
+ * clears the word afterwards.  Plans without such copies report 0.  No
+ * counterpart in the reference. */
 int helm_plan_device_status(helm_plan_t plan, int* code, int reset);
 
 /* Kernel launch variants of the plan: fft4[i] (0..15) for the x, y, inverse y
  * and inverse x FFT passes -- bit 0: 128-thread CTAs, bit 1: radix-8 schedule
  * (lengths 128, 256), bit 2: persistent pipelined pass, bit 3: 512-thread CTAs
  * for passes of length 512 or 1024 (ignored for shorter ones; with bit 2 the
- * tile exceeds shared memory and the solve fails with HELM_ERR_CUDA) -- and rows (0..5) for
+ * tile exceeds shared memory and the solve fails with HELM_ERR_CUDA) -- and rows (0..4) for
  * the row solve: 0, 1 the two kernel shapes of the plan's precision; 2 (FP64 and
  * refined 3D plans with one element, at most 65 GLL points and Ny in {64, 128,
  * 256}) the y pass, the row solve and the inverse y pass fused into one kernel
@@ -283,12 +290,9 @@ int helm_plan_device_status(helm_plan_t plan, int* code, int reset);
  * pipeline of the whole forward solve -- GLL eigen-transform fused with the x
  * FFT, the y FFT, diagonal scaling and inverse y FFT in one pass, and the
  * inverse of the first pass: three kernels in 3D, one in 2D, fft4 unused;
- * adjoint solves run the transposed pipeline; 5 (3D plans that take 4) the
- * same pipeline with two CTAs per y plane in its first and last passes, one per
- * GLL fold (2D plans: the same as 4).  Plan
- * creation times every variant on the plan's own shape and keeps the fastest
- * (environment HELM_AUTOTUNE=0: all 0, rows 5 in 3D and 4 in 2D where they
- * apply).  Setting them
+ * adjoint solves run the transposed pipeline.  Plan creation times every
+ * variant on the plan's own shape and keeps the fastest (environment
+ * HELM_AUTOTUNE=0: all 0, rows 4 where it applies).  Setting them
  * pins the choice, e.g. to reproduce a run bit for bit.  Every variant
  * computes the same solve; the last bits of the results may differ between
  * variants.  No counterpart in the reference, which has one code path. */

@@ -10,7 +10,7 @@
 // three kinds of items that persistent CTAs take from one ordered queue:
 //   1. (problem, 32 x rows): fold and first transform of f's rows on the FP64
 //      tensor cores -> the problem's coefficient rows C[x][2 ld] (scratch);
-//   2. (problem, 16 coefficient column pairs): x FFT, scaling by
+//   2. (problem, up to 16 coefficient column pairs): x FFT, scaling by
 //      1 / ((mu_j - sigma) Nx), inverse x FFT, in place in C;
 //   3. (problem, 32 x rows): second transform, unfold -> u rows.
 // A kind-2 item waits until every kind-1 item of its problem is done, a kind-3
@@ -18,7 +18,7 @@
 // queue holds every kind-1 item before any kind-2 item before any kind-3 item,
 // so a CTA only waits for items that running CTAs have already taken: the
 // launch needs no co-residency guarantee.  Big problems spread over many CTAs
-// (a 512 x 129 problem is 16 + 4 + 16 items), small ones cost one item each.
+// (a 512 x 129 problem is 16 + 16 + 16 items), small ones cost one item each.
 // The coefficient scratch (sum of Nx * 2 ld doubles) mostly stays in L2.
 #include <cuda_runtime.h>
 
@@ -40,9 +40,17 @@ namespace helm {
 
 namespace {
 
-constexpr int BE_THREADS = 512;
+constexpr int BE_THREADS = 256;   // 8 warps; two or three CTAs share an SM
+constexpr int BE_MINB = 2;        // resident CTAs per SM the kernel is built for
 constexpr int BE_ROWS = 32;       // x rows of a kind-1 / kind-3 item
-constexpr int BE_HS = 17;         // double2 per row of a kind-2 tile (16 columns + 1 of pad)
+
+// Complex columns of a kind-2 item: at most 16, and few enough that the tile
+// (Nx rows of CT + 1 double2) stays near 36 KB, so several CTAs fit an SM.
+__host__ __device__ constexpr int be_cols(int nx, int ld)
+{
+    const int cap = nx >= 512 ? 4 : nx >= 256 ? 8 : 16;
+    return ld < cap ? ld : cap;
+}
 constexpr long long BE_WAIT_LIMIT = 1ll << 24;
 constexpr double kBePi = 3.1415926535897932;  // the reference's PI (General.h:14)
 
@@ -76,6 +84,11 @@ struct BeArgs {
     double Lx;
 };
 
+__device__ __forceinline__ void red_release_add(int* p)
+{
+    asm volatile("red.release.gpu.global.add.s32 [%0], 1;\n" ::"l"(p) : "memory");
+}
+
 __device__ __forceinline__ int ld_acquire(const int* p)
 {
     int v;
@@ -87,38 +100,31 @@ __device__ __forceinline__ int ld_acquire(const int* p)
 template <int LD>
 __device__ void be_rows_in(const BeArgs& a, const BeProblem& pr, const BeClass& c, int idx, double* sm)
 {
-    constexpr int NT = LD / 8, KK = LD / 4, NTW = (NT + 1) / 2;
+    constexpr int NT = LD / 8, KK = LD / 4;
     const int R = pr.nx < BE_ROWS ? pr.nx : BE_ROWS, x0 = idx * BE_ROWS, P = c.P, pitch = c.pitch;
     double* st = sm;  // [R][pitch]; the boundary slots stay zero (homogeneous Dirichlet)
     const double* f = a.f + pr.off + (long long)x0 * P;
-    for (int e = threadIdx.x; e < R * P; e += BE_THREADS) {
-        const int r = e / P, k = e - r * P;
-        st[r * pitch + k] = (k > 0 && k < P - 1) ? __ldg(f + e) : 0.0;
-    }
-    __syncthreads();
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, g = lane >> 2, q = lane & 3;
-    const int mt = warp & 3, fold = (warp >> 2) & 1, nt0 = warp >> 3;
-    if (mt * 8 < R && nt0 < NT) {
-        double acc[NTW][2];
+    for (int r = warp; r < R; r += BE_THREADS / 32)  // a warp per row, lanes along the row
+        for (int k = lane; k < P; k += 32) st[r * pitch + k] = (k > 0 && k < P - 1) ? __ldg(f + r * P + k) : 0.0;
+    __syncthreads();
+    const int mt = warp & 3, fold = warp >> 2;  // every n-tile of (m-tile, fold): one A fragment per k step
+    if (mt * 8 < R) {
+        double acc[NT][2];
 #pragma unroll
-        for (int t = 0; t < NTW; ++t) acc[t][0] = acc[t][1] = 0.0;
+        for (int t = 0; t < NT; ++t) acc[t][0] = acc[t][1] = 0.0;
         const double* row = st + (mt * 8 + g) * pitch;
         const double* B = c.first + (size_t)fold * NT * KK * 32;
 #pragma unroll
         for (int kk = 0; kk < KK; ++kk) {
             const double av = fold_value(row, nullptr, 4 * kk + q, fold, c.n, c.m, c.ms);
 #pragma unroll
-            for (int t = 0; t < NTW; ++t) {
-                const int nt = nt0 + 2 * t;
-                if (nt < NT) dmma_8x8x4(acc[t][0], acc[t][1], av, __ldg(B + (nt * KK + kk) * 32 + lane));
-            }
+            for (int nt = 0; nt < NT; ++nt) dmma_8x8x4(acc[nt][0], acc[nt][1], av, __ldg(B + (nt * KK + kk) * 32 + lane));
         }
         double* crow = a.C + pr.coff + (long long)(x0 + mt * 8 + g) * 2 * LD + fold * LD;
 #pragma unroll
-        for (int t = 0; t < NTW; ++t) {
-            const int nt = nt0 + 2 * t;
-            if (nt < NT) *reinterpret_cast<double2*>(crow + nt * 8 + 2 * q) = make_double2(acc[t][0], acc[t][1]);
-        }
+        for (int nt = 0; nt < NT; ++nt)
+            *reinterpret_cast<double2*>(crow + nt * 8 + 2 * q) = make_double2(acc[nt][0], acc[nt][1]);
     }
 }
 
@@ -136,23 +142,23 @@ template <int L>
 __device__ void be_columns(const BeArgs& a, const BeProblem& pr, const BeClass& c, int idx, double* sm)
 {
     constexpr int LOG2 = L == 8 ? 3 : L == 16 ? 4 : L == 32 ? 5 : L == 64 ? 6 : L == 128 ? 7 : L == 256 ? 8 : 9;
-    const int ld2 = 2 * c.ld, CT = c.ld < 16 ? c.ld : 16, col0 = idx * 2 * CT;
-    double2* z = reinterpret_cast<double2*>(sm);  // [L][BE_HS]
+    const int ld2 = 2 * c.ld, CT = be_cols(L, c.ld), col0 = idx * 2 * CT, HS = CT + 1;
+    double2* z = reinterpret_cast<double2*>(sm);  // [L][HS]
     double* Cb = a.C + pr.coff;
     for (int e = threadIdx.x; e < L * CT; e += BE_THREADS) {
         const int x = e / CT, cc = e - x * CT;
-        z[x * BE_HS + cc] = __ldcg(reinterpret_cast<const double2*>(Cb + (long long)x * ld2 + col0 + 2 * cc));
+        z[x * HS + cc] = __ldcg(reinterpret_cast<const double2*>(Cb + (long long)x * ld2 + col0 + 2 * cc));
     }
     __syncthreads();
     const double2* tw = a.tw[LOG2];
-    slab_fft<L, -1, BE_THREADS>(z, BE_HS, CT, tw);
+    slab_fft<L, -1, BE_THREADS>(z, HS, CT, tw);
     // real-to-complex split of each column pair, scaling, and the assembly of
     // the full-length spectrum for the inverse (imaginary parts dropped at
     // kx = 0 and L / 2)
     const double scale = 1.0 / L;
     for (int e = threadIdx.x; e < (L / 2 + 1) * CT; e += BE_THREADS) {
         const int kx = e / CT, cc = e - kx * CT, km = (L - kx) & (L - 1);
-        const double2 zk = z[kx * BE_HS + cc], zm = z[km * BE_HS + cc];
+        const double2 zk = z[kx * HS + cc], zm = z[km * HS + cc];
         double2 X = make_double2(0.5 * (zk.x + zm.x), 0.5 * (zk.y - zm.y));
         double2 Y = make_double2(0.5 * (zk.y + zm.y), 0.5 * (zm.x - zk.x));
         const double sig = pr.lam + 4.0 * kBePi * kBePi * kx * kx / (a.Lx * a.Lx);
@@ -160,14 +166,14 @@ __device__ void be_columns(const BeArgs& a, const BeProblem& pr, const BeClass& 
         X = make_double2(X.x * r0, X.y * r0);
         Y = make_double2(Y.x * r1, Y.y * r1);
         if (kx == 0 || kx == L / 2) { X.y = 0.0; Y.y = 0.0; }
-        z[kx * BE_HS + cc] = make_double2(X.x - Y.y, X.y + Y.x);
-        if (kx > 0 && kx < L / 2) z[km * BE_HS + cc] = make_double2(X.x + Y.y, Y.x - X.y);
+        z[kx * HS + cc] = make_double2(X.x - Y.y, X.y + Y.x);
+        if (kx > 0 && kx < L / 2) z[km * HS + cc] = make_double2(X.x + Y.y, Y.x - X.y);
     }
     __syncthreads();
-    slab_fft<L, 1, BE_THREADS>(z, BE_HS, CT, tw);
+    slab_fft<L, 1, BE_THREADS>(z, HS, CT, tw);
     for (int e = threadIdx.x; e < L * CT; e += BE_THREADS) {
         const int x = e / CT, cc = e - x * CT;
-        __stcg(reinterpret_cast<double2*>(Cb + (long long)x * ld2 + col0 + 2 * cc), z[x * BE_HS + cc]);
+        __stcg(reinterpret_cast<double2*>(Cb + (long long)x * ld2 + col0 + 2 * cc), z[x * HS + cc]);
     }
 }
 
@@ -175,7 +181,7 @@ __device__ void be_columns(const BeArgs& a, const BeProblem& pr, const BeClass& 
 template <int LD>
 __device__ void be_rows_out(const BeArgs& a, const BeProblem& pr, const BeClass& c, int idx, double* sm)
 {
-    constexpr int NT = LD / 8, KK = LD / 4, NTW = (NT + 1) / 2, PITCH = 2 * LD + 4;
+    constexpr int NT = LD / 8, KK = LD / 4, PITCH = 2 * LD + 4;
     const int R = pr.nx < BE_ROWS ? pr.nx : BE_ROWS, x0 = idx * BE_ROWS, P = c.P;
     double* cin = sm;                   // [R][PITCH] coefficients
     double* vout = sm + R * PITCH;      // [R][PITCH] transformed values: s | d
@@ -187,47 +193,43 @@ __device__ void be_rows_out(const BeArgs& a, const BeProblem& pr, const BeClass&
     }
     __syncthreads();
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, g = lane >> 2, q = lane & 3;
-    const int mt = warp & 3, fold = (warp >> 2) & 1, nt0 = warp >> 3;
-    if (mt * 8 < R && nt0 < NT) {
-        double acc[NTW][2];
+    const int mt = warp & 3, fold = warp >> 2;
+    if (mt * 8 < R) {
+        double acc[NT][2];
 #pragma unroll
-        for (int t = 0; t < NTW; ++t) acc[t][0] = acc[t][1] = 0.0;
+        for (int t = 0; t < NT; ++t) acc[t][0] = acc[t][1] = 0.0;
         const double* row = cin + (mt * 8 + g) * PITCH + fold * LD;
         const double* B = c.second + (size_t)fold * NT * KK * 32;
 #pragma unroll
         for (int kk = 0; kk < KK; ++kk) {
             const double av = row[4 * kk + q];
 #pragma unroll
-            for (int t = 0; t < NTW; ++t) {
-                const int nt = nt0 + 2 * t;
-                if (nt < NT) dmma_8x8x4(acc[t][0], acc[t][1], av, __ldg(B + (nt * KK + kk) * 32 + lane));
-            }
+            for (int nt = 0; nt < NT; ++nt) dmma_8x8x4(acc[nt][0], acc[nt][1], av, __ldg(B + (nt * KK + kk) * 32 + lane));
         }
         double* orow = vout + (mt * 8 + g) * PITCH + fold * LD;
 #pragma unroll
-        for (int t = 0; t < NTW; ++t) {
-            const int nt = nt0 + 2 * t;
-            if (nt < NT) *reinterpret_cast<double2*>(orow + nt * 8 + 2 * q) = make_double2(acc[t][0], acc[t][1]);
-        }
+        for (int nt = 0; nt < NT; ++nt)
+            *reinterpret_cast<double2*>(orow + nt * 8 + 2 * q) = make_double2(acc[nt][0], acc[nt][1]);
     }
     __syncthreads();
     const int n = c.n, m = c.m, ms = c.ms;
     double* u = a.u + pr.off + (long long)x0 * P;
-    for (int e = threadIdx.x; e < R * P; e += BE_THREADS) {
-        const int r = e / P, k = e - r * P;
+    for (int r = warp; r < R; r += BE_THREADS / 32) {
         const double* s = vout + r * PITCH;
-        double v = 0.0;
-        if (k > 0 && k < P - 1) {
-            const int j = k - 1;
-            if (j < m) v = kR2 * (s[j] + s[LD + j]);
-            else if (j < ms) v = s[j];
-            else v = kR2 * (s[n - 1 - j] - s[LD + n - 1 - j]);
+        for (int k = lane; k < P; k += 32) {
+            double v = 0.0;
+            if (k > 0 && k < P - 1) {
+                const int j = k - 1;
+                if (j < m) v = kR2 * (s[j] + s[LD + j]);
+                else if (j < ms) v = s[j];
+                else v = kR2 * (s[n - 1 - j] - s[LD + n - 1 - j]);
+            }
+            u[r * P + k] = v;
         }
-        u[e] = v;
     }
 }
 
-__global__ void __launch_bounds__(BE_THREADS, 1) batch_eig_kernel(BeArgs a)
+__global__ void __launch_bounds__(BE_THREADS, BE_MINB) batch_eig_kernel(BeArgs a)
 {
     extern __shared__ __align__(16) double bsm[];
     __shared__ int s_item, s_ok;
@@ -282,10 +284,9 @@ __global__ void __launch_bounds__(BE_THREADS, 1) batch_eig_kernel(BeArgs a)
                 }
             }
         }
-        // publish: every thread's writes before the counter moves
-        __threadfence();
+        // publish: the CTA's writes, then one release increment of the counter
         __syncthreads();
-        if (threadIdx.x == 0 && kind < 3) atomicAdd(kind == 1 ? &a.done1[b] : &a.done2[b], 1);
+        if (threadIdx.x == 0 && kind < 3) red_release_add(kind == 1 ? &a.done1[b] : &a.done2[b]);
     }
 }
 
@@ -433,12 +434,12 @@ int batch_eig_create(int nprob, const int* Nx, const int* N, const double* lambd
         p.nx = Nx[i];
         p.cls = ci;
         p.nchunk = (Nx[i] + BE_ROWS - 1) / BE_ROWS;
-        p.ngroup = c.ld <= 16 ? 1 : c.ld / 16;
+        p.ngroup = c.ld / be_cols(Nx[i], c.ld);
         coff += (long long)Nx[i] * 2 * c.ld;
         const int R = std::min(Nx[i], BE_ROWS);
         smem = std::max(smem, (size_t)R * c.pitch * sizeof(double));
         smem = std::max(smem, (size_t)2 * R * (2 * c.ld + 4) * sizeof(double));
-        smem = std::max(smem, (size_t)Nx[i] * BE_HS * sizeof(double2));
+        smem = std::max(smem, (size_t)Nx[i] * (be_cols(Nx[i], c.ld) + 1) * sizeof(double2));
     }
     if (st) {
         be->release();
@@ -520,7 +521,7 @@ int batch_eig_solve(BatchEig* be, const double* f, double* u, cudaStream_t s)
     a.u = u;
     cudaError_t e = cudaMemsetAsync(be->d_counters, 0, be->counter_bytes, s);
     if (e == cudaSuccess) {
-        const int grid = std::min(be->nsm, be->nitems);
+        const int grid = std::min(BE_MINB * be->nsm, be->nitems);
         e = launch_k(batch_eig_kernel, dim3(grid), dim3(BE_THREADS), be->smem, s, a);
     }
     if (e != cudaSuccess) {

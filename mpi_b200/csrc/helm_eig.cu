@@ -88,8 +88,11 @@ __device__ __forceinline__ void load_plane(const EigArgs& a, const double* f, co
 // slots 0..31 (symmetric fold) and 32..63 (antisymmetric fold).
 template <int MTW>
 __device__ __forceinline__ void first_transform(const EigArgs& a, double* rows, const double* Ms, const double* Ma,
-                                                const double* hbc, int lane)
+                                                const double* hbc, int lane, int in_off = 0)
 {
+    // the staged rows start in_off doubles into each row (a TMA copy whose
+    // source began 8 bytes before the row); the coefficients go to slot 0 on
+    const double* src = rows + in_off;
     const int g = lane >> 2, q = lane & 3;
     const int n = a.n, m = a.m, ms = a.ms, P = a.P;
     double cs[MTW][4][2], ca[MTW][4][2];
@@ -103,7 +106,7 @@ __device__ __forceinline__ void first_transform(const EigArgs& a, double* rows, 
         double as[MTW], aa[MTW];
 #pragma unroll
         for (int mt = 0; mt < MTW; ++mt) {
-            const double* row = rows + (mt * 8 + g) * EP_PITCH;
+            const double* row = src + (mt * 8 + g) * EP_PITCH;
             double vs = 0.0, va = 0.0;
             if (k < m) {
                 const double lo = row[1 + k], hi = row[n - k];
@@ -128,7 +131,7 @@ __device__ __forceinline__ void first_transform(const EigArgs& a, double* rows, 
     double zl[MTW], zr[MTW];
 #pragma unroll
     for (int mt = 0; mt < MTW; ++mt) {
-        const double* row = rows + (mt * 8 + g) * EP_PITCH;
+        const double* row = src + (mt * 8 + g) * EP_PITCH;
         zl[mt] = row[0];
         zr[mt] = row[P - 1];
     }
@@ -231,32 +234,91 @@ __device__ __forceinline__ void r2c_split(const double2* z, int warp, int lane, 
 template <int L, typename Fetch>
 __device__ __forceinline__ void c2r_assemble(double2* z, int warp, int lane, Fetch fetch)
 {
-    for (int kx = warp; kx <= L / 2; kx += EpShape<L>::WARPS) {
-        double2 X, Y;
-        fetch(kx, lane, X, Y);
-        if (kx == 0 || kx == L / 2) { X.y = 0.0; Y.y = 0.0; }
-        z[kx * EP_HS + lane] = make_double2(X.x - Y.y, X.y + Y.x);
-        if (kx > 0 && kx < L / 2) z[(L - kx) * EP_HS + lane] = make_double2(X.x + Y.y, Y.x - X.y);
+    // three rows per round, fetched before any is used
+    constexpr int W = EpShape<L>::WARPS, NB = 3;
+    for (int k0 = warp; k0 <= L / 2; k0 += NB * W) {
+        double2 X[NB], Y[NB];
+#pragma unroll
+        for (int b = 0; b < NB; ++b)
+            if (k0 + b * W <= L / 2) fetch(k0 + b * W, lane, X[b], Y[b]);
+#pragma unroll
+        for (int b = 0; b < NB; ++b) {
+            const int kx = k0 + b * W;
+            if (kx > L / 2) break;
+            if (kx == 0 || kx == L / 2) { X[b].y = 0.0; Y[b].y = 0.0; }
+            z[kx * EP_HS + lane] = make_double2(X[b].x - Y[b].y, X[b].y + Y[b].x);
+            if (kx > 0 && kx < L / 2) z[(L - kx) * EP_HS + lane] = make_double2(X[b].x + Y[b].y, Y[b].x - X[b].y);
+        }
     }
 }
 
 // ------------------------------------------------------------------ pass 1 --
+// Tensor map of pass 1 (kernel parameter, built on the host per solve): f as
+// [Nx][x_stride] doubles, box EP_PITCH x (Nx / 4) (x / 4 rows of one plane).
+struct EigMaps {
+    CUtensorMap f;
+};
+
 template <int L>
-__global__ void __launch_bounds__(EpShape<L>::THREADS, 1) eig_fwd_kernel(EigArgs a)
+struct FwdBoxes {
+    static constexpr int NQ = L >= 32 ? 4 : 1;  // TMA boxes per plane (row quarters)
+    static constexpr int QR = L / NQ;           // rows per box
+};
+
+template <int L>
+__global__ void __launch_bounds__(EpShape<L>::THREADS, 1) eig_fwd_kernel(EigArgs a, const __grid_constant__ EigMaps tm)
 {
     using S = EpShape<L>;
-    extern __shared__ __align__(16) double esm[];
+    using B = FwdBoxes<L>;
+    extern __shared__ __align__(128) double esm[];
+    __shared__ __align__(8) uint64_t bar[B::NQ];
     double* buf = esm;
     double* Mt = esm + (size_t)L * EP_PITCH;
-    copy_mats(Mt, a.mats, 0, 2);
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int y = blockIdx.x;
+    const bool tma = a.tma != 0;
+    if (tma && threadIdx.x == 0) {
+        for (int q = 0; q < B::NQ; ++q) mbar_init(&bar[q], 1);
+        fence_mbar_init();
+    }
+    copy_mats(Mt, a.mats, 0, 2);
+    __syncthreads();
     pdl_enter();
     if (a.lam_out && blockIdx.x == 0 && threadIdx.x == 0) *a.lam_out = 0.0;
-    load_plane<L>(a, a.f, a.adjoint ? nullptr : a.gl, a.adjoint ? nullptr : a.gr, (long long)y * a.P, y, buf);
+    double* rows = buf + warp * S::RW * EP_PITCH;
+    bool tma_ok = true;
+    if (tma) {
+        // the plane in four boxes (one bulk copy each); a warp starts on its
+        // rows as soon as their box has landed.  The copies start at the
+        // 16-byte boundary at or before the plane's first element: element k
+        // of a row lands in slot k + sh.
+        const int sh = (int)(((long long)y * a.P) & 1);
+        if (threadIdx.x == 0) {
+            const int c0 = y * a.P - sh;
+            for (int q = 0; q < B::NQ; ++q) {
+                mbar_arrive_expect_tx(&bar[q], (uint32_t)(B::QR * EP_PITCH * sizeof(double)));
+                tma_load_2d(buf + (size_t)q * B::QR * EP_PITCH, &tm.f, c0, q * B::QR, &bar[q]);
+            }
+        }
+        tma_ok = mbar_wait(&bar[(warp * S::RW) / B::QR], 0);
+        if (!tma_ok && lane == 0 && a.err) atomicExch(a.err, 1);
+        const double* gl = a.adjoint ? nullptr : a.gl;
+        const double* gr = a.adjoint ? nullptr : a.gr;
+        if (lane < S::RW) {  // the GLL boundary slots take zl = gl / beta_l, zr = gr / beta_r
+            const long long x = (long long)warp * S::RW + lane;
+            rows[lane * EP_PITCH + sh] = gl ? gl[x * a.bc_x_stride + y] * a.ibl : 0.0;
+            rows[lane * EP_PITCH + sh + a.P - 1] = gr ? gr[x * a.bc_x_stride + y] * a.ibr : 0.0;
+        }
+        __syncwarp();
+        if (tma_ok) first_transform<S::MTW>(a, rows, Mt, Mt + EP_FRAG, a.hbc, lane, sh);
+    } else {
+        load_plane<L>(a, a.f, a.adjoint ? nullptr : a.gl, a.adjoint ? nullptr : a.gr, (long long)y * a.P, y, buf);
+        __syncthreads();
+        first_transform<S::MTW>(a, rows, Mt, Mt + EP_FRAG, a.hbc, lane);
+    }
     __syncthreads();
-    first_transform<S::MTW>(a, buf + warp * S::RW * EP_PITCH, Mt, Mt + EP_FRAG, a.hbc, lane);
-    __syncthreads();
+    if (tma && threadIdx.x == 0 && !tma_ok)  // copies still in flight land before the CTA ends
+        for (int q = 0; q < B::NQ; ++q) mbar_wait(&bar[q], 0);
     double2* z = reinterpret_cast<double2*>(buf);
     slab_fft<L, -1, S::THREADS>(z, EP_HS, 32, static_cast<const double2*>(a.tw_x));
     double2* Sg = reinterpret_cast<double2*>(a.S);
@@ -269,8 +331,11 @@ __global__ void __launch_bounds__(EpShape<L>::THREADS, 1) eig_fwd_kernel(EigArgs
 }
 
 // ------------------------------------------------------------------ pass 2 --
-template <int NY, int CT>
-__global__ void __launch_bounds__(256) eig_conv_kernel(EigArgs a)
+// CTA shapes of pass 2: 16 coefficient columns per tile and 256 threads (two
+// CTAs per SM), or 8 columns and 128 threads (four per SM, more tiles in
+// flight); launch variant bit 0 of the y pass picks one.
+template <int NY, int CT, int THREADS>
+__global__ void __launch_bounds__(THREADS, 512 / THREADS) eig_conv_kernel(EigArgs a)
 {
     extern __shared__ __align__(16) double esm[];
     double2* sm = reinterpret_cast<double2*>(esm);
@@ -283,19 +348,26 @@ __global__ void __launch_bounds__(256) eig_conv_kernel(EigArgs a)
         cp_async_bytes16(&sm[ky * CT + c], &Sg[(long long)ky * EIG_SLOTS + c], true);
     }
     cp_async_commit();
+    // this thread's scale factors, fetched while the tile is in flight
+    constexpr int PER = (NY * CT + THREADS - 1) / THREADS;
+    double r[PER];
+    const double* rc = a.recip;
+#pragma unroll
+    for (int k = 0; k < PER; ++k) {
+        const int e = threadIdx.x + THREADS * k, ky = e / CT, c = e - ky * CT;
+        r[k] = e < NY * CT ? rc[(long long)a.grp_of_row[kx * NY + ky] * EIG_SLOTS + j0 + c] * a.scale : 0.0;
+    }
     cp_async_wait_all();
     __syncthreads();
     const double2* tw = static_cast<const double2*>(a.tw_y);
-    slab_fft<NY, -1, 256>(sm, CT, CT, tw);
-    const double* rc = a.recip;
-    for (int e = threadIdx.x; e < NY * CT; e += blockDim.x) {
-        const int ky = e / CT, c = e - ky * CT;
-        const double r = rc[(long long)a.grp_of_row[kx * NY + ky] * EIG_SLOTS + j0 + c] * a.scale;
-        const double2 v = sm[ky * CT + c];
-        sm[ky * CT + c] = make_double2(v.x * r, v.y * r);
+    slab_fft<NY, -1, THREADS>(sm, CT, CT, tw);
+#pragma unroll
+    for (int k = 0; k < PER; ++k) {
+        const int e = threadIdx.x + THREADS * k;
+        if (e < NY * CT) sm[e] = make_double2(sm[e].x * r[k], sm[e].y * r[k]);
     }
     __syncthreads();
-    slab_fft<NY, 1, 256>(sm, CT, CT, tw);
+    slab_fft<NY, 1, THREADS>(sm, CT, CT, tw);
     for (int e = threadIdx.x; e < NY * CT; e += blockDim.x) {
         const int ky = e / CT, c = e - ky * CT;
         Sg[(long long)ky * EIG_SLOTS + c] = sm[ky * CT + c];
@@ -490,431 +562,10 @@ __global__ void __launch_bounds__(EpShape<L>::THREADS, 1) eig_solve2d_kernel(Eig
     if (a.lam_out) eig_lambda_sum(a, acc);
 }
 
-// Tensor maps of one solve (kernel parameter, built on the host per call).
-struct EigMaps {
-    CUtensorMap f;    // pass 1: f as [Nx][x_stride] doubles, box 68 x 16
-    CUtensorMap sub;  // pass 1, misfit adjoint: u_obs, the same
-    CUtensorMap S;    // pass 3: S as [nkx][Ny][128] doubles, box 128 x 1 x 16
-    CUtensorMap T;    // pass 2: the same array, box 2 CT x min(Ny, 256) x 1
-};
-
-// ------------------------------------------------ persistent TMA passes --
-// Row variant 5: the three 3D passes as persistent kernels, one CTA per SM,
-// each with one producer warp that moves tiles by TMA (cp.async.bulk.tensor)
-// through a ring of shared-memory slots guarded by mbarriers, and consumer
-// warps that transform them.  A CTA works through its share of planes (passes
-// 1 and 3) or tiles (pass 2) while the producer already fetches the next ones,
-// so HBM latency hides behind the FP64 tensor-core and FFT work.
-//   pass 1: f rows in 16-row chunks (tensor map over f, box 68 x 16; the
-//           chunk's first element rounded down to a 16-byte boundary, the
-//           shift taken out in shared memory) -> fold, first transform on the
-//           FP64 tensor cores -> the plane's coefficient rows; then the x FFT
-//           and plain stores of the coefficient spectrum S[kx][y][64];
-//   pass 2: (kx, 16 coefficient slots) tiles of S (box 32 x Ny x 1) ->
-//           y FFT, scaling, inverse y FFT in place -> TMA store of the tile;
-//   pass 3: S rows of plane y in 16-kx chunks (box 128 x 1 x 16) -> full
-//           spectra of the 32 column pairs -> inverse x FFT, second transform,
-//           unfold, stores of u.
-// Every wait is bounded (kTmaWaitLimit); a wait that runs out records an
-// error in *a.err, and later waits of the CTA return at once, so the kernel
-// ends with every named barrier still met.
-constexpr int TP_PITCH = EP_PITCH;   // doubles per staged f row = box inner extent (68)
-constexpr int TP_F_SLOTS = 8;        // pass 1 ring: f chunks (pairs of slots: f and u_obs, misfit adjoint)
-constexpr int TP_S_SLOTS = 4;        // pass 3 ring: S chunks
-constexpr int TP_C_SLOTS = 3;        // pass 2 ring: S tiles
-
-template <int L>
-struct TmaShape {
-    using E = EpShape<L>;
-    static constexpr int CW = E::WARPS;            // consumer warps
-    static constexpr int CT = E::THREADS;          // consumer threads
-    static constexpr int THREADS = CT + 32;        // + the producer warp
-    static constexpr int RC = L < 16 ? L : 16;     // f rows per chunk (pass 1)
-    static constexpr int NCH1 = L / RC;
-    static constexpr int KC = 16;                  // kx rows per S chunk (pass 3)
-    static constexpr int NCH3 = (L / 2) / KC + 1;  // chunks covering kx = 0 .. L/2
-    static constexpr size_t plane = (size_t)L * TP_PITCH * sizeof(double);
-    static constexpr size_t fslot = (size_t)RC * TP_PITCH * sizeof(double);
-    static constexpr size_t sslot = (size_t)KC * 2 * EIG_SLOTS * sizeof(double);
-    static constexpr size_t mats = 2 * EP_FRAG * sizeof(double);
-    static constexpr size_t smem1 = plane + TP_F_SLOTS * fslot + mats + 2 * TP_F_SLOTS * sizeof(uint64_t);
-    static constexpr size_t smem3 = plane + TP_S_SLOTS * sslot + mats + 2 * TP_S_SLOTS * sizeof(uint64_t);
-};
-
-// Bounded wait of a consumer or producer; false (and the error recorded) once
-// any wait of the CTA has run out.
-__device__ __forceinline__ bool tp_wait(uint64_t* bar, uint32_t parity, volatile int* s_err, int* err, int code)
-{
-    if (*s_err) return false;
-    if (mbar_wait(bar, parity)) return true;
-    *s_err = 1;
-    if (err) atomicExch(err, code);
-    return false;
-}
-
-__device__ __forceinline__ void mbar_arrive(uint64_t* bar)
-{
-    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];\n" ::"r"(smem_u32(bar)) : "memory");
-}
-
-template <int THREADS>
-__device__ __forceinline__ void consumers_sync()
-{
-    asm volatile("bar.sync 1, %0;\n" ::"n"(THREADS) : "memory");
-}
-
-template <int L>
-__global__ void __launch_bounds__(TmaShape<L>::THREADS, 1)
-    eig_fwd_tma_kernel(EigArgs a, const __grid_constant__ EigMaps tm)
-{
-    using T = TmaShape<L>;
-    extern __shared__ __align__(1024) unsigned char tsm[];
-    double* coef = reinterpret_cast<double*>(tsm);                                   // [L][68]
-    double* ring = reinterpret_cast<double*>(tsm + T::plane);                         // [8][RC][68]
-    double* Mt = reinterpret_cast<double*>(tsm + T::plane + TP_F_SLOTS * T::fslot);   // first transforms, sym | anti
-    uint64_t* full = reinterpret_cast<uint64_t*>(tsm + T::plane + TP_F_SLOTS * T::fslot + T::mats);
-    uint64_t* empty = full + TP_F_SLOTS;
-    __shared__ int s_err;
-    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    const int P = a.P, n = a.n, m = a.m, ms = a.ms, Ny = a.Ny;
-    const bool sub = a.sub != nullptr;
-    const int nslot = sub ? TP_F_SLOTS / 2 : TP_F_SLOTS;   // chunk slots (doubled in the misfit adjoint)
-    if (tid == 0) {
-        s_err = 0;
-        for (int i = 0; i < TP_F_SLOTS; ++i) {
-            mbar_init(&full[i], 1);
-            mbar_init(&empty[i], T::CW);
-        }
-        fence_mbar_init();
-    }
-    copy_mats(Mt, a.mats, 0, 2);
-    __syncthreads();
-    pdl_enter();
-    if (a.lam_out && blockIdx.x == 0 && tid == 0) *a.lam_out = 0.0;
-    if (warp == T::CW) {
-        // producer: every chunk of every plane of this CTA, in order
-        int i = 0;
-        for (int y = blockIdx.x; y < Ny; y += gridDim.x) {
-            const int c0 = y * P - ((y * P) & 1);
-            for (int c = 0; c < T::NCH1; ++c, ++i) {
-                const int s = i % nslot;
-                const uint32_t par = ((i / nslot) & 1) ^ 1;
-                if (lane == 0 && tp_wait(&empty[s], par, &s_err, a.err, 1)) {
-                    double* dst = ring + (size_t)s * (sub ? 2 : 1) * T::RC * TP_PITCH;
-                    mbar_arrive_expect_tx(&full[s], (uint32_t)((sub ? 2 : 1) * T::fslot));
-                    tma_load_2d(dst, &tm.f, c0, c * T::RC, &full[s]);
-                    if (sub) tma_load_2d(dst + T::RC * TP_PITCH, &tm.sub, c0, c * T::RC, &full[s]);
-                }
-                __syncwarp();
-            }
-        }
-        // every load issued has landed before the CTA may end (consumers wait
-        // for each; after an error, wait here for the last ones in flight)
-        if (lane == 0 && s_err) {
-            const int last = i;
-            for (int j = (last > nslot ? last - nslot : 0); j < last; ++j) mbar_wait(&full[j % nslot], (j / nslot) & 1);
-        }
-    } else {
-        const int g = lane >> 2, q = lane & 3;
-        const double* gl = a.adjoint ? nullptr : a.gl;
-        const double* gr = a.adjoint ? nullptr : a.gr;
-        int i = 0;
-        for (int y = blockIdx.x; y < Ny; y += gridDim.x) {
-            const int sh = (y * P) & 1;
-            for (int c = 0; c < T::NCH1; ++c, ++i) {
-                const int s = i % nslot;
-                const bool ok = tp_wait(&full[s], (i / nslot) & 1, &s_err, a.err, 2);
-                const double* st = ring + (size_t)s * (sub ? 2 : 1) * T::RC * TP_PITCH;
-                for (int t = warp; ok && t < (T::RC / 8) * 8; t += T::CW) {
-                    const int mt = t >> 3, ntg = t & 7, fold = ntg >> 2, nt = ntg & 3;
-                    const double* Mb = Mt + fold * EP_FRAG;
-                    const int r = mt * 8 + g;
-                    const double* rowp = st + r * TP_PITCH + sh;
-                    const double* rows = sub ? rowp + T::RC * TP_PITCH : nullptr;
-                    double c0 = 0.0, c1 = 0.0, d0 = 0.0, d1 = 0.0;
-#pragma unroll
-                    for (int kk = 0; kk < 8; kk += 2) {
-                        const double v0 = fold_value(rowp, rows, 4 * kk + q, fold, n, m, ms);
-                        const double v1 = fold_value(rowp, rows, 4 * kk + 4 + q, fold, n, m, ms);
-                        dmma_8x8x4(c0, c1, v0, Mb[(nt * 8 + kk) * 32 + lane]);
-                        dmma_8x8x4(d0, d1, v1, Mb[(nt * 8 + kk + 1) * 32 + lane]);
-                    }
-                    const long long x = (long long)c * T::RC + r;
-                    const int i0 = nt * 8 + 2 * q;
-                    double o0 = c0 + d0, o1 = c1 + d1;
-                    if (gl) {
-                        const double zl = gl[x * a.bc_x_stride + y] * a.ibl;
-                        o0 += zl * a.hbc[fold * 2 * EIG_LD + i0];
-                        o1 += zl * a.hbc[fold * 2 * EIG_LD + i0 + 1];
-                    }
-                    if (gr) {
-                        const double zr = gr[x * a.bc_x_stride + y] * a.ibr;
-                        o0 += zr * a.hbc[fold * 2 * EIG_LD + EIG_LD + i0];
-                        o1 += zr * a.hbc[fold * 2 * EIG_LD + EIG_LD + i0 + 1];
-                    }
-                    *reinterpret_cast<double2*>(coef + x * TP_PITCH + ntg * 8 + 2 * q) = make_double2(o0, o1);
-                }
-                __syncwarp();
-                if (lane == 0) mbar_arrive(&empty[s]);
-            }
-            consumers_sync<T::CT>();
-            double2* z = reinterpret_cast<double2*>(coef);
-            slab_fft<L, -1, T::CT, 1>(z, EP_HS, 32, static_cast<const double2*>(a.tw_x));
-            double2* Sg = reinterpret_cast<double2*>(a.S);
-            r2c_split<L>(z, warp, lane, [&](int kx, int cc, double2 X, double2 Y) {
-                double2* row = Sg + ((long long)kx * Ny + y) * EIG_SLOTS;
-                row[2 * cc] = X;
-                row[2 * cc + 1] = Y;
-            });
-            consumers_sync<T::CT>();  // the coefficient rows are rewritten by the next plane
-        }
-    }
-}
-
-template <int L>
-__global__ void __launch_bounds__(TmaShape<L>::THREADS, 1)
-    eig_inv_tma_kernel(EigArgs a, const __grid_constant__ EigMaps tm)
-{
-    using T = TmaShape<L>;
-    using S = EpShape<L>;
-    extern __shared__ __align__(1024) unsigned char tsm[];
-    double* buf = reinterpret_cast<double*>(tsm);                                   // [L][68]
-    double* ring = reinterpret_cast<double*>(tsm + T::plane);                        // [4][16][128]
-    double* Mt = reinterpret_cast<double*>(tsm + T::plane + TP_S_SLOTS * T::sslot);  // second transforms
-    uint64_t* full = reinterpret_cast<uint64_t*>(tsm + T::plane + TP_S_SLOTS * T::sslot + T::mats);
-    uint64_t* empty = full + TP_S_SLOTS;
-    __shared__ int s_err;
-    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    const int Ny = a.Ny;
-    if (tid == 0) {
-        s_err = 0;
-        for (int i = 0; i < TP_S_SLOTS; ++i) {
-            mbar_init(&full[i], 1);
-            mbar_init(&empty[i], T::CW);
-        }
-        fence_mbar_init();
-    }
-    copy_mats(Mt, a.mats, 1, 3);
-    __syncthreads();
-    pdl_enter();
-    double lam_acc = 0.0;
-    if (warp == T::CW) {
-        int i = 0;
-        for (int y = blockIdx.x; y < Ny; y += gridDim.x)
-            for (int c = 0; c < T::NCH3; ++c, ++i) {
-                const int s = i % TP_S_SLOTS;
-                if (lane == 0 && tp_wait(&empty[s], ((i / TP_S_SLOTS) & 1) ^ 1, &s_err, a.err, 3)) {
-                    mbar_arrive_expect_tx(&full[s], (uint32_t)T::sslot);
-                    tma_load_3d(ring + (size_t)s * T::KC * 2 * EIG_SLOTS, &tm.S, 0, y, c * T::KC, &full[s]);
-                }
-                __syncwarp();
-            }
-        if (lane == 0 && s_err) {
-            const int last = i;
-            for (int j = (last > TP_S_SLOTS ? last - TP_S_SLOTS : 0); j < last; ++j)
-                mbar_wait(&full[j % TP_S_SLOTS], (j / TP_S_SLOTS) & 1);
-        }
-    } else {
-        double2* z = reinterpret_cast<double2*>(buf);
-        double* rows = buf + warp * S::RW * EP_PITCH;
-        int i = 0;
-        for (int y = blockIdx.x; y < Ny; y += gridDim.x) {
-            for (int c = 0; c < T::NCH3; ++c, ++i) {
-                const int s = i % TP_S_SLOTS;
-                const bool ok = tp_wait(&full[s], (i / TP_S_SLOTS) & 1, &s_err, a.err, 4);
-                const double2* st = reinterpret_cast<const double2*>(ring + (size_t)s * T::KC * 2 * EIG_SLOTS);
-                // full-length spectra Z = X + i Y of the column pairs (imaginary
-                // parts dropped at kx = 0 and L / 2, as the real part of the
-                // reference's inverse transform does)
-                for (int e = tid; ok && e < T::KC * 32; e += T::CT) {
-                    const int r = e >> 5, cc = e & 31, kx = c * T::KC + r;
-                    if (kx > L / 2) continue;
-                    double2 X = st[r * EIG_SLOTS + 2 * cc], Y = st[r * EIG_SLOTS + 2 * cc + 1];
-                    if (kx == 0 || kx == L / 2) { X.y = 0.0; Y.y = 0.0; }
-                    z[kx * EP_HS + cc] = make_double2(X.x - Y.y, X.y + Y.x);
-                    if (kx > 0 && kx < L / 2) z[(L - kx) * EP_HS + cc] = make_double2(X.x + Y.y, Y.x - X.y);
-                }
-                __syncwarp();
-                if (lane == 0) mbar_arrive(&empty[s]);
-            }
-            consumers_sync<T::CT>();
-            slab_fft<L, 1, T::CT, 1>(z, EP_HS, 32, static_cast<const double2*>(a.tw_x));
-            if (!a.adjoint) {
-                second_transform<S::MTW>(a, rows, Mt, Mt + EP_FRAG, lane);
-                store_plane_rows<L>(a, a.u, a.gl, a.gr, (long long)y * a.P, y, rows, warp * S::RW, lane);
-            } else {
-                double dl = 0.0, dr = 0.0;
-                adjoint_boundary_dots<L>(a, rows, lane, &dl, &dr);
-                __syncwarp();
-                second_transform<S::MTW>(a, rows, Mt, Mt + EP_FRAG, lane);
-                lam_acc += store_adjoint_rows<L>(a, a.u, a.f, (long long)y * a.P, y, rows, warp * S::RW, lane, dl, dr);
-            }
-            consumers_sync<T::CT>();  // the plane buffer is rewritten by the next plane
-        }
-    }
-    if (a.lam_out) eig_lambda_sum(a, lam_acc);
-}
-
-template <int NY, int CT>
-struct ConvShape {
-    static constexpr int CONS = 256;                       // consumer threads
-    static constexpr int THREADS = CONS + 32;
-    static constexpr int TILES_PER_KX = EIG_SLOTS / CT;
-    static constexpr int BOX_Y = NY < 256 ? NY : 256;
-    static constexpr size_t tile = (size_t)NY * CT * sizeof(double2);
-    static constexpr size_t smem = TP_C_SLOTS * tile + 2 * TP_C_SLOTS * sizeof(uint64_t);
-    static constexpr int PER = (NY * CT + CONS - 1) / CONS;  // elements scaled per consumer thread
-};
-
-template <int NY, int CT>
-__global__ void __launch_bounds__(ConvShape<NY, CT>::THREADS, 1)
-    eig_conv_tma_kernel(EigArgs a, const __grid_constant__ EigMaps tm)
-{
-    using C = ConvShape<NY, CT>;
-    extern __shared__ __align__(1024) unsigned char tsm[];
-    double2* ring = reinterpret_cast<double2*>(tsm);
-    uint64_t* full = reinterpret_cast<uint64_t*>(tsm + TP_C_SLOTS * C::tile);
-    uint64_t* done = full + TP_C_SLOTS;
-    __shared__ int s_err;
-    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    const int ntiles = a.nkx * C::TILES_PER_KX;
-    int mine = 0;
-    for (int t = blockIdx.x; t < ntiles; t += gridDim.x) ++mine;
-    if (tid == 0) {
-        s_err = 0;
-        for (int i = 0; i < TP_C_SLOTS; ++i) {
-            mbar_init(&full[i], 1);
-            mbar_init(&done[i], 1);
-        }
-        fence_mbar_init();
-    }
-    __syncthreads();
-    pdl_enter();
-    auto coords = [&](int i, int& kx, int& j0) {
-        const int t = blockIdx.x + i * gridDim.x;
-        kx = t / C::TILES_PER_KX;
-        j0 = (t - kx * C::TILES_PER_KX) * CT;
-    };
-    if (warp == C::CONS / 32) {
-        if (lane == 0) {
-            for (int i = 0; i < mine + TP_C_SLOTS; ++i) {
-                if (i >= TP_C_SLOTS) {  // tile i - SLOTS solved: store it back
-                    const int j = i - TP_C_SLOTS, s = j % TP_C_SLOTS;
-                    if (tp_wait(&done[s], (j / TP_C_SLOTS) & 1, &s_err, a.err, 5)) {
-                        int kx, j0;
-                        coords(j, kx, j0);
-                        for (int yb = 0; yb < NY; yb += C::BOX_Y)
-                            tma_store_3d(&tm.T, 2 * j0, yb, kx, ring + (size_t)s * NY * CT + (size_t)yb * CT);
-                        tma_store_commit();
-                    }
-                }
-                if (i < mine) {
-                    const int s = i % TP_C_SLOTS;
-                    tma_store_wait_read<0>();  // the store of this slot's previous tile has read it
-                    if (!s_err) {
-                        int kx, j0;
-                        coords(i, kx, j0);
-                        mbar_arrive_expect_tx(&full[s], (uint32_t)C::tile);
-                        for (int yb = 0; yb < NY; yb += C::BOX_Y)
-                            tma_load_3d(ring + (size_t)s * NY * CT + (size_t)yb * CT, &tm.T, 2 * j0, yb, kx, &full[s]);
-                    }
-                }
-            }
-            tma_store_wait_all();
-            if (s_err)
-                for (int j = (mine > TP_C_SLOTS ? mine - TP_C_SLOTS : 0); j < mine; ++j)
-                    mbar_wait(&full[j % TP_C_SLOTS], (j / TP_C_SLOTS) & 1);
-        }
-        __syncwarp();
-    } else {
-        const double2* tw = static_cast<const double2*>(a.tw_y);
-        for (int i = 0; i < mine; ++i) {
-            const int s = i % TP_C_SLOTS;
-            int kx, j0;
-            coords(i, kx, j0);
-            // this thread's scale factors, fetched while the tile is in flight
-            double r[C::PER];
-#pragma unroll
-            for (int k = 0; k < C::PER; ++k) {
-                const int e = tid + k * C::CONS, ky = e / CT, cc = e - ky * CT;
-                r[k] = e < NY * CT ? a.recip[(long long)a.grp_of_row[kx * NY + ky] * EIG_SLOTS + j0 + cc] * a.scale
-                                   : 0.0;
-            }
-            const bool ok = tp_wait(&full[s], (i / TP_C_SLOTS) & 1, &s_err, a.err, 6);
-            double2* sm = ring + (size_t)s * NY * CT;
-            if (ok) slab_fft<NY, -1, C::CONS, 1>(sm, CT, CT, tw);
-#pragma unroll
-            for (int k = 0; k < C::PER; ++k) {
-                const int e = tid + k * C::CONS;
-                if (ok && e < NY * CT) sm[e] = make_double2(sm[e].x * r[k], sm[e].y * r[k]);
-            }
-            consumers_sync<C::CONS>();
-            if (ok) slab_fft<NY, 1, C::CONS, 1>(sm, CT, CT, tw);
-            fence_proxy_async_smem();
-            consumers_sync<C::CONS>();
-            if (tid == 0) mbar_arrive(&done[s]);
-        }
-    }
-}
-
 template <typename K>
 cudaError_t prep(K k, size_t smem)
 {
     return cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-}
-
-template <int NY>
-int run_conv_tma(const EigArgs& a, EigMaps& tm, cudaStream_t s)
-{
-    constexpr int CT = NY <= 256 ? 16 : 8;
-    using C = ConvShape<NY, CT>;
-    const uint64_t dims[3] = {2 * EIG_SLOTS, (uint64_t)NY, (uint64_t)a.nkx};
-    const uint64_t str[2] = {2 * EIG_SLOTS * sizeof(double), (uint64_t)NY * 2 * EIG_SLOTS * sizeof(double)};
-    const uint32_t box[3] = {2 * CT, (uint32_t)C::BOX_Y, 1};
-    if (!encode_tmap_f64_3d(&tm.T, a.S, dims, str, box)) return (int)cudaErrorInvalidValue;
-    cudaError_t e = prep(eig_conv_tma_kernel<NY, CT>, C::smem);
-    if (e != cudaSuccess) return (int)e;
-    const int ntiles = a.nkx * C::TILES_PER_KX;
-    const int grid = ntiles < a.nsm ? ntiles : a.nsm;
-    return (int)launch_k(eig_conv_tma_kernel<NY, CT>, dim3(grid), dim3(C::THREADS), C::smem, s, a, tm);
-}
-
-template <int L>
-int run_3d_tma(int pass, const EigArgs& a, cudaStream_t s)
-{
-    using T = TmaShape<L>;
-    EigMaps tm;
-    std::memset(&tm, 0, sizeof(tm));
-    const int grid = a.Ny < a.nsm ? a.Ny : a.nsm;
-    cudaError_t e;
-    if (pass == 0) {
-        const uint64_t dims[2] = {(uint64_t)a.x_stride, (uint64_t)L};
-        const uint64_t str[1] = {(uint64_t)a.x_stride * sizeof(double)};
-        const uint32_t box[2] = {TP_PITCH, T::RC};
-        if (!encode_tmap_f64_2d(&tm.f, a.f, dims, str, box)) return (int)cudaErrorInvalidValue;
-        if (a.sub && !encode_tmap_f64_2d(&tm.sub, a.sub, dims, str, box)) return (int)cudaErrorInvalidValue;
-        if ((e = prep(eig_fwd_tma_kernel<L>, T::smem1)) != cudaSuccess) return (int)e;
-        return (int)launch_k(eig_fwd_tma_kernel<L>, dim3(grid), dim3(T::THREADS), T::smem1, s, a, tm);
-    }
-    if (pass == 2) {
-        const uint64_t dims[3] = {2 * EIG_SLOTS, (uint64_t)a.Ny, (uint64_t)a.nkx};
-        const uint64_t str[2] = {2 * EIG_SLOTS * sizeof(double), (uint64_t)a.Ny * 2 * EIG_SLOTS * sizeof(double)};
-        const uint32_t box[3] = {2 * EIG_SLOTS, 1, (uint32_t)T::KC};
-        if (!encode_tmap_f64_3d(&tm.S, a.S, dims, str, box)) return (int)cudaErrorInvalidValue;
-        if ((e = prep(eig_inv_tma_kernel<L>, T::smem3)) != cudaSuccess) return (int)e;
-        return (int)launch_k(eig_inv_tma_kernel<L>, dim3(grid), dim3(T::THREADS), T::smem3, s, a, tm);
-    }
-    switch (a.Ny) {
-        case 4: return run_conv_tma<4>(a, tm, s);
-        case 8: return run_conv_tma<8>(a, tm, s);
-        case 16: return run_conv_tma<16>(a, tm, s);
-        case 32: return run_conv_tma<32>(a, tm, s);
-        case 64: return run_conv_tma<64>(a, tm, s);
-        case 128: return run_conv_tma<128>(a, tm, s);
-        case 256: return run_conv_tma<256>(a, tm, s);
-        case 512: return run_conv_tma<512>(a, tm, s);
-        default: return (int)cudaErrorInvalidValue;
-    }
 }
 
 template <int L>
@@ -923,31 +574,45 @@ int run_3d(int pass, const EigArgs& a, cudaStream_t s)
     using S = EpShape<L>;
     cudaError_t e;
     const size_t sm1 = S::smem(2);
-    if (a.tma) return run_3d_tma<L>(pass, a, s);
     if (pass == 0) {
+        EigMaps tm;
+        std::memset(&tm, 0, sizeof(tm));
+        EigArgs a1 = a;
+        if (a1.tma) {
+            const uint64_t dims[2] = {(uint64_t)a.x_stride, (uint64_t)L};
+            const uint64_t str[1] = {(uint64_t)a.x_stride * sizeof(double)};
+            const uint32_t box[2] = {EP_PITCH, (uint32_t)FwdBoxes<L>::QR};
+            if (!encode_tmap_f64_2d(&tm.f, a.f, dims, str, box)) a1.tma = 0;  // element-wise loads instead
+        }
         if ((e = prep(eig_fwd_kernel<L>, sm1)) != cudaSuccess) return (int)e;
-        return (int)launch_k(eig_fwd_kernel<L>, dim3(a.Ny), dim3(S::THREADS), sm1, s, a);
+        return (int)launch_k(eig_fwd_kernel<L>, dim3(a.Ny), dim3(S::THREADS), sm1, s, a1, tm);
     }
     if (pass == 2) {
         if ((e = prep(eig_inv_kernel<L>, sm1)) != cudaSuccess) return (int)e;
         return (int)launch_k(eig_inv_kernel<L>, dim3(a.Ny), dim3(S::THREADS), sm1, s, a);
     }
     const int nkx = L / 2 + 1;
+    const bool narrow = a.conv_var & 1;
     switch (a.Ny) {
-#define HELM_EIG_CONV(NY, CT)                                                                                   \
-    case NY: {                                                                                                  \
+#define HELM_EIG_CONV(NY, CT, TH)                                                                               \
+    {                                                                                                           \
         const size_t sm2 = (size_t)NY * CT * sizeof(double2);                                                   \
-        if ((e = prep(eig_conv_kernel<NY, CT>, sm2)) != cudaSuccess) return (int)e;                             \
-        return (int)launch_k(eig_conv_kernel<NY, CT>, dim3(nkx * (EIG_SLOTS / CT)), dim3(256), sm2, s, a);      \
+        if ((e = prep(eig_conv_kernel<NY, CT, TH>, sm2)) != cudaSuccess) return (int)e;                         \
+        return (int)launch_k(eig_conv_kernel<NY, CT, TH>, dim3(nkx * (EIG_SLOTS / CT)), dim3(TH), sm2, s, a);   \
     }
-        HELM_EIG_CONV(4, 16)
-        HELM_EIG_CONV(8, 16)
-        HELM_EIG_CONV(16, 16)
-        HELM_EIG_CONV(32, 16)
-        HELM_EIG_CONV(64, 16)
-        HELM_EIG_CONV(128, 16)
-        HELM_EIG_CONV(256, 16)
-        HELM_EIG_CONV(512, 8)
+#define HELM_EIG_CONV2(NY)                                                                                      \
+    case NY:                                                                                                    \
+        if (narrow) HELM_EIG_CONV(NY, 8, 128) else HELM_EIG_CONV(NY, 16, 256)
+        HELM_EIG_CONV2(4)
+        HELM_EIG_CONV2(8)
+        HELM_EIG_CONV2(16)
+        HELM_EIG_CONV2(32)
+        HELM_EIG_CONV2(64)
+        HELM_EIG_CONV2(128)
+        HELM_EIG_CONV2(256)
+        case 512:
+            if (narrow) HELM_EIG_CONV(512, 4, 256) else HELM_EIG_CONV(512, 8, 256)
+#undef HELM_EIG_CONV2
 #undef HELM_EIG_CONV
         default: return (int)cudaErrorInvalidValue;
     }
@@ -967,8 +632,7 @@ int run_2d(const EigArgs& a, int nprob, cudaStream_t s)
 
 bool eig_tma_ok(const EigArgs& a)
 {
-    auto al = [](const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15) == 0; };
-    return al(a.f) && (!a.sub || al(a.sub)) && al(a.S) && (a.x_stride & 1) == 0;
+    return (reinterpret_cast<uintptr_t>(a.f) & 15) == 0 && (a.x_stride & 1) == 0 && !a.sub;
 }
 
 bool eig_shape_ok(int dim, int Nx, int Ny, int P)

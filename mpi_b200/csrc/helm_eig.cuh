@@ -40,17 +40,17 @@ struct EigArgs {
     double* gbar_r;
     const double* lam_u;
     double* lam_out;
-    // 3D: the persistent TMA-pipelined passes (row variant 5), with one CTA
-    // per SM (nsm), nkx = Nx / 2 + 1 spectrum rows along x, and a device
-    // status word that a wait which ran out sets (NULL: not recorded)
+    // 3D pass 1: load each plane of f with tensor-memory-accelerator copies
+    // (f 16-byte aligned with an even x stride; not the misfit adjoint), and
+    // the device status word that a copy wait which ran out sets (NULL: none)
     int tma;
-    int nsm;
-    int nkx;
     int* err;
+    // 3D pass 2 CTA shape: 0 = 16 columns x 256 threads, 1 = 8 columns x 128
+    // threads (Ny = 512: 8 or 4 columns, 256 threads)
+    int conv_var;
 };
 
-// Whether the TMA-pipelined passes take these arrays: f (and u_obs, when
-// given) start on a 16-byte boundary and their x rows keep that alignment.
+// Whether pass 1 can load these arrays with TMA copies.
 bool eig_tma_ok(const EigArgs& a);
 
 // Whether the pipeline covers a plan of this shape (FP64 arithmetic).

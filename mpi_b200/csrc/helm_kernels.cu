@@ -120,18 +120,36 @@ __device__ __forceinline__ void c2r_store(const FftArgs& a, TIO* out, long long 
         for (int r = 0; r < RL; ++r) {
             const long long row = pass_out_row<RL, NSL, TPC>(tc, t, r);
             const double x0 = (double)(v[t * RL + r].x * sc), x1 = (double)(v[t * RL + r].y * sc);
+            // (accumulate: a refinement sweep adds its correction to fbar and gbar)
+            const double keep = a.accumulate ? 1.0 : 0.0;
             if (b0) {
-                if (k0 == 0 && a.gbar_l) a.gbar_l[row * a.bc_row + j0] = a.adj_scale_l * x0;
-                if (k0 == P - 1 && a.gbar_r) a.gbar_r[row * a.bc_row + j0] = a.adj_scale_r * x0;
+                if (k0 == 0 && a.gbar_l) {
+                    double* g = &a.gbar_l[row * a.bc_row + j0];
+                    *g = keep * *g + a.adj_scale_l * x0;
+                }
+                if (k0 == P - 1 && a.gbar_r) {
+                    double* g = &a.gbar_r[row * a.bc_row + j0];
+                    *g = keep * *g + a.adj_scale_r * x0;
+                }
             }
-            out[row * a.out_row + c0] = zero0 ? (TIO)0 : (TIO)x0;
+            {
+                TIO* o = &out[row * a.out_row + c0];
+                *o = zero0 ? (TIO)0 : (a.accumulate ? (TIO)(*o + x0) : (TIO)x0);
+            }
             acc += x0 * u0[r];
             if (has1) {
                 if (b1) {
-                    if (k1 == 0 && a.gbar_l) a.gbar_l[row * a.bc_row + j1] = a.adj_scale_l * x1;
-                    if (k1 == P - 1 && a.gbar_r) a.gbar_r[row * a.bc_row + j1] = a.adj_scale_r * x1;
+                    if (k1 == 0 && a.gbar_l) {
+                        double* g = &a.gbar_l[row * a.bc_row + j1];
+                        *g = keep * *g + a.adj_scale_l * x1;
+                    }
+                    if (k1 == P - 1 && a.gbar_r) {
+                        double* g = &a.gbar_r[row * a.bc_row + j1];
+                        *g = keep * *g + a.adj_scale_r * x1;
+                    }
                 }
-                out[row * a.out_row + c1] = zero1 ? (TIO)0 : (TIO)x1;
+                TIO* o = &out[row * a.out_row + c1];
+                *o = zero1 ? (TIO)0 : (a.accumulate ? (TIO)(*o + x1) : (TIO)x1);
                 acc += x1 * u1[r];
             }
         }

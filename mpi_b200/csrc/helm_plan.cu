@@ -14,6 +14,7 @@
 #include "helm_kernels.cuh"
 #include "helm_plan.hpp"
 #include "helm_eig.cuh"
+#include "helm_fd_refine.cuh"
 #include "helm_setup.hpp"
 
 #include <algorithm>
@@ -381,11 +382,6 @@ static int setup_fast(Plan& p, const std::vector<double>& A0, int prec_code)
         if (p.dim == 3) {
             const int zero = 0;
             if ((st = p.upload((void**)&p.d_status, &zero, sizeof(int)))) return st;
-            int nsm = 0;
-            if (cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, p.device) == cudaSuccess && nsm > 0)
-                p.nsm = nsm;
-            else
-                cudaGetLastError();
         }
         p.eig_ok = true;
     }
@@ -636,6 +632,16 @@ static int setup_plan(Plan& p)
     return HELM_OK;
 }
 
+// Per-call options of a pipeline run (refinement sweeps of finite-difference
+// plans): element size of the input read by the first pass and of the output
+// written by the last (0: the plan's), and whether the last pass adds its
+// result to the output (and, in an adjoint run, to the boundary cotangents and
+// the lambda sum, which it then does not zero first).
+struct PipeOpts {
+    int io_in = 0, io_out = 0;
+    bool accumulate = false;
+};
+
 // Outputs of the adjoint solve that its last (C2R) pass writes besides fbar.
 struct AdjOut {
     double* glbar;
@@ -648,7 +654,8 @@ struct AdjOut {
 static int fft_pass(Plan& p, int L, int mode, int dir, const void* in, void* out, long long in_row, long long out_row,
                     long long in_batch, long long out_batch, int ncols, int nbatch, double scale, const void* tw,
                     const double* gl, const double* gr, bool inject, bool io_double, int stage, cudaStream_t s,
-                    const AdjOut* adj = nullptr, int deriv_order = 0, double deriv_w = 0.0)
+                    const AdjOut* adj = nullptr, int deriv_order = 0, double deriv_w = 0.0,
+                    const PipeOpts* po = nullptr)
 {
     FftArgs a{};
     a.deriv_order = deriv_order;
@@ -666,7 +673,9 @@ static int fft_pass(Plan& p, int L, int mode, int dir, const void* in, void* out
         a.lam_u = adj->lambda_bar ? adj->u : nullptr;
         a.lam_out = adj->lambda_bar;
     }
-    if (adj && stage == 0) a.zero_out = adj->lambda_bar;
+    const bool acc = po && po->accumulate;
+    if (adj && stage == 0 && !acc) a.zero_out = adj->lambda_bar;
+    a.accumulate = (acc && stage == 3) ? 1 : 0;
     a.in = in;
     a.out = out;
     a.in_row = in_row;
@@ -691,7 +700,9 @@ static int fft_pass(Plan& p, int L, int mode, int dir, const void* in, void* out
     a.out_boff = stage == 3 ? p.d_boff : nullptr;
     const long long ccols = (mode == FFT_C2C) ? ncols : (ncols + 1) / 2;
     const int td = p.precision != HELM_FP32;
-    const int io = (td || io_double) ? 8 : p.io_bytes;
+    int io = (td || io_double) ? 8 : p.io_bytes;
+    if (po && stage == 0 && po->io_in) io = po->io_in;
+    if (po && stage == 3 && po->io_out) io = po->io_out;
     const int kmode = a.adj_mode ? (int)FFT_C2R_ADJ : mode;
     int e = launch_fft(L, kmode, dir, td, io, a, ccols * nbatch, s, sub ? (p.fft_var[stage] & ~4) : p.fft_var[stage]);
     if (e) return set_cuda_error((cudaError_t)e, "fft launch");
@@ -702,7 +713,8 @@ static int fft_pass(Plan& p, int L, int mode, int dir, const void* in, void* out
 // GLL boundary slots of the spectrum, out = u.  Adjoint: in = ubar read in
 // every slot, the transposed row solve, out = A^-T ubar in every slot.
 static int run_pipeline(Plan& p, const void* in, const double* gl, const double* gr, void* out, bool adjoint,
-                        cudaStream_t s, const AdjOut* adj = nullptr, const Workspace* ws = nullptr)
+                        cudaStream_t s, const AdjOut* adj = nullptr, const Workspace* ws = nullptr,
+                        const PipeOpts* po = nullptr)
 {
     const int N = p.N;
     void* const spec = ws ? ws->spec : p.d_spec;
@@ -716,10 +728,9 @@ static int run_pipeline(Plan& p, const void* in, const double* gl, const double*
     mark(0);
     // row variant in effect: the eigen-basis pipeline covers forward solves
     int rv = p.row_var;
-    if (rv == 5 && p.dim != 3) rv = 4;  // 2D: one fused kernel either way
-    if ((rv == 4 || rv == 5) && (!p.eig_ok || (adjoint && !p.d_fmma_adj))) rv = p.precision == HELM_FP64 ? 0 : 3;
+    if (rv == 4 && (!p.eig_ok || (adjoint && !p.d_fmma_adj))) rv = p.precision == HELM_FP64 ? 0 : 3;
     if (rv == 3 && (p.precision != HELM_FP32_REFINE || !p.d_fmma)) rv = 0;
-    if (rv == 4 || rv == 5) {
+    if (rv == 4) {
         // three launches (3D) or one (2D): GLL transform + x FFT, y convolution,
         // inverse; stage events 1 and 4 bracket the middle pass
         EigArgs ea{};
@@ -753,10 +764,9 @@ static int run_pipeline(Plan& p, const void* in, const double* gl, const double*
         ea.tw_y = p.d_tw_y;
         ea.scale = 1.0 / ((double)p.Nx * (p.dim == 3 ? p.Ny : 1));
         ea.boff = p.d_boff;  // size-class plans of a batch: the packed offsets (one problem or more)
-        ea.nsm = p.nsm;
-        ea.nkx = p.Nx / 2 + 1;
         ea.err = p.d_status;
-        ea.tma = (rv == 5 && p.dim == 3 && eig_tma_ok(ea)) ? 1 : 0;
+        ea.tma = (p.dim == 3 && eig_tma_ok(ea)) ? 1 : 0;
+        ea.conv_var = p.fft_var[1] & 1;
         int e = launch_eig_pass(0, p.dim, p.Nx, ea, p.batch, s);
         if (e) return set_cuda_error((cudaError_t)e, "eigen-basis pass 1");
         mark(1);
@@ -772,7 +782,7 @@ static int run_pipeline(Plan& p, const void* in, const double* gl, const double*
     }
     // 1. x: real-to-complex (forward: GLL boundary slots take the boundary data)
     if ((st = fft_pass(p, p.Nx, FFT_R2C, -1, in, spec, p.x_stride, cols, p.elem_stride, p.elem_spec, (int)cols,
-                       p.Ns * p.batch, 1.0, p.d_tw_x, gl, gr, !adjoint, adjoint, 0, s, adj)))
+                       p.Ns * p.batch, 1.0, p.d_tw_x, gl, gr, !adjoint, adjoint, 0, s, adj, 0, 0.0, po)))
         return st;
     mark(1);
     // FP64 and refined 3D plans may run stages 2-4 as one fused kernel per kx slab
@@ -903,7 +913,7 @@ static int run_pipeline(Plan& p, const void* in, const double* gl, const double*
     // 5. x: complex-to-real, scaled by 1/(Nx Ny) (the reference's /Nx, /Ny)
     const double scale = 1.0 / ((double)p.Nx * (p.dim == 3 ? p.Ny : 1));
     if ((st = fft_pass(p, p.Nx, FFT_C2R, 1, spec, out, cols, p.x_stride, p.elem_spec, p.elem_stride, (int)cols,
-                       p.Ns * p.batch, scale, p.d_tw_x, nullptr, nullptr, false, adjoint, 3, s, adj)))
+                       p.Ns * p.batch, scale, p.d_tw_x, nullptr, nullptr, false, adjoint, 3, s, adj, 0, 0.0, po)))
         return st;
     mark(5);
     return HELM_OK;
@@ -945,7 +955,7 @@ static int autotune(Plan& p)
 {
     const char* env = std::getenv("HELM_AUTOTUNE");
     if (env && env[0] == '0') {
-        if (p.eig_ok) p.row_var = p.dim == 3 ? 5 : 4;
+        if (p.eig_ok) p.row_var = 4;
         return HELM_OK;
     }
     const std::string key = std::string(p.fd ? "fd:" : "gll:") + std::to_string(p.dim) + ":" + std::to_string(p.Nx) +
@@ -970,7 +980,7 @@ static int autotune(Plan& p)
     if (cudaMalloc(&f, bytes) != cudaSuccess || cudaMalloc(&u, bytes) != cudaSuccess) {
         cudaGetLastError();
         if (f) cudaFree(f);
-        if (p.eig_ok) p.row_var = p.dim == 3 ? 5 : 4;
+        if (p.eig_ok) p.row_var = 4;
         return HELM_OK;  // keep the defaults
     }
     cudaMemset(f, 0, bytes);
@@ -1011,16 +1021,20 @@ static int autotune(Plan& p)
     cudaGetLastError();
     p.row_var = best_rv;
     // 3. fused alternatives, whole solves
-    std::vector<int> whole = {p.row_var};
-    if (p.slab_ok) whole.push_back(2);
-    if (p.eig_ok) whole.push_back(4);
-    if (p.eig_ok && p.dim == 3) whole.push_back(5);
+    // (row variant, y-pass variant): the eigen-basis pipeline takes bit 0 of the
+    // y-pass variant as the CTA shape of its second pass
+    const int yv = p.fft_var[1];
+    std::vector<std::pair<int, int>> whole = {{p.row_var, yv}};
+    if (p.slab_ok) whole.push_back({2, yv});
+    if (p.eig_ok) whole.push_back({4, 0});
+    if (p.eig_ok && p.dim == 3) whole.push_back({4, 1});
     if (whole.size() > 1) {
         std::vector<float> tot(whole.size(), 0.f);
         bool ok = true;
         for (int rep = 0; rep < 6 && ok; ++rep)
             for (size_t k = 0; k < whole.size() && ok; ++k) {
-                p.row_var = whole[k];
+                p.row_var = whole[k].first;
+                p.fft_var[1] = whole[k].second;
                 if (solve(p, f, nullptr, nullptr, u, 0) || cudaEventSynchronize(p.ev[5]) != cudaSuccess) {
                     ok = false;
                     break;
@@ -1034,7 +1048,8 @@ static int autotune(Plan& p)
         if (ok)
             for (size_t k = 1; k < whole.size(); ++k)
                 if (tot[k] < tot[bk]) bk = k;
-        p.row_var = whole[bk];
+        p.row_var = whole[bk].first;
+        p.fft_var[1] = whole[bk].second;
     }
     p.stage_timing = had;
     cudaFree(f);
@@ -1044,13 +1059,70 @@ static int autotune(Plan& p)
     return HELM_OK;
 }
 
+// The stencil coefficients of a finite-difference plan's residual.
+static FdResidualArgs fd_residual_args(const Plan& p)
+{
+    FdResidualArgs r{};
+    const double dx = p.Lx / p.Nx, dy = p.Ly / p.Ny;
+    r.Nx = p.Nx;
+    r.Ny = p.Ny;
+    r.Nz = p.N;
+    r.cx1 = 1.0 / (dx * dx);
+    r.cy1 = 1.0 / (dy * dy);
+    r.cz1 = p.fd_cz1;
+    r.lam = p.lambda;
+    r.dfirst = p.fd_dfirst;
+    r.sfirst = p.fd_sfirst;
+    r.dlast = p.fd_dlast;
+    r.slast = p.fd_slast;
+    r.scale_l = p.fd_scale_l;
+    r.scale_r = p.fd_scale_r;
+    return r;
+}
+
+// Refined finite-difference solve (HELM_FP32_REFINE): the FP32 solve of the
+// FP64 data, then p.sweeps times the FP64 residual r = f - A_h u and an FP32
+// solve of A_h d = r whose last pass adds d into u.  The adjoint runs the same
+// with the transposed stencil; its last passes also add into the boundary
+// cotangents and the lambda sum.
+static int refine_fd(Plan& p, const void* in, const double* gl, const double* gr, void* out, bool adjoint,
+                     cudaStream_t s, const AdjOut* adj, const Workspace* ws)
+{
+    float* r = static_cast<float*>(ws && ws->refine ? ws->refine : p.d_refine);
+    int st = run_pipeline(p, in, gl, gr, out, adjoint, s, adj, ws);
+    FdResidualArgs ra = fd_residual_args(p);
+    ra.rhs = static_cast<const double*>(in);
+    ra.sub = adjoint && adj ? adj->sub : nullptr;
+    ra.gl = adjoint ? nullptr : gl;
+    ra.gr = adjoint ? nullptr : gr;
+    ra.v = static_cast<const double*>(out);
+    ra.r = r;
+    ra.transpose = adjoint ? 1 : 0;
+    PipeOpts po;
+    po.io_in = 4;
+    po.io_out = 8;
+    po.accumulate = true;
+    AdjOut cadj{};
+    if (adj) {
+        cadj = *adj;
+        cadj.sub = nullptr;  // the residual already holds ubar - u_obs
+    }
+    for (int k = 0; k < p.sweeps && !st; ++k) {
+        if (int e = launch_fd_residual(ra, s)) return set_cuda_error((cudaError_t)e, "refinement residual");
+        st = run_pipeline(p, r, nullptr, nullptr, out, adjoint, s, adj ? &cadj : nullptr, ws, &po);
+    }
+    return st;
+}
+
 int solve(Plan& p, const void* f, const double* gl, const double* gr, void* u, cudaStream_t s, const Workspace* ws)
 {
+    if (p.fd_refine) return refine_fd(p, f, gl, gr, u, false, s, nullptr, ws);
     return run_pipeline(p, f, gl, gr, u, false, s, nullptr, ws);
 }
 
 size_t spec_bytes(const Plan& p) { return p.spec_bytes; }
 size_t cprime_bytes(const Plan& p) { return p.d_cprime ? p.cprime_bytes : 0; }
+size_t refine_bytes(const Plan& p) { return p.d_refine ? p.refine_bytes : 0; }
 
 int check_solve_args(const Plan& p, const void* f, const double* gl, const double* gr, const void* u)
 {
@@ -1079,6 +1151,7 @@ int solve_adjoint(Plan& p, const double* ubar, double* fbar, double* glbar, doub
     // the first pass zeroes lambda_bar; the last writes fbar, splits off glbar /
     // grbar and sums fbar * u into lambda_bar
     const AdjOut adj{glbar, grbar, u, lambda_bar, sub};
+    if (p.fd_refine) return refine_fd(p, ubar, nullptr, nullptr, fbar, true, s, &adj, nullptr);
     return run_pipeline(p, ubar, nullptr, nullptr, fbar, true, s, &adj);
 }
 
@@ -1186,9 +1259,11 @@ static int create_fd_plan(int Nx, int Ny, int Nz, double xl, double xr, double y
     p->Lgll = zr - zl;
     p->bc = bc ? *bc : helm_robin_t{0.0, 1.0, 0.0, 1.0};
     p->lambda = lambda;
-    // the FD path computes in FP64 for FP32_REFINE plans (an O(Nz) Thomas solve
-    // has nothing to refine against: it is bound by the same FP64 bytes)
-    p->precision = precision == HELM_FP32 ? HELM_FP32 : HELM_FP64;
+    // HELM_FP32_REFINE: FP32 spectrum and tridiagonal solves, FP64 input and
+    // output, two FP64-residual refinement sweeps per solve (refine_fd)
+    p->fd_refine = precision == HELM_FP32_REFINE;
+    p->precision = precision == HELM_FP64 ? HELM_FP64 : HELM_FP32;
+    if (p->fd_refine) p->sweeps = 2;
     p->method = HELM_METHOD_LU;
     p->x_stride = (long long)Ny * Nz;
     p->elem_stride = (long long)Nx * Ny * Nz;
@@ -1224,6 +1299,9 @@ static int create_fd_plan(int Nx, int Ny, int Nz, double xl, double xr, double y
     // elimination scratch of the thread-per-row tridiagonal kernel (Nz > 512 only)
     p->cprime_bytes = (size_t)p->elem_spec * (td ? 8 : 4);
     if (!st && Nz > 512) st = p->alloc(&p->d_cprime, p->cprime_bytes);
+    // the residual of a refinement sweep, then its correction (FP32)
+    p->refine_bytes = (size_t)Nx * Ny * Nz * sizeof(float);
+    if (!st && p->fd_refine) st = p->alloc(&p->d_refine, p->refine_bytes);
     if (!st) st = p->upload((void**)&p->d_mx, mx.data(), mx.size() * sizeof(double));
     if (!st) st = p->upload((void**)&p->d_my, my.data(), my.size() * sizeof(double));
     auto up_tw = [&](int L, void** d) -> int {
@@ -1409,7 +1487,7 @@ int helm_plan_set_io_bytes(helm_plan_t plan, int bytes)
 {
     if (!plan || (bytes != 4 && bytes != 8)) return HELM_ERR_INVALID;
     Plan& p = *reinterpret_cast<Plan*>(plan);
-    if (bytes == 4 && p.precision != HELM_FP32) return HELM_ERR_UNSUPPORTED;
+    if (bytes == 4 && (p.precision != HELM_FP32 || p.fd_refine)) return HELM_ERR_UNSUPPORTED;
     p.io_bytes = bytes;
     return HELM_OK;
 }
@@ -1571,7 +1649,7 @@ int helm_plan_get_launch_variants(helm_plan_t plan, int* fft4, int* rows)
 
 int helm_plan_set_launch_variants(helm_plan_t plan, const int* fft4, int rows)
 {
-    if (!plan || !fft4 || rows < 0 || rows > 5) return HELM_ERR_INVALID;
+    if (!plan || !fft4 || rows < 0 || rows > 4) return HELM_ERR_INVALID;
     for (int i = 0; i < 4; ++i)
         if (fft4[i] < 0 || fft4[i] > 15) return HELM_ERR_INVALID;
     Plan& p = *reinterpret_cast<Plan*>(plan);
@@ -1583,7 +1661,7 @@ int helm_plan_set_launch_variants(helm_plan_t plan, const int* fft4, int rows)
         helm::set_last_error("row variant 3 (FP64 tensor-core rows) is for refined plans with one element");
         return HELM_ERR_UNSUPPORTED;
     }
-    if ((rows == 4 || rows == 5) && !p.eig_ok) {
+    if (rows == 4 && !p.eig_ok) {
         helm::set_last_error("the eigen-basis pipeline needs an FP64 or refined plan with one element, Dirichlet ends, "
                              "at most 66 points, Nx in {8..256} and Ny in {4..512}");
         return HELM_ERR_UNSUPPORTED;
@@ -1634,14 +1712,10 @@ const char* helm_plan_kernels(helm_plan_t plan)
     if (!plan) return "";
     Plan& p = *reinterpret_cast<Plan*>(plan);
     int rv = p.row_var;
-    if (rv == 5 && p.dim != 3) rv = 4;
-    if ((rv == 4 || rv == 5) && !p.eig_ok) rv = p.precision == HELM_FP64 ? 0 : 3;
+    if (rv == 4 && !p.eig_ok) rv = p.precision == HELM_FP64 ? 0 : 3;
     if (rv == 3 && (p.precision != HELM_FP32_REFINE || !p.d_fmma)) rv = 0;
     std::string k;
-    if (rv == 5) {
-        // (arrays whose alignment the tensor maps cannot take run variant 4's kernels)
-        k = "eig_fwd_tma_kernel eig_conv_tma_kernel eig_inv_tma_kernel";
-    } else if (rv == 4) {
+    if (rv == 4) {
         k = p.dim == 3 ? "eig_fwd_kernel eig_conv_kernel eig_inv_kernel" : "eig_solve2d_kernel";
     } else {
         const bool slab = rv == 2 && p.slab_ok && p.fast && p.precision != HELM_FP32;
@@ -1658,6 +1732,10 @@ const char* helm_plan_kernels(helm_plan_t plan)
         k += " " + rows;
         if (p.dim == 3 && !slab) k += " fft_kernel(y-inv)";
         k += std::string(" ") + (p.fft_var[3] & 4 ? "fft_pipe_kernel" : "fft_kernel") + "(x-inv)";
+        if (p.fd_refine) {  // per sweep: the residual, then a correction solve
+            const std::string one = k;
+            for (int i = 0; i < p.sweeps; ++i) k += " fd_residual_kernel " + one;
+        }
     }
     p.kernel_names = k;
     return p.kernel_names.c_str();

@@ -101,12 +101,16 @@ struct Plan {
     double* d_mx = nullptr;
     double* d_my = nullptr;
     void* d_cprime = nullptr;
+    // HELM_FP32_REFINE finite-difference plans: FP32 internals with FP64
+    // residual sweeps, and their FP32 residual / correction array
+    bool fd_refine = false;
+    void* d_refine = nullptr;
+    size_t refine_bytes = 0;
     // autotuned launch shapes of the four FFT stages (x, y, inverse y, inverse x)
     int fft_var[4] = {0, 0, 0, 0};
     // row-solve variant: 0, 1 launch shapes of the plan precision's folded kernel;
     // 2 fused y-FFT / rows / inverse y (slab, FP64 arithmetic); 3 refined plans:
-    // the FP64 tensor-core row kernel; 4 the eigen-basis pipeline (whole solve);
-    // 5 its 3D passes as persistent TMA-pipelined kernels
+    // the FP64 tensor-core row kernel; 4 the eigen-basis pipeline (whole solve)
     int row_var = 0;
     bool slab_ok = false;          // FP64 3D plans whose kx slab fits a two-CTA cluster
     // eigen-basis pipeline (helm_eig.cu; row variant 4): one element, Dirichlet
@@ -116,10 +120,8 @@ struct Plan {
     double* d_hbc = nullptr;       // [4][32] first transform of the folded boundary columns
     double* d_frecip64 = nullptr;  // FP64 reciprocal shifts (refined plans; FP64 plans use d_frecip)
     int* d_grp_of_row = nullptr;   // shift group of each spectrum row (slab kernel)
-    // row variant 5 (the TMA-pipelined eigen-basis passes): the device's SM
-    // count (one persistent CTA each) and a device status word that a bounded
-    // wait which ran out sets to a nonzero code (helm_plan_device_status)
-    int nsm = 148;
+    // device status word of the eigen-basis pipeline's TMA loads: a bounded wait
+    // that ran out sets it to a nonzero code (helm_plan_device_status)
     int* d_status = nullptr;
     bool stage_timing = false;
     cudaEvent_t ev[6] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
@@ -139,11 +141,13 @@ struct Plan {
 struct Workspace {
     void* spec = nullptr;
     void* cprime = nullptr;
+    void* refine = nullptr;
 };
 
 // Bytes of spectrum and elimination scratch a solve of this plan writes.
 size_t spec_bytes(const Plan& p);
 size_t cprime_bytes(const Plan& p);
+size_t refine_bytes(const Plan& p);
 
 // Argument checks shared by every solve entry point (status, last error set).
 int check_solve_args(const Plan& p, const void* f, const double* gl, const double* gr, const void* u);

@@ -11,7 +11,8 @@
 // Limits and behaviour:
 //   * The workspace is kHelmStaticScratchBytes = 16 MiB per device; a plan whose
 //     spectrum (plus, for finite-difference plans with more than 512 points in
-//     z, its elimination coefficients) needs more is rejected with
+//     z, its elimination coefficients, and for refined finite-difference plans
+//     their residual array) needs more is rejected with
 //     HELM_ERR_UNSUPPORTED.  Every GPU that
 //     loads this library holds the 16 MiB until the process exits.
 //   * The first call on a device looks up the array's device address
@@ -80,7 +81,8 @@ extern "C" int helm_solve_static_scratch(helm_plan_t plan, const void* f, const 
     // the spectrum, then (finite-difference plans with long z lines) the
     // elimination coefficients, each at a 256-byte boundary
     const size_t spec = (helm::spec_bytes(p) + 255) & ~(size_t)255;
-    const size_t need = spec + helm::cprime_bytes(p);
+    const size_t cpr = (helm::cprime_bytes(p) + 255) & ~(size_t)255;
+    const size_t need = spec + cpr + helm::refine_bytes(p);
     if (need > helm::kHelmStaticScratchBytes) {
         helm::set_last_error("plan needs more than the 16 MiB static scratch");
         return HELM_ERR_UNSUPPORTED;
@@ -103,6 +105,7 @@ extern "C" int helm_solve_static_scratch(helm_plan_t plan, const void* f, const 
         helm::Workspace ws;
         ws.spec = scratch;
         ws.cprime = helm::cprime_bytes(p) ? static_cast<unsigned char*>(scratch) + spec : nullptr;
+        ws.refine = helm::refine_bytes(p) ? static_cast<unsigned char*>(scratch) + spec + cpr : nullptr;
         st = helm::solve(p, f, gl, gr, u, static_cast<cudaStream_t>(stream), &ws);
     }
     if (cur != p.device) cudaSetDevice(cur);

@@ -126,3 +126,48 @@ def test_fd_lambda_gradient(cuda):
     loss = lambda q: 0.5 * float(((q.SolvePDE(f) - uobs) ** 2).sum())  # noqa: E731
     fd = (loss(mk(lam + h)) - loss(mk(lam - h))) / (2 * h)
     assert abs(fd - float(lbar)) < 1e-6 * abs(float(lbar))
+
+
+@pytest.mark.parametrize("bc", [(0.0, 1.0, 0.0, 1.0), (1.0, 0.5, 0.7, 2.0)])
+@pytest.mark.parametrize("shape", [(16, 8, 12), (8, 32, 2), (64, 64, 33), (4, 4, 600)])
+def test_fd_refined_matches_oracle(cuda, bc, shape):
+    """FP32 solves with two FP64-residual refinement sweeps reach FP64 accuracy
+    (1e-10 relative) against the restatement, forward and adjoint (fbar, the
+    boundary cotangents, lambda_bar) against the FP64 plan."""
+    rng = np.random.default_rng(hash((shape, bc, 1)) % 2**32)
+    Nx, Ny, Nz = shape
+    f = rng.standard_normal(shape); gb = rng.standard_normal((Nx, Ny)); gf = rng.standard_normal((Nx, Ny))
+    ref = O.fd3d_solve(f, gb, gf, Lx=1.0, Ly=2.0, Lz=1.5, lam=1.0, bc=bc)
+    pr = Helmholtz3DFD(Nx, Ny, Nz, 0.0, 1.0, 0.0, 2.0, 0.0, 1.5, Lambda=1.0, bc=bc, precision="fp32_refine")
+    assert pr.kernels().count("fd_residual_kernel") == 2
+    u = pr.SolvePDE(_dev(f), _dev(gb), _dev(gf))
+    assert rel_l2(u.cpu().numpy(), ref) < 1e-10
+    p64 = Helmholtz3DFD(Nx, Ny, Nz, 0.0, 1.0, 0.0, 2.0, 0.0, 1.5, Lambda=1.0, bc=bc)
+    u64 = p64.SolvePDE(_dev(f), _dev(gb), _dev(gf))
+    ubar = _dev(rng.standard_normal(shape))
+    got = pr.SolveAdjoint(ubar, u=u64, want_bc=True)
+    want = p64.SolveAdjoint(ubar, u=u64, want_bc=True)
+    for a, b in zip(got, want):
+        assert rel_l2(a.cpu().numpy(), b.cpu().numpy()) < 1e-10
+    uobs = _dev(rng.standard_normal(shape))
+    got = pr.SolveAdjointMisfit(u64, uobs, want_bc=True)
+    want = p64.SolveAdjointMisfit(u64, uobs, want_bc=True)
+    for a, b in zip(got, want):
+        assert rel_l2(a.cpu().numpy(), b.cpu().numpy()) < 1e-10
+
+
+def test_fd_refined_full_size(cuda):
+    """1024 x 1024 x 256: the refined solve against the FP64 solve, and the
+    sweeps' effect (one sweep is not enough at this conditioning, two are)."""
+    Nx, Ny, Nz = 1024, 1024, 256
+    f = _dev(W.smooth_field_fd(Nx, Ny, Nz, seed=1239))
+    p64 = Helmholtz3DFD(Nx, Ny, Nz, 0.0, 1.0, 0.0, 1.0, 0.0, 1.0, Lambda=1.0)
+    u64 = p64.SolvePDE(f)
+    p64.DestroyPDEPlan()
+    pr = Helmholtz3DFD(Nx, Ny, Nz, 0.0, 1.0, 0.0, 1.0, 0.0, 1.0, Lambda=1.0, precision="fp32_refine")
+    errs = []
+    for sweeps in (0, 1, 2):
+        pr.set_refine_sweeps(sweeps)
+        u = pr.SolvePDE(f)
+        errs.append(((u - u64).norm() / u64.norm()).item())
+    assert errs[0] > 1e-6 and errs[1] < errs[0] * 1e-2 and errs[2] < 1e-10, errs
