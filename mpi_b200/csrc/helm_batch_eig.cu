@@ -8,17 +8,17 @@
 // problem): u_int = V (x-FFT^-1 diag(1/(mu_j - sigma(kx))) x-FFT) V^-1 f_int,
 // with V, V^-1 the folded transforms of helm_fdm.cu.  The work is cut into
 // three kinds of items that persistent CTAs take from one ordered queue:
-//   1. (problem, 32 x rows): fold and first transform of f's rows on the FP64
+//   1. (problem, 64 x rows): fold and first transform of f's rows on the FP64
 //      tensor cores -> the problem's coefficient rows C[x][2 ld] (scratch);
 //   2. (problem, up to 16 coefficient column pairs): x FFT, scaling by
 //      1 / ((mu_j - sigma) Nx), inverse x FFT, in place in C;
-//   3. (problem, 32 x rows): second transform, unfold -> u rows.
+//   3. (problem, 64 x rows): second transform, unfold -> u rows.
 // A kind-2 item waits until every kind-1 item of its problem is done, a kind-3
 // item until every kind-2 item is (per-problem counters, bounded waits).  The
 // queue holds every kind-1 item before any kind-2 item before any kind-3 item,
 // so a CTA only waits for items that running CTAs have already taken: the
 // launch needs no co-residency guarantee.  Big problems spread over many CTAs
-// (a 512 x 129 problem is 16 + 16 + 16 items), small ones cost one item each.
+// (a 512 x 129 problem is 8 + 16 + 8 items), small ones cost one item each.
 // The coefficient scratch (sum of Nx * 2 ld doubles) mostly stays in L2.
 #include <cuda_runtime.h>
 
@@ -42,7 +42,7 @@ namespace {
 
 constexpr int BE_THREADS = 256;   // 8 warps; two or three CTAs share an SM
 constexpr int BE_MINB = 2;        // resident CTAs per SM the kernel is built for
-constexpr int BE_ROWS = 32;       // x rows of a kind-1 / kind-3 item
+constexpr int BE_ROWS = 64;       // x rows of a kind-1 / kind-3 item (one 8-row tile per warp)
 
 // Complex columns of a kind-2 item: at most 16, and few enough that the tile
 // (Nx rows of CT + 1 double2) stays near 36 KB, so several CTAs fit an SM.
@@ -96,7 +96,9 @@ __device__ __forceinline__ int ld_acquire(const int* p)
     return v;
 }
 
-// Kind 1: rows x0 .. x0+R-1 of problem pr -> coefficient rows.
+// Kind 1: rows x0 .. x0+R-1 of problem pr -> coefficient rows.  Warp w owns
+// the 8-row tile w and both folds: one pair of row loads feeds the symmetric
+// and the antisymmetric A fragment of every k step.
 template <int LD>
 __device__ void be_rows_in(const BeArgs& a, const BeProblem& pr, const BeClass& c, int idx, double* sm)
 {
@@ -108,23 +110,36 @@ __device__ void be_rows_in(const BeArgs& a, const BeProblem& pr, const BeClass& 
     for (int r = warp; r < R; r += BE_THREADS / 32)  // a warp per row, lanes along the row
         for (int k = lane; k < P; k += 32) st[r * pitch + k] = (k > 0 && k < P - 1) ? __ldg(f + r * P + k) : 0.0;
     __syncthreads();
-    const int mt = warp & 3, fold = warp >> 2;  // every n-tile of (m-tile, fold): one A fragment per k step
-    if (mt * 8 < R) {
-        double acc[NT][2];
+    if (warp * 8 >= R) return;
+    double cs[NT][2], ca[NT][2];
 #pragma unroll
-        for (int t = 0; t < NT; ++t) acc[t][0] = acc[t][1] = 0.0;
-        const double* row = st + (mt * 8 + g) * pitch;
-        const double* B = c.first + (size_t)fold * NT * KK * 32;
+    for (int t = 0; t < NT; ++t) cs[t][0] = cs[t][1] = ca[t][0] = ca[t][1] = 0.0;
+    const double* row = st + (warp * 8 + g) * pitch;
+    const double* Bs = c.first;
+    const double* Ba = c.first + (size_t)NT * KK * 32;
+    const int n = c.n, m = c.m, ms = c.ms;
 #pragma unroll
-        for (int kk = 0; kk < KK; ++kk) {
-            const double av = fold_value(row, nullptr, 4 * kk + q, fold, c.n, c.m, c.ms);
-#pragma unroll
-            for (int nt = 0; nt < NT; ++nt) dmma_8x8x4(acc[nt][0], acc[nt][1], av, __ldg(B + (nt * KK + kk) * 32 + lane));
+    for (int kk = 0; kk < KK; ++kk) {
+        const int k = 4 * kk + q;
+        double vs = 0.0, va = 0.0;
+        if (k < m) {
+            const double lo = row[1 + k], hi = row[n - k];
+            vs = kR2 * (lo + hi);
+            va = kR2 * (lo - hi);
+        } else if (k < ms) {
+            vs = row[1 + k];
         }
-        double* crow = a.C + pr.coff + (long long)(x0 + mt * 8 + g) * 2 * LD + fold * LD;
 #pragma unroll
-        for (int nt = 0; nt < NT; ++nt)
-            *reinterpret_cast<double2*>(crow + nt * 8 + 2 * q) = make_double2(acc[nt][0], acc[nt][1]);
+        for (int nt = 0; nt < NT; ++nt) {
+            dmma_8x8x4(cs[nt][0], cs[nt][1], vs, __ldg(Bs + (nt * KK + kk) * 32 + lane));
+            dmma_8x8x4(ca[nt][0], ca[nt][1], va, __ldg(Ba + (nt * KK + kk) * 32 + lane));
+        }
+    }
+    double* crow = a.C + pr.coff + (long long)(x0 + warp * 8 + g) * 2 * LD;
+#pragma unroll
+    for (int nt = 0; nt < NT; ++nt) {
+        *reinterpret_cast<double2*>(crow + nt * 8 + 2 * q) = make_double2(cs[nt][0], cs[nt][1]);
+        *reinterpret_cast<double2*>(crow + LD + nt * 8 + 2 * q) = make_double2(ca[nt][0], ca[nt][1]);
     }
 }
 
@@ -177,45 +192,52 @@ __device__ void be_columns(const BeArgs& a, const BeProblem& pr, const BeClass& 
     }
 }
 
+// Second transform of one fold of the warp's 8 coefficient rows, in place.
+template <int LD>
+__device__ __forceinline__ void be_second(const double* B, double* rows, int lane)
+{
+    constexpr int NT = LD / 8, KK = LD / 4, PITCH = 2 * LD + 4;
+    const int g = lane >> 2, q = lane & 3;
+    double acc[NT][2];
+#pragma unroll
+    for (int t = 0; t < NT; ++t) acc[t][0] = acc[t][1] = 0.0;
+    const double* row = rows + g * PITCH;
+#pragma unroll
+    for (int kk = 0; kk < KK; ++kk) {
+        const double av = row[4 * kk + q];
+#pragma unroll
+        for (int nt = 0; nt < NT; ++nt) dmma_8x8x4(acc[nt][0], acc[nt][1], av, __ldg(B + (nt * KK + kk) * 32 + lane));
+    }
+    __syncwarp();
+#pragma unroll
+    for (int nt = 0; nt < NT; ++nt)
+        *reinterpret_cast<double2*>(rows + g * PITCH + nt * 8 + 2 * q) = make_double2(acc[nt][0], acc[nt][1]);
+    __syncwarp();
+}
+
 // Kind 3: coefficient rows x0 .. x0+R-1 -> second transform, unfold -> u rows.
+// Warp w owns rows 8 w .. 8 w + 7 from the load to the store.
 template <int LD>
 __device__ void be_rows_out(const BeArgs& a, const BeProblem& pr, const BeClass& c, int idx, double* sm)
 {
     constexpr int NT = LD / 8, KK = LD / 4, PITCH = 2 * LD + 4;
     const int R = pr.nx < BE_ROWS ? pr.nx : BE_ROWS, x0 = idx * BE_ROWS, P = c.P;
-    double* cin = sm;                   // [R][PITCH] coefficients
-    double* vout = sm + R * PITCH;      // [R][PITCH] transformed values: s | d
-    const double* Cb = a.C + pr.coff + (long long)x0 * 2 * LD;
-    for (int e = threadIdx.x; e < R * LD; e += BE_THREADS) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    if (warp * 8 >= R) return;
+    double* rows = sm + warp * 8 * PITCH;  // [8][PITCH]: coefficients, then the transformed values
+    const double* Cb = a.C + pr.coff + (long long)(x0 + warp * 8) * 2 * LD;
+    for (int e = lane; e < 8 * LD; e += 32) {
         const int r = e / LD, j2 = 2 * (e - r * LD);
-        *reinterpret_cast<double2*>(cin + r * PITCH + j2) =
+        *reinterpret_cast<double2*>(rows + r * PITCH + j2) =
             __ldcg(reinterpret_cast<const double2*>(Cb + (long long)r * 2 * LD + j2));
     }
-    __syncthreads();
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, g = lane >> 2, q = lane & 3;
-    const int mt = warp & 3, fold = warp >> 2;
-    if (mt * 8 < R) {
-        double acc[NT][2];
-#pragma unroll
-        for (int t = 0; t < NT; ++t) acc[t][0] = acc[t][1] = 0.0;
-        const double* row = cin + (mt * 8 + g) * PITCH + fold * LD;
-        const double* B = c.second + (size_t)fold * NT * KK * 32;
-#pragma unroll
-        for (int kk = 0; kk < KK; ++kk) {
-            const double av = row[4 * kk + q];
-#pragma unroll
-            for (int nt = 0; nt < NT; ++nt) dmma_8x8x4(acc[nt][0], acc[nt][1], av, __ldg(B + (nt * KK + kk) * 32 + lane));
-        }
-        double* orow = vout + (mt * 8 + g) * PITCH + fold * LD;
-#pragma unroll
-        for (int nt = 0; nt < NT; ++nt)
-            *reinterpret_cast<double2*>(orow + nt * 8 + 2 * q) = make_double2(acc[nt][0], acc[nt][1]);
-    }
-    __syncthreads();
+    __syncwarp();
+    be_second<LD>(c.second, rows, lane);                                          // s: symmetric fold
+    be_second<LD>(c.second + (size_t)NT * KK * 32, rows + LD, lane);              // d: antisymmetric fold
     const int n = c.n, m = c.m, ms = c.ms;
-    double* u = a.u + pr.off + (long long)x0 * P;
-    for (int r = warp; r < R; r += BE_THREADS / 32) {
-        const double* s = vout + r * PITCH;
+    double* u = a.u + pr.off + (long long)(x0 + warp * 8) * P;
+    for (int r = 0; r < 8; ++r) {
+        const double* s = rows + r * PITCH;
         for (int k = lane; k < P; k += 32) {
             double v = 0.0;
             if (k > 0 && k < P - 1) {
@@ -232,13 +254,16 @@ __device__ void be_rows_out(const BeArgs& a, const BeProblem& pr, const BeClass&
 __global__ void __launch_bounds__(BE_THREADS, BE_MINB) batch_eig_kernel(BeArgs a)
 {
     extern __shared__ __align__(16) double bsm[];
-    __shared__ int s_item, s_ok;
+    __shared__ int s_item, s_next, s_ok;
     pdl_enter();
+    if (threadIdx.x == 0) s_item = atomicAdd(a.head, 1);
     for (;;) {
-        if (threadIdx.x == 0) s_item = atomicAdd(a.head, 1);
         __syncthreads();
         const int it = s_item;
         if (it >= a.nitems) break;
+        // take the next item now; it is used after this one (items are still
+        // taken in queue order, so every wait is on an earlier item)
+        if (threadIdx.x == 0) s_next = atomicAdd(a.head, 1);
         const int code = a.items[it];
         const int kind = code >> 28, b = (code >> 12) & 0xffff, idx = code & 0xfff;
         const BeProblem pr = a.prob[b];
@@ -286,7 +311,10 @@ __global__ void __launch_bounds__(BE_THREADS, BE_MINB) batch_eig_kernel(BeArgs a
         }
         // publish: the CTA's writes, then one release increment of the counter
         __syncthreads();
-        if (threadIdx.x == 0 && kind < 3) red_release_add(kind == 1 ? &a.done1[b] : &a.done2[b]);
+        if (threadIdx.x == 0) {
+            if (kind < 3) red_release_add(kind == 1 ? &a.done1[b] : &a.done2[b]);
+            s_item = s_next;
+        }
     }
 }
 
@@ -316,6 +344,10 @@ struct BatchEig {
 
     int alloc(void** p, size_t n)
     {
+        if (alloc_fault_fires()) {
+            *p = nullptr;
+            return HELM_ERR_OOM;
+        }
         if (cudaMalloc(p, n) != cudaSuccess) {
             cudaGetLastError();
             *p = nullptr;
@@ -438,7 +470,7 @@ int batch_eig_create(int nprob, const int* Nx, const int* N, const double* lambd
         coff += (long long)Nx[i] * 2 * c.ld;
         const int R = std::min(Nx[i], BE_ROWS);
         smem = std::max(smem, (size_t)R * c.pitch * sizeof(double));
-        smem = std::max(smem, (size_t)2 * R * (2 * c.ld + 4) * sizeof(double));
+        smem = std::max(smem, (size_t)R * (2 * c.ld + 4) * sizeof(double));
         smem = std::max(smem, (size_t)Nx[i] * (be_cols(Nx[i], c.ld) + 1) * sizeof(double2));
     }
     if (st) {

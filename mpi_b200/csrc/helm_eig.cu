@@ -88,11 +88,14 @@ __device__ __forceinline__ void load_plane(const EigArgs& a, const double* f, co
 // slots 0..31 (symmetric fold) and 32..63 (antisymmetric fold).
 template <int MTW>
 __device__ __forceinline__ void first_transform(const EigArgs& a, double* rows, const double* Ms, const double* Ma,
-                                                const double* hbc, int lane, int in_off = 0)
+                                                const double* hbc, int lane, int in_off = 0,
+                                                const double* sub_rows = nullptr)
 {
     // the staged rows start in_off doubles into each row (a TMA copy whose
-    // source began 8 bytes before the row); the coefficients go to slot 0 on
+    // source began 8 bytes before the row); the coefficients go to slot 0 on.
+    // sub_rows: the same rows of u_obs, subtracted (misfit adjoint)
     const double* src = rows + in_off;
+    const double* sbs = sub_rows ? sub_rows + in_off : nullptr;
     const int g = lane >> 2, q = lane & 3;
     const int n = a.n, m = a.m, ms = a.ms, P = a.P;
     double cs[MTW][4][2], ca[MTW][4][2];
@@ -107,13 +110,18 @@ __device__ __forceinline__ void first_transform(const EigArgs& a, double* rows, 
 #pragma unroll
         for (int mt = 0; mt < MTW; ++mt) {
             const double* row = src + (mt * 8 + g) * EP_PITCH;
+            const double* srow = sbs ? sbs + (mt * 8 + g) * EP_PITCH : nullptr;
             double vs = 0.0, va = 0.0;
             if (k < m) {
-                const double lo = row[1 + k], hi = row[n - k];
+                double lo = row[1 + k], hi = row[n - k];
+                if (srow) {
+                    lo -= srow[1 + k];
+                    hi -= srow[n - k];
+                }
                 vs = kR2 * (lo + hi);
                 va = kR2 * (lo - hi);
             } else if (k < ms) {
-                vs = row[1 + k];
+                vs = srow ? row[1 + k] - srow[1 + k] : row[1 + k];
             }
             as[mt] = vs;
             aa[mt] = va;
@@ -257,6 +265,7 @@ __device__ __forceinline__ void c2r_assemble(double2* z, int warp, int lane, Fet
 // [Nx][x_stride] doubles, box EP_PITCH x (Nx / 4) (x / 4 rows of one plane).
 struct EigMaps {
     CUtensorMap f;
+    CUtensorMap sub;  // the misfit adjoint's u_obs, the same shape (planes up to 128 rows)
 };
 
 template <int L>
@@ -274,6 +283,8 @@ __global__ void __launch_bounds__(EpShape<L>::THREADS, 1) eig_fwd_kernel(EigArgs
     __shared__ __align__(8) uint64_t bar[B::NQ];
     double* buf = esm;
     double* Mt = esm + (size_t)L * EP_PITCH;
+    // misfit adjoint with TMA loads: u_obs's plane after the transforms
+    double* sbuf = (a.tma && a.sub) ? Mt + 2 * EP_FRAG : nullptr;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int y = blockIdx.x;
     const bool tma = a.tma != 0;
@@ -295,9 +306,11 @@ __global__ void __launch_bounds__(EpShape<L>::THREADS, 1) eig_fwd_kernel(EigArgs
         const int sh = (int)(((long long)y * a.P) & 1);
         if (threadIdx.x == 0) {
             const int c0 = y * a.P - sh;
+            const uint32_t box = (uint32_t)(B::QR * EP_PITCH * sizeof(double));
             for (int q = 0; q < B::NQ; ++q) {
-                mbar_arrive_expect_tx(&bar[q], (uint32_t)(B::QR * EP_PITCH * sizeof(double)));
+                mbar_arrive_expect_tx(&bar[q], sbuf ? 2 * box : box);
                 tma_load_2d(buf + (size_t)q * B::QR * EP_PITCH, &tm.f, c0, q * B::QR, &bar[q]);
+                if (sbuf) tma_load_2d(sbuf + (size_t)q * B::QR * EP_PITCH, &tm.sub, c0, q * B::QR, &bar[q]);
             }
         }
         tma_ok = mbar_wait(&bar[(warp * S::RW) / B::QR], 0);
@@ -310,7 +323,9 @@ __global__ void __launch_bounds__(EpShape<L>::THREADS, 1) eig_fwd_kernel(EigArgs
             rows[lane * EP_PITCH + sh + a.P - 1] = gr ? gr[x * a.bc_x_stride + y] * a.ibr : 0.0;
         }
         __syncwarp();
-        if (tma_ok) first_transform<S::MTW>(a, rows, Mt, Mt + EP_FRAG, a.hbc, lane, sh);
+        if (tma_ok)
+            first_transform<S::MTW>(a, rows, Mt, Mt + EP_FRAG, a.hbc, lane, sh,
+                                    sbuf ? sbuf + warp * S::RW * EP_PITCH : nullptr);
     } else {
         load_plane<L>(a, a.f, a.adjoint ? nullptr : a.gl, a.adjoint ? nullptr : a.gr, (long long)y * a.P, y, buf);
         __syncthreads();
@@ -582,10 +597,14 @@ int run_3d(int pass, const EigArgs& a, cudaStream_t s)
             const uint64_t dims[2] = {(uint64_t)a.x_stride, (uint64_t)L};
             const uint64_t str[1] = {(uint64_t)a.x_stride * sizeof(double)};
             const uint32_t box[2] = {EP_PITCH, (uint32_t)FwdBoxes<L>::QR};
-            if (!encode_tmap_f64_2d(&tm.f, a.f, dims, str, box)) a1.tma = 0;  // element-wise loads instead
+            if (!encode_tmap_f64_2d(&tm.f, a.f, dims, str, box) ||
+                (a.sub && !encode_tmap_f64_2d(&tm.sub, a.sub, dims, str, box)))
+                a1.tma = 0;  // element-wise loads instead
         }
-        if ((e = prep(eig_fwd_kernel<L>, sm1)) != cudaSuccess) return (int)e;
-        return (int)launch_k(eig_fwd_kernel<L>, dim3(a.Ny), dim3(S::THREADS), sm1, s, a1, tm);
+        // the misfit adjoint's TMA path stages u_obs's plane beside f's
+        const size_t smf = (a1.tma && a1.sub) ? sm1 + (size_t)L * EP_PITCH * sizeof(double) : sm1;
+        if ((e = prep(eig_fwd_kernel<L>, smf)) != cudaSuccess) return (int)e;
+        return (int)launch_k(eig_fwd_kernel<L>, dim3(a.Ny), dim3(S::THREADS), smf, s, a1, tm);
     }
     if (pass == 2) {
         if ((e = prep(eig_inv_kernel<L>, sm1)) != cudaSuccess) return (int)e;
@@ -630,9 +649,11 @@ int run_2d(const EigArgs& a, int nprob, cudaStream_t s)
 
 }  // namespace
 
-bool eig_tma_ok(const EigArgs& a)
+bool eig_tma_ok(const EigArgs& a, int Nx)
 {
-    return (reinterpret_cast<uintptr_t>(a.f) & 15) == 0 && (a.x_stride & 1) == 0 && !a.sub;
+    auto al = [](const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15) == 0; };
+    // with u_obs the two planes share the shared memory: planes of at most 128 rows
+    return al(a.f) && (a.x_stride & 1) == 0 && (!a.sub || (al(a.sub) && Nx <= 128));
 }
 
 bool eig_shape_ok(int dim, int Nx, int Ny, int P)

@@ -40,8 +40,8 @@ struct EigArgs {
     double* gbar_r;
     const double* lam_u;
     double* lam_out;
-    // 3D pass 1: load each plane of f with tensor-memory-accelerator copies
-    // (f 16-byte aligned with an even x stride; not the misfit adjoint), and
+    // 3D pass 1: load each plane of f (and u_obs) with tensor-memory-accelerator
+    // copies (16-byte aligned arrays with an even x stride), and
     // the device status word that a copy wait which ran out sets (NULL: none)
     int tma;
     int* err;
@@ -50,8 +50,8 @@ struct EigArgs {
     int conv_var;
 };
 
-// Whether pass 1 can load these arrays with TMA copies.
-bool eig_tma_ok(const EigArgs& a);
+// Whether pass 1 can load these arrays with TMA copies (Nx: plane rows).
+bool eig_tma_ok(const EigArgs& a, int Nx);
 
 // Whether the pipeline covers a plan of this shape (FP64 arithmetic).
 bool eig_shape_ok(int dim, int Nx, int Ny, int P);

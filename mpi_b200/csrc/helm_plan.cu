@@ -59,14 +59,20 @@ void Plan::release()
 // fails as a cudaMalloc failure would, and the hook disarms itself.
 static std::atomic<long long> g_alloc_fault{-1};
 
+bool alloc_fault_fires()
+{
+    if (g_alloc_fault.load() >= 0 && g_alloc_fault.fetch_sub(1) == 0) {
+        g_last_error = "device allocation failure injected by helm_debug_fail_alloc";
+        return true;
+    }
+    return false;
+}
+
 int Plan::alloc(void** p, size_t bytes)
 {
     *p = nullptr;
     if (bytes == 0) return HELM_OK;
-    if (g_alloc_fault.load() >= 0 && g_alloc_fault.fetch_sub(1) == 0) {
-        g_last_error = "device allocation failure injected by helm_debug_fail_alloc";
-        return HELM_ERR_OOM;
-    }
+    if (alloc_fault_fires()) return HELM_ERR_OOM;
     cudaError_t e = cudaMalloc(p, bytes);
     if (e != cudaSuccess) {
         *p = nullptr;
@@ -765,7 +771,7 @@ static int run_pipeline(Plan& p, const void* in, const double* gl, const double*
         ea.scale = 1.0 / ((double)p.Nx * (p.dim == 3 ? p.Ny : 1));
         ea.boff = p.d_boff;  // size-class plans of a batch: the packed offsets (one problem or more)
         ea.err = p.d_status;
-        ea.tma = (p.dim == 3 && eig_tma_ok(ea)) ? 1 : 0;
+        ea.tma = (p.dim == 3 && eig_tma_ok(ea, p.Nx)) ? 1 : 0;
         ea.conv_var = p.fft_var[1] & 1;
         int e = launch_eig_pass(0, p.dim, p.Nx, ea, p.batch, s);
         if (e) return set_cuda_error((cudaError_t)e, "eigen-basis pass 1");

@@ -161,5 +161,8 @@ int solve(Plan& p, const void* f, const double* gl, const double* gr, void* u, c
 int create_batch_class(int Nx, int N, double xl, double xr, double yl, double yr, const std::vector<double>& lams,
                        const std::vector<long long>& offs, long long packed_elems, int precision, Plan** out);
 void set_last_error(const char* msg);
+// The host-side allocation fault hook (helm_debug_fail_alloc): true when the
+// caller's next device allocation is to fail (the last error then says so).
+bool alloc_fault_fires();
 
 }  // namespace helm
