@@ -401,7 +401,12 @@ def run_ours(args, ws, rank, local):
 
     res = {}
     for name, p in plans.items():
+        # the headline's timed region is the profiler range (ncu --profile-from-start off)
+        if name == "fp32_refine":
+            torch.cuda.profiler.start()
         total_ms = timed(lambda p=p, name=name: p.SolvePDE(f, out=outs[name]))
+        if name == "fp32_refine":
+            torch.cuda.profiler.stop()
         res[name] = total_ms
     kernels = {k: p.kernels() for k, p in plans.items()}
     launches = len(kernels["fp32_refine"].split()) * args.steps  # the headline's timed solves
@@ -735,7 +740,7 @@ def _leg_fd(dev, flush, stream, steps, warmup, cpu=False):
     us = {}
     peak, _ = _peak_hbm()
     f32 = f.float()
-    for prec in ("fp32", "fp64"):
+    for prec in ("fp32", "fp32_refine", "fp64"):
         p = Helmholtz3DFD(Nx, Ny, Nz, 0.0, 1.0, 0.0, 1.0, 0.0, 1.0, Lambda=1.0, precision=prec)
         # the FP32 plan reads f and writes u in FP32 (4 B per point each way)
         fi = f
@@ -747,6 +752,12 @@ def _leg_fd(dev, flush, stream, steps, warmup, cpu=False):
         ubar = u.double()  # the adjoint takes and returns FP64 arrays
         adj = _ev_ms(lambda: p.SolveAdjoint(ubar), flush, stream, steps, warmup)
         out[prec] = {"value": dof / (fwd * 1e-3) / 1e9, "unit": "GDOF/s", "forward_ms": fwd, "adjoint_ms": adj}
+        if prec == "fp32_refine":
+            # FP32 solve + 2 sweeps of FP64 stencil residual and FP32 correction
+            out[prec]["kernels"] = p.kernels()
+            us[prec] = u
+            p.DestroyPDEPlan()
+            continue
         # per-pass HBM fraction at this size: algorithmic bytes = input + output of each pass
         p.enable_stage_timing(True)
         st = {}
@@ -765,6 +776,7 @@ def _leg_fd(dev, flush, stream, steps, warmup, cpu=False):
         us[prec] = u.double()
         p.DestroyPDEPlan()
     out["rel_l2_fp32_vs_fp64"] = float((us["fp32"] - us["fp64"]).norm() / us["fp64"].norm())
+    out["rel_l2_fp32_refine_vs_fp64"] = float((us["fp32_refine"] - us["fp64"]).norm() / us["fp64"].norm())
     if cpu:
         # no reference implementation of a direct FD solve exists (HypreFDM is
         # iterative and needs HYPRE): the C restatement on one core, 256 x 256 x 256

@@ -78,11 +78,12 @@ __device__ __forceinline__ void pass_to_smem(cplx_t<T>* sm, int tc, int cl, cons
 // The real outputs of one thread of a C2R pass: columns c0 (and c1 when has1)
 // at the rows of its last-pass items v[t RL + r], scaled by sc.  In an adjoint
 // pass (a.adj_mode) the GLL boundary slots also go to the boundary cotangents
-// and acc gathers the lambda sum; the forward solution values it needs are
-// loaded for a whole group of RL rows before any store of that group.
+// (first slot of batch a.gl_batch, last slot of batch a.gr_batch: the first and
+// last GLL element) and acc gathers the lambda sum; the forward solution values
+// it needs are loaded for a whole group of RL rows before any store of that group.
 template <bool ADJ, typename T, typename TIO, int R0, int RL, int NSL, int TPC>
-__device__ __forceinline__ void c2r_store(const FftArgs& a, TIO* out, long long out_base, int tc, int c0, int c1,
-                                          bool has1, const cplx_t<T> (&v)[R0], T sc, double& acc)
+__device__ __forceinline__ void c2r_store(const FftArgs& a, TIO* out, long long out_base, int b, int tc, int c0,
+                                          int c1, bool has1, const cplx_t<T> (&v)[R0], T sc, double& acc)
 {
     if constexpr (!ADJ) {
 #pragma unroll
@@ -106,6 +107,8 @@ __device__ __forceinline__ void c2r_store(const FftArgs& a, TIO* out, long long 
     const int k0 = c0 % P, j0 = c0 / P, k1 = c1 % P, j1 = c1 / P;
     const bool b0 = k0 == 0 || k0 == P - 1, b1 = k1 == 0 || k1 == P - 1;
     const bool zero0 = a.adj_mode == 1 && b0, zero1 = a.adj_mode == 1 && b1;
+    double* const gbl = b == a.gl_batch ? a.gbar_l : nullptr;
+    double* const gbr = b == a.gr_batch ? a.gbar_r : nullptr;
     const double* u = a.lam_u ? a.lam_u + out_base : nullptr;
 #pragma unroll
     for (int t = 0; t < R0 / RL; ++t) {
@@ -123,12 +126,12 @@ __device__ __forceinline__ void c2r_store(const FftArgs& a, TIO* out, long long 
             // (accumulate: a refinement sweep adds its correction to fbar and gbar)
             const double keep = a.accumulate ? 1.0 : 0.0;
             if (b0) {
-                if (k0 == 0 && a.gbar_l) {
-                    double* g = &a.gbar_l[row * a.bc_row + j0];
+                if (k0 == 0 && gbl) {
+                    double* g = &gbl[row * a.bc_row + j0];
                     *g = keep * *g + a.adj_scale_l * x0;
                 }
-                if (k0 == P - 1 && a.gbar_r) {
-                    double* g = &a.gbar_r[row * a.bc_row + j0];
+                if (k0 == P - 1 && gbr) {
+                    double* g = &gbr[row * a.bc_row + j0];
                     *g = keep * *g + a.adj_scale_r * x0;
                 }
             }
@@ -139,12 +142,12 @@ __device__ __forceinline__ void c2r_store(const FftArgs& a, TIO* out, long long 
             acc += x0 * u0[r];
             if (has1) {
                 if (b1) {
-                    if (k1 == 0 && a.gbar_l) {
-                        double* g = &a.gbar_l[row * a.bc_row + j1];
+                    if (k1 == 0 && gbl) {
+                        double* g = &gbl[row * a.bc_row + j1];
                         *g = keep * *g + a.adj_scale_l * x1;
                     }
-                    if (k1 == P - 1 && a.gbar_r) {
-                        double* g = &a.gbar_r[row * a.bc_row + j1];
+                    if (k1 == P - 1 && gbr) {
+                        double* g = &gbr[row * a.bc_row + j1];
                         *g = keep * *g + a.adj_scale_r * x1;
                     }
                 }
@@ -316,7 +319,7 @@ __global__ void __launch_bounds__(THREADS) fft_kernel(FftArgs a, long long total
     } else if constexpr (MODE == FFT_C2R || MODE == FFT_C2R_ADJ) {
         double acc = 0.0;
         if (valid)
-            c2r_store<MODE == FFT_C2R_ADJ, T, TIO, R0, RL, NSL, TPC>(a, static_cast<TIO*>(a.out) + out_base, out_base, tc, c0, c1, has1, v,
+            c2r_store<MODE == FFT_C2R_ADJ, T, TIO, R0, RL, NSL, TPC>(a, static_cast<TIO*>(a.out) + out_base, out_base, b, tc, c0, c1, has1, v,
                                                 sc, acc);
         if constexpr (MODE == FFT_C2R_ADJ)
             if (a.lam_out) c2r_lambda_sum(a, acc);
@@ -549,8 +552,8 @@ __global__ void __launch_bounds__(THREADS) fft_pipe_kernel(FftArgs a, long long 
             }
         } else if constexpr (MODE == FFT_C2R || MODE == FFT_C2R_ADJ) {
             if (valid)
-                c2r_store<MODE == FFT_C2R_ADJ, T, TIO, R0, RL, NSL, TPC>(a, static_cast<TIO*>(a.out) + out_base, out_base, tc, c0, c1, has1,
-                                                    v, sc, lam_acc);
+                c2r_store<MODE == FFT_C2R_ADJ, T, TIO, R0, RL, NSL, TPC>(a, static_cast<TIO*>(a.out) + out_base, out_base, b, tc, c0, c1,
+                                                    has1, v, sc, lam_acc);
         } else {
             __syncthreads();
             pass_to_smem<T, L, RL, NSL, TPC, CT, R0>(sm, tc, cl, v);
@@ -885,9 +888,156 @@ __global__ void __launch_bounds__(ROW_WARPS * 32) rows_kernel(RowArgs a)
             d0ul = a.homs[grp * 4 + 0]; d0ur = a.homs[grp * 4 + 1];
             dNul = a.homs[grp * 4 + 2]; dNur = a.homs[grp * 4 + 3];
         }
+        // the interior collocation solve of one element (transposed in an
+        // adjoint run), with the FP64-residual sweeps of a refined plan
+        auto solve_interior = [&](const TS (&fr)[NSLOT], const TS (&fi)[NSLOT], TS (&xr)[NSLOT], TS (&xi)[NSLOT]) {
+            TF yr[NSLOT], yi[NSLOT];
+#pragma unroll
+            for (int s = 0; s < NSLOT; ++s) { yr[s] = (TF)fr[s]; yi[s] = (TF)fi[s]; }
+            if (METHOD == 1) lu_core<TF, NSLOT>(sMat, ld, sDiag, sPerm, n, yr, yi, reinterpret_cast<TF*>(scrRaw), lane);
+            else fdm_core<TF, NSLOT>(sMat, sMat + (size_t)n * ld, ld, rdiag, n, yr, yi, reinterpret_cast<CF*>(scrRaw), lane);
+#pragma unroll
+            for (int s = 0; s < NSLOT; ++s) { xr[s] = (TS)yr[s]; xi[s] = (TS)yi[s]; }
+            if (REFINE) {
+                // FP64 residual r = f - (D2int x - sigma x), then a corrected FP32 solve
+                CS* scr = reinterpret_cast<CS*>(scrRaw);
+                for (int sw = 0; sw < a.sweeps; ++sw) {
+                    __syncwarp();
+#pragma unroll
+                    for (int s = 0; s < NSLOT; ++s) scr[lane + 32 * s] = mk(xr[s], xi[s]);
+                    __syncwarp();
+                    TS rr_[NSLOT], ri_[NSLOT];
+#pragma unroll
+                    for (int s = 0; s < NSLOT; ++s) {
+                        rr_[s] = fr[s] + (TS)sig * xr[s];
+                        ri_[s] = fi[s] + (TS)sig * xi[s];
+                    }
+                    for (int k = 0; k < n; ++k) {
+                        const CS xk = scr[k];
+                        const double* col = sD2 + (size_t)k * ld;
+#pragma unroll
+                        for (int s = 0; s < NSLOT; ++s) {
+                            const double d = col[lane + 32 * s];
+                            rr_[s] -= d * xk.x;
+                            ri_[s] -= d * xk.y;
+                        }
+                    }
+                    __syncwarp();
+#pragma unroll
+                    for (int s = 0; s < NSLOT; ++s) { yr[s] = (TF)rr_[s]; yi[s] = (TF)ri_[s]; }
+                    if (METHOD == 1) lu_core<TF, NSLOT>(sMat, ld, sDiag, sPerm, n, yr, yi, reinterpret_cast<TF*>(scrRaw), lane);
+                    else fdm_core<TF, NSLOT>(sMat, sMat + (size_t)n * ld, ld, rdiag, n, yr, yi, reinterpret_cast<CF*>(scrRaw), lane);
+#pragma unroll
+                    for (int s = 0; s < NSLOT; ++s) { xr[s] += (TS)yr[s]; xi[s] += (TS)yi[s]; }
+                }
+            }
+        };
         const int r0 = a.grp_start[grp], r1 = a.grp_start[grp + 1];
         for (int rr = r0 + warp; rr < r1; rr += ROW_WARPS) {
             const long long rowoff = (long long)a.grp_rows[rr] * P;
+            if (ADJ && Ns > 1) {
+                // Transposed map of several elements.  Forward: per row the
+                // interface values z_0 .. z_Ns solve T z = h with h_0 = gl +
+                // al D0.phi_0, h_j = D0.phi_j - DN.phi_{j-1}, h_Ns = gr - ar
+                // DN.phi_{Ns-1}, and element j is u = phi_j + z_j ul + z_{j+1} ur
+                // (phi_j = A^-1 f_j).  Transposed: zbar_j gathers ubar at the
+                // nodes equal to z_j and ubar . ul / ur of the adjacent
+                // elements, w = T^-T zbar (the forward LU factors of T, used
+                // transposed), then phibar_j = ubar_j + (d0bar_j D0 + dNbar_j
+                // DN) on the interior, fbar_j = A^-T phibar_j, glbar = w_0,
+                // grbar = w_Ns (left in the boundary slots for the last pass).
+                const double* ul = a.fhom + (size_t)grp * 2 * P;
+                const double* ur = ul + P;
+                const double D0ul = a.fhoms[grp * 4 + 0], D0ur = a.fhoms[grp * 4 + 1];
+                const double DNul = a.fhoms[grp * 4 + 2], DNur = a.fhoms[grp * 4 + 3];
+                if (lane == 0)
+                    for (int j = 0; j <= Ns; ++j) { sNs[j * 6 + 0] = 0; sNs[j * 6 + 1] = 0; }
+                __syncwarp();
+                for (int jj = 0; jj < Ns; ++jj) {
+                    const CS* row = spec + (long long)jj * a.elem_stride + rowoff;
+                    TS slr = 0, sli = 0, srr = 0, sri = 0;
+#pragma unroll
+                    for (int s = 0; s < NSLOT; ++s) {
+                        const int i = lane + 32 * s;
+                        if (i < n) {
+                            const CS v = row[1 + i];
+                            const TS l = (TS)ul[1 + i], r = (TS)ur[1 + i];
+                            slr += l * v.x; sli += l * v.y;
+                            srr += r * v.x; sri += r * v.y;
+                        }
+                    }
+                    slr = warp_sum(slr); sli = warp_sum(sli);
+                    srr = warp_sum(srr); sri = warp_sum(sri);
+                    if (lane == 0) {
+                        const CS b0 = row[0], bN = row[P - 1];
+                        sNs[jj * 6 + 0] += b0.x + slr; sNs[jj * 6 + 1] += b0.y + sli;
+                        sNs[(jj + 1) * 6 + 0] += bN.x + srr; sNs[(jj + 1) * 6 + 1] += bN.y + sri;
+                    }
+                    __syncwarp();
+                }
+                if (lane == 0) {
+                    // T = L U without pivoting, as the forward sweep eliminates:
+                    // U diagonal b_j, super c_j; L sub q_j = T[j][j-1] / b_{j-1}.
+                    // U^T y = zbar (forward), then L^T w = y (backward).
+                    TS bp = 0, cp = 0, yr_ = 0, yi_ = 0;
+                    for (int j = 0; j <= Ns; ++j) {
+                        TS bj, cj;
+                        if (j == 0) {
+                            bj = (TS)(a.bl - a.al * D0ul);
+                            cj = (TS)(-a.al * D0ur);
+                        } else if (j < Ns) {
+                            bj = (TS)(DNur - D0ul) - ((TS)DNul / bp) * cp;
+                            cj = (TS)(-D0ur);
+                        } else {
+                            bj = (TS)(a.ar * DNur + a.br) - ((TS)(a.ar * DNul) / bp) * cp;
+                            cj = 0;
+                        }
+                        yr_ = (sNs[j * 6 + 0] - cp * yr_) / bj;
+                        yi_ = (sNs[j * 6 + 1] - cp * yi_) / bj;
+                        sNs[j * 6 + 2] = yr_; sNs[j * 6 + 3] = yi_; sNs[j * 6 + 4] = bj;
+                        bp = bj; cp = cj;
+                    }
+                    TS wr = sNs[Ns * 6 + 2], wi = sNs[Ns * 6 + 3];
+                    for (int j = Ns - 1; j >= 0; --j) {
+                        const TS q = (j + 1 < Ns ? (TS)DNul : (TS)(a.ar * DNul)) / sNs[j * 6 + 4];
+                        wr = sNs[j * 6 + 2] - q * wr;
+                        wi = sNs[j * 6 + 3] - q * wi;
+                        sNs[j * 6 + 2] = wr; sNs[j * 6 + 3] = wi;
+                    }
+                }
+                __syncwarp();
+                for (int jj = 0; jj < Ns; ++jj) {
+                    CS* row = spec + (long long)jj * a.elem_stride + rowoff;
+                    const TS w0r = sNs[jj * 6 + 2], w0i = sNs[jj * 6 + 3];
+                    const TS w1r = sNs[(jj + 1) * 6 + 2], w1i = sNs[(jj + 1) * 6 + 3];
+                    const TS s0 = jj == 0 ? (TS)a.al : (TS)1;           // d0bar = s0 w_jj
+                    const TS s1 = jj == Ns - 1 ? (TS)-a.ar : (TS)-1;    // dNbar = s1 w_{jj+1}
+                    TS fr[NSLOT], fi[NSLOT], xr[NSLOT], xi[NSLOT];
+#pragma unroll
+                    for (int s = 0; s < NSLOT; ++s) {
+                        const int i = lane + 32 * s;
+                        fr[s] = 0; fi[s] = 0;
+                        if (i < n) {
+                            const CS v = row[1 + i];
+                            const TS c0 = (TS)a.fd0[1 + i], cN = (TS)a.fdN[1 + i];
+                            fr[s] = v.x + s0 * w0r * c0 + s1 * w1r * cN;
+                            fi[s] = v.y + s0 * w0i * c0 + s1 * w1i * cN;
+                        }
+                    }
+                    solve_interior(fr, fi, xr, xi);
+#pragma unroll
+                    for (int s = 0; s < NSLOT; ++s) {
+                        const int i = lane + 32 * s;
+                        if (i < n) row[1 + i] = mk(xr[s], xi[s]);
+                    }
+                    if (lane == 0) {
+                        row[0] = jj == 0 ? mk(w0r, w0i) : mk((TS)0, (TS)0);
+                        row[P - 1] = jj == Ns - 1 ? mk(w1r, w1i) : mk((TS)0, (TS)0);
+                    }
+                }
+                __syncwarp();
+                continue;
+            }
             TS pr = 0, pi = 0;                        // running d/dy of the previous element (Ns > 1)
             TS rhs_r = 0, rhs_i = 0, bprev = 0, cprev = 0;
             TS d0r = 0, d0i = 0, dNr = 0, dNi = 0;
@@ -904,46 +1054,7 @@ __global__ void __launch_bounds__(ROW_WARPS * 32) rows_kernel(RowArgs a)
                     fi[s] = v.y;
                 }
                 // ---- collocation solve of the interior nodes ----
-                TF yr[NSLOT], yi[NSLOT];
-#pragma unroll
-                for (int s = 0; s < NSLOT; ++s) { yr[s] = (TF)fr[s]; yi[s] = (TF)fi[s]; }
-                if (METHOD == 1) lu_core<TF, NSLOT>(sMat, ld, sDiag, sPerm, n, yr, yi, reinterpret_cast<TF*>(scrRaw), lane);
-                else fdm_core<TF, NSLOT>(sMat, sMat + (size_t)n * ld, ld, rdiag, n, yr, yi, reinterpret_cast<CF*>(scrRaw), lane);
-#pragma unroll
-                for (int s = 0; s < NSLOT; ++s) { xr[s] = (TS)yr[s]; xi[s] = (TS)yi[s]; }
-                if (REFINE) {
-                    // FP64 residual r = f - (D2int x - sigma x), then a corrected FP32 solve
-                    CS* scr = reinterpret_cast<CS*>(scrRaw);
-                    for (int sw = 0; sw < a.sweeps; ++sw) {
-                        __syncwarp();
-#pragma unroll
-                        for (int s = 0; s < NSLOT; ++s) scr[lane + 32 * s] = mk(xr[s], xi[s]);
-                        __syncwarp();
-                        TS rr_[NSLOT], ri_[NSLOT];
-#pragma unroll
-                        for (int s = 0; s < NSLOT; ++s) {
-                            rr_[s] = fr[s] + (TS)sig * xr[s];
-                            ri_[s] = fi[s] + (TS)sig * xi[s];
-                        }
-                        for (int k = 0; k < n; ++k) {
-                            const CS xk = scr[k];
-                            const double* col = sD2 + (size_t)k * ld;
-#pragma unroll
-                            for (int s = 0; s < NSLOT; ++s) {
-                                const double d = col[lane + 32 * s];
-                                rr_[s] -= d * xk.x;
-                                ri_[s] -= d * xk.y;
-                            }
-                        }
-                        __syncwarp();
-#pragma unroll
-                        for (int s = 0; s < NSLOT; ++s) { yr[s] = (TF)rr_[s]; yi[s] = (TF)ri_[s]; }
-                        if (METHOD == 1) lu_core<TF, NSLOT>(sMat, ld, sDiag, sPerm, n, yr, yi, reinterpret_cast<TF*>(scrRaw), lane);
-                        else fdm_core<TF, NSLOT>(sMat, sMat + (size_t)n * ld, ld, rdiag, n, yr, yi, reinterpret_cast<CF*>(scrRaw), lane);
-#pragma unroll
-                        for (int s = 0; s < NSLOT; ++s) { xr[s] += (TS)yr[s]; xi[s] += (TS)yi[s]; }
-                    }
-                }
+                solve_interior(fr, fi, xr, xi);
                 if (ADJ) {
                     // transposed collocation system: boundary unknowns from the 2x2
                     // system, interior = psi + v0 pl + vN pr (one element)
@@ -1222,8 +1333,8 @@ static int run_rows(const RowArgs& a, cudaStream_t s)
 template <int NSLOT>
 static int rows_dispatch_prec(int method, int prec, const RowArgs& a, cudaStream_t s)
 {
-    if (a.adjoint) {  // transposed solve: FDM only, one element
-        if (method != 2 || a.Ns != 1) return (int)cudaErrorInvalidValue;
+    if (a.adjoint) {  // transposed solve: FDM only; several elements not periodic
+        if (method != 2 || (a.Ns > 1 && (a.periodic || !a.fhom))) return (int)cudaErrorInvalidValue;
         if (prec == 0) return run_rows<double, double, NSLOT, 2, false, true>(a, s);
         if (prec == 1) return run_rows<float, float, NSLOT, 2, false, true>(a, s);
         return run_rows<double, float, NSLOT, 2, true, true>(a, s);

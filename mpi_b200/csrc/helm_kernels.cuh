@@ -121,6 +121,14 @@ struct RowArgs {
     // DN.ul, DN.ur in both directions, and the adjoint (one element) reads
     // pl = A^-T (DN - D0), pr = 0
     int periodic;
+    // adjoint with several elements (Ns > 1, not periodic): the forward
+    // homogeneous solutions ul, ur [ngroups][2][P], their end slopes
+    // [ngroups][4] and the first / last rows of D (the forward data; vinvT / vT
+    // then hold the transposed transforms for the interior solves)
+    const double* fhom;
+    const double* fhoms;
+    const double* fd0;
+    const double* fdN;
 };
 
 // Derivative along the GLL direction of every row of P values: du = M u with

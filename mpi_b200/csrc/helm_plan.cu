@@ -239,6 +239,34 @@ static int setup_adjoint(Plan& p, const std::vector<double>& A0, const std::vect
     return HELM_OK;
 }
 
+// Transposed interior solves of a plan with several GLL elements (not
+// periodic): A^T = V^-T diag(lam) V^T and D2int^T for the refinement residual.
+// The interface system is transposed inside the row kernel from the forward
+// homogeneous solutions and end slopes, which such a plan already holds.
+static int setup_adjoint_multi(Plan& p, const std::vector<double>& A0, const std::vector<double>& V,
+                               const std::vector<double>& Vi, int prec_code)
+{
+    const int n = p.n, ld = p.ld;
+    std::vector<double> vtT((size_t)n * ld, 0.0), vinvtT((size_t)n * ld, 0.0), d2row((size_t)n * ld, 0.0);
+    for (int k = 0; k < n; ++k)
+        for (int i = 0; i < n; ++i) {
+            vtT[(size_t)k * ld + i] = V[k * n + i];
+            vinvtT[(size_t)k * ld + i] = Vi[k * n + i];
+            d2row[(size_t)k * ld + i] = A0[k * n + i];
+        }
+    auto up_mat = [&](const std::vector<double>& h, void** d) -> int {
+        if (prec_code == 0) return p.upload(d, h.data(), h.size() * sizeof(double));
+        std::vector<float> f(h.begin(), h.end());
+        return p.upload(d, f.data(), f.size() * sizeof(float));
+    };
+    int st;
+    if ((st = up_mat(vtT, &p.d_vtT))) return st;
+    if ((st = up_mat(vinvtT, &p.d_vinvtT))) return st;
+    if ((st = p.upload((void**)&p.d_d2row, d2row.data(), d2row.size() * sizeof(double)))) return st;
+    p.adj_ready = true;
+    return HELM_OK;
+}
+
 // Folded fast-diagonalisation data (helm_fdm.cu): the orthogonal even/odd
 // fold Q of the interior nodes block-diagonalises the centrosymmetric D2int,
 // Q D2int Q^T = diag(Ms, Ma); each block gets its own eigen-decomposition.
@@ -630,6 +658,8 @@ static int setup_plan(Plan& p)
     if (!lu && p.Ns == 1) {
         if (p.packed_elems == 0 && (st = setup_adjoint(p, A0, lam, V, Vi, prec_code, homs))) return st;
         if ((st = setup_fast(p, A0, prec_code))) return st;
+    } else if (!lu && !p.periodic && p.packed_elems == 0 && p.batch == 1) {
+        if ((st = setup_adjoint_multi(p, A0, V, Vi, prec_code))) return st;
     }
     if (!p.fast && rows_smem_bytes(p.method, prec_code, n, p.ld) > kMaxSmemPerBlock) {
         g_last_error = "GLL size too large for the row-solve kernel at this precision";
@@ -842,6 +872,10 @@ static int run_pipeline(Plan& p, const void* in, const double* gl, const double*
         r.d0 = p.d_c0;
         r.dN = p.d_cN;
         r.d2t = p.d_d2row;
+        r.fhom = p.d_hom;
+        r.fhoms = p.d_homs;
+        r.fd0 = p.d_d0;
+        r.fdN = p.d_dN;
     }
     r.periodic = p.periodic ? 1 : 0;
     const int prec = p.precision == HELM_FP64 ? 0 : (p.precision == HELM_FP32 ? 1 : 2);
@@ -1147,7 +1181,7 @@ int solve_adjoint(Plan& p, const double* ubar, double* fbar, double* glbar, doub
                   double* lambda_bar, cudaStream_t s, const double* sub = nullptr)
 {
     if (!p.adj_ready) {
-        g_last_error = "adjoint needs a fast-diagonalisation plan with one GLL element";
+        g_last_error = "adjoint needs a fast-diagonalisation plan (one GLL element, or several not periodic)";
         return HELM_ERR_UNSUPPORTED;
     }
     if (lambda_bar && !u) {

@@ -2,7 +2,8 @@
 
 * A dense FP64 reference gradient: the forward map (f, gl, gr) -> u of the
   oracle assembled column by column at Nx = Ny = 16, N = 17 (and a Robin case
-  at 8 x 8 x 9), then dL/d(.) = S^T ubar, compared with helm_solve_adjoint.
+  at 8 x 8 x 9; several GLL elements at 2D 8 x 3*7, 3D 4 x 4 x 2*7), then
+  dL/d(.) = S^T ubar, compared with helm_solve_adjoint.
 * Central finite differences (h = 1e-6, FP64 forward solves) of
   L = 1/2 ||u - u_obs||^2 at the 128 x 128 x 65, lambda = 5 workload for
   dL/df (directional) and dL/dlambda.
@@ -129,6 +130,68 @@ def test_adjoint_2d(cuda):
     assert rel_l2(fbar.cpu().numpy().ravel(), g[:nf]) < 1e-10
     assert rel_l2(glb.cpu().numpy(), g[nf:nf + Nx]) < 1e-10
     assert rel_l2(grb.cpu().numpy(), g[nf + Nx:]) < 1e-10
+
+
+def _dense_map_elems(dim, Nx, N, Ns, lam, bc, lengths):
+    """Columns of the oracle's map (f [Ns, Nx, (Ny,) N], gl, gr) -> u with
+    several GLL elements (the interface system of the reference's solver)."""
+    fshape = (Ns, Nx, N) if dim == 2 else (Ns, Nx, Nx, N)
+    bshape = (Nx,) if dim == 2 else (Nx, Nx)
+    nf, nb = int(np.prod(fshape)), int(np.prod(bshape))
+    cols = []
+    for e in range(nf + 2 * nb):
+        v = np.zeros(nf + 2 * nb)
+        v[e] = 1.0
+        f, gl, gr = v[:nf].reshape(fshape), v[nf:nf + nb].reshape(bshape), v[nf + nb:].reshape(bshape)
+        if dim == 2:
+            u = O.solve2d(f, gl, gr, Lx=lengths[0], Ly=lengths[1], lam=lam, bc=bc)
+        else:
+            u = O.solve3d(f, gl, gr, Lx=lengths[0], Ly=lengths[1], Lz=lengths[2], lam=lam, bc=bc)
+        cols.append(u.ravel())
+    return np.stack(cols, axis=1), fshape, bshape
+
+
+@pytest.mark.parametrize("dim,Nx,N,Ns,bc,precision", [
+    (2, 8, 7, 3, (1.0, 0.5, 0.7, 2.0), "fp64"),
+    (2, 8, 9, 3, (0.0, 1.0, 0.0, 1.0), "fp32_refine"),
+    (2, 8, 7, 3, (1.0, 0.5, 0.7, 2.0), "fp32"),
+    (3, 4, 7, 2, (0.4, 1.0, 0.3, 2.0), "fp64"),
+    (3, 4, 9, 2, (0.0, 1.0, 0.0, 1.0), "fp32_refine"),
+])
+def test_adjoint_several_elements_dense(cuda, dim, Nx, N, Ns, bc, precision):
+    """The transposed interface system: S^T ubar of the oracle's dense map,
+    and lambda_bar against central differences of the oracle's forward solve."""
+    lam = 2.0
+    lengths = (1.3, 0.9) if dim == 2 else (1.3, 1.1, 0.9)
+    S, fshape, bshape = _dense_map_elems(dim, Nx, N, Ns, lam, bc, lengths)
+    rng = np.random.default_rng(17 + dim)
+    ubar = rng.standard_normal(fshape)
+    g = S.T @ ubar.ravel()
+    nf, nb = int(np.prod(fshape)), int(np.prod(bshape))
+    if dim == 2:
+        p = NonPeriodic2D(Nx, Ns * N, N, 0.0, lengths[0], 0.0, lengths[1], Lambda=lam, bc=bc, precision=precision)
+    else:
+        p = NonPeriodic3D(Nx, Nx, Ns * N, N, 0.0, lengths[0], 0.0, lengths[1], 0.0, lengths[2], Lambda=lam, bc=bc,
+                          precision=precision)
+    f = rng.standard_normal(fshape)
+    if dim == 2:
+        solve = lambda lm: O.solve2d(f, np.zeros(bshape), np.zeros(bshape), Lx=lengths[0], Ly=lengths[1], lam=lm,
+                                     bc=bc)
+    else:
+        solve = lambda lm: O.solve3d(f, np.zeros(bshape), np.zeros(bshape), Lx=lengths[0], Ly=lengths[1],
+                                     Lz=lengths[2], lam=lm, bc=bc)
+    h = 1e-5
+    dlam = float((solve(lam + h) - solve(lam - h)).ravel() @ ubar.ravel()) / (2 * h)
+    u = solve(lam)
+    fbar, lbar, glb, grb = p.SolveAdjoint(_dev(ubar), u=_dev(u), want_bc=True)
+    tol = 1e-4 if precision == "fp32" else 1e-10
+    assert rel_l2(fbar.cpu().numpy().ravel(), g[:nf]) < tol
+    assert rel_l2(glb.cpu().numpy().ravel(), g[nf:nf + nb]) < tol
+    assert rel_l2(grb.cpu().numpy().ravel(), g[nf + nb:]) < tol
+    fb = fbar.cpu().numpy()
+    assert np.all(fb[..., 0] == 0) and np.all(fb[..., -1] == 0)
+    # central differences carry ~1e-9 of their own
+    assert abs(lbar.item() - dlam) < max(tol, 1e-7) * abs(dlam)
 
 
 @pytest.mark.parametrize("bc", [(0.0, 1.0, 0.0, 1.0), (0.4, 1.0, 0.3, 2.0)])
