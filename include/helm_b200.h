@@ -267,10 +267,11 @@ int helm_plan_info(helm_plan_t plan, int* Ns, int* n_operators, int* method, lon
 int helm_plan_set_stage_timing(helm_plan_t plan, int enable);
 int helm_plan_stage_times(helm_plan_t plan, float* ms5);
 
-/* Device status of the plan's tensor-memory-accelerator tile copies (the
- * first pass of the 3D eigen-basis pipeline): 0, or the code of a wait on a
+/* Device status of the plan's tensor-memory-accelerator and bulk copies (the
+ * first pass of the 3D eigen-basis pipeline: code 1; the GLL derivative of
+ * FP64 arrays in the packed layout: code 8): 0, or the code of a wait on a
  * copy that ran out of its iteration limit (the kernel then skipped that work,
- * so that solve's output is not valid).  Waits for the device; reset != 0
+ * so that call's output is not valid).  Waits for the device; reset != 0
  * clears the word afterwards.  Plans without such copies report 0.  No
  * counterpart in the reference. */
 int helm_plan_device_status(helm_plan_t plan, int* code, int reset);
@@ -289,8 +290,10 @@ int helm_plan_device_status(helm_plan_t plan, int* code, int reset);
  * points, Nx in {8, ..., 256}, Ny in {4, ..., 512}, powers of 2) the eigen-basis
  * pipeline of the whole forward solve -- GLL eigen-transform fused with the x
  * FFT, the y FFT, diagonal scaling and inverse y FFT in one pass, and the
- * inverse of the first pass: three kernels in 3D, one in 2D, fft4 unused;
- * adjoint solves run the transposed pipeline.  Plan creation times every
+ * inverse of the first pass: three kernels in 3D, one in 2D; in 3D bit 0 of
+ * fft4[1] picks the CTA shape of the middle pass and bit 1 (Nx >= 64) runs the
+ * first and last passes on pairs of CTAs, each holding half of a plane (the
+ * other fft4 entries are unused); adjoint solves run the transposed pipeline.  Plan creation times every
  * variant on the plan's own shape and keeps the fastest (environment
  * HELM_AUTOTUNE=0: all 0, rows 4 where it applies).  Setting them
  * pins the choice, e.g. to reproduce a run bit for bit.  Every variant

@@ -14,7 +14,8 @@
 //     du_j = sigma_j + alpha_j,      du_{P-1-j} = -/+ (sigma_j - alpha_j)  (first / second)
 // which halves the multiply-adds of the dense product.
 //
-// FP64 arrays run both products on the FP64 tensor cores (gll_deriv_mma_kernel);
+// FP64 arrays run both products on the FP64 tensor cores (gll_deriv_bulk_kernel
+// for the packed layout, gll_deriv_mma_kernel for any other);
 // FP32 arrays run them on the CUDA cores, one lane per row (gll_deriv_kernel).
 // Each warp owns 32 rows of a tile in shared memory (raw rows, then their
 // folded halves) and never waits on another warp.  The raw rows of
@@ -23,6 +24,7 @@
 // broadcasts.  HBM-bound: 2 P values (read + write) per row.
 #include "helm_device.cuh"
 #include "helm_kernels.cuh"
+#include "helm_tma.cuh"
 
 namespace helm {
 
@@ -335,6 +337,186 @@ __global__ void gll_deriv_mma_kernel(GllDerivArgs a, GdMmaLayout L)
     }
 }
 
+// ---------------------------------------------------------------------------
+// FP64 arrays whose rows lie back to back (row R at R P, the packed layout):
+// tiles of GB_ROWS consecutive rows are one contiguous run of memory, moved by
+// untiled bulk copies.  Thread 0 keeps up to `stages` tile loads in flight
+// (mbarrier-tracked); each of the GB_WARPS warps multiplies one 8-row m-tile
+// of the current tile on the FP64 tensor cores (the folded products of
+// gll_deriv_mma_kernel), writes its outputs over its own input rows, and the
+// finished tile goes back to global memory as one bulk store.  A tile whose
+// byte count is not a multiple of 16 (odd P and an odd row count at the end)
+// moves its last 8 bytes with plain loads and stores.
+constexpr int GB_WARPS = 8;
+constexpr int GB_ROWS = 8 * GB_WARPS;
+
+template <int NT>
+__global__ void __launch_bounds__(GB_WARPS * 32, 1) gll_deriv_bulk_kernel(GllDerivArgs a, GdMmaLayout L, int stages)
+{
+    pdl_enter();
+    extern __shared__ __align__(128) unsigned char gb_smem[];
+    const int P = a.P, h = L.h, hs = L.hs;
+    double* BE = reinterpret_cast<double*>(gb_smem);   // [ks][NT][32]
+    double* BF = BE + (size_t)L.ks * NT * 32;          // [ka][NT][32]
+    const size_t tile_elems = (size_t)GB_ROWS * P;
+    double* stage = reinterpret_cast<double*>(gb_smem + L.b_bytes);          // [stages][GB_ROWS][P]
+    uint64_t* full = reinterpret_cast<uint64_t*>(stage + (size_t)stages * tile_elems);
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, g = lane >> 2, q = lane & 3;
+    const double* in = static_cast<const double*>(a.in);
+    double* out = static_cast<double*>(a.out);
+    const double sgn = a.order == 1 ? -1.0 : 1.0;
+    const long long tiles = (a.nrows + GB_ROWS - 1) / GB_ROWS;
+    const int nmine = tiles > blockIdx.x ? (int)((tiles - 1 - blockIdx.x) / gridDim.x + 1) : 0;
+    auto tile_of = [&](int i) { return (long long)blockIdx.x + (long long)i * gridDim.x; };
+    auto bytes_of = [&](long long t) {
+        return (uint32_t)(min((long long)GB_ROWS, a.nrows - t * GB_ROWS) * P * (long long)sizeof(double));
+    };
+    auto issue = [&](int i) {  // thread 0: tile i of this CTA into stage i % stages
+        const long long t = tile_of(i);
+        const uint32_t bulk = bytes_of(t) & ~15u;
+        uint64_t* bar = &full[i % stages];
+        mbar_arrive_expect_tx(bar, bulk);
+        bulk_load(stage + (size_t)(i % stages) * tile_elems, in + t * GB_ROWS * P, bulk, bar);
+    };
+    // the first loads go out before the B fragments are built
+    if (threadIdx.x == 0) {
+        for (int i = 0; i < stages; ++i) mbar_init(&full[i], 1);
+        fence_mbar_init();
+        for (int i = 0; i < min(stages, nmine); ++i) issue(i);
+    }
+    int issued = min(stages, nmine);
+    for (int e = threadIdx.x; e < L.ks * NT * 32; e += blockDim.x) {
+        const int l = e & 31, t = (e >> 5) % NT, k = (e >> 5) / NT;
+        const int j = 8 * t + (l >> 2), kk = 4 * k + (l & 3);
+        double v = 0.0;
+        if (j < hs) {
+            if (kk < h) v = 0.5 * (a.M[j * P + kk] + a.M[j * P + P - 1 - kk]);
+            else if (kk == h && L.odd) v = a.M[j * P + h];
+        }
+        BE[e] = v;
+    }
+    for (int e = threadIdx.x; e < L.ka * NT * 32; e += blockDim.x) {
+        const int l = e & 31, t = (e >> 5) % NT, k = (e >> 5) / NT;
+        const int j = 8 * t + (l >> 2), kk = 4 * k + (l & 3);
+        double v = 0.0;
+        if (j < hs && kk < h) v = 0.5 * (a.M[j * P + kk] - a.M[j * P + P - 1 - kk]);
+        BF[e] = v;
+    }
+    __syncthreads();  // B fragments and the barrier initialisation
+
+    int failed_at = -1;
+    for (int i = 0; i < nmine; ++i) {
+        const long long t = tile_of(i);
+        const uint32_t bytes = bytes_of(t);
+        const int nr = (int)(bytes / (P * sizeof(double)));
+        double* cur = stage + (size_t)(i % stages) * tile_elems;
+        const bool ok = mbar_wait(&full[i % stages], (uint32_t)((i / stages) & 1));
+        if (__syncthreads_or(!ok)) {
+            failed_at = i;
+            break;
+        }
+        if ((bytes & 15u) && threadIdx.x == 0) cur[(size_t)nr * P - 1] = in[t * GB_ROWS * P + (long long)nr * P - 1];
+        __syncthreads();
+        if (8 * warp < nr) {
+            double cs[NT][2], ca[NT][2];
+#pragma unroll
+            for (int n = 0; n < NT; ++n) { cs[n][0] = cs[n][1] = 0.0; ca[n][0] = ca[n][1] = 0.0; }
+            const int row = 8 * warp + g;
+            double* u = cur + (size_t)row * P;
+            const bool live = row < nr;
+#pragma unroll 2
+            for (int kk = 0; kk < L.ks; ++kk) {
+                const int k = 4 * kk + q;
+                double sv = 0.0, av = 0.0;
+                if (live) {
+                    if (k < h) {
+                        const double x = u[k], y = u[P - 1 - k];
+                        sv = x + y;
+                        av = x - y;
+                    } else if (k == h && L.odd) {
+                        sv = u[h];
+                    }
+                }
+                const double* bs = BE + ((size_t)kk * NT) * 32 + lane;
+#pragma unroll
+                for (int n = 0; n < NT; ++n) dmma_8x8x4(cs[n][0], cs[n][1], sv, bs[n * 32]);
+                if (kk < L.ka) {
+                    const double* ba = BF + ((size_t)kk * NT) * 32 + lane;
+#pragma unroll
+                    for (int n = 0; n < NT; ++n) dmma_8x8x4(ca[n][0], ca[n][1], av, ba[n * 32]);
+                }
+            }
+            __syncwarp();  // every lane's reads of the 8 rows are done: overwrite them
+            if (live) {
+#pragma unroll
+                for (int n = 0; n < NT; ++n)
+#pragma unroll
+                    for (int e2 = 0; e2 < 2; ++e2) {
+                        const int j = 8 * n + 2 * q + e2;
+                        const double sg = cs[n][e2], al = ca[n][e2];
+                        if (j < h) {
+                            u[j] = sg + al;
+                            u[P - 1 - j] = sgn * (sg - al);
+                        } else if (j == h && L.odd) {
+                            u[j] = sg + al;
+                        }
+                    }
+            }
+        }
+        fence_proxy_async_smem();  // the outputs, written through the generic proxy, go out by bulk store
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            bulk_store(out + t * GB_ROWS * P, cur, bytes & ~15u);
+            tma_store_commit();
+            if (bytes & 15u) out[t * GB_ROWS * P + (long long)nr * P - 1] = cur[(size_t)nr * P - 1];
+            // refill the stage of tile i - 1: its store, issued one iteration
+            // ago, has read its shared memory once at most this one is pending
+            if (i >= 1 && issued < nmine) {
+                tma_store_wait_read<1>();
+                issue(issued);
+                ++issued;
+            }
+        }
+    }
+    if (threadIdx.x == 0) {
+        if (failed_at >= 0) {
+            if (a.err) atomicExch(a.err, 8);
+            // loads still in flight (tiles failed_at .. issued - 1, one per
+            // stage) land before the CTA's shared memory is released
+            for (int i = failed_at; i < issued; ++i) mbar_wait(&full[i % stages], (uint32_t)((i / stages) & 1));
+        }
+        tma_store_wait_all();
+    }
+}
+
+template <int NT>
+static int run_gll_deriv_bulk(const GllDerivArgs& a, cudaStream_t s)
+{
+    const GdMmaLayout L = gd_mma_layout(a.P);
+    const size_t tile_bytes = (size_t)GB_ROWS * a.P * sizeof(double);
+    int stages = (int)((kMaxSmemPerBlock - L.b_bytes - 64) / (tile_bytes + sizeof(uint64_t)));
+    if (stages > 5) stages = 5;
+    if (stages < 2) return -1;  // not this kernel
+    const size_t smem = L.b_bytes + (size_t)stages * (tile_bytes + sizeof(uint64_t));
+    auto k = gll_deriv_bulk_kernel<NT>;
+    cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return (int)e;
+    int dev = 0, sms = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    const long long tiles = (a.nrows + GB_ROWS - 1) / GB_ROWS;
+    const long long grid = tiles < sms ? tiles : sms;
+    if (grid < 1) return 0;
+    return (int)launch_k(k, dim3((unsigned)grid), dim3(GB_WARPS * 32), smem, s, a, L, stages);
+}
+
+// The packed layout with 16-byte aligned arrays: the bulk-copy kernel.
+static bool gll_deriv_packed(const GllDerivArgs& a)
+{
+    return a.x_stride == (long long)a.rows_per_x * a.P && a.elem_stride == (long long)a.nx * a.x_stride &&
+           (reinterpret_cast<uintptr_t>(a.in) & 15) == 0 && (reinterpret_cast<uintptr_t>(a.out) & 15) == 0;
+}
+
 template <int NT>
 static int run_gll_deriv_mma(const GllDerivArgs& a, cudaStream_t s)
 {
@@ -358,8 +540,28 @@ static int run_gll_deriv_mma(const GllDerivArgs& a, cudaStream_t s)
     return (int)launch_k(k, dim3((unsigned)grid), dim3(warps * 32), smem, s, a, L);
 }
 
+static int launch_gll_deriv_bulk(const GllDerivArgs& a, cudaStream_t s)
+{
+    switch ((a.P / 2 + (a.P & 1) + 7) / 8) {
+        case 1: return run_gll_deriv_bulk<1>(a, s);
+        case 2: return run_gll_deriv_bulk<2>(a, s);
+        case 3: return run_gll_deriv_bulk<3>(a, s);
+        case 4: return run_gll_deriv_bulk<4>(a, s);
+        case 5: return run_gll_deriv_bulk<5>(a, s);
+        case 6: return run_gll_deriv_bulk<6>(a, s);
+        case 7: return run_gll_deriv_bulk<7>(a, s);
+        case 8: return run_gll_deriv_bulk<8>(a, s);
+        case 9: return run_gll_deriv_bulk<9>(a, s);
+        default: return -1;
+    }
+}
+
 static int launch_gll_deriv_mma(const GllDerivArgs& a, cudaStream_t s)
 {
+    if (gll_deriv_packed(a)) {
+        const int e = launch_gll_deriv_bulk(a, s);
+        if (e != -1) return e;
+    }
     switch ((a.P / 2 + (a.P & 1) + 7) / 8) {
         case 1: return run_gll_deriv_mma<1>(a, s);
         case 2: return run_gll_deriv_mma<2>(a, s);

@@ -126,7 +126,7 @@ __device__ __forceinline__ void slab_to_smem(cplx_t<double>* sm, int hs, int tc,
         for (int r = 0; r < R; ++r) sm[slab_out_row<R, NS, TPC>(tc, t, r) * hs + col] = v[t * R + r];
 }
 
-template <int L, int R, int NS, int DIR, int TPC, int R0>
+template <int L, int R, int NS, int DIR, int TPC, int R0, int TWS = 1>
 __device__ __forceinline__ void slab_from_smem(const cplx_t<double>* sm, int hs, const cplx_t<double>* tw, int tc,
                                                int col, cplx_t<double> (&v)[R0])
 {
@@ -139,7 +139,7 @@ __device__ __forceinline__ void slab_from_smem(const cplx_t<double>* sm, int hs,
         for (int r = 0; r < R; ++r) {
             C x = sm[(j + r * (L / R)) * hs + col];
             if (NS > 1 && r > 0) {
-                const C w = tw[r * jm * (L / (NS * R))];
+                const C w = tw[TWS * r * jm * (L / (NS * R))];
                 x = (DIR < 0) ? cmul(x, w) : cmulc(x, w);
             }
             w8[r] = x;
@@ -163,8 +163,9 @@ __device__ __forceinline__ void slab_sync()
 // One length-L FFT (direction DIR, unscaled) of each of the ncol columns of the
 // [L][hs] complex array sm in shared memory, in place; threads 0 .. THREADS-1
 // call it (it synchronises them through slab_sync<BAR, THREADS>).  tw: the
-// length-L twiddle table exp(-2 pi i e / L).
-template <int L, int DIR, int THREADS, int BAR = 0>
+// twiddle table exp(-2 pi i e / (TWS L)), read at every TWS-th entry (TWS = 2:
+// the table of a transform twice as long).
+template <int L, int DIR, int THREADS, int BAR = 0, int TWS = 1>
 __device__ __forceinline__ void slab_fft(cplx_t<double>* sm, int hs, int ncol, const cplx_t<double>* tw)
 {
     using C = cplx_t<double>;
@@ -183,13 +184,13 @@ __device__ __forceinline__ void slab_fft(cplx_t<double>* sm, int hs, int ncol, c
             slab_sync<BAR, THREADS>();
             if (on) slab_to_smem<L, R0, 1, TPC, R0>(sm, hs, tc, col, v);
             slab_sync<BAR, THREADS>();
-            if (on) slab_from_smem<L, R1, R0, DIR, TPC, R0>(sm, hs, tw, tc, col, v);
+            if (on) slab_from_smem<L, R1, R0, DIR, TPC, R0, TWS>(sm, hs, tw, tc, col, v);
         }
         if constexpr (NP >= 3) {
             slab_sync<BAR, THREADS>();
             if (on) slab_to_smem<L, R1, R0, TPC, R0>(sm, hs, tc, col, v);
             slab_sync<BAR, THREADS>();
-            if (on) slab_from_smem<L, R2, R0 * R1, DIR, TPC, R0>(sm, hs, tw, tc, col, v);
+            if (on) slab_from_smem<L, R2, R0 * R1, DIR, TPC, R0, TWS>(sm, hs, tw, tc, col, v);
         }
         slab_sync<BAR, THREADS>();
         if (on) slab_to_smem<L, RL, L / RL, TPC, R0>(sm, hs, tc, col, v);

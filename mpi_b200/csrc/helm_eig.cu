@@ -28,7 +28,10 @@
 #include "helm_kernels.cuh"
 #include "helm_tma.cuh"
 
+#include <cooperative_groups.h>
 #include <cstring>
+
+namespace cg = cooperative_groups;
 
 namespace helm {
 
@@ -57,19 +60,20 @@ __device__ __forceinline__ void copy_mats(double* dst, const double* src, int bl
     for (int e = threadIdx.x; e < EP_FRAG; e += blockDim.x) d[e] = (e < EP_FRAG / 2) ? s0[e] : s1[e - EP_FRAG / 2];
 }
 
-// Loads plane y of f (rows x = 0..L-1, GLL slots 1..P-2) into buf and the
-// scaled boundary values zl, zr into slots 0 and P-1.
+// Loads rows x0 .. x0 + L - 1 of plane y of f (GLL slots 1..P-2) into buf and
+// the scaled boundary values zl, zr into slots 0 and P-1.
 template <int L>
 __device__ __forceinline__ void load_plane(const EigArgs& a, const double* f, const double* gl, const double* gr,
-                                           long long yoff, long long bc_off, double* buf)
+                                           long long yoff, long long bc_off, double* buf, int x0 = 0)
 {
     const int P = a.P;
     for (int e = threadIdx.x; e < L * P; e += blockDim.x) {
-        const int x = e / P, k = e - x * P;
-        double* d = buf + x * EP_PITCH + k;
-        const double* s = f + (long long)x * a.x_stride + yoff + k;
-        if (k == 0) *d = gl ? gl[(long long)x * a.bc_x_stride + bc_off] * a.ibl : 0.0;
-        else if (k == P - 1) *d = gr ? gr[(long long)x * a.bc_x_stride + bc_off] * a.ibr : 0.0;
+        const int xl = e / P, k = e - xl * P;
+        const long long x = x0 + xl;
+        double* d = buf + xl * EP_PITCH + k;
+        const double* s = f + x * a.x_stride + yoff + k;
+        if (k == 0) *d = gl ? gl[x * a.bc_x_stride + bc_off] * a.ibl : 0.0;
+        else if (k == P - 1) *d = gr ? gr[x * a.bc_x_stride + bc_off] * a.ibr : 0.0;
         else cp_async_bytes8(d, s, true);
     }
     cp_async_commit();
@@ -77,8 +81,8 @@ __device__ __forceinline__ void load_plane(const EigArgs& a, const double* f, co
     if (a.sub) {  // adjoint of a least-squares misfit: ubar = u - u_obs at the interior slots
         __syncthreads();
         for (int e = threadIdx.x; e < L * P; e += blockDim.x) {
-            const int x = e / P, k = e - x * P;
-            if (k > 0 && k < P - 1) buf[x * EP_PITCH + k] -= a.sub[(long long)x * a.x_stride + yoff + k];
+            const int xl = e / P, k = e - xl * P;
+            if (k > 0 && k < P - 1) buf[xl * EP_PITCH + k] -= a.sub[(long long)(x0 + xl) * a.x_stride + yoff + k];
         }
     }
 }
@@ -392,14 +396,13 @@ __global__ void __launch_bounds__(THREADS, 512 / THREADS) eig_conv_kernel(EigArg
 // Adjoint: the boundary terms of the transposed map for the warp's rows,
 // b_l . fbar_int = hsl . cs + hal . ca (and the same with the right-hand
 // vectors), from the coefficients in slots 0..63 before the second transform.
-template <int L>
+template <int RW>
 __device__ __forceinline__ void adjoint_boundary_dots(const EigArgs& a, const double* rows, int lane, double* dl,
                                                       double* dr)
 {
-    using S = EpShape<L>;
     const double hs0 = a.hbc[lane], hs1 = a.hbc[EIG_LD + lane], ha0 = a.hbc[2 * EIG_LD + lane],
                  ha1 = a.hbc[3 * EIG_LD + lane];
-    for (int r = 0; r < S::RW; ++r) {
+    for (int r = 0; r < RW; ++r) {
         const double cs = rows[r * EP_PITCH + lane], ca = rows[r * EP_PITCH + 32 + lane];
         double vl = hs0 * cs + ha0 * ca, vr = hs1 * cs + ha1 * ca;
         for (int o = 16; o > 0; o >>= 1) {
@@ -413,14 +416,13 @@ __device__ __forceinline__ void adjoint_boundary_dots(const EigArgs& a, const do
 // Adjoint: writes the warp's rows of fbar (boundary slots 0), the boundary
 // cotangents gbar = (ubar_boundary + dot) / beta, and returns this lane's share
 // of sum(fbar u).
-template <int L>
+template <int RW>
 __device__ __forceinline__ double store_adjoint_rows(const EigArgs& a, double* fbar, const double* ubar,
                                                      long long yoff, long long bc_off, double* rows, int x0, int lane,
                                                      double dl, double dr)
 {
-    using S = EpShape<L>;
     const int P = a.P;
-    if (lane < S::RW) {
+    if (lane < RW) {
         const long long x = x0 + lane;
         const long long o = x * a.x_stride + yoff;
         if (a.gbar_l) {
@@ -436,7 +438,7 @@ __device__ __forceinline__ double store_adjoint_rows(const EigArgs& a, double* f
     }
     __syncwarp();
     double acc = 0.0;
-    for (int r = 0; r < S::RW; ++r) {
+    for (int r = 0; r < RW; ++r) {
         const long long o = (long long)(x0 + r) * a.x_stride + yoff;
         for (int k = lane; k < P; k += 32) {
             const double v = rows[r * EP_PITCH + k];
@@ -464,19 +466,18 @@ __device__ __forceinline__ void eig_lambda_sum(const EigArgs& a, double acc)
 
 // ------------------------------------------------------------------ pass 3 --
 // Writes the warp's rows of plane y: boundary slots from gl, gr, then the rows.
-template <int L>
+template <int RW>
 __device__ __forceinline__ void store_plane_rows(const EigArgs& a, double* u, const double* gl, const double* gr,
                                                  long long yoff, long long bc_off, double* rows, int x0, int lane)
 {
-    using S = EpShape<L>;
     const int P = a.P;
-    if (lane < S::RW) {
+    if (lane < RW) {
         const long long x = x0 + lane;
         rows[lane * EP_PITCH] = gl ? gl[x * a.bc_x_stride + bc_off] * a.ibl : 0.0;
         rows[lane * EP_PITCH + P - 1] = gr ? gr[x * a.bc_x_stride + bc_off] * a.ibr : 0.0;
     }
     __syncwarp();
-    for (int r = 0; r < S::RW; ++r) {
+    for (int r = 0; r < RW; ++r) {
         double* dst = u + (long long)(x0 + r) * a.x_stride + yoff;
         for (int k = lane; k < P; k += 32) dst[k] = rows[r * EP_PITCH + k];
     }
@@ -506,15 +507,213 @@ __global__ void __launch_bounds__(EpShape<L>::THREADS, 1) eig_inv_kernel(EigArgs
     double* rows = buf + warp * S::RW * EP_PITCH;
     if (!a.adjoint) {
         second_transform<S::MTW>(a, rows, Mt, Mt + EP_FRAG, lane);
-        store_plane_rows<L>(a, a.u, a.gl, a.gr, (long long)y * a.P, y, rows, warp * S::RW, lane);
+        store_plane_rows<S::RW>(a, a.u, a.gl, a.gr, (long long)y * a.P, y, rows, warp * S::RW, lane);
         return;
     }
     double dl = 0.0, dr = 0.0;
-    adjoint_boundary_dots<L>(a, rows, lane, &dl, &dr);
+    adjoint_boundary_dots<S::RW>(a, rows, lane, &dl, &dr);
     __syncwarp();
     second_transform<S::MTW>(a, rows, Mt, Mt + EP_FRAG, lane);
     const double acc =
-        store_adjoint_rows<L>(a, a.u, a.f, (long long)y * a.P, y, rows, warp * S::RW, lane, dl, dr);
+        store_adjoint_rows<S::RW>(a, a.u, a.f, (long long)y * a.P, y, rows, warp * S::RW, lane, dl, dr);
+    if (a.lam_out) eig_lambda_sum(a, acc);
+}
+
+// ------------------------------------------------- pair-split passes 1, 3 --
+// Passes 1 and 3 with each plane shared by a cluster of two CTAs: CTA rank r
+// holds rows x = r H .. r H + H - 1 (H = L / 2), so a CTA needs half the
+// shared memory and two fit on an SM, overlapping one CTA's copies with the
+// other's arithmetic.  The length-L FFT along x is split by the parity of
+// the wavenumber: pass 1 takes the first radix-2 step of a decimation in
+// frequency across the pair (rank 0 keeps a_m = z_m + z_{m+H}, rank 1 keeps
+// b_m = (z_m - z_{m+H}) w^m, w = exp(-2 pi i / L)), reading the partner's rows
+// from its shared memory, then a length-H FFT gives the even (rank 0) or odd
+// (rank 1) wavenumbers.  Pass 3 runs the mirror image: a length-H inverse FFT
+// of its parity's wavenumbers, then the last step of a decimation in time
+// across the pair, x_m = E_m + conj(w^m) O_m (rank 0) and x_{m+H} = E_m -
+// conj(w^m) O_m (rank 1).
+template <int L>
+struct SplitShape {
+    static constexpr int H = L / 2;
+    static constexpr int WARPS = (H / 16 < 8) ? H / 16 : 8;
+    static constexpr int THREADS = 32 * WARPS;
+    static constexpr int RW = H / WARPS;  // 16 rows per warp
+    static constexpr int MTW = RW / 8;
+    static constexpr int NQ = 2;          // TMA boxes per CTA
+    static constexpr int QR = H / NQ;
+    static_assert(RW == 16 && QR == FwdBoxes<L>::QR, "pair-split shape");
+    static constexpr size_t smem(int nmats) { return ((size_t)H * EP_PITCH + (size_t)nmats * EP_FRAG) * sizeof(double); }
+};
+
+// The cross-pair butterfly on the [H][EP_HS] complex rows z: every thread
+// reads its elements of the partner's rows, the pair synchronises (both have
+// read), and combine(m, own, partner) replaces each element.  The caller has
+// synchronised the pair after its last write of z.
+template <int L, typename Combine>
+__device__ __forceinline__ void pair_exchange(cg::cluster_group& cluster, double2* z, Combine combine)
+{
+    using S = SplitShape<L>;
+    constexpr int PER = S::H * 32 / S::THREADS;
+    const double2* zp = cluster.map_shared_rank(z, (int)cluster.block_rank() ^ 1);
+    double2 pv[PER];
+#pragma unroll
+    for (int k = 0; k < PER; ++k) {
+        const int e = threadIdx.x + k * S::THREADS, m = e >> 5, c = e & 31;
+        pv[k] = zp[m * EP_HS + c];
+    }
+    cluster.sync();
+#pragma unroll
+    for (int k = 0; k < PER; ++k) {
+        const int e = threadIdx.x + k * S::THREADS, m = e >> 5, c = e & 31;
+        z[m * EP_HS + c] = combine(m, z[m * EP_HS + c], pv[k]);
+    }
+    __syncthreads();
+}
+
+template <int L>
+__global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(SplitShape<L>::THREADS, 2)
+    eig_fwd_split_kernel(EigArgs a, const __grid_constant__ EigMaps tm)
+{
+    using S = SplitShape<L>;
+    constexpr int H = S::H;
+    extern __shared__ __align__(128) double esm[];
+    __shared__ __align__(8) uint64_t bar[S::NQ];
+    cg::cluster_group cluster = cg::this_cluster();
+    const int rank = (int)cluster.block_rank();
+    double* buf = esm;
+    double* Mt = esm + (size_t)H * EP_PITCH;
+    double* sbuf = (a.tma && a.sub) ? Mt + 2 * EP_FRAG : nullptr;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int y = blockIdx.x >> 1, x0 = rank * H;
+    const bool tma = a.tma != 0;
+    if (tma && threadIdx.x == 0) {
+        for (int q = 0; q < S::NQ; ++q) mbar_init(&bar[q], 1);
+        fence_mbar_init();
+    }
+    copy_mats(Mt, a.mats, 0, 2);
+    __syncthreads();
+    pdl_enter();
+    if (a.lam_out && blockIdx.x == 0 && threadIdx.x == 0) *a.lam_out = 0.0;
+    double* rows = buf + warp * S::RW * EP_PITCH;
+    bool tma_ok = true;
+    if (tma) {
+        const int sh = (int)(((long long)y * a.P) & 1);
+        if (threadIdx.x == 0) {
+            const int c0 = y * a.P - sh;
+            const uint32_t box = (uint32_t)(S::QR * EP_PITCH * sizeof(double));
+            for (int q = 0; q < S::NQ; ++q) {
+                mbar_arrive_expect_tx(&bar[q], sbuf ? 2 * box : box);
+                tma_load_2d(buf + (size_t)q * S::QR * EP_PITCH, &tm.f, c0, x0 + q * S::QR, &bar[q]);
+                if (sbuf) tma_load_2d(sbuf + (size_t)q * S::QR * EP_PITCH, &tm.sub, c0, x0 + q * S::QR, &bar[q]);
+            }
+        }
+        tma_ok = mbar_wait(&bar[(warp * S::RW) / S::QR], 0);
+        if (!tma_ok && lane == 0 && a.err) atomicExch(a.err, 1);
+        const double* gl = a.adjoint ? nullptr : a.gl;
+        const double* gr = a.adjoint ? nullptr : a.gr;
+        if (lane < S::RW) {
+            const long long x = x0 + (long long)warp * S::RW + lane;
+            rows[lane * EP_PITCH + sh] = gl ? gl[x * a.bc_x_stride + y] * a.ibl : 0.0;
+            rows[lane * EP_PITCH + sh + a.P - 1] = gr ? gr[x * a.bc_x_stride + y] * a.ibr : 0.0;
+        }
+        __syncwarp();
+        if (tma_ok)
+            first_transform<S::MTW>(a, rows, Mt, Mt + EP_FRAG, a.hbc, lane, sh,
+                                    sbuf ? sbuf + warp * S::RW * EP_PITCH : nullptr);
+    } else {
+        load_plane<H>(a, a.f, a.adjoint ? nullptr : a.gl, a.adjoint ? nullptr : a.gr, (long long)y * a.P, y, buf, x0);
+        __syncthreads();
+        first_transform<S::MTW>(a, rows, Mt, Mt + EP_FRAG, a.hbc, lane);
+    }
+    __syncthreads();
+    if (tma && threadIdx.x == 0 && !tma_ok)  // copies still in flight land before the CTA ends
+        for (int q = 0; q < S::NQ; ++q) mbar_wait(&bar[q], 0);
+    cluster.sync();  // both halves of the plane are transformed
+    double2* z = reinterpret_cast<double2*>(buf);
+    const double2* tw = static_cast<const double2*>(a.tw_x);
+    pair_exchange<L>(cluster, z, [&](int m, double2 own, double2 other) {
+        if (rank == 0) return make_double2(own.x + other.x, own.y + other.y);
+        return cmul(make_double2(other.x - own.x, other.y - own.y), tw[m]);
+    });
+    slab_fft<H, -1, S::THREADS, 0, 2>(z, EP_HS, 32, tw);
+    // local row k' holds wavenumber 2 k' + rank; its mirror L - k is local
+    // row (H - k') mod H (even) or H - 1 - k' (odd)
+    double2* Sg = reinterpret_cast<double2*>(a.S);
+    const long long Ny = a.Ny;
+    const int kmax = rank == 0 ? H / 2 : H / 2 - 1;
+    for (int kp = warp; kp <= kmax; kp += S::WARPS) {
+        const int km = rank == 0 ? ((H - kp) & (H - 1)) : (H - 1 - kp);
+        const double2 zk = z[kp * EP_HS + lane], zm = z[km * EP_HS + lane];
+        double2* row = Sg + ((long long)(2 * kp + rank) * Ny + y) * EIG_SLOTS;
+        row[2 * lane] = make_double2(0.5 * (zk.x + zm.x), 0.5 * (zk.y - zm.y));
+        row[2 * lane + 1] = make_double2(0.5 * (zk.y + zm.y), 0.5 * (zm.x - zk.x));
+    }
+}
+
+template <int L>
+__global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(SplitShape<L>::THREADS, 2) eig_inv_split_kernel(EigArgs a)
+{
+    using S = SplitShape<L>;
+    constexpr int H = S::H;
+    extern __shared__ __align__(16) double esm[];
+    cg::cluster_group cluster = cg::this_cluster();
+    const int rank = (int)cluster.block_rank();
+    double* buf = esm;
+    double* Mt = esm + (size_t)H * EP_PITCH;
+    copy_mats(Mt, a.mats, 1, 3);
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int y = blockIdx.x >> 1, x0 = rank * H;
+    double2* z = reinterpret_cast<double2*>(buf);
+    const double2* Sg = reinterpret_cast<const double2*>(a.S);
+    const long long Ny = a.Ny;
+    pdl_enter();
+    // wavenumbers of this rank's parity, kx = 2 kp + rank <= L / 2, three
+    // rows per round fetched before any is used
+    constexpr int W = S::WARPS, NB = 3;
+    const int kmax = rank == 0 ? H / 2 : H / 2 - 1;
+    for (int k0 = warp; k0 <= kmax; k0 += NB * W) {
+        double2 X[NB], Y[NB];
+#pragma unroll
+        for (int b = 0; b < NB; ++b)
+            if (k0 + b * W <= kmax) {
+                const double2* row = Sg + ((long long)(2 * (k0 + b * W) + rank) * Ny + y) * EIG_SLOTS;
+                X[b] = row[2 * lane];
+                Y[b] = row[2 * lane + 1];
+            }
+#pragma unroll
+        for (int b = 0; b < NB; ++b) {
+            const int kp = k0 + b * W;
+            if (kp > kmax) break;
+            const int kx = 2 * kp + rank;
+            if (kx == 0 || kx == L / 2) { X[b].y = 0.0; Y[b].y = 0.0; }
+            z[kp * EP_HS + lane] = make_double2(X[b].x - Y[b].y, X[b].y + Y[b].x);
+            if (kx > 0 && kx < L / 2) z[((L - kx - rank) / 2) * EP_HS + lane] = make_double2(X[b].x + Y[b].y, Y[b].x - X[b].y);
+        }
+    }
+    __syncthreads();
+    const double2* tw = static_cast<const double2*>(a.tw_x);
+    slab_fft<H, 1, S::THREADS, 0, 2>(z, EP_HS, 32, tw);
+    cluster.sync();  // both parities are transformed
+    pair_exchange<L>(cluster, z, [&](int m, double2 own, double2 other) {
+        if (rank == 0) {
+            const double2 t = cmulc(other, tw[m]);
+            return make_double2(own.x + t.x, own.y + t.y);
+        }
+        const double2 t = cmulc(own, tw[m]);
+        return make_double2(other.x - t.x, other.y - t.y);
+    });
+    double* rows = buf + warp * S::RW * EP_PITCH;
+    const int xw = x0 + warp * S::RW;
+    if (!a.adjoint) {
+        second_transform<S::MTW>(a, rows, Mt, Mt + EP_FRAG, lane);
+        store_plane_rows<S::RW>(a, a.u, a.gl, a.gr, (long long)y * a.P, y, rows, xw, lane);
+        return;
+    }
+    double dl = 0.0, dr = 0.0;
+    adjoint_boundary_dots<S::RW>(a, rows, lane, &dl, &dr);
+    __syncwarp();
+    second_transform<S::MTW>(a, rows, Mt, Mt + EP_FRAG, lane);
+    const double acc = store_adjoint_rows<S::RW>(a, a.u, a.f, (long long)y * a.P, y, rows, xw, lane, dl, dr);
     if (a.lam_out) eig_lambda_sum(a, acc);
 }
 
@@ -566,14 +765,14 @@ __global__ void __launch_bounds__(EpShape<L>::THREADS, 1) eig_solve2d_kernel(Eig
     slab_fft<L, 1, S::THREADS>(z, EP_HS, 32, tw);
     if (!a.adjoint) {
         second_transform<S::MTW>(a, rows, M2, M2 + EP_FRAG, lane);
-        store_plane_rows<L>(a, a.u + off, gl, gr, 0, 0, rows, warp * S::RW, lane);
+        store_plane_rows<S::RW>(a, a.u + off, gl, gr, 0, 0, rows, warp * S::RW, lane);
         return;
     }
     double dl = 0.0, dr = 0.0;
-    adjoint_boundary_dots<L>(a, rows, lane, &dl, &dr);
+    adjoint_boundary_dots<S::RW>(a, rows, lane, &dl, &dr);
     __syncwarp();
     second_transform<S::MTW>(a, rows, M2, M2 + EP_FRAG, lane);
-    const double acc = store_adjoint_rows<L>(a, a.u, a.f, 0, 0, rows, warp * S::RW, lane, dl, dr);
+    const double acc = store_adjoint_rows<S::RW>(a, a.u, a.f, 0, 0, rows, warp * S::RW, lane, dl, dr);
     if (a.lam_out) eig_lambda_sum(a, acc);
 }
 
@@ -601,12 +800,27 @@ int run_3d(int pass, const EigArgs& a, cudaStream_t s)
                 (a.sub && !encode_tmap_f64_2d(&tm.sub, a.sub, dims, str, box)))
                 a1.tma = 0;  // element-wise loads instead
         }
+        if constexpr (L >= 64) {
+            if (a.split) {
+                using SS = SplitShape<L>;
+                const size_t sms = SS::smem(2) + ((a1.tma && a1.sub) ? (size_t)SS::H * EP_PITCH * sizeof(double) : 0);
+                if ((e = prep(eig_fwd_split_kernel<L>, sms)) != cudaSuccess) return (int)e;
+                return (int)launch_k(eig_fwd_split_kernel<L>, dim3(2 * a.Ny), dim3(SS::THREADS), sms, s, a1, tm);
+            }
+        }
         // the misfit adjoint's TMA path stages u_obs's plane beside f's
         const size_t smf = (a1.tma && a1.sub) ? sm1 + (size_t)L * EP_PITCH * sizeof(double) : sm1;
         if ((e = prep(eig_fwd_kernel<L>, smf)) != cudaSuccess) return (int)e;
         return (int)launch_k(eig_fwd_kernel<L>, dim3(a.Ny), dim3(S::THREADS), smf, s, a1, tm);
     }
     if (pass == 2) {
+        if constexpr (L >= 64) {
+            if (a.split) {
+                using SS = SplitShape<L>;
+                if ((e = prep(eig_inv_split_kernel<L>, SS::smem(2))) != cudaSuccess) return (int)e;
+                return (int)launch_k(eig_inv_split_kernel<L>, dim3(2 * a.Ny), dim3(SS::THREADS), SS::smem(2), s, a);
+            }
+        }
         if ((e = prep(eig_inv_kernel<L>, sm1)) != cudaSuccess) return (int)e;
         return (int)launch_k(eig_inv_kernel<L>, dim3(a.Ny), dim3(S::THREADS), sm1, s, a);
     }

@@ -48,6 +48,9 @@ struct EigArgs {
     // 3D pass 2 CTA shape: 0 = 16 columns x 256 threads, 1 = 8 columns x 128
     // threads (Ny = 512: 8 or 4 columns, 256 threads)
     int conv_var;
+    // 3D passes 1 and 3 (Nx >= 64): each plane on a cluster of two CTAs, half
+    // the rows each (the x FFT split by wavenumber parity across the pair)
+    int split;
 };
 
 // Whether pass 1 can load these arrays with TMA copies (Nx: plane rows).

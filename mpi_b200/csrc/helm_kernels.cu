@@ -197,6 +197,45 @@ __device__ __forceinline__ void deriv_mul(const FftArgs& a, int k, cplx_t<T>& A,
     }
 }
 
+// The same multiplication on the full spectrum Z = A + i B of two packed real
+// columns: the multiplier is Hermitian (its value at L - k is the conjugate of
+// its value at k), so Z_k (i w K)^order is the packed spectrum of the two
+// derivatives.  At K = -L/2 the first derivative vanishes (the real part the
+// reference keeps) and the second keeps -(w L/2)^2.
+template <typename T, int L>
+__device__ __forceinline__ cplx_t<T> deriv_mul_packed(int order, double w, int k, cplx_t<T> Z)
+{
+    const double K = (k < L / 2) ? (double)k : (double)(k - L);
+    const double wk = w * K;
+    if (order == 1) {
+        const T m = (k == L / 2) ? (T)0 : (T)wk;
+        return mk(-m * Z.y, m * Z.x);
+    }
+    const T m = (T)(-wk * wk);
+    return mk(m * Z.x, m * Z.y);
+}
+
+// Forward (DIR2 = -1) or inverse (+1) Stockham passes of a transform whose
+// first-pass inputs v[r] (rows tc + r TPC) are in registers; on return v holds
+// the outputs of the last pass (rows pass_out_row).
+template <typename T, int L, int DIR2, int TPC, int CT, int R0, int R1, int R2, int NP>
+__device__ __forceinline__ void fft_reg_passes(cplx_t<T>* sm, const cplx_t<T>* tw, int tc, int cl, cplx_t<T> (&v)[R0])
+{
+    dft_reg<R0, DIR2, T>(v);
+    if constexpr (NP >= 2) {
+        __syncthreads();
+        pass_to_smem<T, L, R0, 1, TPC, CT, R0>(sm, tc, cl, v);
+        __syncthreads();
+        pass_from_smem<T, L, R1, R0, DIR2, TPC, CT, R0>(sm, tw, tc, cl, v);
+    }
+    if constexpr (NP >= 3) {
+        __syncthreads();
+        pass_to_smem<T, L, R1, R0, TPC, CT, R0>(sm, tc, cl, v);
+        __syncthreads();
+        pass_from_smem<T, L, R2, R0 * R1, DIR2, TPC, CT, R0>(sm, tw, tc, cl, v);
+    }
+}
+
 template <typename T, typename TIO, int L, int DIR, int MODE, int THREADS, int SMALL>
 __global__ void __launch_bounds__(THREADS) fft_kernel(FftArgs a, long long total_cols)
 {
@@ -241,6 +280,18 @@ __global__ void __launch_bounds__(THREADS) fft_kernel(FftArgs a, long long total
         __syncthreads();
 #pragma unroll
         for (int r = 0; r < R0; ++r) v[r] = sm[(tc + r * TPC) * CT + cl];
+    } else if constexpr (MODE == FFT_DERIV) {
+        const TIO* in = static_cast<const TIO*>(a.in) + in_base;
+#pragma unroll
+        for (int r = 0; r < R0; ++r) {
+            const long long row = tc + r * TPC;
+            T x0 = 0, x1 = 0;
+            if (valid) {
+                x0 = (T)in[row * a.in_row + c0];
+                if (has1) x1 = (T)in[row * a.in_row + c1];
+            }
+            v[r] = mk(x0, x1);
+        }
     } else if constexpr (MODE == FFT_R2C) {
         const TIO* in = static_cast<const TIO*>(a.in) + in_base;
         const TIO* sub = a.in_sub ? static_cast<const TIO*>(a.in_sub) + in_base : nullptr;
@@ -305,7 +356,33 @@ __global__ void __launch_bounds__(THREADS) fft_kernel(FftArgs a, long long total
 
     // ---------------------------------------------------------- output --
     const T sc = (T)a.scale;
-    if constexpr (MODE == FFT_C2C) {
+    if constexpr (MODE == FFT_DERIV) {
+        // multiply in place, back to natural row order through shared memory,
+        // then the inverse transform and the two real output columns
+#pragma unroll
+        for (int t = 0; t < R0 / RL; ++t)
+#pragma unroll
+            for (int r = 0; r < RL; ++r)
+                v[t * RL + r] = deriv_mul_packed<T, L>(a.deriv_order, a.deriv_w, pass_out_row<RL, NSL, TPC>(tc, t, r),
+                                                       v[t * RL + r]);
+        __syncthreads();
+        pass_to_smem<T, L, RL, NSL, TPC, CT, R0>(sm, tc, cl, v);
+        __syncthreads();
+#pragma unroll
+        for (int r = 0; r < R0; ++r) v[r] = sm[(tc + r * TPC) * CT + cl];
+        fft_reg_passes<T, L, 1, TPC, CT, R0, R1, R2, NP>(sm, tw, tc, cl, v);
+        if (valid) {
+            TIO* out = static_cast<TIO*>(a.out) + out_base;
+#pragma unroll
+            for (int t = 0; t < R0 / RL; ++t)
+#pragma unroll
+                for (int r = 0; r < RL; ++r) {
+                    const long long row = pass_out_row<RL, NSL, TPC>(tc, t, r);
+                    out[row * a.out_row + c0] = (TIO)(v[t * RL + r].x * sc);
+                    if (has1) out[row * a.out_row + c1] = (TIO)(v[t * RL + r].y * sc);
+                }
+        }
+    } else if constexpr (MODE == FFT_C2C) {
         if (valid) {
             C* out = static_cast<C*>(a.out) + out_base;
 #pragma unroll
@@ -612,7 +689,7 @@ static int run_fft(const FftArgs& a, long long total_cols, cudaStream_t s)
 template <typename T, typename TIO, int L, int THREADS, int SMALL>
 static int fft_dispatch_mode(int mode, int dir, const FftArgs& a, long long tc, cudaStream_t s, bool pipe)
 {
-    if (pipe) {
+    if (pipe && mode != FFT_DERIV) {
         if (mode == FFT_C2C)
             return dir < 0 ? run_fft_pipe<T, T, L, -1, FFT_C2C, THREADS, SMALL>(a, tc, s)
                            : run_fft_pipe<T, T, L, 1, FFT_C2C, THREADS, SMALL>(a, tc, s);
@@ -627,6 +704,7 @@ static int fft_dispatch_mode(int mode, int dir, const FftArgs& a, long long tc, 
         return dir < 0 ? run_fft<T, T, L, -1, FFT_C2C, THREADS, SMALL>(a, tc, s)
                        : run_fft<T, T, L, 1, FFT_C2C, THREADS, SMALL>(a, tc, s);
     if (mode == FFT_R2C) return run_fft<T, TIO, L, -1, FFT_R2C, THREADS, SMALL>(a, tc, s);
+    if (mode == FFT_DERIV) return run_fft<T, TIO, L, -1, FFT_DERIV, THREADS, SMALL>(a, tc, s);
     if (mode == FFT_C2R_ADJ) {
         if constexpr (sizeof(TIO) == 8) return run_fft<T, TIO, L, 1, FFT_C2R_ADJ, THREADS, SMALL>(a, tc, s);
         return (int)cudaErrorInvalidValue;

@@ -8,7 +8,10 @@ namespace helm {
 
 // FFT_C2R_ADJ: the C2R pass of an adjoint solve (FftArgs adj_* fields), a
 // separate instantiation so the forward C2R carries none of its code.
-enum FftMode { FFT_C2C = 0, FFT_R2C = 1, FFT_C2R = 2, FFT_C2R_ADJ = 3 };
+// FFT_DERIV: real in, real out -- the forward transform of each pair of real
+// columns packed as one complex column, the multiplication by (i deriv_w K)^
+// deriv_order, the inverse transform and the scaling, in one kernel.
+enum FftMode { FFT_C2C = 0, FFT_R2C = 1, FFT_C2R = 2, FFT_C2R_ADJ = 3, FFT_DERIV = 4 };
 
 // One batched FFT along a strided axis.  The transform index is the row; the
 // data of one row are `ncols` contiguous columns; batches are `*_batch` apart.
@@ -143,6 +146,7 @@ struct GllDerivArgs {
     int rows_per_x;         // rows in one x row (Ny in 3D, 1 in 2D)
     int nx;                 // x rows per element
     long long x_stride, elem_stride;  // in elements of the io type
+    int* err;               // device status word: set when a copy wait ran out, or NULL
 };
 int launch_gll_deriv(int io_double, const GllDerivArgs& a, cudaStream_t s);
 

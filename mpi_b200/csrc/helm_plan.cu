@@ -413,10 +413,6 @@ static int setup_fast(Plan& p, const std::vector<double>& A0, int prec_code)
                 hbc[3 * EIG_LD + i] += Vai[(size_t)i * ma + j] * fbr[ld + j];
             }
         if ((st = p.upload((void**)&p.d_hbc, hbc.data(), hbc.size() * sizeof(double)))) return st;
-        if (p.dim == 3) {
-            const int zero = 0;
-            if ((st = p.upload((void**)&p.d_status, &zero, sizeof(int)))) return st;
-        }
         p.eig_ok = true;
     }
     if ((st = p.upload((void**)&p.d_fe0, fe0.data(), fe0.size() * sizeof(double)))) return st;
@@ -626,6 +622,10 @@ static int setup_plan(Plan& p)
     if ((st = p.upload((void**)&p.d_d0, D.data(), N * sizeof(double)))) return st;
     if ((st = p.upload((void**)&p.d_dN, D.data() + (size_t)(N - 1) * N, N * sizeof(double)))) return st;
     if ((st = p.upload((void**)&p.d_Dfull, D.data(), (size_t)N * N * sizeof(double)))) return st;
+    {
+        const int zero = 0;  // device status word of the kernels with bounded copy waits
+        if ((st = p.upload((void**)&p.d_status, &zero, sizeof(int)))) return st;
+    }
     if ((st = p.upload((void**)&p.d_D2full, D2.data(), (size_t)N * N * sizeof(double)))) return st;
     // refinement: interior D2 column-major with leading dimension ld
     std::vector<double> d2t((size_t)n * ld, 0.0);
@@ -803,6 +803,7 @@ static int run_pipeline(Plan& p, const void* in, const double* gl, const double*
         ea.err = p.d_status;
         ea.tma = (p.dim == 3 && eig_tma_ok(ea, p.Nx)) ? 1 : 0;
         ea.conv_var = p.fft_var[1] & 1;
+        ea.split = (p.dim == 3 && p.Nx >= 64 && (p.fft_var[1] & 2)) ? 1 : 0;
         int e = launch_eig_pass(0, p.dim, p.Nx, ea, p.batch, s);
         if (e) return set_cuda_error((cudaError_t)e, "eigen-basis pass 1");
         mark(1);
@@ -1062,12 +1063,17 @@ static int autotune(Plan& p)
     p.row_var = best_rv;
     // 3. fused alternatives, whole solves
     // (row variant, y-pass variant): the eigen-basis pipeline takes bit 0 of the
-    // y-pass variant as the CTA shape of its second pass
+    // y-pass variant as the CTA shape of its second pass and bit 1 as the
+    // pair-split form of its first and third passes
     const int yv = p.fft_var[1];
     std::vector<std::pair<int, int>> whole = {{p.row_var, yv}};
     if (p.slab_ok) whole.push_back({2, yv});
     if (p.eig_ok) whole.push_back({4, 0});
     if (p.eig_ok && p.dim == 3) whole.push_back({4, 1});
+    if (p.eig_ok && p.dim == 3 && p.Nx >= 64) {
+        whole.push_back({4, 2});
+        whole.push_back({4, 3});
+    }
     if (whole.size() > 1) {
         std::vector<float> tot(whole.size(), 0.f);
         bool ok = true;
@@ -1213,6 +1219,7 @@ int gll_derivative(Plan& p, int order, const void* u, void* du, cudaStream_t s)
     a.nrows = (long long)p.Ns * p.Nx * a.rows_per_x;
     a.x_stride = p.x_stride;
     a.elem_stride = p.elem_stride;
+    a.err = p.d_status;
     const int io_double = (p.precision != HELM_FP32 || p.io_bytes == 8) ? 1 : 0;
     const int e = launch_gll_deriv(io_double, a, s);
     if (e) return set_cuda_error((cudaError_t)e, "GLL derivative launch");
@@ -1225,37 +1232,30 @@ int gll_derivative(Plan& p, int order, const void* u, void* du, cudaStream_t s)
 int fourier_derivative(Plan& p, int axis, int order, const void* u, void* du, cudaStream_t s)
 {
     if (p.batch > 1) { g_last_error = "derivative of a batched plan"; return HELM_ERR_UNSUPPORTED; }
+    // one launch per call (per element when elements are not packed back to
+    // back along y): forward transform, multiplication, inverse transform
     const int N = p.N;
     const bool tdbl = p.precision != HELM_FP32;
-    const size_t celem = tdbl ? 16 : 8;
     int st;
     if (axis == 0) {
         const long long cols = (long long)(p.dim == 3 ? p.Ny : 1) * N;
         const double w = 2.0 * kRefPi / p.Lx;
-        if ((st = fft_pass(p, p.Nx, FFT_R2C, -1, u, p.d_spec, p.x_stride, cols, p.elem_stride, p.elem_spec, (int)cols,
-                           p.Ns, 1.0, p.d_tw_x, nullptr, nullptr, false, false, 0, s)))
-            return st;
-        return fft_pass(p, p.Nx, FFT_C2R, 1, p.d_spec, du, cols, p.x_stride, p.elem_spec, p.elem_stride, (int)cols,
-                        p.Ns, 1.0 / p.Nx, p.d_tw_x, nullptr, nullptr, false, false, 3, s, nullptr, order, w);
+        return fft_pass(p, p.Nx, FFT_DERIV, -1, u, du, p.x_stride, p.x_stride, p.elem_stride, p.elem_stride,
+                        (int)cols, p.Ns, 1.0 / p.Nx, p.d_tw_x, nullptr, nullptr, false, false, 0, s, nullptr, order, w);
     }
     if (axis != 1 || p.dim != 3) {
         g_last_error = "axis must be 0 (x) or, for 3D plans, 1 (y)";
         return HELM_ERR_INVALID;
     }
-    // y rows of one element are uniform batches when elements are packed back to back
     const double w = 2.0 * kRefPi / p.Ly;
-    const long long hspec = (long long)(p.Ny / 2 + 1) * N;  // one x row's half spectrum
     const bool uniform = p.elem_stride == (long long)p.Nx * p.x_stride;
     const int nb = uniform ? p.Ns * p.Nx : p.Nx;
+    const size_t esz = (tdbl || p.io_bytes == 8) ? 8 : 4;
     for (int e = 0; e < (uniform ? 1 : p.Ns); ++e) {
-        const char* ue = static_cast<const char*>(u) + (size_t)e * p.elem_stride * (tdbl || p.io_bytes == 8 ? 8 : 4);
-        char* de = static_cast<char*>(du) + (size_t)e * p.elem_stride * (tdbl || p.io_bytes == 8 ? 8 : 4);
-        char* sp = static_cast<char*>(p.d_spec) + (size_t)e * p.Nx * hspec * celem;
-        if ((st = fft_pass(p, p.Ny, FFT_R2C, -1, ue, sp, N, N, p.x_stride, hspec, N, nb, 1.0, p.d_tw_y, nullptr,
-                           nullptr, false, false, 0, s)))
-            return st;
-        if ((st = fft_pass(p, p.Ny, FFT_C2R, 1, sp, de, N, N, hspec, p.x_stride, N, nb, 1.0 / p.Ny, p.d_tw_y, nullptr,
-                           nullptr, false, false, 3, s, nullptr, order, w)))
+        const char* ue = static_cast<const char*>(u) + (size_t)e * p.elem_stride * esz;
+        char* de = static_cast<char*>(du) + (size_t)e * p.elem_stride * esz;
+        if ((st = fft_pass(p, p.Ny, FFT_DERIV, -1, ue, de, N, N, p.x_stride, p.x_stride, N, nb, 1.0 / p.Ny, p.d_tw_y,
+                           nullptr, nullptr, false, false, 1, s, nullptr, order, w)))
             return st;
     }
     return HELM_OK;
@@ -1756,7 +1756,9 @@ const char* helm_plan_kernels(helm_plan_t plan)
     if (rv == 3 && (p.precision != HELM_FP32_REFINE || !p.d_fmma)) rv = 0;
     std::string k;
     if (rv == 4) {
-        k = p.dim == 3 ? "eig_fwd_kernel eig_conv_kernel eig_inv_kernel" : "eig_solve2d_kernel";
+        if (p.dim != 3) k = "eig_solve2d_kernel";
+        else if (p.Nx >= 64 && (p.fft_var[1] & 2)) k = "eig_fwd_split_kernel eig_conv_kernel eig_inv_split_kernel";
+        else k = "eig_fwd_kernel eig_conv_kernel eig_inv_kernel";
     } else {
         const bool slab = rv == 2 && p.slab_ok && p.fast && p.precision != HELM_FP32;
         std::string rows;

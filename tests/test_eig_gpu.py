@@ -26,6 +26,7 @@ pytestmark = pytest.mark.gpu
 
 BC_DIR = (0.0, 0.5, 0.0, 2.0)  # Dirichlet ends with beta_l = 0.5, beta_r = 2
 KERNELS3 = {4: "eig_fwd_kernel eig_conv_kernel eig_inv_kernel"}
+KERNELS3_SPLIT = "eig_fwd_split_kernel eig_conv_kernel eig_inv_split_kernel"
 
 
 def _status_ok(p):
@@ -38,16 +39,17 @@ def _dev(a):
 
 
 def _pin(p, rows, conv=None):
-    """Pins the row variant (and, given conv, the CTA shape of the 3D second
-    pass: bit 0 of the y-pass variant, 0 = 16 columns x 256 threads, 1 = 8 x 128)."""
+    """Pins the row variant (and, given conv, bits 0-1 of the y-pass variant:
+    bit 0 the CTA shape of the 3D second pass, 0 = 16 columns x 256 threads,
+    1 = 8 x 128; bit 1 the pair-split first and third passes, Nx >= 64)."""
     fft = p.launch_variants()["fft"]
     if conv is not None:
-        fft[1] = (fft[1] & ~1) | conv
+        fft[1] = (fft[1] & ~3) | conv
     p.set_launch_variants(fft, rows)
     assert p.launch_variants()["rows"] == rows
 
 
-@pytest.mark.parametrize("conv", [0, 1])
+@pytest.mark.parametrize("conv", [0, 1, 2, 3])
 @pytest.mark.parametrize("rv", [4])
 @pytest.mark.parametrize("precision", ["fp64", "fp32_refine"])
 @pytest.mark.parametrize("Nx,Ny,N", [(8, 4, 5), (16, 8, 9), (32, 16, 17), (64, 32, 33), (128, 64, 65),
@@ -60,7 +62,7 @@ def test_eig_3d_vs_oracle(cuda, Nx, Ny, N, precision, rv, conv):
     ref = O.solve3d(f, gl, gr, Lx=1.3, Ly=0.7, Lz=0.9, lam=lam, bc=BC_DIR)
     p = NonPeriodic3D(Nx, Ny, N, N, 0.0, 1.3, 0.0, 0.7, 0.0, 0.9, Lambda=lam, bc=BC_DIR, precision=precision)
     _pin(p, rv, conv)
-    assert p.kernels() == KERNELS3[rv]
+    assert p.kernels() == (KERNELS3_SPLIT if (conv & 2 and Nx >= 64) else KERNELS3[rv])
     fd, gld, grd = _dev(f), _dev(gl), _dev(gr)
     for _ in range(2):  # the spectrum scratch is reused: two solves in a row
         u = p.SolvePDE(fd, gld, grd).cpu().numpy()
@@ -107,7 +109,7 @@ def test_eig_golden_3d(cuda, rv):
     assert max_rel(p.SolvePDE(_dev(g["f"])).cpu().numpy(), g["u"]) < 1e-12
 
 
-@pytest.mark.parametrize("conv", [0, 1])
+@pytest.mark.parametrize("conv", [0, 1, 2, 3])
 @pytest.mark.parametrize("rv", [4])
 @pytest.mark.parametrize("precision", ["fp64", "fp32_refine"])
 def test_eig_full_size_vs_oracle(cuda, precision, rv, conv):
@@ -123,19 +125,20 @@ def test_eig_full_size_vs_oracle(cuda, precision, rv, conv):
     _status_ok(p)
 
 
+@pytest.mark.parametrize("Nx,split", [(32, 0), (64, 0), (64, 2)])
 @pytest.mark.parametrize("rv", [4])
-def test_eig_reference_layout(cuda, rv):
+def test_eig_reference_layout(cuda, rv, Nx, split):
     """The reference's padded arrays rhsPDE[2Nx][2Ny][N], leftBC[2Nx][2Ny]:
     results in the [Nx][Ny] corner, padding untouched."""
     rng = np.random.default_rng(5)
-    Nx, Ny, N = 32, 16, 17
+    Ny, N = 16, 17
     f, gl, gr = rng.standard_normal((Nx, Ny, N)), rng.standard_normal((Nx, Ny)), rng.standard_normal((Nx, Ny))
     ref = O.solve3d(f, gl, gr, Lx=1.0, Ly=2.0, Lz=1.5, lam=2.0, bc=BC_DIR)
     F = np.zeros((2 * Nx, 2 * Ny, N)); F[:Nx, :Ny] = f
     GL = np.zeros((2 * Nx, 2 * Ny)); GL[:Nx, :Ny] = gl
     GR = np.zeros((2 * Nx, 2 * Ny)); GR[:Nx, :Ny] = gr
     p = NonPeriodic3D(Nx, Ny, N, N, 0.0, 1.0, 0.0, 2.0, 0.0, 1.5, Lambda=2.0, bc=BC_DIR)
-    _pin(p, rv)
+    _pin(p, rv, split)
     p.set_layout(x_stride=2 * Ny * N, elem_stride=2 * Nx * 2 * Ny * N, bc_x_stride=2 * Ny)
     fd, gld, grd = _dev(F), _dev(GL), _dev(GR)
     ud = torch.full((2 * Nx, 2 * Ny, N), 7.0, dtype=torch.float64, device="cuda")
@@ -166,10 +169,12 @@ def test_eig_declines_other_plans(cuda):
         _pin(p, 4)
 
 
-@pytest.mark.parametrize("dim,shape,rv", [(3, (8, 4, 5), 4), (3, (32, 16, 17), 4), (3, (128, 64, 65), 4),
-                                          (3, (256, 8, 66), 4), (2, (64, 33), 4), (2, (256, 66), 4)])
+@pytest.mark.parametrize("dim,shape,rv,split", [(3, (8, 4, 5), 4, 0), (3, (32, 16, 17), 4, 0),
+                                                (3, (128, 64, 65), 4, 0), (3, (128, 64, 65), 4, 2),
+                                                (3, (256, 8, 66), 4, 0), (3, (256, 8, 66), 4, 2),
+                                                (3, (64, 16, 33), 4, 2), (2, (64, 33), 4, 0), (2, (256, 66), 4, 0)])
 @pytest.mark.parametrize("precision", ["fp64", "fp32_refine"])
-def test_eig_adjoint_matches_row_kernel_adjoint(cuda, dim, shape, rv, precision):
+def test_eig_adjoint_matches_row_kernel_adjoint(cuda, dim, shape, rv, split, precision):
     """The transposed pipeline (row variant 4) against the transposed row-kernel
     pipeline (variant 0; checked against dense adjoint maps in
     test_adjoint_gpu.py): fbar, the boundary cotangents (beta != 1) and
@@ -186,7 +191,7 @@ def test_eig_adjoint_matches_row_kernel_adjoint(cuda, dim, shape, rv, precision)
     uobs = _dev(rng.standard_normal(shape))
     out = {}
     for v in (0, rv):
-        _pin(p, v)
+        _pin(p, v, split if v == rv and dim == 3 else None)
         u = p.SolvePDE(f)
         fb, lb, glb, grb = p.SolveAdjoint(ubar, u=u, want_bc=True)
         mfb, mlb, mglb, mgrb = p.SolveAdjointMisfit(u, uobs, want_bc=True)
