@@ -28,6 +28,7 @@
 #include <new>
 #include <numeric>
 #include <string>
+#include <type_traits>
 #include <vector>
 
 #include "../../include/helm_b200.h"
@@ -44,11 +45,14 @@ constexpr int BE_THREADS = 256;   // 8 warps; two or three CTAs share an SM
 constexpr int BE_MINB = 2;        // resident CTAs per SM the kernel is built for
 constexpr int BE_ROWS = 64;       // x rows of a kind-1 / kind-3 item (one 8-row tile per warp)
 
-// Complex columns of a kind-2 item: at most 16, and few enough that the tile
-// (Nx rows of CT + 1 double2) stays near 36 KB, so several CTAs fit an SM.
+// Complex columns of a kind-2 item: as many as the CTA's FFT transforms in
+// one round (256 threads over nx / r0 threads per column, r0 the first radix
+// of a length-nx transform), at most ld.  The tile (nx rows of CT + 1
+// double2) stays at or below 74 KB, so two CTAs fit an SM.
 __host__ __device__ constexpr int be_cols(int nx, int ld)
 {
-    const int cap = nx >= 512 ? 4 : nx >= 256 ? 8 : 16;
+    const int r0 = (nx >= 128) ? 16 : nx <= 16 ? nx : 8;  // 512: the radix-16-first schedule
+    const int cap = 256 * r0 / nx;
     return ld < cap ? ld : cap;
 }
 constexpr long long BE_WAIT_LIMIT = 1ll << 24;
@@ -81,7 +85,7 @@ struct BeArgs {
     int* done2;               // kind-2 items finished, per problem
     int* err;                 // status word: 7 when a dependency wait ran out
     const double2* tw[10];    // exp(-2 pi i e / 2^k), k = 3 .. 9
-    double Lx;
+    double w2;                // (2 pi / Lx)^2: the shift of wavenumber kx is lam + w2 kx^2
 };
 
 __device__ __forceinline__ void red_release_add(int* p)
@@ -96,9 +100,10 @@ __device__ __forceinline__ int ld_acquire(const int* p)
     return v;
 }
 
-// Kind 1: rows x0 .. x0+R-1 of problem pr -> coefficient rows.  Warp w owns
-// the 8-row tile w and both folds: one pair of row loads feeds the symmetric
-// and the antisymmetric A fragment of every k step.
+// Kind 1: rows x0 .. x0+R-1 of problem pr -> coefficient rows.  The rows
+// are staged once for the CTA; warp w then owns n-tile w % NT of both folds
+// over NT consecutive 8-row m-tiles (all eight when NT = 8), so each B
+// fragment it loads feeds NT products of each fold.
 template <int LD>
 __device__ void be_rows_in(const BeArgs& a, const BeProblem& pr, const BeClass& c, int idx, double* sm)
 {
@@ -107,49 +112,84 @@ __device__ void be_rows_in(const BeArgs& a, const BeProblem& pr, const BeClass& 
     double* st = sm;  // [R][pitch]; the boundary slots stay zero (homogeneous Dirichlet)
     const double* f = a.f + pr.off + (long long)x0 * P;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, g = lane >> 2, q = lane & 3;
-    for (int r = warp; r < R; r += BE_THREADS / 32)  // a warp per row, lanes along the row
-        for (int k = lane; k < P; k += 32) st[r * pitch + k] = (k > 0 && k < P - 1) ? __ldg(f + r * P + k) : 0.0;
+    // a warp per row, lanes along the row: asynchronous copies, all in flight
+    // before the one wait
+    for (int r = warp; r < R; r += BE_THREADS / 32)
+        for (int k = lane; k < P; k += 32) {
+            if (k > 0 && k < P - 1) cp_async_bytes8(st + r * pitch + k, f + r * P + k, true);
+            else st[r * pitch + k] = 0.0;
+        }
+    cp_async_commit();
+    cp_async_wait_all();
     __syncthreads();
-    if (warp * 8 >= R) return;
+    // fold each row in place, once: slots [0, LD) the symmetric fold, [LD, 2 LD)
+    // the antisymmetric one, zero past ms / m (a warp per row: all reads, then
+    // all writes)
+    const int n = c.n, m = c.m, ms = c.ms;
+    for (int r = warp; r < R; r += BE_THREADS / 32) {
+        double* row = st + r * pitch;
+        double fs[(LD + 31) / 32], fa[(LD + 31) / 32];
+#pragma unroll
+        for (int i = 0; i < (LD + 31) / 32; ++i) {
+            const int k = lane + 32 * i;
+            double vs = 0.0, va = 0.0;
+            if (k < m) {
+                const double lo = row[1 + k], hi = row[n - k];
+                vs = kR2 * (lo + hi);
+                va = kR2 * (lo - hi);
+            } else if (k < ms) {
+                vs = row[1 + k];
+            }
+            fs[i] = vs;
+            fa[i] = va;
+        }
+        __syncwarp();
+#pragma unroll
+        for (int i = 0; i < (LD + 31) / 32; ++i) {
+            const int k = lane + 32 * i;
+            if (k < LD) {
+                row[k] = fs[i];
+                row[LD + k] = fa[i];
+            }
+        }
+    }
+    __syncthreads();
+    const int nt = warp % NT, mt0 = (warp / NT) * NT;
+    if (mt0 * 8 >= R) return;
+    const int nmt = min(NT, R / 8 - mt0);  // live m-tiles of this warp
     double cs[NT][2], ca[NT][2];
 #pragma unroll
     for (int t = 0; t < NT; ++t) cs[t][0] = cs[t][1] = ca[t][0] = ca[t][1] = 0.0;
-    const double* row = st + (warp * 8 + g) * pitch;
-    const double* Bs = c.first;
-    const double* Ba = c.first + (size_t)NT * KK * 32;
-    const int n = c.n, m = c.m, ms = c.ms;
-#pragma unroll
+    const double* Bs = c.first + (size_t)nt * KK * 32 + lane;
+    const double* Ba = c.first + (size_t)(NT + nt) * KK * 32 + lane;
+#pragma unroll 4
     for (int kk = 0; kk < KK; ++kk) {
-        const int k = 4 * kk + q;
-        double vs = 0.0, va = 0.0;
-        if (k < m) {
-            const double lo = row[1 + k], hi = row[n - k];
-            vs = kR2 * (lo + hi);
-            va = kR2 * (lo - hi);
-        } else if (k < ms) {
-            vs = row[1 + k];
-        }
+        const double bs = __ldg(Bs + kk * 32), ba = __ldg(Ba + kk * 32);
 #pragma unroll
-        for (int nt = 0; nt < NT; ++nt) {
-            dmma_8x8x4(cs[nt][0], cs[nt][1], vs, __ldg(Bs + (nt * KK + kk) * 32 + lane));
-            dmma_8x8x4(ca[nt][0], ca[nt][1], va, __ldg(Ba + (nt * KK + kk) * 32 + lane));
+        for (int t = 0; t < NT; ++t) {
+            if (t < nmt) {
+                const double* row = st + ((mt0 + t) * 8 + g) * pitch;
+                dmma_8x8x4(cs[t][0], cs[t][1], row[4 * kk + q], bs);
+                dmma_8x8x4(ca[t][0], ca[t][1], row[LD + 4 * kk + q], ba);
+            }
         }
     }
-    double* crow = a.C + pr.coff + (long long)(x0 + warp * 8 + g) * 2 * LD;
 #pragma unroll
-    for (int nt = 0; nt < NT; ++nt) {
-        *reinterpret_cast<double2*>(crow + nt * 8 + 2 * q) = make_double2(cs[nt][0], cs[nt][1]);
-        *reinterpret_cast<double2*>(crow + LD + nt * 8 + 2 * q) = make_double2(ca[nt][0], ca[nt][1]);
+    for (int t = 0; t < NT; ++t) {
+        if (t < nmt) {
+            double* crow = a.C + pr.coff + (long long)(x0 + (mt0 + t) * 8 + g) * 2 * LD;
+            *reinterpret_cast<double2*>(crow + nt * 8 + 2 * q) = make_double2(cs[t][0], cs[t][1]);
+            *reinterpret_cast<double2*>(crow + LD + nt * 8 + 2 * q) = make_double2(ca[t][0], ca[t][1]);
+        }
     }
 }
 
-// 1 / ((mu_j - sigma) Nx) of real coefficient column j (zero on padding slots).
-__device__ __forceinline__ double be_recip(const BeClass& c, int j, double sig, double scale)
+// Eigenvalue of real coefficient column j; live = false on padding slots.
+__device__ __forceinline__ double be_mu(const BeClass& c, int j, bool& live)
 {
     const int ld = c.ld;
-    const bool live = j < ld ? j < c.ms : (j - ld) < c.ma;
-    if (!live) return 0.0;
-    return scale / (c.mu[j < ld ? j : c.ms + (j - ld)] - sig);
+    live = j < ld ? j < c.ms : (j - ld) < c.ma;
+    return live ? c.mu[j < ld ? j : c.ms + (j - ld)] : 0.0;
 }
 
 // Kind 2: column pairs [16 idx, 16 idx + CT) of problem pr, along x.
@@ -162,22 +202,30 @@ __device__ void be_columns(const BeArgs& a, const BeProblem& pr, const BeClass& 
     double* Cb = a.C + pr.coff;
     for (int e = threadIdx.x; e < L * CT; e += BE_THREADS) {
         const int x = e / CT, cc = e - x * CT;
-        z[x * HS + cc] = __ldcg(reinterpret_cast<const double2*>(Cb + (long long)x * ld2 + col0 + 2 * cc));
+        cp_async_bytes16(&z[x * HS + cc], Cb + (long long)x * ld2 + col0 + 2 * cc, true);
     }
+    cp_async_commit();
+    cp_async_wait_all();
     __syncthreads();
     const double2* tw = a.tw[LOG2];
-    slab_fft<L, -1, BE_THREADS>(z, HS, CT, tw);
+    using RS = typename std::conditional<L == 512, Radix512Wide, Radix<L>>::type;
+    slab_fft<L, -1, BE_THREADS, 0, 1, RS>(z, HS, CT, tw);
     // real-to-complex split of each column pair, scaling, and the assembly of
     // the full-length spectrum for the inverse (imaginary parts dropped at
     // kx = 0 and L / 2)
+    // a thread keeps one column pair (BE_THREADS is a multiple of CT): its two
+    // eigenvalues are loaded once, the shift of each kx is lam + w2 kx^2
     const double scale = 1.0 / L;
+    const int cc = threadIdx.x % CT;
+    bool live0, live1;
+    const double mu0 = be_mu(c, col0 + 2 * cc, live0), mu1 = be_mu(c, col0 + 2 * cc + 1, live1);
     for (int e = threadIdx.x; e < (L / 2 + 1) * CT; e += BE_THREADS) {
-        const int kx = e / CT, cc = e - kx * CT, km = (L - kx) & (L - 1);
+        const int kx = e / CT, km = (L - kx) & (L - 1);
         const double2 zk = z[kx * HS + cc], zm = z[km * HS + cc];
         double2 X = make_double2(0.5 * (zk.x + zm.x), 0.5 * (zk.y - zm.y));
         double2 Y = make_double2(0.5 * (zk.y + zm.y), 0.5 * (zm.x - zk.x));
-        const double sig = pr.lam + 4.0 * kBePi * kBePi * kx * kx / (a.Lx * a.Lx);
-        const double r0 = be_recip(c, col0 + 2 * cc, sig, scale), r1 = be_recip(c, col0 + 2 * cc + 1, sig, scale);
+        const double sig = pr.lam + a.w2 * (double)(kx * kx);
+        const double r0 = live0 ? scale / (mu0 - sig) : 0.0, r1 = live1 ? scale / (mu1 - sig) : 0.0;
         X = make_double2(X.x * r0, X.y * r0);
         Y = make_double2(Y.x * r1, Y.y * r1);
         if (kx == 0 || kx == L / 2) { X.y = 0.0; Y.y = 0.0; }
@@ -185,66 +233,72 @@ __device__ void be_columns(const BeArgs& a, const BeProblem& pr, const BeClass& 
         if (kx > 0 && kx < L / 2) z[km * HS + cc] = make_double2(X.x + Y.y, Y.x - X.y);
     }
     __syncthreads();
-    slab_fft<L, 1, BE_THREADS>(z, HS, CT, tw);
+    slab_fft<L, 1, BE_THREADS, 0, 1, RS>(z, HS, CT, tw);
     for (int e = threadIdx.x; e < L * CT; e += BE_THREADS) {
         const int x = e / CT, cc = e - x * CT;
         __stcg(reinterpret_cast<double2*>(Cb + (long long)x * ld2 + col0 + 2 * cc), z[x * HS + cc]);
     }
 }
 
-// Second transform of one fold of the warp's 8 coefficient rows, in place.
-template <int LD>
-__device__ __forceinline__ void be_second(const double* B, double* rows, int lane)
-{
-    constexpr int NT = LD / 8, KK = LD / 4, PITCH = 2 * LD + 4;
-    const int g = lane >> 2, q = lane & 3;
-    double acc[NT][2];
-#pragma unroll
-    for (int t = 0; t < NT; ++t) acc[t][0] = acc[t][1] = 0.0;
-    const double* row = rows + g * PITCH;
-#pragma unroll
-    for (int kk = 0; kk < KK; ++kk) {
-        const double av = row[4 * kk + q];
-#pragma unroll
-        for (int nt = 0; nt < NT; ++nt) dmma_8x8x4(acc[nt][0], acc[nt][1], av, __ldg(B + (nt * KK + kk) * 32 + lane));
-    }
-    __syncwarp();
-#pragma unroll
-    for (int nt = 0; nt < NT; ++nt)
-        *reinterpret_cast<double2*>(rows + g * PITCH + nt * 8 + 2 * q) = make_double2(acc[nt][0], acc[nt][1]);
-    __syncwarp();
-}
-
 // Kind 3: coefficient rows x0 .. x0+R-1 -> second transform, unfold -> u rows.
-// Warp w owns rows 8 w .. 8 w + 7 from the load to the store.
+// The coefficient rows are staged once for the CTA; warp w owns n-tile w % NT
+// of both folds over NT m-tiles (as kind 1), and after every warp has read the
+// rows its results overwrite them, ready for the unfold.
 template <int LD>
 __device__ void be_rows_out(const BeArgs& a, const BeProblem& pr, const BeClass& c, int idx, double* sm)
 {
     constexpr int NT = LD / 8, KK = LD / 4, PITCH = 2 * LD + 4;
     const int R = pr.nx < BE_ROWS ? pr.nx : BE_ROWS, x0 = idx * BE_ROWS, P = c.P;
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    if (warp * 8 >= R) return;
-    double* rows = sm + warp * 8 * PITCH;  // [8][PITCH]: coefficients, then the transformed values
-    const double* Cb = a.C + pr.coff + (long long)(x0 + warp * 8) * 2 * LD;
-    for (int e = lane; e < 8 * LD; e += 32) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, g = lane >> 2, q = lane & 3;
+    double* rows = sm;  // [R][PITCH]: coefficients (s | d), then the transformed values
+    const double* Cb = a.C + pr.coff + (long long)x0 * 2 * LD;
+    for (int e = threadIdx.x; e < R * LD; e += BE_THREADS) {
         const int r = e / LD, j2 = 2 * (e - r * LD);
-        *reinterpret_cast<double2*>(rows + r * PITCH + j2) =
-            __ldcg(reinterpret_cast<const double2*>(Cb + (long long)r * 2 * LD + j2));
+        cp_async_bytes16(rows + r * PITCH + j2, Cb + (long long)r * 2 * LD + j2, true);
     }
-    __syncwarp();
-    be_second<LD>(c.second, rows, lane);                                          // s: symmetric fold
-    be_second<LD>(c.second + (size_t)NT * KK * 32, rows + LD, lane);              // d: antisymmetric fold
+    cp_async_commit();
+    cp_async_wait_all();
+    __syncthreads();
+    const int nt = warp % NT, mt0 = (warp / NT) * NT;
+    const int nmt = mt0 * 8 >= R ? 0 : min(NT, R / 8 - mt0);
+    double vs[NT][2], vd[NT][2];
+#pragma unroll
+    for (int t = 0; t < NT; ++t) vs[t][0] = vs[t][1] = vd[t][0] = vd[t][1] = 0.0;
+    const double* Bs = c.second + (size_t)nt * KK * 32 + lane;
+    const double* Bd = c.second + (size_t)(NT + nt) * KK * 32 + lane;
+#pragma unroll 4
+    for (int kk = 0; kk < KK; ++kk) {
+        const double bs = __ldg(Bs + kk * 32), bd = __ldg(Bd + kk * 32);
+#pragma unroll
+        for (int t = 0; t < NT; ++t) {
+            if (t < nmt) {
+                const double* row = rows + ((mt0 + t) * 8 + g) * PITCH;
+                dmma_8x8x4(vs[t][0], vs[t][1], row[4 * kk + q], bs);
+                dmma_8x8x4(vd[t][0], vd[t][1], row[LD + 4 * kk + q], bd);
+            }
+        }
+    }
+    __syncthreads();  // every warp has read the coefficients
+#pragma unroll
+    for (int t = 0; t < NT; ++t) {
+        if (t < nmt) {
+            double* row = rows + ((mt0 + t) * 8 + g) * PITCH;
+            *reinterpret_cast<double2*>(row + nt * 8 + 2 * q) = make_double2(vs[t][0], vs[t][1]);
+            *reinterpret_cast<double2*>(row + LD + nt * 8 + 2 * q) = make_double2(vd[t][0], vd[t][1]);
+        }
+    }
+    __syncthreads();
     const int n = c.n, m = c.m, ms = c.ms;
-    double* u = a.u + pr.off + (long long)(x0 + warp * 8) * P;
-    for (int r = 0; r < 8; ++r) {
-        const double* s = rows + r * PITCH;
+    double* u = a.u + pr.off + (long long)x0 * P;
+    for (int r = warp; r < R; r += BE_THREADS / 32) {
+        const double* sr = rows + r * PITCH;
         for (int k = lane; k < P; k += 32) {
             double v = 0.0;
             if (k > 0 && k < P - 1) {
                 const int j = k - 1;
-                if (j < m) v = kR2 * (s[j] + s[LD + j]);
-                else if (j < ms) v = s[j];
-                else v = kR2 * (s[n - 1 - j] - s[LD + n - 1 - j]);
+                if (j < m) v = kR2 * (sr[j] + sr[LD + j]);
+                else if (j < ms) v = sr[j];
+                else v = kR2 * (sr[n - 1 - j] - sr[LD + n - 1 - j]);
             }
             u[r * P + k] = v;
         }
@@ -418,8 +472,11 @@ int batch_eig_create(int nprob, const int* Nx, const int* N, const double* lambd
         c.ms = fe.ms;
         c.ma = fe.ma;
         c.ld = fe.ms <= 8 ? 8 : fe.ms <= 16 ? 16 : fe.ms <= 32 ? 32 : 64;
-        c.pitch = 4 + 16 * ((P + 11) / 16);  // >= P, = 4 mod 16: conflict-free fragment loads
         const int ld = c.ld;
+        // staged row: the P values, then in place their two folds (2 ld slots);
+        // = 4 mod 16 doubles: conflict-free fragment loads
+        c.pitch = 4;
+        while (c.pitch < std::max(P, 2 * ld)) c.pitch += 16;
         const size_t frag = (size_t)ld * ld;
         std::vector<double> first(2 * frag), second(2 * frag), mu(2 * (size_t)ld, 0.0);
         swizzle_b(fe.Vsi, fe.ms, ld, first.data());
@@ -448,8 +505,9 @@ int batch_eig_create(int nprob, const int* Nx, const int* N, const double* lambd
         const int ci = cls_of[N[i]];
         const BeClass& c = cls[ci];
         const FoldedEigen& fe = eig[ci];
+        const double w2 = 4.0 * kBePi * kBePi / (Lx * Lx);  // as the kernel forms the shift
         for (int kx = 0; kx <= Nx[i] / 2 && !st; ++kx) {
-            const double sig = lambda[i] + 4.0 * kBePi * kBePi * kx * kx / (Lx * Lx);
+            const double sig = lambda[i] + w2 * (double)(kx * kx);
             for (double l : fe.ls)
                 if (!(std::fabs(l - sig) > 1e-12 * std::max(std::fabs(l), std::fabs(sig)))) st = HELM_ERR_SINGULAR;
             for (double l : fe.la)
@@ -529,7 +587,7 @@ int batch_eig_create(int nprob, const int* Nx, const int* N, const double* lambd
     a.done1 = be->d_counters + 1;
     a.done2 = be->d_counters + 1 + nprob;
     a.err = static_cast<int*>(derr);
-    a.Lx = Lx;
+    a.w2 = 4.0 * kBePi * kBePi / (Lx * Lx);
     be->nitems = a.nitems;
     be->smem = smem;
     int nsm = 0;

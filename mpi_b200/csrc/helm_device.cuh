@@ -160,16 +160,19 @@ __device__ __forceinline__ void slab_sync()
     else asm volatile("bar.sync %0, %1;\n" ::"n"(BAR), "n"(THREADS) : "memory");
 }
 
+// Length-512 schedule with a radix-16 first pass: 32 threads per column
+// instead of 64 (twice the columns per round of a slab FFT).
+struct Radix512Wide { static constexpr int n = 3, r0 = 16, r1 = 8, r2 = 4; };
+
 // One length-L FFT (direction DIR, unscaled) of each of the ncol columns of the
 // [L][hs] complex array sm in shared memory, in place; threads 0 .. THREADS-1
 // call it (it synchronises them through slab_sync<BAR, THREADS>).  tw: the
 // twiddle table exp(-2 pi i e / (TWS L)), read at every TWS-th entry (TWS = 2:
-// the table of a transform twice as long).
-template <int L, int DIR, int THREADS, int BAR = 0, int TWS = 1>
+// the table of a transform twice as long); RS: the radix schedule.
+template <int L, int DIR, int THREADS, int BAR = 0, int TWS = 1, class RS = Radix<L>>
 __device__ __forceinline__ void slab_fft(cplx_t<double>* sm, int hs, int ncol, const cplx_t<double>* tw)
 {
     using C = cplx_t<double>;
-    using RS = Radix<L>;
     constexpr int R0 = RS::r0, R1 = RS::r1, R2 = RS::r2, NP = RS::n, TPC = L / R0, CPR = THREADS / TPC;
     constexpr int RL = (NP == 1) ? R0 : (NP == 2 ? R1 : R2);
     const int tc = threadIdx.x / CPR, cl = threadIdx.x - tc * CPR;

@@ -716,12 +716,16 @@ static int fft_dispatch_mode(int mode, int dir, const FftArgs& a, long long tc, 
 // columns per tile), bit 1 -> radix-8 schedule (lengths 128 and 256), bit 2 ->
 // the persistent pipelined kernel, bit 3 -> 512-thread CTAs for lengths 512 and
 // 1024 (twice the columns per tile: 128-byte runs of each row instead of 64 on
-// the strided x pass; bit 0 is then ignored).
+// the strided x pass); bits 3 and 0 together on an FP32 pass of length 1024:
+// 1024-thread CTAs (16 column pairs, whole 128-byte lines of FP32 rows).
 template <typename T, typename TIO, int L>
 static int fft_dispatch_variant(int variant, int mode, int dir, const FftArgs& a, long long tc, cudaStream_t s)
 {
     const bool small_cta = !(variant & 8) && (variant & 1) && (L / Radix<L>::r0 <= 128);
     const bool pipe = (variant & 4) != 0;
+    if constexpr (L == 1024 && sizeof(T) == 4) {
+        if ((variant & 9) == 9 && !pipe) return fft_dispatch_mode<T, TIO, L, 1024, 0>(mode, dir, a, tc, s, false);
+    }
     if constexpr (L >= 512) {
         if (variant & 8) return fft_dispatch_mode<T, TIO, L, 512, 0>(mode, dir, a, tc, s, pipe);
     }
