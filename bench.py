@@ -72,11 +72,14 @@ def profile_case(which: str):
         from mpi_b200 import Helmholtz3DFD
 
         # fd32x: the length-1024 x passes of the FD workload on a 1024 x 512 x 64
-        # grid (134 MB FP32 field, larger than L2)
+        # grid (134 MB FP32 field, larger than L2), FP32 I/O as the bench's FD leg
         nx, ny, nz = (1024, 512, 64) if which == "fd32x" else (256, 256, 256)
         f = torch.from_numpy(W.smooth_field_fd(nx, ny, nz, seed=1239)).cuda()
         p = Helmholtz3DFD(nx, ny, nz, 0.0, 1.0, 0.0, 1.0, 0.0, 1.0, Lambda=1.0,
                           precision="fp64" if which == "fd64" else "fp32")
+        if which == "fd32x":
+            p.set_io_bytes(4)
+            f = f.float()
         run = lambda: p.SolvePDE(f)  # noqa: E731
     elif which == "deriv":
         from mpi_b200 import NonPeriodic3D
