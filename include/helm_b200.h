@@ -202,8 +202,10 @@ int helm_solve(helm_plan_t plan, const void* f, const double* gl, const double* 
  *     dL/dlambda = sum over the interior collocation nodes of fbar * u
  * (d(A u)/d lambda = -u on the interior rows, so du/dlambda = A^-1 u), where u
  * must be the forward solution of the same plan; the sum is written to the
- * DEVICE double *lambda_bar.  Ns = 1 plans.  No counterpart in the reference,
- * which has no gradients. */
+ * DEVICE double *lambda_bar.  Plans with the FDM method (one GLL element, or
+ * several elements not periodic in the GLL direction) and finite-difference
+ * plans; LU plans (operator callbacks) return HELM_ERR_UNSUPPORTED.  No
+ * counterpart in the reference, which has no gradients. */
 int helm_solve_adjoint(helm_plan_t plan, const double* ubar, double* fbar, double* glbar, double* grbar,
                        const double* u, double* lambda_bar, void* stream);
 
