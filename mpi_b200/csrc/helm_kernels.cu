@@ -1508,26 +1508,27 @@ struct TriEq {
     cplx_t<T> d;
 };
 
+// Shuffles of a whole equation within segments of w lanes.
 template <typename T>
-__device__ __forceinline__ TriEq<T> tri_shfl_up(const TriEq<T>& e, int k)
+__device__ __forceinline__ TriEq<T> tri_shfl_up(const TriEq<T>& e, int k, int w = 32)
 {
     TriEq<T> o;
-    o.a = __shfl_up_sync(0xffffffffu, e.a, k);
-    o.b = __shfl_up_sync(0xffffffffu, e.b, k);
-    o.c = __shfl_up_sync(0xffffffffu, e.c, k);
-    o.d.x = __shfl_up_sync(0xffffffffu, e.d.x, k);
-    o.d.y = __shfl_up_sync(0xffffffffu, e.d.y, k);
+    o.a = __shfl_up_sync(0xffffffffu, e.a, k, w);
+    o.b = __shfl_up_sync(0xffffffffu, e.b, k, w);
+    o.c = __shfl_up_sync(0xffffffffu, e.c, k, w);
+    o.d.x = __shfl_up_sync(0xffffffffu, e.d.x, k, w);
+    o.d.y = __shfl_up_sync(0xffffffffu, e.d.y, k, w);
     return o;
 }
 template <typename T>
-__device__ __forceinline__ TriEq<T> tri_shfl_down(const TriEq<T>& e, int k)
+__device__ __forceinline__ TriEq<T> tri_shfl_down(const TriEq<T>& e, int k, int w = 32)
 {
     TriEq<T> o;
-    o.a = __shfl_down_sync(0xffffffffu, e.a, k);
-    o.b = __shfl_down_sync(0xffffffffu, e.b, k);
-    o.c = __shfl_down_sync(0xffffffffu, e.c, k);
-    o.d.x = __shfl_down_sync(0xffffffffu, e.d.x, k);
-    o.d.y = __shfl_down_sync(0xffffffffu, e.d.y, k);
+    o.a = __shfl_down_sync(0xffffffffu, e.a, k, w);
+    o.b = __shfl_down_sync(0xffffffffu, e.b, k, w);
+    o.c = __shfl_down_sync(0xffffffffu, e.c, k, w);
+    o.d.x = __shfl_down_sync(0xffffffffu, e.d.x, k, w);
+    o.d.y = __shfl_down_sync(0xffffffffu, e.d.y, k, w);
     return o;
 }
 // One cyclic-reduction update of equation e with its neighbours lo (index - s)
@@ -1546,49 +1547,61 @@ __device__ __forceinline__ TriEq<T> tri_reduce(const TriEq<T>& e, const TriEq<T>
 
 constexpr int TRI_WARPS = 4;
 
-// Copies row r of the spectrum into the lane-chunked buffer sb (asynchronous,
-// coalesced: step j moves elements 32 j .. 32 j + 31); elements >= Nz read 0.
-template <typename T, int M>
-__device__ __forceinline__ void tri_issue_row(const ThomasArgs& a, long long r, cplx_t<T>* sb, int lane)
+// Copies row r of the spectrum into the lane-chunked buffer sb of LPR chunks
+// of M (asynchronous, coalesced: step j moves elements 32 j .. 32 j + 31);
+// elements >= Nz, and every element of a row past the end (live = false), read 0.
+template <typename T, int M, int LPR>
+__device__ __forceinline__ void tri_issue_row(const ThomasArgs& a, long long r, bool live, cplx_t<T>* sb, int lane)
 {
     using C = cplx_t<T>;
-    const C* x = static_cast<const C*>(a.spec) + r * a.Nz;
+    const C* x = static_cast<const C*>(a.spec) + (live ? r : 0) * a.Nz;
 #pragma unroll
-    for (int j = 0; j < M; ++j) {
+    for (int j = 0; j < (LPR * M + 31) / 32; ++j) {
         const int e = j * 32 + lane;
-        const bool ok = e < a.Nz;
+        const bool ok = live && e < a.Nz;
         cp_async_elem<sizeof(C)>(&sb[(e / M) * (M + 1) + e % M], ok ? (const void*)&x[e] : a.spec, ok);
     }
 }
 
-template <typename T, int M>
+// LPR = 16: each half-warp solves its own row (two rows per warp, 16 chunks of
+// M per row, cyclic reduction over 16-lane segments: one step and half the
+// shuffles fewer per row than LPR = 32).
+template <typename T, int M, int LPR = 32>
 __global__ void __launch_bounds__(TRI_WARPS * 32, (M <= 8 ? 4 : 2)) thomas_warp_kernel(ThomasArgs a)
 {
     pdl_enter();
     using C = cplx_t<T>;
+    constexpr int RPW = 32 / LPR;            // rows per warp
+    constexpr int RB = LPR * (M + 1);        // one row's buffer
     extern __shared__ __align__(16) unsigned char tri_smem[];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    C* bufs = reinterpret_cast<C*>(tri_smem) + (size_t)warp * 2 * 32 * (M + 1);
+    const int li = lane % LPR, hrow = lane / LPR;  // lane within its row, row within the warp
+    C* bufs = reinterpret_cast<C*>(tri_smem) + (size_t)warp * 2 * RPW * RB;
     const int Nz = a.Nz;
     const T cz = (T)a.cz1;
     const TriEq<T> ident{(T)0, (T)1, (T)0, mk((T)0, (T)0)};
-    const long long stride = (long long)gridDim.x * TRI_WARPS;
-    long long r = (long long)blockIdx.x * TRI_WARPS + warp;
+    const long long stride = (long long)gridDim.x * TRI_WARPS * RPW;
+    long long r0 = ((long long)blockIdx.x * TRI_WARPS + warp) * RPW;  // first row of the warp
     int cur = 0;
-    if (r < a.nrows) tri_issue_row<T, M>(a, r, bufs, lane);
+    if (r0 < a.nrows)
+        for (int hh = 0; hh < RPW; ++hh) tri_issue_row<T, M, LPR>(a, r0 + hh, r0 + hh < a.nrows, bufs + hh * RB, lane);
     cp_async_commit();
-    for (; r < a.nrows; r += stride, cur ^= 1) {
-        C* sb = bufs + (size_t)cur * 32 * (M + 1);
-        if (r + stride < a.nrows) tri_issue_row<T, M>(a, r + stride, bufs + (size_t)(cur ^ 1) * 32 * (M + 1), lane);
+    for (; r0 < a.nrows; r0 += stride, cur ^= 1) {
+        C* sbw = bufs + (size_t)cur * RPW * RB;
+        if (r0 + stride < a.nrows)
+            for (int hh = 0; hh < RPW; ++hh)
+                tri_issue_row<T, M, LPR>(a, r0 + stride + hh, r0 + stride + hh < a.nrows,
+                                         bufs + (size_t)(cur ^ 1) * RPW * RB + hh * RB, lane);
         cp_async_commit();
         cp_async_wait_prev();
         __syncwarp();
-        C* x = static_cast<C*>(a.spec) + r * Nz;
+        C* sb = sbw + hrow * RB;  // this lane's row
+        const long long r = min(r0 + hrow, a.nrows - 1);  // rows past the end solve zeros, unstored
         const int kx = (int)(r / a.Ny), ky = (int)(r - (long long)kx * a.Ny);
         const double dg = -2.0 * a.cz1 - a.lambda - a.mx[kx] - a.my[ky];
         C dv[M];
 #pragma unroll
-        for (int i = 0; i < M; ++i) dv[i] = sb[lane * (M + 1) + i];
+        for (int i = 0; i < M; ++i) dv[i] = sb[li * (M + 1) + i];
         // row k: sub (k >= 1), diagonal, super (k <= Nz - 2); transposed, the sub of
         // row k is the super of row k - 1 and the super of row k the sub of row k + 1.
         // Rows k >= Nz are identity rows.
@@ -1609,7 +1622,7 @@ __global__ void __launch_bounds__(TRI_WARPS * 32, (M <= 8 ? 4 : 2)) thomas_warp_
             if (k == Nz - 1) b += a.d_last;
             return (T)b;
         };
-        const int k0 = lane * M;
+        const int k0 = li * M;
         // ---- 1. eliminate the lane's interior rows ----
         TriEq<T> e0, e1;
         C y[M > 2 ? M - 2 : 1];
@@ -1644,25 +1657,25 @@ __global__ void __launch_bounds__(TRI_WARPS * 32, (M <= 8 ? 4 : 2)) thomas_warp_
             e1 = TriEq<T>{-aM * v[NI - 1], dia(k0 + M - 1) - aM * w[NI - 1], sup(k0 + M - 1),
                           mk(dv[M - 1].x - aM * y[NI - 1].x, dv[M - 1].y - aM * y[NI - 1].y)};
         }
-        // ---- 2. cyclic reduction of the 64 reduced equations (2 lane, 2 lane + 1) ----
+        // ---- 2. cyclic reduction of the 2 LPR reduced equations (2 li, 2 li + 1) ----
         {
             // stride 1: e0's lower neighbour is lane - 1's e1, e1's upper one lane + 1's e0
-            const TriEq<T> r0{e0.a, (T)1 / e0.b, e0.c, e0.d}, r1{e1.a, (T)1 / e1.b, e1.c, e1.d};
-            TriEq<T> lo = tri_shfl_up(r1, 1), hi = tri_shfl_down(r0, 1);
-            if (lane == 0) lo = ident;
-            if (lane == 31) hi = ident;
-            const TriEq<T> n0 = tri_reduce(e0, lo, r1);
-            const TriEq<T> n1 = tri_reduce(e1, r0, hi);
+            const TriEq<T> q0{e0.a, (T)1 / e0.b, e0.c, e0.d}, q1{e1.a, (T)1 / e1.b, e1.c, e1.d};
+            TriEq<T> lo = tri_shfl_up(q1, 1, LPR), hi = tri_shfl_down(q0, 1, LPR);
+            if (li == 0) lo = ident;
+            if (li == LPR - 1) hi = ident;
+            const TriEq<T> n0 = tri_reduce(e0, lo, q1);
+            const TriEq<T> n1 = tri_reduce(e1, q0, hi);
             e0 = n0;
             e1 = n1;
         }
 #pragma unroll
-        for (int k = 1; k < 32; k <<= 1) {  // strides 2, 4, .., 32 of the reduced index
-            const TriEq<T> r0{e0.a, (T)1 / e0.b, e0.c, e0.d}, r1{e1.a, (T)1 / e1.b, e1.c, e1.d};
-            TriEq<T> l0 = tri_shfl_up(r0, k), h0 = tri_shfl_down(r0, k);
-            TriEq<T> l1 = tri_shfl_up(r1, k), h1 = tri_shfl_down(r1, k);
-            if (lane < k) { l0 = ident; l1 = ident; }
-            if (lane + k > 31) { h0 = ident; h1 = ident; }
+        for (int k = 1; k < LPR; k <<= 1) {  // strides 2, 4, .., 2 LPR of the reduced index
+            const TriEq<T> q0{e0.a, (T)1 / e0.b, e0.c, e0.d}, q1{e1.a, (T)1 / e1.b, e1.c, e1.d};
+            TriEq<T> l0 = tri_shfl_up(q0, k, LPR), h0 = tri_shfl_down(q0, k, LPR);
+            TriEq<T> l1 = tri_shfl_up(q1, k, LPR), h1 = tri_shfl_down(q1, k, LPR);
+            if (li < k) { l0 = ident; l1 = ident; }
+            if (li + k > LPR - 1) { h0 = ident; h1 = ident; }
             const TriEq<T> n0 = tri_reduce(e0, l0, h0);
             const TriEq<T> n1 = tri_reduce(e1, l1, h1);
             e0 = n0;
@@ -1672,30 +1685,35 @@ __global__ void __launch_bounds__(TRI_WARPS * 32, (M <= 8 ? 4 : 2)) thomas_warp_
         const C xe = mk(e1.d.x / e1.b, e1.d.y / e1.b);
         // ---- 3. interior unknowns, coalesced store ----
         __syncwarp();
-        sb[lane * (M + 1)] = xs;
-        sb[lane * (M + 1) + M - 1] = xe;
+        sb[li * (M + 1)] = xs;
+        sb[li * (M + 1) + M - 1] = xe;
         if constexpr (M > 2) {
 #pragma unroll
             for (int j = 0; j < M - 2; ++j)
-                sb[lane * (M + 1) + j + 1] =
+                sb[li * (M + 1) + j + 1] =
                     mk(y[j].x - xs.x * v[j] - xe.x * w[j], y[j].y - xs.y * v[j] - xe.y * w[j]);
         }
         __syncwarp();
+        for (int hh = 0; hh < RPW; ++hh) {
+            if (r0 + hh >= a.nrows) break;
+            C* x = static_cast<C*>(a.spec) + (r0 + hh) * Nz;
+            const C* sr = sbw + hh * RB;
 #pragma unroll
-        for (int j = 0; j < M; ++j) {
-            const int e = j * 32 + lane;
-            if (e < Nz) x[e] = sb[(e / M) * (M + 1) + e % M];
+            for (int j = 0; j < (LPR * M + 31) / 32; ++j) {
+                const int e = j * 32 + lane;
+                if (e < Nz) x[e] = sr[(e / M) * (M + 1) + e % M];
+            }
         }
-        __syncwarp();  // sb is refilled by the copy issued in the next iteration
+        __syncwarp();  // the buffers are refilled by the copies issued in the next iteration
     }
     asm volatile("cp.async.wait_all;\n" ::);
 }
 
-template <typename T, int M>
+template <typename T, int M, int LPR = 32>
 static int run_thomas_warp(const ThomasArgs& a, cudaStream_t s)
 {
-    auto k = thomas_warp_kernel<T, M>;
-    const size_t smem = (size_t)TRI_WARPS * 2 * 32 * (M + 1) * sizeof(cplx_t<T>);
+    auto k = thomas_warp_kernel<T, M, LPR>;
+    const size_t smem = (size_t)TRI_WARPS * 2 * (32 / LPR) * LPR * (M + 1) * sizeof(cplx_t<T>);
     cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return (int)e;
     int dev = 0, sms = 148, per = 1;
@@ -1703,7 +1721,8 @@ static int run_thomas_warp(const ThomasArgs& a, cudaStream_t s)
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k, TRI_WARPS * 32, smem);
     if (per < 1) per = 1;
-    long long grid = (a.nrows + TRI_WARPS - 1) / TRI_WARPS;
+    const long long rows_per_cta = (long long)TRI_WARPS * (32 / LPR);
+    long long grid = (a.nrows + rows_per_cta - 1) / rows_per_cta;
     if (grid > (long long)sms * per) grid = (long long)sms * per;
     if (grid <= 0) return 0;
     return (int)launch_k(k, dim3((unsigned)grid), dim3(TRI_WARPS * 32), smem, s, a);
@@ -1712,6 +1731,12 @@ static int run_thomas_warp(const ThomasArgs& a, cudaStream_t s)
 template <typename T>
 static int thomas_dispatch(const ThomasArgs& a, cudaStream_t s)
 {
+    if (a.half) {  // a row per half-warp
+        if (a.Nz <= 32) return run_thomas_warp<T, 2, 16>(a, s);
+        if (a.Nz <= 64) return run_thomas_warp<T, 4, 16>(a, s);
+        if (a.Nz <= 128) return run_thomas_warp<T, 8, 16>(a, s);
+        if (a.Nz <= 256) return run_thomas_warp<T, 16, 16>(a, s);
+    }
     if (a.Nz <= 64) return run_thomas_warp<T, 2>(a, s);
     if (a.Nz <= 128) return run_thomas_warp<T, 4>(a, s);
     if (a.Nz <= 256) return run_thomas_warp<T, 8>(a, s);

@@ -83,6 +83,7 @@ struct ThomasArgs {
     const double* my;     // [Ny]
     double cz1, lambda, d_first, s_first, d_last, s_last;
     int transpose;        // solve with the transposed matrix (adjoint)
+    int half;             // Nz <= 256: one row per half-warp instead of per warp
 };
 
 // Per-wavenumber solve of the spectrum rows, grouped by shift sigma.

@@ -897,6 +897,7 @@ static int run_pipeline(Plan& p, const void* in, const double* gl, const double*
         ta.d_last = p.fd_dlast;
         ta.s_last = p.fd_slast;
         ta.transpose = adjoint ? 1 : 0;
+        ta.half = rv & 1;
         e = launch_thomas(prec, ta, s);
     } else if (p.fast) {
         FdmArgs fa{};
@@ -1049,6 +1050,8 @@ static int autotune(Plan& p)
     if (p.fast) {
         rows_cand = {0, 1};
         if (p.precision == HELM_FP32_REFINE && p.d_fmma) rows_cand.push_back(3);
+    } else if (p.fd && p.N <= 256) {
+        rows_cand = {0, 1};  // the tridiagonal solves: a row per warp or per half-warp
     } else {
         rows_cand = {0};
     }

@@ -40,15 +40,20 @@ def _stencil_residual(u, f, gb, gf, Lx, Ly, Lz, lam, bc):
     return ((f - au).norm() / f.norm()).item()
 
 
+@pytest.mark.parametrize("rows", [0, 1])
 @pytest.mark.parametrize("bc", [(0.0, 1.0, 0.0, 1.0), (1.0, 0.5, 0.7, 2.0)])
-@pytest.mark.parametrize("shape", [(16, 8, 12), (8, 32, 2), (64, 64, 33), (8, 8, 100), (8, 4, 300), (4, 4, 600)])
+@pytest.mark.parametrize("shape", [(16, 8, 12), (8, 32, 2), (64, 64, 33), (8, 8, 100), (8, 4, 300), (4, 4, 600),
+                                   (8, 4, 256)])
 @pytest.mark.parametrize("precision", ["fp64", "fp32"])
-def test_fd_matches_oracle(cuda, bc, shape, precision):
+def test_fd_matches_oracle(cuda, bc, shape, precision, rows):
+    """Both tridiagonal shapes (row variant 0: a row per warp; 1: a row per
+    half-warp for Nz <= 256, ignored above)."""
     rng = np.random.default_rng(hash((shape, bc)) % 2**32)
     Nx, Ny, Nz = shape
     f = rng.standard_normal(shape); gb = rng.standard_normal((Nx, Ny)); gf = rng.standard_normal((Nx, Ny))
     ref = O.fd3d_solve(f, gb, gf, Lx=1.0, Ly=2.0, Lz=1.5, lam=1.0, bc=bc)
     p = Helmholtz3DFD(Nx, Ny, Nz, 0.0, 1.0, 0.0, 2.0, 0.0, 1.5, Lambda=1.0, bc=bc, precision=precision)
+    p.set_launch_variants(p.launch_variants()["fft"], rows)
     u = p.SolvePDE(_dev(f), _dev(gb), _dev(gf)).cpu().numpy()
     if precision == "fp64":
         assert max_rel(u, ref) < 1e-12
@@ -90,7 +95,8 @@ def test_fd_robin_residual_midsize(cuda):
 
 
 @pytest.mark.parametrize("bc", [(0.0, 1.0, 0.0, 1.0), (1.0, 0.5, 0.7, 2.0)])
-def test_fd_adjoint_dense(cuda, bc):
+@pytest.mark.parametrize("rows", [0, 1])
+def test_fd_adjoint_dense(cuda, bc, rows):
     Nx, Ny, Nz, lam = 8, 4, 5, 2.0
     nf, nb = Nx * Ny * Nz, Nx * Ny
     cols = []
@@ -108,6 +114,7 @@ def test_fd_adjoint_dense(cuda, bc):
     ubar = np.random.default_rng(9).standard_normal((Nx, Ny, Nz))
     g = S.T @ ubar.ravel()
     p = Helmholtz3DFD(Nx, Ny, Nz, 0.0, 1.0, 0.0, 1.3, 0.0, 0.8, Lambda=lam, bc=bc)
+    p.set_launch_variants(p.launch_variants()["fft"], rows)
     fbar, _, glb, grb = p.SolveAdjoint(_dev(ubar), want_bc=True)
     assert rel_l2(fbar.cpu().numpy().ravel(), g[:nf]) < 1e-10
     assert rel_l2(glb.cpu().numpy().ravel(), g[nf:nf + nb]) < 1e-10
