@@ -283,7 +283,8 @@ int helm_plan_device_status(helm_plan_t plan, int* code, int reset);
  * (lengths 128, 256), bit 2: persistent pipelined pass, bit 3: 512-thread CTAs
  * for passes of length 512 or 1024 (ignored for shorter ones; with bit 2 the
  * tile exceeds shared memory and the solve fails with HELM_ERR_CUDA) -- and rows (0..4) for
- * the row solve: 0, 1 the two kernel shapes of the plan's precision; 2 (FP64 and
+ * the row solve: 0, 1 the two kernel shapes of the plan's precision (finite-
+ * difference plans: a tridiagonal row per warp, or per half-warp when Nz <= 256); 2 (FP64 and
  * refined 3D plans with one element, at most 65 GLL points and Ny in {64, 128,
  * 256}) the y pass, the row solve and the inverse y pass fused into one kernel
  * per kx slab, the two y entries of fft4 then unused; 3 (refined plans with one
