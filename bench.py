@@ -53,7 +53,8 @@ def _args():
     ap.add_argument("--impl", choices=("ours", "reference"), default="ours")
     ap.add_argument("--skip-cpu-baseline", action="store_true", help="omit the CPU leg (profiling runs)")
     ap.add_argument("--skip-side", action="store_true", help="omit the batch / adjoint / finite-difference / periodic / derivative legs")
-    ap.add_argument("--profile-case", choices=("fp64", "fp32_refine", "fp32", "fd64", "fd32", "fd32x", "batch", "deriv"),
+    ap.add_argument("--profile-case", choices=("fp64", "fp32_refine", "fp32", "fd64", "fd64h", "fd32", "fd32x", "batch",
+                                               "deriv"),
                     help="run three untimed solves of one workload and exit (a small case for ncu captures)")
     return ap.parse_args()
 
@@ -61,14 +62,15 @@ def _args():
 def profile_case(which: str):
     """Plan creation (with its autotuning), then three solves: the headline
     256 x 256 x 65 workload at one precision, a 256 x 256 x 256 finite-difference
-    solve, or the 512-problem batch; or ("deriv") three rounds of the z, x and y
-    derivatives of a 512 x 256 x 65 FP64 field."""
+    solve (fd64: a tridiagonal row per warp; fd64h: per half-warp), or the
+    512-problem batch; or ("deriv") three rounds of the z, x and y derivatives of
+    a 512 x 256 x 65 FP64 field."""
     import torch
 
     from mpi_b200 import workloads as W
 
     torch.cuda.set_device(0)
-    if which in ("fd64", "fd32", "fd32x"):
+    if which in ("fd64", "fd64h", "fd32", "fd32x"):
         from mpi_b200 import Helmholtz3DFD
 
         # fd32x: the length-1024 x passes of the FD workload on a 1024 x 512 x 64
@@ -76,7 +78,9 @@ def profile_case(which: str):
         nx, ny, nz = (1024, 512, 64) if which == "fd32x" else (256, 256, 256)
         f = torch.from_numpy(W.smooth_field_fd(nx, ny, nz, seed=1239)).cuda()
         p = Helmholtz3DFD(nx, ny, nz, 0.0, 1.0, 0.0, 1.0, 0.0, 1.0, Lambda=1.0,
-                          precision="fp64" if which == "fd64" else "fp32")
+                          precision="fp64" if which in ("fd64", "fd64h") else "fp32")
+        # fd64h: the tridiagonal solves pinned to a row per half-warp (row variant 1)
+        p.set_launch_variants(p.launch_variants()["fft"], 1 if which == "fd64h" else 0)
         if which == "fd32x":
             p.set_io_bytes(4)
             f = f.float()
