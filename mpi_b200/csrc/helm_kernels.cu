@@ -1567,7 +1567,7 @@ __device__ __forceinline__ void tri_issue_row(const ThomasArgs& a, long long r, 
 // M per row, cyclic reduction over 16-lane segments: one step and half the
 // shuffles fewer per row than LPR = 32).
 template <typename T, int M, int LPR = 32>
-__global__ void __launch_bounds__(TRI_WARPS * 32, (M <= 8 ? 4 : 2)) thomas_warp_kernel(ThomasArgs a)
+__global__ void __launch_bounds__(TRI_WARPS * 32, (M <= 8 ? 4 : (sizeof(T) == 8 ? 2 : 3))) thomas_warp_kernel(ThomasArgs a)
 {
     pdl_enter();
     using C = cplx_t<T>;
@@ -1599,9 +1599,9 @@ __global__ void __launch_bounds__(TRI_WARPS * 32, (M <= 8 ? 4 : 2)) thomas_warp_
         const long long r = min(r0 + hrow, a.nrows - 1);  // rows past the end solve zeros, unstored
         const int kx = (int)(r / a.Ny), ky = (int)(r - (long long)kx * a.Ny);
         const double dg = -2.0 * a.cz1 - a.lambda - a.mx[kx] - a.my[ky];
-        C dv[M];
-#pragma unroll
-        for (int i = 0; i < M; ++i) dv[i] = sb[li * (M + 1) + i];
+        // the lane's chunk is read from the staging buffer where it is used
+        // (no register copy: registers for the elimination's arrays)
+        const C* dv = sb + li * (M + 1);
         // row k: sub (k >= 1), diagonal, super (k <= Nz - 2); transposed, the sub of
         // row k is the super of row k - 1 and the super of row k the sub of row k + 1.
         // Rows k >= Nz are identity rows.
