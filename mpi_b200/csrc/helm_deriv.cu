@@ -494,7 +494,15 @@ static int run_gll_deriv_bulk(const GllDerivArgs& a, cudaStream_t s)
 {
     const GdMmaLayout L = gd_mma_layout(a.P);
     const size_t tile_bytes = (size_t)GB_ROWS * a.P * sizeof(double);
-    int stages = (int)((kMaxSmemPerBlock - L.b_bytes - 64) / (tile_bytes + sizeof(uint64_t)));
+    // two CTAs per SM (16 warps) with two tiles in flight each where they fit,
+    // else one CTA with up to five
+    constexpr size_t kPerSm = 233472;  // shared memory of an SM, 1 KB of it reserved per CTA
+    int per_sm = 2;
+    int stages = (int)(((kPerSm / 2 - 1024) - L.b_bytes - 64) / (tile_bytes + sizeof(uint64_t)));
+    if (stages < 2) {
+        per_sm = 1;
+        stages = (int)((kMaxSmemPerBlock - L.b_bytes - 64) / (tile_bytes + sizeof(uint64_t)));
+    }
     if (stages > 5) stages = 5;
     if (stages < 2) return -1;  // not this kernel
     const size_t smem = L.b_bytes + (size_t)stages * (tile_bytes + sizeof(uint64_t));
@@ -505,7 +513,7 @@ static int run_gll_deriv_bulk(const GllDerivArgs& a, cudaStream_t s)
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     const long long tiles = (a.nrows + GB_ROWS - 1) / GB_ROWS;
-    const long long grid = tiles < sms ? tiles : sms;
+    const long long grid = tiles < (long long)sms * per_sm ? tiles : (long long)sms * per_sm;
     if (grid < 1) return 0;
     return (int)launch_k(k, dim3((unsigned)grid), dim3(GB_WARPS * 32), smem, s, a, L, stages);
 }
