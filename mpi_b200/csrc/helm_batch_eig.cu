@@ -8,17 +8,17 @@
 // problem): u_int = V (x-FFT^-1 diag(1/(mu_j - sigma(kx))) x-FFT) V^-1 f_int,
 // with V, V^-1 the folded transforms of helm_fdm.cu.  The work is cut into
 // three kinds of items that persistent CTAs take from one ordered queue:
-//   1. (problem, 64 x rows): fold and first transform of f's rows on the FP64
-//      tensor cores -> the problem's coefficient rows C[x][2 ld] (scratch);
+//   1. (problem, 4096 / ld x rows): fold and first transform of f's rows on the
+//      FP64 tensor cores -> the problem's coefficient rows C[x][2 ld] (scratch);
 //   2. (problem, up to 16 coefficient column pairs): x FFT, scaling by
 //      1 / ((mu_j - sigma) Nx), inverse x FFT, in place in C;
-//   3. (problem, 64 x rows): second transform, unfold -> u rows.
+//   3. (problem, 4096 / ld x rows): second transform, unfold -> u rows.
 // A kind-2 item waits until every kind-1 item of its problem is done, a kind-3
 // item until every kind-2 item is (per-problem counters, bounded waits).  The
 // queue holds every kind-1 item before any kind-2 item before any kind-3 item,
 // so a CTA only waits for items that running CTAs have already taken: the
 // launch needs no co-residency guarantee.  Big problems spread over many CTAs
-// (a 512 x 129 problem is 8 + 16 + 8 items), small ones cost one item each.
+// (a 512 x 129 problem is 8 + 8 + 8 items), small ones cost one item each.
 // The coefficient scratch (sum of Nx * 2 ld doubles) mostly stays in L2.
 #include <cuda_runtime.h>
 
@@ -43,7 +43,11 @@ namespace {
 
 constexpr int BE_THREADS = 256;   // 8 warps; two or three CTAs share an SM
 constexpr int BE_MINB = 2;        // resident CTAs per SM the kernel is built for
-constexpr int BE_ROWS = 64;       // x rows of a kind-1 / kind-3 item (one 8-row tile per warp)
+// x rows of a kind-1 / kind-3 item of a class with ld slots: 4096 / ld (512 for
+// ld = 8 down to 64 for ld = 64), so that each warp runs eight 8-row m-tiles of
+// one n-tile in every class (the same work and registers as ld = 64)
+__host__ __device__ constexpr int be_item_rows(int ld) { return 4096 / ld; }
+constexpr int BE_MTW = 8;         // m-tiles per warp in a row item
 
 // Complex columns of a kind-2 item: as many as the CTA's FFT transforms in
 // one round (256 threads over nx / r0 threads per column, r0 the first radix
@@ -102,13 +106,13 @@ __device__ __forceinline__ int ld_acquire(const int* p)
 
 // Kind 1: rows x0 .. x0+R-1 of problem pr -> coefficient rows.  The rows
 // are staged once for the CTA; warp w then owns n-tile w % NT of both folds
-// over NT consecutive 8-row m-tiles (all eight when NT = 8), so each B
-// fragment it loads feeds NT products of each fold.
+// over eight consecutive 8-row m-tiles, so each B fragment it loads feeds
+// eight products of each fold.
 template <int LD>
 __device__ void be_rows_in(const BeArgs& a, const BeProblem& pr, const BeClass& c, int idx, double* sm)
 {
-    constexpr int NT = LD / 8, KK = LD / 4;
-    const int R = pr.nx < BE_ROWS ? pr.nx : BE_ROWS, x0 = idx * BE_ROWS, P = c.P, pitch = c.pitch;
+    constexpr int NT = LD / 8, KK = LD / 4, IR = be_item_rows(LD);
+    const int R = pr.nx < IR ? pr.nx : IR, x0 = idx * IR, P = c.P, pitch = c.pitch;
     double* st = sm;  // [R][pitch]; the boundary slots stay zero (homogeneous Dirichlet)
     const double* f = a.f + pr.off + (long long)x0 * P;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, g = lane >> 2, q = lane & 3;
@@ -154,19 +158,19 @@ __device__ void be_rows_in(const BeArgs& a, const BeProblem& pr, const BeClass& 
         }
     }
     __syncthreads();
-    const int nt = warp % NT, mt0 = (warp / NT) * NT;
+    const int nt = warp % NT, mt0 = (warp / NT) * BE_MTW;
     if (mt0 * 8 >= R) return;
-    const int nmt = min(NT, R / 8 - mt0);  // live m-tiles of this warp
-    double cs[NT][2], ca[NT][2];
+    const int nmt = min(BE_MTW, R / 8 - mt0);  // live m-tiles of this warp
+    double cs[BE_MTW][2], ca[BE_MTW][2];
 #pragma unroll
-    for (int t = 0; t < NT; ++t) cs[t][0] = cs[t][1] = ca[t][0] = ca[t][1] = 0.0;
+    for (int t = 0; t < BE_MTW; ++t) cs[t][0] = cs[t][1] = ca[t][0] = ca[t][1] = 0.0;
     const double* Bs = c.first + (size_t)nt * KK * 32 + lane;
     const double* Ba = c.first + (size_t)(NT + nt) * KK * 32 + lane;
 #pragma unroll 4
     for (int kk = 0; kk < KK; ++kk) {
         const double bs = __ldg(Bs + kk * 32), ba = __ldg(Ba + kk * 32);
 #pragma unroll
-        for (int t = 0; t < NT; ++t) {
+        for (int t = 0; t < BE_MTW; ++t) {
             if (t < nmt) {
                 const double* row = st + ((mt0 + t) * 8 + g) * pitch;
                 dmma_8x8x4(cs[t][0], cs[t][1], row[4 * kk + q], bs);
@@ -175,7 +179,7 @@ __device__ void be_rows_in(const BeArgs& a, const BeProblem& pr, const BeClass& 
         }
     }
 #pragma unroll
-    for (int t = 0; t < NT; ++t) {
+    for (int t = 0; t < BE_MTW; ++t) {
         if (t < nmt) {
             double* crow = a.C + pr.coff + (long long)(x0 + (mt0 + t) * 8 + g) * 2 * LD;
             *reinterpret_cast<double2*>(crow + nt * 8 + 2 * q) = make_double2(cs[t][0], cs[t][1]);
@@ -242,13 +246,13 @@ __device__ void be_columns(const BeArgs& a, const BeProblem& pr, const BeClass& 
 
 // Kind 3: coefficient rows x0 .. x0+R-1 -> second transform, unfold -> u rows.
 // The coefficient rows are staged once for the CTA; warp w owns n-tile w % NT
-// of both folds over NT m-tiles (as kind 1), and after every warp has read the
+// of both folds over eight m-tiles (as kind 1), and after every warp has read the
 // rows its results overwrite them, ready for the unfold.
 template <int LD>
 __device__ void be_rows_out(const BeArgs& a, const BeProblem& pr, const BeClass& c, int idx, double* sm)
 {
-    constexpr int NT = LD / 8, KK = LD / 4, PITCH = 2 * LD + 4;
-    const int R = pr.nx < BE_ROWS ? pr.nx : BE_ROWS, x0 = idx * BE_ROWS, P = c.P;
+    constexpr int NT = LD / 8, KK = LD / 4, PITCH = 2 * LD + 4, IR = be_item_rows(LD);
+    const int R = pr.nx < IR ? pr.nx : IR, x0 = idx * IR, P = c.P;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, g = lane >> 2, q = lane & 3;
     double* rows = sm;  // [R][PITCH]: coefficients (s | d), then the transformed values
     const double* Cb = a.C + pr.coff + (long long)x0 * 2 * LD;
@@ -259,18 +263,18 @@ __device__ void be_rows_out(const BeArgs& a, const BeProblem& pr, const BeClass&
     cp_async_commit();
     cp_async_wait_all();
     __syncthreads();
-    const int nt = warp % NT, mt0 = (warp / NT) * NT;
-    const int nmt = mt0 * 8 >= R ? 0 : min(NT, R / 8 - mt0);
-    double vs[NT][2], vd[NT][2];
+    const int nt = warp % NT, mt0 = (warp / NT) * BE_MTW;
+    const int nmt = mt0 * 8 >= R ? 0 : min(BE_MTW, R / 8 - mt0);
+    double vs[BE_MTW][2], vd[BE_MTW][2];
 #pragma unroll
-    for (int t = 0; t < NT; ++t) vs[t][0] = vs[t][1] = vd[t][0] = vd[t][1] = 0.0;
+    for (int t = 0; t < BE_MTW; ++t) vs[t][0] = vs[t][1] = vd[t][0] = vd[t][1] = 0.0;
     const double* Bs = c.second + (size_t)nt * KK * 32 + lane;
     const double* Bd = c.second + (size_t)(NT + nt) * KK * 32 + lane;
 #pragma unroll 4
     for (int kk = 0; kk < KK; ++kk) {
         const double bs = __ldg(Bs + kk * 32), bd = __ldg(Bd + kk * 32);
 #pragma unroll
-        for (int t = 0; t < NT; ++t) {
+        for (int t = 0; t < BE_MTW; ++t) {
             if (t < nmt) {
                 const double* row = rows + ((mt0 + t) * 8 + g) * PITCH;
                 dmma_8x8x4(vs[t][0], vs[t][1], row[4 * kk + q], bs);
@@ -280,7 +284,7 @@ __device__ void be_rows_out(const BeArgs& a, const BeProblem& pr, const BeClass&
     }
     __syncthreads();  // every warp has read the coefficients
 #pragma unroll
-    for (int t = 0; t < NT; ++t) {
+    for (int t = 0; t < BE_MTW; ++t) {
         if (t < nmt) {
             double* row = rows + ((mt0 + t) * 8 + g) * PITCH;
             *reinterpret_cast<double2*>(row + nt * 8 + 2 * q) = make_double2(vs[t][0], vs[t][1]);
@@ -523,10 +527,10 @@ int batch_eig_create(int nprob, const int* Nx, const int* N, const double* lambd
         p.lam = lambda[i];
         p.nx = Nx[i];
         p.cls = ci;
-        p.nchunk = (Nx[i] + BE_ROWS - 1) / BE_ROWS;
+        p.nchunk = (Nx[i] + be_item_rows(c.ld) - 1) / be_item_rows(c.ld);
         p.ngroup = c.ld / be_cols(Nx[i], c.ld);
         coff += (long long)Nx[i] * 2 * c.ld;
-        const int R = std::min(Nx[i], BE_ROWS);
+        const int R = std::min(Nx[i], be_item_rows(c.ld));
         smem = std::max(smem, (size_t)R * c.pitch * sizeof(double));
         smem = std::max(smem, (size_t)R * (2 * c.ld + 4) * sizeof(double));
         smem = std::max(smem, (size_t)Nx[i] * (be_cols(Nx[i], c.ld) + 1) * sizeof(double2));
