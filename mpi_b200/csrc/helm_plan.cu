@@ -740,7 +740,13 @@ static int fft_pass(Plan& p, int L, int mode, int dir, const void* in, void* out
     if (po && stage == 0 && po->io_in) io = po->io_in;
     if (po && stage == 3 && po->io_out) io = po->io_out;
     const int kmode = a.adj_mode ? (int)FFT_C2R_ADJ : mode;
-    int e = launch_fft(L, kmode, dir, td, io, a, ccols * nbatch, s, sub ? (p.fft_var[stage] & ~4) : p.fft_var[stage]);
+    // Spectral derivatives take their own launch shape: the solve's variant of
+    // the same stage is tuned for another kernel (on eigen-basis plans the
+    // stage-1 bits select the y-convolution pass).  Radix-8 schedule with
+    // 256-thread CTAs up to length 256 (at 256^2 x 65 FP64: d/dx 33.7 us
+    // against 41.9-44.0 for the radix-16 shapes), 512-thread CTAs above.
+    const int var = mode == FFT_DERIV ? (L >= 512 ? 8 : 2) : sub ? (p.fft_var[stage] & ~4) : p.fft_var[stage];
+    int e = launch_fft(L, kmode, dir, td, io, a, ccols * nbatch, s, var);
     if (e) return set_cuda_error((cudaError_t)e, "fft launch");
     return HELM_OK;
 }
