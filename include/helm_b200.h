@@ -305,6 +305,17 @@ int helm_plan_device_status(helm_plan_t plan, int* code, int reset);
 int helm_plan_get_launch_variants(helm_plan_t plan, int* fft4, int* rows);
 int helm_plan_set_launch_variants(helm_plan_t plan, const int* fft4, int rows);
 
+/* Launch variant of the spectral derivative passes (helm_fourier_derivative),
+ * with the bits of the FFT variants above (bit 2: the persistent pipelined
+ * kernel).  -1, the default, picks by transform length and precision:
+ * 512-thread CTAs from length 512; below, the radix-8 schedule, pipelined for
+ * FP32 plans.  Pipelined shapes whose tile buffers exceed shared memory are
+ * refused with HELM_ERR_CUDA and launch nothing.  Every
+ * variant computes the same derivative up to the last bits.  No counterpart in
+ * the reference, which has one code path. */
+int helm_plan_set_derivative_variant(helm_plan_t plan, int variant);
+int helm_plan_get_derivative_variant(helm_plan_t plan, int* variant);
+
 /* The kernels a forward helm_solve of the plan launches, as a short
  * space-separated list of kernel names in launch order (for reports: which
  * row kernel ran, e.g. whether a refined plan ran its FP32 tensor-core kernel or

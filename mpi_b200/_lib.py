@@ -40,6 +40,7 @@ EXPORTS = (
     "helm_write_tecplot", "helm_write_vtk", "helm_solve_adjoint_misfit", "helm_solve_static_scratch",
     "helm_plan_kernels", "helm_debug_fail_alloc", "helm_plan_device_status", "helm_plan_set_operator_callback",
     "helm_gll_grid", "helm_lu_factor", "helm_lu_solve", "helm_max_abs_diff", "helm_batch_device_status",
+    "helm_plan_set_derivative_variant", "helm_plan_get_derivative_variant",
 )
 
 # operator callback of helm_plan_set_operator_callback: void op(int iw, int jw, double* op, int ld, void* user)
@@ -112,6 +113,8 @@ def lib() -> ctypes.CDLL:
     L.helm_batch_destroy.argtypes = [vp]
     L.helm_plan_get_launch_variants.argtypes = [vp, P(i), P(i)]
     L.helm_plan_set_launch_variants.argtypes = [vp, P(i), i]
+    L.helm_plan_set_derivative_variant.argtypes = [vp, i]
+    L.helm_plan_get_derivative_variant.argtypes = [vp, P(i)]
     L.helm_status_string.argtypes = [i]
     L.helm_status_string.restype = ctypes.c_char_p
     L.helm_last_error.argtypes = []

@@ -465,7 +465,7 @@ __device__ __forceinline__ void pipe_issue(const FftArgs& a, long long total_col
             const long long row = tc + r * TPC;
             cp_async_elem<sizeof(C)>(&st[row * CT + cl], valid ? &in[row * a.in_row + c] : a.in, valid);
         }
-    } else if constexpr (MODE == FFT_R2C) {
+    } else if constexpr (MODE == FFT_R2C || MODE == FFT_DERIV) {
         const TIO* in = static_cast<const TIO*>(a.in) + in_base;
         TIO* st = reinterpret_cast<TIO*>(stage);
         const int c0 = 2 * c, c1 = 2 * c + 1;
@@ -557,7 +557,7 @@ __global__ void __launch_bounds__(THREADS) fft_pipe_kernel(FftArgs a, long long 
 #pragma unroll
             for (int r = 0; r < R0; ++r) v[r] = sm[(tc + r * TPC) * CT + cl];
             __syncthreads();
-        } else if constexpr (MODE == FFT_R2C) {
+        } else if constexpr (MODE == FFT_R2C || MODE == FFT_DERIV) {
             const TIO* st = reinterpret_cast<const TIO*>(buf);
             int k0 = -1, k1 = -1, j0 = 0, j1 = 0;
             if (a.P > 0) { k0 = c0 % a.P; j0 = c0 / a.P; k1 = c1 % a.P; j1 = c1 / a.P; }
@@ -616,7 +616,33 @@ __global__ void __launch_bounds__(THREADS) fft_pipe_kernel(FftArgs a, long long 
 
         // ------------------------------------------------------ output --
         const T sc = (T)a.scale;
-        if constexpr (MODE == FFT_C2C) {
+        if constexpr (MODE == FFT_DERIV) {
+            // multiplier in registers, natural row order through the tile's
+            // buffer, inverse transform, the two real output columns
+#pragma unroll
+            for (int t = 0; t < R0 / RL; ++t)
+#pragma unroll
+                for (int r = 0; r < RL; ++r)
+                    v[t * RL + r] = deriv_mul_packed<T, L>(a.deriv_order, a.deriv_w,
+                                                           pass_out_row<RL, NSL, TPC>(tc, t, r), v[t * RL + r]);
+            __syncthreads();
+            pass_to_smem<T, L, RL, NSL, TPC, CT, R0>(sm, tc, cl, v);
+            __syncthreads();
+#pragma unroll
+            for (int r = 0; r < R0; ++r) v[r] = sm[(tc + r * TPC) * CT + cl];
+            fft_reg_passes<T, L, 1, TPC, CT, R0, R1, R2, NP>(sm, tw, tc, cl, v);
+            if (valid) {
+                TIO* out = static_cast<TIO*>(a.out) + out_base;
+#pragma unroll
+                for (int t = 0; t < R0 / RL; ++t)
+#pragma unroll
+                    for (int r = 0; r < RL; ++r) {
+                        const long long row = pass_out_row<RL, NSL, TPC>(tc, t, r);
+                        out[row * a.out_row + c0] = (TIO)(v[t * RL + r].x * sc);
+                        if (has1) out[row * a.out_row + c1] = (TIO)(v[t * RL + r].y * sc);
+                    }
+            }
+        } else if constexpr (MODE == FFT_C2C) {
             if (valid) {
                 C* out = static_cast<C*>(a.out) + out_base;
 #pragma unroll
@@ -689,7 +715,8 @@ static int run_fft(const FftArgs& a, long long total_cols, cudaStream_t s)
 template <typename T, typename TIO, int L, int THREADS, int SMALL>
 static int fft_dispatch_mode(int mode, int dir, const FftArgs& a, long long tc, cudaStream_t s, bool pipe)
 {
-    if (pipe && mode != FFT_DERIV) {
+    if (pipe) {
+        if (mode == FFT_DERIV) return run_fft_pipe<T, TIO, L, -1, FFT_DERIV, THREADS, SMALL>(a, tc, s);
         if (mode == FFT_C2C)
             return dir < 0 ? run_fft_pipe<T, T, L, -1, FFT_C2C, THREADS, SMALL>(a, tc, s)
                            : run_fft_pipe<T, T, L, 1, FFT_C2C, THREADS, SMALL>(a, tc, s);

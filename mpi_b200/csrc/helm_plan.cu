@@ -742,10 +742,13 @@ static int fft_pass(Plan& p, int L, int mode, int dir, const void* in, void* out
     const int kmode = a.adj_mode ? (int)FFT_C2R_ADJ : mode;
     // Spectral derivatives take their own launch shape: the solve's variant of
     // the same stage is tuned for another kernel (on eigen-basis plans the
-    // stage-1 bits select the y-convolution pass).  Radix-8 schedule with
-    // 256-thread CTAs up to length 256 (at 256^2 x 65 FP64: d/dx 33.7 us
-    // against 41.9-44.0 for the radix-16 shapes), 512-thread CTAs above.
-    const int var = mode == FFT_DERIV ? (L >= 512 ? 8 : 2) : sub ? (p.fft_var[stage] & ~4) : p.fft_var[stage];
+    // stage-1 bits select the y-convolution pass).  Unless pinned: 512-thread
+    // CTAs from length 512; below, the radix-8 schedule, in the persistent
+    // pipelined kernel for FP32 transforms.  Measured at 256^2 x 65 (FP64 I/O):
+    // FP64 d/dx 33.8 us (radix-16 shapes 44.0, pipelined 37.9), FP32 31.7 us
+    // (plain 33.8); at 512^2 x 33 FP64 d/dx 62.4 us (256 threads 76.7).
+    const int dvar = p.deriv_var >= 0 ? p.deriv_var : (L >= 512 ? 8 : td ? 2 : 6);
+    const int var = mode == FFT_DERIV ? dvar : sub ? (p.fft_var[stage] & ~4) : p.fft_var[stage];
     int e = launch_fft(L, kmode, dir, td, io, a, ccols * nbatch, s, var);
     if (e) return set_cuda_error((cudaError_t)e, "fft launch");
     return HELM_OK;
@@ -1717,6 +1720,20 @@ int helm_plan_set_launch_variants(helm_plan_t plan, const int* fft4, int rows)
     }
     for (int i = 0; i < 4; ++i) p.fft_var[i] = fft4[i];
     p.row_var = rows;
+    return HELM_OK;
+}
+
+int helm_plan_set_derivative_variant(helm_plan_t plan, int variant)
+{
+    if (!plan || variant < -1 || variant > 15) return HELM_ERR_INVALID;
+    reinterpret_cast<Plan*>(plan)->deriv_var = variant;
+    return HELM_OK;
+}
+
+int helm_plan_get_derivative_variant(helm_plan_t plan, int* variant)
+{
+    if (!plan || !variant) return HELM_ERR_INVALID;
+    *variant = reinterpret_cast<Plan*>(plan)->deriv_var;
     return HELM_OK;
 }
 

@@ -108,6 +108,8 @@ struct Plan {
     size_t refine_bytes = 0;
     // autotuned launch shapes of the four FFT stages (x, y, inverse y, inverse x)
     int fft_var[4] = {0, 0, 0, 0};
+    // launch variant of the spectral derivative passes (-1: chosen by length)
+    int deriv_var = -1;
     // row-solve variant: 0, 1 launch shapes of the plan precision's folded kernel;
     // 2 fused y-FFT / rows / inverse y (slab, FP64 arithmetic); 3 refined plans:
     // the FP64 tensor-core row kernel; 4 the eigen-basis pipeline (whole solve)

@@ -267,6 +267,17 @@ class _PlanBase:
         f4 = (ctypes.c_int * 4)(*fft)
         L.check(self._lib.helm_plan_set_launch_variants(self._plan, f4, int(rows)), "helm_plan_set_launch_variants")
 
+    def derivative_variant(self) -> int:
+        """Launch variant of the spectral derivatives (-1: chosen by length)."""
+        v = ctypes.c_int()
+        L.check(self._lib.helm_plan_get_derivative_variant(self._plan, ctypes.byref(v)),
+                "helm_plan_get_derivative_variant")
+        return v.value
+
+    def set_derivative_variant(self, variant: int) -> None:
+        L.check(self._lib.helm_plan_set_derivative_variant(self._plan, int(variant)),
+                "helm_plan_set_derivative_variant")
+
     def device_status(self, reset: bool = True) -> int:
         """0, or the code of a tile-copy wait of the TMA-pipelined kernels that ran
         out of its iteration limit (waits for the device)."""

@@ -134,3 +134,38 @@ def test_derivatives_in_the_reference_array_layout(cuda):
         D = od.cpu().numpy()
         assert max_rel(D[:, :Nx, :Ny], ref) < 1e-12
         assert np.all(D[:, Nx:] == 5.0) and np.all(D[:, :, Ny:] == 5.0)
+
+
+@pytest.mark.parametrize("Nx,Ny,N,prec", [(256, 64, 33, "fp64"), (1024, 8, 9, "fp64"), (32, 512, 5, "fp64"),
+                                          (4, 16, 7, "fp64"), (256, 32, 17, "fp32"), (1024, 4, 9, "fp32")])
+def test_fourier_derivative_every_launch_variant(cuda, Nx, Ny, N, prec):
+    """Every launch shape of the spectral derivative (plain and persistent
+    pipelined kernels, 128/256/512/1024-thread CTAs, radix-8 and radix-16
+    schedules) against the oracle, with odd column counts (a lone last column)
+    and, at 256 x 64 x 33, more tiles than the persistent grid has CTAs.
+    Pipelined shapes whose two tile buffers exceed shared memory are refused
+    with an error, not run."""
+    from mpi_b200._lib import HelmError
+    rng = np.random.default_rng(Nx * 7 + Ny + N)
+    Lx, Ly = 2 * math.pi, 1.5
+    u = rng.standard_normal((Nx, Ny, N))
+    p = NonPeriodic3D(Nx, Ny, N, N, 0.0, Lx, 0.0, Ly, 0.0, 2.0, Lambda=1.0, precision=prec)
+    fp32 = prec == "fp32"
+    if fp32:
+        p.set_io_bytes(4)
+    ud = _dev(u, torch.float32 if fp32 else torch.float64)
+    refs = {(a, o): O.fourier_deriv(u, axis=a, order=o, L=(Lx, Ly)[a]) for a in (0, 1) for o in (1, 2)}
+    assert p.derivative_variant() == -1
+    for v in [-1] + list(range(16)):
+        p.set_derivative_variant(v)
+        for (axis, order), ref in refs.items():
+            L_ax = (Nx, Ny)[axis]
+            try:
+                d = p._derivative(axis, order, ud, None, None).double().cpu().numpy()
+            except HelmError:
+                assert v & 4 and L_ax >= 512, f"variant {v} refused on length {L_ax}"
+                continue
+            err = rel_l2(d, ref) if fp32 else max_rel(d, ref)
+            assert err < (1e-5 if fp32 else 1e-12), f"variant {v}, axis {axis}, order {order}: {err:.3e}"
+    with pytest.raises(HelmError):
+        p.set_derivative_variant(16)
