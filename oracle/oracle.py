@@ -11,6 +11,10 @@ Two libraries, both built by ``oracle/Makefile``:
   ``ref_driver2d.cpp`` / ``ref_driver3d.cpp`` / ``ref_driver2dp.cpp`` /
   ``ref_driver3dp.cpp``.  Present only where the reference tree was available
   at build time; :func:`have_reference` says whether they were built.
+* ``_ref/libreffd3d.so`` -- the reference's HypreFDM 3D solver
+  (``Helmholtz3D_MPI.cpp``) compiled unchanged against an in-memory HYPRE IJ
+  stub, its assembled system solved directly (``ref_driver_fd3d.cpp``);
+  :func:`have_reference_fd`.
 
 Only ``tests/``, ``__graft_entry__.smoke`` and the CPU-baseline leg of
 ``bench.py`` may import this module, and only as the checker.
@@ -272,6 +276,34 @@ def ref_solve3d(f, gl, gr, *, xl, xr, yl, yr, zl, zr, lam, bc=(0.0, 1.0, 0.0, 1.
         raise RuntimeError(f"reference chose Ns={ns}, expected {Ns}")
     out = u[0] if squeeze else u
     return (out, ms[0]) if return_time else out
+
+
+_reffd = None
+
+
+def have_reference_fd() -> bool:
+    return os.path.exists(os.path.join(_HERE, "_ref", "libreffd3d.so"))
+
+
+def ref_fd3d_solve(f, gb, gf, *, Lx, Ly, Lz, lam, bc=(0.0, 1.0, 0.0, 1.0)):
+    """The reference's own HypreFDM 3D solver (Helmholtz3D_MPI.cpp SetA / Setb
+    assembly, x and y periodic, Robin ends in z) with the assembled system
+    solved directly.  f: [Nx, Ny, Nz] interior points; gb, gf: [Nx, Ny] Robin
+    data at z = 0 and z = Lz; bc = (alpha_back, beta_back, alpha_front,
+    beta_front).  Returns the interior solution [Nx, Ny, Nz]."""
+    global _reffd
+    if _reffd is None:
+        _reffd = ctypes.CDLL(os.path.join(_HERE, "_ref", "libreffd3d.so"))
+        _reffd.oracle_ref_fd3d_solve.restype = _I
+        _reffd.oracle_ref_fd3d_solve.argtypes = [_I] * 3 + [_D] * 11 + [_P] * 4
+    f = _c64(f)
+    Nx, Ny, Nz = f.shape
+    u = np.zeros_like(f)
+    st = _reffd.oracle_ref_fd3d_solve(Nx, Ny, Nz, 0.0, Lx, 0.0, Ly, 0.0, Lz, *bc, lam,
+                                      _p(f), _p(_c64(gb)), _p(_c64(gf)), _p(u))
+    if st:
+        raise RuntimeError(f"oracle_ref_fd3d_solve status {st}")
+    return u
 
 
 def ref_set_cdiag(dim: int, c=None):

@@ -1,5 +1,5 @@
 /* Single-rank stand-in for <mpi.h>, used only to compile the reference's
- * DirectPseudoSpectral sources into the oracle library under oracle/_ref.
+ * DirectPseudoSpectral and HypreFDM sources into the oracle library under oracle/_ref.
  *
  * Test infrastructure: the product never includes this header.
  *
@@ -45,5 +45,23 @@ static inline int MPI_Send(const void*, int, MPI_Datatype, int, int, MPI_Comm) {
 static inline int MPI_Recv(void*, int, MPI_Datatype, int, int, MPI_Comm, MPI_Status*) {
     std::fprintf(stderr, "oracle stub mpi.h: MPI_Recv reached with one rank\n");
     std::abort();
+}
+/* The HypreFDM solvers: derived datatypes for their halo exchange, and
+ * non-blocking halo messages that, with one rank, are never posted (a periodic
+ * neighbour is the rank itself and is copied in place). */
+static inline int MPI_Type_indexed(int, const int*, const int*, MPI_Datatype, MPI_Datatype* t) { *t = MPI_DOUBLE; return 0; }
+static inline int MPI_Type_commit(MPI_Datatype*) { return 0; }
+static inline int MPI_Isend(const void*, int, MPI_Datatype, int, int, MPI_Comm, MPI_Request*) {
+    std::fprintf(stderr, "oracle stub mpi.h: MPI_Isend reached with one rank\n");
+    std::abort();
+}
+static inline int MPI_Irecv(void*, int, MPI_Datatype, int, int, MPI_Comm, MPI_Request*) {
+    std::fprintf(stderr, "oracle stub mpi.h: MPI_Irecv reached with one rank\n");
+    std::abort();
+}
+static inline int MPI_Wait(MPI_Request*, MPI_Status*) { return 0; }
+static inline int MPI_Abort(MPI_Comm, int code) {
+    std::fprintf(stderr, "oracle stub mpi.h: MPI_Abort(%d)\n", code);
+    std::exit(code);
 }
 #endif

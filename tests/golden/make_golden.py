@@ -1,7 +1,8 @@
 """Generate the golden vectors in tests/golden/ from the reference's own solver.
 
-Runs the reference's DirectPseudoSpectral SolvePDE (compiled from its sources by
-oracle/Makefile into oracle/_ref) on small seeded problems and stores inputs and
+Runs the reference's DirectPseudoSpectral SolvePDE and its HypreFDM 3D
+assembly (compiled from its sources by oracle/Makefile into oracle/_ref) on
+small seeded problems and stores inputs and
 outputs as compressed .npz files.  Needs the reference tree at build time; the
 committed .npz files are what the tests read.
 
@@ -132,6 +133,23 @@ def main():
     O.ref_set_cdiag(3, None)
     d.update(f3=f, gl3=gl, gr3=gr, u3=u, c3=c3, dom3=[0.0, 1.0, 0.0, 1.0, 0.0, 1.5], lam3=0.5)
     out["user_operator"] = d
+
+    # the reference's HypreFDM 3D solver (its own SetA / Setb assembly; the
+    # assembled system solved directly): x, y periodic, Robin ends in z
+    if O.have_reference_fd():
+        frng = np.random.default_rng(20241204)
+        d = {}
+        cases = [((8, 4, 6), (0.0, 1.0, 0.0, 1.0), 1.0, (1.0, 0.5, 1.5)),
+                 ((16, 8, 12), (1.0, 0.5, 0.7, 2.0), 3.0, (1.3, 0.7, 1.9)),
+                 ((4, 16, 9), (1.0, 0.3, 0.0, 1.0), 0.5, (2.0, 1.0, 0.8))]
+        for c, (shape, bc, lam, (Lx, Ly, Lz)) in enumerate(cases):
+            f = frng.standard_normal(shape)
+            gb = frng.standard_normal(shape[:2]); gf = frng.standard_normal(shape[:2])
+            u = O.ref_fd3d_solve(f, gb, gf, Lx=Lx, Ly=Ly, Lz=Lz, lam=lam, bc=bc)
+            d.update({f"f{c}": f, f"gb{c}": gb, f"gf{c}": gf, f"u{c}": u, f"bc{c}": list(bc), f"lam{c}": lam,
+                      f"L{c}": [Lx, Ly, Lz]})
+        d["ncases"] = len(cases)
+        out["fd3d_reference"] = d
 
     only = sys.argv[1:]  # optional: names of the fixtures to (re)write
     for name, d in out.items():

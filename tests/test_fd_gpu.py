@@ -1,8 +1,9 @@
 """The finite-difference FFT/Thomas variant on the GPU (the HypreFDM stencil with
-periodic x, y and Robin rows in z).  There is no reference implementation of a
-direct FD solve in the tree, so parity is against the C restatement
-(oracle/helm_oracle.c: orc_fd3d_solve, pinned by its own stencil residual) and,
-at the 1024 x 1024 x 256 size, through the stencil residual of the GPU solution
+periodic x, y and Robin rows in z).  Parity against the reference's own
+HypreFDM 3D assembly (Helmholtz3D_MPI.cpp SetA / Setb with the assembled system
+solved directly: tests/golden/fd3d_reference.npz), against the C restatement
+(oracle/helm_oracle.c: orc_fd3d_solve, itself pinned to those goldens) and, at
+the 1024 x 1024 x 256 size, through the stencil residual of the GPU solution
 itself.  Tolerances: FP64 1e-12 relative; FP32 eps_32 times the condition
 number of the worst spectrum row."""
 import math
@@ -38,6 +39,24 @@ def _stencil_residual(u, f, gb, gf, Lx, Ly, Lz, lam, bc):
     au = (cx1 * (torch.roll(u, 1, 0) + torch.roll(u, -1, 0)) + cy1 * (torch.roll(u, 1, 1) + torch.roll(u, -1, 1))
           + cz1 * (um + up) + (-2 * (cx1 + cy1 + cz1) - lam) * u)
     return ((f - au).norm() / f.norm()).item()
+
+
+@pytest.mark.parametrize("precision", ["fp64", "fp32_refine"])
+def test_fd_matches_reference_golden(cuda, precision):
+    """The GPU FD solve against the reference's own discretisation: Dirichlet,
+    Robin and mixed ends (FP64 1e-12, refined 1e-10 relative, max-norm)."""
+    from tests.helpers import golden
+    g = golden("fd3d_reference")
+    for c in range(int(g["ncases"])):
+        f = g[f"f{c}"]
+        Nx, Ny, Nz = f.shape
+        Lx, Ly, Lz = (float(v) for v in g[f"L{c}"])
+        bc = tuple(float(v) for v in g[f"bc{c}"])
+        p = Helmholtz3DFD(Nx, Ny, Nz, 0.0, Lx, 0.0, Ly, 0.0, Lz, Lambda=float(g[f"lam{c}"]), bc=bc,
+                          precision=precision)
+        u = p.SolvePDE(_dev(f), _dev(g[f"gb{c}"]), _dev(g[f"gf{c}"])).double().cpu().numpy()
+        err = max_rel(u, g[f"u{c}"])
+        assert err < (1e-12 if precision == "fp64" else 1e-10), f"case {c}: {err:.3e}"
 
 
 @pytest.mark.parametrize("rows", [0, 1])
