@@ -285,21 +285,41 @@ def have_reference_fd() -> bool:
     return os.path.exists(os.path.join(_HERE, "_ref", "libreffd3d.so"))
 
 
+def _ref_fd():
+    global _reffd
+    if _reffd is None:
+        _reffd = ctypes.CDLL(os.path.join(_HERE, "_ref", "libreffd3d.so"))
+        for fn in (_reffd.oracle_ref_fd3d_solve, _reffd.oracle_ref_fd3d_adjoint):
+            fn.restype = _I
+            fn.argtypes = [_I] * 3 + [_D] * 11 + [_P] * 4
+    return _reffd
+
+
+def ref_fd3d_adjoint(ubar, *, Lx, Ly, Lz, lam, bc=(0.0, 1.0, 0.0, 1.0)):
+    """The transpose of ref_fd3d_solve's linear map (f, gb, gf) -> u, from the
+    reference's own assembled matrix: (fbar, gbbar, gfbar) for the cotangent
+    ubar [Nx, Ny, Nz]."""
+    ubar = _c64(ubar)
+    Nx, Ny, Nz = ubar.shape
+    fbar = np.zeros_like(ubar)
+    gbb = np.zeros((Nx, Ny)); gfb = np.zeros((Nx, Ny))
+    st = _ref_fd().oracle_ref_fd3d_adjoint(Nx, Ny, Nz, 0.0, Lx, 0.0, Ly, 0.0, Lz, *bc, lam,
+                                           _p(ubar), _p(fbar), _p(gbb), _p(gfb))
+    if st:
+        raise RuntimeError(f"oracle_ref_fd3d_adjoint status {st}")
+    return fbar, gbb, gfb
+
+
 def ref_fd3d_solve(f, gb, gf, *, Lx, Ly, Lz, lam, bc=(0.0, 1.0, 0.0, 1.0)):
     """The reference's own HypreFDM 3D solver (Helmholtz3D_MPI.cpp SetA / Setb
     assembly, x and y periodic, Robin ends in z) with the assembled system
     solved directly.  f: [Nx, Ny, Nz] interior points; gb, gf: [Nx, Ny] Robin
     data at z = 0 and z = Lz; bc = (alpha_back, beta_back, alpha_front,
     beta_front).  Returns the interior solution [Nx, Ny, Nz]."""
-    global _reffd
-    if _reffd is None:
-        _reffd = ctypes.CDLL(os.path.join(_HERE, "_ref", "libreffd3d.so"))
-        _reffd.oracle_ref_fd3d_solve.restype = _I
-        _reffd.oracle_ref_fd3d_solve.argtypes = [_I] * 3 + [_D] * 11 + [_P] * 4
     f = _c64(f)
     Nx, Ny, Nz = f.shape
     u = np.zeros_like(f)
-    st = _reffd.oracle_ref_fd3d_solve(Nx, Ny, Nz, 0.0, Lx, 0.0, Ly, 0.0, Lz, *bc, lam,
+    st = _ref_fd().oracle_ref_fd3d_solve(Nx, Ny, Nz, 0.0, Lx, 0.0, Ly, 0.0, Lz, *bc, lam,
                                       _p(f), _p(_c64(gb)), _p(_c64(gf)), _p(u))
     if st:
         raise RuntimeError(f"oracle_ref_fd3d_solve status {st}")

@@ -18,14 +18,23 @@
 #include <cmath>
 #include <vector>
 
-// Dense LU with partial pivoting of the captured rows; solution into x.
+// Adjoint mode: HypreSolve solves A^T x = g_adj_rhs instead (the right-hand
+// side assembled by Setb is ignored) and leaves x in g_adj_out.
+static bool g_adjoint = false;
+static std::vector<double> g_adj_rhs, g_adj_out;
+
+// Dense LU with partial pivoting of the captured rows (of A, or of A^T in
+// adjoint mode); solution into x.
 void HypreSolve(HYPRE_ParCSRMatrix A, HYPRE_ParVector b, HYPRE_ParVector x, int& iterations, double& residual,
                 const int, const double, const int, const bool)
 {
     const int n = A->hi - A->lo + 1;
-    std::vector<double> M((size_t)n * n, 0.0), r(b->v);
+    std::vector<double> M((size_t)n * n, 0.0), r(g_adjoint ? g_adj_rhs : b->v);
     for (int i = 0; i < n; ++i)
-        for (const auto& kv : A->rows[i]) M[(size_t)i * n + (kv.first - A->lo)] = kv.second;
+        for (const auto& kv : A->rows[i]) {
+            const int j = kv.first - A->lo;
+            M[g_adjoint ? (size_t)j * n + i : (size_t)i * n + j] = kv.second;
+        }
     std::vector<int> perm(n);
     for (int i = 0; i < n; ++i) perm[i] = i;
     for (int c = 0; c < n; ++c) {
@@ -49,6 +58,7 @@ void HypreSolve(HYPRE_ParCSRMatrix A, HYPRE_ParVector b, HYPRE_ParVector x, int&
         for (int j = i + 1; j < n; ++j) s -= M[(size_t)i * n + j] * x->v[j];
         x->v[i] = s / M[(size_t)i * n + i];
     }
+    if (g_adjoint) g_adj_out = x->v;
     iterations = 0;
     residual = 0.0;
 }
@@ -84,5 +94,35 @@ extern "C" int oracle_ref_fd3d_solve(int nx, int ny, int nz, double xl_, double 
             for (int k = 0; k < nz; ++k) u[((size_t)i * ny + j) * nz + k] = V[i][j][k + 1];
     Deallocate(V, Nx + 2 * offset, Ny + 2 * offset, Nz + 2 * offset, offset, offset, offset);
     DestroyPDEPlan();
+    return 0;
+}
+
+// The transpose of the same map (f, gback, gfront) -> u: for a cotangent ubar
+// of the interior solution, fbar = (A^-T P^T ubar) at the interior rows and
+// gbback / gbfront at the Robin rows (A: the reference's assembled system,
+// P: the interior points).  Same arguments and layouts as the forward entry.
+extern "C" int oracle_ref_fd3d_adjoint(int nx, int ny, int nz, double xl_, double xr_, double yl_, double yr_,
+                                       double zl_, double zr_, double ab, double bb, double af, double bf, double lam,
+                                       const double* ubar, double* fbar, double* gbback, double* gbfront)
+{
+    const int nzr = nz + 2;
+    // global index of the reference: k Nx Ny + j Nx + i (one rank)
+    g_adj_rhs.assign((size_t)nx * ny * nzr, 0.0);
+    for (int i = 0; i < nx; ++i)
+        for (int j = 0; j < ny; ++j)
+            for (int k = 0; k < nz; ++k)
+                g_adj_rhs[(size_t)(k + 1) * nx * ny + (size_t)j * nx + i] = ubar[((size_t)i * ny + j) * nz + k];
+    std::vector<double> zf((size_t)nx * ny * nz, 0.0), zb((size_t)nx * ny, 0.0), zu((size_t)nx * ny * nz);
+    g_adjoint = true;
+    oracle_ref_fd3d_solve(nx, ny, nz, xl_, xr_, yl_, yr_, zl_, zr_, ab, bb, af, bf, lam, zf.data(), zb.data(),
+                          zb.data(), zu.data());
+    g_adjoint = false;
+    for (int i = 0; i < nx; ++i)
+        for (int j = 0; j < ny; ++j) {
+            gbback[(size_t)i * ny + j] = g_adj_out[(size_t)j * nx + i];
+            gbfront[(size_t)i * ny + j] = g_adj_out[(size_t)(nzr - 1) * nx * ny + (size_t)j * nx + i];
+            for (int k = 0; k < nz; ++k)
+                fbar[((size_t)i * ny + j) * nz + k] = g_adj_out[(size_t)(k + 1) * nx * ny + (size_t)j * nx + i];
+        }
     return 0;
 }

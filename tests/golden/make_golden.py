@@ -135,7 +135,8 @@ def main():
     out["user_operator"] = d
 
     # the reference's HypreFDM 3D solver (its own SetA / Setb assembly; the
-    # assembled system solved directly): x, y periodic, Robin ends in z
+    # assembled system solved directly, and its transpose for the adjoint):
+    # x, y periodic, Robin ends in z
     if O.have_reference_fd():
         frng = np.random.default_rng(20241204)
         d = {}
@@ -148,6 +149,12 @@ def main():
             u = O.ref_fd3d_solve(f, gb, gf, Lx=Lx, Ly=Ly, Lz=Lz, lam=lam, bc=bc)
             d.update({f"f{c}": f, f"gb{c}": gb, f"gf{c}": gf, f"u{c}": u, f"bc{c}": list(bc), f"lam{c}": lam,
                       f"L{c}": [Lx, Ly, Lz]})
+        # the transpose of each map, from the reference's own assembled matrix
+        arng = np.random.default_rng(20241205)
+        for c, (shape, bc, lam, (Lx, Ly, Lz)) in enumerate(cases):
+            ub = arng.standard_normal(shape)
+            fb, gbb, gfb = O.ref_fd3d_adjoint(ub, Lx=Lx, Ly=Ly, Lz=Lz, lam=lam, bc=bc)
+            d.update({f"ubar{c}": ub, f"fbar{c}": fb, f"gbbar{c}": gbb, f"gfbar{c}": gfb})
         d["ncases"] = len(cases)
         out["fd3d_reference"] = d
 

@@ -160,6 +160,22 @@ def test_fd_restatement_matches_reference_golden():
         assert max_rel(u, g[f"u{c}"]) < 1e-13, f"case {c}"
 
 
+def test_fd_reference_adjoint_golden_is_the_transpose_of_the_restatement():
+    """The golden FD cotangents (the transpose of the reference's own assembled
+    matrix) against the restatement's forward map: <u(f, gb, gf), ubar> =
+    <f, fbar> + <gb, gbbar> + <gf, gfbar> for random inputs."""
+    g = golden("fd3d_reference")
+    rng = np.random.default_rng(29)
+    for c in range(int(g["ncases"])):
+        shape = g[f"ubar{c}"].shape
+        for _ in range(3):
+            f = rng.standard_normal(shape); gb = rng.standard_normal(shape[:2]); gf = rng.standard_normal(shape[:2])
+            u = O.fd3d_solve(f, gb, gf, **_fd_case(g, c))
+            lhs = float((u * g[f"ubar{c}"]).sum())
+            rhs = float((f * g[f"fbar{c}"]).sum() + (gb * g[f"gbbar{c}"]).sum() + (gf * g[f"gfbar{c}"]).sum())
+            assert abs(lhs - rhs) < 1e-12 * max(1.0, abs(lhs)), f"case {c}: {lhs} vs {rhs}"
+
+
 @pytest.mark.skipif(not O.have_reference_fd(), reason="reference HypreFDM library not built")
 @pytest.mark.parametrize("bc", [(0.0, 1.0, 0.0, 1.0), (1.0, 0.5, 0.7, 2.0), (1.0, 0.0, 1.0, 0.0)])
 def test_fd_restatement_matches_reference_random(bc):
